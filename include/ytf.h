@@ -1,0 +1,127 @@
+/* ytf.h -- C ABI of libytf, the B200 (sm_100a) implementation of YellowThinFilms'
+ * spectral Green's-function path: per-k-node Berreman mode solve, S-matrix cascade and
+ * cavity transfer maps, Sommerfeld k-quadrature nodes, and the synthesis of
+ * G(ρ, z, z') on a lateral grid.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: YTF_OK (0) or a YTF_ERR_* code; the
+ *     message is in ytf_last_error(ctx). No C++ exception crosses this boundary.
+ *   - Layer indices are 1-based, as in the reference's Julia API (source_layer,
+ *     obs_layers, obs_layer). The last layer is semi-infinite and hosts no source.
+ *   - Complex arrays are interleaved (re, im) doubles. 3x3 tensors are column-major
+ *     (Julia's order). Output G has Julia's Array{ComplexF64,5} layout
+ *     (Nx, Ny, Nz, 3 field components, 3 moments), column-major.
+ *   - Node, weight and coordinate inputs are host pointers (copied). `out` of
+ *     ytf_green is a host pointer unless out_is_device != 0.
+ *   - Calls are synchronous on the context's stream (ytf_ctx_set_stream).
+ *   - One context per host thread; handles are owned by the library and freed by the
+ *     matching *_destroy.
+ *   - Per-node numerical failures are data (valid / Tvalid / status arrays), never
+ *     errors, as in the reference (mod_CavityTransfer.jl:226-251).
+ */
+#ifndef YTF_H
+#define YTF_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ytf_ctx ytf_ctx;
+typedef struct ytf_stack ytf_stack;
+typedef struct ytf_cache ytf_cache;
+
+enum {
+  YTF_OK = 0,
+  YTF_ERR_ARG = 1,   /* argument error; message mirrors the reference's `error(...)` text */
+  YTF_ERR_CUDA = 2,  /* CUDA runtime error (no device, launch failure, ...) */
+  YTF_ERR_NOMEM = 3, /* device allocation failed */
+  YTF_ERR_STATE = 4  /* handle used with the wrong context or kind */
+};
+/* `terms` of closed_form_G (mod_ClosedFormField.jl:143-160) */
+enum { YTF_TERMS_ALL = 0, YTF_TERMS_DIRECT = 1, YTF_TERMS_SCATTERED = 2, YTF_TERMS_TOEPLITZ = 3, YTF_TERMS_HANKEL = 4 };
+/* arithmetic of the synthesis contraction */
+enum { YTF_PREC_FP64 = 0, YTF_PREC_SPLIT_BF16 = 1 };
+/* `rotation` of build_cavity_transfer_2d (mod_CavityTransfer.jl:307-318) */
+enum { YTF_ROT_AUTO = -1, YTF_ROT_OFF = 0, YTF_ROT_ON = 1 };
+/* material kinds (the reference's material TYPES, mod_ModeSolver.jl:28-65) */
+enum { YTF_ISOTROPIC = 0, YTF_UNIAXIAL = 1, YTF_BIAXIAL = 2, YTF_GENERAL = 3 };
+
+int ytf_version(void);
+
+/* Context: one CUDA device and stream, plus the library's reusable device workspace. */
+int ytf_ctx_create(ytf_ctx** out, int device);
+int ytf_ctx_destroy(ytf_ctx* ctx);
+int ytf_ctx_set_stream(ytf_ctx* ctx, void* cuda_stream);
+int ytf_ctx_sync(ytf_ctx* ctx);
+const char* ytf_last_error(const ytf_ctx* ctx);
+
+/* Per-kernel accounting of this library's own launches (no counterpart in the reference;
+ * it serves the measurement). ytf_ctx_profile resets the counters and turns CUDA-event
+ * timing of every launch on the context's stream on or off. ytf_ctx_profile_read
+ * returns, per kernel name (32-byte slots), the summed event time (ms) and the number
+ * of launches since the reset; *n receives the number of distinct kernels. */
+int ytf_ctx_profile(ytf_ctx* ctx, int enable);
+int ytf_ctx_profile_read(ytf_ctx* ctx, int max_entries, char* names, double* total_ms, long* launches, int* n);
+
+/* Stack (replaces Vector{<:AbstractLayer} of FlatOpticalLayer / FlatLayer,
+ * mod_ModeSolver.jl:71-80). eps, mu: nL x 9 complex, column-major 3x3; mu may be NULL
+ * (μ = 1, FlatOpticalLayer); mu_kind may be NULL (isotropic). */
+int ytf_stack_create(ytf_ctx* ctx, int nL, const int* eps_kind, const int* mu_kind, const double* eps,
+                     const double* mu, const double* d, ytf_stack** out);
+int ytf_stack_destroy(ytf_stack* stack);
+
+/* build_cavity_transfer_1d(stack, ω, source_layer, kx_nodes, wt_nodes; obs_layers,
+ * check_symmetry) (mod_CavityTransfer.jl:196-258). obs_layers == NULL means 1:nL. */
+int ytf_transfer_1d(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer, int nk,
+                    const double* kx_nodes, const double* wt_nodes, int nobs, const int* obs_layers,
+                    int check_symmetry, ytf_cache** out);
+
+/* build_cavity_transfer_2d(stack, ω, source_layer, kρ, wρ, φ, wφ; obs_layers, rotation)
+ * (mod_CavityTransfer.jl:307-398). Nodes are (kρ_k, φ_p), flat index k + nkr * p. */
+int ytf_transfer_2d(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer, int nkr,
+                    const double* kr_nodes, const double* kr_weights, int nphi, const double* phi_nodes,
+                    const double* phi_weights, int nobs, const int* obs_layers, int rotation, ytf_cache** out);
+
+int ytf_cache_destroy(ytf_cache* cache);
+
+/* Sizes of a cache: flat node count, obs layers (up to 32), 2D flag, rotation flag. */
+int ytf_cache_info(const ytf_cache* cache, long* n_nodes, int* n_obs, int* obs_layers, int* is2d, int* rotation);
+
+/* valid[k] and Tvalid[o][k] of CavityTransferCache1D/2D (mod_CavityTransfer.jl:160-178),
+ * plus the per-node status bit mask (1 valid, 2 eigen non-convergence, 4 mode-sort
+ * overflow, 8 singular solve, 16 non-finite seeds, 32 non-finite T). Host buffers;
+ * any may be NULL. tvalid is [n_obs][n_nodes]. */
+int ytf_cache_status(ytf_ctx* ctx, const ytf_cache* cache, unsigned char* valid, unsigned char* tvalid,
+                     unsigned char* status);
+
+/* The cache's per-node arrays (CavityTransferCache1D/2D fields T, Qf_src, Qb_src, sf,
+ * sb, basis), host buffers, any may be NULL: T [n_obs][n][4x4 col-major], Qf/Qb [n][2],
+ * sf/sb [n][2x3 col-major], basis [n_obs][n][8 fields x 2 modes] in the order
+ * Exf Eyf Ezf Exb Eyb Ezb KZf KZb. All complex. */
+int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* cache, double* T, double* Qf, double* Qb, double* sf, double* sb,
+                     double* basis);
+
+/* closed_form_G(cache, obs_layer, zsrc_local, z_obs, xs, ys; terms)
+ * (1D: mod_ClosedFormField.jl:435-487; 2D, lateral=:direct: :711-753). out: Nx*Ny*Nz*9
+ * complex, Julia layout. precision: YTF_PREC_FP64 (CUDA-core FP64 contraction) or
+ * YTF_PREC_SPLIT_BF16 (tensor-core contraction, FP32 accumulation). */
+int ytf_green(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, double zsrc_local, int nz, const double* z_obs,
+              int nx, const double* xs, int ny, const double* ys, int terms, int precision, double* out,
+              int out_is_device);
+
+/* FastGaussQuadrature.gausslegendre(n) (used at mod_KxGrid.jl:362): ascending nodes on
+ * [-1, 1] and weights, correctly rounded. */
+int ytf_gauss_legendre(int n, double* x, double* w);
+
+/* gl_rule(panels; order, singular) (mod_KxGrid.jl:361-384), expanded on the device:
+ * composite Gauss-Legendre with the u² substitution on panels that end on a singular
+ * value. nodes/weights: npanels*order, host buffers. Bit-exact with an IEEE-double CPU
+ * evaluation of the same expressions. */
+int ytf_gl_rule(ytf_ctx* ctx, int npanels, const double* pa, const double* pb, int order, int nsing,
+                const double* singular, double* nodes, double* weights);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YTF_H */

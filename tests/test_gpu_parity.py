@@ -1,0 +1,185 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle on identical
+nodes. FP64 synthesis: ≤ 1e-10 relative (norm over the array, the reference's relerr);
+the per-node cache to 1e-9; k-grid construction bit-exact."""
+import numpy as np
+import pytest
+
+from helpers import (FOUNDATION_STACKS, e_free, krho_grid, lay, m_bi, m_gl, m_gyr, m_gyr4, m_uni, m_vac, relerr,
+                     uniform_phi)
+from yellowthinfilms_b200.materials import IsotropicMaterial, UniaxialMaterial
+
+pytestmark = pytest.mark.gpu
+
+W = 2 * np.pi
+
+
+@pytest.fixture(scope="module")
+def ytf():
+    from yellowthinfilms_b200 import api
+    return api
+
+
+def config1_stack(d_air=200.0):
+    """Air / uniaxial film (εo = -3+0.4i, εe = 4+0.2i, 50 nm) / glass 2.25 (nm units)."""
+    return [lay(IsotropicMaterial(1.0), d_air), lay(UniaxialMaterial(-3.0 + 0.4j, 4.0 + 0.2j), 50.0),
+            lay(IsotropicMaterial(2.25), 100.0)]
+
+
+def _cmp_cache(gc, oc, tol=1e-9):
+    g, o = gc.export(), oc.export()
+    vg, tg, _ = gc.status()
+    assert np.array_equal(vg, o["valid"])
+    assert np.array_equal(tg, o["Tvalid"])
+    for key in ("Qf", "Qb"):
+        assert relerr(g[key], o[key]) < tol, key
+    # seeds and T depend on the per-mode normalisation only through a phase; compare
+    # the observable combination T·[sf; sb] per node
+    for i in range(len(gc.obs_layers)):
+        ug = np.einsum("nij,njq->niq", g["T"][i][:, :, :2], g["sf"]) + np.einsum("nij,njq->niq", g["T"][i][:, :, 2:], g["sb"])
+        uo = np.einsum("nij,njq->niq", o["T"][i][:, :, :2], o["sf"]) + np.einsum("nij,njq->niq", o["T"][i][:, :, 2:], o["sb"])
+        eg = np.einsum("nfm,nmq->nfq", g["basis"][i][:, 0:3], ug[:, :2]) + np.einsum("nfm,nmq->nfq", g["basis"][i][:, 3:6], ug[:, 2:])
+        eo = np.einsum("nfm,nmq->nfq", o["basis"][i][:, 0:3], uo[:, :2]) + np.einsum("nfm,nmq->nfq", o["basis"][i][:, 3:6], uo[:, 2:])
+        assert relerr(eg, eo) < tol
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_transfer_1d_cache_matches_oracle(ytf, oracle, idx):
+    _, st = FOUNDATION_STACKS[idx]
+    kx, wt = krho_grid(st, W, kmax=15.0)
+    for src in range(1, len(st)):
+        gc = ytf.build_cavity_transfer_1d(st, W, src, kx, wt)
+        oc = oracle.build_cavity_transfer_1d(st, W, src, kx, wt)
+        _cmp_cache(gc, oc)
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_green_1d_matches_oracle(ytf, oracle, idx):
+    _, st = FOUNDATION_STACKS[idx]
+    kx, wt = krho_grid(st, W, kmax=15.0)
+    xs = np.array([-0.3, 0.0, 0.2, 0.45])
+    ys = np.array([0.0, 0.15, -0.25])
+    N = len(st)
+    for src in range(1, N):
+        gc = ytf.build_cavity_transfer_1d(st, W, src, kx, wt)
+        oc = oracle.build_cavity_transfer_1d(st, W, src, kx, wt)
+        zs = 0.4 * st[src - 1].d
+        for obs in range(1, N + 1):
+            d = st[obs - 1].d
+            zo = [0.1 * d, 0.4 * d, 0.75 * d] if obs != src else [0.05 * d, 0.4 * d, 0.95 * d]
+            terms_list = ["all", "scattered", "direct", "toeplitz", "hankel"] if obs == src else ["all"]
+            for terms in terms_list:
+                G = ytf.closed_form_G(gc, obs, zs, zo, xs, ys, terms=terms)
+                Go = oracle.closed_form_G(oc, obs, zs, zo, xs, ys, terms=terms)
+                assert G.shape == (4, 3, 3, 3, 3)
+                assert relerr(G, Go) < 1e-10, (src, obs, terms, relerr(G, Go))
+
+
+def test_config1_gzz_1d_matches_oracle(ytf, oracle):
+    """Vertical dipole 20 nm above the uniaxial film, real-axis GL panels to 20 k0."""
+    st = config1_stack()
+    k0 = 2 * np.pi / 600.0
+    panels = [(20 * k0 * i / 128, 20 * k0 * (i + 1) / 128) for i in range(128)]
+    kx, wt = oracle.gl_rule(panels, 8)
+    gc = ytf.build_cavity_transfer_1d(st, k0, 1, kx, wt, obs_layers=[1])
+    oc = oracle.build_cavity_transfer_1d(st, k0, 1, kx, wt, obs_layers=[1])
+    rho = np.geomspace(6.0, 3000.0, 32)
+    zo = np.linspace(0.0, 200.0, 9)
+    zsrc = 20.0  # local height above the 1/2 interface
+    G = ytf.closed_form_G(gc, 1, zsrc, zo, rho, [0.0])
+    Go = oracle.closed_form_G(oc, 1, zsrc, zo, rho, [0.0])
+    assert relerr(G[..., 2, 2], Go[..., 2, 2]) < 1e-10
+    assert relerr(G, Go) < 1e-10
+
+
+@pytest.mark.parametrize("idx", [3, 4])
+def test_transfer_2d_full_solve_matches_oracle(ytf, oracle, idx):
+    """Biaxial and gyrotropic stacks: the general 4x4 eigen path on the device."""
+    _, st = FOUNDATION_STACKS[idx]
+    kr, wr = krho_grid(st, W, kmax=10.0, width=1.0)
+    ph, wp = uniform_phi(8)
+    for src in (1, 2):
+        gc = ytf.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp)
+        oc = oracle.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp)
+        _cmp_cache(gc, oc, tol=1e-8)
+        xs = np.array([-0.2, 0.0, 0.3])
+        for obs in range(1, len(st) + 1):
+            d = st[obs - 1].d
+            zo = [0.2 * d, 0.7 * d]
+            G = ytf.closed_form_G(gc, obs, 0.3 * st[src - 1].d, zo, xs, xs)
+            Go = oracle.closed_form_G(oc, obs, 0.3 * st[src - 1].d, zo, xs, xs)
+            assert relerr(G, Go) < 1e-9, (src, obs, relerr(G, Go))
+
+
+def test_transfer_2d_rotation_fill_matches_oracle(ytf, oracle):
+    st = [lay(m_vac, 1.0), lay(m_uni, 0.8), lay(m_gl, 0.5), lay(m_vac, 1.0)]
+    kr, wr = krho_grid(st, W, kmax=12.0, width=1.0)
+    ph, wp = uniform_phi(12)
+    gc = ytf.build_cavity_transfer_2d(st, W, 2, kr, wr, ph, wp)
+    assert gc.rotation
+    oc = oracle.build_cavity_transfer_2d(st, W, 2, kr, wr, ph, wp)
+    _cmp_cache(gc, oc)
+    gf = ytf.build_cavity_transfer_2d(st, W, 2, kr, wr, ph, wp, rotation=False)
+    xs = np.array([-0.2, 0.1, 0.3])
+    for obs in (1, 2, 3, 4):
+        d = st[obs - 1].d
+        G = ytf.closed_form_G(gc, obs, 0.35, [0.3 * d], xs, xs)
+        assert relerr(G, oracle.closed_form_G(oc, obs, 0.35, [0.3 * d], xs, xs)) < 1e-10
+        assert relerr(G, ytf.closed_form_G(gf, obs, 0.35, [0.3 * d], xs, xs)) < 1e-10
+
+
+def test_free_space_dipole_on_gpu(ytf, oracle):
+    """Absolute normalization on the device (Gz_ClosedForm_Point_Validation.jl [f])."""
+    for omega in (2 * np.pi, 1.0):
+        ef = 1.0 + 1e-4j
+        st = [lay(IsotropicMaterial(ef), 3.0) for _ in range(3)]
+        kx, wt, _ = oracle.fixed_grid_1d(st, omega, 2, h_min=0.025, rho_max=1.0, scan=False, rtol=1e-10)
+        Gref = np.stack([e_free(np.array([0.4, 0, 0.7]), np.eye(3)[q].astype(complex), omega * np.sqrt(ef), ef)
+                         for q in range(3)], axis=1)
+        G1 = ytf.closed_form_G(ytf.build_cavity_transfer_1d(st, omega, 2, kx, wt), 2, 1.0, [1.7], [0.4], [0.0])[0, 0, 0]
+        assert relerr(G1, Gref) < 1e-7
+
+
+def test_gl_rule_bitexact_with_oracle(ytf, oracle):
+    rng = np.random.default_rng(7)
+    brk = np.sort(rng.uniform(0, 50, 40))
+    panels = list(zip(brk[:-1], brk[1:]))
+    sing = [brk[5], brk[17], brk[30]]
+    for order in (8, 12):
+        n, w = ytf.gl_rule(panels, order, sing)
+        no, wo = oracle.gl_rule(panels, order, sing)
+        assert np.array_equal(n, no) and np.array_equal(w, wo)
+
+
+def test_argument_errors_match_reference_messages(ytf):
+    st = [lay(m_vac, 1.0), lay(m_bi, 0.7), lay(m_vac, 1.0)]
+    with pytest.raises(ytf.YTFError, match="source_layer=3 must be in 1:2"):
+        ytf.build_cavity_transfer_1d(st, W, 3, [1.0], [1.0], check_symmetry=False)
+    with pytest.raises(ytf.YTFError, match="requires an isotropic/uniaxial stack"):
+        ytf.build_cavity_transfer_1d(st, W, 1, [1.0], [1.0])
+    with pytest.raises(ytf.YTFError, match="rotation=true requires an azimuthally symmetric stack"):
+        ytf.build_cavity_transfer_2d(st, W, 1, [1.0], [1.0], [0.0], [1.0], rotation=True)
+    c = ytf.build_cavity_transfer_1d([lay(m_vac, 1.0), lay(m_gl, 0.7), lay(m_vac, 1.0)], W, 2, [1.0, 2.0], [0.5, 0.5],
+                                     obs_layers=[2, 3])
+    with pytest.raises(ytf.YTFError, match="not in this cache's obs_layers"):
+        ytf.closed_form_G(c, 1, 0.3, [0.5], [0.0], [0.0])
+    with pytest.raises(ytf.YTFError, match="terms needs obs_layer == source_layer"):
+        ytf.closed_form_G(c, 3, 0.3, [0.5], [0.0], [0.0], terms="toeplitz")
+    with pytest.raises(ytf.YTFError, match="outside"):
+        ytf.closed_form_G(c, 2, 0.9, [0.5], [0.0], [0.0])
+
+
+def test_empty_and_single_node_inputs(ytf, oracle):
+    st = [lay(m_vac, 1.0), lay(m_gl, 0.7), lay(m_vac, 1.0)]
+    c0 = ytf.build_cavity_transfer_1d(st, W, 2, [], [])
+    G0 = ytf.closed_form_G(c0, 2, 0.3, [0.5], [0.1], [0.0])
+    assert G0.shape == (1, 1, 1, 3, 3) and np.all(G0 == 0)
+    c1 = ytf.build_cavity_transfer_1d(st, W, 2, [3.0], [0.25])
+    o1 = oracle.build_cavity_transfer_1d(st, W, 2, [3.0], [0.25])
+    assert relerr(ytf.closed_form_G(c1, 1, 0.3, [0.5], [0.1], [0.2]),
+                  oracle.closed_form_G(o1, 1, 0.3, [0.5], [0.1], [0.2])) < 1e-12
+    # ρ = 0 exactly and a ragged lateral grid
+    xs = np.array([0.0, 0.05, 0.3]); ys = np.array([0.0])
+    kx, wt = krho_grid(st, W, kmax=10.0)
+    c = ytf.build_cavity_transfer_1d(st, W, 2, kx, wt)
+    o = oracle.build_cavity_transfer_1d(st, W, 2, kx, wt)
+    assert relerr(ytf.closed_form_G(c, 2, 0.3, [0.2, 0.5], xs, ys), oracle.closed_form_G(o, 2, 0.3, [0.2, 0.5], xs, ys)) < 1e-10

@@ -1,0 +1,64 @@
+"""ctypes binding of libytf.so (the C ABI of include/ytf.h).
+
+There is no CPU fallback: if the library is missing or no CUDA device is present the
+calls raise. Build it with ``python -m yellowthinfilms_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libytf.so")
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.POINTER(ctypes.c_int)
+_u8 = ctypes.POINTER(ctypes.c_ubyte)
+_vp = ctypes.c_void_p
+
+# name -> (restype, argtypes); every symbol include/ytf.h declares
+SIGNATURES = {
+    "ytf_version": (ctypes.c_int, []),
+    "ytf_ctx_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int]),
+    "ytf_ctx_destroy": (ctypes.c_int, [_vp]),
+    "ytf_ctx_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "ytf_ctx_sync": (ctypes.c_int, [_vp]),
+    "ytf_last_error": (ctypes.c_char_p, [_vp]),
+    "ytf_ctx_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "ytf_ctx_profile_read": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_char_p, _d, ctypes.POINTER(ctypes.c_long), _i]),
+    "ytf_stack_create": (ctypes.c_int, [_vp, ctypes.c_int, _i, _i, _d, _d, _d, ctypes.POINTER(_vp)]),
+    "ytf_stack_destroy": (ctypes.c_int, [_vp]),
+    "ytf_transfer_1d": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _d, _d, ctypes.c_int, _i,
+                                       ctypes.c_int, ctypes.POINTER(_vp)]),
+    "ytf_transfer_2d": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _d, _d, ctypes.c_int, _d, _d,
+                                       ctypes.c_int, _i, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "ytf_cache_destroy": (ctypes.c_int, [_vp]),
+    "ytf_cache_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_long), _i, _i, _i, _i]),
+    "ytf_cache_status": (ctypes.c_int, [_vp, _vp, _u8, _u8, _u8]),
+    "ytf_cache_export": (ctypes.c_int, [_vp, _vp, _d, _d, _d, _d, _d, _d]),
+    "ytf_green": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _d, ctypes.c_int, _d, ctypes.c_int,
+                                 _d, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int]),
+    "ytf_gauss_legendre": (ctypes.c_int, [ctypes.c_int, _d, _d]),
+    "ytf_gl_rule": (ctypes.c_int, [_vp, ctypes.c_int, _d, _d, ctypes.c_int, ctypes.c_int, _d, _d, _d]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libytf.so once; raise if it is absent (no silent fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libytf.so not found at {LIB_PATH}: build it with `python -m yellowthinfilms_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def ptr(a, t=_d):
+    return None if a is None else a.ctypes.data_as(t)

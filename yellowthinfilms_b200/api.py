@@ -1,0 +1,302 @@
+"""Python host API with the reference's names and argument meanings.
+
+Mirrors the Julia entry points this library replaces:
+  build_cavity_transfer_1d  (mod_CavityTransfer.jl:196-258)
+  build_cavity_transfer_2d  (mod_CavityTransfer.jl:307-398)
+  closed_form_G             (mod_ClosedFormField.jl:435-487, 711-753; lateral=:direct)
+  gl_rule, halve_panels, build_kphi_grid, gausslegendre (mod_KxGrid.jl:361-394)
+Layer indices are 1-based; G comes back as an (Nx, Ny, Nz, 3, 3) complex array indexed
+G[x, y, z, field component, moment], exactly as the reference's Array{ComplexF64,5}.
+
+Every call runs on the GPU through libytf.so; argument errors raise YTFError with the
+reference's message text.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native
+from ._native import _i, _u8, lib, ptr
+from .materials import stack_arrays
+
+TERMS = {"all": 0, "direct": 1, "scattered": 2, "toeplitz": 3, "hankel": 4}
+PRECISION = {"fp64": 0, "split_bf16": 1}
+
+
+class YTFError(ValueError):
+    """An argument error reported by libytf (the reference raises `error(...)` there)."""
+
+
+class Context:
+    """A libytf context: one CUDA device and the stream its calls run on."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        rc = lib().ytf_ctx_create(ctypes.byref(h), int(device))
+        if rc != 0:
+            raise RuntimeError(f"ytf_ctx_create(device={device}) failed with code {rc}: no usable CUDA device")
+        self.h = h
+        self.device = device
+
+    def set_stream(self, cuda_stream: int) -> None:
+        lib().ytf_ctx_set_stream(self.h, ctypes.c_void_p(int(cuda_stream)))
+
+    def sync(self) -> None:
+        self.check(lib().ytf_ctx_sync(self.h))
+
+    def error(self) -> str:
+        return lib().ytf_last_error(self.h).decode()
+
+    def profile(self, enable: bool = True) -> None:
+        """Reset the per-kernel counters; time every launch with CUDA events if enabled."""
+        self.check(lib().ytf_ctx_profile(self.h, int(bool(enable))))
+
+    def profile_read(self) -> dict:
+        """{kernel name: (summed event ms, launches)} since the last profile() call."""
+        n = ctypes.c_int(0)
+        self.check(lib().ytf_ctx_profile_read(self.h, 0, None, None, None, ctypes.byref(n)))
+        m = max(n.value, 1)
+        names = ctypes.create_string_buffer(32 * m)
+        ms = np.zeros(m)
+        launches = np.zeros(m, dtype=np.int64)
+        self.check(lib().ytf_ctx_profile_read(self.h, m, names, ptr(ms), launches.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_long)), ctypes.byref(n)))
+        raw = names.raw
+        return {raw[32 * i:32 * i + 32].split(b"\0")[0].decode(): (float(ms[i]), int(launches[i])) for i in range(n.value)}
+
+    def check(self, rc: int) -> None:
+        if rc == 0:
+            return
+        msg = self.error()
+        if rc == 1:
+            raise YTFError(msg)
+        raise RuntimeError(f"libytf error {rc}: {msg}")
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and _native._lib is not None:
+            _native._lib.ytf_ctx_destroy(self.h)
+            self.h = None
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class Stack:
+    """A stack uploaded to the device (layers of FlatOpticalLayer / FlatLayer)."""
+
+    def __init__(self, layers, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.layers = list(layers)
+        ek, mk, eps, mu, d = stack_arrays(self.layers)
+        self._keep = (ek, mk, eps, mu, d)
+        h = ctypes.c_void_p()
+        rc = lib().ytf_stack_create(self.ctx.h, len(self.layers), ptr(ek, _i), ptr(mk, _i), ptr(eps.view(np.float64)),
+                                    ptr(mu.view(np.float64)), ptr(d), ctypes.byref(h))
+        self.ctx.check(rc)
+        self.h = h
+
+    def __len__(self):
+        return len(self.layers)
+
+    def __getitem__(self, i):
+        return self.layers[i]
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and _native._lib is not None:
+            _native._lib.ytf_stack_destroy(self.h)
+            self.h = None
+
+
+def _as_stack(stack, ctx) -> Stack:
+    if isinstance(stack, Stack):
+        return stack
+    return Stack(stack, ctx)
+
+
+class _Cache:
+    is2d = False
+
+    def __init__(self, h, stack: Stack, omega, source_layer):
+        self.h, self.stack, self.ctx = h, stack, stack.ctx
+        self.omega, self.source_layer = float(omega), int(source_layer)
+        n = ctypes.c_long()
+        no = ctypes.c_int()
+        obs = (ctypes.c_int * 32)()
+        is2d = ctypes.c_int()
+        rot = ctypes.c_int()
+        lib().ytf_cache_info(h, ctypes.byref(n), ctypes.byref(no), obs, ctypes.byref(is2d), ctypes.byref(rot))
+        self.n = int(n.value)
+        self.obs_layers = [int(obs[i]) for i in range(no.value)]
+        self.rotation = bool(rot.value)
+        self.d_src = float(stack.layers[source_layer - 1].d)
+        self.d_obs = {o: float(stack.layers[o - 1].d) for o in self.obs_layers}
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and _native._lib is not None:
+            _native._lib.ytf_cache_destroy(self.h)
+            self.h = None
+
+    def status(self):
+        """(valid[n], Tvalid[n_obs, n], status bits[n]) as numpy arrays."""
+        n, no = self.n, len(self.obs_layers)
+        valid = np.zeros(n, np.uint8)
+        tvalid = np.zeros(no * n, np.uint8)
+        st = np.zeros(n, np.uint8)
+        self.ctx.check(lib().ytf_cache_status(self.ctx.h, self.h, ptr(valid, _u8), ptr(tvalid, _u8), ptr(st, _u8)))
+        return valid.astype(bool), tvalid.reshape(no, n).astype(bool), st
+
+    @property
+    def valid(self):
+        return self.status()[0]
+
+    @property
+    def Tvalid(self):
+        v = self.status()[1]
+        return {o: v[i] for i, o in enumerate(self.obs_layers)}
+
+    def export(self):
+        """The cache's per-node arrays (T, Qf_src, Qb_src, sf, sb, basis) as numpy."""
+        n, no = self.n, len(self.obs_layers)
+        T = np.zeros(no * n * 32)
+        Qf = np.zeros(4 * n)
+        Qb = np.zeros(4 * n)
+        sf = np.zeros(12 * n)
+        sb = np.zeros(12 * n)
+        basis = np.zeros(no * n * 32)
+        self.ctx.check(lib().ytf_cache_export(self.ctx.h, self.h, ptr(T), ptr(Qf), ptr(Qb), ptr(sf), ptr(sb), ptr(basis)))
+        c = lambda x: x.view(np.complex128)
+        return dict(T=c(T).reshape(no, n, 4, 4).transpose(0, 1, 3, 2), Qf=c(Qf).reshape(n, 2), Qb=c(Qb).reshape(n, 2),
+                    sf=c(sf).reshape(n, 3, 2).transpose(0, 2, 1), sb=c(sb).reshape(n, 3, 2).transpose(0, 2, 1),
+                    basis=c(basis).reshape(no, n, 8, 2))
+
+
+class CavityTransferCache1D(_Cache):
+    """Device-resident CavityTransferCache1D (mod_CavityTransfer.jl:160-178)."""
+
+    def __init__(self, h, stack, omega, source_layer, kx, wt):
+        super().__init__(h, stack, omega, source_layer)
+        self.kx_nodes, self.wt_nodes = kx, wt
+
+
+class CavityTransferCache2D(_Cache):
+    """Device-resident CavityTransferCache2D (mod_CavityTransfer.jl:273-294)."""
+    is2d = True
+
+    def __init__(self, h, stack, omega, source_layer, kr, wr, phi, wphi):
+        super().__init__(h, stack, omega, source_layer)
+        self.kr_nodes, self.kr_weights, self.phi_nodes, self.phi_weights = kr, wr, phi, wphi
+
+
+def _f64(x):
+    return np.ascontiguousarray(np.atleast_1d(np.asarray(x, dtype=np.float64)))
+
+
+def _obs_arg(obs_layers):
+    if obs_layers is None:
+        return 0, None
+    a = np.ascontiguousarray(np.asarray(list(obs_layers), dtype=np.int32))
+    return len(a), a
+
+
+def build_cavity_transfer_1d(stack, omega, source_layer, kx_nodes, wt_nodes, obs_layers=None, check_symmetry=True,
+                             ctx: Optional[Context] = None) -> CavityTransferCache1D:
+    st = _as_stack(stack, ctx)
+    kx, wt = _f64(kx_nodes), _f64(wt_nodes)
+    if len(kx) != len(wt):
+        raise YTFError("build_cavity_transfer_1d: kx_nodes/wt_nodes length mismatch")
+    no, ob = _obs_arg(obs_layers)
+    h = ctypes.c_void_p()
+    rc = lib().ytf_transfer_1d(st.ctx.h, st.h, float(omega), int(source_layer), len(kx), ptr(kx), ptr(wt), no, ptr(ob, _i),
+                               int(bool(check_symmetry)), ctypes.byref(h))
+    st.ctx.check(rc)
+    return CavityTransferCache1D(h, st, omega, source_layer, kx, wt)
+
+
+def build_cavity_transfer_2d(stack, omega, source_layer, kr_nodes, kr_weights, phi_nodes, phi_weights, obs_layers=None,
+                             rotation="auto", ctx: Optional[Context] = None) -> CavityTransferCache2D:
+    st = _as_stack(stack, ctx)
+    kr, wr, ph, wp = _f64(kr_nodes), _f64(kr_weights), _f64(phi_nodes), _f64(phi_weights)
+    if len(kr) != len(wr):
+        raise YTFError("build_cavity_transfer_2d: kρ nodes/weights length mismatch")
+    if len(ph) != len(wp):
+        raise YTFError("build_cavity_transfer_2d: φ nodes/weights length mismatch")
+    rot = -1 if rotation == "auto" else int(bool(rotation))
+    no, ob = _obs_arg(obs_layers)
+    h = ctypes.c_void_p()
+    rc = lib().ytf_transfer_2d(st.ctx.h, st.h, float(omega), int(source_layer), len(kr), ptr(kr), ptr(wr), len(ph), ptr(ph),
+                               ptr(wp), no, ptr(ob, _i), rot, ctypes.byref(h))
+    st.ctx.check(rc)
+    return CavityTransferCache2D(h, st, omega, source_layer, kr, wr, ph, wp)
+
+
+def closed_form_G(cache: _Cache, obs_layer: int, zsrc_local: float, z_obs, xs, ys, terms: str = "all",
+                  precision: str = "fp64", out=None):
+    """G[x, y, z, component, moment] of a point source (terms as the reference).
+
+    ``out``: optional torch tensor (complex128, Nx*Ny*Nz*9 elements, Julia order) to write
+    into instead of returning a new host array: a CUDA tensor (G stays on the device) or
+    a pinned host tensor (G is copied back inside the call).
+    """
+    if terms not in TERMS:
+        raise YTFError(f"closed_form_G: terms must be :all, :direct, :scattered, :toeplitz or :hankel (got :{terms})")
+    zo, x, y = _f64(z_obs), _f64(xs), _f64(ys)
+    nx, ny, nz = len(x), len(y), len(zo)
+    ctx = cache.ctx
+    if out is not None:
+        if out.numel() != nx * ny * nz * 9:
+            raise YTFError("closed_form_G: out has the wrong size")
+        on_dev = int(bool(getattr(out, "is_cuda", False)))
+        rc = lib().ytf_green(ctx.h, cache.h, int(obs_layer), float(zsrc_local), nz, ptr(zo), nx, ptr(x), ny, ptr(y),
+                             TERMS[terms], PRECISION[precision], ctypes.c_void_p(out.data_ptr()), on_dev)
+        ctx.check(rc)
+        return out
+    G = np.zeros(2 * 9 * nz * nx * ny)
+    rc = lib().ytf_green(ctx.h, cache.h, int(obs_layer), float(zsrc_local), nz, ptr(zo), nx, ptr(x), ny, ptr(y),
+                         TERMS[terms], PRECISION[precision], G.ctypes.data_as(ctypes.c_void_p), 0)
+    ctx.check(rc)
+    return G.view(np.complex128).reshape(3, 3, nz, ny, nx).transpose(4, 3, 2, 1, 0)
+
+
+def gausslegendre(n: int):
+    x = np.zeros(n)
+    w = np.zeros(n)
+    if lib().ytf_gauss_legendre(int(n), ptr(x), ptr(w)) != 0:
+        raise YTFError("gausslegendre: n must be ≥ 1")
+    return x, w
+
+
+def gl_rule(panels: Sequence, order: int = 8, singular=(), ctx: Optional[Context] = None):
+    """Composite Gauss–Legendre rule on `panels` (mod_KxGrid.jl:361-384), on the device."""
+    ctx = ctx or default_context()
+    pa = _f64([p[0] for p in panels]) if len(panels) else np.zeros(0)
+    pb = _f64([p[1] for p in panels]) if len(panels) else np.zeros(0)
+    s = _f64(list(singular)) if len(singular) else np.zeros(1)
+    nodes = np.zeros(len(panels) * order)
+    wts = np.zeros(len(panels) * order)
+    ctx.check(lib().ytf_gl_rule(ctx.h, len(panels), ptr(pa), ptr(pb), int(order), len(singular), ptr(s), ptr(nodes),
+                                ptr(wts)))
+    return nodes, wts
+
+
+def halve_panels(panels):
+    """`panels` with every panel split in two (mod_KxGrid.jl:387-388)."""
+    out = []
+    for a, b in panels:
+        m = (a + b) / 2
+        out += [(float(a), m), (m, float(b))]
+    return out
+
+
+def build_kphi_grid(N_phi: int):
+    """Uniform trapezoid in φ (mod_KxGrid.jl:390-394)."""
+    return np.array([2 * np.pi * p / N_phi for p in range(N_phi)]), np.full(N_phi, 2 * np.pi / N_phi)

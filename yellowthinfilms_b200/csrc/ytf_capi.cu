@@ -1,0 +1,815 @@
+// ytf_capi.cu -- the C ABI of libytf (include/ytf.h): handles, argument checks with the
+// reference's error messages, device workspace, and the host-side orchestration of the
+// transfer and synthesis kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <set>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/ytf.h"
+#include "ytf_kernels.h"
+
+using namespace ytf;
+
+struct ProfSpan {
+  const char* name;
+  cudaEvent_t a, b;
+};
+
+struct ytf_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::map<std::string, std::pair<void*, size_t>> ws;  // grow-only device workspace
+  std::multimap<size_t, void*> pool;                   // released cache blocks, by size
+  int refs = 0;                                        // live stacks and caches
+  bool closing = false;
+  // per-kernel accounting: launches always, CUDA-event time when profiling is on
+  bool prof = false;
+  std::vector<ProfSpan> spans;
+  std::vector<cudaEvent_t> free_events;
+  std::map<std::string, std::pair<double, long>> ktime;  // name -> (ms, timed launches)
+  std::map<std::string, long> klaunch;                   // name -> launches
+  ~ytf_ctx() {
+    for (auto& kv : ws) cudaFree(kv.second.first);
+    for (auto& kv : pool) cudaFree(kv.second);
+    for (auto& sp : spans) { cudaEventDestroy(sp.a); cudaEventDestroy(sp.b); }
+    for (auto e : free_events) cudaEventDestroy(e);
+  }
+};
+
+struct ytf_stack {
+  ytf_ctx* ctx;
+  int nL;
+  std::vector<LayerDev> host;
+  LayerDev* dev = nullptr;
+};
+
+struct ytf_cache {
+  ytf_ctx* ctx;
+  const ytf_stack* stack_ref = nullptr;
+  int nL, src, nobs;
+  int obs[MAXL];
+  bool is2d = false, rotation = false;
+  int Nk = 0, Np = 1;
+  long n = 0;
+  double omega = 0, d_src = 0;
+  std::vector<double> kr, wr, phi, wphi, d_layer;
+  void* block = nullptr;  // one device allocation for every array below
+  size_t block_bytes = 0;
+  double *d_kr = nullptr, *d_wr = nullptr, *d_phi = nullptr, *d_wphi = nullptr;
+  uint8_t *d_status = nullptr, *d_valid = nullptr, *d_tvalid = nullptr;
+  double2 *d_T = nullptr, *d_Qf = nullptr, *d_Qb = nullptr, *d_sf = nullptr, *d_sb = nullptr, *d_basis = nullptr;
+  int oidx(int o) const {
+    for (int i = 0; i < nobs; ++i)
+      if (obs[i] == o) return i;
+    return -1;
+  }
+};
+
+namespace {
+
+int fail(ytf_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) return fail(ctx, YTF_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+cudaEvent_t take_event(ytf_ctx* ctx) {
+  if (!ctx->free_events.empty()) {
+    cudaEvent_t e = ctx->free_events.back();
+    ctx->free_events.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// launch one kernel through `f`, counting it and (when profiling) bracketing it with
+// CUDA events on the context's stream
+template <class F>
+cudaError_t launch_named(ytf_ctx* ctx, const char* name, F&& f) {
+  ctx->klaunch[name] += 1;
+  if (!ctx->prof) return f();
+  ProfSpan sp{name, take_event(ctx), take_event(ctx)};
+  cudaEventRecord(sp.a, ctx->stream);
+  cudaError_t e = f();
+  cudaEventRecord(sp.b, ctx->stream);
+  ctx->spans.push_back(sp);
+  return e;
+}
+#define LAUNCH(name, expr) launch_named(ctx, name, [&]() { return (expr); })
+
+// fold completed spans into the per-kernel totals (the stream has been synchronised)
+void prof_collect(ytf_ctx* ctx) {
+  for (auto& sp : ctx->spans) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, sp.a, sp.b) == cudaSuccess) {
+      auto& t = ctx->ktime[sp.name];
+      t.first += ms;
+      t.second += 1;
+    }
+    ctx->free_events.push_back(sp.a);
+    ctx->free_events.push_back(sp.b);
+  }
+  ctx->spans.clear();
+}
+
+void ctx_release(ytf_ctx* ctx) {
+  if (--ctx->refs <= 0 && ctx->closing) delete ctx;
+}
+
+void* ws_get(ytf_ctx* ctx, const char* name, size_t bytes, cudaError_t* e) {
+  *e = cudaSuccess;
+  if (bytes == 0) bytes = 16;
+  auto it = ctx->ws.find(name);
+  if (it != ctx->ws.end() && it->second.second >= bytes) return it->second.first;
+  if (it != ctx->ws.end()) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(it->second.first);
+    ctx->ws.erase(it);
+  }
+  void* p = nullptr;
+  *e = cudaMalloc(&p, bytes);
+  if (*e != cudaSuccess) return nullptr;
+  ctx->ws[name] = {p, bytes};
+  return p;
+}
+
+#define WS(ptr, type, name, count)                                                                           \
+  type* ptr = nullptr;                                                                                       \
+  {                                                                                                          \
+    cudaError_t e_;                                                                                          \
+    ptr = (type*)ws_get(ctx, name, sizeof(type) * (size_t)(count), &e_);                                     \
+    if (!ptr) return fail(ctx, YTF_ERR_NOMEM, std::string("workspace ") + name + ": " + cudaGetErrorString(e_)); \
+  }
+
+std::string obs_str(const int* obs, int n) {
+  std::string s = "[";
+  for (int i = 0; i < n; ++i) s += (i ? ", " : "") + std::to_string(obs[i]);
+  return s + "]";
+}
+
+bool closed_form(const LayerDev& L) { return (L.ekind == 0 || L.ekind == 1) && L.mkind == 0; }
+
+int upload(ytf_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  return YTF_OK;
+}
+
+// allocate the cache's arrays in one block
+int alloc_cache(ytf_ctx* ctx, ytf_cache* c) {
+  long n = c->n;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  size_t o_kr = take(8 * c->kr.size()), o_wr = take(8 * c->wr.size()), o_phi = take(8 * std::max<size_t>(1, c->phi.size())),
+         o_wphi = take(8 * std::max<size_t>(1, c->wphi.size()));
+  size_t o_status = take(n), o_valid = take(n), o_tvalid = take((size_t)n * c->nobs);
+  size_t o_T = take(16 * 16 * (size_t)n * c->nobs), o_Qf = take(16 * 2 * (size_t)n), o_Qb = take(16 * 2 * (size_t)n);
+  size_t o_sf = take(16 * 6 * (size_t)n), o_sb = take(16 * 6 * (size_t)n), o_basis = take(16 * 16 * (size_t)n * c->nobs);
+  c->block_bytes = off;
+  auto it = ctx->pool.lower_bound(off);
+  if (it != ctx->pool.end() && it->first <= 2 * off + (size_t(1) << 20)) {
+    c->block = it->second;
+    c->block_bytes = it->first;
+    ctx->pool.erase(it);
+  } else {
+    CK(cudaMalloc(&c->block, off));
+  }
+  char* b = (char*)c->block;
+  c->d_kr = (double*)(b + o_kr); c->d_wr = (double*)(b + o_wr);
+  c->d_phi = (double*)(b + o_phi); c->d_wphi = (double*)(b + o_wphi);
+  c->d_status = (uint8_t*)(b + o_status); c->d_valid = (uint8_t*)(b + o_valid); c->d_tvalid = (uint8_t*)(b + o_tvalid);
+  c->d_T = (double2*)(b + o_T); c->d_Qf = (double2*)(b + o_Qf); c->d_Qb = (double2*)(b + o_Qb);
+  c->d_sf = (double2*)(b + o_sf); c->d_sb = (double2*)(b + o_sb); c->d_basis = (double2*)(b + o_basis);
+  CK(cudaMemsetAsync(c->block, 0, off, ctx->stream));
+  (void)o_status;
+  int rc;
+  if ((rc = upload(ctx, c->d_kr, c->kr.data(), 8 * c->kr.size()))) return rc;
+  if ((rc = upload(ctx, c->d_wr, c->wr.data(), 8 * c->wr.size()))) return rc;
+  if (!c->phi.empty()) {
+    if ((rc = upload(ctx, c->d_phi, c->phi.data(), 8 * c->phi.size()))) return rc;
+    if ((rc = upload(ctx, c->d_wphi, c->wphi.data(), 8 * c->wphi.size()))) return rc;
+  }
+  return YTF_OK;
+}
+
+// which SLeft/SRight slots the walk to the observation layers reads (k_chain)
+void need_masks(int N, int src, const int* obs, int nobs, uint32_t& needL, uint32_t& needR) {
+  needL = needR = 0;
+  for (int i = 0; i < nobs; ++i) {
+    int o = obs[i];
+    if (o < src) {
+      for (int k : {o, o + 1})
+        if (k >= 2 && k <= src - 1) needL |= 1u << (k - 1);
+    } else if (o > src) {
+      for (int k : {o, o + 1})
+        if (k >= src + 1 && k <= N - 1) needR |= 1u << (k - 1);
+    }
+  }
+}
+
+int common_checks(ytf_ctx* ctx, const ytf_stack* st, const char* fn, int src, int nobs, const int* obs_in, std::vector<int>& obs) {
+  if (!ctx) return YTF_ERR_ARG;
+  if (!st) return fail(ctx, YTF_ERR_ARG, std::string(fn) + ": stack is NULL");
+  if (st->ctx != ctx) return fail(ctx, YTF_ERR_STATE, std::string(fn) + ": stack belongs to another context");
+  int N = st->nL;
+  if (!(1 <= src && src < N))
+    return fail(ctx, YTF_ERR_ARG, std::string(fn) + ": source_layer=" + std::to_string(src) + " must be in 1:" +
+                                      std::to_string(N - 1) + " (the last, semi-infinite layer cannot host a source).");
+  std::set<int> os;
+  if (obs_in == nullptr || nobs <= 0) {
+    for (int o = 1; o <= N; ++o) os.insert(o);
+  } else {
+    for (int i = 0; i < nobs; ++i) os.insert(obs_in[i]);
+  }
+  for (int o : os)
+    if (o < 1 || o > N) return fail(ctx, YTF_ERR_ARG, std::string(fn) + ": obs_layers out of range 1:" + std::to_string(N));
+  obs.assign(os.begin(), os.end());
+  if ((int)obs.size() > MAXL) return fail(ctx, YTF_ERR_ARG, std::string(fn) + ": too many obs layers");
+  return YTF_OK;
+}
+
+void fill_params(TransferParams& p, const ytf_stack* st, const ytf_cache* c) {
+  std::memset(&p, 0, sizeof(p));
+  p.layers = st->dev;
+  p.nL = st->nL;
+  p.src = c->src;
+  p.nobs = c->nobs;
+  for (int i = 0; i < c->nobs; ++i) p.obs[i] = c->obs[i];
+  need_masks(st->nL, c->src, c->obs, c->nobs, p.needL, p.needR);
+  p.omega = c->omega;
+  p.Nk = c->Nk;
+  p.Np = c->Np;
+  p.kr = c->d_kr;
+  p.phi = c->d_phi;
+  p.status = c->d_status;
+  p.valid = c->d_valid;
+  p.tvalid = c->d_tvalid;
+  p.Tout = c->d_T;
+  p.Qf = c->d_Qf;
+  p.Qb = c->d_Qb;
+  p.sf = c->d_sf;
+  p.sb = c->d_sb;
+  p.basis = c->d_basis;
+}
+
+// per-node scratch bytes of the transfer kernels
+size_t scratch_per_node(int N, uint32_t needL, uint32_t needR) {
+  size_t b = (size_t)N * 20 * 16 + (size_t)std::max(N - 1, 1) * 16 * 16 + (size_t)N;
+  if (needL) b += (size_t)N * 16 * 16;
+  if (needR) b += (size_t)N * 16 * 16;
+  return b;
+}
+
+// run k_layer_modes + k_chain over [0, total) in chunks that fit the scratch budget
+int run_transfer(ytf_ctx* ctx, TransferParams p, long total) {
+  const int N = p.nL;
+  size_t per = scratch_per_node(N, p.needL, p.needR);
+  const size_t budget = (size_t)6 << 30;  // 6 GiB of scratch per pass
+  long chunk = (long)std::max<size_t>(1024, budget / per);
+  chunk = std::min(chunk, total);
+  WS(modes, double2, "tr_modes", (size_t)N * 20 * chunk);
+  WS(lstat, uint8_t, "tr_lstat", (size_t)N * chunk);
+  WS(sint, double2, "tr_sint", (size_t)std::max(N - 1, 1) * 16 * chunk);
+  double2* sleft = nullptr;
+  double2* sright = nullptr;
+  if (p.needL) { WS(sl, double2, "tr_sleft", (size_t)N * 16 * chunk); sleft = sl; }
+  if (p.needR) { WS(sr, double2, "tr_sright", (size_t)N * 16 * chunk); sright = sr; }
+  p.modes = modes;
+  p.lstat = lstat;
+  p.sint = sint;
+  p.sleft = sleft;
+  p.sright = sright;
+  for (long off = 0; off < total; off += chunk) {
+    p.off = off;
+    p.n = std::min(chunk, total - off);
+    CK(LAUNCH("k_layer_modes", launch_layer_modes(p, ctx->stream)));
+    CK(LAUNCH("k_chain", launch_chain(p, ctx->stream)));
+  }
+  return YTF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ytf_version(void) { return 10000; }
+
+int ytf_ctx_create(ytf_ctx** out, int device) {
+  if (!out) return YTF_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return YTF_ERR_CUDA;
+  if (device < 0 || device >= ndev) return YTF_ERR_ARG;
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return YTF_ERR_CUDA;
+  ytf_ctx* c = new ytf_ctx();
+  c->device = device;
+  c->stream = nullptr;  // legacy default stream until ytf_ctx_set_stream
+  *out = c;
+  return YTF_OK;
+}
+
+int ytf_ctx_destroy(ytf_ctx* ctx) {
+  if (!ctx) return YTF_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->closing = true;
+  if (ctx->refs <= 0) delete ctx;  // otherwise freed with its last stack or cache
+  return YTF_OK;
+}
+
+int ytf_ctx_profile(ytf_ctx* ctx, int enable) {
+  if (!ctx) return YTF_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  prof_collect(ctx);
+  ctx->ktime.clear();
+  ctx->klaunch.clear();
+  ctx->prof = enable != 0;
+  return YTF_OK;
+}
+
+int ytf_ctx_profile_read(ytf_ctx* ctx, int max_entries, char* names, double* total_ms, long* launches, int* n) {
+  if (!ctx || !n) return YTF_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  prof_collect(ctx);
+  int i = 0;
+  for (auto& kv : ctx->klaunch) {
+    if (i < max_entries) {
+      if (names) {
+        std::strncpy(names + 32 * i, kv.first.c_str(), 31);
+        names[32 * i + 31] = 0;
+      }
+      auto it = ctx->ktime.find(kv.first);
+      if (total_ms) total_ms[i] = it == ctx->ktime.end() ? 0.0 : it->second.first;
+      if (launches) launches[i] = kv.second;
+    }
+    ++i;
+  }
+  *n = i;
+  return YTF_OK;
+}
+
+int ytf_ctx_set_stream(ytf_ctx* ctx, void* stream) {
+  if (!ctx) return YTF_ERR_ARG;
+  ctx->stream = (cudaStream_t)stream;
+  return YTF_OK;
+}
+
+int ytf_ctx_sync(ytf_ctx* ctx) {
+  if (!ctx) return YTF_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return YTF_OK;
+}
+
+const char* ytf_last_error(const ytf_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int ytf_stack_create(ytf_ctx* ctx, int nL, const int* eps_kind, const int* mu_kind, const double* eps, const double* mu,
+                     const double* d, ytf_stack** out) {
+  if (!ctx || !out) return YTF_ERR_ARG;
+  *out = nullptr;
+  if (nL < 2 || nL > MAXL) return fail(ctx, YTF_ERR_ARG, "ytf_stack_create: nL must be in 2:" + std::to_string(MAXL));
+  if (!eps_kind || !eps || !d) return fail(ctx, YTF_ERR_ARG, "ytf_stack_create: eps_kind, eps and d are required");
+  CK(cudaSetDevice(ctx->device));
+  ytf_stack* s = new ytf_stack();
+  s->ctx = ctx;
+  ctx->refs += 1;
+  s->nL = nL;
+  s->host.resize(nL);
+  for (int l = 0; l < nL; ++l) {
+    LayerDev& L = s->host[l];
+    L.ekind = eps_kind[l];
+    L.mkind = mu_kind ? mu_kind[l] : 0;
+    if (L.ekind < 0 || L.ekind > 3 || L.mkind < 0 || L.mkind > 3) {
+      delete s;
+      ctx->refs -= 1;
+      return fail(ctx, YTF_ERR_ARG, "ytf_stack_create: material kind must be 0..3");
+    }
+    for (int i = 0; i < 18; ++i) {
+      L.eps[i] = eps[18 * l + i];
+      L.mu[i] = mu ? mu[18 * l + i] : ((i == 0 || i == 8 || i == 16) ? 1.0 : 0.0);
+    }
+    L.d = d[l];
+  }
+  cudaError_t e = cudaMalloc(&s->dev, sizeof(LayerDev) * nL);
+  if (e != cudaSuccess) { delete s; ctx->refs -= 1; return fail(ctx, YTF_ERR_NOMEM, "ytf_stack_create: cudaMalloc failed"); }
+  e = cudaMemcpy(s->dev, s->host.data(), sizeof(LayerDev) * nL, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { cudaFree(s->dev); delete s; ctx->refs -= 1; return fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e)); }
+  *out = s;
+  return YTF_OK;
+}
+
+int ytf_stack_destroy(ytf_stack* s) {
+  if (!s) return YTF_OK;
+  ytf_ctx* ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(s->dev);
+  delete s;
+  ctx_release(ctx);
+  return YTF_OK;
+}
+
+int ytf_transfer_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, int nk, const double* kx_nodes,
+                    const double* wt_nodes, int nobs, const int* obs_layers, int check_symmetry, ytf_cache** out) {
+  if (!ctx || !out) return YTF_ERR_ARG;
+  *out = nullptr;
+  std::vector<int> obs;
+  int rc = common_checks(ctx, st, "build_cavity_transfer_1d", source_layer, nobs, obs_layers, obs);
+  if (rc) return rc;
+  if (nk < 0 || (nk > 0 && (!kx_nodes || !wt_nodes)))
+    return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_1d: kx_nodes/wt_nodes length mismatch");
+  if (check_symmetry)
+    for (auto& L : st->host)
+      if (!closed_form(L))
+        return fail(ctx, YTF_ERR_ARG,
+                    "build_cavity_transfer_1d: the 1D path requires an isotropic/uniaxial stack "
+                    "(`_is_azimuthally_symmetric_stack`); use the 2D (kρ,φ) cache for biaxial/gyrotropic.");
+  CK(cudaSetDevice(ctx->device));
+  ytf_cache* c = new ytf_cache();
+  c->ctx = ctx;
+  ctx->refs += 1;
+  c->stack_ref = st;
+  c->nL = st->nL;
+  c->src = source_layer;
+  c->nobs = (int)obs.size();
+  for (int i = 0; i < c->nobs; ++i) c->obs[i] = obs[i];
+  c->omega = omega;
+  c->Nk = nk;
+  c->Np = 1;
+  c->n = nk;
+  c->kr.assign(kx_nodes, kx_nodes + nk);
+  c->wr.assign(wt_nodes, wt_nodes + nk);
+  for (auto& L : st->host) c->d_layer.push_back(L.d);
+  c->d_src = st->host[source_layer - 1].d;
+  if ((rc = alloc_cache(ctx, c))) { ytf_cache_destroy(c); return rc; }
+  TransferParams p;
+  fill_params(p, st, c);
+  p.mode = 0;
+  p.nout = c->n;
+  if (c->n > 0 && (rc = run_transfer(ctx, p, c->n))) { ytf_cache_destroy(c); return rc; }
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) { ytf_cache_destroy(c); return fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e)); }
+  prof_collect(ctx);
+  *out = c;
+  return YTF_OK;
+}
+
+int ytf_transfer_2d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, int nkr, const double* kr_nodes,
+                    const double* kr_weights, int nphi, const double* phi_nodes, const double* phi_weights, int nobs,
+                    const int* obs_layers, int rotation, ytf_cache** out) {
+  if (!ctx || !out) return YTF_ERR_ARG;
+  *out = nullptr;
+  std::vector<int> obs;
+  int rc = common_checks(ctx, st, "build_cavity_transfer_2d", source_layer, nobs, obs_layers, obs);
+  if (rc) return rc;
+  if (nkr < 0 || (nkr > 0 && (!kr_nodes || !kr_weights)))
+    return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: kρ nodes/weights length mismatch");
+  if (nphi < 0 || (nphi > 0 && (!phi_nodes || !phi_weights)))
+    return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: φ nodes/weights length mismatch");
+  bool sym = true;
+  for (auto& L : st->host) sym = sym && closed_form(L);
+  bool use_rot = rotation == YTF_ROT_AUTO ? sym : rotation != 0;
+  if (use_rot && !sym)
+    return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: rotation=true requires an azimuthally symmetric stack");
+  CK(cudaSetDevice(ctx->device));
+  ytf_cache* c = new ytf_cache();
+  c->ctx = ctx;
+  ctx->refs += 1;
+  c->stack_ref = st;
+  c->nL = st->nL;
+  c->src = source_layer;
+  c->nobs = (int)obs.size();
+  for (int i = 0; i < c->nobs; ++i) c->obs[i] = obs[i];
+  c->omega = omega;
+  c->is2d = true;
+  c->rotation = use_rot;
+  c->Nk = nkr;
+  c->Np = nphi;
+  c->n = (long)nkr * nphi;
+  c->kr.assign(kr_nodes, kr_nodes + nkr);
+  c->wr.assign(kr_weights, kr_weights + nkr);
+  c->phi.assign(phi_nodes, phi_nodes + nphi);
+  c->wphi.assign(phi_weights, phi_weights + nphi);
+  for (auto& L : st->host) c->d_layer.push_back(L.d);
+  c->d_src = st->host[source_layer - 1].d;
+  if ((rc = alloc_cache(ctx, c))) { ytf_cache_destroy(c); return rc; }
+  TransferParams p;
+  fill_params(p, st, c);
+  if (c->n > 0) {
+    if (!use_rot) {
+      p.mode = 1;
+      p.nout = c->n;
+      if ((rc = run_transfer(ctx, p, c->n))) { ytf_cache_destroy(c); return rc; }
+    } else {
+      // φ = 0 base solve per kρ, then the exact rotation to every φ
+      long nb = nkr;
+      int N = st->nL;
+      WS(modes, double2, "tr_modes", (size_t)N * 20 * nb);
+      WS(lstat, uint8_t, "tr_lstat", (size_t)N * nb);
+      WS(sint, double2, "tr_sint", (size_t)std::max(N - 1, 1) * 16 * nb);
+      WS(bstat, uint8_t, "tr_bstatus", (size_t)nb);
+      WS(btv, uint8_t, "tr_btvalid", (size_t)nb * c->nobs);
+      WS(bT, double2, "tr_bT", (size_t)16 * nb * c->nobs);
+      TransferParams b = p;
+      b.mode = 2;
+      b.n = nb;
+      b.off = 0;
+      b.nout = nb;
+      b.modes = modes;
+      b.lstat = lstat;
+      b.sint = sint;
+      if (b.needL) { WS(sl, double2, "tr_sleft", (size_t)N * 16 * nb); b.sleft = sl; }
+      if (b.needR) { WS(sr, double2, "tr_sright", (size_t)N * 16 * nb); b.sright = sr; }
+      b.status = bstat;
+      b.tvalid = btv;
+      b.Tout = bT;
+      CK(LAUNCH("k_layer_modes", launch_layer_modes(b, ctx->stream)));
+      CK(LAUNCH("k_chain", launch_chain(b, ctx->stream)));
+      TransferParams f = p;
+      f.mode = 1;
+      f.n = nb;
+      f.off = 0;
+      f.nout = c->n;
+      f.modes = modes;
+      CK(LAUNCH("k_rotate_fill", launch_rotate_fill(f, bstat, btv, bT, ctx->stream)));
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) { ytf_cache_destroy(c); return fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e)); }
+  prof_collect(ctx);
+  *out = c;
+  return YTF_OK;
+}
+
+int ytf_cache_destroy(ytf_cache* c) {
+  if (!c) return YTF_OK;
+  ytf_ctx* ctx = c->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (c->block) {
+    if (ctx->closing) cudaFree(c->block);
+    else ctx->pool.emplace(c->block_bytes, c->block);
+  }
+  delete c;
+  ctx_release(ctx);
+  return YTF_OK;
+}
+
+int ytf_cache_info(const ytf_cache* c, long* n_nodes, int* n_obs, int* obs_layers, int* is2d, int* rotation) {
+  if (!c) return YTF_ERR_ARG;
+  if (n_nodes) *n_nodes = c->n;
+  if (n_obs) *n_obs = c->nobs;
+  if (obs_layers)
+    for (int i = 0; i < c->nobs; ++i) obs_layers[i] = c->obs[i];
+  if (is2d) *is2d = c->is2d;
+  if (rotation) *rotation = c->rotation;
+  return YTF_OK;
+}
+
+int ytf_cache_status(ytf_ctx* ctx, const ytf_cache* c, unsigned char* valid, unsigned char* tvalid, unsigned char* status) {
+  if (!ctx || !c) return YTF_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (valid) CK(cudaMemcpyAsync(valid, c->d_valid, c->n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (tvalid) CK(cudaMemcpyAsync(tvalid, c->d_tvalid, (size_t)c->n * c->nobs, cudaMemcpyDeviceToHost, ctx->stream));
+  if (status) CK(cudaMemcpyAsync(status, c->d_status, c->n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return YTF_OK;
+}
+
+int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* c, double* T, double* Qf, double* Qb, double* sf, double* sb,
+                     double* basis) {
+  if (!ctx || !c) return YTF_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  long n = c->n;
+  auto fetch = [&](const double2* dsrc, long elems, long nn, double* dst, bool per_obs, int no) -> int {
+    // device SoA [o][e][n] -> host AoS [o][n][e]
+    std::vector<double2> h((size_t)elems * nn * no);
+    cudaError_t e = cudaMemcpy(h.data(), dsrc, sizeof(double2) * h.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e));
+    for (int o = 0; o < no; ++o)
+      for (long k = 0; k < nn; ++k)
+        for (long el = 0; el < elems; ++el) {
+          double2 v = h[((size_t)o * elems + el) * nn + k];
+          size_t di = (((size_t)o * nn + k) * elems + el) * 2;
+          dst[di] = v.x;
+          dst[di + 1] = v.y;
+        }
+    (void)per_obs;
+    return YTF_OK;
+  };
+  CK(cudaStreamSynchronize(ctx->stream));
+  int rc;
+  if (T && (rc = fetch(c->d_T, 16, n, T, true, c->nobs))) return rc;
+  if (Qf && (rc = fetch(c->d_Qf, 2, n, Qf, false, 1))) return rc;
+  if (Qb && (rc = fetch(c->d_Qb, 2, n, Qb, false, 1))) return rc;
+  if (sf && (rc = fetch(c->d_sf, 6, n, sf, false, 1))) return rc;
+  if (sb && (rc = fetch(c->d_sb, 6, n, sb, false, 1))) return rc;
+  if (basis && (rc = fetch(c->d_basis, 16, n, basis, true, c->nobs))) return rc;
+  return YTF_OK;
+}
+
+int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local, int nz, const double* z_obs, int nx,
+              const double* xs, int ny, const double* ys, int terms, int precision, double* out, int out_is_device) {
+  if (!ctx || !c || !out) return YTF_ERR_ARG;
+  if (c->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "closed_form_G: cache belongs to another context");
+  int oi = c->oidx(obs_layer);
+  if (oi < 0)
+    return fail(ctx, YTF_ERR_ARG, "amplitude_at: obs_layer=" + std::to_string(obs_layer) +
+                                      " not in this cache's obs_layers " + obs_str(c->obs, c->nobs));
+  if (terms < 0 || terms > 4)
+    return fail(ctx, YTF_ERR_ARG, "closed_form_G: terms must be :all, :direct, :scattered, :toeplitz or :hankel");
+  bool same = obs_layer == c->src;
+  if ((terms == YTF_TERMS_TOEPLITZ || terms == YTF_TERMS_HANKEL || terms == YTF_TERMS_DIRECT) && !same)
+    return fail(ctx, YTF_ERR_ARG, "closed_form_G: terms needs obs_layer == source_layer (" + std::to_string(c->src) +
+                                      "), got " + std::to_string(obs_layer));
+  if (precision != YTF_PREC_FP64 && precision != YTF_PREC_SPLIT_BF16)
+    return fail(ctx, YTF_ERR_ARG, "closed_form_G: unknown precision mode");
+  double zpos = c->src == 1 ? c->d_src - zsrc_local : zsrc_local;
+  const double se = 1.4901161193847656e-08;
+  if (!(-se <= zpos && zpos <= c->d_src + se))
+    return fail(ctx, YTF_ERR_ARG, "amplitude_at: zsrc_local=" + std::to_string(zsrc_local) + " outside [0," +
+                                      std::to_string(c->d_src) + "]");
+  if (nz < 0 || nx < 0 || ny < 0) return fail(ctx, YTF_ERR_ARG, "closed_form_G: negative grid size");
+  CK(cudaSetDevice(ctx->device));
+  long npix = (long)nx * ny;
+  long nout = npix * nz * 9;
+  if (nout == 0) return YTF_OK;
+  SynthParams sp;
+  std::memset(&sp, 0, sizeof(sp));
+  CacheView& v = sp.c;
+  v.n = c->n; v.Nk = c->Nk; v.Np = c->Np; v.src = c->src; v.d_src = c->d_src;
+  v.kr = c->d_kr; v.wr = c->d_wr; v.phi = c->d_phi; v.wphi = c->d_wphi;
+  v.valid = c->d_valid;
+  v.tvalid = c->d_tvalid + (size_t)oi * c->n;
+  v.T = c->d_T + (size_t)oi * 16 * c->n;
+  v.Qf = c->d_Qf; v.Qb = c->d_Qb; v.sf = c->d_sf; v.sb = c->d_sb;
+  v.basis = c->d_basis + (size_t)oi * 16 * c->n;
+  sp.same = same;
+  switch (terms) {
+    case YTF_TERMS_ALL: sp.uf_F = sp.ub_F = sp.uf_B = sp.ub_B = 1.0; sp.with_direct = same; break;
+    case YTF_TERMS_SCATTERED: sp.uf_F = sp.ub_F = sp.uf_B = sp.ub_B = 1.0; sp.with_direct = 0; break;
+    case YTF_TERMS_DIRECT: sp.with_direct = 1; break;
+    case YTF_TERMS_TOEPLITZ: sp.uf_F = 1.0; sp.ub_B = 1.0; sp.with_direct = 1; break;
+    case YTF_TERMS_HANKEL: sp.ub_F = 1.0; sp.uf_B = 1.0; sp.with_direct = 0; break;
+  }
+  sp.zpos = zpos;
+  sp.d_obs = c->d_layer[obs_layer - 1];
+  sp.nz = nz;
+  WS(dzo, double, "g_zo", nz);
+  WS(dxs, double, "g_xs", nx);
+  WS(dys, double, "g_ys", ny);
+  int rc;
+  if ((rc = upload(ctx, dzo, z_obs, 8 * (size_t)nz))) return rc;
+  if ((rc = upload(ctx, dxs, xs, 8 * (size_t)nx))) return rc;
+  if ((rc = upload(ctx, dys, ys, 8 * (size_t)ny))) return rc;
+  sp.zo = dzo;
+  double2* G;
+  if (out_is_device) {
+    G = (double2*)out;
+  } else {
+    WS(g, double2, "g_out", nout);
+    G = g;
+  }
+  int nsm = 148;
+  {
+    int dev = ctx->device;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  if (c->n == 0) {  // an empty rule integrates to zero
+    CK(cudaMemsetAsync(G, 0, sizeof(double2) * nout, ctx->stream));
+  } else if (!c->is2d) {
+    // distinct radii in first-occurrence order over (i fastest, j), as the reference
+    std::vector<double> ur;
+    std::vector<int> rmap(npix);
+    std::unordered_map<double, int> idx;
+    idx.reserve(npix * 2);
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        double r = std::hypot(xs[i], ys[j]);
+        auto it = idx.find(r);
+        if (it == idx.end()) { idx.emplace(r, (int)ur.size()); rmap[i + (long)nx * j] = (int)ur.size(); ur.push_back(r); }
+        else rmap[i + (long)nx * j] = it->second;
+      }
+    int nr = (int)ur.size();
+    long nk = c->n;
+    WS(drho, double, "g_rho", nr);
+    WS(drmap, int, "g_rmap", npix);
+    if ((rc = upload(ctx, drho, ur.data(), 8 * (size_t)nr))) return rc;
+    if ((rc = upload(ctx, drmap, rmap.data(), 4 * (size_t)npix))) return rc;
+    WS(J, double, "g_J", 3 * (size_t)nr * nk);
+    WS(C, double, "g_C", 26 * (size_t)nz * nk);
+    WS(P, double, "g_P", 26 * (size_t)nz * nr);
+    double *J0 = J, *J1 = J + (size_t)nr * nk, *J2 = J + 2 * (size_t)nr * nk;
+    double *C0 = C, *C1 = C + 10 * (size_t)nz * nk, *C2 = C + 18 * (size_t)nz * nk;
+    double *P0 = P, *P1 = P + 10 * (size_t)nz * nr, *P2 = P + 18 * (size_t)nz * nr;
+    CK(LAUNCH("k_coef1d", launch_coef1d(sp, C0, C1, C2, ctx->stream)));
+    CK(LAUNCH("k_bessel", launch_bessel(c->d_kr, nk, drho, nr, J0, J1, J2, ctx->stream)));
+    auto splits_for = [&](int M, int N) {
+      long tiles = (long)((M + 127) / 128) * ((N + 127) / 128);
+      long want = (2L * nsm + tiles - 1) / tiles;
+      long maxs = std::max(1L, nk / 256);
+      return (int)std::max(1L, std::min(want, maxs));
+    };
+    int s0 = splits_for(nr, 10 * nz), s1 = splits_for(nr, 8 * nz);
+    size_t part = std::max((size_t)s0 * nr * 10 * nz, (size_t)s1 * nr * 8 * nz);
+    WS(Pp, double, "g_partial", part);
+    const double* Jn[3] = {J0, J1, J2};
+    const double* Cn[3] = {C0, C1, C2};
+    double* Pn[3] = {P0, P1, P2};
+    const int Nn[3] = {10 * nz, 8 * nz, 8 * nz};
+    for (int o = 0; o < 3; ++o) {
+      int sp_ = dgemm_splits((int)nk, o == 0 ? s0 : s1);
+      CK(LAUNCH("k_dgemm_nt", launch_dgemm_nt(nr, Nn[o], (int)nk, Jn[o], Cn[o], Pp, sp_, ctx->stream)));
+      CK(LAUNCH("k_reduce_splits", launch_reduce_splits((long)nr * Nn[o], sp_, Pp, Pn[o], ctx->stream)));
+    }
+    CK(LAUNCH("k_assemble1d", launch_assemble1d(nx, ny, nz, dxs, dys, drmap, nr, P0, P1, P2, G, ctx->stream)));
+  } else {
+    int ncol = 9 * nz;
+    WS(S, double2, "g_S", (size_t)ncol * c->n);
+    CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream)));
+    long tiles = ((npix + 63) / 64) * ((ncol + 31) / 32);
+    long want = (4L * nsm + tiles - 1) / tiles;
+    int splits = (int)std::max(1L, std::min(want, std::max(1L, c->n / 512)));
+    splits = lateral_splits(c->n, splits);
+    WS(Gp, double2, "g_partial2", (size_t)splits * npix * ncol);
+    CK(LAUNCH("k_lateral", launch_lateral(v, nx, ny, dxs, dys, ncol, S, Gp, splits, ctx->stream)));
+    CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, splits, Gp, G, ctx->stream)));
+  }
+  if (!out_is_device) CK(cudaMemcpyAsync(out, G, sizeof(double2) * nout, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  prof_collect(ctx);
+  return YTF_OK;
+}
+
+// Gauss-Legendre rule: Newton on the three-term recurrence in long double, rounded once
+int ytf_gauss_legendre(int n, double* x, double* w) {
+  if (n < 1 || !x || !w) return YTF_ERR_ARG;
+  for (int i = 0; i < n; ++i) {
+    long double z = cosl(3.14159265358979323846264338327950288L * (i + 0.75L) / (n + 0.5L));
+    long double p0 = 1, p1 = z, dp = 0;
+    for (int it = 0; it < 100; ++it) {
+      p0 = 1; p1 = z;
+      for (int k = 2; k <= n; ++k) { long double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k; p0 = p1; p1 = p2; }
+      dp = n * (z * p1 - p0) / (z * z - 1);
+      long double dz = p1 / dp;
+      z -= dz;
+      if (fabsl(dz) < 1e-30L) break;
+    }
+    p0 = 1; p1 = z;
+    for (int k = 2; k <= n; ++k) { long double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k; p0 = p1; p1 = p2; }
+    dp = n * (z * p1 - p0) / (z * z - 1);
+    x[n - 1 - i] = (double)z;
+    w[n - 1 - i] = (double)(2.0L / ((1 - z * z) * dp * dp));
+  }
+  if (n % 2 == 1) x[n / 2] = 0.0;
+  return YTF_OK;
+}
+
+int ytf_gl_rule(ytf_ctx* ctx, int npanels, const double* pa, const double* pb, int order, int nsing, const double* singular,
+                double* nodes, double* weights) {
+  if (!ctx || npanels < 0 || order < 1 || (npanels > 0 && (!pa || !pb || !nodes || !weights))) return YTF_ERR_ARG;
+  if (npanels == 0) return YTF_OK;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<double> xi(order), wx(order);
+  ytf_gauss_legendre(order, xi.data(), wx.data());
+  std::set<double> S;
+  for (int i = 0; i < nsing; ++i) S.insert(singular[i]);
+  std::vector<int> side(npanels);
+  for (int i = 0; i < npanels; ++i) side[i] = S.count(pa[i]) ? 1 : (S.count(pb[i]) ? -1 : 0);
+  size_t np = npanels, tot = (size_t)npanels * order;
+  WS(buf, double, "gl_buf", 2 * np + 2 * (size_t)order + 2 * tot);
+  WS(dside, int, "gl_side", np);
+  double *da = buf, *db = buf + np, *dxi = buf + 2 * np, *dwx = dxi + order, *dn = dwx + order, *dw = dn + tot;
+  int rc;
+  if ((rc = upload(ctx, da, pa, 8 * np)) || (rc = upload(ctx, db, pb, 8 * np)) || (rc = upload(ctx, dxi, xi.data(), 8 * (size_t)order)) ||
+      (rc = upload(ctx, dwx, wx.data(), 8 * (size_t)order)) || (rc = upload(ctx, dside, side.data(), 4 * np)))
+    return rc;
+  CK(LAUNCH("k_gl_nodes", launch_gl_nodes(npanels, da, db, dside, dxi, dwx, order, dn, dw, ctx->stream)));
+  CK(cudaMemcpyAsync(nodes, dn, 8 * tot, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(weights, dw, 8 * tot, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return YTF_OK;
+}
+
+}  // extern "C"

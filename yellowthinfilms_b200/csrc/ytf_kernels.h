@@ -1,0 +1,117 @@
+// ytf_kernels.h -- parameter blocks and launchers shared by the libytf kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ytf {
+
+constexpr int MAXL = 32;  // layers per stack (bit masks below are 32 wide)
+
+// per-node status bits (the reference's numerical guards, as data instead of exceptions)
+enum : uint8_t {
+  ST_VALID = 1,        // node contributes (valid[k] of the reference)
+  ST_EIGEN = 2,        // 4x4 QR did not converge
+  ST_SORT = 4,         // more than two modes in one direction (reference: BoundsError)
+  ST_SINGULAR = 8,     // exact zero pivot in an interface or projection solve
+  ST_SEEDS = 16,       // non-finite point seeds (reference: `continue`)
+  ST_TNONFINITE = 32,  // some T^o non-finite (Tvalid[o][k] = false)
+};
+
+// one layer: kinds (0 iso, 1 uniaxial, 2 biaxial, 3 general), column-major 3x3 ε and μ
+// (interleaved re/im), thickness
+struct LayerDev {
+  int ekind, mkind;
+  double eps[18];
+  double mu[18];
+  double d;
+};
+
+struct TransferParams {
+  const LayerDev* layers;  // device, nL entries
+  int nL, src, nobs;       // src, obs[] are 1-based
+  int obs[MAXL];
+  uint32_t needL, needR;   // layers (bit l-1) whose SLeft / SRight are kept in scratch
+  double omega;
+  int mode;                // 0: 1D nodes; 1: 2D full solve; 2: 2D rotation base (φ = 0)
+  long n;                  // nodes solved by k_layer_modes / k_chain (this chunk)
+  long off;                // global index of the chunk's first node
+  long nout;               // nodes of the output cache (== n except the rotation fill)
+  int Nk, Np;
+  const double* kr;        // 1D: kx nodes; 2D: kρ nodes
+  const double* phi;       // 2D: φ nodes
+  // scratch
+  double2* modes;          // [nL][20][n]
+  uint8_t* lstat;          // [nL][n]
+  double2* sint;           // [nL-1][16][n]
+  double2* sleft;          // [nL][16][n]
+  double2* sright;         // [nL][16][n]
+  // outputs
+  uint8_t* status;         // [nout] (rotation base: [n])
+  uint8_t* valid;          // [nout]
+  uint8_t* tvalid;         // [nobs][nout]
+  double2* Tout;           // [nobs][16][nout], column-major 4x4 per node
+  double2* Qf;             // [2][nout]
+  double2* Qb;             // [2][nout]
+  double2* sf;             // [6][nout], column-major 2x3
+  double2* sb;             // [6][nout]
+  double2* basis;          // [nobs][16][nout]: exf0 exf1 eyf0 eyf1 ezf0 ezf1 exb.. eyb.. ezb.. kzf0 kzf1 kzb0 kzb1
+};
+
+cudaError_t launch_layer_modes(const TransferParams& p, cudaStream_t stream);
+cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream);
+cudaError_t launch_rotate_fill(const TransferParams& p, const uint8_t* base_status, const uint8_t* base_tvalid,
+                               const double2* Tbase, cudaStream_t stream);
+
+// read-only view of a device transfer cache for the synthesis kernels
+struct CacheView {
+  long n;
+  int Nk, Np;
+  int src;          // 1-based
+  double d_src;
+  const double* kr;    // [Nk]
+  const double* wr;    // [Nk]
+  const double* phi;   // [Np]
+  const double* wphi;  // [Np]
+  const uint8_t* valid;
+  const uint8_t* tvalid;  // of the obs layer in use: [n]
+  const double2* T;       // of the obs layer: [16][n]
+  const double2* Qf;
+  const double2* Qb;
+  const double2* sf;
+  const double2* sb;
+  const double2* basis;   // of the obs layer: [16][n]
+};
+
+struct SynthParams {
+  CacheView c;
+  int same;          // obs layer == source layer
+  int with_direct;   // add the same-layer direct term
+  double uf_F, ub_F, uf_B, ub_B;  // seed masks of the reflected amplitudes (terms)
+  double zpos;       // source position in the cavity frame
+  double d_obs;
+  int nz;
+  const double* zo;  // [nz] device
+};
+
+// 1D Jacobi-Anger synthesis
+cudaError_t launch_coef1d(const SynthParams& p, double* C0, double* C1, double* C2, cudaStream_t s);
+cudaError_t launch_bessel(const double* kr, long nk, const double* rho, int nr, double* J0, double* J1, double* J2,
+                          cudaStream_t s);
+int dgemm_splits(int K, int splits);  // effective split count of launch_dgemm_nt
+cudaError_t launch_dgemm_nt(int M, int N, int K, const double* A, const double* B, double* partial, int splits,
+                            cudaStream_t s);
+cudaError_t launch_reduce_splits(long len, int splits, const double* partial, double* C, cudaStream_t s);
+cudaError_t launch_assemble1d(int nx, int ny, int nz, const double* xs, const double* ys, const int* rmap, int nr,
+                              const double* P0, const double* P1, const double* P2, double2* G, cudaStream_t s);
+// 2D direct lateral synthesis
+cudaError_t launch_strengths2d(const SynthParams& p, double2* S, cudaStream_t s);
+int lateral_splits(long n, int splits);  // effective split count of launch_lateral
+cudaError_t launch_lateral(const CacheView& c, int nx, int ny, const double* xs, const double* ys, int ncol, const double2* S,
+                           double2* partial, int splits, cudaStream_t s);
+cudaError_t launch_reduce_splits2(long len, int splits, const double2* partial, double2* G, cudaStream_t s);
+
+// Gauss-Legendre panels -> nodes/weights, bit-exact with the CPU restatement
+cudaError_t launch_gl_nodes(int npanels, const double* pa, const double* pb, const int* sing_side, const double* xi,
+                            const double* wx, int order, double* nodes, double* wts, cudaStream_t s);
+
+}  // namespace ytf

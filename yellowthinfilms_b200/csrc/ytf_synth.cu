@@ -1,0 +1,547 @@
+// ytf_synth.cu -- synthesis of G(ρ, z, z') from a device transfer cache.
+//
+// 1D (point source, azimuthally symmetric stack; closed_form_G for CavityTransferCache1D,
+// mod_ClosedFormField.jl:435-487): the Jacobi–Anger pixel integral
+// (_integrate_pixel_1d, :344-390) is linear in (J0, J1, J2)(kρ), so for every distinct
+// radius and z-row it is the contraction
+//     R[ρ, col] = Σ_k J_n(k ρ) · C_n[k, col],   n = 0, 1, 2,
+// of a Bessel table with per-node coefficients (weighted amplitude × mode field × phase ×
+// k). k_coef1d builds C_n (13 complex columns per z-row), k_bessel the tables, a GEMM
+// does the contraction and k_assemble1d combines orders, rotates by the pixel azimuth
+// and writes Julia's (Nx, Ny, Nz, 3, 3) column-major layout.
+//
+// 2D (any stack; closed_form_G for CavityTransferCache2D, lateral=:direct, :711-753):
+// k_strengths2d forms the 9 strengths per (node, z-row) (_strengths_row!, :616-659) and
+// k_lateral evaluates G[pix, col] = Σ_n e^{i(kx_n x + ky_n y)} S[col, n] as a complex GEMM
+// whose A operand is generated in shared memory from the node's (kx, ky).
+#include "ytf_complex.cuh"
+#include "ytf_kernels.h"
+
+#include <algorithm>
+
+namespace ytf {
+
+__device__ __forceinline__ cd ldc(const double2* b, long e, long n, long i) {
+  double2 v = b[e * n + i];
+  return cd{v.x, v.y};
+}
+
+// _phase (mod_ClosedFormField.jl:59-69): clamped exp(i kz z)
+__device__ __forceinline__ cd phase_cl(cd kz, double z) {
+  double a = -kz.y * z, b = kz.x * z;
+  if (!isfinite(a) || !isfinite(b) || a > 700.0 || a < -700.0) return cd{0.0, 0.0};
+  return cexp(cd{a, b});
+}
+__device__ __forceinline__ cd fin0(cd z) { return isfin(z) ? z : cd{0.0, 0.0}; }
+
+// reflected amplitudes of node k (amplitude_at, :175-203) with the term masks
+__device__ __forceinline__ void reflected_amp(const SynthParams& p, long k, cd Af[2][3], cd Ab[2][3]) {
+  const CacheView& c = p.c;
+  for (int m = 0; m < 2; ++m)
+    for (int q = 0; q < 3; ++q) { Af[m][q] = cd{0, 0}; Ab[m][q] = cd{0, 0}; }
+  if (!(c.valid[k] && c.tvalid[k])) return;
+  const double d = c.d_src, zp = p.zpos;
+  cd Pf[2], Pb[2];
+  for (int m = 0; m < 2; ++m) {
+    Pf[m] = cexp(mul_i(ldc(c.Qf, m, c.n, k)) * (d - zp));
+    Pb[m] = cexp(mul_i(-ldc(c.Qb, m, c.n, k)) * zp);
+  }
+  cd T[4][4];
+  for (int r = 0; r < 4; ++r)
+    for (int cc = 0; cc < 4; ++cc) T[r][cc] = ldc(c.T, r + 4 * cc, c.n, k);
+  for (int q = 0; q < 3; ++q) {
+    cd sf0 = ldc(c.sf, 0 + 2 * q, c.n, k) * Pf[0], sf1 = ldc(c.sf, 1 + 2 * q, c.n, k) * Pf[1];
+    cd sb0 = ldc(c.sb, 0 + 2 * q, c.n, k) * Pb[0], sb1 = ldc(c.sb, 1 + 2 * q, c.n, k) * Pb[1];
+    // rows 0,1 (Af) use the F masks, rows 2,3 (Ab) the B masks
+    cd uF[4] = {p.uf_F * sf0, p.uf_F * sf1, p.ub_F * sb0, p.ub_F * sb1};
+    cd uB[4] = {p.uf_B * sf0, p.uf_B * sf1, p.ub_B * sb0, p.ub_B * sb1};
+    for (int m = 0; m < 2; ++m) {
+      cd a = T[m][0] * uF[0];
+      a += T[m][1] * uF[1];
+      a += T[m][2] * uF[2];
+      a += T[m][3] * uF[3];
+      Af[m][q] = a;
+      cd b = T[2 + m][0] * uB[0];
+      b += T[2 + m][1] * uB[1];
+      b += T[2 + m][2] * uB[2];
+      b += T[2 + m][3] * uB[3];
+      Ab[m][q] = b;
+    }
+  }
+}
+
+// same-layer direct amplitudes at z_obs (direct_amplitude, :232-259), point source
+__device__ __forceinline__ void direct_amp(const SynthParams& p, long k, double z, cd Afd[2][3], cd Abd[2][3]) {
+  const CacheView& c = p.c;
+  for (int m = 0; m < 2; ++m)
+    for (int q = 0; q < 3; ++q) { Afd[m][q] = cd{0, 0}; Abd[m][q] = cd{0, 0}; }
+  if (!c.valid[k]) return;
+  const double zeta = z - p.zpos;
+  if (zeta > 0) {
+    for (int m = 0; m < 2; ++m) {
+      cd e = phase_cl(ldc(c.Qf, m, c.n, k), zeta);
+      for (int q = 0; q < 3; ++q) Afd[m][q] = ldc(c.sf, m + 2 * q, c.n, k) * e;
+    }
+  } else if (zeta < 0) {
+    for (int m = 0; m < 2; ++m) {
+      cd e = phase_cl(ldc(c.Qb, m, c.n, k), zeta);
+      for (int q = 0; q < 3; ++q) Abd[m][q] = ldc(c.sb, m + 2 * q, c.n, k) * e;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// 1D coefficients. Columns per z-row: order 0: xx yx xy yy zz; order 1: zx zy xz yz;
+// order 2: xx yx xy yy (c q). Output rows are real: row 2*(zi*ncol + col) + part, node fastest.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_coef1d(SynthParams p, double* C0, double* C1, double* C2) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int zi = blockIdx.y;
+  const CacheView& c = p.c;
+  if (k >= c.n) return;
+  const long n = c.n;
+  cd Af[2][3], Ab[2][3];
+  reflected_amp(p, k, Af, Ab);
+  const double z = p.zo[zi];
+  const cd W{0.0, c.wr[k] / (2.0 * 3.14159265358979323846)};
+  const double kx = c.kr[k];
+  cd c0[5], c1[4], c2[4];
+  for (int i = 0; i < 5; ++i) c0[i] = cd{0, 0};
+  for (int i = 0; i < 4; ++i) { c1[i] = cd{0, 0}; c2[i] = cd{0, 0}; }
+  cd Afd[2][3], Abd[2][3];
+  if (p.with_direct) direct_amp(p, k, z, Afd, Abd);
+  const cd half_i{0.0, 0.5};
+  for (int m = 0; m < 2; ++m) {
+    cd kzf = ldc(c.basis, 12 + m, n, k), kzb = ldc(c.basis, 14 + m, n, k);
+    cd af[3], ab[3], gf, gb;
+    if (p.with_direct) {
+      cd pf = phase_cl(kzf, z), pb = phase_cl(kzb, z - p.d_obs);
+      for (int q = 0; q < 3; ++q) {
+        af[q] = fin0(W * (Afd[m][q] + Af[m][q] * pf));
+        ab[q] = fin0(W * (Abd[m][q] + Ab[m][q] * pb));
+      }
+      gf = cd{kx, 0.0};
+      gb = cd{kx, 0.0};
+    } else {
+      for (int q = 0; q < 3; ++q) { af[q] = fin0(W * Af[m][q]); ab[q] = fin0(W * Ab[m][q]); }
+      gf = phase_cl(kzf, z) * kx;
+      gb = phase_cl(kzb, z - p.d_obs) * kx;
+    }
+    for (int br = 0; br < 2; ++br) {
+      const cd* a = br == 0 ? af : ab;
+      cd g = br == 0 ? gf : gb;
+      cd ex = ldc(c.basis, (br == 0 ? 0 : 6) + m, n, k);
+      cd ey = ldc(c.basis, (br == 0 ? 2 : 8) + m, n, k);
+      cd ez = ldc(c.basis, (br == 0 ? 4 : 10) + m, n, k);
+      cd ax = a[0] * g, ay = a[1] * g, az = a[2] * g;
+      // q = x: A = ax, B = ay
+      c0[0] += half_i * (-(ax * ex) - ay * ey);  // xx
+      c2[0] += half_i * (ax * ex - ay * ey);
+      c0[1] += half_i * (-(ax * ey) + ay * ex);  // yx
+      c2[1] += half_i * (ax * ey + ay * ex);
+      c1[0] += ax * ez;                          // zx
+      // q = y: A = ay, B = -ax
+      c0[2] += half_i * (-(ay * ex) + ax * ey);  // xy
+      c2[2] += half_i * (ay * ex + ax * ey);
+      c0[3] += half_i * (-(ay * ey) - ax * ex);  // yy
+      c2[3] += half_i * (ay * ey - ax * ex);
+      c1[1] += ay * ez;                          // zy
+      // q = z: C = az
+      c1[2] += az * ex;                          // xz
+      c1[3] += az * ey;                          // yz
+      c0[4] += cd{0.0, -1.0} * (az * ez);        // zz
+    }
+  }
+  for (int i = 0; i < 5; ++i) {
+    long r = 2L * (zi * 5 + i);
+    C0[r * n + k] = c0[i].x;
+    C0[(r + 1) * n + k] = c0[i].y;
+  }
+  for (int i = 0; i < 4; ++i) {
+    long r = 2L * (zi * 4 + i);
+    C1[r * n + k] = c1[i].x;
+    C1[(r + 1) * n + k] = c1[i].y;
+    C2[r * n + k] = c2[i].x;
+    C2[(r + 1) * n + k] = c2[i].y;
+  }
+}
+
+cudaError_t launch_coef1d(const SynthParams& p, double* C0, double* C1, double* C2, cudaStream_t s) {
+  dim3 grid((unsigned)((p.c.n + 127) / 128), (unsigned)p.nz);
+  k_coef1d<<<grid, 128, 0, s>>>(p, C0, C1, C2);
+  return cudaGetLastError();
+}
+
+// Bessel tables J_n(k ρ), n = 0, 1, 2; row r = radius, k contiguous
+__global__ void k_bessel(const double* kr, long nk, const double* rho, int nr, double* J0, double* J1, double* J2) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (k >= nk) return;
+  double x = kr[k] * rho[r];
+  long o = (long)r * nk + k;
+  double a0 = j0(x), a1 = j1(x), a2;
+  if (fabs(x) < 1.0) {
+    // J2(x) = Σ_m (-1)^m (x/2)^{2m+2} / (m! (m+2)!)  (A&S 9.1.10); exact 0 at x = 0
+    double h2 = 0.25 * x * x, t = 0.5 * h2, s = t;
+    for (int m = 0; m < 12; ++m) {
+      t *= -h2 / ((m + 1.0) * (m + 3.0));
+      s += t;
+    }
+    a2 = s;
+  } else {
+    a2 = (2.0 / x) * a1 - a0;  // three-term recurrence (A&S 9.1.27)
+  }
+  J0[o] = a0;
+  J1[o] = a1;
+  J2[o] = a2;
+}
+
+cudaError_t launch_bessel(const double* kr, long nk, const double* rho, int nr, double* J0, double* J1, double* J2,
+                          cudaStream_t s) {
+  dim3 grid((unsigned)((nk + 127) / 128), (unsigned)nr);
+  k_bessel<<<grid, 128, 0, s>>>(kr, nk, rho, nr, J0, J1, J2);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// FP64 GEMM C[M][N] = A[M][K] · B[N][K]^T (both operands K-contiguous), split-K with a
+// deterministic reduction. 128x128 tile, 8 k per stage, 8x8 outputs per thread.
+// ------------------------------------------------------------------------------------
+constexpr int GT = 128, GK = 8;
+__global__ void __launch_bounds__(256) k_dgemm_nt(int M, int N, int K, const double* __restrict__ A,
+                                                  const double* __restrict__ B, double* __restrict__ Cp, int kchunk) {
+  __shared__ double As[GK][GT];
+  __shared__ double Bs[GK][GT];
+  const int bm = blockIdx.y * GT, bn = blockIdx.x * GT, sp = blockIdx.z;
+  const long k0 = (long)sp * kchunk;
+  const long k1 = min((long)K, k0 + kchunk);
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  for (long kk = k0; kk < k1; kk += GK) {
+    // 128x8 tile of A and of B: 1024 elements each, 4 per thread; k fastest in memory
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      int idx = tid + 256 * e;
+      int row = idx / GK, col = idx % GK;
+      long kg = kk + col;
+      int ra = bm + row, rb = bn + row;
+      As[col][row] = (ra < M && kg < k1) ? A[(long)ra * K + kg] : 0.0;
+      Bs[col][row] = (rb < N && kg < k1) ? B[(long)rb * K + kg] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < GK; ++t) {
+      double a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = As[t][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = Bs[t][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  double* C = Cp + (long)sp * M * N;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int r = bm + ty + 16 * i;
+    if (r >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      int cc = bn + tx + 16 * j;
+      if (cc < N) C[(long)r * N + cc] = acc[i][j];
+    }
+  }
+}
+
+__global__ void k_reduce_splits(long len, int splits, const double* __restrict__ P, double* __restrict__ C) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= len) return;
+  double s = 0.0;
+  for (int k = 0; k < splits; ++k) s += P[(long)k * len + i];
+  C[i] = s;
+}
+
+int dgemm_splits(int K, int splits) {
+  int kchunk = (K + splits - 1) / splits;
+  kchunk = ((kchunk + GK - 1) / GK) * GK;
+  if (kchunk <= 0) return 1;
+  return std::max(1, (K + kchunk - 1) / kchunk);
+}
+
+cudaError_t launch_dgemm_nt(int M, int N, int K, const double* A, const double* B, double* partial, int splits,
+                            cudaStream_t s) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  splits = dgemm_splits(K, splits);
+  int kchunk = (K + splits - 1) / splits;
+  kchunk = ((kchunk + GK - 1) / GK) * GK;
+  dim3 grid((unsigned)((N + GT - 1) / GT), (unsigned)((M + GT - 1) / GT), (unsigned)splits);
+  k_dgemm_nt<<<grid, 256, 0, s>>>(M, N, K, A, B, partial, kchunk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_splits(long len, int splits, const double* partial, double* C, cudaStream_t s) {
+  if (len <= 0) return cudaSuccess;
+  k_reduce_splits<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(len, splits, partial, C);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// 1D assembly: combine orders, rotate per pixel, Julia layout (Nx, Ny, Nz, 3, 3)
+// ------------------------------------------------------------------------------------
+__global__ void k_assemble1d(int nx, int ny, int nz, const double* xs, const double* ys, const int* rmap, int nr,
+                             const double* P0, const double* P1, const double* P2, double2* G) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long npix = (long)nx * ny;
+  if (t >= npix * nz) return;
+  long pix = t % npix;
+  int zi = (int)(t / npix);
+  int i = (int)(pix % nx), j = (int)(pix / nx);
+  int r = rmap[pix];
+  const long n0 = 10L * nz, n1 = 8L * nz;
+  auto g0 = [&](int col) { long o = (long)r * n0 + 2L * (zi * 5 + col); return cd{P0[o], P0[o + 1]}; };
+  auto g1 = [&](int col) { long o = (long)r * n1 + 2L * (zi * 4 + col); return cd{P1[o], P1[o + 1]}; };
+  auto g2 = [&](int col) { long o = (long)r * n1 + 2L * (zi * 4 + col); return cd{P2[o], P2[o + 1]}; };
+  cd R[3][3];
+  R[0][0] = g0(0) + g2(0);
+  R[1][0] = g0(1) + g2(1);
+  R[2][0] = g1(0);
+  R[0][1] = g0(2) + g2(2);
+  R[1][1] = g0(3) + g2(3);
+  R[2][1] = g1(1);
+  R[0][2] = g1(2);
+  R[1][2] = g1(3);
+  R[2][2] = g0(4);
+  double x = xs[i], y = ys[j];
+  double rho = hypot(x, y);
+  double cp = rho == 0.0 ? 1.0 : x / rho, sp = rho == 0.0 ? 0.0 : y / rho;
+  double Rot[3][3] = {{cp, -sp, 0.0}, {sp, cp, 0.0}, {0.0, 0.0, 1.0}};
+  for (int q = 0; q < 3; ++q)
+    for (int cc = 0; cc < 3; ++cc) {
+      cd s{0, 0};
+      for (int a = 0; a < 3; ++a) {
+        cd tt = Rot[cc][0] * R[0][a] + Rot[cc][1] * R[1][a] + Rot[cc][2] * R[2][a];
+        s += tt * Rot[q][a];
+      }
+      G[pix + npix * (zi + (long)nz * (cc + 3 * q))] = make_double2(s.x, s.y);
+    }
+}
+
+cudaError_t launch_assemble1d(int nx, int ny, int nz, const double* xs, const double* ys, const int* rmap, int nr,
+                              const double* P0, const double* P1, const double* P2, double2* G, cudaStream_t s) {
+  long tot = (long)nx * ny * nz;
+  k_assemble1d<<<(unsigned)((tot + 127) / 128), 128, 0, s>>>(nx, ny, nz, xs, ys, rmap, nr, P0, P1, P2, G);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// 2D strengths per (node, z-row): S[col'][n], col' = zi + nz (c + 3q)
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_strengths2d(SynthParams p, double2* S) {
+  long nidx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int zi = blockIdx.y;
+  const CacheView& c = p.c;
+  if (nidx >= c.n) return;
+  const long n = c.n;
+  long k = nidx % c.Nk, pp = nidx / c.Nk;
+  const double w = c.kr[k] * c.wr[k] * c.wphi[pp] / (4.0 * 3.14159265358979323846 * 3.14159265358979323846);
+  const cd W{w, 0.0};
+  cd Af[2][3], Ab[2][3];
+  reflected_amp(p, nidx, Af, Ab);
+  const double z = p.zo[zi];
+  cd Afd[2][3], Abd[2][3];
+  if (p.with_direct) direct_amp(p, nidx, z, Afd, Abd);
+  cd s[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) s[a][b] = cd{0, 0};
+  for (int m = 0; m < 2; ++m) {
+    cd pf = phase_cl(ldc(c.basis, 12 + m, n, nidx), z);
+    cd pb = phase_cl(ldc(c.basis, 14 + m, n, nidx), z - p.d_obs);
+    cd exf = ldc(c.basis, 0 + m, n, nidx), eyf = ldc(c.basis, 2 + m, n, nidx), ezf = ldc(c.basis, 4 + m, n, nidx);
+    cd exb = ldc(c.basis, 6 + m, n, nidx), eyb = ldc(c.basis, 8 + m, n, nidx), ezb = ldc(c.basis, 10 + m, n, nidx);
+    for (int q = 0; q < 3; ++q) {
+      cd tf = Af[m][q] * pf, tb = Ab[m][q] * pb;
+      if (p.with_direct) { tf += Afd[m][q]; tb += Abd[m][q]; }
+      cd af = fin0(W * tf), ab = fin0(W * tb);
+      s[0][q] += exf * af + exb * ab;
+      s[1][q] += eyf * af + eyb * ab;
+      s[2][q] += ezf * af + ezb * ab;
+    }
+  }
+  for (int q = 0; q < 3; ++q)
+    for (int cc = 0; cc < 3; ++cc) {
+      long col = zi + (long)p.nz * (cc + 3 * q);
+      S[col * n + nidx] = make_double2(s[cc][q].x, s[cc][q].y);
+    }
+}
+
+cudaError_t launch_strengths2d(const SynthParams& p, double2* S, cudaStream_t s) {
+  dim3 grid((unsigned)((p.c.n + 127) / 128), (unsigned)p.nz);
+  k_strengths2d<<<grid, 128, 0, s>>>(p, S);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// 2D lateral sum: G[pix][col] = Σ_n e^{i(kx_n x_i + ky_n y_j)} S[col][n] (complex FP64)
+// Tile: 64 pixels x 32 columns, 16 nodes per stage; 256 threads, 4 pixels x 2 columns each.
+// The phase operand is generated per stage in shared memory (sincos per node and
+// coordinate, then one complex product per (node, pixel)).
+// ------------------------------------------------------------------------------------
+constexpr int LP = 64, LC = 32, LK = 16;
+__global__ void __launch_bounds__(256) k_lateral(CacheView c, int nx, int ny, const double* __restrict__ xs,
+                                                 const double* __restrict__ ys, int ncol, const double2* __restrict__ S,
+                                                 double2* __restrict__ Gp, long kchunk) {
+  __shared__ double2 Ps[LK][LP];
+  __shared__ double2 Ss[LK][LC];
+  __shared__ double kxs[LK], kys[LK];
+  const long npix = (long)nx * ny;
+  const long p0 = (long)blockIdx.x * LP;
+  const int c0 = blockIdx.y * LC;
+  const int sp = blockIdx.z;
+  const long n = c.n;
+  const long k0 = (long)sp * kchunk, k1 = min(n, k0 + kchunk);
+  const int tid = threadIdx.x;
+  const int tp = tid % 16, tc = tid / 16;  // pixels tp + 16 a (a < 4), columns tc + 16 b (b < 2)
+  double2 acc[4][2];
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 2; ++b) acc[a][b] = make_double2(0.0, 0.0);
+  for (long kk = k0; kk < k1; kk += LK) {
+    if (tid < LK) {
+      long nn = kk + tid;
+      double kx = 0.0, ky = 0.0;
+      if (nn < k1) {
+        long k = nn % c.Nk, q = nn / c.Nk;
+        double s, co;
+        sincos(c.phi[q], &s, &co);
+        kx = c.kr[k] * co;
+        ky = c.kr[k] * s;
+      }
+      kxs[tid] = kx;
+      kys[tid] = ky;
+    }
+    __syncthreads();
+    // phases: LK x LP = 1024 products, 4 per thread
+    for (int e = 0; e < 4; ++e) {
+      int idx = tid + 256 * e;
+      int t = idx / LP, pl = idx % LP;
+      long pix = p0 + pl;
+      double2 v = make_double2(0.0, 0.0);
+      if (pix < npix && kk + t < k1) {
+        int i = (int)(pix % nx), j = (int)(pix / nx);
+        double sx, cx, sy, cy;
+        sincos(kxs[t] * xs[i], &sx, &cx);
+        sincos(kys[t] * ys[j], &sy, &cy);
+        v = make_double2(cx * cy - sx * sy, cx * sy + sx * cy);
+      }
+      Ps[t][pl] = v;
+    }
+    // strengths: LK x LC = 512, 2 per thread
+    for (int e = 0; e < 2; ++e) {
+      int idx = tid + 256 * e;
+      int t = idx % LK, cl = idx / LK;
+      long nn = kk + t;
+      int col = c0 + cl;
+      Ss[t][cl] = (nn < k1 && col < ncol) ? S[(long)col * n + nn] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int t = 0; t < LK; ++t) {
+      double2 pv[4], sv[2];
+      for (int a = 0; a < 4; ++a) pv[a] = Ps[t][tp + 16 * a];
+      for (int b = 0; b < 2; ++b) sv[b] = Ss[t][tc + 16 * b];
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 2; ++b) {
+          acc[a][b].x = fma(pv[a].x, sv[b].x, fma(-pv[a].y, sv[b].y, acc[a][b].x));
+          acc[a][b].y = fma(pv[a].x, sv[b].y, fma(pv[a].y, sv[b].x, acc[a][b].y));
+        }
+    }
+    __syncthreads();
+  }
+  double2* G = Gp + (long)sp * npix * ncol;
+  for (int a = 0; a < 4; ++a) {
+    long pix = p0 + tp + 16 * a;
+    if (pix >= npix) continue;
+    for (int b = 0; b < 2; ++b) {
+      int col = c0 + tc + 16 * b;
+      if (col < ncol) G[pix + npix * col] = acc[a][b];
+    }
+  }
+}
+
+__global__ void k_reduce_splits2(long len, int splits, const double2* __restrict__ P, double2* __restrict__ C) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= len) return;
+  double2 s = make_double2(0.0, 0.0);
+  for (int k = 0; k < splits; ++k) {
+    double2 v = P[(long)k * len + i];
+    s.x += v.x;
+    s.y += v.y;
+  }
+  C[i] = s;
+}
+
+int lateral_splits(long n, int splits) {
+  long kchunk = (n + splits - 1) / splits;
+  kchunk = ((kchunk + LK - 1) / LK) * LK;
+  if (kchunk <= 0) return 1;
+  return (int)std::max(1L, (n + kchunk - 1) / kchunk);
+}
+
+cudaError_t launch_lateral(const CacheView& c, int nx, int ny, const double* xs, const double* ys, int ncol, const double2* S,
+                           double2* partial, int splits, cudaStream_t s) {
+  long npix = (long)nx * ny;
+  splits = lateral_splits(c.n, splits);
+  long kchunk = (c.n + splits - 1) / splits;
+  kchunk = ((kchunk + LK - 1) / LK) * LK;
+  dim3 grid((unsigned)((npix + LP - 1) / LP), (unsigned)((ncol + LC - 1) / LC), (unsigned)splits);
+  k_lateral<<<grid, 256, 0, s>>>(c, nx, ny, xs, ys, ncol, S, partial, kchunk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_splits2(long len, int splits, const double2* partial, double2* G, cudaStream_t s) {
+  if (len <= 0) return cudaSuccess;
+  k_reduce_splits2<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(len, splits, partial, G);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// gl_rule panel expansion (mod_KxGrid.jl:361-384), no FMA contraction: bit-exact with a
+// CPU evaluation of the same expressions in IEEE double
+// ------------------------------------------------------------------------------------
+__global__ void k_gl_nodes(int npanels, const double* pa, const double* pb, const int* sing_side, const double* xi,
+                           const double* wx, int order, double* nodes, double* wts) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)npanels * order) return;
+  int pi = (int)(t / order), j = (int)(t % order);
+  double a = pa[pi], b = pb[pi];
+  int sg = sing_side[pi];  // 0 regular, +1 singular at a, -1 singular at b
+  if (sg == 0) {
+    double h = __dmul_rn(0.5, __dsub_rn(b, a));
+    double cc = __dmul_rn(0.5, __dadd_rn(a, b));
+    nodes[t] = __dadd_rn(cc, __dmul_rn(h, xi[j]));
+    wts[t] = __dmul_rn(h, wx[j]);
+  } else {
+    double L = sg > 0 ? a : b;
+    double U = __dsqrt_rn(__dsub_rn(b, a));
+    double hU = __dmul_rn(0.5, U);
+    double u = __dmul_rn(hU, __dadd_rn(1.0, xi[j]));
+    nodes[t] = __dadd_rn(L, __dmul_rn((double)sg, __dmul_rn(u, u)));
+    wts[t] = __dmul_rn(__dmul_rn(hU, wx[j]), __dmul_rn(2.0, u));
+  }
+}
+
+cudaError_t launch_gl_nodes(int npanels, const double* pa, const double* pb, const int* sing_side, const double* xi,
+                            const double* wx, int order, double* nodes, double* wts, cudaStream_t s) {
+  long tot = (long)npanels * order;
+  if (tot == 0) return cudaSuccess;
+  k_gl_nodes<<<(unsigned)((tot + 127) / 128), 128, 0, s>>>(npanels, pa, pb, sing_side, xi, wx, order, nodes, wts);
+  return cudaGetLastError();
+}
+
+}  // namespace ytf

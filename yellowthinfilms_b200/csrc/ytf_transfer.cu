@@ -1,0 +1,823 @@
+// ytf_transfer.cu -- per-k-node spectral solve on sm_100a: Berreman modes, S-matrix
+// cascade, cavity transfer map T^o, source projection and observation-layer mode basis.
+//
+// Replaces build_cavity_transfer_1d / build_cavity_transfer_2d
+// (mod_CavityTransfer.jl:196-258, 307-398) and everything they call per node
+// (mod_ModeSolver.jl, mod_ScatteringMatrix.jl, mod_FieldSolver.jl:72-341,
+// mod_SourceProj.jl:34-60).
+//
+// Work decomposition (B200-first, not a translation of the reference's loops):
+//   k_layer_modes : one thread per (node, layer). Closed-form TE/TM modes for
+//                   isotropic/uniaxial layers, otherwise a balanced complex Hessenberg QR
+//                   of the 4x4 Berreman matrix. Eigenvectors are normalised as LAPACK's
+//                   ZGEEVX does (unit 2-norm), eigenpairs sorted by (real, imag) as Julia's
+//                   eigen, then split forward/backward by Poynting flux. Layer-major
+//                   indexing keeps one layer (one material kind) per warp: no divergence
+//                   between the closed-form and the general path.
+//   k_chain       : one thread per node. Mode matching through the stack, interface
+//                   matrices, forward/backward Redheffer scans, cavity resummation, the
+//                   stack walk reduced to the observation layers, T^o, seeds and basis.
+//   k_rotate_fill : one thread per (kρ, φ) node of an azimuthally symmetric 2D grid: the
+//                   φ = 0 solve rotated exactly (mod_ModeSolver.jl:471-482).
+// Per-(node, layer) intermediates live in a global scratch arena, structure-of-arrays
+// with the node index fastest, so every warp access is one contiguous 512-byte line.
+// All arithmetic is FP64 (B200 runs FP64 at half the FP32 rate; the branchy mode
+// classification and the near-singular 2x2 solves keep the reference's FP64 semantics).
+#include "ytf_complex.cuh"
+#include "ytf_kernels.h"
+
+namespace ytf {
+
+// ------------------------------------------------------------------------------------
+// scratch / output accessors (SoA: element-major, node fastest)
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ cd ld(const double2* base, long elem, long n, long node) {
+  double2 v = base[elem * n + node];
+  return cd{v.x, v.y};
+}
+__device__ __forceinline__ void st(double2* base, long elem, long n, long node, cd v) {
+  base[elem * n + node] = make_double2(v.x, v.y);
+}
+
+__device__ __forceinline__ const cd& E(const LayerDev& L, int i, int j) { return *reinterpret_cast<const cd*>(&L.eps[2 * ((i - 1) + 3 * (j - 1))]); }
+__device__ __forceinline__ const cd& U(const LayerDev& L, int i, int j) { return *reinterpret_cast<const cd*>(&L.mu[2 * ((i - 1) + 3 * (j - 1))]); }
+
+__device__ __forceinline__ void node_k(const TransferParams& p, long node, double& kx, double& ky) {
+  if (p.mode == 0) {  // 1D radial nodes kt = (kx, 0)
+    kx = p.kr[node];
+    ky = 0.0;
+  } else if (p.mode == 1) {  // full 2D solve, node = k + Nk * q
+    long k = node % p.Nk, q = node / p.Nk;
+    double s, c;
+    sincos(p.phi[q], &s, &c);
+    kx = p.kr[k] * c;
+    ky = p.kr[k] * s;
+  } else {  // rotation base: φ = 0
+    kx = p.kr[node] * 1.0;
+    ky = p.kr[node] * 0.0;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Berreman matrix (mod_ModeSolver.jl:122-193), real in-plane wavevector
+// ------------------------------------------------------------------------------------
+__device__ void berreman(const LayerDev& L, double w, double kx, double ky, cd B[4][4]) {
+  cd e11 = E(L, 1, 1), e12 = E(L, 1, 2), e21 = E(L, 2, 1), e22 = E(L, 2, 2);
+  cd e13 = E(L, 1, 3), e23 = E(L, 2, 3), e31 = E(L, 3, 1), e32 = E(L, 3, 2), e33 = E(L, 3, 3);
+  cd m11 = U(L, 1, 1), m12 = U(L, 1, 2), m21 = U(L, 2, 1), m22 = U(L, 2, 2);
+  cd m13 = U(L, 1, 3), m23 = U(L, 2, 3), m31 = U(L, 3, 1), m32 = U(L, 3, 2), m33 = U(L, 3, 3);
+  cd k1{kx, 0.0}, k2{ky, 0.0};
+  cd de = recip(e33), dm = recip(m33);
+  cd iw{1.0 / w, 0.0};
+  cd Se11 = e11 - e13 * de * e31, Se12 = e12 - e13 * de * e32;
+  cd Se21 = e21 - e23 * de * e31, Se22 = e22 - e23 * de * e32;
+  cd Sm11 = m11 - m13 * dm * m31, Sm12 = m12 - m13 * dm * m32;
+  cd Sm21 = m21 - m23 * dm * m31, Sm22 = m22 - m23 * dm * m32;
+  cd re1 = de * e31, re2 = de * e32, se1 = e13 * de, se2 = e23 * de;
+  cd rm1 = dm * m31, rm2 = dm * m32, sm1 = m13 * dm, sm2 = m23 * dm;
+  cd t21 = -conj(k2), t22 = conj(k1);
+  cd t31 = iw * k1, t32 = iw * k2;
+  cd Rsm1 = sm2, Rsm2 = -sm1, Rse1 = se2, Rse2 = -se1;
+  B[0][0] = Rsm1 * t21 - k1 * re1; B[0][1] = Rsm1 * t22 - k1 * re2;
+  B[1][0] = Rsm2 * t21 - k2 * re1; B[1][1] = Rsm2 * t22 - k2 * re2;
+  B[0][2] = w * Sm21 - t31 * de * t21; B[0][3] = w * Sm22 - t31 * de * t22;
+  B[1][2] = (-w) * Sm11 - t32 * de * t21; B[1][3] = (-w) * Sm12 - t32 * de * t22;
+  B[2][0] = t31 * dm * t21 - w * Se21; B[2][1] = t31 * dm * t22 - w * Se22;
+  B[3][0] = t32 * dm * t21 - (-w) * Se11; B[3][1] = t32 * dm * t22 - (-w) * Se12;
+  B[2][2] = Rse1 * t21 - k1 * rm1; B[2][3] = Rse1 * t22 - k1 * rm2;
+  B[3][2] = Rse2 * t21 - k2 * rm1; B[3][3] = Rse2 * t22 - k2 * rm2;
+}
+
+// ------------------------------------------------------------------------------------
+// General 4x4 complex eigen solve: diagonal balancing, Householder reduction to
+// Hessenberg form, single-shift complex QR with Wilkinson shifts and full Schur-vector
+// accumulation, eigenvectors of the triangular factor by back substitution.
+// Published algorithm (Golub & Van Loan, Matrix Computations, §7.4-7.6; the LAPACK
+// ZGEBAL/ZGEHRD/ZLAHQR/ZTREVC sequence). Returns false if QR does not converge.
+// ------------------------------------------------------------------------------------
+__device__ bool eig4(cd A[4][4], cd lam[4], cd V[4][4]) {
+  // balancing by powers of 2 (scaling only, as ZGEBAL with job 'S')
+  double D[4] = {1.0, 1.0, 1.0, 1.0};
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    bool changed = false;
+    for (int i = 0; i < 4; ++i) {
+      double c = 0.0, r = 0.0;
+      for (int j = 0; j < 4; ++j)
+        if (j != i) { c += cabs1(A[j][i]); r += cabs1(A[i][j]); }
+      if (c == 0.0 || r == 0.0) continue;
+      double s = c + r, f = 1.0, g = r / 2.0;
+      while (c < g && f < 1e150) { f *= 2.0; c *= 2.0; r /= 2.0; g /= 2.0; }
+      g = c / 2.0;
+      while (g >= r && f > 1e-150) { f /= 2.0; c /= 2.0; g /= 2.0; r *= 2.0; }
+      if (c + r >= 0.95 * s) continue;
+      changed = true;
+      D[i] *= f;
+      for (int j = 0; j < 4; ++j) { A[i][j] = A[i][j] * (1.0 / f); A[j][i] = A[j][i] * f; }
+    }
+    if (!changed) break;
+  }
+  cd Z[4][4];
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) Z[i][j] = cd{i == j ? 1.0 : 0.0, 0.0};
+  // Householder reduction to upper Hessenberg
+  for (int k = 0; k < 2; ++k) {
+    double xn = 0.0;
+    for (int i = k + 1; i < 4; ++i) xn += norm2(A[i][k]);
+    if (xn == 0.0) continue;
+    xn = sqrt(xn);
+    cd a = A[k + 1][k];
+    double aa = cabs(a);
+    cd ph = aa > 0.0 ? a * (1.0 / aa) : cd{1.0, 0.0};
+    cd v[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    v[k + 1] = a + ph * xn;
+    for (int i = k + 2; i < 4; ++i) v[i] = A[i][k];
+    double vn = 0.0;
+    for (int i = k + 1; i < 4; ++i) vn += norm2(v[i]);
+    if (vn == 0.0) continue;
+    double tau = 2.0 / vn;
+    // A <- (I - tau v v^H) A
+    for (int j = 0; j < 4; ++j) {
+      cd s{0, 0};
+      for (int i = k + 1; i < 4; ++i) s += conj(v[i]) * A[i][j];
+      s = s * tau;
+      for (int i = k + 1; i < 4; ++i) A[i][j] -= v[i] * s;
+    }
+    // A <- A (I - tau v v^H), Z <- Z (I - tau v v^H)
+    for (int i = 0; i < 4; ++i) {
+      cd s{0, 0}, t{0, 0};
+      for (int j = k + 1; j < 4; ++j) { s += A[i][j] * v[j]; t += Z[i][j] * v[j]; }
+      s = s * tau; t = t * tau;
+      for (int j = k + 1; j < 4; ++j) { A[i][j] -= s * conj(v[j]); Z[i][j] -= t * conj(v[j]); }
+    }
+    for (int i = k + 2; i < 4; ++i) A[i][k] = cd{0, 0};
+  }
+  // shifted QR on the Hessenberg matrix
+  const double eps = 2.220446049250313e-16;
+  int hi = 3, its = 0, total = 0;
+  while (hi > 0) {
+    int l = hi;
+    while (l > 0) {
+      double s = cabs1(A[l - 1][l - 1]) + cabs1(A[l][l]);
+      if (cabs1(A[l][l - 1]) <= eps * s || cabs1(A[l][l - 1]) < 1e-300) { A[l][l - 1] = cd{0, 0}; break; }
+      --l;
+    }
+    if (l == hi) { --hi; its = 0; continue; }
+    if (++total > 120) return false;
+    ++its;
+    cd mu;
+    if (its == 10 || its == 20) {
+      mu = A[hi][hi] + cd{0.75 * fabs(A[hi][hi - 1].x), 0.0};  // exceptional shift
+    } else {
+      cd a = A[hi - 1][hi - 1], b = A[hi - 1][hi], c = A[hi][hi - 1], d = A[hi][hi];
+      cd hd = (a - d) * 0.5;
+      cd disc = csqrt(hd * hd + b * c);
+      cd m1 = d - (b * c) / (hd + disc), m2 = d - (b * c) / (hd - disc);
+      if (iszero(hd + disc)) m1 = d;
+      if (iszero(hd - disc)) m2 = d;
+      mu = norm2(m1 - d) <= norm2(m2 - d) ? m1 : m2;
+      if (!isfin(mu)) mu = d;
+    }
+    cd x = A[l][l] - mu, y = A[l + 1][l];
+    for (int k = l; k < hi; ++k) {
+      if (k > l) { x = A[k][k - 1]; y = A[k + 1][k - 1]; }
+      double ax = cabs(x), ay = cabs(y);
+      double nr = hypot(ax, ay);
+      cd c, s;
+      if (ay == 0.0) { c = cd{1.0, 0.0}; s = cd{0.0, 0.0}; }
+      else if (ax == 0.0) { c = cd{0.0, 0.0}; s = conj(y) * (1.0 / ay); }
+      else { c = cd{ax / nr, 0.0}; s = (x * (1.0 / ax)) * conj(y) * (1.0 / nr); }
+      // rows k, k+1 (all columns from k-1 for the full Schur form)
+      for (int j = (k > 0 ? k - 1 : 0); j < 4; ++j) {
+        cd h1 = A[k][j], h2 = A[k + 1][j];
+        A[k][j] = c * h1 + s * h2;
+        A[k + 1][j] = c * h2 - conj(s) * h1;
+      }
+      int rmax = k + 2 < hi ? k + 2 : hi;
+      for (int i = 0; i <= rmax; ++i) {
+        cd h1 = A[i][k], h2 = A[i][k + 1];
+        A[i][k] = c * h1 + conj(s) * h2;
+        A[i][k + 1] = c * h2 - s * h1;
+      }
+      for (int i = 0; i < 4; ++i) {
+        cd z1 = Z[i][k], z2 = Z[i][k + 1];
+        Z[i][k] = c * z1 + conj(s) * z2;
+        Z[i][k + 1] = c * z2 - s * z1;
+      }
+      if (k > l) A[k + 1][k - 1] = cd{0, 0};
+    }
+  }
+  for (int i = 0; i < 4; ++i) lam[i] = A[i][i];
+  // eigenvectors of the upper-triangular Schur factor
+  double anorm = 0.0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) anorm = fmax(anorm, cabs1(A[i][j]));
+  double smin = fmax(eps * anorm, 1e-290);
+  for (int k = 0; k < 4; ++k) {
+    cd xv[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    xv[k] = cd{1.0, 0.0};
+    for (int i = k - 1; i >= 0; --i) {
+      cd s{0, 0};
+      for (int j = i + 1; j <= k; ++j) s += A[i][j] * xv[j];
+      cd den = A[i][i] - A[k][k];
+      if (cabs1(den) < smin) den = cd{smin, 0.0};
+      xv[i] = -(s / den);
+    }
+    cd v[4];
+    for (int i = 0; i < 4; ++i) {
+      cd s{0, 0};
+      for (int j = 0; j <= k; ++j) s += Z[i][j] * xv[j];
+      v[i] = s * D[i];
+    }
+    // LAPACK normalisation: unit 2-norm, largest component real
+    double nn = 0.0, best = -1.0;
+    int ib = 0;
+    for (int i = 0; i < 4; ++i) {
+      double a2 = norm2(v[i]);
+      nn += a2;
+      if (a2 > best) { best = a2; ib = i; }
+    }
+    double inv = 1.0 / sqrt(nn);
+    cd ph = conj(v[ib]) * (1.0 / sqrt(best));
+    for (int i = 0; i < 4; ++i) V[i][k] = (v[i] * ph) * inv;
+  }
+  // sort eigenpairs by (real, imag) (Julia's eigsortby), stable insertion sort
+  for (int i = 1; i < 4; ++i) {
+    for (int j = i; j > 0; --j) {
+      bool sw = lam[j].x < lam[j - 1].x || (lam[j].x == lam[j - 1].x && lam[j].y < lam[j - 1].y);
+      if (!sw) break;
+      cd t = lam[j]; lam[j] = lam[j - 1]; lam[j - 1] = t;
+      for (int r = 0; r < 4; ++r) { cd u = V[r][j]; V[r][j] = V[r][j - 1]; V[r][j - 1] = u; }
+    }
+  }
+  return true;
+}
+
+// closed-form TE/TM modes (mod_ModeSolver.jl:243-265)
+__device__ void closed_modes(const LayerDev& L, double w, double kx, double ky, cd Q[4], cd V[4][4]) {
+  cd et = E(L, 1, 1), ez = E(L, 3, 3), mr = U(L, 1, 1);
+  cd wc{w, 0.0};
+  double kr = hypot(kx, ky);
+  double phi = kr == 0 ? 0.0 : atan2(ky, kx);
+  double s, c;
+  sincos(phi, &s, &c);
+  cd kzo = csqrt(wc * wc * et * mr - cd{kr * kr, 0.0});
+  cd kze = csqrt(et * (wc * wc * mr - cd{kr * kr, 0.0} / ez));
+  cd A = recip(wc * mr), Bn = recip(wc * et);
+  cd mA = -A, mB = -Bn;
+  V[0][0] = cd{-s, 0}; V[1][0] = cd{c, 0}; V[2][0] = mA * kzo * c; V[3][0] = mA * kzo * s;
+  V[0][1] = cd{-s, 0}; V[1][1] = cd{c, 0}; V[2][1] = A * kzo * c; V[3][1] = A * kzo * s;
+  V[0][2] = Bn * kze * c; V[1][2] = Bn * kze * s; V[2][2] = cd{-s, 0}; V[3][2] = cd{c, 0};
+  V[0][3] = mB * kze * c; V[1][3] = mB * kze * s; V[2][3] = cd{-s, 0}; V[3][3] = cd{c, 0};
+  Q[0] = kzo; Q[1] = -kzo; Q[2] = kze; Q[3] = -kze;
+}
+
+// ------------------------------------------------------------------------------------
+// K1: modes of one (node, layer), sorted forward/backward (mod_ModeSolver.jl:274-326).
+// Scratch record per (layer, node): Vf[4x2] (8), Vb[4x2] (8), Qf (2), Qb (2); column-major.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_layer_modes(TransferParams p) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long n = p.n;
+  if (t >= n * p.nL) return;
+  int layer = (int)(t / n);
+  long node = t - (long)layer * n;
+  double kx, ky;
+  node_k(p, p.off + node, kx, ky);
+  const LayerDev& L = p.layers[layer];
+  cd Q[4], V[4][4];
+  uint8_t stat = 0;
+  if ((L.ekind == 0 || L.ekind == 1) && L.mkind == 0) {
+    closed_modes(L, p.omega, kx, ky, Q, V);
+  } else {
+    cd B[4][4];
+    berreman(L, p.omega, kx, ky, B);
+    if (!eig4(B, Q, V)) stat |= ST_EIGEN;
+  }
+  // Poynting flux Pz = ¼ Re(V_j · W_j), W = R4s V = (V3, -V2, -V1, V0)
+  double Pz[4];
+  for (int j = 0; j < 4; ++j) {
+    cd s = conj(V[0][j]) * V[3][j];
+    s += conj(V[1][j]) * (-V[2][j]);
+    s += conj(V[2][j]) * (-V[1][j]);
+    s += conj(V[3][j]) * V[0][j];
+    Pz[j] = 0.25 * s.x;
+  }
+  const double tol = 1.4901161193847656e-08;
+  int fsel[2] = {-1, -1}, bsel[2] = {-1, -1}, deg[4];
+  int nf = 0, nb = 0, nd = 0;
+  for (int j = 0; j < 4; ++j) {
+    if (fabs(Pz[j]) > tol) {
+      if (Pz[j] > 0) { if (nf < 2) fsel[nf] = j; ++nf; }
+      else { if (nb < 2) bsel[nb] = j; ++nb; }
+    } else if (fabs(Q[j].y) > tol) {
+      if (Q[j].y > tol) { if (nf < 2) fsel[nf] = j; ++nf; }
+      else if (Q[j].y < -tol) { if (nb < 2) bsel[nb] = j; ++nb; }
+    } else {
+      deg[nd++] = j;
+    }
+  }
+  if (nf > 2 || nb > 2) stat |= ST_SORT;
+  for (int i = 0; i < nd; ++i) {
+    if (nf < 2) fsel[nf++] = deg[i];
+    else if (nb < 2) bsel[nb++] = deg[i];
+  }
+  double2* rec = p.modes + (long)layer * 20 * n;
+  for (int m = 0; m < 2; ++m) {
+    int jf = fsel[m], jb = bsel[m];
+    for (int i = 0; i < 4; ++i) {
+      st(rec, i + 4 * m, n, node, jf >= 0 ? V[i][jf] : cd{0, 0});
+      st(rec, 8 + i + 4 * m, n, node, jb >= 0 ? V[i][jb] : cd{0, 0});
+    }
+    st(rec, 16 + m, n, node, jf >= 0 ? Q[jf] : cd{0, 0});
+    st(rec, 18 + m, n, node, jb >= 0 ? Q[jb] : cd{0, 0});
+  }
+  p.lstat[(long)layer * n + node] = stat;
+}
+
+// ------------------------------------------------------------------------------------
+// K2 helpers
+// ------------------------------------------------------------------------------------
+struct Mode4 {  // one layer's modes: Vf, Vb (4x2, V[i][m]), Qf, Qb
+  cd vf[4][2], vb[4][2], qf[2], qb[2];
+};
+
+__device__ __forceinline__ void load_modes(const TransferParams& p, int layer, long node, Mode4& M) {
+  const double2* rec = p.modes + (long)layer * 20 * p.n;
+  for (int m = 0; m < 2; ++m) {
+    for (int i = 0; i < 4; ++i) {
+      M.vf[i][m] = ld(rec, i + 4 * m, p.n, node);
+      M.vb[i][m] = ld(rec, 8 + i + 4 * m, p.n, node);
+    }
+    M.qf[m] = ld(rec, 16 + m, p.n, node);
+    M.qb[m] = ld(rec, 18 + m, p.n, node);
+  }
+}
+__device__ __forceinline__ void store_modes(const TransferParams& p, int layer, long node, const Mode4& M) {
+  double2* rec = p.modes + (long)layer * 20 * p.n;
+  for (int m = 0; m < 2; ++m) {
+    for (int i = 0; i < 4; ++i) {
+      st(rec, i + 4 * m, p.n, node, M.vf[i][m]);
+      st(rec, 8 + i + 4 * m, p.n, node, M.vb[i][m]);
+    }
+    st(rec, 16 + m, p.n, node, M.qf[m]);
+    st(rec, 18 + m, p.n, node, M.qb[m]);
+  }
+}
+// W = R4s V row map: W0 = V3, W1 = -V2, W2 = -V1, W3 = V0
+__device__ __forceinline__ cd Wof(const cd v[4][2], int i, int m) {
+  switch (i) {
+    case 0: return v[3][m];
+    case 1: return -v[2][m];
+    case 2: return -v[1][m];
+    default: return v[0][m];
+  }
+}
+// _match_modes (mod_ModeSolver.jl:333-349) for one direction: swap b's columns if needed
+__device__ __forceinline__ void match_dir(const cd wa_src[4][2], cd vb[4][2], cd qb[2]) {
+  cd C[2][2];
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      cd s = conj(Wof(wa_src, 0, a)) * vb[0][b];
+      for (int i = 1; i < 4; ++i) s += conj(Wof(wa_src, i, a)) * vb[i][b];
+      C[a][b] = s;
+    }
+  double sid = norm2(C[0][0]) + norm2(C[1][1]);
+  double ssw = norm2(C[0][1]) + norm2(C[1][0]);
+  if (ssw > sid) {
+    for (int i = 0; i < 4; ++i) { cd t = vb[i][0]; vb[i][0] = vb[i][1]; vb[i][1] = t; }
+    cd t = qb[0]; qb[0] = qb[1]; qb[1] = t;
+  }
+}
+
+// 4x4 LU solve with partial pivoting, NR right-hand sides; false on an exact zero pivot
+template <int NR>
+__device__ __forceinline__ bool lu_solve4(cd A[4][4], cd B[4][NR]) {
+  for (int k = 0; k < 4; ++k) {
+    int pv = k;
+    double best = norm2(A[k][k]);
+    for (int i = k + 1; i < 4; ++i) {
+      double v = norm2(A[i][k]);
+      if (v > best) { best = v; pv = i; }
+    }
+    if (best == 0.0) return false;
+    if (pv != k) {
+      for (int j = 0; j < 4; ++j) { cd t = A[pv][j]; A[pv][j] = A[k][j]; A[k][j] = t; }
+      for (int j = 0; j < NR; ++j) { cd t = B[pv][j]; B[pv][j] = B[k][j]; B[k][j] = t; }
+    }
+    cd piv = recip(A[k][k]);
+    for (int i = k + 1; i < 4; ++i) {
+      cd l = A[i][k] * piv;
+      for (int j = k + 1; j < 4; ++j) A[i][j] -= l * A[k][j];
+      for (int j = 0; j < NR; ++j) B[i][j] -= l * B[k][j];
+    }
+  }
+  for (int j = 0; j < NR; ++j)
+    for (int i = 3; i >= 0; --i) {
+      cd s = B[i][j];
+      for (int k = i + 1; k < 4; ++k) s -= A[i][k] * B[k][j];
+      B[i][j] = s / A[i][i];
+    }
+  return true;
+}
+
+// _S_Interface_Matrix (mod_ScatteringMatrix.jl:27-47): [-Vf_B Vb_A] \ [-Vf_A Vb_B]
+__device__ __forceinline__ bool interface_matrix(const Mode4& A, const Mode4& B, S4& S) {
+  cd L[4][4], R[4][4];
+  for (int i = 0; i < 4; ++i) {
+    L[i][0] = -B.vf[i][0]; L[i][1] = -B.vf[i][1]; L[i][2] = A.vb[i][0]; L[i][3] = A.vb[i][1];
+    R[i][0] = -A.vf[i][0]; R[i][1] = -A.vf[i][1]; R[i][2] = B.vb[i][0]; R[i][3] = B.vb[i][1];
+  }
+  bool ok = lu_solve4<4>(L, R);
+  S.b11 = M2{R[0][0], R[0][1], R[1][0], R[1][1]};
+  S.b12 = M2{R[0][2], R[0][3], R[1][2], R[1][3]};
+  S.b21 = M2{R[2][0], R[2][1], R[3][0], R[3][1]};
+  S.b22 = M2{R[2][2], R[2][3], R[3][2], R[3][3]};
+  return ok;
+}
+
+__device__ __forceinline__ void st_s4(double2* base, long slot, long n, long node, const S4& S) {
+  double2* b = base + slot * 16 * n;
+  const cd* v = reinterpret_cast<const cd*>(&S);
+  for (int e = 0; e < 16; ++e) st(b, e, n, node, v[e]);
+}
+__device__ __forceinline__ S4 ld_s4(const double2* base, long slot, long n, long node) {
+  S4 S;
+  cd* v = reinterpret_cast<cd*>(&S);
+  const double2* b = base + slot * 16 * n;
+  for (int e = 0; e < 16; ++e) v[e] = ld(b, e, n, node);
+  return S;
+}
+
+// Source_projection_Berreman_xyz (mod_SourceProj.jl:34-60); returns (sif, sib) 2x3 each
+__device__ bool source_projection(double kx, double ky, double w, const LayerDev& L, const Mode4& M, cd sif[2][3], cd sib[2][3]) {
+  cd etz1 = E(L, 1, 3), etz2 = E(L, 2, 3), ezz = E(L, 3, 3);
+  cd jw{0.0, -w};
+  cd J[4][3];
+  cd ezw = ezz * w;
+  cd jz = jw;  // (-iω)·ẑ column only
+  for (int q = 0; q < 3; ++q) {
+    cd z = q == 2 ? jz : cd{0.0, 0.0} * jw;
+    J[0][q] = cd{kx, 0.0} * z / ezw;
+    J[1][q] = cd{ky, 0.0} * z / ezw;
+    cd jtx = q == 0 ? jw : cd{0.0, 0.0}, jty = q == 1 ? jw : cd{0.0, 0.0};
+    J[2][q] = jty - etz2 * z / ezz;
+    J[3][q] = -jtx - (-etz1) * z / ezz;
+  }
+  cd V[4][4], W[4][4];
+  for (int i = 0; i < 4; ++i) {
+    V[i][0] = M.vf[i][0]; V[i][1] = M.vf[i][1]; V[i][2] = M.vb[i][0]; V[i][3] = M.vb[i][1];
+  }
+  for (int j = 0; j < 4; ++j) {
+    W[0][j] = V[3][j]; W[1][j] = -V[2][j]; W[2][j] = -V[1][j]; W[3][j] = V[0][j];
+  }
+  cd WV[4][4], WJ[4][3];
+  for (int a = 0; a < 4; ++a) {
+    for (int b = 0; b < 4; ++b) {
+      cd s = conj(W[0][a]) * V[0][b];
+      for (int i = 1; i < 4; ++i) s += conj(W[i][a]) * V[i][b];
+      WV[a][b] = s;
+    }
+    for (int q = 0; q < 3; ++q) {
+      cd s = conj(W[0][a]) * J[0][q];
+      for (int i = 1; i < 4; ++i) s += conj(W[i][a]) * J[i][q];
+      WJ[a][q] = s;
+    }
+  }
+  if (!lu_solve4<3>(WV, WJ)) return false;
+  for (int q = 0; q < 3; ++q) {
+    sif[0][q] = WJ[0][q]; sif[1][q] = WJ[1][q];
+    sib[0][q] = WJ[2][q]; sib[1][q] = WJ[3][q];
+  }
+  return true;
+}
+
+// mode field basis of one obs layer (mod_CavityTransfer.jl:87-130)
+__device__ void write_basis(const TransferParams& p, int oi, long node, long nout, const LayerDev& L, const Mode4& M,
+                            double kx, double ky) {
+  cd ezt1 = E(L, 3, 1), ezt2 = E(L, 3, 2), ezz = E(L, 3, 3);
+  double iw = 1.0 / p.omega;
+  double2* b = p.basis + (long)oi * 16 * nout;
+  for (int m = 0; m < 2; ++m) {
+    cd exf = M.vf[0][m], eyf = M.vf[1][m];
+    cd ezf = -(ezt1 * M.vf[0][m] + ezt2 * M.vf[1][m] + iw * (cd{kx, 0} * M.vf[3][m] - cd{ky, 0} * M.vf[2][m])) / ezz;
+    cd exb = M.vb[0][m], eyb = M.vb[1][m];
+    cd ezb = -(ezt1 * M.vb[0][m] + ezt2 * M.vb[1][m] + iw * (cd{kx, 0} * M.vb[3][m] - cd{ky, 0} * M.vb[2][m])) / ezz;
+    cd kzf = M.qf[m], kzb = M.qb[m];
+    bool ok = isfin(exf) && isfin(eyf) && isfin(ezf) && isfin(exb) && isfin(eyb) && isfin(ezb) && isfin(kzf) && isfin(kzb);
+    cd z{0, 0};
+    st(b, 0 + m, nout, node, ok ? exf : z);
+    st(b, 2 + m, nout, node, ok ? eyf : z);
+    st(b, 4 + m, nout, node, ok ? ezf : z);
+    st(b, 6 + m, nout, node, ok ? exb : z);
+    st(b, 8 + m, nout, node, ok ? eyb : z);
+    st(b, 10 + m, nout, node, ok ? ezb : z);
+    st(b, 12 + m, nout, node, ok ? kzf : z);
+    st(b, 14 + m, nout, node, ok ? kzb : z);
+  }
+}
+
+__device__ __forceinline__ void write_seeds(const TransferParams& p, long node, long nout, const Mode4& M, cd sif[2][3], cd sib[2][3]) {
+  for (int m = 0; m < 2; ++m) {
+    st(p.Qf, m, nout, node, M.qf[m]);
+    st(p.Qb, m, nout, node, M.qb[m]);
+    for (int q = 0; q < 3; ++q) {
+      st(p.sf, m + 2 * q, nout, node, sif[m][q]);
+      st(p.sb, m + 2 * q, nout, node, -sib[m][q]);
+    }
+  }
+}
+
+// 2x4 matrix (two column pairs)
+struct M24 {
+  M2 L, R;
+};
+__device__ __forceinline__ M24 mul24(const M2& A, const M24& B) { return M24{mul(A, B.L), mul(A, B.R)}; }
+__device__ __forceinline__ M24 add24(const M24& A, const M24& B) { return M24{add(A.L, B.L), add(A.R, B.R)}; }
+__device__ __forceinline__ M24 dl24(cd p0, cd p1, const M24& A) { return M24{dl(p0, p1, A.L), dl(p0, p1, A.R)}; }
+__device__ __forceinline__ M2 flush2(const M2& A) { return M2{flush(A.a00), flush(A.a01), flush(A.a10), flush(A.a11)}; }
+__device__ __forceinline__ M24 flush24(const M24& A) { return M24{flush2(A.L), flush2(A.R)}; }
+__device__ __forceinline__ bool fin2(const M2& A) { return isfin(A.a00) && isfin(A.a01) && isfin(A.a10) && isfin(A.a11); }
+
+__device__ __forceinline__ void write_T(const TransferParams& p, int oi, long idx, long nT, const M24& Ef, const M24& Eb) {
+  // T^o = [Ef; Eb] (4x4), stored column-major: element r + 4 c
+  double2* b = p.Tout + (long)oi * 16 * nT;
+  const M24* rows[2] = {&Ef, &Eb};
+  for (int h = 0; h < 2; ++h) {
+    const M24& X = *rows[h];
+    st(b, 2 * h + 0 + 4 * 0, nT, idx, X.L.a00); st(b, 2 * h + 0 + 4 * 1, nT, idx, X.L.a01);
+    st(b, 2 * h + 1 + 4 * 0, nT, idx, X.L.a10); st(b, 2 * h + 1 + 4 * 1, nT, idx, X.L.a11);
+    st(b, 2 * h + 0 + 4 * 2, nT, idx, X.R.a00); st(b, 2 * h + 0 + 4 * 3, nT, idx, X.R.a01);
+    st(b, 2 * h + 1 + 4 * 2, nT, idx, X.R.a10); st(b, 2 * h + 1 + 4 * 3, nT, idx, X.R.a11);
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// K2: per-node chain
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_chain(TransferParams p) {
+  long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long n = p.n;
+  if (node >= n) return;
+  const int N = p.nL, src = p.src;
+  const bool base = p.mode == 2;  // rotation base: seeds/basis are filled per φ later
+  const long nT = base ? n : p.nout;
+  const long gnode = base ? node : p.off + node;  // index into the outputs
+  uint8_t stat = 0;
+  for (int l = 0; l < N; ++l) stat |= p.lstat[(long)l * n + node];
+  double kx, ky;
+  node_k(p, p.off + node, kx, ky);
+  const cd z{0.0, 0.0};
+  // outputs default to "invalid"
+  if (!base) p.valid[gnode] = 0;
+  for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * nT + gnode] = 0;
+  if (stat & (ST_EIGEN | ST_SORT)) {
+    p.status[gnode] = stat;
+    return;
+  }
+  // forward pass: matching, interfaces, SLeft prefix scan
+  Mode4 prev;
+  load_modes(p, 0, node, prev);
+  S4 S0 = s4_diag(expi(prev.qf[0], p.layers[0].d), expi(prev.qf[1], p.layers[0].d), expi(-prev.qb[0], p.layers[0].d),
+                  expi(-prev.qb[1], p.layers[0].d));
+  S4 SLsrc = s4_identity();
+  if ((p.needL >> 0) & 1u) st_s4(p.sleft, 0, n, node, s4_identity());
+  bool seeds_ok = true;
+  cd sif[2][3], sib[2][3];
+  if (src == 1 && !base) {
+    seeds_ok = source_projection(kx, ky, p.omega, p.layers[0], prev, sif, sib);
+  }
+  for (int oi = 0; oi < p.nobs; ++oi)
+    if (p.obs[oi] == 1 && !base) write_basis(p, oi, gnode, p.nout, p.layers[0], prev, kx, ky);
+  if (src == 1 && !base) write_seeds(p, gnode, p.nout, prev, sif, sib);
+  for (int j = 2; j <= N; ++j) {
+    Mode4 cur;
+    load_modes(p, j - 1, node, cur);
+    {
+      cd wf[4][2], wb[4][2];
+      for (int i = 0; i < 4; ++i)
+        for (int m = 0; m < 2; ++m) { wf[i][m] = prev.vf[i][m]; wb[i][m] = prev.vb[i][m]; }
+      match_dir(wf, cur.vf, cur.qf);
+      match_dir(wb, cur.vb, cur.qb);
+    }
+    store_modes(p, j - 1, node, cur);
+    S4 Si;
+    if (!interface_matrix(prev, cur, Si)) stat |= ST_SINGULAR;
+    st_s4(p.sint, j - 2, n, node, Si);
+    S4 SL = redheffer(S0, Si);
+    if ((p.needL >> (j - 1)) & 1u) st_s4(p.sleft, j - 1, n, node, SL);
+    if (j == src) SLsrc = SL;
+    const double d = p.layers[j - 1].d;
+    cd pf0 = expi(cur.qf[0], d), pf1 = expi(cur.qf[1], d), pb0 = expi(-cur.qb[0], d), pb1 = expi(-cur.qb[1], d);
+    // Redheffer(SL, diag(pf0, pf1, pb0, pb1))
+    S0.b11 = dl(pf0, pf1, SL.b11);
+    S0.b12 = dl(pf0, pf1, dr(SL.b12, pb0, pb1));
+    S0.b21 = SL.b21;
+    S0.b22 = dr(SL.b22, pb0, pb1);
+    if (!base) {
+      if (j == src) {
+        seeds_ok = source_projection(kx, ky, p.omega, p.layers[j - 1], cur, sif, sib);
+        write_seeds(p, gnode, p.nout, cur, sif, sib);
+      }
+      for (int oi = 0; oi < p.nobs; ++oi)
+        if (p.obs[oi] == j) write_basis(p, oi, gnode, p.nout, p.layers[j - 1], cur, kx, ky);
+    }
+    prev = cur;
+  }
+  if (stat & ST_SINGULAR) {
+    p.status[gnode] = stat;
+    return;
+  }
+  // backward pass: SRight suffix scan down to the source layer
+  S4 SR = s4_identity();
+  if (N >= 1 && ((p.needR >> (N - 1)) & 1u)) st_s4(p.sright, N - 1, n, node, SR);
+  for (int k = N - 1; k >= src; --k) {
+    // Q of layer k (1-based) from the matched records
+    const double2* rec = p.modes + (long)(k - 1) * 20 * n;
+    cd qf0 = ld(rec, 16, n, node), qf1 = ld(rec, 17, n, node), qb0 = ld(rec, 18, n, node), qb1 = ld(rec, 19, n, node);
+    const double d = p.layers[k - 1].d;
+    S4 Si = ld_s4(p.sint, k - 1, n, node);
+    S4 eff = redheffer_diag_left(expi(qf0, d), expi(qf1, d), expi(-qb0, d), expi(-qb1, d), Si);
+    SR = redheffer(eff, SR);
+    if ((p.needR >> (k - 1)) & 1u) st_s4(p.sright, k - 1, n, node, SR);
+  }
+  // cavity at the source layer (_R_cavity, _cavity_resummation)
+  const double2* srec = p.modes + (long)(src - 1) * 20 * n;
+  cd Qf0 = ld(srec, 16, n, node), Qf1 = ld(srec, 17, n, node), Qb0 = ld(srec, 18, n, node), Qb1 = ld(srec, 19, n, node);
+  const double ds = p.layers[src - 1].d;
+  M2 RL = SLsrc.b12;
+  M2 RR = M2{z, z, z, z};
+  S4 RRr = s4_identity();
+  M24 Fp, Fm;
+  const M2 I2 = M2{cd{1, 0}, z, z, cd{1, 0}}, Z2 = M2{z, z, z, z};
+  if (src < N) {
+    // SΦ = diag(e^{iQf(-d)}, e^{iQb d}) ⋆ SRight[src]
+    RRr = redheffer_diag_left(expi(Qf0, -ds), expi(Qf1, -ds), expi(Qb0, ds), expi(Qb1, ds), SR);
+    RR = RRr.b21;
+    cd PF0 = expi(Qf0, ds), PF1 = expi(Qf1, ds), PB0 = expi(Qb0, -ds), PB1 = expi(Qb1, -ds);
+    M2 Mx = mul(dr(dl(PF0, PF1, RL), PB0, PB1), RR);
+    M2 D = imin(Mx);
+    // RHS = S₊ + ΦF (RL S₋) = [I, ΦF RL]
+    Fp.L = solve(D, I2);
+    Fp.R = solve(D, dl(PF0, PF1, RL));
+    // F⁻ = S₋ + ΦB (RR F⁺)
+    Fm.L = dl(PB0, PB1, mul(RR, Fp.L));
+    Fm.R = add(I2, dl(PB0, PB1, mul(RR, Fp.R)));
+  } else {
+    Fp = M24{Z2, Z2};
+    Fm = M24{Z2, I2};
+  }
+  // T^o per observation layer
+  bool any_tbad = false;
+  for (int oi = 0; oi < p.nobs; ++oi) {
+    const int o = p.obs[oi];
+    M24 Ef, Eb;
+    if (o == src) {
+      Ef = mul24(RL, Fm);
+      Eb = mul24(RR, Fp);
+    } else if (o > src) {
+      M24 cp = mul24(RRr.b11, Fp);
+      if (o == N) {
+        Ef = flush24(cp);
+        Eb = M24{Z2, Z2};
+      } else {
+        S4 SRo = ld_s4(p.sright, o - 1, n, node);
+        M24 bp = cond2x2_eq(SRo.b11) > 1e8 ? M24{Z2, Z2} : M24{solve(SRo.b11, cp.L), solve(SRo.b11, cp.R)};
+        Ef = flush24(bp);
+        M24 Ebn;
+        if (o + 1 == N) {
+          Ebn = M24{Z2, Z2};
+        } else {
+          S4 SRn = ld_s4(p.sright, o, n, node);
+          M24 bn = cond2x2_eq(SRn.b11) > 1e8 ? M24{Z2, Z2} : M24{solve(SRn.b11, cp.L), solve(SRn.b11, cp.R)};
+          Ebn = flush24(mul24(SRn.b21, bn));
+        }
+        const double2* orec = p.modes + (long)(o - 1) * 20 * n;
+        const double dO = p.layers[o - 1].d;
+        cd f0 = expi(ld(orec, 16, n, node), dO), f1 = expi(ld(orec, 17, n, node), dO);
+        S4 Si = ld_s4(p.sint, o - 1, n, node);
+        Eb = flush24(add24(mul24(Si.b21, dl24(f0, f1, Ef)), mul24(Si.b22, Ebn)));
+      }
+    } else {  // o < src
+      M2 S22 = SLsrc.b22;
+      M24 am = mul24(S22, Fm);
+      auto bminus = [&](int k) -> M24 {  // b₋ of walk-left layer k (2 ≤ k ≤ src-1)
+        S4 SLk = ld_s4(p.sleft, k - 1, n, node);
+        return cond2x2_eq(SLk.b22) > 1e8 ? M24{Z2, Z2} : M24{solve(SLk.b22, am.L), solve(SLk.b22, am.R)};
+      };
+      if (o == 1) {
+        Ef = M24{Z2, Z2};
+      } else {
+        S4 SLo = ld_s4(p.sleft, o - 1, n, node);
+        M24 bm = cond2x2_eq(SLo.b22) > 1e8 ? M24{Z2, Z2} : M24{solve(SLo.b22, am.L), solve(SLo.b22, am.R)};
+        Ef = flush24(mul24(SLo.b12, bm));
+      }
+      M24 Ebn = (o == src - 1) ? Fm : flush24(bminus(o + 1));
+      const double2* orec = p.modes + (long)(o - 1) * 20 * n;
+      const double dO = p.layers[o - 1].d;
+      cd f0 = expi(ld(orec, 16, n, node), dO), f1 = expi(ld(orec, 17, n, node), dO);
+      S4 Si = ld_s4(p.sint, o - 1, n, node);
+      Eb = flush24(add24(mul24(Si.b21, dl24(f0, f1, Ef)), mul24(Si.b22, Ebn)));
+    }
+    bool fin = fin2(Ef.L) && fin2(Ef.R) && fin2(Eb.L) && fin2(Eb.R);
+    if (!fin) any_tbad = true;
+    if (fin) write_T(p, oi, gnode, nT, Ef, Eb);
+    else write_T(p, oi, gnode, nT, M24{Z2, Z2}, M24{Z2, Z2});
+    p.tvalid[(long)oi * nT + gnode] = fin ? 1 : 0;
+  }
+  if (any_tbad) stat |= ST_TNONFINITE;
+  if (!base) {
+    bool sfin = seeds_ok;
+    for (int m = 0; m < 2 && sfin; ++m)
+      for (int q = 0; q < 3; ++q) sfin = sfin && isfin(sif[m][q]) && isfin(sib[m][q]);
+    if (!seeds_ok) stat |= ST_SINGULAR;
+    if (!sfin) {
+      stat |= ST_SEEDS;
+      for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * p.nout + gnode] = 0;
+      p.valid[gnode] = 0;
+    } else {
+      p.valid[gnode] = 1;
+      stat |= ST_VALID;
+    }
+  } else {
+    stat |= ST_VALID;  // the base solve succeeded; seeds are checked per φ
+  }
+  p.status[gnode] = stat;
+}
+
+// ------------------------------------------------------------------------------------
+// K3: rotation fill of an azimuthally symmetric 2D grid (mod_CavityTransfer.jl:361-378)
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_rotate_fill(TransferParams p, const uint8_t* base_status, const uint8_t* base_tvalid,
+                                                     const double2* Tbase) {
+  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long nout = p.nout, nb = p.n;  // p.n = Nk (base nodes)
+  if (idx >= nout) return;
+  long k = idx % p.Nk, q = idx / p.Nk;
+  double s, c;
+  sincos(p.phi[q], &s, &c);
+  double kx = p.kr[k] * c, ky = p.kr[k] * s;
+  p.valid[idx] = 0;
+  for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * nout + idx] = 0;
+  uint8_t bst = base_status[k];
+  if (!(bst & ST_VALID)) { p.status[idx] = bst; return; }
+  auto rot = [&](Mode4& M) {
+    for (int m = 0; m < 2; ++m) {
+      cd a0 = M.vf[0][m], a1 = M.vf[1][m], a2 = M.vf[2][m], a3 = M.vf[3][m];
+      M.vf[0][m] = c * a0 - s * a1; M.vf[1][m] = s * a0 + c * a1;
+      M.vf[2][m] = c * a2 - s * a3; M.vf[3][m] = s * a2 + c * a3;
+      cd b0 = M.vb[0][m], b1 = M.vb[1][m], b2 = M.vb[2][m], b3 = M.vb[3][m];
+      M.vb[0][m] = c * b0 - s * b1; M.vb[1][m] = s * b0 + c * b1;
+      M.vb[2][m] = c * b2 - s * b3; M.vb[3][m] = s * b2 + c * b3;
+    }
+  };
+  TransferParams pb = p;
+  pb.n = nb;
+  Mode4 Ms;
+  load_modes(pb, p.src - 1, k, Ms);
+  rot(Ms);
+  cd sif[2][3], sib[2][3];
+  bool ok = source_projection(kx, ky, p.omega, p.layers[p.src - 1], Ms, sif, sib);
+  for (int m = 0; m < 2 && ok; ++m)
+    for (int qq = 0; qq < 3; ++qq) ok = ok && isfin(sif[m][qq]) && isfin(sib[m][qq]);
+  uint8_t stat = bst & ~ST_VALID;
+  if (!ok) { p.status[idx] = stat | ST_SEEDS; return; }
+  for (int oi = 0; oi < p.nobs; ++oi) {
+    uint8_t tv = base_tvalid[(long)oi * nb + k];
+    const double2* tb = Tbase + (long)oi * 16 * nb;
+    double2* to = p.Tout + (long)oi * 16 * nout;
+    for (int e = 0; e < 16; ++e) to[e * nout + idx] = tv ? tb[e * nb + k] : make_double2(0.0, 0.0);
+    p.tvalid[(long)oi * nout + idx] = tv;
+    Mode4 Mo;
+    load_modes(pb, p.obs[oi] - 1, k, Mo);
+    rot(Mo);
+    write_basis(p, oi, idx, nout, p.layers[p.obs[oi] - 1], Mo, kx, ky);
+  }
+  write_seeds(p, idx, nout, Ms, sif, sib);
+  p.valid[idx] = 1;
+  p.status[idx] = stat | ST_VALID;
+}
+
+// ------------------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------------------
+cudaError_t launch_layer_modes(const TransferParams& p, cudaStream_t stream) {
+  long tot = (long)p.n * p.nL;
+  if (tot <= 0) return cudaSuccess;
+  k_layer_modes<<<(unsigned)((tot + 127) / 128), 128, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream) {
+  if (p.n <= 0) return cudaSuccess;
+  k_chain<<<(unsigned)((p.n + 127) / 128), 128, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rotate_fill(const TransferParams& p, const uint8_t* base_status, const uint8_t* base_tvalid,
+                               const double2* Tbase, cudaStream_t stream) {
+  if (p.nout <= 0) return cudaSuccess;
+  k_rotate_fill<<<(unsigned)((p.nout + 127) / 128), 128, 0, stream>>>(p, base_status, base_tvalid, Tbase);
+  return cudaGetLastError();
+}
+
+}  // namespace ytf
