@@ -120,6 +120,21 @@ int ytf_gauss_legendre(int n, double* x, double* w);
 int ytf_gl_rule(ytf_ctx* ctx, int npanels, const double* pa, const double* pb, int order, int nsing,
                 const double* singular, double* nodes, double* weights);
 
+/* Allocation-free variant of ytf_green for 2D caches (no counterpart in the reference).
+ * For callers that must not have the library allocate device memory: a host that owns all
+ * device memory through its own pool (e.g. a Julia CUDA.jl session or a caching
+ * allocator), or code that cannot afford cudaMalloc's device-wide synchronisation. The
+ * strengths and the split-k partial sums use a fixed 64 MiB array inside the library
+ * (held on every GPU that loads it until exit) instead of cudaMalloc'd workspace. Limit:
+ * 9*nz*(n_nodes + nx*ny) <= 4,194,304 complex values; larger requests return YTF_ERR_ARG.
+ * z_obs_dev, xs_dev, ys_dev and out_dev are DEVICE pointers (out: nx*ny*nz*9 complex,
+ * Julia layout). The first call on a device looks up the array's device address; make it
+ * before any stream capture. All calls share the array: calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialised by the caller. */
+int ytf_green_noalloc(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, double zsrc_local, int nz,
+                      const double* z_obs_dev, int nx, const double* xs_dev, int ny, const double* ys_dev, int terms,
+                      double* out_dev);
+
 #ifdef __cplusplus
 }
 #endif

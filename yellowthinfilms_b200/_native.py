@@ -38,6 +38,8 @@ SIGNATURES = {
     "ytf_cache_export": (ctypes.c_int, [_vp, _vp, _d, _d, _d, _d, _d, _d]),
     "ytf_green": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _d, ctypes.c_int, _d, ctypes.c_int,
                                  _d, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int]),
+    "ytf_green_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                         ctypes.c_int, _vp, ctypes.c_int, _vp]),
     "ytf_gauss_legendre": (ctypes.c_int, [ctypes.c_int, _d, _d]),
     "ytf_gl_rule": (ctypes.c_int, [_vp, ctypes.c_int, _d, _d, ctypes.c_int, ctypes.c_int, _d, _d, _d]),
 }

@@ -300,3 +300,26 @@ def halve_panels(panels):
 def build_kphi_grid(N_phi: int):
     """Uniform trapezoid in φ (mod_KxGrid.jl:390-394)."""
     return np.array([2 * np.pi * p / N_phi for p in range(N_phi)]), np.full(N_phi, 2 * np.pi / N_phi)
+
+
+def closed_form_G_noalloc(cache: CavityTransferCache2D, obs_layer: int, zsrc_local: float, z_obs, xs, ys, out,
+                          terms: str = "all"):
+    """closed_form_G for a 2D cache that allocates no device memory inside the library.
+
+    For hosts that keep all device memory in their own pool, or that must not trigger the
+    device-wide synchronisation of cudaMalloc: the library's scratch is a fixed 64 MiB
+    array (limit 9·nz·(n_nodes + Nx·Ny) ≤ 4,194,304 complex values). ``z_obs``, ``xs``,
+    ``ys`` (float64) and ``out`` (complex128, Nx·Ny·Nz·9, Julia order) are CUDA tensors
+    the caller allocated. Concurrent calls on the GPU share the scratch and must be
+    serialised by the caller; the first call on a device should precede any stream capture.
+    """
+    if terms not in TERMS:
+        raise YTFError(f"closed_form_G: terms must be :all, :direct, :scattered, :toeplitz or :hankel (got :{terms})")
+    nz, nx, ny = z_obs.numel(), xs.numel(), ys.numel()
+    if out.numel() != nx * ny * nz * 9:
+        raise YTFError("closed_form_G: out has the wrong size")
+    v = lambda t: ctypes.c_void_p(t.data_ptr())
+    rc = lib().ytf_green_noalloc(cache.ctx.h, cache.h, int(obs_layer), float(zsrc_local), nz, v(z_obs), nx, v(xs), ny, v(ys),
+                                 TERMS[terms], v(out))
+    cache.ctx.check(rc)
+    return out
