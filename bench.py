@@ -165,7 +165,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_lambda * N_LAMBDA * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
-            "config": CONFIG,
+            "config": dict(CONFIG, precision="fp64 (CPU oracle)"),
             "cpu_baseline": {"value": value, "unit": "entries/s", "cores": oracle.num_threads(), "kind": "port",
                              "sample": f"1 wavelength per step, {N_PHI // 4} of {N_PHI} φ nodes x 1024 kρ "
                                        f"(4096 of 65536 nodes), time scaled x16 (linear in nodes)"},
@@ -185,7 +185,22 @@ CONFIG = {"workload": "batched spectral solve + full 3x3 G: 8-layer biaxial/gyro
 # --------------------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------------------
-FLOPS_LATERAL_PER_CMAC = 8  # one complex multiply-add = 8 real flops
+# DRAM bytes (read + write) per launch from one ncu capture of the kernel on this workload
+# (profiles/k_lateral_fp64_bench_config2.md); None until captured
+TRAFFIC = {"k_lateral": 81.7e6}
+
+
+def measured_peaks():
+    """Denominators: MEASURED_PEAKS.json of this pool, else the stated fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        m = json.load(open(path))
+        return {"bf16_sustained": (float(m["bf16_tflops_sustained"]), "measured (MEASURED_PEAKS.json, sustained bf16)"),
+                "bf16_burst": (float(m["bf16_tflops"]), "measured (MEASURED_PEAKS.json, burst bf16)"),
+                "hbm": (float(m["hbm_gbs"]), "measured (MEASURED_PEAKS.json)")}
+    except (OSError, KeyError, ValueError):
+        return {"bf16_sustained": (1400.0, "fallback (sustained bf16 on this pool)"),
+                "bf16_burst": (1590.0, "fallback"), "hbm": (6650.0, "fallback")}
 
 
 def run_ours(args):
@@ -213,7 +228,8 @@ def run_ours(args):
     def step(host_out):
         for i, ((k0, kr, wr, phi, wphi), (zsrc, zo, xs, ys)) in enumerate(per):
             c = api.build_cavity_transfer_2d(stack, k0, SRC, kr, wr, phi, wphi, obs_layers=[SRC], rotation=False)
-            api.closed_form_G(c, SRC, zsrc, zo, xs, ys, out=(G_host[i] if host_out else G_dev[i]))
+            api.closed_form_G(c, SRC, zsrc, zo, xs, ys, precision=args.precision,
+                              out=(G_host[i] if host_out else G_dev[i]))
             del c
 
     def timed(host_out, profile):
@@ -257,7 +273,7 @@ def run_ours(args):
         k0, kr, wr, phi, wphi = grids(lams[0], phi_take=4)
         zsrc, zo, xs, ys = obs_set(stack.layers, lams[0])
         c = api.build_cavity_transfer_2d(stack, k0, SRC, kr, wr, phi, wphi, obs_layers=[SRC], rotation=False)
-        G = api.closed_form_G(c, SRC, zsrc, zo, xs, ys)
+        G = api.closed_form_G(c, SRC, zsrc, zo, xs, ys, precision=args.precision)
         oc = oracle.build_cavity_transfer_2d(stack.layers, k0, SRC, kr, wr, phi, wphi, obs_layers=[SRC], rotation=False)
         Go = oracle.closed_form_G(oc, SRC, zsrc, zo, xs, ys)
         err = float(np.linalg.norm(G - Go) / np.linalg.norm(Go))
@@ -270,22 +286,26 @@ def run_ours(args):
     top = max(prof.items(), key=lambda kv: kv[1][0]) if prof else (None, (0.0, 0))
     name, (tot_ms, nl) = top
     nodes = N_PANELS * ORDER * N_PHI
-    work = {
-        "k_lateral": ("fp64", 8.0 * NXY * NXY * nodes * NZ * 9, "TFLOP/s"),
-    }
-    roof = None
-    if name in work and nl:
-        bound, per_launch, unit = work[name]
-        achieved = per_launch / (tot_ms / nl * 1e-3) / 1e12
-        peak = 37.2
-        roof = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
-                "traffic": None, "peak_source": "nominal FP64 (148 SM x 64 FMA/clk x 1.965 GHz); no measured FP64 peak"}
-    elif name:
-        roof = {"kernel": name, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None}
+    cmacs = float(NXY * NXY * nodes * NZ * 9)  # complex multiply-adds of one lateral contraction
+    peaks = measured_peaks()
+    roof = {"kernel": name, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None}
+    if name == "k_lateral_tc" and nl:
+        achieved = 8.0 * cmacs / (tot_ms / nl * 1e-3) / 1e12
+        peak, src = peaks["bf16_sustained"]
+        roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": TRAFFIC.get(name), "peak_source": src,
+                "work": "8 flop per complex multiply-add x 1024 pixels x 65536 nodes x 72 columns per launch",
+                "split_multiplier": 6, "tensor_flops_executed_per_launch": 6 * 8.0 * cmacs}
+    elif name == "k_lateral" and nl:
+        achieved = 8.0 * cmacs / (tot_ms / nl * 1e-3) / 1e12
+        roof = {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": 37.2, "unit": "TFLOP/s",
+                "frac": achieved / 37.2, "traffic": TRAFFIC.get(name),
+                "peak_source": "nominal FP64 (148 SM x 64 FMA/clk x 1.965 GHz); no measured FP64 peak"}
     launches = int(sum(v[1] for v in prof.values()))
     line = {"metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded)", "config": CONFIG, "max_rel_err_vs_oracle": err,
+            "dtype": "f64" if args.precision == "fp64" else "f64 solve, split-bf16 x3 tensor-core synthesis (fp32 accum)",
+            "data": "synthetic (seeded)", "config": dict(CONFIG, precision=args.precision), "max_rel_err_vs_oracle": err,
             "e2e": {"value": e2e, "unit": "entries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": ms_e2e},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
@@ -305,6 +325,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--precision", default="split_bf16", choices=["split_bf16", "fp64"],
+                    help="synthesis contraction: tensor cores (split-BF16, FP32 accumulate) or FP64 CUDA cores")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -1823,6 +1823,50 @@ int ytfo_amplitude_at(void* h, int obs_layer, double zsrc, int seeds, double* Af
   } catch (std::exception& e) { g_err = e.what(); return 1; }
 }
 
+// Strengths of one z-row of a 2D cache (_strengths_row!, mod_ClosedFormField.jl:616-659):
+// S[n][c + 3q] complex, and the node wavevectors kx[n], ky[n].
+int ytfo_strengths_2d(void* h, int obs_layer, double zsrc, double z, int terms, double* S, double* kx, double* ky) {
+  try {
+    Cache* c = (Cache*)h;
+    if (!c->is2d) throw std::runtime_error("needs a 2D cache");
+    int oi = c->oidx(obs_layer);
+    if (oi < 0) throw std::runtime_error("obs layer not in cache");
+    int Nk = c->Nk, Np = c->Np, Nn = Nk * Np;
+    Amp R;
+    bool same = term_amplitudes(*c, obs_layer, zsrc, terms, R);
+    Amp D;
+    if (same) direct_amplitude(*c, zsrc, z, D);
+    double d = c->d_obs[oi];
+    for (int p = 0; p < Np; ++p)
+      for (int k = 0; k < Nk; ++k) {
+        int n = k + Nk * p;
+        cd w(c->kr[k] * c->wr[k] * c->wphi[p] / (4 * PI * PI), 0.0);
+        cd sacc[3][3];
+        for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) sacc[a][b] = 0.0;
+        const Basis& b = c->basis[oi][n];
+        for (int m = 0; m < 2; ++m) {
+          cd pf = phase(b.kzf[m], z), pb = phase(b.kzb[m], z - d);
+          for (int q = 0; q < 3; ++q) {
+            cd af_ = R.F(n, m, q) * pf, ab_ = R.B(n, m, q) * pb;
+            if (same) { af_ += D.F(n, m, q); ab_ += D.B(n, m, q); }
+            cd af = finite_or_zero(w * af_), ab = finite_or_zero(w * ab_);
+            sacc[0][q] += b.exf[m] * af + b.exb[m] * ab;
+            sacc[1][q] += b.eyf[m] * af + b.eyb[m] * ab;
+            sacc[2][q] += b.ezf[m] * af + b.ezb[m] * ab;
+          }
+        }
+        for (int q = 0; q < 3; ++q)
+          for (int cc = 0; cc < 3; ++cc) {
+            S[2 * (9 * (size_t)n + cc + 3 * q)] = sacc[cc][q].real();
+            S[2 * (9 * (size_t)n + cc + 3 * q) + 1] = sacc[cc][q].imag();
+          }
+        kx[n] = c->kxn[n];
+        ky[n] = c->kyn[n];
+      }
+    return 0;
+  } catch (std::exception& e) { g_err = e.what(); return 1; }
+}
+
 int ytfo_gauss_legendre(int n, double* x, double* w) {
   std::vector<double> xv, wv;
   gauss_legendre(n, xv, wv);

@@ -296,3 +296,14 @@ def own_reflectance(stack, k0, theta_deg, pol):
     a = _StackArrays(stack)
     return float(lib().ytfo_own_reflectance(*a.args(), ctypes.c_double(k0), ctypes.c_double(theta_deg),
                                             ctypes.c_int(1 if pol == "s" else 0)))
+
+
+def strengths_2d(cache, obs_layer, zsrc_local, z, terms="all"):
+    """Per-node strengths S[n, c + 3q] of one z-row and the node (kx, ky) of a 2D cache."""
+    n = cache.n
+    S = np.zeros(18 * n); kx = np.zeros(n); ky = np.zeros(n)
+    rc = lib().ytfo_strengths_2d(ctypes.c_void_p(cache.h), ctypes.c_int(obs_layer), ctypes.c_double(zsrc_local),
+                                 ctypes.c_double(z), ctypes.c_int(TERMS[terms]), _p(S), _p(kx), _p(ky))
+    if rc != 0:
+        raise RuntimeError(_err())
+    return S.view(np.complex128).reshape(n, 9), kx, ky

@@ -183,3 +183,39 @@ def test_empty_and_single_node_inputs(ytf, oracle):
     c = ytf.build_cavity_transfer_1d(st, W, 2, kx, wt)
     o = oracle.build_cavity_transfer_1d(st, W, 2, kx, wt)
     assert relerr(ytf.closed_form_G(c, 2, 0.3, [0.2, 0.5], xs, ys), oracle.closed_form_G(o, 2, 0.3, [0.2, 0.5], xs, ys)) < 1e-10
+
+
+@pytest.mark.parametrize("idx", [3, 4])
+def test_lateral_split_bf16_tensor_cores_match_fp64(ytf, oracle, idx):
+    """The tensor-core lateral synthesis (3-term BF16 split, FP32 accumulation in tensor
+    memory, FP64 sum of node slices) against the FP64 path and the oracle: ≤ 1e-6
+    relative (the metric's bound), on biaxial and gyrotropic stacks."""
+    _, st = FOUNDATION_STACKS[idx]
+    kr, wr = krho_grid(st, W, kmax=10.0, width=0.5)
+    ph, wp = uniform_phi(32)
+    gc = ytf.build_cavity_transfer_2d(st, W, 2, kr, wr, ph, wp, obs_layers=[1, 2, 3])
+    xs = np.linspace(-0.3, 0.3, 11)
+    ys = np.linspace(-0.25, 0.2, 9)
+    for obs, zo in ((2, [0.1, 0.35, 0.6]), (1, [0.4]), (3, [0.2, 0.3])):
+        G64 = ytf.closed_form_G(gc, obs, 0.3, zo, xs, ys)
+        Gtc = ytf.closed_form_G(gc, obs, 0.3, zo, xs, ys, precision="split_bf16")
+        assert relerr(Gtc, G64) < 1e-6, (obs, relerr(Gtc, G64))
+    oc = oracle.build_cavity_transfer_2d(st, W, 2, kr, wr, ph, wp, obs_layers=[2])
+    Go = oracle.closed_form_G(oc, 2, 0.3, [0.1, 0.6], xs, ys)
+    assert relerr(ytf.closed_form_G(gc, 2, 0.3, [0.1, 0.6], xs, ys, precision="split_bf16"), Go) < 1e-6
+
+
+def test_lateral_split_bf16_ragged_tiles(ytf):
+    """Pixel counts and column counts that do not fill a 128-pixel tile or a 16-wide MMA,
+    node counts that do not fill a 16-node stage, and more than 128 columns (two N-tiles)."""
+    _, st = FOUNDATION_STACKS[4]
+    kr, wr = krho_grid(st, W, kmax=6.0, width=0.7)
+    ph, wp = uniform_phi(6)
+    gc = ytf.build_cavity_transfer_2d(st, W, 2, kr[:-3], wr[:-3], ph, wp, obs_layers=[2])
+    for nx, ny, nz in ((1, 1, 1), (7, 3, 2), (13, 11, 16)):
+        xs = np.linspace(-0.2, 0.3, nx)
+        ys = np.linspace(-0.1, 0.15, ny)
+        zo = list(np.linspace(0.05, 0.85, nz))
+        G64 = ytf.closed_form_G(gc, 2, 0.3, zo, xs, ys)
+        Gtc = ytf.closed_form_G(gc, 2, 0.3, zo, xs, ys, precision="split_bf16")
+        assert relerr(Gtc, G64) < 1e-6, (nx, ny, nz, relerr(Gtc, G64))

@@ -300,6 +300,7 @@ int run_transfer(ytf_ctx* ctx, TransferParams p, long total) {
     p.off = off;
     p.n = std::min(chunk, total - off);
     CK(LAUNCH("k_layer_modes", launch_layer_modes(p, ctx->stream)));
+    CK(LAUNCH("k_layer_modes_qr", launch_layer_modes_qr(p, ctx->stream)));
     CK(LAUNCH("k_chain", launch_chain(p, ctx->stream)));
   }
   return YTF_OK;
@@ -545,6 +546,7 @@ int ytf_transfer_2d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_
       b.tvalid = btv;
       b.Tout = bT;
       CK(LAUNCH("k_layer_modes", launch_layer_modes(b, ctx->stream)));
+      CK(LAUNCH("k_layer_modes_qr", launch_layer_modes_qr(b, ctx->stream)));
       CK(LAUNCH("k_chain", launch_chain(b, ctx->stream)));
       TransferParams f = p;
       f.mode = 1;
@@ -748,6 +750,40 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
     int ncol = 9 * nz;
     WS(S, double2, "g_S", (size_t)ncol * c->n);
     CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream)));
+    if (precision == YTF_PREC_SPLIT_BF16) {
+      // tensor cores: FP32 phase tables, split-BF16 contraction, FP64 reduction of the slices
+      WS(Px, float2, "g_px", (size_t)c->n * nx);
+      WS(Py, float2, "g_py", (size_t)c->n * ny);
+      CK(LAUNCH("k_phase_tables", launch_phase_tables(v, nx, ny, dxs, dys, Px, Py, ctx->stream)));
+      LateralTC lp;
+      std::memset(&lp, 0, sizeof(lp));
+      lp.npix = npix; lp.n = c->n; lp.nx = nx; lp.ny = ny; lp.ncol = ncol;
+      lp.ctile = lateral_tc_ctile(ncol);
+      lp.Np = ((2 * lp.ctile + 15) / 16) * 16;
+      lp.Px = Px; lp.Py = Py; lp.S = S;
+      // one CTA per SM (tensor memory, registers): tiles x node slices fill one wave
+      long tiles = ((npix + 127) / 128) * ((ncol + lp.ctile - 1) / lp.ctile);
+      long want = std::max(1L, (long)nsm / tiles);
+      long kchunk = (c->n + want - 1) / want;
+      kchunk = std::max(16L, ((kchunk + 15) / 16) * 16);
+      int splits = (int)((c->n + kchunk - 1) / kchunk);
+      lp.kchunk = kchunk;
+      WS(Gp, double2, "g_partial2", (size_t)splits * npix * ncol);
+      WS(err, unsigned, "g_tc_err", 1);
+      lp.partial = Gp;
+      lp.err = err;
+      CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+      CK(LAUNCH("k_lateral_tc", launch_lateral_tc(lp, splits, ctx->stream)));
+      CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, splits, Gp, G, ctx->stream)));
+      unsigned herr = 0;
+      CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
+      if (!out_is_device) CK(cudaMemcpyAsync(out, G, sizeof(double2) * nout, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      prof_collect(ctx);
+      return YTF_OK;
+    }
     long tiles = ((npix + 63) / 64) * ((ncol + 31) / 32);
     long want = (4L * nsm + tiles - 1) / tiles;
     int splits = (int)std::max(1L, std::min(want, std::max(1L, c->n / 512)));

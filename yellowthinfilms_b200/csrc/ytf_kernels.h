@@ -58,6 +58,7 @@ struct TransferParams {
 };
 
 cudaError_t launch_layer_modes(const TransferParams& p, cudaStream_t stream);
+cudaError_t launch_layer_modes_qr(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_rotate_fill(const TransferParams& p, const uint8_t* base_status, const uint8_t* base_tvalid,
                                const double2* Tbase, cudaStream_t stream);
@@ -109,6 +110,25 @@ int lateral_splits(long n, int splits);  // effective split count of launch_late
 cudaError_t launch_lateral(const CacheView& c, int nx, int ny, const double* xs, const double* ys, int ncol, const double2* S,
                            double2* partial, int splits, cudaStream_t s);
 cudaError_t launch_reduce_splits2(long len, int splits, const double2* partial, double2* G, cudaStream_t s);
+
+// 2D lateral synthesis on the tensor cores (split-BF16, FP32 accumulation)
+struct LateralTC {
+  long npix, n;
+  int nx, ny, ncol;
+  int ctile;  // complex columns per CTA tile (≤ 128)
+  int Np;     // 2 * ctile rounded up to a multiple of 16 (MMA N)
+  const float2* Px;   // [n][nx]
+  const float2* Py;   // [n][ny]
+  const double2* S;   // [ncol][n]
+  double2* partial;   // [splits][npix * ncol]
+  long kchunk;        // nodes per split
+  unsigned* err;      // set to nonzero if a wait timed out
+};
+cudaError_t launch_phase_tables(const CacheView& c, int nx, int ny, const double* xs, const double* ys, float2* Px,
+                                float2* Py, cudaStream_t s);
+size_t lateral_tc_smem(int Np);
+int lateral_tc_ctile(int ncol);
+cudaError_t launch_lateral_tc(const LateralTC& p, int splits, cudaStream_t s);
 
 // Gauss-Legendre panels -> nodes/weights, bit-exact with the CPU restatement
 cudaError_t launch_gl_nodes(int npanels, const double* pa, const double* pb, const int* sing_side, const double* xi,

@@ -93,15 +93,90 @@ __device__ void berreman(const LayerDev& L, double w, double kx, double ky, cd B
 // Hessenberg form, single-shift complex QR with Wilkinson shifts and full Schur-vector
 // accumulation, eigenvectors of the triangular factor by back substitution.
 // Published algorithm (Golub & Van Loan, Matrix Computations, §7.4-7.6; the LAPACK
-// ZGEBAL/ZGEHRD/ZLAHQR/ZTREVC sequence). Returns false if QR does not converge.
+// ZGEBAL/ZGEHRD/ZLAHQR/ZTREVC sequence). Every array index is a compile-time constant
+// (the active QR window is a template parameter, the sweep start a predicate), so the
+// matrices stay in registers. Returns false if QR does not converge.
 // ------------------------------------------------------------------------------------
+__device__ __forceinline__ void givens(cd x, cd y, cd& c, cd& s) {
+  double ax = cabs(x), ay = cabs(y);
+  if (ay == 0.0) { c = cd{1.0, 0.0}; s = cd{0.0, 0.0}; return; }
+  if (ax == 0.0) { c = cd{0.0, 0.0}; s = conj(y) * (1.0 / ay); return; }
+  double nr = hypot(ax, ay);
+  c = cd{ax / nr, 0.0};
+  s = (x * (1.0 / ax)) * conj(y) * (1.0 / nr);
+}
+
+// QR iterations on the window [l, HI] until H[HI][HI-1] deflates
+template <int HI>
+__device__ __forceinline__ bool qr_window(cd H[4][4], cd Z[4][4]) {
+  const double eps = 2.220446049250313e-16;
+  for (int it = 0; it < 60; ++it) {
+    int l = 0;
+#pragma unroll
+    for (int m = HI; m >= 1; --m) {
+      if (l == 0) {
+        double sm = cabs1(H[m - 1][m - 1]) + cabs1(H[m][m]);
+        if (cabs1(H[m][m - 1]) <= eps * sm || cabs1(H[m][m - 1]) < 1e-300) {
+          H[m][m - 1] = cd{0.0, 0.0};
+          l = m;
+        }
+      }
+    }
+    if (l == HI) return true;
+    cd mu;
+    if (it == 10 || it == 20 || it == 40) {
+      mu = H[HI][HI] + cd{0.75 * fabs(H[HI][HI - 1].x), 0.0};  // exceptional shift
+    } else {
+      cd a = H[HI - 1][HI - 1], b = H[HI - 1][HI], c = H[HI][HI - 1], d = H[HI][HI];
+      cd hd = (a - d) * 0.5;
+      cd disc = csqrt(hd * hd + b * c);
+      cd m1 = iszero(hd + disc) ? d : d - (b * c) / (hd + disc);
+      cd m2 = iszero(hd - disc) ? d : d - (b * c) / (hd - disc);
+      mu = norm2(m1 - d) <= norm2(m2 - d) ? m1 : m2;
+      if (!isfin(mu)) mu = d;
+    }
+    cd x{0.0, 0.0}, y{0.0, 0.0};
+#pragma unroll
+    for (int m = 0; m < HI; ++m)
+      if (m == l) { x = H[m][m] - mu; y = H[m + 1][m]; }
+#pragma unroll
+    for (int k = 0; k < HI; ++k) {
+      if (k < l) continue;
+      if (k > l) { x = H[k][k - 1]; y = H[k + 1][k - 1]; }
+      cd c, s;
+      givens(x, y, c, s);
+      // rows k, k+1 of H; columns k, k+1 of H and Z (entries outside the Hessenberg band
+      // are exact zeros and stay zero)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        cd h1 = H[k][j], h2 = H[k + 1][j];
+        H[k][j] = c * h1 + s * h2;
+        H[k + 1][j] = c * h2 - conj(s) * h1;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        cd h1 = H[i][k], h2 = H[i][k + 1];
+        H[i][k] = c * h1 + conj(s) * h2;
+        H[i][k + 1] = c * h2 - s * h1;
+        cd z1 = Z[i][k], z2 = Z[i][k + 1];
+        Z[i][k] = c * z1 + conj(s) * z2;
+        Z[i][k + 1] = c * z2 - s * z1;
+      }
+      if (k > l) H[k + 1][k - 1] = cd{0.0, 0.0};
+    }
+  }
+  return false;
+}
+
 __device__ bool eig4(cd A[4][4], cd lam[4], cd V[4][4]) {
   // balancing by powers of 2 (scaling only, as ZGEBAL with job 'S')
   double D[4] = {1.0, 1.0, 1.0, 1.0};
   for (int sweep = 0; sweep < 8; ++sweep) {
     bool changed = false;
+#pragma unroll
     for (int i = 0; i < 4; ++i) {
       double c = 0.0, r = 0.0;
+#pragma unroll
       for (int j = 0; j < 4; ++j)
         if (j != i) { c += cabs1(A[j][i]); r += cabs1(A[i][j]); }
       if (c == 0.0 || r == 0.0) continue;
@@ -112,16 +187,22 @@ __device__ bool eig4(cd A[4][4], cd lam[4], cd V[4][4]) {
       if (c + r >= 0.95 * s) continue;
       changed = true;
       D[i] *= f;
-      for (int j = 0; j < 4; ++j) { A[i][j] = A[i][j] * (1.0 / f); A[j][i] = A[j][i] * f; }
+      const double fi = 1.0 / f;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) { A[i][j] = A[i][j] * fi; A[j][i] = A[j][i] * f; }
     }
     if (!changed) break;
   }
   cd Z[4][4];
+#pragma unroll
   for (int i = 0; i < 4; ++i)
+#pragma unroll
     for (int j = 0; j < 4; ++j) Z[i][j] = cd{i == j ? 1.0 : 0.0, 0.0};
   // Householder reduction to upper Hessenberg
+#pragma unroll
   for (int k = 0; k < 2; ++k) {
     double xn = 0.0;
+#pragma unroll
     for (int i = k + 1; i < 4; ++i) xn += norm2(A[i][k]);
     if (xn == 0.0) continue;
     xn = sqrt(xn);
@@ -130,125 +211,93 @@ __device__ bool eig4(cd A[4][4], cd lam[4], cd V[4][4]) {
     cd ph = aa > 0.0 ? a * (1.0 / aa) : cd{1.0, 0.0};
     cd v[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
     v[k + 1] = a + ph * xn;
+#pragma unroll
     for (int i = k + 2; i < 4; ++i) v[i] = A[i][k];
     double vn = 0.0;
+#pragma unroll
     for (int i = k + 1; i < 4; ++i) vn += norm2(v[i]);
     if (vn == 0.0) continue;
-    double tau = 2.0 / vn;
-    // A <- (I - tau v v^H) A
+    const double tau = 2.0 / vn;
+#pragma unroll
     for (int j = 0; j < 4; ++j) {
       cd s{0, 0};
+#pragma unroll
       for (int i = k + 1; i < 4; ++i) s += conj(v[i]) * A[i][j];
       s = s * tau;
+#pragma unroll
       for (int i = k + 1; i < 4; ++i) A[i][j] -= v[i] * s;
     }
-    // A <- A (I - tau v v^H), Z <- Z (I - tau v v^H)
+#pragma unroll
     for (int i = 0; i < 4; ++i) {
       cd s{0, 0}, t{0, 0};
+#pragma unroll
       for (int j = k + 1; j < 4; ++j) { s += A[i][j] * v[j]; t += Z[i][j] * v[j]; }
-      s = s * tau; t = t * tau;
+      s = s * tau;
+      t = t * tau;
+#pragma unroll
       for (int j = k + 1; j < 4; ++j) { A[i][j] -= s * conj(v[j]); Z[i][j] -= t * conj(v[j]); }
     }
+#pragma unroll
     for (int i = k + 2; i < 4; ++i) A[i][k] = cd{0, 0};
   }
-  // shifted QR on the Hessenberg matrix
-  const double eps = 2.220446049250313e-16;
-  int hi = 3, its = 0, total = 0;
-  while (hi > 0) {
-    int l = hi;
-    while (l > 0) {
-      double s = cabs1(A[l - 1][l - 1]) + cabs1(A[l][l]);
-      if (cabs1(A[l][l - 1]) <= eps * s || cabs1(A[l][l - 1]) < 1e-300) { A[l][l - 1] = cd{0, 0}; break; }
-      --l;
-    }
-    if (l == hi) { --hi; its = 0; continue; }
-    if (++total > 120) return false;
-    ++its;
-    cd mu;
-    if (its == 10 || its == 20) {
-      mu = A[hi][hi] + cd{0.75 * fabs(A[hi][hi - 1].x), 0.0};  // exceptional shift
-    } else {
-      cd a = A[hi - 1][hi - 1], b = A[hi - 1][hi], c = A[hi][hi - 1], d = A[hi][hi];
-      cd hd = (a - d) * 0.5;
-      cd disc = csqrt(hd * hd + b * c);
-      cd m1 = d - (b * c) / (hd + disc), m2 = d - (b * c) / (hd - disc);
-      if (iszero(hd + disc)) m1 = d;
-      if (iszero(hd - disc)) m2 = d;
-      mu = norm2(m1 - d) <= norm2(m2 - d) ? m1 : m2;
-      if (!isfin(mu)) mu = d;
-    }
-    cd x = A[l][l] - mu, y = A[l + 1][l];
-    for (int k = l; k < hi; ++k) {
-      if (k > l) { x = A[k][k - 1]; y = A[k + 1][k - 1]; }
-      double ax = cabs(x), ay = cabs(y);
-      double nr = hypot(ax, ay);
-      cd c, s;
-      if (ay == 0.0) { c = cd{1.0, 0.0}; s = cd{0.0, 0.0}; }
-      else if (ax == 0.0) { c = cd{0.0, 0.0}; s = conj(y) * (1.0 / ay); }
-      else { c = cd{ax / nr, 0.0}; s = (x * (1.0 / ax)) * conj(y) * (1.0 / nr); }
-      // rows k, k+1 (all columns from k-1 for the full Schur form)
-      for (int j = (k > 0 ? k - 1 : 0); j < 4; ++j) {
-        cd h1 = A[k][j], h2 = A[k + 1][j];
-        A[k][j] = c * h1 + s * h2;
-        A[k + 1][j] = c * h2 - conj(s) * h1;
-      }
-      int rmax = k + 2 < hi ? k + 2 : hi;
-      for (int i = 0; i <= rmax; ++i) {
-        cd h1 = A[i][k], h2 = A[i][k + 1];
-        A[i][k] = c * h1 + conj(s) * h2;
-        A[i][k + 1] = c * h2 - s * h1;
-      }
-      for (int i = 0; i < 4; ++i) {
-        cd z1 = Z[i][k], z2 = Z[i][k + 1];
-        Z[i][k] = c * z1 + conj(s) * z2;
-        Z[i][k + 1] = c * z2 - s * z1;
-      }
-      if (k > l) A[k + 1][k - 1] = cd{0, 0};
-    }
-  }
+  if (!qr_window<3>(A, Z)) return false;
+  if (!qr_window<2>(A, Z)) return false;
+  if (!qr_window<1>(A, Z)) return false;
+#pragma unroll
   for (int i = 0; i < 4; ++i) lam[i] = A[i][i];
   // eigenvectors of the upper-triangular Schur factor
+  const double eps = 2.220446049250313e-16;
   double anorm = 0.0;
+#pragma unroll
   for (int i = 0; i < 4; ++i)
+#pragma unroll
     for (int j = i; j < 4; ++j) anorm = fmax(anorm, cabs1(A[i][j]));
-  double smin = fmax(eps * anorm, 1e-290);
+  const double smin = fmax(eps * anorm, 1e-290);
+#pragma unroll
   for (int k = 0; k < 4; ++k) {
     cd xv[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
     xv[k] = cd{1.0, 0.0};
+#pragma unroll
     for (int i = k - 1; i >= 0; --i) {
       cd s{0, 0};
+#pragma unroll
       for (int j = i + 1; j <= k; ++j) s += A[i][j] * xv[j];
       cd den = A[i][i] - A[k][k];
       if (cabs1(den) < smin) den = cd{smin, 0.0};
       xv[i] = -(s / den);
     }
     cd v[4];
+#pragma unroll
     for (int i = 0; i < 4; ++i) {
       cd s{0, 0};
+#pragma unroll
       for (int j = 0; j <= k; ++j) s += Z[i][j] * xv[j];
       v[i] = s * D[i];
     }
     // LAPACK normalisation: unit 2-norm, largest component real
     double nn = 0.0, best = -1.0;
-    int ib = 0;
+    cd vb{1.0, 0.0};
+#pragma unroll
     for (int i = 0; i < 4; ++i) {
       double a2 = norm2(v[i]);
       nn += a2;
-      if (a2 > best) { best = a2; ib = i; }
+      if (a2 > best) { best = a2; vb = v[i]; }
     }
-    double inv = 1.0 / sqrt(nn);
-    cd ph = conj(v[ib]) * (1.0 / sqrt(best));
+    const double inv = 1.0 / sqrt(nn);
+    const cd ph = conj(vb) * (1.0 / sqrt(best));
+#pragma unroll
     for (int i = 0; i < 4; ++i) V[i][k] = (v[i] * ph) * inv;
   }
-  // sort eigenpairs by (real, imag) (Julia's eigsortby), stable insertion sort
-  for (int i = 1; i < 4; ++i) {
-    for (int j = i; j > 0; --j) {
-      bool sw = lam[j].x < lam[j - 1].x || (lam[j].x == lam[j - 1].x && lam[j].y < lam[j - 1].y);
-      if (!sw) break;
-      cd t = lam[j]; lam[j] = lam[j - 1]; lam[j - 1] = t;
-      for (int r = 0; r < 4; ++r) { cd u = V[r][j]; V[r][j] = V[r][j - 1]; V[r][j - 1] = u; }
+  // sort eigenpairs by (real, imag) (Julia's eigsortby): a 4-input sorting network
+  auto cswap = [&](int a, int b) {
+    bool sw = lam[b].x < lam[a].x || (lam[b].x == lam[a].x && lam[b].y < lam[a].y);
+    if (sw) {
+      cd t = lam[a]; lam[a] = lam[b]; lam[b] = t;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) { cd u = V[r][a]; V[r][a] = V[r][b]; V[r][b] = u; }
     }
-  }
+  };
+  cswap(0, 1); cswap(2, 3); cswap(0, 2); cswap(1, 3); cswap(1, 2);
   return true;
 }
 
@@ -272,9 +321,132 @@ __device__ void closed_modes(const LayerDev& L, double w, double kx, double ky, 
 }
 
 // ------------------------------------------------------------------------------------
-// K1: modes of one (node, layer), sorted forward/backward (mod_ModeSolver.jl:274-326).
-// Scratch record per (layer, node): Vf[4x2] (8), Vb[4x2] (8), Qf (2), Qb (2); column-major.
+// Layers without xz/yz coupling (ε13 = ε23 = ε31 = ε32 = 0 and the same for μ: every
+// biaxial and every ε_xy-gyrotropic layer) have ρ = σ = 0 in the Berreman construction, so
+// B = [[0, B12], [B21, 0]] and B² = diag(B12 B21, B21 B12). The eigenvalues are
+// q = ±√μ_i with μ_i the eigenvalues of the 2x2 matrix M = B12 B21, and the eigenvectors
+// (a; ±B21 a / q) with M a = μ_i a. Returns false (general QR path) when the two μ_i are
+// within 1e-6 of each other or q ≈ 0, where this construction loses accuracy.
 // ------------------------------------------------------------------------------------
+__device__ __forceinline__ bool no_z_coupling(const LayerDev& L) {
+  return iszero(E(L, 1, 3)) && iszero(E(L, 2, 3)) && iszero(E(L, 3, 1)) && iszero(E(L, 3, 2)) && iszero(U(L, 1, 3)) &&
+         iszero(U(L, 2, 3)) && iszero(U(L, 3, 1)) && iszero(U(L, 3, 2));
+}
+
+__device__ bool block_modes(const LayerDev& L, double w, double kx, double ky, cd Q[4], cd V[4][4]) {
+  cd B[4][4];
+  berreman(L, w, kx, ky, B);
+  // M = B12 B21 (B12 = rows 0-1, cols 2-3; B21 = rows 2-3, cols 0-1)
+  cd m11 = B[0][2] * B[2][0] + B[0][3] * B[3][0], m12 = B[0][2] * B[2][1] + B[0][3] * B[3][1];
+  cd m21 = B[1][2] * B[2][0] + B[1][3] * B[3][0], m22 = B[1][2] * B[2][1] + B[1][3] * B[3][1];
+  cd hd = (m11 - m22) * 0.5;
+  cd disc = csqrt(hd * hd + m12 * m21);
+  cd mid = (m11 + m22) * 0.5;
+  cd mu[2] = {mid + disc, mid - disc};
+  double scale = fmax(fmax(cabs(m11), cabs(m22)), fmax(cabs(m12), cabs(m21)));
+  if (!(scale > 0) || !isfinite(scale)) return false;
+  if (cabs(mu[0] - mu[1]) <= 1e-6 * fmax(cabs(mu[0]), cabs(mu[1]))) return false;
+  int col = 0;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    // eigenvector of M for mu_i: (m12, mu_i - m11) or (mu_i - m22, m21), the larger one;
+    // mu_i - m11 = -hd ± disc and mu_i - m22 = hd ± disc, formed without cancellation
+    const cd sg = i == 0 ? disc : -disc;
+    cd a1x = m12, a1y = sg - hd;
+    cd a2x = hd + sg, a2y = m21;
+    double n1 = norm2(a1x) + norm2(a1y), n2 = norm2(a2x) + norm2(a2y);
+    cd ax = n1 >= n2 ? a1x : a2x, ay = n1 >= n2 ? a1y : a2y;
+    if (!(fmax(n1, n2) > 0)) return false;
+    cd q = csqrt(mu[i]);
+    if (!(cabs(q) > 1e-12 * sqrt(scale))) return false;
+    // b = B21 a / q
+    cd bx = (B[2][0] * ax + B[2][1] * ay) / q, by = (B[3][0] * ax + B[3][1] * ay) / q;
+#pragma unroll
+    for (int sgn = 0; sgn < 2; ++sgn) {
+      cd v[4] = {ax, ay, sgn ? -bx : bx, sgn ? -by : by};
+      double nn = 0.0, best = -1.0;
+      cd vb{1.0, 0.0};
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        double a2 = norm2(v[r]);
+        nn += a2;
+        if (a2 > best) { best = a2; vb = v[r]; }
+      }
+      const double inv = 1.0 / sqrt(nn);
+      const cd ph = conj(vb) * (1.0 / sqrt(best));
+#pragma unroll
+      for (int r = 0; r < 4; ++r) V[r][col] = (v[r] * ph) * inv;
+      Q[col] = sgn ? -q : q;
+      ++col;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    if (!isfin(Q[c]) || !isfin(V[0][c]) || !isfin(V[1][c]) || !isfin(V[2][c]) || !isfin(V[3][c])) return false;
+  // sort eigenpairs by (real, imag) (Julia's eigsortby): a 4-input sorting network
+  auto cswap = [&](int x, int y) {
+    bool sw = Q[y].x < Q[x].x || (Q[y].x == Q[x].x && Q[y].y < Q[x].y);
+    if (sw) {
+      cd t = Q[x]; Q[x] = Q[y]; Q[y] = t;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) { cd u = V[r][x]; V[r][x] = V[r][y]; V[r][y] = u; }
+    }
+  };
+  cswap(0, 1); cswap(2, 3); cswap(0, 2); cswap(1, 3); cswap(1, 2);
+  return true;
+}
+
+// Forward/backward split of one layer's four eigenpairs (mod_ModeSolver.jl:274-326) and
+// the scratch record: Vf[4x2] (8), Vb[4x2] (8), Qf (2), Qb (2); column-major. Each
+// eigenpair is written straight to its slot, so no register array is indexed at run time.
+__device__ __forceinline__ uint8_t classify_store(const TransferParams& p, int layer, long node, const cd Q[4],
+                                                  const cd V[4][4]) {
+  const long n = p.n;
+  const double tol = 1.4901161193847656e-08;
+  int cls[4];  // 0 forward, 1 backward, 2 degenerate
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    // Poynting flux Pz = ¼ Re(V_j · W_j), W = R4s V = (V3, -V2, -V1, V0)
+    cd s = conj(V[0][j]) * V[3][j];
+    s += conj(V[1][j]) * (-V[2][j]);
+    s += conj(V[2][j]) * (-V[1][j]);
+    s += conj(V[3][j]) * V[0][j];
+    double Pz = 0.25 * s.x;
+    if (fabs(Pz) > tol) cls[j] = Pz > 0 ? 0 : 1;
+    else if (fabs(Q[j].y) > tol) cls[j] = Q[j].y > tol ? 0 : 1;
+    else cls[j] = 2;
+  }
+  // slots in eigen order; the degenerate ones then fill forward first (the reference's order)
+  int nf = 0, nb = 0, slot[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (cls[j] == 0) slot[j] = nf++;
+    else if (cls[j] == 1) slot[j] = 2 + nb++;
+  }
+  if (nf > 2 || nb > 2) return ST_SORT;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (cls[j] == 2) {
+      if (nf < 2) slot[j] = nf++;
+      else slot[j] = 2 + nb++;
+    }
+  }
+  double2* rec = p.modes + (long)layer * 20 * n;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int sl = slot[j];
+    const int dirb = sl >> 1, m = sl & 1;  // dirb 0: forward, 1: backward
+#pragma unroll
+    for (int i = 0; i < 4; ++i) st(rec, 8 * dirb + i + 4 * m, n, node, V[i][j]);
+    st(rec, 16 + 2 * dirb + m, n, node, Q[j]);
+  }
+  return 0;
+}
+
+constexpr uint8_t ST_NEED_QR = 128;  // internal: this (node, layer) awaits the general QR pass
+
+// K1: closed-form TE/TM modes (isotropic/uniaxial) and the block path; everything else is
+// flagged for k_layer_modes_qr. Layer-major indexing: one layer, one material kind per warp.
 __global__ void __launch_bounds__(128) k_layer_modes(TransferParams p) {
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long n = p.n;
@@ -285,52 +457,32 @@ __global__ void __launch_bounds__(128) k_layer_modes(TransferParams p) {
   node_k(p, p.off + node, kx, ky);
   const LayerDev& L = p.layers[layer];
   cd Q[4], V[4][4];
-  uint8_t stat = 0;
+  bool done;
   if ((L.ekind == 0 || L.ekind == 1) && L.mkind == 0) {
     closed_modes(L, p.omega, kx, ky, Q, V);
+    done = true;
   } else {
-    cd B[4][4];
-    berreman(L, p.omega, kx, ky, B);
-    if (!eig4(B, Q, V)) stat |= ST_EIGEN;
+    done = no_z_coupling(L) && block_modes(L, p.omega, kx, ky, Q, V);
   }
-  // Poynting flux Pz = ¼ Re(V_j · W_j), W = R4s V = (V3, -V2, -V1, V0)
-  double Pz[4];
-  for (int j = 0; j < 4; ++j) {
-    cd s = conj(V[0][j]) * V[3][j];
-    s += conj(V[1][j]) * (-V[2][j]);
-    s += conj(V[2][j]) * (-V[1][j]);
-    s += conj(V[3][j]) * V[0][j];
-    Pz[j] = 0.25 * s.x;
-  }
-  const double tol = 1.4901161193847656e-08;
-  int fsel[2] = {-1, -1}, bsel[2] = {-1, -1}, deg[4];
-  int nf = 0, nb = 0, nd = 0;
-  for (int j = 0; j < 4; ++j) {
-    if (fabs(Pz[j]) > tol) {
-      if (Pz[j] > 0) { if (nf < 2) fsel[nf] = j; ++nf; }
-      else { if (nb < 2) bsel[nb] = j; ++nb; }
-    } else if (fabs(Q[j].y) > tol) {
-      if (Q[j].y > tol) { if (nf < 2) fsel[nf] = j; ++nf; }
-      else if (Q[j].y < -tol) { if (nb < 2) bsel[nb] = j; ++nb; }
-    } else {
-      deg[nd++] = j;
-    }
-  }
-  if (nf > 2 || nb > 2) stat |= ST_SORT;
-  for (int i = 0; i < nd; ++i) {
-    if (nf < 2) fsel[nf++] = deg[i];
-    else if (nb < 2) bsel[nb++] = deg[i];
-  }
-  double2* rec = p.modes + (long)layer * 20 * n;
-  for (int m = 0; m < 2; ++m) {
-    int jf = fsel[m], jb = bsel[m];
-    for (int i = 0; i < 4; ++i) {
-      st(rec, i + 4 * m, n, node, jf >= 0 ? V[i][jf] : cd{0, 0});
-      st(rec, 8 + i + 4 * m, n, node, jb >= 0 ? V[i][jb] : cd{0, 0});
-    }
-    st(rec, 16 + m, n, node, jf >= 0 ? Q[jf] : cd{0, 0});
-    st(rec, 18 + m, n, node, jb >= 0 ? Q[jb] : cd{0, 0});
-  }
+  p.lstat[(long)layer * n + node] = done ? classify_store(p, layer, node, Q, V) : ST_NEED_QR;
+}
+
+// K1b: the general 4x4 QR path for the (node, layer) pairs K1 left
+__global__ void __launch_bounds__(128) k_layer_modes_qr(TransferParams p) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long n = p.n;
+  if (t >= n * p.nL) return;
+  int layer = (int)(t / n);
+  long node = t - (long)layer * n;
+  if (p.lstat[(long)layer * n + node] != ST_NEED_QR) return;
+  double kx, ky;
+  node_k(p, p.off + node, kx, ky);
+  const LayerDev& L = p.layers[layer];
+  cd Q[4], V[4][4], B[4][4];
+  berreman(L, p.omega, kx, ky, B);
+  uint8_t stat = 0;
+  if (!eig4(B, Q, V)) stat = ST_EIGEN;
+  else stat = classify_store(p, layer, node, Q, V);
   p.lstat[(long)layer * n + node] = stat;
 }
 
@@ -804,6 +956,13 @@ cudaError_t launch_layer_modes(const TransferParams& p, cudaStream_t stream) {
   long tot = (long)p.n * p.nL;
   if (tot <= 0) return cudaSuccess;
   k_layer_modes<<<(unsigned)((tot + 127) / 128), 128, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_layer_modes_qr(const TransferParams& p, cudaStream_t stream) {
+  long tot = (long)p.n * p.nL;
+  if (tot <= 0) return cudaSuccess;
+  k_layer_modes_qr<<<(unsigned)((tot + 127) / 128), 128, 0, stream>>>(p);
   return cudaGetLastError();
 }
 
