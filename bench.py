@@ -188,6 +188,9 @@ CONFIG = {"workload": "batched spectral solve + full 3x3 G: 8-layer biaxial/gyro
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel on this workload
 # (profiles/k_lateral_fp64_bench_config2.md); None until captured
 TRAFFIC = {"k_lateral": 81.7e6}
+DTYPE = {"int8x3": "f64 solve, int8 x3-digit tensor-core synthesis (exact int32 accum)",
+         "split_bf16": "f64 solve, split-bf16 x3 tensor-core synthesis (fp32 accum)",
+         "fp64": "f64"}
 
 
 def measured_peaks():
@@ -201,6 +204,49 @@ def measured_peaks():
     except (OSError, KeyError, ValueError):
         return {"bf16_sustained": (1400.0, "fallback (sustained bf16 on this pool)"),
                 "bf16_burst": (1590.0, "fallback"), "hbm": (6650.0, "fallback")}
+
+
+# FP64 operations per node of the per-node solve kernels on this workload, from one ncu count
+# of their DFMA/DADD/DMUL instructions (2 per DFMA); None until captured
+FP64_OPS_PER_NODE = {}
+FP64_NOMINAL = 37.2  # TFLOP/s: 148 SM x 64 FP64 FMA/clk x 2 x 1.965 GHz (no measured FP64 peak)
+
+
+def roofline(name, prof):
+    """Roofline entry of one kernel from its CUDA-event time in the timed region."""
+    roof = {"kernel": name, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None,
+            "traffic": TRAFFIC.get(name)}
+    if name is None or name not in prof or not prof[name][1]:
+        return roof
+    tot_ms, nl = prof[name]
+    t = tot_ms / nl * 1e-3  # seconds per launch
+    nodes = N_PANELS * ORDER * N_PHI
+    cmacs = float(NXY * NXY * nodes * NZ * 9)  # complex multiply-adds of one lateral contraction
+    work = "8 flop per complex multiply-add x 1024 pixels x 65536 nodes x 72 columns per launch"
+    peaks = measured_peaks()
+    if name in ("k_lateral_tc", "k_lateral_i8"):
+        achieved = 8.0 * cmacs / t / 1e12
+        peak, src = peaks["bf16_sustained"]
+        roof.update(bound="tensor", achieved=achieved, peak=peak, unit="TFLOP/s", frac=achieved / peak,
+                    peak_source=src, work=work)
+        if name == "k_lateral_tc":
+            roof.update(split_multiplier=6, tensor_flops_executed_per_launch=6 * 8.0 * cmacs)
+        else:
+            # six int8 digit products; int8 runs at twice the bf16 rate (nominal 4.5 vs 2.25 PFLOP/s)
+            ex = 6 * 8.0 * cmacs
+            roof.update(split_multiplier=6, int8_ops_executed_per_launch=ex,
+                        executed_frac_of_int8_peak=ex / t / 1e12 / (2 * peak),
+                        int8_peak_note="int8 peak taken as 2 x the measured bf16 figure (nominal ratio)")
+    elif name == "k_lateral":
+        achieved = 8.0 * cmacs / t / 1e12
+        roof.update(bound="fp64", achieved=achieved, peak=FP64_NOMINAL, unit="TFLOP/s", frac=achieved / FP64_NOMINAL,
+                    peak_source="nominal FP64; no measured FP64 peak", work=work)
+    elif FP64_OPS_PER_NODE.get(name):
+        achieved = FP64_OPS_PER_NODE[name] * nodes / t / 1e12
+        roof.update(bound="fp64", achieved=achieved, peak=FP64_NOMINAL, unit="TFLOP/s",
+                    frac=achieved / FP64_NOMINAL, peak_source="nominal FP64; no measured FP64 peak",
+                    work=f"{FP64_OPS_PER_NODE[name]:.0f} FP64 ops per node x {nodes} nodes per launch (ncu count)")
+    return roof
 
 
 def run_ours(args):
@@ -282,29 +328,17 @@ def run_ours(args):
                "kind": "port", "sample": f"1 wavelength, {n} of {N_PANELS * ORDER * N_PHI} nodes "
                                          f"({N_PHI // 4} φ x 1024 kρ), time scaled x{scale:g} (linear in nodes)"}
 
-    # roofline of the dominant kernel, from the CUDA-event profile of the timed region
-    top = max(prof.items(), key=lambda kv: kv[1][0]) if prof else (None, (0.0, 0))
-    name, (tot_ms, nl) = top
-    nodes = N_PANELS * ORDER * N_PHI
-    cmacs = float(NXY * NXY * nodes * NZ * 9)  # complex multiply-adds of one lateral contraction
-    peaks = measured_peaks()
-    roof = {"kernel": name, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None}
-    if name == "k_lateral_tc" and nl:
-        achieved = 8.0 * cmacs / (tot_ms / nl * 1e-3) / 1e12
-        peak, src = peaks["bf16_sustained"]
-        roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": TRAFFIC.get(name), "peak_source": src,
-                "work": "8 flop per complex multiply-add x 1024 pixels x 65536 nodes x 72 columns per launch",
-                "split_multiplier": 6, "tensor_flops_executed_per_launch": 6 * 8.0 * cmacs}
-    elif name == "k_lateral" and nl:
-        achieved = 8.0 * cmacs / (tot_ms / nl * 1e-3) / 1e12
-        roof = {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": 37.2, "unit": "TFLOP/s",
-                "frac": achieved / 37.2, "traffic": TRAFFIC.get(name),
-                "peak_source": "nominal FP64 (148 SM x 64 FMA/clk x 1.965 GHz); no measured FP64 peak"}
+    # roofline of the dominant kernel (and of the lateral contraction), from the CUDA-event
+    # profile of the timed region
+    top = max(prof.items(), key=lambda kv: kv[1][0])[0] if prof else None
+    lateral = next((k for k in ("k_lateral_i8", "k_lateral_tc", "k_lateral") if k in prof), None)
+    roof = roofline(top, prof)
+    if lateral and lateral != top:
+        roof["lateral"] = roofline(lateral, prof)
     launches = int(sum(v[1] for v in prof.values()))
     line = {"metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f64 solve, split-bf16 x3 tensor-core synthesis (fp32 accum)",
+            "dtype": DTYPE[args.precision],
             "data": "synthetic (seeded)", "config": dict(CONFIG, precision=args.precision), "max_rel_err_vs_oracle": err,
             "e2e": {"value": e2e, "unit": "entries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": ms_e2e},
@@ -325,8 +359,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-check", action="store_true")
-    ap.add_argument("--precision", default="split_bf16", choices=["split_bf16", "fp64"],
-                    help="synthesis contraction: tensor cores (split-BF16, FP32 accumulate) or FP64 CUDA cores")
+    ap.add_argument("--precision", default="int8x3", choices=list(DTYPE),
+                    help="lateral contraction: int8 tensor cores (three base-256 digits, exact INT32 "
+                         "accumulation), split-BF16 tensor cores (FP32 accumulation) or FP64 CUDA cores")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -40,7 +40,7 @@ enum {
 /* `terms` of closed_form_G (mod_ClosedFormField.jl:143-160) */
 enum { YTF_TERMS_ALL = 0, YTF_TERMS_DIRECT = 1, YTF_TERMS_SCATTERED = 2, YTF_TERMS_TOEPLITZ = 3, YTF_TERMS_HANKEL = 4 };
 /* arithmetic of the synthesis contraction */
-enum { YTF_PREC_FP64 = 0, YTF_PREC_SPLIT_BF16 = 1 };
+enum { YTF_PREC_FP64 = 0, YTF_PREC_SPLIT_BF16 = 1, YTF_PREC_INT8X3 = 2 };
 /* `rotation` of build_cavity_transfer_2d (mod_CavityTransfer.jl:307-318) */
 enum { YTF_ROT_AUTO = -1, YTF_ROT_OFF = 0, YTF_ROT_ON = 1 };
 /* material kinds (the reference's material TYPES, mod_ModeSolver.jl:28-65) */
@@ -103,8 +103,11 @@ int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* cache, double* T, double* Qf
 
 /* closed_form_G(cache, obs_layer, zsrc_local, z_obs, xs, ys; terms)
  * (1D: mod_ClosedFormField.jl:435-487; 2D, lateral=:direct: :711-753). out: Nx*Ny*Nz*9
- * complex, Julia layout. precision: YTF_PREC_FP64 (CUDA-core FP64 contraction) or
- * YTF_PREC_SPLIT_BF16 (tensor-core contraction, FP32 accumulation). */
+ * complex, Julia layout. precision: YTF_PREC_FP64 (CUDA-core FP64 contraction),
+ * YTF_PREC_SPLIT_BF16 (tensor-core contraction, split-BF16 operands, FP32 accumulation) or
+ * YTF_PREC_INT8X3 (int8 tensor-core contraction: operands in three fixed-point base-256
+ * digits, exact INT32 accumulation). The two tensor-core modes apply to the 2D lateral sum;
+ * the 1D Bessel synthesis is FP64 in every mode. */
 int ytf_green(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, double zsrc_local, int nz, const double* z_obs,
               int nx, const double* xs, int ny, const double* ys, int terms, int precision, double* out,
               int out_is_device);

@@ -185,11 +185,13 @@ def test_empty_and_single_node_inputs(ytf, oracle):
     assert relerr(ytf.closed_form_G(c, 2, 0.3, [0.2, 0.5], xs, ys), oracle.closed_form_G(o, 2, 0.3, [0.2, 0.5], xs, ys)) < 1e-10
 
 
+@pytest.mark.parametrize("prec", ["split_bf16", "int8x3"])
 @pytest.mark.parametrize("idx", [3, 4])
-def test_lateral_split_bf16_tensor_cores_match_fp64(ytf, oracle, idx):
-    """The tensor-core lateral synthesis (3-term BF16 split, FP32 accumulation in tensor
-    memory, FP64 sum of node slices) against the FP64 path and the oracle: ≤ 1e-6
-    relative (the metric's bound), on biaxial and gyrotropic stacks."""
+def test_lateral_tensor_cores_match_fp64(ytf, oracle, idx, prec):
+    """The tensor-core lateral synthesis against the FP64 path and the oracle: ≤ 1e-6
+    relative (the metric's bound), on biaxial and gyrotropic stacks. split_bf16: 3-term
+    BF16 split, FP32 accumulation in tensor memory; int8x3: three fixed-point base-256
+    digits per operand, exact INT32 accumulation; both sum node slices in FP64."""
     _, st = FOUNDATION_STACKS[idx]
     kr, wr = krho_grid(st, W, kmax=10.0, width=0.5)
     ph, wp = uniform_phi(32)
@@ -198,14 +200,15 @@ def test_lateral_split_bf16_tensor_cores_match_fp64(ytf, oracle, idx):
     ys = np.linspace(-0.25, 0.2, 9)
     for obs, zo in ((2, [0.1, 0.35, 0.6]), (1, [0.4]), (3, [0.2, 0.3])):
         G64 = ytf.closed_form_G(gc, obs, 0.3, zo, xs, ys)
-        Gtc = ytf.closed_form_G(gc, obs, 0.3, zo, xs, ys, precision="split_bf16")
+        Gtc = ytf.closed_form_G(gc, obs, 0.3, zo, xs, ys, precision=prec)
         assert relerr(Gtc, G64) < 1e-6, (obs, relerr(Gtc, G64))
     oc = oracle.build_cavity_transfer_2d(st, W, 2, kr, wr, ph, wp, obs_layers=[2])
     Go = oracle.closed_form_G(oc, 2, 0.3, [0.1, 0.6], xs, ys)
-    assert relerr(ytf.closed_form_G(gc, 2, 0.3, [0.1, 0.6], xs, ys, precision="split_bf16"), Go) < 1e-6
+    assert relerr(ytf.closed_form_G(gc, 2, 0.3, [0.1, 0.6], xs, ys, precision=prec), Go) < 1e-6
 
 
-def test_lateral_split_bf16_ragged_tiles(ytf):
+@pytest.mark.parametrize("prec", ["split_bf16", "int8x3"])
+def test_lateral_tensor_cores_ragged_tiles(ytf, prec):
     """Pixel counts and column counts that do not fill a 128-pixel tile or a 16-wide MMA,
     node counts that do not fill a 16-node stage, and more than 128 columns (two N-tiles)."""
     _, st = FOUNDATION_STACKS[4]
@@ -217,5 +220,24 @@ def test_lateral_split_bf16_ragged_tiles(ytf):
         ys = np.linspace(-0.1, 0.15, ny)
         zo = list(np.linspace(0.05, 0.85, nz))
         G64 = ytf.closed_form_G(gc, 2, 0.3, zo, xs, ys)
-        Gtc = ytf.closed_form_G(gc, 2, 0.3, zo, xs, ys, precision="split_bf16")
+        Gtc = ytf.closed_form_G(gc, 2, 0.3, zo, xs, ys, precision=prec)
         assert relerr(Gtc, G64) < 1e-6, (nx, ny, nz, relerr(Gtc, G64))
+
+
+def test_lateral_int8_slices_capped_and_exact(ytf):
+    """int8x3 with more pixel tiles than SMs, so one CTA would take every node: the host
+    caps a node slice at 16384 nodes (INT32 headroom) and the slices are summed in FP64.
+    The integer contraction is exact, so two calls agree bit for bit and the error stays
+    far inside the bound (the operands carry ~23 bits each)."""
+    _, st = FOUNDATION_STACKS[3]
+    kr, wr = krho_grid(st, W, kmax=8.0, width=0.5)
+    nphi = max(1, -(-20000 // len(kr)))
+    ph, wp = uniform_phi(nphi)
+    gc = ytf.build_cavity_transfer_2d(st, W, 2, kr, wr, ph, wp, obs_layers=[2])
+    assert gc.n > 16384
+    xs = np.linspace(-0.3, 0.3, 160)
+    ys = np.linspace(-0.25, 0.2, 120)
+    G64 = ytf.closed_form_G(gc, 2, 0.3, [0.45], xs, ys)
+    G8 = ytf.closed_form_G(gc, 2, 0.3, [0.45], xs, ys, precision="int8x3")
+    assert relerr(G8, G64) < 2e-7, relerr(G8, G64)
+    assert np.array_equal(G8, ytf.closed_form_G(gc, 2, 0.3, [0.45], xs, ys, precision="int8x3"))

@@ -23,7 +23,7 @@ from ._native import _i, _u8, lib, ptr
 from .materials import stack_arrays
 
 TERMS = {"all": 0, "direct": 1, "scattered": 2, "toeplitz": 3, "hankel": 4}
-PRECISION = {"fp64": 0, "split_bf16": 1}
+PRECISION = {"fp64": 0, "split_bf16": 1, "int8x3": 2}
 
 
 class YTFError(ValueError):
@@ -242,6 +242,11 @@ def build_cavity_transfer_2d(stack, omega, source_layer, kr_nodes, kr_weights, p
 def closed_form_G(cache: _Cache, obs_layer: int, zsrc_local: float, z_obs, xs, ys, terms: str = "all",
                   precision: str = "fp64", out=None):
     """G[x, y, z, component, moment] of a point source (terms as the reference).
+
+    ``precision`` selects the arithmetic of the 2D lateral sum: "fp64" (CUDA-core FP64),
+    "split_bf16" (tensor cores, split-BF16 operands, FP32 accumulation) or "int8x3" (int8
+    tensor cores, operands in three fixed-point base-256 digits, exact INT32 accumulation).
+    The 1D Bessel synthesis is FP64 in every mode.
 
     ``out``: optional torch tensor (complex128, Nx*Ny*Nz*9 elements, Julia order) to write
     into instead of returning a new host array: a CUDA tensor (G stays on the device) or

@@ -645,7 +645,7 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
   if ((terms == YTF_TERMS_TOEPLITZ || terms == YTF_TERMS_HANKEL || terms == YTF_TERMS_DIRECT) && !same)
     return fail(ctx, YTF_ERR_ARG, "closed_form_G: terms needs obs_layer == source_layer (" + std::to_string(c->src) +
                                       "), got " + std::to_string(obs_layer));
-  if (precision != YTF_PREC_FP64 && precision != YTF_PREC_SPLIT_BF16)
+  if (precision != YTF_PREC_FP64 && precision != YTF_PREC_SPLIT_BF16 && precision != YTF_PREC_INT8X3)
     return fail(ctx, YTF_ERR_ARG, "closed_form_G: unknown precision mode");
   double zpos = c->src == 1 ? c->d_src - zsrc_local : zsrc_local;
   const double se = 1.4901161193847656e-08;
@@ -750,6 +750,45 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
     int ncol = 9 * nz;
     WS(S, double2, "g_S", (size_t)ncol * c->n);
     CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream)));
+    if (precision == YTF_PREC_INT8X3) {
+      // int8 tensor cores: FP32 phase tables, fixed-point digits, exact INT32 accumulation,
+      // FP64 reduction of the node slices
+      WS(Px, float2, "g_px", (size_t)c->n * nx);
+      WS(Py, float2, "g_py", (size_t)c->n * ny);
+      CK(LAUNCH("k_phase_tables", launch_phase_tables(v, nx, ny, dxs, dys, Px, Py, ctx->stream)));
+      LateralI8 lp;
+      std::memset(&lp, 0, sizeof(lp));
+      lp.npix = npix; lp.n = c->n; lp.nx = nx; lp.ny = ny; lp.ncol = ncol;
+      lp.ctile = lateral_i8_ctile(ncol);
+      lp.Np = ((2 * lp.ctile + 15) / 16) * 16;
+      lp.ntile = (ncol + lp.ctile - 1) / lp.ctile;
+      lp.Px = Px; lp.Py = Py; lp.S = S;
+      // one CTA per SM: (pixel tiles x column tiles) x node slices fill one wave; a slice
+      // holds at most 16384 nodes so the INT32 accumulators cannot overflow
+      long tiles = ((npix + 127) / 128) * lp.ntile;
+      long want = std::max(1L, (long)nsm / tiles);
+      long kchunk = (c->n + want - 1) / want;
+      kchunk = std::min(16384L, std::max(32L, ((kchunk + 31) / 32) * 32));
+      lp.kchunk = kchunk;
+      lp.nchunk = (int)((c->n + kchunk - 1) / kchunk);
+      WS(Bq, uint8_t, "g_i8_b", (size_t)lp.ntile * lp.nchunk * (kchunk / 32) * lateral_i8_stage_bytes(lp.Np));
+      WS(sB, double, "g_i8_sb", (size_t)lp.nchunk * ncol);
+      WS(fac, double, "g_i8_fac", (size_t)lp.nchunk * ncol);
+      WS(Gp, double2, "g_partial2", (size_t)lp.nchunk * npix * ncol);
+      WS(err, unsigned, "g_tc_err", 1);
+      lp.Bq = Bq; lp.sB = sB; lp.fac = fac; lp.partial = Gp; lp.err = err;
+      CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+      CK(LAUNCH("k_lateral_i8", launch_lateral_i8(lp, ctx->stream)));
+      CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, lp.nchunk, Gp, G, ctx->stream)));
+      unsigned herr = 0;
+      CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
+      if (!out_is_device) CK(cudaMemcpyAsync(out, G, sizeof(double2) * nout, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      prof_collect(ctx);
+      return YTF_OK;
+    }
     if (precision == YTF_PREC_SPLIT_BF16) {
       // tensor cores: FP32 phase tables, split-BF16 contraction, FP64 reduction of the slices
       WS(Px, float2, "g_px", (size_t)c->n * nx);

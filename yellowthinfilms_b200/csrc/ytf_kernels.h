@@ -130,6 +130,30 @@ size_t lateral_tc_smem(int Np);
 int lateral_tc_ctile(int ncol);
 cudaError_t launch_lateral_tc(const LateralTC& p, int splits, cudaStream_t s);
 
+// 2D lateral synthesis on the int8 tensor cores (three base-256 digits per operand, exact
+// INT32 accumulation)
+struct LateralI8 {
+  long npix, n;
+  int nx, ny, ncol;
+  int ctile;         // complex columns per column tile (≤ 80)
+  int Np;            // 2 * ctile rounded up to a multiple of 16 (MMA N, ≤ 160)
+  int ntile;         // column tiles
+  long kchunk;       // nodes per slice: a multiple of 32, ≤ 16384
+  int nchunk;        // slices = ceil(n / kchunk)
+  const float2* Px;  // [n][nx]
+  const float2* Py;  // [n][ny]
+  const double2* S;  // [ncol][n]
+  uint8_t* Bq;       // [ntile][nchunk][kchunk/32][3 planes][Np rows x 64 B] digit images
+  double* sB;        // [nchunk][ncol] fixed-point scale of the strengths
+  double* fac;       // [nchunk][ncol] output factor 2^16 / (sA sB)
+  double2* partial;  // [nchunk][npix * ncol]
+  unsigned* err;     // nonzero if a pipeline wait timed out
+};
+size_t lateral_i8_stage_bytes(int Np);
+size_t lateral_i8_smem(int Np);
+int lateral_i8_ctile(int ncol);
+cudaError_t launch_lateral_i8(const LateralI8& p, cudaStream_t s);
+
 // Gauss-Legendre panels -> nodes/weights, bit-exact with the CPU restatement
 cudaError_t launch_gl_nodes(int npanels, const double* pa, const double* pb, const int* sing_side, const double* xi,
                             const double* wx, int order, double* nodes, double* wts, cudaStream_t s);

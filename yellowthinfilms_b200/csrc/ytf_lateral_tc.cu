@@ -28,6 +28,7 @@
 
 #include "ytf_complex.cuh"
 #include "ytf_kernels.h"
+#include "ytf_tcgen05.cuh"
 
 namespace ytf {
 
@@ -41,31 +42,9 @@ constexpr int TC_XCOL = 128;     // tensor-memory column of the cross-product ac
 constexpr int TC_PERIOD = 8;     // stages (8 x 16 nodes) between FP64 drains
 constexpr int TC_SMAX = 3;       // (column, node) strength pairs per thread and stage: 48 x 16 / 256
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// byte offset of element (row r, k) in an R x 32 bf16 plane
+__device__ __forceinline__ uint32_t plane_off_bf(int r, int k) { return plane_off(r, 2 * k); }
 
-// byte offset of element (row r, k) in an R x 32 bf16 plane: [R/8][4 K-cores][8 rows][8 elems]
-__device__ __forceinline__ uint32_t plane_off(int r, int k) {
-  return (uint32_t)((r >> 3) * 512 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
-}
-
-// shared-memory matrix descriptor: start >> 4, LBO = 128 B (the two K-cores of one K=16
-// MMA), SBO = 512 B (consecutive 8-row groups), descriptor version 1, no swizzle
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(512u >> 4) << 32) |
-         (1ull << 46);
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred P1;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, P1;\n\t}"
-      : "=r"(ok)
-      : "r"(addr), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
 __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
   for (long i = 0; i < TC_WAIT_LIMIT; ++i)
     if (mbar_try(addr, parity)) return true;
@@ -89,13 +68,6 @@ __device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t ad, uint64_t bd,
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, PD;\n\t}"
       ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
       : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld8(uint32_t ta, uint32_t v[8]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-               : "r"(ta)
-               : "memory");
 }
 
 // Operands of one 16-node stage, held in registers between the global loads (issued one
@@ -147,7 +119,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_lateral_tc(LateralTC p) {
       uint8_t* Bp = smem + s * stageBytes + 3 * planeA + pl * planeB;
       for (int idx = tid; idx < (p.Np - 2 * nct) * 16; idx += TC_THREADS) {
         int r = 2 * nct + idx / 16, kk = 2 * (idx % 16);
-        *reinterpret_cast<uint32_t*>(Bp + plane_off(r, kk)) = 0u;
+        *reinterpret_cast<uint32_t*>(Bp + plane_off_bf(r, kk)) = 0u;
       }
     }
   if (tid == 0) {
@@ -213,7 +185,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_lateral_tc(LateralTC p) {
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
           uint4 v = make_uint4(w[pl][half][0], w[pl][half][1], w[pl][half][2], w[pl][half][3]);
-          *reinterpret_cast<uint4*>(A + pl * planeA + plane_off(r, 16 * hh + 8 * half)) = v;
+          *reinterpret_cast<uint4*>(A + pl * planeA + plane_off_bf(r, 16 * hh + 8 * half)) = v;
         }
     }
     // ---- B: strengths of nct columns x 16 nodes ----
@@ -229,8 +201,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_lateral_tc(LateralTC p) {
 #pragma unroll
         for (int pl = 0; pl < 3; ++pl) {
           uint8_t* Bp = B + pl * planeB;
-          *reinterpret_cast<uint32_t*>(Bp + plane_off(2 * c, 2 * q)) = pack2(rs[pl], __hneg(is[pl]));
-          *reinterpret_cast<uint32_t*>(Bp + plane_off(2 * c + 1, 2 * q)) = pack2(is[pl], rs[pl]);
+          *reinterpret_cast<uint32_t*>(Bp + plane_off_bf(2 * c, 2 * q)) = pack2(rs[pl], __hneg(is[pl]));
+          *reinterpret_cast<uint32_t*>(Bp + plane_off_bf(2 * c + 1, 2 * q)) = pack2(is[pl], rs[pl]);
         }
       }
     }
