@@ -4,20 +4,23 @@
 // mod_ClosedFormField.jl:743-753) as one real GEMM per tile, as in the split-BF16 kernel:
 //   A'[pix, 2n + {0,1}] = (Re P, Im P),  P = Px[n, i] · Py[n, j]
 //   B'[(col, re), 2n + {0,1}] = (Sr, -Si),  B'[(col, im), 2n + {0,1}] = (Si, Sr)
-// but in fixed point: A' as X = rint(sA · a) with sA = 4194000 (|P| = 1, so |X| < 2^22), and
-// B' per (column, node slice) as Y = rint(sB · b) with sB = 2^(22 - e), 2^(e-1) <= max|S| < 2^e.
-// X and Y are written in three signed base-256 digits (X = 65536 d0 + 256 d1 + d2, d0 in
-// [-64, 64], d1, d2 in [-128, 127]) and the six digit products of weight ≥ 256^2 are summed
-// exactly by the tensor cores in INT32: level L = i + j in tensor-memory accumulator L. The
-// dropped products (weight ≤ 256) are ~2^-22 of the leading one. Integer accumulation is
-// exact, so the result depends on no accumulation order; the only roundings are the FP32 phase
-// product, the two fixed-point quantisations and the FP64 combination at the end:
+// but in fixed point: A' as X = rint(sA · a) with sA = 4194000 (|P| = 1, so |X| < 2^22: the
+// range of the magic-number rounding below), and B' per (column, node slice) as
+// Y = rint(sB · b) with sB = 8355000 / max|S| over the slice (|Y| ≤ 8355000 < 2^23).
+// X and Y are written in three signed base-256 digits (X = 65536 d0 + 256 d1 + d2, top digit
+// in [-64, 64] for X and [-127, 127] for Y, d1, d2 in [-128, 127]) and the six digit products
+// of weight ≥ 256^2 are summed exactly by the tensor cores in INT32: level L = i + j in
+// tensor-memory accumulator L. The dropped products (weight ≤ 256) are ~2^-23 of the leading
+// one and dominate the error (a fourth accumulator would not fit: 4 x 144 columns > 512).
+// Integer accumulation is exact, so the result depends on no accumulation order; the only
+// roundings are the FP32 phase product, the two fixed-point quantisations and the FP64
+// combination at the end:
 //   X·Y / 2^16 = 65536 acc0 + 256 acc1 + acc2,   G = that · 2^16 / (sA · sB).
-// Overflow: per real term |level-2 product sum| ≤ 64·128 + 128·128 + 128·64 = 32768; the host
-// keeps each CTA's node slice ≤ 16384 nodes (K ≤ 32768 real terms), so |acc| ≤ 2^30.
+// Overflow: per real term |level-2 product sum| ≤ 64·128 + 128·128 + 128·127 = 40832; the
+// host keeps each CTA's node slice ≤ 16384 nodes (K ≤ 32768 real terms), so |acc| < 1.4e9.
 //
 // Kernels:
-//   k_bscale : per (node slice, column) exponent of max|S| -> sB and the output factor
+//   k_bscale : per (node slice, column) max|S| -> sB and the output factor
 //   k_bslice : B' digits, written once per launch in the exact shared-memory image of each
 //              32-node stage (3 planes x Np rows x 64 B, canonical K-major core matrices)
 //   k_lateral_i8 : one CTA per (128-pixel tile, column tile, node slice); 8 producer warps
@@ -92,9 +95,9 @@ __global__ void k_bscale(LateralI8 p) {
       p.sB[o] = 0.0;
       p.fac[o] = __longlong_as_double(0x7ff8000000000000LL);
     } else if (m > 0.0) {
-      int e;
-      frexp(m, &e);  // 2^(e-1) <= m < 2^e
-      const double sB = ldexp(1.0, 22 - e);
+      // |S sB| ≤ 8355000 (one rounding of the product above it is still below 8355000.5), so
+      // the top digit (Y + 32896) >> 16 stays in [-127, 127]
+      const double sB = 8355000.0 / m;
       p.sB[o] = sB;
       p.fac[o] = 65536.0 / ((double)I8_SA * sB);
     } else {
@@ -104,7 +107,7 @@ __global__ void k_bscale(LateralI8 p) {
   }
 }
 
-// three signed base-256 digits of Y (|Y| ≤ 2^22), most significant first, as bytes
+// three signed base-256 digits of Y (|Y| ≤ 8355000), most significant first, as bytes
 __device__ __forceinline__ void digits3(int Y, uint32_t& d0, uint32_t& d1, uint32_t& d2) {
   d2 = (uint32_t)Y & 255u;
   d1 = (uint32_t)((Y + 128) >> 8) & 255u;
