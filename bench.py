@@ -185,8 +185,8 @@ CONFIG = {"workload": "batched spectral solve + full 3x3 G: 8-layer biaxial/gyro
 # --------------------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------------------
-# DRAM bytes (read + write) per launch from one ncu capture of the kernel on this workload
-# (profiles/k_lateral_fp64_bench_config2.md); None until captured
+# DRAM bytes (read + write) per launch from one ncu capture of the kernel on this workload;
+# absent until captured
 TRAFFIC = {"k_lateral": 81.7e6}
 DTYPE = {"int8x3": "f64 solve, int8 x3-digit tensor-core synthesis (exact int32 accum)",
          "split_bf16": "f64 solve, split-bf16 x3 tensor-core synthesis (fp32 accum)",
