@@ -52,6 +52,38 @@ def test_transfer_1d_cache_matches_oracle(ytf, oracle, idx):
         _cmp_cache(gc, oc)
 
 
+@pytest.mark.parametrize("idx", [1, 3, 4])
+def test_source_only_chain_matches_general_chain(ytf, oracle, idx):
+    """A cache whose only observation layer is the source layer takes the forward-only
+    chain (SRight[src] accumulated left to right, no stored interfaces); the same node
+    solve with every layer observed takes the general chain (backward SRight scan). The
+    source-layer rows must agree (to rounding: the star products are grouped differently),
+    and the fast-path cache must match the oracle, for top, middle and last finite source
+    layers, 1D and 2D."""
+    _, st = FOUNDATION_STACKS[idx]
+    kr, wr = krho_grid(st, W, kmax=12.0)
+    ph, wp = uniform_phi(4)
+    N = len(st)
+    two_d = idx >= 3
+    for src in sorted({1, max(1, N // 2), N - 1}):
+        if two_d:
+            fast = ytf.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp, obs_layers=[src])
+            full = ytf.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp, obs_layers=list(range(1, N + 1)))
+            oc = oracle.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp, obs_layers=[src])
+        else:
+            fast = ytf.build_cavity_transfer_1d(st, W, src, kr, wr, obs_layers=[src])
+            full = ytf.build_cavity_transfer_1d(st, W, src, kr, wr, obs_layers=list(range(1, N + 1)))
+            oc = oracle.build_cavity_transfer_1d(st, W, src, kr, wr, obs_layers=[src])
+        gf, gg = fast.export(), full.export()
+        i = full.obs_layers.index(src)
+        assert relerr(gf["T"][0], gg["T"][i]) < 1e-11, src
+        for key in ("Qf", "Qb", "sf", "sb"):
+            assert relerr(gf[key], gg[key]) < 1e-13, (src, key)
+        assert relerr(gf["basis"][0], gg["basis"][i]) < 1e-13, src
+        assert np.array_equal(fast.status()[0], full.status()[0])
+        _cmp_cache(fast, oc)
+
+
 @pytest.mark.parametrize("idx", [0, 1, 2])
 def test_green_1d_matches_oracle(ytf, oracle, idx):
     _, st = FOUNDATION_STACKS[idx]

@@ -210,6 +210,13 @@ int alloc_cache(ytf_ctx* ctx, ytf_cache* c) {
 }
 
 // which SLeft/SRight slots the walk to the observation layers reads (k_chain)
+// the forward-only chain applies when every observation layer is the source layer
+bool only_source_observed(const TransferParams& p) {
+  for (int i = 0; i < p.nobs; ++i)
+    if (p.obs[i] != p.src) return false;
+  return true;
+}
+
 void need_masks(int N, int src, const int* obs, int nobs, uint32_t& needL, uint32_t& needR) {
   needL = needR = 0;
   for (int i = 0; i < nobs; ++i) {
@@ -301,7 +308,8 @@ int run_transfer(ytf_ctx* ctx, TransferParams p, long total) {
     p.n = std::min(chunk, total - off);
     CK(LAUNCH("k_layer_modes", launch_layer_modes(p, ctx->stream)));
     CK(LAUNCH("k_layer_modes_qr", launch_layer_modes_qr(p, ctx->stream)));
-    CK(LAUNCH("k_chain", launch_chain(p, ctx->stream)));
+    if (only_source_observed(p)) CK(LAUNCH("k_chain_src", launch_chain_src(p, ctx->stream)));
+    else CK(LAUNCH("k_chain", launch_chain(p, ctx->stream)));
   }
   return YTF_OK;
 }
@@ -547,7 +555,8 @@ int ytf_transfer_2d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_
       b.Tout = bT;
       CK(LAUNCH("k_layer_modes", launch_layer_modes(b, ctx->stream)));
       CK(LAUNCH("k_layer_modes_qr", launch_layer_modes_qr(b, ctx->stream)));
-      CK(LAUNCH("k_chain", launch_chain(b, ctx->stream)));
+      if (only_source_observed(b)) CK(LAUNCH("k_chain_src", launch_chain_src(b, ctx->stream)));
+      else CK(LAUNCH("k_chain", launch_chain(b, ctx->stream)));
       TransferParams f = p;
       f.mode = 1;
       f.n = nb;
@@ -753,16 +762,13 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
     if (precision == YTF_PREC_INT8X3) {
       // int8 tensor cores: FP32 phase tables, fixed-point digits, exact INT32 accumulation,
       // FP64 reduction of the node slices
-      WS(Px, float2, "g_px", (size_t)c->n * nx);
-      WS(Py, float2, "g_py", (size_t)c->n * ny);
-      CK(LAUNCH("k_phase_tables", launch_phase_tables(v, nx, ny, dxs, dys, Px, Py, ctx->stream)));
       LateralI8 lp;
       std::memset(&lp, 0, sizeof(lp));
       lp.npix = npix; lp.n = c->n; lp.nx = nx; lp.ny = ny; lp.ncol = ncol;
       lp.ctile = lateral_i8_ctile(ncol);
       lp.Np = ((2 * lp.ctile + 15) / 16) * 16;
       lp.ntile = (ncol + lp.ctile - 1) / lp.ctile;
-      lp.Px = Px; lp.Py = Py; lp.S = S;
+      lp.S = S;
       // one CTA per SM: (pixel tiles x column tiles) x node slices fill one wave; a slice
       // holds at most 16384 nodes so the INT32 accumulators cannot overflow
       long tiles = ((npix + 127) / 128) * lp.ntile;
@@ -771,6 +777,11 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
       kchunk = std::min(16384L, std::max(32L, ((kchunk + 31) / 32) * 32));
       lp.kchunk = kchunk;
       lp.nchunk = (int)((c->n + kchunk - 1) / kchunk);
+      lp.n_pad = (long)lp.nchunk * kchunk;
+      WS(Px, float2, "g_px", (size_t)lp.n_pad * nx);
+      WS(Py, float2, "g_py", (size_t)lp.n_pad * ny);
+      CK(LAUNCH("k_phase_tables", launch_phase_tables_pad(v, nx, ny, dxs, dys, lp.n_pad, Px, Py, ctx->stream)));
+      lp.Px = Px; lp.Py = Py;
       WS(Bq, uint8_t, "g_i8_b", (size_t)lp.ntile * lp.nchunk * (kchunk / 32) * lateral_i8_stage_bytes(lp.Np));
       WS(sB, double, "g_i8_sb", (size_t)lp.nchunk * ncol);
       WS(fac, double, "g_i8_fac", (size_t)lp.nchunk * ncol);

@@ -60,6 +60,8 @@ struct TransferParams {
 cudaError_t launch_layer_modes(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_layer_modes_qr(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream);
+// k_chain when every observation layer is the source layer
+cudaError_t launch_chain_src(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_rotate_fill(const TransferParams& p, const uint8_t* base_status, const uint8_t* base_tvalid,
                                const double2* Tbase, cudaStream_t stream);
 
@@ -140,8 +142,9 @@ struct LateralI8 {
   int ntile;         // column tiles
   long kchunk;       // nodes per slice: a multiple of 32, ≤ 16384
   int nchunk;        // slices = ceil(n / kchunk)
-  const float2* Px;  // [n][nx]
-  const float2* Py;  // [n][ny]
+  long n_pad;        // nchunk * kchunk: node rows of the phase tables
+  const float2* Px;  // [n_pad][nx], zero beyond n
+  const float2* Py;  // [n_pad][ny]
   const double2* S;  // [ncol][n]
   uint8_t* Bq;       // [ntile][nchunk][kchunk/32][3 planes][Np rows x 64 B] digit images
   double* sB;        // [nchunk][ncol] fixed-point scale of the strengths
@@ -153,6 +156,8 @@ size_t lateral_i8_stage_bytes(int Np);
 size_t lateral_i8_smem(int Np);
 int lateral_i8_ctile(int ncol);
 cudaError_t launch_lateral_i8(const LateralI8& p, cudaStream_t s);
+cudaError_t launch_phase_tables_pad(const CacheView& c, int nx, int ny, const double* xs, const double* ys, long n_pad,
+                                    float2* Px, float2* Py, cudaStream_t s);
 
 // Gauss-Legendre panels -> nodes/weights, bit-exact with the CPU restatement
 cudaError_t launch_gl_nodes(int npanels, const double* pa, const double* pb, const int* sing_side, const double* xi,

@@ -24,7 +24,8 @@
 //   k_bslice : B' digits, written once per launch in the exact shared-memory image of each
 //              32-node stage (3 planes x Np rows x 64 B, canonical K-major core matrices)
 //   k_lateral_i8 : one CTA per (128-pixel tile, column tile, node slice); 8 producer warps
-//              build A' digits from the FP32 phase tables into a 4-deep ring, warp 8 copies
+//              build A' digits from the FP32 phase tables (zero-padded to the slice grid)
+//              into a 4-deep ring, warp 8 copies
 //              each stage's B' image with one bulk copy, one thread of warp 9 issues the
 //              12 MMAs of a stage (6 digit products x 2 K-halves, M=128, N=Np, K=32) and
 //              commits them to the stage's "empty" barrier. At the end all 8 producer warps
@@ -59,6 +60,38 @@ size_t lateral_i8_smem(int Np) {
 int lateral_i8_ctile(int ncol) {
   int ntiles = (ncol + 79) / 80;
   return (ncol + ntiles - 1) / ntiles;
+}
+
+// ------------------------------------------------------------------------------------
+// FP32 phase tables Px[n][i] = e^{i kx_n x_i}, Py[n][j] = e^{i ky_n y_j} (computed in FP64),
+// zero for the padding nodes n <= node < n_pad
+// ------------------------------------------------------------------------------------
+__global__ void k_phase_tables_pad(CacheView c, int nx, int ny, const double* xs, const double* ys, long n_pad,
+                                   float2* Px, float2* Py) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = nx + ny;
+  if (t >= n_pad * (long)m) return;
+  const long nn = t / m;
+  const int e = (int)(t % m);
+  float2 v = make_float2(0.f, 0.f);
+  if (nn < c.n) {
+    const long k = nn % c.Nk, q = nn / c.Nk;
+    double s, co, sn, cs;
+    sincos(c.phi[q], &s, &co);
+    if (e < nx) sincos(c.kr[k] * co * xs[e], &sn, &cs);
+    else sincos(c.kr[k] * s * ys[e - nx], &sn, &cs);
+    v = make_float2((float)cs, (float)sn);
+  }
+  if (e < nx) Px[nn * nx + e] = v;
+  else Py[nn * ny + (e - nx)] = v;
+}
+
+cudaError_t launch_phase_tables_pad(const CacheView& c, int nx, int ny, const double* xs, const double* ys, long n_pad,
+                                    float2* Px, float2* Py, cudaStream_t s) {
+  long tot = n_pad * (long)(nx + ny);
+  if (tot <= 0) return cudaSuccess;
+  k_phase_tables_pad<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(c, nx, ny, xs, ys, n_pad, Px, Py);
+  return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------------------------
@@ -206,22 +239,18 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t ad, uint64_t bd, 
       : "memory");
 }
 
-// the phase operands of one thread for one stage: 16 nodes of one pixel
+// the phase operands of one thread for one stage: 16 nodes of one pixel, from the zero-padded
+// phase tables [n_pad][nx], [n_pad][ny] (no bounds checks: a warp's lanes read consecutive
+// pixels of one node row, so each load is one or two cache lines)
 struct PhaseRegs {
   float2 px[16], py[16];
 };
 
-__device__ __forceinline__ void i8_load(const LateralI8& p, long nbase, long k1, bool pv, int i, int j, PhaseRegs& R) {
+__device__ __forceinline__ void i8_load(const float2* px, const float2* py, long sx, long sy, PhaseRegs& R) {
 #pragma unroll
   for (int q = 0; q < 16; ++q) {
-    const long nn = nbase + q;
-    if (pv && nn < k1) {
-      R.px[q] = __ldg(p.Px + nn * p.nx + i);
-      R.py[q] = __ldg(p.Py + nn * p.ny + j);
-    } else {
-      R.px[q] = make_float2(0.f, 0.f);
-      R.py[q] = make_float2(0.f, 0.f);
-    }
+    R.px[q] = __ldg(px + q * sx);
+    R.py[q] = __ldg(py + q * sy);
   }
 }
 
@@ -270,18 +299,22 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
 
   if (warp < I8_PRODUCERS / 32) {
     // ---------------- producers: A' digits ----------------
+    // pixel r of the tile, nodes 16h..16h+15 of each stage; a pixel beyond npix reads pixel 0
+    // (its output row is never stored, and each A' row only reaches its own output row)
     const int r = tid & 127, h = tid >> 7;
     const long pix = p0 + r;
     const bool pv = pix < p.npix;
     const int i = pv ? (int)(pix % p.nx) : 0, j = pv ? (int)(pix / p.nx) : 0;
-    PhaseRegs cur, nxt;
-    if (nst > 0) i8_load(p, k0 + 16 * h, k1, pv, i, j, cur);
-    for (int s = 0; s < nst; ++s) {
+    const long sx = p.nx, sy = p.ny;
+    const float2* pxb = p.Px + (k0 + 16 * h) * sx + i;
+    const float2* pyb = p.Py + (k0 + 16 * h) * sy + j;
+    // one stage from `use` while `pre` receives the next stage's loads; false = give up
+    auto stage = [&](int s, PhaseRegs& use, PhaseRegs& pre) -> bool {
       const int slot = s % I8_STAGES;
-      if (s + 1 < nst) i8_load(p, k0 + (long)(s + 1) * I8_NODES + 16 * h, k1, pv, i, j, nxt);
+      if (s + 1 < nst) i8_load(pxb + (s + 1) * I8_NODES * sx, pyb + (s + 1) * I8_NODES * sy, sx, sy, pre);
       bool ok = true;
       if (s >= I8_STAGES) ok = i8_wait(smem_u32(&sh->empty[slot]), ((s / I8_STAGES) - 1) & 1, abort_flag, p.err);
-      if (!__all_sync(0xffffffffu, ok)) break;
+      if (!__all_sync(0xffffffffu, ok)) return false;
       uint8_t* A = smA + slot * stageA;
 #pragma unroll
       for (int half = 0; half < 2; ++half) {
@@ -292,8 +325,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
           uint32_t u0[2], u1[2], u2[2];
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
-            const int q = 8 * half + 2 * wd + e;
-            const float2 a = cur.px[q], b = cur.py[q];
+            const float2 a = use.px[8 * half + 2 * wd + e], b = use.py[8 * half + 2 * wd + e];
             const float re = fmaf(a.x, b.x, -a.y * b.y), im = fmaf(a.x, b.y, a.y * b.x);
             const uint32_t xr = fx_bits(re), xi = fx_bits(im);
             // digit bytes: d2 = byte 0 of X, d1 = byte 1 of X + 128, d0 = byte 2 of X + 32896
@@ -314,7 +346,13 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&sh->full_a[slot]));
-      cur = nxt;
+      return true;
+    };
+    PhaseRegs ra, rb;
+    if (nst > 0) i8_load(pxb, pyb, sx, sy, ra);
+    for (int s = 0; s < nst; s += 2) {
+      if (!stage(s, ra, rb)) break;
+      if (s + 1 < nst && !stage(s + 1, rb, ra)) break;
     }
   } else if (warp == 8) {
     // ---------------- bulk copies of the prepared B' stage images ----------------
@@ -409,7 +447,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
 cudaError_t launch_lateral_i8(const LateralI8& p, cudaStream_t s) {
   if (p.npix <= 0 || p.ncol <= 0 || p.n <= 0) return cudaSuccess;
   if (p.kchunk % I8_NODES != 0 || p.kchunk > 16384 || p.Np % 16 != 0 || p.Np > I8_ACC_STRIDE || p.Np < 2 * p.ctile ||
-      (long)p.nchunk * p.kchunk < p.n)
+      p.n_pad != (long)p.nchunk * p.kchunk || p.n_pad < p.n)
     return cudaErrorInvalidValue;
   {
     dim3 g((unsigned)p.ncol, (unsigned)p.nchunk);

@@ -541,31 +541,55 @@ __device__ __forceinline__ void match_dir(const cd wa_src[4][2], cd vb[4][2], cd
   }
 }
 
-// 4x4 LU solve with partial pivoting, NR right-hand sides; false on an exact zero pivot
+// 4x4 LU solve with partial pivoting, NR right-hand sides; false on an exact zero pivot.
+// Every array index is a compile-time constant (the pivot row swap is a predicated exchange
+// with each candidate row), so the matrices stay in registers.
 template <int NR>
 __device__ __forceinline__ bool lu_solve4(cd A[4][4], cd B[4][NR]) {
+  bool ok = true;
+#pragma unroll
   for (int k = 0; k < 4; ++k) {
     int pv = k;
     double best = norm2(A[k][k]);
+#pragma unroll
     for (int i = k + 1; i < 4; ++i) {
       double v = norm2(A[i][k]);
       if (v > best) { best = v; pv = i; }
     }
-    if (best == 0.0) return false;
-    if (pv != k) {
-      for (int j = 0; j < 4; ++j) { cd t = A[pv][j]; A[pv][j] = A[k][j]; A[k][j] = t; }
-      for (int j = 0; j < NR; ++j) { cd t = B[pv][j]; B[pv][j] = B[k][j]; B[k][j] = t; }
-    }
-    cd piv = recip(A[k][k]);
+    if (best == 0.0) ok = false;
+#pragma unroll
     for (int i = k + 1; i < 4; ++i) {
-      cd l = A[i][k] * piv;
+      const bool sw = pv == i;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const cd t = A[i][j];
+        A[i][j] = sw ? A[k][j] : t;
+        A[k][j] = sw ? t : A[k][j];
+      }
+#pragma unroll
+      for (int j = 0; j < NR; ++j) {
+        const cd t = B[i][j];
+        B[i][j] = sw ? B[k][j] : t;
+        B[k][j] = sw ? t : B[k][j];
+      }
+    }
+    const cd piv = recip(A[k][k]);
+#pragma unroll
+    for (int i = k + 1; i < 4; ++i) {
+      const cd l = A[i][k] * piv;
+#pragma unroll
       for (int j = k + 1; j < 4; ++j) A[i][j] -= l * A[k][j];
+#pragma unroll
       for (int j = 0; j < NR; ++j) B[i][j] -= l * B[k][j];
     }
   }
+  if (!ok) return false;
+#pragma unroll
   for (int j = 0; j < NR; ++j)
+#pragma unroll
     for (int i = 3; i >= 0; --i) {
       cd s = B[i][j];
+#pragma unroll
       for (int k = i + 1; k < 4; ++k) s -= A[i][k] * B[k][j];
       B[i][j] = s / A[i][i];
     }
@@ -897,6 +921,204 @@ __global__ void __launch_bounds__(128) k_chain(TransferParams p) {
 }
 
 // ------------------------------------------------------------------------------------
+// K2': the same solve when every observation layer is the source layer (needL = needR = 0):
+// no walk to other layers, so SRight is needed at the source layer only. The Redheffer
+// product is associative, so SRight[src] = eff_src ⋆ eff_src+1 ⋆ … ⋆ eff_N-1 accumulates in
+// the forward sweep (left to right) instead of a backward scan over stored interface
+// matrices: N-1 star products instead of N-1 + (N-src), and no interface, SRight or
+// matched-mode records written. One S4 register set serves as the SLeft prefix up to the
+// source layer and as the SRight product after it. The mode vectors of a layer are read
+// from the (read-only) mode records with its matching swaps applied instead of being held
+// across iterations.
+// ------------------------------------------------------------------------------------
+struct ModeV {  // one layer's mode vectors: Vf, Vb (4x2)
+  cd vf[4][2], vb[4][2];
+};
+
+__device__ __forceinline__ void load_v(const TransferParams& p, int layer, long node, uint32_t swaps, ModeV& M) {
+  const double2* rec = p.modes + (long)layer * 20 * p.n;
+  const int sf = (swaps >> (2 * layer)) & 1, sb = (swaps >> (2 * layer + 1)) & 1;
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      M.vf[i][m] = ld(rec, i + 4 * (m ^ sf), p.n, node);
+      M.vb[i][m] = ld(rec, 8 + i + 4 * (m ^ sb), p.n, node);
+    }
+}
+__device__ __forceinline__ void load_q(const TransferParams& p, int layer, long node, uint32_t swaps, cd qf[2], cd qb[2]) {
+  const double2* rec = p.modes + (long)layer * 20 * p.n;
+  const int sf = (swaps >> (2 * layer)) & 1, sb = (swaps >> (2 * layer + 1)) & 1;
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    qf[m] = ld(rec, 16 + (m ^ sf), p.n, node);
+    qb[m] = ld(rec, 18 + (m ^ sb), p.n, node);
+  }
+}
+__device__ __forceinline__ void load_matched(const TransferParams& p, int layer, long node, uint32_t swaps, Mode4& M) {
+  ModeV v;
+  load_v(p, layer, node, swaps, v);
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int m = 0; m < 2; ++m) { M.vf[i][m] = v.vf[i][m]; M.vb[i][m] = v.vb[i][m]; }
+  load_q(p, layer, node, swaps, M.qf, M.qb);
+}
+// _match_modes (mod_ModeSolver.jl:333-349) for one direction: true if b's columns swap
+__device__ __forceinline__ bool match_swap(const cd va[4][2], const cd vb[4][2]) {
+  cd C[2][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      cd s = conj(Wof(va, 0, a)) * vb[0][b];
+#pragma unroll
+      for (int i = 1; i < 4; ++i) s += conj(Wof(va, i, a)) * vb[i][b];
+      C[a][b] = s;
+    }
+  return norm2(C[0][1]) + norm2(C[1][0]) > norm2(C[0][0]) + norm2(C[1][1]);
+}
+
+__global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
+  long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long n = p.n;
+  if (node >= n) return;
+  const int N = p.nL, src = p.src;
+  const bool base = p.mode == 2;
+  const long nT = base ? n : p.nout;
+  const long gnode = base ? node : p.off + node;
+  uint8_t stat = 0;
+  for (int l = 0; l < N; ++l) stat |= p.lstat[(long)l * n + node];
+  double kx, ky;
+  node_k(p, p.off + node, kx, ky);
+  const cd z{0.0, 0.0};
+  if (!base) p.valid[gnode] = 0;
+  for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * nT + gnode] = 0;
+  if (stat & (ST_EIGEN | ST_SORT)) {
+    p.status[gnode] = stat;
+    return;
+  }
+  uint32_t swaps = 0;  // bit 2l: forward columns of layer l swapped by matching, bit 2l+1: backward
+  bool seeds_ok = true, seeds_fin = true;
+  auto seeds_and_basis = [&](int layer) {  // layer 0-based, the source layer
+    if (base) return;
+    Mode4 M;
+    load_matched(p, layer, node, swaps, M);
+    cd sif[2][3], sib[2][3];
+    seeds_ok = source_projection(kx, ky, p.omega, p.layers[layer], M, sif, sib);
+    for (int m = 0; m < 2; ++m)
+      for (int q = 0; q < 3; ++q) seeds_fin = seeds_fin && isfin(sif[m][q]) && isfin(sib[m][q]);
+    write_seeds(p, gnode, p.nout, M, sif, sib);
+    for (int oi = 0; oi < p.nobs; ++oi) write_basis(p, oi, gnode, p.nout, p.layers[layer], M, kx, ky);
+  };
+  cd Qs[4];  // Qf0 Qf1 Qb0 Qb1 of the source layer
+  M2 RL = M2{z, z, z, z};
+  S4 acc;
+  {
+    cd qf[2], qb[2];
+    load_q(p, 0, node, 0u, qf, qb);
+    const double d0 = p.layers[0].d;
+    if (src == 1) {
+      Qs[0] = qf[0]; Qs[1] = qf[1]; Qs[2] = qb[0]; Qs[3] = qb[1];
+      acc = s4_identity();
+      seeds_and_basis(0);
+    } else {
+      acc = s4_diag(expi(qf[0], d0), expi(qf[1], d0), expi(-qb[0], d0), expi(-qb[1], d0));
+    }
+  }
+  for (int j = 2; j <= N; ++j) {
+    const int a = j - 2, b = j - 1;  // 0-based layers on either side of interface j-1|j
+    S4 Si;
+    {
+      ModeV va, vb;
+      load_v(p, a, node, swaps, va);
+      load_v(p, b, node, 0u, vb);
+      const bool sf = match_swap(va.vf, vb.vf), sb = match_swap(va.vb, vb.vb);
+      swaps |= (sf ? 1u : 0u) << (2 * b) | (sb ? 1u : 0u) << (2 * b + 1);
+      Mode4 A, B;
+      for (int i = 0; i < 4; ++i)
+        for (int m = 0; m < 2; ++m) {
+          A.vf[i][m] = va.vf[i][m]; A.vb[i][m] = va.vb[i][m];
+          B.vf[i][m] = sf ? vb.vf[i][1 - m] : vb.vf[i][m];
+          B.vb[i][m] = sb ? vb.vb[i][1 - m] : vb.vb[i][m];
+        }
+      if (!interface_matrix(A, B, Si)) stat |= ST_SINGULAR;
+    }
+    if (j <= src) {
+      const S4 SL = redheffer(acc, Si);
+      cd qf[2], qb[2];
+      load_q(p, b, node, swaps, qf, qb);
+      if (j == src) {
+        RL = SL.b12;
+        Qs[0] = qf[0]; Qs[1] = qf[1]; Qs[2] = qb[0]; Qs[3] = qb[1];
+        acc = s4_identity();
+        seeds_and_basis(b);
+      } else {
+        const double d = p.layers[b].d;
+        const cd pf0 = expi(qf[0], d), pf1 = expi(qf[1], d), pb0 = expi(-qb[0], d), pb1 = expi(-qb[1], d);
+        acc.b11 = dl(pf0, pf1, SL.b11);
+        acc.b12 = dl(pf0, pf1, dr(SL.b12, pb0, pb1));
+        acc.b21 = SL.b21;
+        acc.b22 = dr(SL.b22, pb0, pb1);
+      }
+    } else {
+      // layer k = a+1 (1-based) >= src: eff = diag(e^{iQf d}, e^{-iQb d}) of layer k ⋆ Sint[k]
+      cd qf[2], qb[2];
+      load_q(p, a, node, swaps, qf, qb);
+      const double d = p.layers[a].d;
+      const S4 eff = redheffer_diag_left(expi(qf[0], d), expi(qf[1], d), expi(-qb[0], d), expi(-qb[1], d), Si);
+      acc = redheffer(acc, eff);
+    }
+  }
+  if (stat & ST_SINGULAR) {
+    p.status[gnode] = stat;
+    return;
+  }
+  // cavity at the source layer (_R_cavity, _cavity_resummation), as k_chain
+  const double ds = p.layers[src - 1].d;
+  M2 RR = M2{z, z, z, z};
+  M24 Fp, Fm;
+  const M2 I2 = M2{cd{1, 0}, z, z, cd{1, 0}}, Z2 = M2{z, z, z, z};
+  if (src < N) {
+    const S4 RRr = redheffer_diag_left(expi(Qs[0], -ds), expi(Qs[1], -ds), expi(Qs[2], ds), expi(Qs[3], ds), acc);
+    RR = RRr.b21;
+    const cd PF0 = expi(Qs[0], ds), PF1 = expi(Qs[1], ds), PB0 = expi(Qs[2], -ds), PB1 = expi(Qs[3], -ds);
+    const M2 Mx = mul(dr(dl(PF0, PF1, RL), PB0, PB1), RR);
+    const M2 D = imin(Mx);
+    Fp.L = solve(D, I2);
+    Fp.R = solve(D, dl(PF0, PF1, RL));
+    Fm.L = dl(PB0, PB1, mul(RR, Fp.L));
+    Fm.R = add(I2, dl(PB0, PB1, mul(RR, Fp.R)));
+  } else {
+    Fp = M24{Z2, Z2};
+    Fm = M24{Z2, I2};
+  }
+  // T^o of the source layer: Ef = RL F⁻, Eb = RR F⁺ (the same for every listed obs index)
+  const M24 Ef = mul24(RL, Fm), Eb = mul24(RR, Fp);
+  const bool fin = fin2(Ef.L) && fin2(Ef.R) && fin2(Eb.L) && fin2(Eb.R);
+  for (int oi = 0; oi < p.nobs; ++oi) {
+    if (fin) write_T(p, oi, gnode, nT, Ef, Eb);
+    else write_T(p, oi, gnode, nT, M24{Z2, Z2}, M24{Z2, Z2});
+    p.tvalid[(long)oi * nT + gnode] = fin ? 1 : 0;
+  }
+  if (!fin && p.nobs > 0) stat |= ST_TNONFINITE;
+  if (!base) {
+    if (!seeds_ok) stat |= ST_SINGULAR;
+    if (!(seeds_ok && seeds_fin)) {
+      stat |= ST_SEEDS;
+      for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * p.nout + gnode] = 0;
+      p.valid[gnode] = 0;
+    } else {
+      p.valid[gnode] = 1;
+      stat |= ST_VALID;
+    }
+  } else {
+    stat |= ST_VALID;
+  }
+  p.status[gnode] = stat;
+}
+
+// ------------------------------------------------------------------------------------
 // K3: rotation fill of an azimuthally symmetric 2D grid (mod_CavityTransfer.jl:361-378)
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_rotate_fill(TransferParams p, const uint8_t* base_status, const uint8_t* base_tvalid,
@@ -963,6 +1185,12 @@ cudaError_t launch_layer_modes_qr(const TransferParams& p, cudaStream_t stream) 
   long tot = (long)p.n * p.nL;
   if (tot <= 0) return cudaSuccess;
   k_layer_modes_qr<<<(unsigned)((tot + 127) / 128), 128, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chain_src(const TransferParams& p, cudaStream_t stream) {
+  if (p.n <= 0) return cudaSuccess;
+  k_chain_src<<<(unsigned)((p.n + 127) / 128), 128, 0, stream>>>(p);
   return cudaGetLastError();
 }
 
