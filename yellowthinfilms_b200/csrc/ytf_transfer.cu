@@ -1021,14 +1021,15 @@ __global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
     if (src == 1) {
       Qs[0] = qf[0]; Qs[1] = qf[1]; Qs[2] = qb[0]; Qs[3] = qb[1];
       acc = s4_identity();
-      seeds_and_basis(0);
     } else {
       acc = s4_diag(expi(qf[0], d0), expi(qf[1], d0), expi(-qb[0], d0), expi(-qb[1], d0));
     }
   }
+  // one star product per interface: up to the source layer acc = SLeft ⋆ Sint, then the
+  // propagation of the next layer on the right; after it acc ⋆ (diag(prop of layer j-1) ⋆ Sint)
   for (int j = 2; j <= N; ++j) {
     const int a = j - 2, b = j - 1;  // 0-based layers on either side of interface j-1|j
-    S4 Si;
+    S4 X;
     {
       ModeV va, vb;
       load_v(p, a, node, swaps, va);
@@ -1042,34 +1043,29 @@ __global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
           B.vf[i][m] = sf ? vb.vf[i][1 - m] : vb.vf[i][m];
           B.vb[i][m] = sb ? vb.vb[i][1 - m] : vb.vb[i][m];
         }
-      if (!interface_matrix(A, B, Si)) stat |= ST_SINGULAR;
+      if (!interface_matrix(A, B, X)) stat |= ST_SINGULAR;
     }
-    if (j <= src) {
-      const S4 SL = redheffer(acc, Si);
-      cd qf[2], qb[2];
-      load_q(p, b, node, swaps, qf, qb);
-      if (j == src) {
-        RL = SL.b12;
-        Qs[0] = qf[0]; Qs[1] = qf[1]; Qs[2] = qb[0]; Qs[3] = qb[1];
-        acc = s4_identity();
-        seeds_and_basis(b);
-      } else {
-        const double d = p.layers[b].d;
-        const cd pf0 = expi(qf[0], d), pf1 = expi(qf[1], d), pb0 = expi(-qb[0], d), pb1 = expi(-qb[1], d);
-        acc.b11 = dl(pf0, pf1, SL.b11);
-        acc.b12 = dl(pf0, pf1, dr(SL.b12, pb0, pb1));
-        acc.b21 = SL.b21;
-        acc.b22 = dr(SL.b22, pb0, pb1);
-      }
+    const bool left = j <= src;
+    cd qf[2], qb[2];
+    load_q(p, left ? b : a, node, swaps, qf, qb);
+    const double d = p.layers[left ? b : a].d;
+    const cd pf0 = expi(qf[0], d), pf1 = expi(qf[1], d), pb0 = expi(-qb[0], d), pb1 = expi(-qb[1], d);
+    if (!left) X = redheffer_diag_left(pf0, pf1, pb0, pb1, X);
+    const S4 R = redheffer(acc, X);
+    if (!left) {
+      acc = R;
+    } else if (j == src) {
+      RL = R.b12;
+      Qs[0] = qf[0]; Qs[1] = qf[1]; Qs[2] = qb[0]; Qs[3] = qb[1];
+      acc = s4_identity();
     } else {
-      // layer k = a+1 (1-based) >= src: eff = diag(e^{iQf d}, e^{-iQb d}) of layer k ⋆ Sint[k]
-      cd qf[2], qb[2];
-      load_q(p, a, node, swaps, qf, qb);
-      const double d = p.layers[a].d;
-      const S4 eff = redheffer_diag_left(expi(qf[0], d), expi(qf[1], d), expi(-qb[0], d), expi(-qb[1], d), Si);
-      acc = redheffer(acc, eff);
+      acc.b11 = dl(pf0, pf1, R.b11);
+      acc.b12 = dl(pf0, pf1, dr(R.b12, pb0, pb1));
+      acc.b21 = R.b21;
+      acc.b22 = dr(R.b22, pb0, pb1);
     }
   }
+  seeds_and_basis(src - 1);
   if (stat & ST_SINGULAR) {
     p.status[gnode] = stat;
     return;
