@@ -758,7 +758,6 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
   } else {
     int ncol = 9 * nz;
     WS(S, double2, "g_S", (size_t)ncol * c->n);
-    CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream)));
     if (precision == YTF_PREC_INT8X3) {
       // int8 tensor cores: FP32 phase tables, fixed-point digits, exact INT32 accumulation,
       // FP64 reduction of the node slices
@@ -783,11 +782,12 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
       CK(LAUNCH("k_phase_tables", launch_phase_tables_pad(v, nx, ny, dxs, dys, lp.n_pad, Px, Py, ctx->stream)));
       lp.Px = Px; lp.Py = Py;
       WS(Bq, uint8_t, "g_i8_b", (size_t)lp.ntile * lp.nchunk * (kchunk / 32) * lateral_i8_stage_bytes(lp.Np));
-      WS(sB, double, "g_i8_sb", (size_t)lp.nchunk * ncol);
-      WS(fac, double, "g_i8_fac", (size_t)lp.nchunk * ncol);
+      WS(cmax, unsigned long long, "g_i8_cmax", (size_t)lp.nchunk * ncol);
+      CK(cudaMemsetAsync(cmax, 0, sizeof(unsigned long long) * lp.nchunk * ncol, ctx->stream));
+      CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream, cmax, kchunk)));
       WS(Gp, double2, "g_partial2", (size_t)lp.nchunk * npix * ncol);
       WS(err, unsigned, "g_tc_err", 1);
-      lp.Bq = Bq; lp.sB = sB; lp.fac = fac; lp.partial = Gp; lp.err = err;
+      lp.Bq = Bq; lp.colmax = cmax; lp.partial = Gp; lp.err = err;
       CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
       CK(LAUNCH("k_lateral_i8", launch_lateral_i8(lp, ctx->stream)));
       CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, lp.nchunk, Gp, G, ctx->stream)));
@@ -800,6 +800,7 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
       prof_collect(ctx);
       return YTF_OK;
     }
+    CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream)));
     if (precision == YTF_PREC_SPLIT_BF16) {
       // tensor cores: FP32 phase tables, split-BF16 contraction, FP64 reduction of the slices
       WS(Px, float2, "g_px", (size_t)c->n * nx);

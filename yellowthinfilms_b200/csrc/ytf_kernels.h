@@ -107,7 +107,9 @@ cudaError_t launch_reduce_splits(long len, int splits, const double* partial, do
 cudaError_t launch_assemble1d(int nx, int ny, int nz, const double* xs, const double* ys, const int* rmap, int nr,
                               const double* P0, const double* P1, const double* P2, double2* G, cudaStream_t s);
 // 2D direct lateral synthesis
-cudaError_t launch_strengths2d(const SynthParams& p, double2* S, cudaStream_t s);
+// colmax (optional, zeroed by the caller): [n / kchunk][9 nz] IEEE bits of max(|Re|, |Im|)
+cudaError_t launch_strengths2d(const SynthParams& p, double2* S, cudaStream_t s, unsigned long long* colmax = nullptr,
+                               long kchunk = 0);
 int lateral_splits(long n, int splits);  // effective split count of launch_lateral
 cudaError_t launch_lateral(const CacheView& c, int nx, int ny, const double* xs, const double* ys, int ncol, const double2* S,
                            double2* partial, int splits, cudaStream_t s);
@@ -147,8 +149,7 @@ struct LateralI8 {
   const float2* Py;  // [n_pad][ny]
   const double2* S;  // [ncol][n]
   uint8_t* Bq;       // [ntile][nchunk][kchunk/32][3 planes][Np rows x 64 B] digit images
-  double* sB;        // [nchunk][ncol] fixed-point scale of the strengths
-  double* fac;       // [nchunk][ncol] output factor 2^16 / (sA sB)
+  const unsigned long long* colmax;  // [nchunk][ncol] bits of max(|Re S|, |Im S|) (k_strengths2d)
   double2* partial;  // [nchunk][npix * ncol]
   unsigned* err;     // nonzero if a pipeline wait timed out
 };

@@ -20,7 +20,7 @@
 // host keeps each CTA's node slice ≤ 16384 nodes (K ≤ 32768 real terms), so |acc| < 1.4e9.
 //
 // Kernels:
-//   k_bscale : per (node slice, column) max|S| -> sB and the output factor
+//   (k_strengths2d reduces max|S| per (node slice, column) while it writes S)
 //   k_bslice : B' digits, written once per launch in the exact shared-memory image of each
 //              32-node stage (3 planes x Np rows x 64 B, canonical K-major core matrices)
 //   k_lateral_i8 : one CTA per (128-pixel tile, column tile, node slice); 8 producer warps
@@ -97,47 +97,18 @@ cudaError_t launch_phase_tables_pad(const CacheView& c, int nx, int ny, const do
 // ------------------------------------------------------------------------------------
 // B' preparation
 // ------------------------------------------------------------------------------------
-__global__ void k_bscale(LateralI8 p) {
-  const int col = blockIdx.x, z = blockIdx.y;
-  const long k0 = (long)z * p.kchunk, k1 = min(p.n, k0 + p.kchunk);
-  const double2* s = p.S + (long)col * p.n;
-  double m = 0.0;
-  bool fin = true;
-  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-    const double2 v = s[k];
-    fin = fin && isfinite(v.x) && isfinite(v.y);
-    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
-  }
-  __shared__ double red[256];
-  __shared__ int redf[256];
-  red[threadIdx.x] = m;
-  redf[threadIdx.x] = fin ? 1 : 0;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) {
-      red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
-      redf[threadIdx.x] &= redf[threadIdx.x + w];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    const long o = (long)z * p.ncol + col;
-    m = red[0];
-    if (!redf[0]) {
-      // a non-finite strength poisons its column, as the FP64 contraction would
-      p.sB[o] = 0.0;
-      p.fac[o] = __longlong_as_double(0x7ff8000000000000LL);
-    } else if (m > 0.0) {
-      // |S sB| ≤ 8355000 (one rounding of the product above it is still below 8355000.5), so
-      // the top digit (Y + 32896) >> 16 stays in [-127, 127]
-      const double sB = 8355000.0 / m;
-      p.sB[o] = sB;
-      p.fac[o] = 65536.0 / ((double)I8_SA * sB);
-    } else {
-      p.sB[o] = 0.0;
-      p.fac[o] = 0.0;
-    }
-  }
+// fixed-point scale of one (node slice, column) of strengths from its max(|Re|, |Im|):
+// |S sB| ≤ 8355000 (one rounding of the product above it is still below 8355000.5), so the
+// top digit (Y + 32896) >> 16 stays in [-127, 127]. 0 for an all-zero column; a non-finite
+// maximum poisons the column's output (fac = NaN), as the FP64 contraction would.
+__device__ __forceinline__ double slice_scale(unsigned long long bits) {
+  const double m = __longlong_as_double((long long)bits);
+  return (m > 0.0 && isfinite(m)) ? 8355000.0 / m : 0.0;
+}
+__device__ __forceinline__ double slice_factor(unsigned long long bits) {
+  const double m = __longlong_as_double((long long)bits);
+  if (!isfinite(m)) return __longlong_as_double(0x7ff8000000000000LL);
+  return m > 0.0 ? 65536.0 / ((double)I8_SA * slice_scale(bits)) : 0.0;
 }
 
 // three signed base-256 digits of Y (|Y| ≤ 8355000), most significant first, as bytes
@@ -164,7 +135,7 @@ __global__ void k_bslice(LateralI8 p) {
   const int col = ct * p.ctile + cl;
   const bool cv = cl < p.ctile && col < p.ncol;
   const long o = (long)z * p.ncol + (cv ? col : 0);
-  const double sB = cv ? p.sB[o] : 0.0;
+  const double sB = cv ? slice_scale(p.colmax[o]) : 0.0;
   const long nstage = p.kchunk / I8_NODES;
   const int s = (int)(g / 4), kb = (int)(g % 4) * 16;
   uint32_t w[2][3][4];  // [row re/im][plane][word]
@@ -415,7 +386,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
       const uint32_t lanebase = (uint32_t)(32 * q) << 16;
       const long pix = p0 + 32 * q + lane;
       double2* out = p.partial + (long)z * p.npix * p.ncol;
-      const double* fac = p.fac + (long)z * p.ncol;
+      const unsigned long long* cmax = p.colmax + (long)z * p.ncol;
       for (int e0 = 0; e0 < half; e0 += 8) {
         uint32_t v0[8], v1[8], v2[8];
         const uint32_t col = (uint32_t)(hh * half + e0);
@@ -431,7 +402,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
                 (long long)(int)v0[e] * 65536 + (long long)(int)v1[e] * 256 + (long long)(int)v2[e];
             const long long im =
                 (long long)(int)v0[e + 1] * 65536 + (long long)(int)v1[e + 1] * 256 + (long long)(int)v2[e + 1];
-            const double f = fac[c0 + cc];
+            const double f = slice_factor(cmax[c0 + cc]);
             out[pix + p.npix * (long)(c0 + cc)] = make_double2((double)re * f, (double)im * f);
           }
         }
@@ -449,12 +420,6 @@ cudaError_t launch_lateral_i8(const LateralI8& p, cudaStream_t s) {
   if (p.kchunk % I8_NODES != 0 || p.kchunk > 16384 || p.Np % 16 != 0 || p.Np > I8_ACC_STRIDE || p.Np < 2 * p.ctile ||
       p.n_pad != (long)p.nchunk * p.kchunk || p.n_pad < p.n)
     return cudaErrorInvalidValue;
-  {
-    dim3 g((unsigned)p.ncol, (unsigned)p.nchunk);
-    k_bscale<<<g, 256, 0, s>>>(p);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
   {
     const long total = (long)p.ntile * (p.Np / 2) * p.nchunk * (p.kchunk / 8);
     k_bslice<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p);

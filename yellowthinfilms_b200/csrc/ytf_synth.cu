@@ -342,48 +342,84 @@ cudaError_t launch_assemble1d(int nx, int ny, int nz, const double* xs, const do
 
 // ------------------------------------------------------------------------------------
 // 2D strengths per (node, z-row): S[col'][n], col' = zi + nz (c + 3q)
+// One thread per (node, group of SG_Z z-rows): the reflected amplitudes (z-independent) and
+// the mode basis are formed once per group. With `colmax` set, the kernel also reduces
+// max(|Re S|, |Im S|) over each (node slice of `kchunk` nodes, column): a warp max (a warp's
+// 32 nodes lie in one slice, kchunk being a multiple of 32) and one atomicMax per warp on
+// the IEEE bits, which order like the values for non-negative doubles (Inf/NaN sort above
+// every finite value, so a non-finite strength shows in the slice's maximum).
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_strengths2d(SynthParams p, double2* S) {
-  long nidx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  int zi = blockIdx.y;
+constexpr int SG_Z = 2;  // z-rows per thread
+
+__global__ void __launch_bounds__(128) k_strengths2d(SynthParams p, double2* S, unsigned long long* colmax, long kchunk) {
+  const long nidx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const CacheView& c = p.c;
-  if (nidx >= c.n) return;
   const long n = c.n;
-  long k = nidx % c.Nk, pp = nidx / c.Nk;
+  const bool live = nidx < n;
+  const long node = live ? nidx : n - 1;
+  const long k = node % c.Nk, pp = node / c.Nk;
   const double w = c.kr[k] * c.wr[k] * c.wphi[pp] / (4.0 * 3.14159265358979323846 * 3.14159265358979323846);
   const cd W{w, 0.0};
   cd Af[2][3], Ab[2][3];
-  reflected_amp(p, nidx, Af, Ab);
-  const double z = p.zo[zi];
-  cd Afd[2][3], Abd[2][3];
-  if (p.with_direct) direct_amp(p, nidx, z, Afd, Abd);
-  cd s[3][3];
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) s[a][b] = cd{0, 0};
+  reflected_amp(p, node, Af, Ab);
+  cd kzf[2], kzb[2], ef[2][3], eb[2][3];
+#pragma unroll
   for (int m = 0; m < 2; ++m) {
-    cd pf = phase_cl(ldc(c.basis, 12 + m, n, nidx), z);
-    cd pb = phase_cl(ldc(c.basis, 14 + m, n, nidx), z - p.d_obs);
-    cd exf = ldc(c.basis, 0 + m, n, nidx), eyf = ldc(c.basis, 2 + m, n, nidx), ezf = ldc(c.basis, 4 + m, n, nidx);
-    cd exb = ldc(c.basis, 6 + m, n, nidx), eyb = ldc(c.basis, 8 + m, n, nidx), ezb = ldc(c.basis, 10 + m, n, nidx);
-    for (int q = 0; q < 3; ++q) {
-      cd tf = Af[m][q] * pf, tb = Ab[m][q] * pb;
-      if (p.with_direct) { tf += Afd[m][q]; tb += Abd[m][q]; }
-      cd af = fin0(W * tf), ab = fin0(W * tb);
-      s[0][q] += exf * af + exb * ab;
-      s[1][q] += eyf * af + eyb * ab;
-      s[2][q] += ezf * af + ezb * ab;
+    kzf[m] = ldc(c.basis, 12 + m, n, node);
+    kzb[m] = ldc(c.basis, 14 + m, n, node);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      ef[m][a] = ldc(c.basis, 2 * a + m, n, node);
+      eb[m][a] = ldc(c.basis, 6 + 2 * a + m, n, node);
     }
   }
-  for (int q = 0; q < 3; ++q)
-    for (int cc = 0; cc < 3; ++cc) {
-      long col = zi + (long)p.nz * (cc + 3 * q);
-      S[col * n + nidx] = make_double2(s[cc][q].x, s[cc][q].y);
+  const int z0 = blockIdx.y * SG_Z, z1 = min(p.nz, z0 + SG_Z);
+  for (int zi = z0; zi < z1; ++zi) {
+    const double z = p.zo[zi];
+    cd Afd[2][3], Abd[2][3];
+    if (p.with_direct) direct_amp(p, node, z, Afd, Abd);
+    cd s[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) s[a][b] = cd{0, 0};
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const cd pf = phase_cl(kzf[m], z);
+      const cd pb = phase_cl(kzb[m], z - p.d_obs);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        cd tf = Af[m][q] * pf, tb = Ab[m][q] * pb;
+        if (p.with_direct) { tf += Afd[m][q]; tb += Abd[m][q]; }
+        const cd af = fin0(W * tf), ab = fin0(W * tb);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) s[a][q] += ef[m][a] * af + eb[m][a] * ab;
+      }
     }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        const long col = zi + (long)p.nz * (cc + 3 * q);
+        if (live) S[col * n + nidx] = make_double2(s[cc][q].x, s[cc][q].y);
+        if (colmax) {
+          double m = live ? fmax(fabs(s[cc][q].x), fabs(s[cc][q].y)) : 0.0;
+          if (live && !(isfinite(s[cc][q].x) && isfinite(s[cc][q].y))) m = __longlong_as_double(0x7ff0000000000000LL);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+          // fmax drops a NaN operand; Inf (set above for any non-finite entry) survives
+          if ((threadIdx.x & 31) == 0 && live)
+            atomicMax(colmax + (nidx / kchunk) * (long)(9 * p.nz) + col, (unsigned long long)__double_as_longlong(m));
+        }
+      }
+  }
 }
 
-cudaError_t launch_strengths2d(const SynthParams& p, double2* S, cudaStream_t s) {
-  dim3 grid((unsigned)((p.c.n + 127) / 128), (unsigned)p.nz);
-  k_strengths2d<<<grid, 128, 0, s>>>(p, S);
+cudaError_t launch_strengths2d(const SynthParams& p, double2* S, cudaStream_t s, unsigned long long* colmax, long kchunk) {
+  if (p.c.n <= 0) return cudaSuccess;
+  if (colmax && (kchunk <= 0 || kchunk % 32 != 0)) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((p.c.n + 127) / 128), (unsigned)((p.nz + SG_Z - 1) / SG_Z));
+  k_strengths2d<<<grid, 128, 0, s>>>(p, S, colmax, kchunk);
   return cudaGetLastError();
 }
 
