@@ -208,7 +208,7 @@ def measured_peaks():
 
 # FP64 operations per node of the per-node solve kernels on this workload, from one ncu count
 # of their DFMA/DADD/DMUL instructions (2 per DFMA); None until captured
-FP64_OPS_PER_NODE = {}
+FP64_OPS_PER_NODE = {"k_chain_src": 31.7e3}  # 7.95e8 DFMA + 1.80e8 DADD + 3.10e8 DMUL per 65536-node launch
 FP64_NOMINAL = 37.2  # TFLOP/s: 148 SM x 64 FP64 FMA/clk x 2 x 1.965 GHz (no measured FP64 peak)
 
 
