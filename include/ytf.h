@@ -101,6 +101,54 @@ int ytf_cache_status(ytf_ctx* ctx, const ytf_cache* cache, unsigned char* valid,
 int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* cache, double* T, double* Qf, double* Qb, double* sf, double* sb,
                      double* basis);
 
+/* One problem of a batched transfer build: the arguments of build_cavity_transfer_1d
+ * (is2d = 0: k_nodes/k_weights are kx nodes and weights, check_symmetry applies) or of
+ * build_cavity_transfer_2d (is2d = 1 or nphi > 0: kρ nodes/weights and φ nodes/weights,
+ * rotation applies). */
+typedef struct {
+  const ytf_stack* stack;
+  double omega;
+  int source_layer;
+  int nk;
+  const double* k_nodes;
+  const double* k_weights;
+  int nphi;
+  const double* phi_nodes;
+  const double* phi_weights;
+  int nobs;
+  const int* obs_layers; /* NULL or nobs <= 0: every layer */
+  int check_symmetry;
+  int rotation;          /* YTF_ROT_* */
+  int is2d;
+} ytf_transfer_desc;
+
+/* Many independent builds (stacks, frequencies, source layers, grids of any sizes) in one
+ * call: out[i] is the cache build_cavity_transfer_1d/2d(desc[i]) would return, bit for bit.
+ * The reference builds one cache per call and threads over the nodes inside it
+ * (mod_CavityTransfer.jl:224, :330); its callers loop over stacks and frequencies
+ * (e.g. chunked_2d, mod_ClosedFormGrid.jl:457-467). Here the node solves of all items run
+ * in the same kernel launches (grouped under a 6 GiB scratch budget); azimuthally symmetric
+ * 2D items with rotation take the rotation path. Argument errors name the item; on any
+ * error no cache is returned. */
+int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* desc, ytf_cache** out);
+
+/* One item of ytf_green_batch: the arguments of ytf_green. */
+typedef struct {
+  const ytf_cache* cache;
+  int obs_layer;
+  double zsrc_local;
+  int nz;
+  const double* z_obs;
+  int nx;
+  const double* xs;
+  int ny;
+  const double* ys;
+  int terms;
+  int precision;
+  double* out;
+  int out_is_device;
+} ytf_green_desc;
+
 /* closed_form_G(cache, obs_layer, zsrc_local, z_obs, xs, ys; terms)
  * (1D: mod_ClosedFormField.jl:435-487; 2D, lateral=:direct: :711-753). out: Nx*Ny*Nz*9
  * complex, Julia layout. precision: YTF_PREC_FP64 (CUDA-core FP64 contraction),
@@ -111,6 +159,13 @@ int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* cache, double* T, double* Qf
 int ytf_green(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, double zsrc_local, int nz, const double* z_obs,
               int nx, const double* xs, int ny, const double* ys, int terms, int precision, double* out,
               int out_is_device);
+
+/* closed_form_G over many (cache, observation set) items with one synchronisation: the
+ * same results as ytf_green per item, in order, on the context's stream; the coordinates of
+ * all items go up in one copy and the items' kernels queue back to back. The reference
+ * calls closed_form_G once per cache (mod_ClosedFormField.jl:435, :711); its callers loop
+ * (e.g. build_closed_form_green, mod_ClosedFormAssembly.jl:114). */
+int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* desc);
 
 /* FastGaussQuadrature.gausslegendre(n) (used at mod_KxGrid.jl:362): ascending nodes on
  * [-1, 1] and weights, correctly rounded. */

@@ -274,3 +274,75 @@ def test_lateral_int8_slices_capped_and_exact(ytf):
     G8 = ytf.closed_form_G(gc, 2, 0.3, [0.45], xs, ys, precision="int8x3")
     assert relerr(G8, G64) < 3e-7, relerr(G8, G64)
     assert np.array_equal(G8, ytf.closed_form_G(gc, 2, 0.3, [0.45], xs, ys, precision="int8x3"))
+
+
+def _exports_equal(a, b):
+    ea, eb = a.export(), b.export()
+    for key in ea:
+        assert np.array_equal(np.asarray(ea[key]), np.asarray(eb[key])), key
+    for x, y in zip(a.status(), b.status()):
+        assert np.array_equal(x, y)
+
+
+def test_transfer_batch_matches_single_builds(ytf):
+    """One ytf_transfer_batch call over a mixed, uneven batch (1D and 2D, forward-only and
+    general chains, different stacks, layer counts, sizes and frequencies, a rotation item
+    and an empty rule) returns, item by item, the caches of the single builds bit for bit:
+    the batched kernels run the same per-node code on each item's own parameters."""
+    items, singles = [], []
+    for idx, src, obs, nk in ((0, 1, None, 48), (1, 2, [2], 100), (2, 1, [1, 3], 7), (2, 2, [2], 0)):
+        _, st = FOUNDATION_STACKS[idx]
+        kx, wt = krho_grid(st, W * (1 + 0.1 * idx), kmax=12.0)
+        kx, wt = kx[:nk], wt[:nk]
+        items.append(dict(stack=st, omega=W * (1 + 0.1 * idx), source_layer=src, kx_nodes=kx, wt_nodes=wt,
+                          obs_layers=obs))
+        singles.append(ytf.build_cavity_transfer_1d(st, W * (1 + 0.1 * idx), src, kx, wt, obs_layers=obs))
+    for idx, src, obs, nphi, rot in ((3, 2, [2], 5, "auto"), (4, 1, None, 3, "auto"), (4, 2, [2], 8, "auto"),
+                                     (1, 2, [2, 3], 4, "auto"), (1, 2, [2], 4, False)):
+        _, st = FOUNDATION_STACKS[idx]
+        kr, wr = krho_grid(st, W, kmax=10.0)
+        ph, wp = uniform_phi(nphi)
+        items.append(dict(stack=st, omega=W, source_layer=src, kr_nodes=kr, kr_weights=wr, phi_nodes=ph,
+                          phi_weights=wp, obs_layers=obs, rotation=rot))
+        singles.append(ytf.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp, obs_layers=obs, rotation=rot))
+    batch = ytf.build_cavity_transfer_batch(items)
+    assert len(batch) == len(singles)
+    assert batch[-2].rotation and not batch[-1].rotation
+    for b, s in zip(batch, singles):
+        assert b.n == s.n and b.obs_layers == s.obs_layers
+        _exports_equal(b, s)
+
+
+def test_transfer_batch_argument_error_names_the_item(ytf):
+    _, st = FOUNDATION_STACKS[1]
+    kx, wt = krho_grid(st, W, kmax=5.0)
+    good = dict(stack=st, omega=W, source_layer=1, kx_nodes=kx, wt_nodes=wt)
+    bad = dict(good, source_layer=len(st))
+    with pytest.raises(ytf.YTFError, match=r"source_layer=.*batch item 1"):
+        ytf.build_cavity_transfer_batch([good, bad])
+
+
+def test_green_batch_matches_single_calls(ytf):
+    """ytf_green_batch over 1D and 2D caches, every precision, host and device outputs:
+    item for item the same arrays as closed_form_G (bit for bit)."""
+    import torch
+    _, st1 = FOUNDATION_STACKS[1]
+    kx, wt = krho_grid(st1, W, kmax=12.0)
+    c1 = ytf.build_cavity_transfer_1d(st1, W, 2, kx, wt)
+    _, st4 = FOUNDATION_STACKS[4]
+    kr, wr = krho_grid(st4, W, kmax=10.0)
+    ph, wp = uniform_phi(6)
+    c2 = ytf.build_cavity_transfer_2d(st4, W, 2, kr, wr, ph, wp, obs_layers=[2])
+    xs, ys = np.linspace(-0.3, 0.3, 9), np.linspace(-0.2, 0.25, 7)
+    specs = [(c1, 2, 0.3, [0.1, 0.4], xs, ys, "fp64"), (c2, 2, 0.3, [0.2], xs, ys, "int8x3"),
+             (c2, 2, 0.3, [0.2, 0.6], xs[:5], ys, "split_bf16"), (c2, 2, 0.3, [0.5], xs, ys[:3], "fp64"),
+             (c2, 2, 0.3, [0.5], xs, ys, "int8x3")]
+    dev = torch.empty(len(xs) * len(ys) * 9, dtype=torch.complex128, device="cuda")
+    items = [dict(cache=c, obs_layer=o, zsrc_local=z, z_obs=zo, xs=x, ys=y, precision=p)
+             for c, o, z, zo, x, y, p in specs]
+    items[-1]["out"] = dev
+    res = ytf.closed_form_G_batch(items)
+    for (c, o, z, zo, x, y, p), r in zip(specs, res):
+        ref = ytf.closed_form_G(c, o, z, zo, x, y, precision=p)
+        got = r.cpu().numpy().reshape(3, 3, 1, len(y), len(x)).transpose(4, 3, 2, 1, 0) if hasattr(r, "cpu") else r
+        assert np.array_equal(got, ref), p

@@ -16,6 +16,21 @@ _i = ctypes.POINTER(ctypes.c_int)
 _u8 = ctypes.POINTER(ctypes.c_ubyte)
 _vp = ctypes.c_void_p
 
+class TransferDesc(ctypes.Structure):
+    """ytf_transfer_desc (include/ytf.h)."""
+    _fields_ = [("stack", _vp), ("omega", ctypes.c_double), ("source_layer", ctypes.c_int), ("nk", ctypes.c_int),
+                ("k_nodes", _d), ("k_weights", _d), ("nphi", ctypes.c_int), ("phi_nodes", _d), ("phi_weights", _d),
+                ("nobs", ctypes.c_int), ("obs_layers", _i), ("check_symmetry", ctypes.c_int),
+                ("rotation", ctypes.c_int), ("is2d", ctypes.c_int)]
+
+
+class GreenDesc(ctypes.Structure):
+    """ytf_green_desc (include/ytf.h)."""
+    _fields_ = [("cache", _vp), ("obs_layer", ctypes.c_int), ("zsrc_local", ctypes.c_double), ("nz", ctypes.c_int),
+                ("z_obs", _d), ("nx", ctypes.c_int), ("xs", _d), ("ny", ctypes.c_int), ("ys", _d),
+                ("terms", ctypes.c_int), ("precision", ctypes.c_int), ("out", _vp), ("out_is_device", ctypes.c_int)]
+
+
 # name -> (restype, argtypes); every symbol include/ytf.h declares
 SIGNATURES = {
     "ytf_version": (ctypes.c_int, []),
@@ -40,6 +55,8 @@ SIGNATURES = {
                                  _d, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int]),
     "ytf_green_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                          ctypes.c_int, _vp, ctypes.c_int, _vp]),
+    "ytf_transfer_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(TransferDesc), ctypes.POINTER(_vp)]),
+    "ytf_green_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(GreenDesc)]),
     "ytf_gauss_legendre": (ctypes.c_int, [ctypes.c_int, _d, _d]),
     "ytf_gl_rule": (ctypes.c_int, [_vp, ctypes.c_int, _d, _d, ctypes.c_int, ctypes.c_int, _d, _d, _d]),
 }

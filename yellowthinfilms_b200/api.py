@@ -272,6 +272,106 @@ def closed_form_G(cache: _Cache, obs_layer: int, zsrc_local: float, z_obs, xs, y
     return G.view(np.complex128).reshape(3, 3, nz, ny, nx).transpose(4, 3, 2, 1, 0)
 
 
+def build_cavity_transfer_batch(items, ctx: Optional[Context] = None):
+    """Many caches in one call (ytf_transfer_batch): each item is a dict with the keyword
+    arguments of build_cavity_transfer_1d (``kx_nodes``, ``wt_nodes``) or
+    build_cavity_transfer_2d (``kr_nodes``, ``kr_weights``, ``phi_nodes``, ``phi_weights``),
+    plus ``stack``, ``omega``, ``source_layer`` and optionally ``obs_layers``,
+    ``check_symmetry`` (1D) and ``rotation`` (2D). The node solves of all items share the
+    same kernel launches. Returns the caches in order."""
+    from ._native import TransferDesc
+    descs = (TransferDesc * max(1, len(items)))()
+    keep, meta = [], []
+    for i, it in enumerate(items):
+        st = _as_stack(it["stack"], ctx)
+        ctx = ctx or st.ctx
+        is2d = "kr_nodes" in it
+        if is2d:
+            k, w = _f64(it["kr_nodes"]), _f64(it["kr_weights"])
+            ph, wp = _f64(it["phi_nodes"]), _f64(it["phi_weights"])
+            if len(ph) != len(wp):
+                raise YTFError("build_cavity_transfer_2d: φ nodes/weights length mismatch")
+        else:
+            k, w = _f64(it["kx_nodes"]), _f64(it["wt_nodes"])
+            ph = wp = np.zeros(0)
+        if len(k) != len(w):
+            raise YTFError("build_cavity_transfer_%s: node/weight length mismatch" % ("2d" if is2d else "1d"))
+        no, ob = _obs_arg(it.get("obs_layers"))
+        rot = it.get("rotation", "auto")
+        d = descs[i]
+        d.stack = st.h
+        d.omega = float(it["omega"])
+        d.source_layer = int(it["source_layer"])
+        d.nk = len(k)
+        d.k_nodes, d.k_weights = ptr(k), ptr(w)
+        d.nphi = len(ph)
+        d.phi_nodes, d.phi_weights = ptr(ph), ptr(wp)
+        d.nobs, d.obs_layers = no, ptr(ob, _i)
+        d.check_symmetry = int(bool(it.get("check_symmetry", True)))
+        d.rotation = -1 if rot == "auto" else int(bool(rot))
+        d.is2d = int(is2d)
+        keep += [k, w, ph, wp, ob]
+        meta.append((st, is2d, k, w, ph, wp, it))
+    hs = (ctypes.c_void_p * max(1, len(items)))()
+    if items:
+        ctx.check(lib().ytf_transfer_batch(ctx.h, len(items), descs, hs))
+    out = []
+    for i, (st, is2d, k, w, ph, wp, it) in enumerate(meta):
+        h = ctypes.c_void_p(hs[i])
+        if is2d:
+            out.append(CavityTransferCache2D(h, st, it["omega"], it["source_layer"], k, w, ph, wp))
+        else:
+            out.append(CavityTransferCache1D(h, st, it["omega"], it["source_layer"], k, w))
+    return out
+
+
+def closed_form_G_batch(items, precision: str = "fp64"):
+    """closed_form_G over many items with one synchronisation (ytf_green_batch). Each item is
+    a tuple (cache, obs_layer, zsrc_local, z_obs, xs, ys) or a dict with those keys plus
+    optional ``terms``, ``precision`` and ``out`` (as closed_form_G). Returns the G arrays
+    (or the ``out`` tensors) in order."""
+    from ._native import GreenDesc
+    descs = (GreenDesc * max(1, len(items)))()
+    keep, outs = [], []
+    ctx = None
+    for i, it in enumerate(items):
+        if not isinstance(it, dict):
+            it = dict(zip(("cache", "obs_layer", "zsrc_local", "z_obs", "xs", "ys"), it))
+        cache = it["cache"]
+        ctx = ctx or cache.ctx
+        terms = it.get("terms", "all")
+        if terms not in TERMS:
+            raise YTFError(f"closed_form_G: terms must be :all, :direct, :scattered, :toeplitz or :hankel (got :{terms})")
+        zo, x, y = _f64(it["z_obs"]), _f64(it["xs"]), _f64(it["ys"])
+        nx, ny, nz = len(x), len(y), len(zo)
+        out = it.get("out")
+        if out is not None:
+            if out.numel() != nx * ny * nz * 9:
+                raise YTFError("closed_form_G: out has the wrong size")
+            optr, on_dev = out.data_ptr(), int(bool(getattr(out, "is_cuda", False)))
+            outs.append(out)
+        else:
+            G = np.zeros(2 * 9 * nz * nx * ny)
+            optr, on_dev = G.ctypes.data, 0
+            outs.append((G, nx, ny, nz))
+        d = descs[i]
+        d.cache, d.obs_layer, d.zsrc_local = cache.h, int(it["obs_layer"]), float(it["zsrc_local"])
+        d.nz, d.z_obs, d.nx, d.xs, d.ny, d.ys = nz, ptr(zo), nx, ptr(x), ny, ptr(y)
+        d.terms, d.precision = TERMS[terms], PRECISION[it.get("precision", precision)]
+        d.out, d.out_is_device = optr, on_dev
+        keep += [zo, x, y]
+    if items:
+        ctx.check(lib().ytf_green_batch(ctx.h, len(items), descs))
+    res = []
+    for o in outs:
+        if isinstance(o, tuple):
+            G, nx, ny, nz = o
+            res.append(G.view(np.complex128).reshape(3, 3, nz, ny, nx).transpose(4, 3, 2, 1, 0))
+        else:
+            res.append(o)
+    return res
+
+
 def gausslegendre(n: int):
     x = np.zeros(n)
     w = np.zeros(n)

@@ -35,7 +35,10 @@ struct ytf_ctx {
   std::vector<cudaEvent_t> free_events;
   std::map<std::string, std::pair<double, long>> ktime;  // name -> (ms, timed launches)
   std::map<std::string, long> klaunch;                   // name -> launches
+  void* pinned = nullptr;                                // page-locked staging of batched uploads
+  size_t pinned_bytes = 0;
   ~ytf_ctx() {
+    if (pinned) cudaFreeHost(pinned);
     for (auto& kv : ws) cudaFree(kv.second.first);
     for (auto& kv : pool) cudaFree(kv.second);
     for (auto& sp : spans) { cudaEventDestroy(sp.a); cudaEventDestroy(sp.b); }
@@ -168,8 +171,34 @@ int upload(ytf_ctx* ctx, void* dst, const void* src, size_t bytes) {
   return YTF_OK;
 }
 
+// page-locked staging buffer of at least `bytes` (the stream is idle when it is replaced:
+// every entry point that fills it synchronises before returning)
+void* pinned_staging(ytf_ctx* ctx, size_t bytes) {
+  if (ctx->pinned_bytes >= bytes) return ctx->pinned;
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  ctx->pinned = nullptr;
+  ctx->pinned_bytes = 0;
+  size_t want = std::max(bytes, (size_t)1 << 20);
+  if (cudaHostAlloc(&ctx->pinned, want, cudaHostAllocDefault) != cudaSuccess) {
+    ctx->pinned = nullptr;
+    return nullptr;
+  }
+  ctx->pinned_bytes = want;
+  return ctx->pinned;
+}
+
+// state shared by the items of one ytf_green_batch call: pre-uploaded coordinates, one
+// tensor-core error word, no per-item synchronisation
+struct GreenBatch {
+  const double* dzo;
+  const double* dxs;
+  const double* dys;
+  unsigned* err;
+};
+
 // allocate the cache's arrays in one block
-int alloc_cache(ytf_ctx* ctx, ytf_cache* c) {
+int alloc_cache(ytf_ctx* ctx, ytf_cache* c, bool upload_nodes = true) {
   long n = c->n;
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -200,6 +229,7 @@ int alloc_cache(ytf_ctx* ctx, ytf_cache* c) {
   CK(cudaMemsetAsync(c->block, 0, off, ctx->stream));
   (void)o_status;
   int rc;
+  if (!upload_nodes) return YTF_OK;
   if ((rc = upload(ctx, c->d_kr, c->kr.data(), 8 * c->kr.size()))) return rc;
   if ((rc = upload(ctx, c->d_wr, c->wr.data(), 8 * c->wr.size()))) return rc;
   if (!c->phi.empty()) {
@@ -439,21 +469,43 @@ int ytf_stack_destroy(ytf_stack* s) {
   return YTF_OK;
 }
 
-int ytf_transfer_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, int nk, const double* kx_nodes,
-                    const double* wt_nodes, int nobs, const int* obs_layers, int check_symmetry, ytf_cache** out) {
-  if (!ctx || !out) return YTF_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// validation and cache creation shared by the 1D/2D builds and the batch (no solve): the
+// argument checks and messages of build_cavity_transfer_1d (mod_CavityTransfer.jl:196-205)
+// and build_cavity_transfer_2d (:307-318)
+int prepare_cache(ytf_ctx* ctx, const ytf_stack* st, bool is2d, double omega, int source_layer, int nk,
+                  const double* k_nodes, const double* k_weights, int nphi, const double* phi_nodes,
+                  const double* phi_weights, int nobs, const int* obs_layers, int check_symmetry, int rotation,
+                  bool upload_nodes, ytf_cache** out, bool* use_rot) {
   *out = nullptr;
+  *use_rot = false;
+  const char* fn = is2d ? "build_cavity_transfer_2d" : "build_cavity_transfer_1d";
   std::vector<int> obs;
-  int rc = common_checks(ctx, st, "build_cavity_transfer_1d", source_layer, nobs, obs_layers, obs);
+  int rc = common_checks(ctx, st, fn, source_layer, nobs, obs_layers, obs);
   if (rc) return rc;
-  if (nk < 0 || (nk > 0 && (!kx_nodes || !wt_nodes)))
-    return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_1d: kx_nodes/wt_nodes length mismatch");
-  if (check_symmetry)
-    for (auto& L : st->host)
-      if (!closed_form(L))
-        return fail(ctx, YTF_ERR_ARG,
-                    "build_cavity_transfer_1d: the 1D path requires an isotropic/uniaxial stack "
-                    "(`_is_azimuthally_symmetric_stack`); use the 2D (kρ,φ) cache for biaxial/gyrotropic.");
+  if (!is2d) {
+    if (nk < 0 || (nk > 0 && (!k_nodes || !k_weights)))
+      return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_1d: kx_nodes/wt_nodes length mismatch");
+    if (check_symmetry)
+      for (auto& L : st->host)
+        if (!closed_form(L))
+          return fail(ctx, YTF_ERR_ARG,
+                      "build_cavity_transfer_1d: the 1D path requires an isotropic/uniaxial stack "
+                      "(`_is_azimuthally_symmetric_stack`); use the 2D (kρ,φ) cache for biaxial/gyrotropic.");
+  } else {
+    if (nk < 0 || (nk > 0 && (!k_nodes || !k_weights)))
+      return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: kρ nodes/weights length mismatch");
+    if (nphi < 0 || (nphi > 0 && (!phi_nodes || !phi_weights)))
+      return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: φ nodes/weights length mismatch");
+    bool sym = true;
+    for (auto& L : st->host) sym = sym && closed_form(L);
+    *use_rot = rotation == YTF_ROT_AUTO ? sym : rotation != 0;
+    if (*use_rot && !sym)
+      return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: rotation=true requires an azimuthally symmetric stack");
+  }
   CK(cudaSetDevice(ctx->device));
   ytf_cache* c = new ytf_cache();
   c->ctx = ctx;
@@ -464,19 +516,62 @@ int ytf_transfer_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_
   c->nobs = (int)obs.size();
   for (int i = 0; i < c->nobs; ++i) c->obs[i] = obs[i];
   c->omega = omega;
+  c->is2d = is2d;
+  c->rotation = *use_rot;
   c->Nk = nk;
-  c->Np = 1;
-  c->n = nk;
-  c->kr.assign(kx_nodes, kx_nodes + nk);
-  c->wr.assign(wt_nodes, wt_nodes + nk);
+  c->Np = is2d ? nphi : 1;
+  c->n = is2d ? (long)nk * nphi : nk;
+  c->kr.assign(k_nodes, k_nodes + nk);
+  c->wr.assign(k_weights, k_weights + nk);
+  if (is2d) {
+    c->phi.assign(phi_nodes, phi_nodes + nphi);
+    c->wphi.assign(phi_weights, phi_weights + nphi);
+  }
   for (auto& L : st->host) c->d_layer.push_back(L.d);
   c->d_src = st->host[source_layer - 1].d;
-  if ((rc = alloc_cache(ctx, c))) { ytf_cache_destroy(c); return rc; }
-  TransferParams p;
-  fill_params(p, st, c);
-  p.mode = 0;
-  p.nout = c->n;
-  if (c->n > 0 && (rc = run_transfer(ctx, p, c->n))) { ytf_cache_destroy(c); return rc; }
+  if ((rc = alloc_cache(ctx, c, upload_nodes))) { ytf_cache_destroy(c); return rc; }
+  *out = c;
+  return YTF_OK;
+}
+
+// φ = 0 base solve per kρ, then the exact rotation to every φ (azimuthally symmetric stack)
+int solve_rotation(ytf_ctx* ctx, const ytf_stack* st, ytf_cache* c, const TransferParams& p) {
+  long nb = c->Nk;
+  int N = st->nL;
+  WS(modes, double2, "tr_modes", (size_t)N * 20 * nb);
+  WS(lstat, uint8_t, "tr_lstat", (size_t)N * nb);
+  WS(sint, double2, "tr_sint", (size_t)std::max(N - 1, 1) * 16 * nb);
+  WS(bstat, uint8_t, "tr_bstatus", (size_t)nb);
+  WS(btv, uint8_t, "tr_btvalid", (size_t)nb * c->nobs);
+  WS(bT, double2, "tr_bT", (size_t)16 * nb * c->nobs);
+  TransferParams b = p;
+  b.mode = 2;
+  b.n = nb;
+  b.off = 0;
+  b.nout = nb;
+  b.modes = modes;
+  b.lstat = lstat;
+  b.sint = sint;
+  if (b.needL) { WS(sl, double2, "tr_sleft", (size_t)N * 16 * nb); b.sleft = sl; }
+  if (b.needR) { WS(sr, double2, "tr_sright", (size_t)N * 16 * nb); b.sright = sr; }
+  b.status = bstat;
+  b.tvalid = btv;
+  b.Tout = bT;
+  CK(LAUNCH("k_layer_modes", launch_layer_modes(b, ctx->stream)));
+  CK(LAUNCH("k_layer_modes_qr", launch_layer_modes_qr(b, ctx->stream)));
+  if (only_source_observed(b)) CK(LAUNCH("k_chain_src", launch_chain_src(b, ctx->stream)));
+  else CK(LAUNCH("k_chain", launch_chain(b, ctx->stream)));
+  TransferParams f = p;
+  f.mode = 1;
+  f.n = nb;
+  f.off = 0;
+  f.nout = c->n;
+  f.modes = modes;
+  CK(LAUNCH("k_rotate_fill", launch_rotate_fill(f, bstat, btv, bT, ctx->stream)));
+  return YTF_OK;
+}
+
+int finish_build(ytf_ctx* ctx, ytf_cache* c, ytf_cache** out) {
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) { ytf_cache_destroy(c); return fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e)); }
   prof_collect(ctx);
@@ -484,92 +579,204 @@ int ytf_transfer_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_
   return YTF_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int ytf_transfer_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, int nk, const double* kx_nodes,
+                    const double* wt_nodes, int nobs, const int* obs_layers, int check_symmetry, ytf_cache** out) {
+  if (!ctx || !out) return YTF_ERR_ARG;
+  *out = nullptr;
+  ytf_cache* c;
+  bool rot;
+  int rc = prepare_cache(ctx, st, false, omega, source_layer, nk, kx_nodes, wt_nodes, 0, nullptr, nullptr, nobs,
+                         obs_layers, check_symmetry, YTF_ROT_OFF, true, &c, &rot);
+  if (rc) return rc;
+  TransferParams p;
+  fill_params(p, st, c);
+  p.mode = 0;
+  p.nout = c->n;
+  if (c->n > 0 && (rc = run_transfer(ctx, p, c->n))) { ytf_cache_destroy(c); return rc; }
+  return finish_build(ctx, c, out);
+}
+
 int ytf_transfer_2d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, int nkr, const double* kr_nodes,
                     const double* kr_weights, int nphi, const double* phi_nodes, const double* phi_weights, int nobs,
                     const int* obs_layers, int rotation, ytf_cache** out) {
   if (!ctx || !out) return YTF_ERR_ARG;
   *out = nullptr;
-  std::vector<int> obs;
-  int rc = common_checks(ctx, st, "build_cavity_transfer_2d", source_layer, nobs, obs_layers, obs);
+  ytf_cache* c;
+  bool use_rot;
+  int rc = prepare_cache(ctx, st, true, omega, source_layer, nkr, kr_nodes, kr_weights, nphi, phi_nodes, phi_weights,
+                         nobs, obs_layers, 1, rotation, true, &c, &use_rot);
   if (rc) return rc;
-  if (nkr < 0 || (nkr > 0 && (!kr_nodes || !kr_weights)))
-    return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: kρ nodes/weights length mismatch");
-  if (nphi < 0 || (nphi > 0 && (!phi_nodes || !phi_weights)))
-    return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: φ nodes/weights length mismatch");
-  bool sym = true;
-  for (auto& L : st->host) sym = sym && closed_form(L);
-  bool use_rot = rotation == YTF_ROT_AUTO ? sym : rotation != 0;
-  if (use_rot && !sym)
-    return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: rotation=true requires an azimuthally symmetric stack");
-  CK(cudaSetDevice(ctx->device));
-  ytf_cache* c = new ytf_cache();
-  c->ctx = ctx;
-  ctx->refs += 1;
-  c->stack_ref = st;
-  c->nL = st->nL;
-  c->src = source_layer;
-  c->nobs = (int)obs.size();
-  for (int i = 0; i < c->nobs; ++i) c->obs[i] = obs[i];
-  c->omega = omega;
-  c->is2d = true;
-  c->rotation = use_rot;
-  c->Nk = nkr;
-  c->Np = nphi;
-  c->n = (long)nkr * nphi;
-  c->kr.assign(kr_nodes, kr_nodes + nkr);
-  c->wr.assign(kr_weights, kr_weights + nkr);
-  c->phi.assign(phi_nodes, phi_nodes + nphi);
-  c->wphi.assign(phi_weights, phi_weights + nphi);
-  for (auto& L : st->host) c->d_layer.push_back(L.d);
-  c->d_src = st->host[source_layer - 1].d;
-  if ((rc = alloc_cache(ctx, c))) { ytf_cache_destroy(c); return rc; }
   TransferParams p;
   fill_params(p, st, c);
   if (c->n > 0) {
     if (!use_rot) {
       p.mode = 1;
       p.nout = c->n;
-      if ((rc = run_transfer(ctx, p, c->n))) { ytf_cache_destroy(c); return rc; }
+      rc = run_transfer(ctx, p, c->n);
     } else {
-      // φ = 0 base solve per kρ, then the exact rotation to every φ
-      long nb = nkr;
-      int N = st->nL;
-      WS(modes, double2, "tr_modes", (size_t)N * 20 * nb);
-      WS(lstat, uint8_t, "tr_lstat", (size_t)N * nb);
-      WS(sint, double2, "tr_sint", (size_t)std::max(N - 1, 1) * 16 * nb);
-      WS(bstat, uint8_t, "tr_bstatus", (size_t)nb);
-      WS(btv, uint8_t, "tr_btvalid", (size_t)nb * c->nobs);
-      WS(bT, double2, "tr_bT", (size_t)16 * nb * c->nobs);
-      TransferParams b = p;
-      b.mode = 2;
-      b.n = nb;
-      b.off = 0;
-      b.nout = nb;
-      b.modes = modes;
-      b.lstat = lstat;
-      b.sint = sint;
-      if (b.needL) { WS(sl, double2, "tr_sleft", (size_t)N * 16 * nb); b.sleft = sl; }
-      if (b.needR) { WS(sr, double2, "tr_sright", (size_t)N * 16 * nb); b.sright = sr; }
-      b.status = bstat;
-      b.tvalid = btv;
-      b.Tout = bT;
-      CK(LAUNCH("k_layer_modes", launch_layer_modes(b, ctx->stream)));
-      CK(LAUNCH("k_layer_modes_qr", launch_layer_modes_qr(b, ctx->stream)));
-      if (only_source_observed(b)) CK(LAUNCH("k_chain_src", launch_chain_src(b, ctx->stream)));
-      else CK(LAUNCH("k_chain", launch_chain(b, ctx->stream)));
-      TransferParams f = p;
-      f.mode = 1;
-      f.n = nb;
-      f.off = 0;
-      f.nout = c->n;
-      f.modes = modes;
-      CK(LAUNCH("k_rotate_fill", launch_rotate_fill(f, bstat, btv, bT, ctx->stream)));
+      rc = solve_rotation(ctx, st, c, p);
     }
+    if (rc) { ytf_cache_destroy(c); return rc; }
+  }
+  return finish_build(ctx, c, out);
+}
+
+int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cache** out) {
+  if (!ctx || nb < 0 || (nb > 0 && (!d || !out))) return YTF_ERR_ARG;
+  for (int i = 0; i < nb; ++i) out[i] = nullptr;
+  if (nb == 0) return YTF_OK;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<ytf_cache*> cs(nb, nullptr);
+  std::vector<char> rot(nb, 0);
+  auto abort_all = [&](int rc) {
+    cudaStreamSynchronize(ctx->stream);
+    for (auto c : cs)
+      if (c) ytf_cache_destroy(c);
+    return rc;
+  };
+  // 1. validate and create every cache; node arrays go up from one page-locked block
+  size_t stage = 0;
+  for (int i = 0; i < nb; ++i) {
+    bool r = false;
+    const bool is2d = d[i].nphi > 0 || d[i].is2d;
+    int rc = prepare_cache(ctx, d[i].stack, is2d, d[i].omega, d[i].source_layer, d[i].nk, d[i].k_nodes, d[i].k_weights,
+                           d[i].nphi, d[i].phi_nodes, d[i].phi_weights, d[i].nobs, d[i].obs_layers,
+                           d[i].check_symmetry, d[i].rotation, false, &cs[i], &r);
+    if (rc) {
+      std::string m = ctx->err;
+      abort_all(rc);
+      return fail(ctx, rc, m + " (batch item " + std::to_string(i) + ")");
+    }
+    rot[i] = r;
+    stage += 2 * cs[i]->kr.size() + 2 * cs[i]->phi.size();
+  }
+  // 2. the fused passes: items grouped so that their node scratch fits the budget
+  const size_t budget = (size_t)6 << 30;
+  std::vector<TransferParams> ps(nb);
+  std::vector<size_t> scratch(nb, 0);
+  for (int i = 0; i < nb; ++i) {
+    fill_params(ps[i], d[i].stack, cs[i]);
+    ps[i].mode = cs[i]->is2d ? 1 : 0;
+    ps[i].n = cs[i]->n;
+    ps[i].off = 0;
+    ps[i].nout = cs[i]->n;
+    const int N = ps[i].nL;
+    const bool fast = only_source_observed(ps[i]);
+    size_t per = (size_t)N * 20 * 16 + (size_t)N;
+    if (!fast) per = scratch_per_node(N, ps[i].needL, ps[i].needR);
+    scratch[i] = per * (size_t)cs[i]->n + 4 * 256;
+  }
+  // per pass: every item's block, then the forward-only and general subsets, 3 offset arrays
+  size_t pbytes = 2 * (size_t)nb * sizeof(TransferParams) + 3 * (size_t)(nb + 1) * sizeof(long);
+  char* h = (char*)pinned_staging(ctx, 8 * std::max<size_t>(stage, 1) + pbytes + 64);
+  if (!h) return abort_all(fail(ctx, YTF_ERR_NOMEM, "build_cavity_transfer: page-locked staging allocation failed"));
+  {
+    double* hd = (double*)h;
+    size_t k = 0;
+    for (int i = 0; i < nb; ++i) {
+      ytf_cache* c = cs[i];
+      auto put = [&](double* dst, const std::vector<double>& v) -> int {
+        if (v.empty()) return YTF_OK;
+        std::memcpy(hd + k, v.data(), 8 * v.size());
+        cudaError_t e = cudaMemcpyAsync(dst, hd + k, 8 * v.size(), cudaMemcpyHostToDevice, ctx->stream);
+        k += v.size();
+        return e == cudaSuccess ? YTF_OK : fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e));
+      };
+      int rc;
+      if ((rc = put(c->d_kr, c->kr)) || (rc = put(c->d_wr, c->wr)) || (rc = put(c->d_phi, c->phi)) ||
+          (rc = put(c->d_wphi, c->wphi)))
+        return abort_all(rc);
+    }
+    h += ((8 * k + 63) / 64) * 64;
+  }
+  // rotation items and items too large for one pass take the single-problem paths
+  for (int i = 0; i < nb; ++i) {
+    if (cs[i]->n == 0 || !(rot[i] || scratch[i] > budget)) continue;
+    int rc = rot[i] ? solve_rotation(ctx, d[i].stack, cs[i], ps[i]) : run_transfer(ctx, ps[i], cs[i]->n);
+    if (rc) return abort_all(rc);
+  }
+  int first = 0;
+  while (first < nb) {
+    std::vector<int> items;
+    size_t used = 0;
+    int i = first;
+    for (; i < nb; ++i) {
+      if (cs[i]->n == 0 || rot[i] || scratch[i] > budget) continue;
+      if (used + scratch[i] > budget) break;
+      items.push_back(i);
+      used += scratch[i];
+    }
+    first = i;
+    if (items.empty()) continue;
+    WS(arena, char, "tb_scratch", used);
+    size_t o = 0;
+    auto carve = [&](size_t bytes) {
+      char* q = arena + o;
+      o += (bytes + 255) & ~size_t(255);
+      return q;
+    };
+    const int m = (int)items.size();
+    TransferParams* hp = (TransferParams*)h;
+    long* offm = (long*)(hp + m);
+    long* offs = offm + (m + 1);
+    long* offg = offs + (m + 1);
+    std::vector<int> fast_ids, gen_ids;
+    offm[0] = 0;
+    for (int j = 0; j < m; ++j) {
+      TransferParams& q = ps[items[j]];
+      const int N = q.nL;
+      const long n = q.n;
+      q.modes = (double2*)carve((size_t)N * 20 * 16 * n);
+      q.lstat = (uint8_t*)carve((size_t)N * n);
+      if (only_source_observed(q)) {
+        fast_ids.push_back(j);
+      } else {
+        q.sint = (double2*)carve((size_t)std::max(N - 1, 1) * 16 * 16 * n);
+        q.sleft = q.needL ? (double2*)carve((size_t)N * 16 * 16 * n) : nullptr;
+        q.sright = q.needR ? (double2*)carve((size_t)N * 16 * 16 * n) : nullptr;
+        gen_ids.push_back(j);
+      }
+      offm[j + 1] = offm[j] + (long)N * n;
+    }
+    // parameter blocks: all items (mode kernels), then the forward-only and general subsets
+    const int nf = (int)fast_ids.size(), ng = (int)gen_ids.size();
+    std::vector<TransferParams> all(m);
+    for (int j = 0; j < m; ++j) all[j] = ps[items[j]];
+    std::memcpy(hp, all.data(), sizeof(TransferParams) * m);
+    offs[0] = 0;
+    offg[0] = 0;
+    std::vector<TransferParams> pf, pg;
+    for (int j = 0; j < nf; ++j) { pf.push_back(all[fast_ids[j]]); offs[j + 1] = offs[j] + all[fast_ids[j]].n; }
+    for (int j = 0; j < ng; ++j) { pg.push_back(all[gen_ids[j]]); offg[j + 1] = offg[j] + all[gen_ids[j]].n; }
+    const size_t blk = sizeof(TransferParams) * m + 3 * sizeof(long) * (m + 1);
+    TransferParams* hpf = (TransferParams*)(h + blk);
+    TransferParams* hpg = hpf + nf;
+    if (nf) std::memcpy(hpf, pf.data(), sizeof(TransferParams) * nf);
+    if (ng) std::memcpy(hpg, pg.data(), sizeof(TransferParams) * ng);
+    const size_t tot = blk + sizeof(TransferParams) * (nf + ng);
+    WS(dpar, char, "tb_params", tot);
+    CK(cudaMemcpyAsync(dpar, h, tot, cudaMemcpyHostToDevice, ctx->stream));
+    const TransferParams* dp = (const TransferParams*)dpar;
+    const long* doffm = (const long*)(dp + m);
+    const long* doffs = doffm + (m + 1);
+    const long* doffg = doffs + (m + 1);
+    const TransferParams* dpf = (const TransferParams*)(dpar + blk);
+    const TransferParams* dpg = dpf + nf;
+    CK(LAUNCH("k_layer_modes", launch_transfer_batch(0, dp, doffm, m, offm[m], ctx->stream)));
+    CK(LAUNCH("k_layer_modes_qr", launch_transfer_batch(1, dp, doffm, m, offm[m], ctx->stream)));
+    if (nf) CK(LAUNCH("k_chain_src", launch_transfer_batch(2, dpf, doffs, nf, offs[nf], ctx->stream)));
+    if (ng) CK(LAUNCH("k_chain", launch_transfer_batch(3, dpg, doffg, ng, offg[ng], ctx->stream)));
+    // the staging block is reused by the next pass: let this pass's upload land first
+    if (first < nb) CK(cudaStreamSynchronize(ctx->stream));
   }
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) { ytf_cache_destroy(c); return fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e)); }
+  if (e != cudaSuccess) return abort_all(fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e)));
   prof_collect(ctx);
-  *out = c;
+  for (int i = 0; i < nb; ++i) out[i] = cs[i];
   return YTF_OK;
 }
 
@@ -640,8 +847,9 @@ int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* c, double* T, double* Qf, do
   return YTF_OK;
 }
 
-int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local, int nz, const double* z_obs, int nx,
-              const double* xs, int ny, const double* ys, int terms, int precision, double* out, int out_is_device) {
+static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local, int nz, const double* z_obs,
+                      int nx, const double* xs, int ny, const double* ys, int terms, int precision, double* out,
+                      int out_is_device, const GreenBatch* gb) {
   if (!ctx || !c || !out) return YTF_ERR_ARG;
   if (c->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "closed_form_G: cache belongs to another context");
   int oi = c->oidx(obs_layer);
@@ -687,13 +895,19 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
   sp.zpos = zpos;
   sp.d_obs = c->d_layer[obs_layer - 1];
   sp.nz = nz;
-  WS(dzo, double, "g_zo", nz);
-  WS(dxs, double, "g_xs", nx);
-  WS(dys, double, "g_ys", ny);
+  const double *dzo, *dxs, *dys;
   int rc;
-  if ((rc = upload(ctx, dzo, z_obs, 8 * (size_t)nz))) return rc;
-  if ((rc = upload(ctx, dxs, xs, 8 * (size_t)nx))) return rc;
-  if ((rc = upload(ctx, dys, ys, 8 * (size_t)ny))) return rc;
+  if (gb) {
+    dzo = gb->dzo; dxs = gb->dxs; dys = gb->dys;
+  } else {
+    WS(uzo, double, "g_zo", nz);
+    WS(uxs, double, "g_xs", nx);
+    WS(uys, double, "g_ys", ny);
+    if ((rc = upload(ctx, uzo, z_obs, 8 * (size_t)nz))) return rc;
+    if ((rc = upload(ctx, uxs, xs, 8 * (size_t)nx))) return rc;
+    if ((rc = upload(ctx, uys, ys, 8 * (size_t)ny))) return rc;
+    dzo = uzo; dxs = uxs; dys = uys;
+  }
   sp.zo = dzo;
   double2* G;
   if (out_is_device) {
@@ -786,66 +1000,125 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
       CK(cudaMemsetAsync(cmax, 0, sizeof(unsigned long long) * lp.nchunk * ncol, ctx->stream));
       CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream, cmax, kchunk)));
       WS(Gp, double2, "g_partial2", (size_t)lp.nchunk * npix * ncol);
-      WS(err, unsigned, "g_tc_err", 1);
+      unsigned* err = gb ? gb->err : nullptr;
+      if (!err) {
+        WS(e1, unsigned, "g_tc_err", 1);
+        err = e1;
+        CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+      }
       lp.Bq = Bq; lp.colmax = cmax; lp.partial = Gp; lp.err = err;
-      CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
       CK(LAUNCH("k_lateral_i8", launch_lateral_i8(lp, ctx->stream)));
       CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, lp.nchunk, Gp, G, ctx->stream)));
-      unsigned herr = 0;
-      CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
-      if (!out_is_device) CK(cudaMemcpyAsync(out, G, sizeof(double2) * nout, cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      prof_collect(ctx);
-      return YTF_OK;
+      if (!gb) {
+        unsigned herr = 0;
+        CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
+      }
+    } else {
+      CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream)));
+      if (precision == YTF_PREC_SPLIT_BF16) {
+        // tensor cores: FP32 phase tables, split-BF16 contraction, FP64 reduction of the slices
+        WS(Px, float2, "g_px", (size_t)c->n * nx);
+        WS(Py, float2, "g_py", (size_t)c->n * ny);
+        CK(LAUNCH("k_phase_tables", launch_phase_tables(v, nx, ny, dxs, dys, Px, Py, ctx->stream)));
+        LateralTC lp;
+        std::memset(&lp, 0, sizeof(lp));
+        lp.npix = npix; lp.n = c->n; lp.nx = nx; lp.ny = ny; lp.ncol = ncol;
+        lp.ctile = lateral_tc_ctile(ncol);
+        lp.Np = ((2 * lp.ctile + 15) / 16) * 16;
+        lp.Px = Px; lp.Py = Py; lp.S = S;
+        // one CTA per SM (tensor memory, registers): tiles x node slices fill one wave
+        long tiles = ((npix + 127) / 128) * ((ncol + lp.ctile - 1) / lp.ctile);
+        long want = std::max(1L, (long)nsm / tiles);
+        long kchunk = (c->n + want - 1) / want;
+        kchunk = std::max(16L, ((kchunk + 15) / 16) * 16);
+        int splits = (int)((c->n + kchunk - 1) / kchunk);
+        lp.kchunk = kchunk;
+        WS(Gp, double2, "g_partial2", (size_t)splits * npix * ncol);
+        unsigned* err = gb ? gb->err : nullptr;
+        if (!err) {
+          WS(e1, unsigned, "g_tc_err", 1);
+          err = e1;
+          CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+        }
+        lp.partial = Gp;
+        lp.err = err;
+        CK(LAUNCH("k_lateral_tc", launch_lateral_tc(lp, splits, ctx->stream)));
+        CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, splits, Gp, G, ctx->stream)));
+        if (!gb) {
+          unsigned herr = 0;
+          CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+          CK(cudaStreamSynchronize(ctx->stream));
+          if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
+        }
+      } else {
+        long tiles = ((npix + 63) / 64) * ((ncol + 31) / 32);
+        long want = (4L * nsm + tiles - 1) / tiles;
+        int splits = (int)std::max(1L, std::min(want, std::max(1L, c->n / 512)));
+        splits = lateral_splits(c->n, splits);
+        WS(Gp, double2, "g_partial2", (size_t)splits * npix * ncol);
+        CK(LAUNCH("k_lateral", launch_lateral(v, nx, ny, dxs, dys, ncol, S, Gp, splits, ctx->stream)));
+        CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, splits, Gp, G, ctx->stream)));
+      }
     }
-    CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream)));
-    if (precision == YTF_PREC_SPLIT_BF16) {
-      // tensor cores: FP32 phase tables, split-BF16 contraction, FP64 reduction of the slices
-      WS(Px, float2, "g_px", (size_t)c->n * nx);
-      WS(Py, float2, "g_py", (size_t)c->n * ny);
-      CK(LAUNCH("k_phase_tables", launch_phase_tables(v, nx, ny, dxs, dys, Px, Py, ctx->stream)));
-      LateralTC lp;
-      std::memset(&lp, 0, sizeof(lp));
-      lp.npix = npix; lp.n = c->n; lp.nx = nx; lp.ny = ny; lp.ncol = ncol;
-      lp.ctile = lateral_tc_ctile(ncol);
-      lp.Np = ((2 * lp.ctile + 15) / 16) * 16;
-      lp.Px = Px; lp.Py = Py; lp.S = S;
-      // one CTA per SM (tensor memory, registers): tiles x node slices fill one wave
-      long tiles = ((npix + 127) / 128) * ((ncol + lp.ctile - 1) / lp.ctile);
-      long want = std::max(1L, (long)nsm / tiles);
-      long kchunk = (c->n + want - 1) / want;
-      kchunk = std::max(16L, ((kchunk + 15) / 16) * 16);
-      int splits = (int)((c->n + kchunk - 1) / kchunk);
-      lp.kchunk = kchunk;
-      WS(Gp, double2, "g_partial2", (size_t)splits * npix * ncol);
-      WS(err, unsigned, "g_tc_err", 1);
-      lp.partial = Gp;
-      lp.err = err;
-      CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
-      CK(LAUNCH("k_lateral_tc", launch_lateral_tc(lp, splits, ctx->stream)));
-      CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, splits, Gp, G, ctx->stream)));
-      unsigned herr = 0;
-      CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
-      if (!out_is_device) CK(cudaMemcpyAsync(out, G, sizeof(double2) * nout, cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      prof_collect(ctx);
-      return YTF_OK;
-    }
-    long tiles = ((npix + 63) / 64) * ((ncol + 31) / 32);
-    long want = (4L * nsm + tiles - 1) / tiles;
-    int splits = (int)std::max(1L, std::min(want, std::max(1L, c->n / 512)));
-    splits = lateral_splits(c->n, splits);
-    WS(Gp, double2, "g_partial2", (size_t)splits * npix * ncol);
-    CK(LAUNCH("k_lateral", launch_lateral(v, nx, ny, dxs, dys, ncol, S, Gp, splits, ctx->stream)));
-    CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, splits, Gp, G, ctx->stream)));
   }
   if (!out_is_device) CK(cudaMemcpyAsync(out, G, sizeof(double2) * nout, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!gb) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    prof_collect(ctx);
+  }
+  return YTF_OK;
+}
+
+int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local, int nz, const double* z_obs, int nx,
+              const double* xs, int ny, const double* ys, int terms, int precision, double* out, int out_is_device) {
+  return green_impl(ctx, c, obs_layer, zsrc_local, nz, z_obs, nx, xs, ny, ys, terms, precision, out, out_is_device,
+                    nullptr);
+}
+
+int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
+  if (!ctx || nb < 0 || (nb > 0 && !d)) return YTF_ERR_ARG;
+  if (nb == 0) return YTF_OK;
+  CK(cudaSetDevice(ctx->device));
+  // every item's coordinates in one page-locked block, one upload
+  size_t tot = 0;
+  for (int i = 0; i < nb; ++i) {
+    if (d[i].nz < 0 || d[i].nx < 0 || d[i].ny < 0)
+      return fail(ctx, YTF_ERR_ARG, "closed_form_G: negative grid size (batch item " + std::to_string(i) + ")");
+    tot += (size_t)d[i].nz + d[i].nx + d[i].ny;
+  }
+  double* h = (double*)pinned_staging(ctx, 8 * std::max<size_t>(tot, 1));
+  if (!h) return fail(ctx, YTF_ERR_NOMEM, "closed_form_G: page-locked staging allocation failed");
+  std::vector<size_t> o(nb);
+  size_t k = 0;
+  for (int i = 0; i < nb; ++i) {
+    o[i] = k;
+    if (d[i].nz) std::memcpy(h + k, d[i].z_obs, 8 * (size_t)d[i].nz);
+    k += d[i].nz;
+    if (d[i].nx) std::memcpy(h + k, d[i].xs, 8 * (size_t)d[i].nx);
+    k += d[i].nx;
+    if (d[i].ny) std::memcpy(h + k, d[i].ys, 8 * (size_t)d[i].ny);
+    k += d[i].ny;
+  }
+  WS(dc, double, "gb_coords", std::max<size_t>(tot, 1));
+  WS(err, unsigned, "gb_tc_err", 1);
+  CK(cudaMemcpyAsync(dc, h, 8 * tot, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+  for (int i = 0; i < nb; ++i) {
+    GreenBatch gb{dc + o[i], dc + o[i] + d[i].nz, dc + o[i] + d[i].nz + d[i].nx, err};
+    int rc = green_impl(ctx, d[i].cache, d[i].obs_layer, d[i].zsrc_local, d[i].nz, d[i].z_obs, d[i].nx, d[i].xs,
+                        d[i].ny, d[i].ys, d[i].terms, d[i].precision, d[i].out, d[i].out_is_device, &gb);
+    if (rc) {
+      cudaStreamSynchronize(ctx->stream);
+      return rc;
+    }
+  }
+  unsigned herr = 0;
+  CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   prof_collect(ctx);
+  if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
   return YTF_OK;
 }
 

@@ -55,6 +55,9 @@ struct TransferParams {
   double2* sf;             // [6][nout], column-major 2x3
   double2* sb;             // [6][nout]
   double2* basis;          // [nobs][16][nout]: exf0 exf1 eyf0 eyf1 ezf0 ezf1 exb.. eyb.. ezb.. kzf0 kzf1 kzb0 kzb1
+  // response mode of the forward-only chain (_cavity_response): when set, k_chain_src writes
+  // resp[node] and the status only (no T^o, seeds, basis, valid flags)
+  double* resp;            // [nout]
 };
 
 cudaError_t launch_layer_modes(const TransferParams& p, cudaStream_t stream);
@@ -62,6 +65,10 @@ cudaError_t launch_layer_modes_qr(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream);
 // k_chain when every observation layer is the source layer
 cudaError_t launch_chain_src(const TransferParams& p, cudaStream_t stream);
+// batched transfer kernels over nb problems (device arrays probs[nb], off[nb + 1]; total =
+// off[nb]): kernel 0 = layer modes, 1 = general QR pass, 2 = forward-only chain, 3 = chain
+cudaError_t launch_transfer_batch(int kernel, const TransferParams* probs, const long* off, int nb, long total,
+                                  cudaStream_t stream);
 cudaError_t launch_rotate_fill(const TransferParams& p, const uint8_t* base_status, const uint8_t* base_tvalid,
                                const double2* Tbase, cudaStream_t stream);
 

@@ -447,12 +447,8 @@ constexpr uint8_t ST_NEED_QR = 128;  // internal: this (node, layer) awaits the 
 
 // K1: closed-form TE/TM modes (isotropic/uniaxial) and the block path; everything else is
 // flagged for k_layer_modes_qr. Layer-major indexing: one layer, one material kind per warp.
-__global__ void __launch_bounds__(128) k_layer_modes(TransferParams p) {
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long n = p.n;
-  if (t >= n * p.nL) return;
-  int layer = (int)(t / n);
-  long node = t - (long)layer * n;
+__device__ __forceinline__ void layer_modes_body(const TransferParams& p, int layer, long node) {
+  const long n = p.n;
   double kx, ky;
   node_k(p, p.off + node, kx, ky);
   const LayerDev& L = p.layers[layer];
@@ -466,14 +462,16 @@ __global__ void __launch_bounds__(128) k_layer_modes(TransferParams p) {
   }
   p.lstat[(long)layer * n + node] = done ? classify_store(p, layer, node, Q, V) : ST_NEED_QR;
 }
+__global__ void __launch_bounds__(128) k_layer_modes(TransferParams p) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.n * p.nL) return;
+  const int layer = (int)(t / p.n);
+  layer_modes_body(p, layer, t - (long)layer * p.n);
+}
 
 // K1b: the general 4x4 QR path for the (node, layer) pairs K1 left
-__global__ void __launch_bounds__(128) k_layer_modes_qr(TransferParams p) {
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long n = p.n;
-  if (t >= n * p.nL) return;
-  int layer = (int)(t / n);
-  long node = t - (long)layer * n;
+__device__ __forceinline__ void layer_modes_qr_body(const TransferParams& p, int layer, long node) {
+  const long n = p.n;
   if (p.lstat[(long)layer * n + node] != ST_NEED_QR) return;
   double kx, ky;
   node_k(p, p.off + node, kx, ky);
@@ -484,6 +482,12 @@ __global__ void __launch_bounds__(128) k_layer_modes_qr(TransferParams p) {
   if (!eig4(B, Q, V)) stat = ST_EIGEN;
   else stat = classify_store(p, layer, node, Q, V);
   p.lstat[(long)layer * n + node] = stat;
+}
+__global__ void __launch_bounds__(128) k_layer_modes_qr(TransferParams p) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.n * p.nL) return;
+  const int layer = (int)(t / p.n);
+  layer_modes_qr_body(p, layer, t - (long)layer * p.n);
 }
 
 // ------------------------------------------------------------------------------------
@@ -730,10 +734,8 @@ __device__ __forceinline__ void write_T(const TransferParams& p, int oi, long id
 // ------------------------------------------------------------------------------------
 // K2: per-node chain
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_chain(TransferParams p) {
-  long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long n = p.n;
-  if (node >= n) return;
+__device__ __forceinline__ void chain_body(const TransferParams& p, long node) {
+  const long n = p.n;
   const int N = p.nL, src = p.src;
   const bool base = p.mode == 2;  // rotation base: seeds/basis are filled per φ later
   const long nT = base ? n : p.nout;
@@ -931,6 +933,14 @@ __global__ void __launch_bounds__(128) k_chain(TransferParams p) {
 // from the (read-only) mode records with its matching swaps applied instead of being held
 // across iterations.
 // ------------------------------------------------------------------------------------
+// largest singular value of a 2x2 complex matrix: √ of the larger eigenvalue of A^H A
+__device__ __forceinline__ double sigma_max2(const M2& A) {
+  const double g00 = norm2(A.a00) + norm2(A.a10), g11 = norm2(A.a01) + norm2(A.a11);
+  const cd g01 = conj(A.a00) * A.a01 + conj(A.a10) * A.a11;
+  const double t = g00 + g11, dt = g00 * g11 - norm2(g01);
+  return sqrt(fmax((t + sqrt(fmax(t * t - 4.0 * dt, 0.0))) / 2.0, 0.0));
+}
+
 struct ModeV {  // one layer's mode vectors: Vf, Vb (4x2)
   cd vf[4][2], vb[4][2];
 };
@@ -979,10 +989,8 @@ __device__ __forceinline__ bool match_swap(const cd va[4][2], const cd vb[4][2])
   return norm2(C[0][1]) + norm2(C[1][0]) > norm2(C[0][0]) + norm2(C[1][1]);
 }
 
-__global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
-  long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long n = p.n;
-  if (node >= n) return;
+__device__ __forceinline__ void chain_src_body(const TransferParams& p, long node) {
+  const long n = p.n;
   const int N = p.nL, src = p.src;
   const bool base = p.mode == 2;
   const long nT = base ? n : p.nout;
@@ -996,12 +1004,13 @@ __global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
   for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * nT + gnode] = 0;
   if (stat & (ST_EIGEN | ST_SORT)) {
     p.status[gnode] = stat;
+    if (p.resp) p.resp[gnode] = 0.0;
     return;
   }
   uint32_t swaps = 0;  // bit 2l: forward columns of layer l swapped by matching, bit 2l+1: backward
   bool seeds_ok = true, seeds_fin = true;
   auto seeds_and_basis = [&](int layer) {  // layer 0-based, the source layer
-    if (base) return;
+    if (base || p.resp) return;
     Mode4 M;
     load_matched(p, layer, node, swaps, M);
     cd sif[2][3], sib[2][3];
@@ -1068,6 +1077,7 @@ __global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
   seeds_and_basis(src - 1);
   if (stat & ST_SINGULAR) {
     p.status[gnode] = stat;
+    if (p.resp) p.resp[gnode] = 0.0;
     return;
   }
   // cavity at the source layer (_R_cavity, _cavity_resummation), as k_chain
@@ -1088,6 +1098,15 @@ __global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
   } else {
     Fp = M24{Z2, Z2};
     Fm = M24{Z2, I2};
+  }
+  if (p.resp) {
+    // _cavity_response (mod_KSpaceFeatures.jl:109-127): max σ of RL, RR and, below the top
+    // layer, of (I - ΦF RL ΦB RR)^-1 = F⁺'s left block
+    double r = fmax(sigma_max2(RL), sigma_max2(RR));
+    if (src > 1 && src < N) r = fmax(r, sigma_max2(Fp.L));
+    p.resp[gnode] = isfinite(r) ? r : 0.0;
+    p.status[gnode] = stat | ST_VALID;
+    return;
   }
   // T^o of the source layer: Ef = RL F⁻, Eb = RR F⁺ (the same for every listed obs index)
   const M24 Ef = mul24(RL, Fm), Eb = mul24(RR, Fp);
@@ -1112,6 +1131,65 @@ __global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
     stat |= ST_VALID;
   }
   p.status[gnode] = stat;
+}
+
+__global__ void __launch_bounds__(128) k_chain(TransferParams p) {
+  const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (node < p.n) chain_body(p, node);
+}
+__global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
+  const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (node < p.n) chain_src_body(p, node);
+}
+
+// ------------------------------------------------------------------------------------
+// Batched forms: many independent problems (stacks, frequencies, grids) in one launch.
+// probs[i] is problem i's parameter block; off[i] the first flat index of problem i
+// (off[nb] = total): (node, layer) pairs for the mode kernels, nodes for the chains. A
+// thread finds its problem by binary search over off.
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ int find_problem(const long* __restrict__ off, int nb, long t) {
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+__global__ void __launch_bounds__(128) k_layer_modes_batch(const TransferParams* __restrict__ probs,
+                                                           const long* __restrict__ off, int nb) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= off[nb]) return;
+  const int i = find_problem(off, nb, t);
+  const TransferParams& p = probs[i];
+  const long lt = t - off[i];
+  const int layer = (int)(lt / p.n);
+  layer_modes_body(p, layer, lt - (long)layer * p.n);
+}
+__global__ void __launch_bounds__(128) k_layer_modes_qr_batch(const TransferParams* __restrict__ probs,
+                                                              const long* __restrict__ off, int nb) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= off[nb]) return;
+  const int i = find_problem(off, nb, t);
+  const TransferParams& p = probs[i];
+  const long lt = t - off[i];
+  const int layer = (int)(lt / p.n);
+  layer_modes_qr_body(p, layer, lt - (long)layer * p.n);
+}
+__global__ void __launch_bounds__(128) k_chain_batch(const TransferParams* __restrict__ probs,
+                                                     const long* __restrict__ off, int nb) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= off[nb]) return;
+  const int i = find_problem(off, nb, t);
+  chain_body(probs[i], t - off[i]);
+}
+__global__ void __launch_bounds__(128) k_chain_src_batch(const TransferParams* __restrict__ probs,
+                                                         const long* __restrict__ off, int nb) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= off[nb]) return;
+  const int i = find_problem(off, nb, t);
+  chain_src_body(probs[i], t - off[i]);
 }
 
 // ------------------------------------------------------------------------------------
@@ -1193,6 +1271,19 @@ cudaError_t launch_chain_src(const TransferParams& p, cudaStream_t stream) {
 cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream) {
   if (p.n <= 0) return cudaSuccess;
   k_chain<<<(unsigned)((p.n + 127) / 128), 128, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transfer_batch(int kernel, const TransferParams* probs, const long* off, int nb, long total,
+                                  cudaStream_t stream) {
+  if (nb <= 0 || total <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((total + 127) / 128);
+  switch (kernel) {
+    case 0: k_layer_modes_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
+    case 1: k_layer_modes_qr_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
+    case 2: k_chain_src_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
+    default: k_chain_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
+  }
   return cudaGetLastError();
 }
 
