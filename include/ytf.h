@@ -101,6 +101,50 @@ int ytf_cache_status(ytf_ctx* ctx, const ytf_cache* cache, unsigned char* valid,
 int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* cache, double* T, double* Qf, double* Qb, double* sf, double* sb,
                      double* basis);
 
+/* _cavity_response(stack, ω, s, kρ, φ) (mod_KSpaceFeatures.jl:109-127) at n values of kρ
+ * (host arrays): the largest singular value of the source-layer reflections RL, RR and,
+ * below the top layer, of the cavity resolvent (I - ΦF RL ΦB RR)^-1; 0 where the node
+ * solve fails or is not finite. The pole scan of kspace_features evaluates it on a
+ * logarithmic kρ grid; one call solves all n nodes on the device. */
+int ytf_cavity_response(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer, long n,
+                        const double* kr, double phi, double* out);
+
+/* layer_light_lines(layer, ω, φ) (mod_KxGrid.jl:41-59) of one layer given as raw arrays
+ * (column-major 3x3 ε and μ, interleaved re/im; mu NULL = identity): up to 2 values into
+ * out (ascending), their count in *n. Host arithmetic; needs no context or GPU. */
+int ytf_layer_light_lines(const double* eps, const double* mu, double omega, double phi, double* out, int* n);
+
+/* Parameters of the point rule (kspace_features dims=1 + fixed_kρ_rule). */
+typedef struct {
+  double h_min;        /* smallest |z - z'| (or source-image distance) to resolve: Kcut >= target_decay / h_min */
+  double rho_max;      /* largest lateral distance (flat-region width 4 / rho_max); 0: none */
+  double target_decay; /* e-folds of evanescent decay at the cut (the reference's 25) */
+  double kr_cap;       /* absolute cap on Kcut; 0: 1e5 x the largest light line */
+  int scan;            /* 1: scan the real axis for guided-mode poles (log step 1e-3) */
+  int order;           /* Gauss-Legendre order per panel (8) */
+  double rtol;         /* relative accuracy the pole panels are sized for (1e-6) */
+} ytf_grid_params;
+
+#define YTF_GRID_MAX_POLES 256
+#define YTF_GRID_MAX_LINES 64
+typedef struct {
+  double Kcut, kmax;
+  long n_panels;
+  int n_poles, n_light_lines;
+  double poles[YTF_GRID_MAX_POLES][2]; /* (q, Γ) of the first poles found */
+  double light_lines[YTF_GRID_MAX_LINES];
+} ytf_grid_info;
+
+/* point_kx_grid (mod_ClosedFormGrid.jl:381-424) with the :fixed engine: kspace_features for
+ * a point rule at φ = 0 (light lines of every layer, Kcut, the real-axis pole scan of the
+ * source layer's cavity response (mod_KSpaceFeatures.jl:151-204) with golden-section peaks
+ * and half-power widths, clusters) and fixed_kρ_rule (:396-419): graded panels between the
+ * light lines, u² substitution at the half-space light lines, Gauss-Legendre nodes. The
+ * cavity response is evaluated on the device (ytf_cavity_response), the panels on the host,
+ * the nodes by ytf_gl_rule. k = w = NULL: size query (*n, info). cap: capacity of k and w. */
+int ytf_nodes_1d(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer, const ytf_grid_params* params,
+                 long cap, double* k, double* w, long* n, ytf_grid_info* info);
+
 /* One problem of a batched transfer build: the arguments of build_cavity_transfer_1d
  * (is2d = 0: k_nodes/k_weights are kx nodes and weights, check_symmetry applies) or of
  * build_cavity_transfer_2d (is2d = 1 or nphi > 0: kρ nodes/weights and φ nodes/weights,

@@ -61,3 +61,11 @@ def e_free(r, p, k, eps):
     n = r / R
     return (np.exp(1j * k * R) / (4 * np.pi * eps)) * (
         k ** 2 * np.cross(np.cross(n, p), n) / R + (3 * n * np.dot(n, p) - p) * (1 / R ** 3 - 1j * k / R ** 2))
+
+
+def config1_like_stack():
+    """Air / uniaxial hyperbolic film / glass in wavelength units (600 nm → 1): the film is
+    εo = -3+0.4i, εe = 4+0.2i, 50 nm; air 200 nm above it. It carries guided-mode poles
+    for the pole scan."""
+    return [lay(IsotropicMaterial(1.0), 200.0 / 600.0), lay(UniaxialMaterial(-3.0 + 0.4j, 4.0 + 0.2j), 50.0 / 600.0),
+            lay(IsotropicMaterial(2.25), 100.0 / 600.0)]

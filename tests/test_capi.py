@@ -44,3 +44,23 @@ def test_no_gpu_context_fails_loudly():
     import pytest
     with pytest.raises(RuntimeError):
         api.Context(0)
+
+
+def test_host_light_lines_bit_exact_with_oracle(oracle):
+    """libytf's host light lines (ytf_layer_light_lines: the k-grid's panel breaks) equal the
+    oracle's bit for bit, for every layer of the test stacks and the bench stack, several
+    frequencies and azimuths (no GPU needed)."""
+    import bench
+    from helpers import FOUNDATION_STACKS
+    from yellowthinfilms_b200 import api
+    stacks = [s for _, s in FOUNDATION_STACKS] + [bench.make_stack()]
+    n = 0
+    for st in stacks:
+        for L in st:
+            for w in (1.0, 2 * np.pi, 0.0104719755, 3.7):
+                for phi in (0.0, 0.3, 1.2):
+                    a = api.layer_light_lines(L, w, phi)
+                    b = np.asarray(oracle.light_lines(L, w, phi))
+                    assert len(a) == len(b) and np.array_equal(a, b), (a, b)
+                    n += 1
+    assert n > 300

@@ -346,3 +346,47 @@ def test_green_batch_matches_single_calls(ytf):
         ref = ytf.closed_form_G(c, o, z, zo, x, y, precision=p)
         got = r.cpu().numpy().reshape(3, 3, 1, len(y), len(x)).transpose(4, 3, 2, 1, 0) if hasattr(r, "cpu") else r
         assert np.array_equal(got, ref), p
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_cavity_response_matches_oracle(ytf, oracle, idx):
+    """_cavity_response on the device (forward-only chain in response mode) against the
+    oracle, every source layer, across the light lines and the guided-mode region."""
+    _, st = FOUNDATION_STACKS[idx]
+    ks = np.linspace(0.05, 4.0, 97) * W
+    for src in range(1, len(st)):
+        g = ytf.cavity_response(st, W, src, ks)
+        o = np.array([oracle.cavity_response(st, W, src, k) for k in ks])
+        assert relerr(g, o) < 1e-9, (src, relerr(g, o))
+
+
+def test_point_kx_grid_without_scan_bit_exact(ytf, oracle):
+    """point_kx_grid with the pole scan off: light lines, panels (host) and Gauss–Legendre
+    nodes (device) equal the oracle's rule bit for bit."""
+    for idx in (0, 1, 2):
+        _, st = FOUNDATION_STACKS[idx]
+        for h, rho in ((0.05, 1.0), (0.2, 0.0)):
+            k, w, info = ytf.point_kx_grid(st, W, 1, h_min=h, rho_max=rho, scan=False)
+            ko, wo, io = oracle.fixed_grid_1d(st, W, 1, h_min=h, rho_max=rho, scan=False)
+            assert np.array_equal(k, ko) and np.array_equal(w, wo), idx
+            assert info["Kcut"] == io["Kcut"] and info["n_panels"] == io["n_panels"]
+
+
+def test_point_kx_grid_with_pole_scan_matches_oracle(ytf, oracle):
+    """With the real-axis pole scan (device cavity responses, host peak search): the same
+    poles and panels as the oracle's scan to refinement precision, and G integrated with
+    either rule agrees to 1e-9."""
+    from helpers import config1_like_stack
+    for st, src in ((FOUNDATION_STACKS[1][1], 2), (config1_like_stack(), 1)):
+        k, w, info = ytf.point_kx_grid(st, W, src, h_min=0.05, rho_max=1.0)
+        ko, wo, io = oracle.fixed_grid_1d(st, W, src, h_min=0.05, rho_max=1.0)
+        assert info["n_poles"] == io["n_poles"] and info["n_panels"] == io["n_panels"]
+        assert len(k) == len(ko)
+        assert np.max(np.abs(k - ko)) <= 1e-9 * info["Kcut"]
+        c = ytf.build_cavity_transfer_1d(st, W, src, k, w, obs_layers=[src])
+        co = ytf.build_cavity_transfer_1d(st, W, src, ko, wo, obs_layers=[src])
+        xs, ys = np.array([0.1, 0.4]), np.array([0.0, 0.3])
+        d = st[src - 1].d
+        G = ytf.closed_form_G(c, src, 0.3 * d, [0.6 * d], xs, ys)
+        Go = ytf.closed_form_G(co, src, 0.3 * d, [0.6 * d], xs, ys)
+        assert relerr(G, Go) < 1e-9

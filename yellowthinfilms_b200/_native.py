@@ -31,6 +31,19 @@ class GreenDesc(ctypes.Structure):
                 ("terms", ctypes.c_int), ("precision", ctypes.c_int), ("out", _vp), ("out_is_device", ctypes.c_int)]
 
 
+class GridParams(ctypes.Structure):
+    """ytf_grid_params (include/ytf.h)."""
+    _fields_ = [("h_min", ctypes.c_double), ("rho_max", ctypes.c_double), ("target_decay", ctypes.c_double),
+                ("kr_cap", ctypes.c_double), ("scan", ctypes.c_int), ("order", ctypes.c_int), ("rtol", ctypes.c_double)]
+
+
+class GridInfo(ctypes.Structure):
+    """ytf_grid_info (include/ytf.h)."""
+    _fields_ = [("Kcut", ctypes.c_double), ("kmax", ctypes.c_double), ("n_panels", ctypes.c_long),
+                ("n_poles", ctypes.c_int), ("n_light_lines", ctypes.c_int), ("poles", (ctypes.c_double * 2) * 256),
+                ("light_lines", ctypes.c_double * 64)]
+
+
 # name -> (restype, argtypes); every symbol include/ytf.h declares
 SIGNATURES = {
     "ytf_version": (ctypes.c_int, []),
@@ -55,6 +68,11 @@ SIGNATURES = {
                                  _d, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int]),
     "ytf_green_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                          ctypes.c_int, _vp, ctypes.c_int, _vp]),
+    "ytf_cavity_response": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_long, _d, ctypes.c_double,
+                                           _d]),
+    "ytf_layer_light_lines": (ctypes.c_int, [_d, _d, ctypes.c_double, ctypes.c_double, _d, _i]),
+    "ytf_nodes_1d": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams), ctypes.c_long, _d,
+                                    _d, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(GridInfo)]),
     "ytf_transfer_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(TransferDesc), ctypes.POINTER(_vp)]),
     "ytf_green_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(GreenDesc)]),
     "ytf_gauss_legendre": (ctypes.c_int, [ctypes.c_int, _d, _d]),

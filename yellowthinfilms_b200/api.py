@@ -272,6 +272,51 @@ def closed_form_G(cache: _Cache, obs_layer: int, zsrc_local: float, z_obs, xs, y
     return G.view(np.complex128).reshape(3, 3, nz, ny, nx).transpose(4, 3, 2, 1, 0)
 
 
+def cavity_response(stack, omega, s, kr, phi=0.0, ctx: Optional[Context] = None):
+    """_cavity_response(stack, ω, s, kρ, φ) (mod_KSpaceFeatures.jl:109-127) at every kρ of
+    ``kr`` (array), solved on the device."""
+    st = _as_stack(stack, ctx)
+    k = _f64(np.atleast_1d(kr))
+    out = np.zeros(len(k))
+    st.ctx.check(lib().ytf_cavity_response(st.ctx.h, st.h, float(omega), int(s), len(k), ptr(k), float(phi), ptr(out)))
+    return out
+
+
+def layer_light_lines(layer, omega, phi=0.0):
+    """layer_light_lines(layer, ω, φ) (mod_KxGrid.jl:41-59): host arithmetic of libytf."""
+    from .materials import stack_arrays
+    _, _, eps, mu, _ = stack_arrays([layer])
+    out = np.zeros(3)
+    n = ctypes.c_int(0)
+    rc = lib().ytf_layer_light_lines(ptr(eps), ptr(mu), float(omega), float(phi), ptr(out), ctypes.byref(n))
+    if rc != 0:
+        raise YTFError("layer_light_lines: bad arguments")
+    return out[:n.value].copy()
+
+
+def point_kx_grid(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=25.0, kr_cap=0.0, scan=True, order=8,
+                  rtol=1e-6, ctx: Optional[Context] = None):
+    """point_kx_grid (mod_ClosedFormGrid.jl:381-424) with the :fixed engine: (kx, wt, info).
+    The pole scan's cavity responses are solved on the device; panels on the host; nodes by
+    the device Gauss–Legendre expansion."""
+    from ._native import GridInfo, GridParams
+    st = _as_stack(stack, ctx)
+    prm = GridParams(float(h_min), float(rho_max), float(target_decay), float(kr_cap), int(bool(scan)), int(order),
+                     float(rtol))
+    info = GridInfo()
+    n = ctypes.c_long(0)
+    st.ctx.check(lib().ytf_nodes_1d(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm), 0, None, None,
+                                    ctypes.byref(n), ctypes.byref(info)))
+    k = np.zeros(n.value)
+    w = np.zeros(n.value)
+    st.ctx.check(lib().ytf_nodes_1d(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm), n.value, ptr(k),
+                                    ptr(w), ctypes.byref(n), ctypes.byref(info)))
+    meta = dict(Kcut=info.Kcut, kmax=info.kmax, n_poles=info.n_poles, n_panels=info.n_panels,
+                poles=[(info.poles[i][0], info.poles[i][1]) for i in range(min(info.n_poles, 256))],
+                light_lines=[info.light_lines[i] for i in range(min(info.n_light_lines, 64))])
+    return k, w, meta
+
+
 def build_cavity_transfer_batch(items, ctx: Optional[Context] = None):
     """Many caches in one call (ytf_transfer_batch): each item is a dict with the keyword
     arguments of build_cavity_transfer_1d (``kx_nodes``, ``wt_nodes``) or

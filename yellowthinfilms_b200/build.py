@@ -23,6 +23,9 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC", "-shared",
+    # host complex arithmetic without the C99 Annex-G NaN recovery and without contraction,
+    # as the oracle build: the host-side k-grid (light lines, panels) then agrees bit for bit
+    "-Xcompiler", "-fcx-fortran-rules", "-Xcompiler", "-ffp-contract=off",
     "-diag-suppress", "177",
 ]
 

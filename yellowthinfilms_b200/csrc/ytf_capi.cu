@@ -13,6 +13,7 @@
 
 #include "../../include/ytf.h"
 #include "ytf_kernels.h"
+#include "ytf_grid.h"
 
 using namespace ytf;
 
@@ -623,6 +624,113 @@ int ytf_transfer_2d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_
     if (rc) { ytf_cache_destroy(c); return rc; }
   }
   return finish_build(ctx, c, out);
+}
+
+int ytf_cavity_response(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, long n, const double* kr,
+                        double phi, double* out) {
+  if (!ctx || (n > 0 && (!kr || !out)) || n < 0) return YTF_ERR_ARG;
+  if (!st) return fail(ctx, YTF_ERR_ARG, "_cavity_response: stack is NULL");
+  if (st->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "_cavity_response: stack belongs to another context");
+  const int N = st->nL;
+  if (!(1 <= source_layer && source_layer < N))
+    return fail(ctx, YTF_ERR_ARG, "_cavity_response: source layer " + std::to_string(source_layer) + " outside 1:" +
+                                      std::to_string(N - 1));
+  if (n == 0) return YTF_OK;
+  CK(cudaSetDevice(ctx->device));
+  // a (kρ, φ) grid of n x 1 nodes solved by the forward-only chain in response mode
+  WS(dk, double, "cr_k", n);
+  WS(dphi, double, "cr_phi", 1);
+  WS(dresp, double, "cr_out", n);
+  WS(dstat, uint8_t, "cr_status", n);
+  int rc;
+  if ((rc = upload(ctx, dk, kr, 8 * (size_t)n))) return rc;
+  if ((rc = upload(ctx, dphi, &phi, 8))) return rc;
+  TransferParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.layers = st->dev;
+  p.nL = N;
+  p.src = source_layer;
+  p.nobs = 1;
+  p.obs[0] = source_layer;
+  p.omega = omega;
+  p.mode = 1;
+  p.Nk = (int)n;
+  p.Np = 1;
+  p.kr = dk;
+  p.phi = dphi;
+  p.nout = n;
+  p.status = dstat;
+  p.resp = dresp;
+  if ((rc = run_transfer(ctx, p, n))) return rc;
+  CK(cudaMemcpyAsync(out, dresp, 8 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  prof_collect(ctx);
+  return YTF_OK;
+}
+
+int ytf_layer_light_lines(const double* eps, const double* mu, double omega, double phi, double* out, int* n) {
+  if (!eps || !n) return YTF_ERR_ARG;
+  static const double mu_one[18] = {1, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 1, 0};
+  auto L = grid::layer_light_lines(eps, mu ? mu : mu_one, omega, phi);
+  if (out)
+    for (size_t i = 0; i < L.size() && i < 3; ++i) out[i] = L[i];
+  *n = (int)L.size();
+  return YTF_OK;
+}
+
+int ytf_nodes_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm, long cap,
+                 double* k, double* w, long* n, ytf_grid_info* info) {
+  if (!ctx || !prm || !n) return YTF_ERR_ARG;
+  if (!st) return fail(ctx, YTF_ERR_ARG, "point_kx_grid: stack is NULL");
+  if (st->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "point_kx_grid: stack belongs to another context");
+  const int N = st->nL;
+  if (!(1 <= source_layer && source_layer < N))
+    return fail(ctx, YTF_ERR_ARG, "point_kx_grid: source_layer=" + std::to_string(source_layer) + " must be in 1:" +
+                                      std::to_string(N - 1));
+  if (!(prm->h_min > 0)) return fail(ctx, YTF_ERR_ARG, "point_kx_grid: h_min must be positive");
+  if (prm->order < 1) return fail(ctx, YTF_ERR_ARG, "point_kx_grid: order must be ≥ 1");
+  if (!(prm->rtol > 0 && prm->rtol < 1)) return fail(ctx, YTF_ERR_ARG, "point_kx_grid: rtol must be in (0, 1)");
+  std::vector<const double*> eps(N), mu(N);
+  for (int j = 0; j < N; ++j) { eps[j] = st->host[j].eps; mu[j] = st->host[j].mu; }
+  // the pole scan's evaluator: the cavity response of the source layer at φ = 0, on the device
+  grid::Eval f = [&](const std::vector<double>& ks, std::vector<double>& out) -> int {
+    out.assign(ks.size(), 0.0);
+    if (ks.empty()) return 0;
+    return ytf_cavity_response(ctx, st, omega, source_layer, (long)ks.size(), ks.data(), 0.0, out.data());
+  };
+  grid::Features F;
+  int rc = grid::features_1d(eps, mu, omega, prm->h_min, prm->rho_max, prm->target_decay, prm->kr_cap, 1e5,
+                             prm->scan != 0, 1e-3, 1.05, f, F);
+  if (rc) return rc;
+  std::vector<std::pair<double, double>> panels;
+  try {
+    panels = grid::fixed_kr_panels(F, prm->order, prm->rtol, 0.5, 12, 0.05, 4.0, 4.0, 0.5);
+  } catch (std::exception& e) {
+    return fail(ctx, YTF_ERR_ARG, e.what());
+  }
+  const long tot = (long)panels.size() * prm->order;
+  *n = tot;
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->Kcut = F.Kcut;
+    info->kmax = F.kmax;
+    info->n_panels = (long)panels.size();
+    info->n_poles = (int)F.poles.size();
+    for (int i = 0; i < (int)F.poles.size() && i < YTF_GRID_MAX_POLES; ++i) {
+      info->poles[i][0] = F.poles[i].q;
+      info->poles[i][1] = F.poles[i].G;
+    }
+    info->n_light_lines = (int)F.light_lines.size();
+    for (int i = 0; i < (int)F.light_lines.size() && i < YTF_GRID_MAX_LINES; ++i) info->light_lines[i] = F.light_lines[i];
+  }
+  if (!k || !w) return YTF_OK;  // size query
+  if (cap < tot)
+    return fail(ctx, YTF_ERR_ARG, "point_kx_grid: output capacity " + std::to_string(cap) + " < " + std::to_string(tot) +
+                                      " nodes");
+  std::vector<double> pa(panels.size()), pb(panels.size());
+  for (size_t i = 0; i < panels.size(); ++i) { pa[i] = panels[i].first; pb[i] = panels[i].second; }
+  return ytf_gl_rule(ctx, (int)panels.size(), pa.data(), pb.data(), prm->order, (int)F.singular_lines.size(),
+                     F.singular_lines.data(), k, w);
 }
 
 int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cache** out) {

@@ -1,0 +1,61 @@
+// ytf_grid.h -- host side of the Sommerfeld k-grid builder (the :fixed point rule):
+// light lines, the real-axis pole scan over a device-evaluated cavity response, pole
+// clusters and graded Gauss-Legendre panels. The cavity response comes in through an
+// evaluator callback (ytf_cavity_response on the device), so this code holds no GPU state.
+#pragma once
+#include <functional>
+#include <utility>
+#include <vector>
+
+namespace ytf {
+namespace grid {
+
+// light lines of one layer at azimuth φ (mod_KxGrid.jl:41-59): √Re of the roots q = kt² with
+// positive real part of det(ω² ε + q K(φ) μ⁻¹ K(φ)) = 0, ascending, merged at 1e-7 relative.
+// eps, mu: column-major 3x3, interleaved re/im (18 doubles each)
+std::vector<double> layer_light_lines(const double* eps, const double* mu, double w, double phi);
+
+// values of the cavity response at the given kρ (one device solve per call)
+using Eval = std::function<int(const std::vector<double>& k, std::vector<double>& out)>;
+
+struct Pole {
+  double q, G, phi, prom;
+};
+struct Cluster {
+  double a, b, G;
+};
+
+// real_axis_poles (mod_KSpaceFeatures.jl:151-204) at one azimuth: log-grid scan, local maxima
+// with prominence, golden-section peak, half-power crossings by bisection. The refinements of
+// all peaks run in lockstep so that each iteration is one evaluator call; per peak the
+// sequence of operations is the sequential algorithm's.
+int real_axis_poles(const Eval& f, double phi, double k_lo, double k_hi, double scan_step, double prominence,
+                    const std::vector<double>& exclude, std::vector<Pole>& out, double floor_rel = 1e-6,
+                    double floor_abs = 1e-10);
+
+// _clusters (mod_KSpaceFeatures.jl:217-229)
+std::vector<Cluster> clusters(std::vector<Pole> ps, double merge_rel);
+
+struct Features {
+  std::vector<double> light_lines, singular_lines;
+  double kmax = 0, Kcut = 0, h_min = 0, rho_max = 0, K_geom = 0, K_cap = 0;
+  bool capped = false;
+  std::vector<Pole> poles;
+  std::vector<Cluster> cl;
+};
+
+// kspace_features for a point rule at φ = 0 (mod_KSpaceFeatures.jl:295-360): light lines of
+// every layer (singular lines: those of the two half-spaces), Kcut, and the pole scan
+int features_1d(const std::vector<const double*>& eps, const std::vector<const double*>& mu, double w, double h_min,
+                double rho_max, double target_decay, double kr_cap, double kr_cap_rel, bool scan, double scan_step,
+                double prominence, const Eval& f, Features& F);
+
+// fixed_kρ_rule (mod_KSpaceFeatures.jl:396-419) up to the panels: graded_panels
+// (mod_KxGrid.jl:331-347) between 0, the light lines below Kcut and Kcut. Throws
+// std::runtime_error with the reference's messages.
+std::vector<std::pair<double, double>> fixed_kr_panels(const Features& F, int order, double rtol, double alpha,
+                                                       int grade, double r_rel, double c_h, double c_rho,
+                                                       double pole_safety);
+
+}  // namespace grid
+}  // namespace ytf

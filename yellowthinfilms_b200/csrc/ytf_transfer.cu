@@ -1000,8 +1000,10 @@ __device__ __forceinline__ void chain_src_body(const TransferParams& p, long nod
   double kx, ky;
   node_k(p, p.off + node, kx, ky);
   const cd z{0.0, 0.0};
-  if (!base) p.valid[gnode] = 0;
-  for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * nT + gnode] = 0;
+  if (!p.resp) {  // response mode writes status and resp only
+    if (!base) p.valid[gnode] = 0;
+    for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * nT + gnode] = 0;
+  }
   if (stat & (ST_EIGEN | ST_SORT)) {
     p.status[gnode] = stat;
     if (p.resp) p.resp[gnode] = 0.0;
