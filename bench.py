@@ -58,6 +58,63 @@ def make_stack(seed=SEED):
     return layers
 
 
+def uneven_batch(n_stacks=1024, seed=SEED, nk_lo=1024, nk_hi=32768):
+    """The uneven-batch workload: n_stacks seeded stacks, 2-24 layers each (half-spaces
+    isotropic dielectrics; interior layers isotropic, uniaxial-hyperbolic (sign Re εo ≠ sign
+    Re εe) or gyrotropic; d U[5, 300] nm), λ U[450, 750] nm, source in a random layer above
+    the last, observed in the source layer. Node counts log-uniform in [nk_lo, nk_hi]: a 1D
+    (kx) rule for azimuthally symmetric stacks, a 2D (kρ, 8 φ) rule for gyrotropic ones, GL-8
+    panels on [0, 20 k0]. Returns (transfer items, synthesis items without caches)."""
+    from yellowthinfilms_b200.materials import FlatOpticalLayer, GyrotropicMaterial, IsotropicMaterial, UniaxialMaterial
+    rng = np.random.default_rng(seed + 4)
+    tr, syn = [], []
+    for _ in range(n_stacks):
+        nl = int(rng.integers(2, 25))
+        layers, gyro = [], False
+        for l in range(nl):
+            d = float(rng.uniform(5.0, 300.0))
+            kind = 0 if l in (0, nl - 1) else int(rng.integers(0, 3))
+            if kind == 0:
+                lo, hi = (1.0, 2.5) if l in (0, nl - 1) else (1.0, 6.0)
+                m = IsotropicMaterial(complex(rng.uniform(lo, hi), rng.uniform(0.001, 0.3)))
+            elif kind == 1:
+                eo = complex(-rng.uniform(1.0, 6.0), rng.uniform(0.01, 0.5))
+                ee = complex(rng.uniform(1.0, 6.0), rng.uniform(0.01, 0.5))
+                if rng.random() < 0.5:
+                    eo, ee = -eo.real + 1j * eo.imag, -ee.real + 1j * ee.imag
+                m = UniaxialMaterial(eo, ee)
+            else:
+                g = rng.uniform(0.0, 1.5)
+                eps = np.diag(rng.uniform(1.0, 6.0, 3) + 1j * rng.uniform(0.01, 0.5, 3)).astype(np.complex128)
+                eps[0, 1], eps[1, 0] = 1j * g, -1j * g
+                m = GyrotropicMaterial(eps)
+                gyro = True
+            layers.append(FlatOpticalLayer(m, d))
+        lam = float(rng.uniform(450.0, 750.0))
+        k0 = 2 * np.pi / lam
+        src = int(rng.integers(1, nl))
+        nk = int(np.exp(rng.uniform(np.log(nk_lo), np.log(nk_hi))))
+        from yellowthinfilms_b200.api import gausslegendre
+        xg, wg = gausslegendre(ORDER)
+        nkr = max(ORDER, (nk // 8 if gyro else nk) // ORDER * ORDER)
+        npan = nkr // ORDER
+        edges = np.linspace(0.0, 20.0 * k0, npan + 1)
+        h = 0.5 * np.diff(edges)
+        kr = (0.5 * (edges[1:] + edges[:-1])[:, None] + h[:, None] * xg[None, :]).ravel()
+        wr = (h[:, None] * wg[None, :]).ravel()
+        ds = layers[src - 1].d
+        item = dict(stack=layers, omega=k0, source_layer=src, obs_layers=[src])
+        if gyro:
+            item.update(kr_nodes=kr, kr_weights=wr, phi_nodes=2 * np.pi * np.arange(8) / 8,
+                        phi_weights=np.full(8, 2 * np.pi / 8), rotation=False)
+        else:
+            item.update(kx_nodes=kr, wt_nodes=wr)
+        tr.append(item)
+        xy = np.linspace(-0.2 * lam, 0.2 * lam, 4)
+        syn.append(dict(obs_layer=src, zsrc_local=0.5 * ds, z_obs=np.linspace(0.1 * ds, 0.9 * ds, 4), xs=xy, ys=xy))
+    return tr, syn
+
+
 def grids(lam, kr_stride=1, phi_take=None):
     """(ω, kρ, wρ, φ, wφ, z_src, z_obs, xs, ys) for one wavelength (nm units)."""
     from yellowthinfilms_b200.api import gausslegendre
@@ -363,6 +420,76 @@ def run_ours(args):
     return 0
 
 
+def run_uneven(args):
+    """The uneven-batch workload through ytf_transfer_batch + ytf_green_batch, one GPU."""
+    import torch
+    from yellowthinfilms_b200 import api
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    tr, syn = uneven_batch()
+    stacks = [api.Stack(t["stack"], ctx) for t in tr]
+    items = [dict(t, stack=s) for t, s in zip(tr, stacks)]
+    prec = args.precision if args.precision != "int8x3" else "fp64"  # 4 x 4 pixels: the FP64 contraction
+
+    def step():
+        caches = api.build_cavity_transfer_batch(items, ctx=ctx)
+        out = api.closed_form_G_batch([dict(y, cache=c, precision=prec) for y, c in zip(syn, caches)])
+        del caches
+        return out
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            G = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    prof = ctx.profile_read()
+    entries = sum(g.size for g in G)
+    nodes = sum(len(t.get("kx_nodes", ())) or len(t["kr_nodes"]) * len(t["phi_nodes"]) for t in tr)
+    err = None
+    if not args.no_check:  # two items against the oracle on identical nodes
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ytf_oracle as oracle
+        oracle.set_threads(os.cpu_count() or 1)
+        errs = []
+        small = sorted(range(len(tr)), key=lambda i: len(tr[i].get("kx_nodes", ())) or 8 * len(tr[i]["kr_nodes"]))[:2]
+        for i in small:
+            t = tr[i]
+            if "kx_nodes" in t:
+                oc = oracle.build_cavity_transfer_1d(t["stack"], t["omega"], t["source_layer"], t["kx_nodes"],
+                                                     t["wt_nodes"], obs_layers=t["obs_layers"])
+            else:
+                oc = oracle.build_cavity_transfer_2d(t["stack"], t["omega"], t["source_layer"], t["kr_nodes"],
+                                                     t["kr_weights"], t["phi_nodes"], t["phi_weights"],
+                                                     obs_layers=t["obs_layers"], rotation=False)
+            y = syn[i]
+            Go = oracle.closed_form_G(oc, y["obs_layer"], y["zsrc_local"], y["z_obs"], y["xs"], y["ys"])
+            errs.append(float(np.linalg.norm(G[i] - Go) / np.linalg.norm(Go)))
+        err = max(errs)
+    line = {"metric": METRIC, "value": args.steps and entries / (ms * 1e-3), "unit": "entries/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[prec], "data": "synthetic (seeded)",
+            "config": {"workload": "uneven batch: 1024 stacks, 2-24 layers (isotropic / uniaxial-hyperbolic / "
+                                   "gyrotropic), node counts log-uniform in [1024, 32768] (1D kx or 2D kρ x 8 φ), "
+                                   "4 z rows x 4x4 lateral offsets each", "stacks": len(tr), "nodes_per_step": nodes,
+                       "entries_per_step": int(entries), "precision": prec,
+                       "calls": "ytf_transfer_batch + ytf_green_batch"},
+            "max_rel_err_vs_oracle": err, "clocks": clk.summary(),
+            "nodes_per_s": nodes / (ms * 1e-3),
+            "kernels_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items())},
+            "gpu_launches": int(sum(v[1] for v in prof.values()))}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,6 +497,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--workload", default="gyro32", choices=["gyro32", "uneven"],
+                    help="gyro32: the 8-layer stack at 32 wavelengths (default); uneven: 1024 uneven stacks")
     ap.add_argument("--per-call", action="store_true",
                     help="one build + synthesis call per wavelength instead of the batched calls")
     ap.add_argument("--precision", default="int8x3", choices=list(DTYPE),
@@ -378,6 +507,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "uneven":
+        return run_uneven(args)
     return run_ours(args)
 
 

@@ -390,3 +390,34 @@ def test_point_kx_grid_with_pole_scan_matches_oracle(ytf, oracle):
         G = ytf.closed_form_G(c, src, 0.3 * d, [0.6 * d], xs, ys)
         Go = ytf.closed_form_G(co, src, 0.3 * d, [0.6 * d], xs, ys)
         assert relerr(G, Go) < 1e-9
+
+
+def test_uneven_batch_workload_shape(ytf, oracle):
+    """The uneven-batch workload at reduced node counts: 24 stacks of 2-24 layers (isotropic,
+    uniaxial-hyperbolic, gyrotropic; 1D and 2D rules) built in one ytf_transfer_batch call
+    equal the single builds bit for bit, and the smallest items match the oracle."""
+    import bench
+    tr, syn = bench.uneven_batch(n_stacks=24, nk_lo=64, nk_hi=512)
+    assert len({len(t["stack"]) for t in tr}) > 5
+    batch = ytf.build_cavity_transfer_batch(tr)
+    for t, b in zip(tr, batch):
+        if "kx_nodes" in t:
+            s = ytf.build_cavity_transfer_1d(t["stack"], t["omega"], t["source_layer"], t["kx_nodes"], t["wt_nodes"],
+                                             obs_layers=t["obs_layers"])
+        else:
+            s = ytf.build_cavity_transfer_2d(t["stack"], t["omega"], t["source_layer"], t["kr_nodes"], t["kr_weights"],
+                                             t["phi_nodes"], t["phi_weights"], obs_layers=t["obs_layers"], rotation=False)
+        _exports_equal(b, s)
+    order = sorted(range(len(tr)), key=lambda i: len(tr[i].get("kx_nodes", ())) or 8 * len(tr[i]["kr_nodes"]))
+    for i in order[:3]:
+        t, y = tr[i], syn[i]
+        if "kx_nodes" in t:
+            oc = oracle.build_cavity_transfer_1d(t["stack"], t["omega"], t["source_layer"], t["kx_nodes"], t["wt_nodes"],
+                                                 obs_layers=t["obs_layers"])
+        else:
+            oc = oracle.build_cavity_transfer_2d(t["stack"], t["omega"], t["source_layer"], t["kr_nodes"],
+                                                 t["kr_weights"], t["phi_nodes"], t["phi_weights"],
+                                                 obs_layers=t["obs_layers"], rotation=False)
+        G = ytf.closed_form_G_batch([dict(y, cache=batch[i])])[0]
+        Go = oracle.closed_form_G(oc, y["obs_layer"], y["zsrc_local"], y["z_obs"], y["xs"], y["ys"])
+        assert relerr(G, Go) < 1e-9, (i, relerr(G, Go))
