@@ -133,6 +133,8 @@ typedef struct {
   int n_poles, n_light_lines;
   double poles[YTF_GRID_MAX_POLES][2]; /* (q, Γ) of the first poles found */
   double light_lines[YTF_GRID_MAX_LINES];
+  double* panels;   /* optional, set by the caller: receives the panels (a, b) pairs ... */
+  long panels_cap;  /* ... when panels_cap >= n_panels */
 } ytf_grid_info;
 
 /* point_kx_grid (mod_ClosedFormGrid.jl:381-424) with the :fixed engine: kspace_features for
@@ -144,6 +146,14 @@ typedef struct {
  * the nodes by ytf_gl_rule. k = w = NULL: size query (*n, info). cap: capacity of k and w. */
 int ytf_nodes_1d(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer, const ytf_grid_params* params,
                  long cap, double* k, double* w, long* n, ytf_grid_info* info);
+
+/* The same rule with the real-axis poles (q, Γ) given by the caller instead of scanned (the
+ * learned node placement proposes them): light lines, Kcut, clusters of the given poles,
+ * fixed_kρ_rule panels, Gauss-Legendre nodes. No counterpart in the reference, whose
+ * kspace_features always scans (mod_KSpaceFeatures.jl:295-360). */
+int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer,
+                         const ytf_grid_params* params, int npoles, const double* q, const double* G, long cap,
+                         double* k, double* w, long* n, ytf_grid_info* info);
 
 /* One problem of a batched transfer build: the arguments of build_cavity_transfer_1d
  * (is2d = 0: k_nodes/k_weights are kx nodes and weights, check_symmetry applies) or of
@@ -236,6 +246,33 @@ int ytf_gl_rule(ytf_ctx* ctx, int npanels, const double* pa, const double* pb, i
 int ytf_green_noalloc(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, double zsrc_local, int nz,
                       const double* z_obs_dev, int nx, const double* xs_dev, int ny, const double* ys_dev, int terms,
                       double* out_dev);
+
+/* ---------------------------------------------------------------------------------------
+ * The small MLP of the learned node placement. No counterpart in the reference: the
+ * reference places quadrature nodes from a pole scan of solved responses
+ * (mod_KSpaceFeatures.jl:151-204); this network predicts the scanned quantity (the log
+ * cavity response and a pole-proximity score) from a stack descriptor, the frequency and k,
+ * so a node placement can be proposed without the scan. Every proposed node is still solved
+ * exactly by the transfer path, which is also the fallback.
+ *
+ * sizes[0..nlayers]: layer widths (input features first, 2 outputs last); GELU between
+ * layers; FP32 master parameters, BF16 weights in every product, FP32 accumulation.
+ * Parameter vector: for each layer W [out x in] row-major, then b [out]. Loss: mean squared
+ * error of output 0 plus the logistic loss of output 1 (targets T: [B][2]). Inputs X: [B][n0]
+ * row-major float. ytf_mlp_train takes DEVICE pointers to a resident training set (n
+ * samples) and runs `steps` Adam steps (β = 0.9, 0.999) on mini-batches drawn on the device
+ * from a seeded hash; losses[steps] (optional) receives the mini-batch losses. */
+typedef struct ytf_mlp ytf_mlp;
+int ytf_mlp_create(int device, int nlayers, const int* sizes, unsigned long long seed, ytf_mlp** out);
+int ytf_mlp_destroy(ytf_mlp* net);
+const char* ytf_mlp_last_error(const ytf_mlp* net);
+long ytf_mlp_num_params(const ytf_mlp* net);
+int ytf_mlp_set_stream(ytf_mlp* net, void* stream);
+int ytf_mlp_params(ytf_mlp* net, float* get, const float* set);
+int ytf_mlp_forward(ytf_mlp* net, int B, const float* X, float* out, int on_device);
+int ytf_mlp_gradients(ytf_mlp* net, int B, const float* X, const float* T, float* grad, float* loss, int on_device);
+int ytf_mlp_train(ytf_mlp* net, long n, const float* X, const float* T, int batch, int steps, float lr,
+                  unsigned long long seed, float* losses);
 
 #ifdef __cplusplus
 }

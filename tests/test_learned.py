@@ -1,0 +1,156 @@
+"""The learned node placement: MLP kernels against the FP64 restatement, training on
+solver-generated data, and what the trained network gains over the plain fixed grid."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def L():
+    from yellowthinfilms_b200 import learned
+    return learned
+
+
+def _random_net(L, seed=0):
+    net = L.new_network(seed=seed)
+    rng = np.random.default_rng(seed)
+    p = net.params
+    net.params = (p + rng.normal(0, 0.02, p.size)).astype(np.float32)
+    return net
+
+
+def test_mlp_forward_and_gradients_match_oracle(L):
+    """ytf_mlp forward outputs and the backward kernels' parameter gradient against the FP64
+    numpy restatement (same BF16-rounded weights): FP32 accumulation over ≤ 256-term dot
+    products, so ≤ 1e-4 relative."""
+    import ytf_mlp_ref as R
+    net = _random_net(L, 3)
+    rng = np.random.default_rng(4)
+    B = 96
+    X = rng.normal(0, 1, (B, L.N_FEATURES)).astype(np.float32)
+    T = np.stack([rng.normal(0, 1, B), rng.uniform(0, 1, B)], 1).astype(np.float32)
+    p = net.params.astype(np.float64)
+    out = net.forward(X)
+    _, H = R.forward(p, net.sizes, X)
+    assert np.max(np.abs(out - H[-1])) <= 1e-4 * max(1.0, np.max(np.abs(H[-1])))
+    loss, g = net.gradients(X, T)
+    lo, go = R.loss_and_grad(p, net.sizes, X, T)
+    assert abs(loss - lo) <= 1e-5 * max(1.0, abs(lo))
+    assert np.linalg.norm(g - go) <= 1e-4 * np.linalg.norm(go), np.linalg.norm(g - go) / np.linalg.norm(go)
+    # layer by layer too (the small last layer would hide in the global norm)
+    o = 0
+    for l in range(1, len(net.sizes)):
+        n = net.sizes[l] * net.sizes[l - 1] + net.sizes[l]
+        assert np.linalg.norm(g[o:o + n] - go[o:o + n]) <= 1e-4 * np.linalg.norm(go[o:o + n]) + 1e-12, l
+        o += n
+
+
+def test_mlp_training_reduces_loss(L):
+    """Adam steps of libytf's kernels on a solver-generated set lower the loss (its floor is
+    not 0: the logistic term on soft pole scores keeps their entropy)."""
+    X, T = L.training_set(24, n_k=512, seed=5)
+    net = L.new_network(seed=1)
+    l0, _ = net.gradients(X[:4096], T[:4096])
+    losses = L.train(net, X, T, steps=300, batch=2048, lr=1e-3)
+    l1, _ = net.gradients(X[:4096], T[:4096])
+    assert np.all(np.isfinite(losses))
+    assert l1 < 0.6 * l0, (l0, l1)
+
+
+def _check_fn(api, st, k0, rho_max_wl=5.0):
+    lam = 2 * np.pi / k0
+    rho = np.exp(np.linspace(np.log(0.01 * lam), np.log(rho_max_wl * lam), 16))
+    z = np.linspace(60.0, 200.0, 6)
+
+    def G(k, w):
+        c = api.build_cavity_transfer_1d(st, k0, 1, k, w, obs_layers=[1])
+        return api.closed_form_G(c, 1, 20.0, z, rho, [0.0], terms="scattered")
+    return G
+
+
+def plain_nodes_to(L, api, st, k0, rho_max, G, Gref, tol, max_halvings=7):
+    """Nodes of the plain fixed rule (point_kx_grid without the pole scan), halved until G is
+    within tol of the reference; None if it never is."""
+    k, w, info = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rho_max, scan=False)
+    panels = info["panels"]
+    sing = sorted(set(api.layer_light_lines(st[0], k0)) | set(api.layer_light_lines(st[-1], k0)))
+    for _ in range(max_halvings + 1):
+        if np.linalg.norm(G(k, w) - Gref) <= tol * np.linalg.norm(Gref):
+            return len(k)
+        panels = api.halve_panels([tuple(p) for p in panels])
+        k, w = api.gl_rule(panels, 8, singular=sing)
+    return None
+
+
+def test_learned_rule_gains_over_the_method_without_it(L):
+    """What the trained network gains. On held-out stacks (losses from sharp to broad guided
+    modes): the network proposes candidate poles, one batched device call samples the exact
+    response around them, fixed_kρ_rule is built on the result, and the halving check accepts
+    the rule or falls back to the scanned rule. Against a converged reference (scanned rule at
+    rtol 1e-10, halving-checked):
+      * every rule the check accepts is within 2e-6 (the check is a reliable judge), and most
+        are accepted;
+      * accepted rules are built several times faster than the scanned rule (the reference's
+        method: thousands of device solves and ~110 sequential refinement rounds) with as few
+        nodes;
+      * against the plain fixed rule without pole knowledge (light-line breaks, u² substitution,
+        halved until 1e-6): for lateral offsets out to 5 λ the Bessel oscillation sets the panel
+        width and both need about the same nodes; for a near-field set (ρ ≤ 0.2 λ) the sharp
+        poles set the plain rule's count and the learned rule needs fewer nodes."""
+    import time
+    from yellowthinfilms_b200 import api
+    X, T = L.training_set(600, n_k=1024, seed=11)
+    net = L.new_network(seed=2)
+    L.train(net, X, T, steps=4000, batch=4096, lr=1e-3)
+    st0, lam0 = L.film_stack(np.random.default_rng(0))
+    L.propose_poles(net, st0, 2 * np.pi / lam0)  # warm the path
+    rng = np.random.default_rng(123)
+    rows = []
+    for _ in range(6):
+        st, lam = L.film_stack(rng)
+        k0 = 2 * np.pi / lam
+        for rw in (5.0, 0.2):
+            G = _check_fn(api, st, k0, rw)
+            kr, wr, ir = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rw * lam, rtol=1e-10)
+            Gref = G(*L.halved(st, k0, ir["panels"], 8))
+            assert np.linalg.norm(G(kr, wr) - Gref) <= 1e-9 * np.linalg.norm(Gref)
+            t = time.perf_counter()
+            ks, ws, _ = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rw * lam)
+            t_scan = time.perf_counter() - t
+            t = time.perf_counter()
+            k, w, info = L.learned_rule(net, st, k0, 1, h_min=80.0, rho_max=rw * lam)
+            t_learned = time.perf_counter() - t
+            Gk = G(k, w)
+            acc = bool(np.linalg.norm(Gk - G(*L.halved(st, k0, info["panels"], 8))) <= 1e-6 * np.linalg.norm(Gk))
+            err = np.linalg.norm(Gk - Gref) / np.linalg.norm(Gref)
+            n_plain = plain_nodes_to(L, api, st, k0, rw * lam, G, Gref, 1e-6)
+            rows.append(dict(rw=rw, acc=acc, err=err, n=len(k), n_scan=len(ks), n_plain=n_plain,
+                             speedup=t_scan / t_learned))
+    msg = "\n".join(str(r) for r in rows)
+    acc = [r for r in rows if r["acc"]]
+    assert all(r["err"] <= 2e-6 for r in acc), msg
+    assert len(acc) >= 8, msg
+    assert np.mean([r["n"] / r["n_scan"] for r in acc]) <= 1.25, msg
+    assert np.median([r["speedup"] for r in acc]) >= 4.0, msg
+    far = [r for r in acc if r["rw"] == 5.0 and r["n_plain"]]
+    near = [r for r in acc if r["rw"] == 0.2 and r["n_plain"]]
+    assert np.mean([r["n_plain"] / r["n"] for r in far]) >= 0.9, msg
+    assert max(r["n_plain"] / r["n"] for r in near) >= 1.5, msg
+
+
+def test_untrained_network_falls_back_to_the_plain_method(L):
+    """An untrained network proposes poles in the wrong places; the halving check rejects
+    its rule and the scanned rule is returned (the plain method as judge and fallback)."""
+    from yellowthinfilms_b200 import api
+    net = L.new_network(seed=9)
+    rng = np.random.default_rng(77)
+    st, lam = L.film_stack(rng)
+    k0 = 2 * np.pi / lam
+    G = _check_fn(api, st, k0)
+    k, w, info = L.learned_rule(net, st, k0, 1, h_min=80.0, rho_max=5 * lam, check=G)
+    ks, ws, _ = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=5 * lam)
+    if not info["learned"]:
+        assert np.array_equal(k, ks)
+    else:  # accepted only if it passed the check
+        assert np.linalg.norm(G(k, w) - G(*L.halved(st, k0, info["panels"], 8))) <= 1e-6 * np.linalg.norm(G(k, w))

@@ -243,3 +243,22 @@ def test_rotation_covariance(oracle):
             err = max(np.linalg.norm(GB[No - 1 - j, i, 0] - R @ GA[i, j, 0] @ R.T) for i in range(No) for j in range(No))
             worst = max(worst, err / max(np.linalg.norm(GA[i, j, 0]) for i in range(No) for j in range(No)))
     assert worst < 1e-10
+
+
+def test_mlp_reference_gradient_matches_finite_differences():
+    """The FP64 MLP restatement (the checker of the GPU training kernels) differentiates its
+    own loss correctly: central differences at unrounded weights."""
+    import ytf_mlp_ref as R
+    rng = np.random.default_rng(3)
+    sizes = [7, 9, 8, 2]
+    n = sum(sizes[i] * sizes[i + 1] + sizes[i + 1] for i in range(len(sizes) - 1))
+    p = rng.normal(0, 0.5, n)
+    X = rng.normal(0, 1, (5, 7))
+    T = np.stack([rng.normal(0, 1, 5), rng.uniform(0, 1, 5)], 1)
+    _, g = R.loss_and_grad(p, sizes, X, T, round_weights=False)
+    h = 1e-6
+    fd = np.zeros(n)
+    for i in range(n):
+        e = np.zeros(n); e[i] = h
+        fd[i] = (R.loss_and_grad(p + e, sizes, X, T, False)[0] - R.loss_and_grad(p - e, sizes, X, T, False)[0]) / (2 * h)
+    assert np.max(np.abs(fd - g)) < 1e-7 * max(1.0, np.max(np.abs(g)))

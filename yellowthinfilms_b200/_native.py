@@ -41,7 +41,7 @@ class GridInfo(ctypes.Structure):
     """ytf_grid_info (include/ytf.h)."""
     _fields_ = [("Kcut", ctypes.c_double), ("kmax", ctypes.c_double), ("n_panels", ctypes.c_long),
                 ("n_poles", ctypes.c_int), ("n_light_lines", ctypes.c_int), ("poles", (ctypes.c_double * 2) * 256),
-                ("light_lines", ctypes.c_double * 64)]
+                ("light_lines", ctypes.c_double * 64), ("panels", _d), ("panels_cap", ctypes.c_long)]
 
 
 # name -> (restype, argtypes); every symbol include/ytf.h declares
@@ -73,6 +73,20 @@ SIGNATURES = {
     "ytf_layer_light_lines": (ctypes.c_int, [_d, _d, ctypes.c_double, ctypes.c_double, _d, _i]),
     "ytf_nodes_1d": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams), ctypes.c_long, _d,
                                     _d, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(GridInfo)]),
+    "ytf_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _i, ctypes.c_ulonglong, ctypes.POINTER(_vp)]),
+    "ytf_mlp_destroy": (ctypes.c_int, [_vp]),
+    "ytf_mlp_last_error": (ctypes.c_char_p, [_vp]),
+    "ytf_mlp_num_params": (ctypes.c_long, [_vp]),
+    "ytf_mlp_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "ytf_mlp_params": (ctypes.c_int, [_vp, _vp, _vp]),
+    "ytf_mlp_forward": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int]),
+    "ytf_mlp_gradients": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float),
+                                         ctypes.c_int]),
+    "ytf_mlp_train": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                     ctypes.c_ulonglong, _vp]),
+    "ytf_nodes_from_poles": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams),
+                                            ctypes.c_int, _d, _d, ctypes.c_long, _d, _d, ctypes.POINTER(ctypes.c_long),
+                                            ctypes.POINTER(GridInfo)]),
     "ytf_transfer_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(TransferDesc), ctypes.POINTER(_vp)]),
     "ytf_green_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(GreenDesc)]),
     "ytf_gauss_legendre": (ctypes.c_int, [ctypes.c_int, _d, _d]),

@@ -298,23 +298,121 @@ def point_kx_grid(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=2
                   rtol=1e-6, ctx: Optional[Context] = None):
     """point_kx_grid (mod_ClosedFormGrid.jl:381-424) with the :fixed engine: (kx, wt, info).
     The pole scan's cavity responses are solved on the device; panels on the host; nodes by
-    the device Gauss–Legendre expansion."""
+    the device Gauss–Legendre expansion. ``poles``: (q, Γ) pairs to use instead of the scan
+    (ytf_nodes_from_poles)."""
+    return _grid(stack, omega, source_layer, h_min, rho_max, target_decay, kr_cap, scan, order, rtol, ctx, None)
+
+
+def _grid(stack, omega, source_layer, h_min, rho_max, target_decay, kr_cap, scan, order, rtol, ctx, poles):
     from ._native import GridInfo, GridParams
     st = _as_stack(stack, ctx)
     prm = GridParams(float(h_min), float(rho_max), float(target_decay), float(kr_cap), int(bool(scan)), int(order),
                      float(rtol))
     info = GridInfo()
     n = ctypes.c_long(0)
-    st.ctx.check(lib().ytf_nodes_1d(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm), 0, None, None,
-                                    ctypes.byref(n), ctypes.byref(info)))
+    if poles is None:
+        call = lambda cap, kp, wp: lib().ytf_nodes_1d(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm),
+                                                      cap, kp, wp, ctypes.byref(n), ctypes.byref(info))
+    else:
+        pq = _f64([p[0] for p in poles]) if len(poles) else np.zeros(1)
+        pg = _f64([p[1] for p in poles]) if len(poles) else np.zeros(1)
+        call = lambda cap, kp, wp: lib().ytf_nodes_from_poles(st.ctx.h, st.h, float(omega), int(source_layer),
+                                                              ctypes.byref(prm), len(poles), ptr(pq), ptr(pg), cap, kp,
+                                                              wp, ctypes.byref(n), ctypes.byref(info))
+    st.ctx.check(call(0, None, None))
     k = np.zeros(n.value)
     w = np.zeros(n.value)
-    st.ctx.check(lib().ytf_nodes_1d(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm), n.value, ptr(k),
-                                    ptr(w), ctypes.byref(n), ctypes.byref(info)))
+    pan = np.zeros(2 * max(1, info.n_panels))
+    info.panels = ptr(pan)
+    info.panels_cap = info.n_panels
+    st.ctx.check(call(n.value, ptr(k), ptr(w)))
     meta = dict(Kcut=info.Kcut, kmax=info.kmax, n_poles=info.n_poles, n_panels=info.n_panels,
+                panels=pan[:2 * info.n_panels].reshape(-1, 2).copy(),
                 poles=[(info.poles[i][0], info.poles[i][1]) for i in range(min(info.n_poles, 256))],
                 light_lines=[info.light_lines[i] for i in range(min(info.n_light_lines, 64))])
     return k, w, meta
+
+
+class MLP:
+    """The node-placement MLP on the device (ytf_mlp_*): widths sizes[0] -> ... -> 2, GELU
+    between layers, BF16 weights with FP32 accumulation, trained by libytf's own forward,
+    backward and Adam kernels."""
+
+    def __init__(self, sizes=(154, 256, 256, 256, 256, 2), seed=0, device=0):
+        self.sizes = [int(x) for x in sizes]
+        arr = np.asarray(self.sizes, np.int32)
+        h = ctypes.c_void_p()
+        rc = lib().ytf_mlp_create(int(device), len(self.sizes) - 1, ptr(arr, _i), ctypes.c_ulonglong(seed),
+                                  ctypes.byref(h))
+        if rc != 0:
+            raise YTFError(f"ytf_mlp_create failed ({rc})")
+        self.h = h
+        self.nparam = int(lib().ytf_mlp_num_params(h))
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and _native._lib is not None:
+            _native._lib.ytf_mlp_destroy(self.h)
+            self.h = None
+
+    def _check(self, rc):
+        if rc != 0:
+            raise YTFError(lib().ytf_mlp_last_error(self.h).decode())
+
+    def set_stream(self, stream_handle):
+        self._check(lib().ytf_mlp_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    @property
+    def params(self):
+        p = np.zeros(self.nparam, np.float32)
+        self._check(lib().ytf_mlp_params(self.h, p.ctypes.data_as(ctypes.c_void_p), None))
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparam
+        self._check(lib().ytf_mlp_params(self.h, None, p.ctypes.data_as(ctypes.c_void_p)))
+
+    def forward(self, X):
+        """Outputs [B, 2] for inputs X [B, sizes[0]] (numpy, or a CUDA float32 tensor)."""
+        if hasattr(X, "is_cuda") and X.is_cuda:
+            import torch
+            out = torch.empty((X.shape[0], 2), dtype=torch.float32, device=X.device)
+            self._check(lib().ytf_mlp_forward(self.h, X.shape[0], ctypes.c_void_p(X.data_ptr()),
+                                              ctypes.c_void_p(out.data_ptr()), 1))
+            return out
+        X = np.ascontiguousarray(X, np.float32)
+        out = np.zeros((X.shape[0], 2), np.float32)
+        self._check(lib().ytf_mlp_forward(self.h, X.shape[0], X.ctypes.data_as(ctypes.c_void_p),
+                                          out.ctypes.data_as(ctypes.c_void_p), 0))
+        return out
+
+    def gradients(self, X, T):
+        """(loss, gradient of the loss w.r.t. the parameter vector) for one batch (numpy)."""
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        g = np.zeros(self.nparam, np.float32)
+        loss = ctypes.c_float(0)
+        self._check(lib().ytf_mlp_gradients(self.h, X.shape[0], X.ctypes.data_as(ctypes.c_void_p),
+                                            T.ctypes.data_as(ctypes.c_void_p), g.ctypes.data_as(ctypes.c_void_p),
+                                            ctypes.byref(loss), 0))
+        return float(loss.value), g
+
+    def train(self, X, T, batch=4096, steps=100, lr=1e-3, seed=1, record=True):
+        """Adam steps on mini-batches of the device-resident set X [n, d], T [n, 2] (CUDA float32
+        tensors). Returns the per-step mini-batch losses (numpy) when ``record``."""
+        losses = np.zeros(steps, np.float32) if record else None
+        self._check(lib().ytf_mlp_train(self.h, X.shape[0], ctypes.c_void_p(X.data_ptr()),
+                                        ctypes.c_void_p(T.data_ptr()), int(batch), int(steps), float(lr),
+                                        ctypes.c_ulonglong(seed),
+                                        losses.ctypes.data_as(ctypes.c_void_p) if record else None))
+        return losses
+
+
+def grid_from_poles(stack, omega, source_layer, poles, h_min, rho_max=0.0, target_decay=25.0, kr_cap=0.0, order=8,
+                    rtol=1e-6, ctx: Optional[Context] = None):
+    """The point rule with given real-axis poles (q, Γ) instead of the scan (ytf_nodes_from_poles)."""
+    return _grid(stack, omega, source_layer, h_min, rho_max, target_decay, kr_cap, False, order, rtol, ctx, list(poles))
 
 
 def build_cavity_transfer_batch(items, ctx: Optional[Context] = None):

@@ -678,8 +678,9 @@ int ytf_layer_light_lines(const double* eps, const double* mu, double omega, dou
   return YTF_OK;
 }
 
-int ytf_nodes_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm, long cap,
-                 double* k, double* w, long* n, ytf_grid_info* info) {
+static int nodes_1d_impl(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm,
+                         int npoles, const double* pq, const double* pG, long cap, double* k, double* w, long* n,
+                         ytf_grid_info* info) {
   if (!ctx || !prm || !n) return YTF_ERR_ARG;
   if (!st) return fail(ctx, YTF_ERR_ARG, "point_kx_grid: stack is NULL");
   if (st->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "point_kx_grid: stack belongs to another context");
@@ -700,8 +701,14 @@ int ytf_nodes_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_lay
   };
   grid::Features F;
   int rc = grid::features_1d(eps, mu, omega, prm->h_min, prm->rho_max, prm->target_decay, prm->kr_cap, 1e5,
-                             prm->scan != 0, 1e-3, 1.05, f, F);
+                             npoles < 0 && prm->scan != 0, 1e-3, 1.05, f, F);
   if (rc) return rc;
+  if (npoles >= 0) {  // poles proposed by the caller instead of the scan
+    F.poles.clear();
+    for (int i = 0; i < npoles; ++i)
+      if (pq[i] > 0 && pG[i] > 0 && pq[i] < F.Kcut) F.poles.push_back({pq[i], pG[i], 0.0, 0.0});
+    F.cl = grid::clusters(F.poles, 0.0);
+  }
   std::vector<std::pair<double, double>> panels;
   try {
     panels = grid::fixed_kr_panels(F, prm->order, prm->rtol, 0.5, 12, 0.05, 4.0, 4.0, 0.5);
@@ -711,7 +718,13 @@ int ytf_nodes_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_lay
   const long tot = (long)panels.size() * prm->order;
   *n = tot;
   if (info) {
+    double* pan = info->panels;
+    const long pcap = info->panels_cap;
     std::memset(info, 0, sizeof(*info));
+    info->panels = pan;
+    info->panels_cap = pcap;
+    if (pan && pcap >= (long)panels.size())
+      for (size_t i = 0; i < panels.size(); ++i) { pan[2 * i] = panels[i].first; pan[2 * i + 1] = panels[i].second; }
     info->Kcut = F.Kcut;
     info->kmax = F.kmax;
     info->n_panels = (long)panels.size();
@@ -731,6 +744,18 @@ int ytf_nodes_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_lay
   for (size_t i = 0; i < panels.size(); ++i) { pa[i] = panels[i].first; pb[i] = panels[i].second; }
   return ytf_gl_rule(ctx, (int)panels.size(), pa.data(), pb.data(), prm->order, (int)F.singular_lines.size(),
                      F.singular_lines.data(), k, w);
+}
+
+int ytf_nodes_1d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm, long cap,
+                 double* k, double* w, long* n, ytf_grid_info* info) {
+  return nodes_1d_impl(ctx, st, omega, source_layer, prm, -1, nullptr, nullptr, cap, k, w, n, info);
+}
+
+int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm,
+                         int npoles, const double* q, const double* G, long cap, double* k, double* w, long* n,
+                         ytf_grid_info* info) {
+  if (npoles < 0 || (npoles > 0 && (!q || !G))) return YTF_ERR_ARG;
+  return nodes_1d_impl(ctx, st, omega, source_layer, prm, npoles, q, G, cap, k, w, n, info);
 }
 
 int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cache** out) {

@@ -1,0 +1,224 @@
+"""Learned node placement for the Sommerfeld k-quadrature (no counterpart in the reference).
+
+The reference places its point-rule nodes from a scan of the source layer's cavity response
+along the real kρ axis (kspace_features / real_axis_poles, mod_KSpaceFeatures.jl:151-360):
+thousands of full stack solves, then golden-section and bisection refinements per peak. Here
+a small MLP (libytf's ytf_mlp: 154 -> 256 x4 -> 2, GELU, BF16 weights, FP32 accumulation,
+trained by libytf's own kernels) predicts that scanned curve — log R(k) and a pole-proximity
+score — from a stack descriptor, the frequency and k. Its peaks are candidate poles; one
+batched device call samples the EXACT response on a small window around every candidate,
+which fixes each pole's (q, Γ) for fixed_kρ_rule (ytf_nodes_from_poles) in place of the
+scan's thousands of samples and sequential refinement rounds. Every node of the resulting
+rule is then solved exactly by the transfer path. The plain method stays the judge and the fallback: a
+proposed rule is accepted only if it agrees with its own refinement (every panel halved) to
+the requested tolerance; otherwise the scanned rule is used.
+
+Training data come from the solver itself: random stacks of the air / uniaxial film /
+substrate form, each scanned on a log kρ grid by ytf_cavity_response on the device.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import api
+from .materials import FlatOpticalLayer, IsotropicMaterial, UniaxialMaterial, stack_arrays
+
+MAX_LAYERS = 8
+N_FEATURES = MAX_LAYERS * 19 + 2  # 154
+LAMBDA_REF = 600.0                 # nm: frequency feature = λ_ref / λ
+K_LO, K_HI = 0.25, 20.0            # scan range in units of k0
+LOG_SCALE = 4.0                    # target 0 = log R / LOG_SCALE
+
+
+def film_stack(rng, lam=None):
+    """A random stack of the air / uniaxial film / substrate form (nm): the film has
+    εo = -U[1, 6] + i 10^U[-2.5, -0.3], εe = U[2, 6] + i 10^U[-2.7, -0.5] (losses from sharp to
+    broad guided modes), d U[20, 100]; the substrate ε U[1.5, 4]; air is 200 nm above the
+    film. Returns (stack, λ)."""
+    if lam is None:
+        lam = float(rng.uniform(450.0, 750.0))
+    eo = complex(-rng.uniform(1.0, 6.0), 10 ** rng.uniform(-2.5, -0.3))
+    ee = complex(rng.uniform(2.0, 6.0), 10 ** rng.uniform(-2.7, -0.5))
+    st = [FlatOpticalLayer(IsotropicMaterial(1.0), 200.0),
+          FlatOpticalLayer(UniaxialMaterial(eo, ee), float(rng.uniform(20.0, 100.0))),
+          FlatOpticalLayer(IsotropicMaterial(float(rng.uniform(1.5, 4.0))), 100.0)]
+    return st, lam
+
+
+def scan_grid(k0, n):
+    """n log-spaced kρ over [K_LO, K_HI] k0."""
+    return k0 * np.exp(np.linspace(np.log(K_LO), np.log(K_HI), n))
+
+
+def features(stack, k0, ks):
+    """[len(ks), 154] float32: per layer (up to 8) Re and Im of the 9 ε entries / 10 and the
+    thickness in wavelengths; then λ_ref / λ and k / (K_HI k0)."""
+    _, _, eps, _, d = stack_arrays(stack)
+    row = np.zeros(N_FEATURES)
+    for l in range(min(len(stack), MAX_LAYERS)):
+        row[19 * l:19 * l + 9] = eps[l].real / 10.0
+        row[19 * l + 9:19 * l + 18] = eps[l].imag / 10.0
+        row[19 * l + 18] = d[l] * k0 / (2 * np.pi)
+    row[-2] = k0 * LAMBDA_REF / (2 * np.pi)
+    X = np.repeat(row[None, :], len(ks), axis=0)
+    X[:, -1] = np.asarray(ks) / (K_HI * k0)
+    return X.astype(np.float32)
+
+
+def peaks(ks, logR, prominence=np.log(1.05), floor_rel=1e-6):
+    """Peaks of a sampled log-response (the scan's rule of real_axis_poles on samples): local
+    maxima with prominence, position by a parabola through the three samples in log k, width
+    Γ from the nearer half-power crossing (linear interpolation). Returns [(q, Γ)]."""
+    y = np.asarray(logR, np.float64)
+    n = len(y)
+    if n < 3:
+        return []
+    ymin = max(y.max() + np.log(floor_rel), np.log(1e-10))
+    lk = np.log(ks)
+    step = lk[1] - lk[0]
+    W = int(np.ceil(np.log(4.0) / step))
+    out = []
+    for i in range(1, n - 1):
+        if not (y[i] > y[i - 1] and y[i] >= y[i + 1] and y[i] >= ymin):
+            continue
+        lo, hi = max(0, i - W), min(n - 1, i + W)
+        jl = i
+        while jl > lo and y[jl - 1] <= y[i]:
+            jl -= 1
+        jr = i
+        while jr < hi and y[jr + 1] <= y[i]:
+            jr += 1
+        base = max(y[jl:i + 1].min(), y[i:jr + 1].min())
+        if y[i] - base < prominence:
+            continue
+        den = y[i - 1] - 2 * y[i] + y[i + 1]
+        off = 0.5 * (y[i - 1] - y[i + 1]) / den if den < 0 else 0.0
+        q = float(np.exp(lk[i] + np.clip(off, -0.5, 0.5) * step))
+        P = np.exp(y[i])
+        lvl = np.log(np.exp(base) + (P - np.exp(base)) / np.sqrt(2.0))
+        G = np.inf
+        for rng_ in (range(i, jl - 1, -1), range(i, jr + 1)):
+            prev = None
+            for j in rng_:
+                if y[j] <= lvl and prev is not None:
+                    t = (y[prev] - lvl) / (y[prev] - y[j])
+                    kc = np.exp(lk[prev] + t * (lk[j] - lk[prev]))
+                    G = min(G, abs(kc - q))
+                    break
+                prev = j
+        if np.isfinite(G) and G > 0:
+            out.append((q, float(G)))
+    return out
+
+
+def pole_score(ks, poles):
+    """Pole-proximity score: max over poles of exp(-((k - q) / (2Γ))²)."""
+    s = np.zeros(len(ks))
+    for q, G in poles:
+        s = np.maximum(s, np.exp(-((np.asarray(ks) - q) / (2 * G)) ** 2))
+    return s
+
+
+def training_set(n_stacks, n_k=2048, seed=0, ctx=None):
+    """(X [n_stacks n_k, 154], T [n_stacks n_k, 2]) from device scans of random film stacks
+    (source in the air layer)."""
+    rng = np.random.default_rng(seed)
+    Xs, Ts = [], []
+    for _ in range(n_stacks):
+        st, lam = film_stack(rng)
+        k0 = 2 * np.pi / lam
+        ks = scan_grid(k0, n_k)
+        R = api.cavity_response(st, k0, 1, ks, ctx=ctx)
+        logR = np.log(np.maximum(R, 1e-12))
+        Xs.append(features(st, k0, ks))
+        Ts.append(np.stack([logR / LOG_SCALE, pole_score(ks, peaks(ks, logR))], 1).astype(np.float32))
+    return np.concatenate(Xs), np.concatenate(Ts)
+
+
+def new_network(seed=0, device=0):
+    return api.MLP((N_FEATURES, 256, 256, 256, 256, 2), seed=seed, device=device)
+
+
+def train(net, X, T, steps, batch=4096, lr=1e-3, seed=1):
+    """Adam on the device-resident set; returns the mini-batch losses."""
+    import torch
+    Xd = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+    Td = torch.from_numpy(np.ascontiguousarray(T)).cuda()
+    losses = net.train(Xd, Td, batch=batch, steps=steps, lr=lr, seed=seed)
+    torch.cuda.synchronize()
+    return losses
+
+
+def propose_poles(net, stack, k0, n_k=4096):
+    """Candidate real-axis poles (q, Γ) from the network: peaks of its predicted response and
+    maxima of its pole score (> 0.3) on a fine log grid."""
+    ks = scan_grid(k0, n_k)
+    out = net.forward(features(stack, k0, ks)).astype(np.float64)
+    cand = peaks(ks, out[:, 0] * LOG_SCALE)
+    s = 1.0 / (1.0 + np.exp(-out[:, 1]))
+    for i in range(1, len(ks) - 1):
+        if s[i] > 0.3 and s[i] >= s[i - 1] and s[i] > s[i + 1]:
+            if all(abs(ks[i] - q) > 2 * G for q, G in cand):
+                cand.append((float(ks[i]), float(ks[i] * 2e-3)))
+    return sorted(cand)
+
+
+def refine_poles(stack, k0, source_layer, cand, n_local=129, ctx=None):
+    """(q, Γ) of each candidate from the EXACT cavity response sampled on a small log window
+    around it (±6 max(Γ/q, 2e-3)), all windows in one device call; candidates whose window
+    shows no peak are dropped."""
+    if not cand:
+        return []
+    wins = []
+    for q, G in cand:
+        w = max(G / q, 2e-3)
+        wins.append(q * np.exp(np.linspace(-6 * w, 6 * w, n_local)))
+    R = api.cavity_response(stack, k0, source_layer, np.concatenate(wins), ctx=ctx)
+    out = []
+    for i, ks in enumerate(wins):
+        y = np.log(np.maximum(R[i * n_local:(i + 1) * n_local], 1e-12))
+        pk = peaks(ks, y)
+        if pk:
+            out.append(max(pk, key=lambda qg: y[np.searchsorted(ks, qg[0]) - 1]))
+    out.sort()
+    merged = []
+    for q, G in out:  # windows of neighbouring candidates may find the same pole
+        if merged and abs(q - merged[-1][0]) <= 1e-6 * q:
+            continue
+        merged.append((q, G))
+    return merged
+
+
+def halved(stack, omega, panels, order):
+    """The rule on the same panels split in two (the acceptance check), with the u²
+    substitution at the half-space light lines as the original rule."""
+    sing = sorted(set(api.layer_light_lines(stack[0], omega)) | set(api.layer_light_lines(stack[-1], omega)))
+    p2 = api.halve_panels([tuple(p) for p in panels])
+    return api.gl_rule(p2, order, singular=sing)
+
+
+def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol=1e-6, check=None, ctx=None):
+    """The learned point rule with the plain method as judge and fallback.
+
+    Proposes poles with the network, builds fixed_kρ_rule on them, and — if ``check`` is a
+    callable rule -> G — accepts the rule only when G agrees with the halved rule to rtol;
+    otherwise returns the scanned rule. Returns (k, w, info) with info["learned"] True/False."""
+    poles = refine_poles(stack, k0, source_layer, propose_poles(net, stack, k0), ctx=ctx)
+    k, w, info = api.grid_from_poles(stack, k0, source_layer, poles, h_min=h_min, rho_max=rho_max, order=order,
+                                     rtol=rtol, ctx=ctx)
+    info = dict(info, learned=True, proposed_poles=poles)
+    if check is not None:
+        G = check(k, w)
+        kh, wh = halved(stack, k0, info["panels"], order)
+        Gh = check(kh, wh)
+        if not (np.linalg.norm(G - Gh) <= rtol * np.linalg.norm(Gh)):
+            k, w, info = api.point_kx_grid(stack, k0, source_layer, h_min=h_min, rho_max=rho_max, order=order,
+                                           rtol=rtol, ctx=ctx)
+            info = dict(info, learned=False, proposed_poles=poles)
+    return k, w, info
+
+
+def uniform_rule(k0, kmax, npanels, order=8):
+    """The plain fixed grid: npanels equal Gauss-Legendre panels on [0, kmax]."""
+    edges = np.linspace(0.0, kmax, npanels + 1)
+    return api.gl_rule(list(zip(edges[:-1], edges[1:])), order)
