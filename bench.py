@@ -490,6 +490,113 @@ def run_uneven(args):
     return 0
 
 
+def run_learned(args):
+    """Learned adaptive quadrature vs the plain fixed rule (one GPU): train the node-placement
+    MLP on 1e7 solver samples, then for held-out film stacks compare the time to a G accurate to
+    1e-6 (rule construction, every exact solve, the synthesis and the acceptance check; the plain
+    rule halves until it passes) against a converged reference."""
+    import torch
+    from yellowthinfilms_b200 import api
+    from yellowthinfilms_b200 import learned as L
+    torch.cuda.set_device(0)
+    n_train, n_k, n_test = 4883, 2048, int(os.environ.get("YTF_LEARNED_TEST_STACKS", "48"))
+    t = time.perf_counter()
+    X, T = L.training_set(n_train, n_k=n_k, seed=SEED)
+    t_data = time.perf_counter() - t
+    net = L.new_network(seed=SEED)
+    steps, batch = 2 * len(X) // 8192, 8192
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    Xd = torch.from_numpy(X).cuda()
+    Td = torch.from_numpy(T).cuda()
+    del X, T
+    torch.cuda.synchronize()
+    e0.record()
+    losses = net.train(Xd, Td, batch=batch, steps=steps, lr=1e-3, seed=SEED)
+    e1.record()
+    torch.cuda.synchronize()
+    t_train = e0.elapsed_time(e1) * 1e-3
+    del Xd, Td
+    rng = np.random.default_rng(SEED + 5)
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        r = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(b) * 1e-3
+
+    res = {}
+    for rw in (0.2, 5.0):
+        res[rw] = dict(entries=0, t_plain=0.0, t_learned=0.0, n_plain=[], n_learned=[], accepted=0, err=0.0)
+    for _ in range(n_test):
+        st, lam = L.film_stack(rng)
+        k0 = 2 * np.pi / lam
+        for rw in (0.2, 5.0):
+            rho = np.exp(np.linspace(np.log(0.01 * lam), np.log(rw * lam), 16))
+            z = np.linspace(60.0, 200.0, 6)
+
+            def G(k, w):
+                c = api.build_cavity_transfer_1d(st, k0, 1, k, w, obs_layers=[1])
+                return api.closed_form_G(c, 1, 20.0, z, rho, [0.0], terms="scattered")
+            kr, wr, ir = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rw * lam, rtol=1e-10)
+            Gref = G(*L.halved(st, k0, ir["panels"], 8))
+
+            def plain():
+                k, w, info = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rw * lam, scan=False)
+                panels = info["panels"]
+                sing = sorted(set(api.layer_light_lines(st[0], k0)) | set(api.layer_light_lines(st[-1], k0)))
+                Gk = G(k, w)
+                for _ in range(8):
+                    panels = api.halve_panels([tuple(p) for p in panels])
+                    kh, wh = api.gl_rule(panels, 8, singular=sing)
+                    Gh = G(kh, wh)
+                    if np.linalg.norm(Gk - Gh) <= 1e-6 * np.linalg.norm(Gh):
+                        return Gk, len(k)
+                    k, w, Gk = kh, wh, Gh
+                return Gk, len(k)
+
+            def learned():
+                k, w, info = L.learned_rule(net, st, k0, 1, h_min=80.0, rho_max=rw * lam, check=G)
+                return info["G"], len(k), info["learned"]
+
+            (Gp, npl), tp = timed(plain)
+            (Gl, nle, acc), tl = timed(learned)
+            r = res[rw]
+            r["entries"] += Gref.size
+            r["t_plain"] += tp
+            r["t_learned"] += tl
+            r["n_plain"].append(npl)
+            r["n_learned"].append(nle)
+            r["accepted"] += int(acc)
+            r["err"] = max(r["err"], float(np.linalg.norm(Gl - Gref) / np.linalg.norm(Gref)),
+                           float(np.linalg.norm(Gp - Gref) / np.linalg.norm(Gref)))
+    near = res[0.2]
+    line = {"metric": METRIC, "value": near["entries"] / near["t_learned"], "unit": "entries/s", "n_gpus": 1,
+            "steps": n_test, "warmup": 0, "ms_per_step": 1e3 * near["t_learned"] / n_test, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve and synthesis; MLP bf16 weights, fp32 accum",
+            "data": "synthetic (seeded)", "impl": "learned-adaptive",
+            "config": {"workload": "learned adaptive quadrature: air / uniaxial film / substrate stacks, vertical dipole "
+                                   "20 nm above the film, 16 ρ x 6 heights (60-200 nm) x 9 components, scattered term",
+                       "train_samples": n_train * n_k, "train_steps": steps, "batch": batch, "held_out_stacks": n_test,
+                       "tolerance": 1e-6},
+            "plain_entries_per_s": near["entries"] / near["t_plain"],
+            "learned_vs_plain": near["t_plain"] / near["t_learned"],
+            "max_rel_err_vs_reference": max(r["err"] for r in res.values()),
+            "regimes": {f"rho_max {rw} lambda": {"learned_entries_per_s": r["entries"] / r["t_learned"],
+                                                "plain_entries_per_s": r["entries"] / r["t_plain"],
+                                                "learned_vs_plain": r["t_plain"] / r["t_learned"],
+                                                "mean_nodes_learned": float(np.mean(r["n_learned"])),
+                                                "mean_nodes_plain": float(np.mean(r["n_plain"])),
+                                                "accepted": r["accepted"], "stacks": n_test}
+                        for rw, r in res.items()},
+            "training": {"data_s": t_data, "train_s": t_train, "first_loss": float(losses[0]),
+                         "last_loss": float(np.mean(losses[-50:]))}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -497,8 +604,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-check", action="store_true")
-    ap.add_argument("--workload", default="gyro32", choices=["gyro32", "uneven"],
-                    help="gyro32: the 8-layer stack at 32 wavelengths (default); uneven: 1024 uneven stacks")
+    ap.add_argument("--workload", default="gyro32", choices=["gyro32", "uneven", "learned"],
+                    help="gyro32: the 8-layer stack at 32 wavelengths (default); uneven: 1024 uneven stacks; "
+                         "learned: learned adaptive quadrature vs the plain fixed rule")
     ap.add_argument("--per-call", action="store_true",
                     help="one build + synthesis call per wavelength instead of the batched calls")
     ap.add_argument("--precision", default="int8x3", choices=list(DTYPE),
@@ -509,6 +617,8 @@ def main():
         return run_reference(args)
     if args.workload == "uneven":
         return run_uneven(args)
+    if args.workload == "learned":
+        return run_learned(args)
     return run_ours(args)
 
 

@@ -11,7 +11,8 @@ which fixes each pole's (q, Γ) for fixed_kρ_rule (ytf_nodes_from_poles) in pla
 scan's thousands of samples and sequential refinement rounds. Every node of the resulting
 rule is then solved exactly by the transfer path. The plain method stays the judge and the fallback: a
 proposed rule is accepted only if it agrees with its own refinement (every panel halved) to
-the requested tolerance; otherwise the scanned rule is used.
+the requested tolerance; otherwise the plain method refines it by halving until two levels
+agree (and the scanned rule is the last resort).
 
 Training data come from the solver itself: random stacks of the air / uniaxial film /
 substrate form, each scanned on a log kρ grid by ytf_cavity_response on the device.
@@ -197,24 +198,37 @@ def halved(stack, omega, panels, order):
     return api.gl_rule(p2, order, singular=sing)
 
 
-def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol=1e-6, check=None, ctx=None):
+def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol=1e-6, check=None, max_halvings=6,
+                 ctx=None):
     """The learned point rule with the plain method as judge and fallback.
 
-    Proposes poles with the network, builds fixed_kρ_rule on them, and — if ``check`` is a
-    callable rule -> G — accepts the rule only when G agrees with the halved rule to rtol;
-    otherwise returns the scanned rule. Returns (k, w, info) with info["learned"] True/False."""
+    Proposes poles with the network, fixes them with one exact batched sampling, and builds
+    fixed_kρ_rule on them. With ``check`` (a callable rule -> G) the rule is accepted when G
+    agrees with G on the halved rule to rtol; otherwise the plain method takes over: the rule
+    is halved again until two successive levels agree (at most max_halvings times), and if
+    they never do, the scanned rule is returned. Returns (k, w, info): info["learned"] is True
+    when the proposed rule itself was accepted, info["halvings"] counts the plain refinements,
+    info["G"] is G on the returned rule when ``check`` was given."""
     poles = refine_poles(stack, k0, source_layer, propose_poles(net, stack, k0), ctx=ctx)
     k, w, info = api.grid_from_poles(stack, k0, source_layer, poles, h_min=h_min, rho_max=rho_max, order=order,
                                      rtol=rtol, ctx=ctx)
-    info = dict(info, learned=True, proposed_poles=poles)
-    if check is not None:
-        G = check(k, w)
-        kh, wh = halved(stack, k0, info["panels"], order)
+    info = dict(info, learned=True, halvings=0, proposed_poles=poles)
+    if check is None:
+        return k, w, info
+    sing = sorted(set(api.layer_light_lines(stack[0], k0)) | set(api.layer_light_lines(stack[-1], k0)))
+    panels = info["panels"]
+    G = check(k, w)
+    for h in range(max_halvings + 1):
+        panels2 = api.halve_panels([tuple(p) for p in panels])
+        kh, wh = api.gl_rule(panels2, order, singular=sing)
         Gh = check(kh, wh)
-        if not (np.linalg.norm(G - Gh) <= rtol * np.linalg.norm(Gh)):
-            k, w, info = api.point_kx_grid(stack, k0, source_layer, h_min=h_min, rho_max=rho_max, order=order,
-                                           rtol=rtol, ctx=ctx)
-            info = dict(info, learned=False, proposed_poles=poles)
+        if np.linalg.norm(G - Gh) <= rtol * np.linalg.norm(Gh):
+            info.update(learned=h == 0, halvings=h, G=G, panels=np.asarray(panels))
+            return k, w, info
+        panels, k, w, G = panels2, kh, wh, Gh
+    k, w, info2 = api.point_kx_grid(stack, k0, source_layer, h_min=h_min, rho_max=rho_max, order=order, rtol=rtol,
+                                    ctx=ctx)
+    info.update(info2, learned=False, halvings=max_halvings + 1, G=check(k, w))
     return k, w, info
 
 
