@@ -106,6 +106,49 @@ def test_green_1d_matches_oracle(ytf, oracle, idx):
                 assert relerr(G, Go) < 1e-10, (src, obs, terms, relerr(G, Go))
 
 
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_green_1d_int8_tensor_cores_match_fp64(ytf, oracle, idx):
+    """The 1D Bessel contraction on the int8 tensor cores (J_n(kρ) and the coefficient
+    columns in three fixed-point digits, exact INT32 accumulation) against the FP64 path and
+    the oracle, every source/obs layer and term selection: ≤ 1e-6 relative."""
+    _, st = FOUNDATION_STACKS[idx]
+    kx, wt = krho_grid(st, W, kmax=15.0)
+    xs = np.array([-0.3, 0.0, 0.2, 0.45])
+    ys = np.array([0.0, 0.15, -0.25])
+    N = len(st)
+    for src in range(1, N):
+        gc = ytf.build_cavity_transfer_1d(st, W, src, kx, wt)
+        zs = 0.4 * st[src - 1].d
+        for obs in range(1, N + 1):
+            d = st[obs - 1].d
+            zo = [0.1 * d, 0.4 * d, 0.75 * d] if obs != src else [0.05 * d, 0.4 * d, 0.95 * d]
+            for terms in (["all", "scattered", "toeplitz"] if obs == src else ["all"]):
+                G64 = ytf.closed_form_G(gc, obs, zs, zo, xs, ys, terms=terms)
+                G8 = ytf.closed_form_G(gc, obs, zs, zo, xs, ys, terms=terms, precision="int8x3")
+                assert relerr(G8, G64) < 1e-6, (src, obs, terms, relerr(G8, G64))
+    oc = oracle.build_cavity_transfer_1d(st, W, 1, kx, wt)
+    gc = ytf.build_cavity_transfer_1d(st, W, 1, kx, wt)
+    zo = [0.2 * st[0].d, 0.7 * st[0].d]
+    assert relerr(ytf.closed_form_G(gc, 1, 0.4 * st[0].d, zo, xs, ys, precision="int8x3"),
+                  oracle.closed_form_G(oc, 1, 0.4 * st[0].d, zo, xs, ys)) < 1e-6
+
+
+def test_green_1d_int8_many_radii_nodes_and_rows(ytf):
+    """The int8 Bessel contraction with several radius tiles (~300 distinct radii), node
+    slices (40000 nodes) and column tiles (20 z rows: 200 order-0 columns > 160): ≤ 1e-6."""
+    st = config1_stack()
+    k0 = 2 * np.pi / 600.0
+    panels = [(20 * k0 * i / 5000, 20 * k0 * (i + 1) / 5000) for i in range(5000)]
+    kx, wt = ytf.gl_rule(panels, 8)
+    gc = ytf.build_cavity_transfer_1d(st, k0, 1, kx, wt, obs_layers=[1])
+    rho = np.geomspace(6.0, 3000.0, 300)
+    zo = np.linspace(30.0, 190.0, 20)
+    G64 = ytf.closed_form_G(gc, 1, 20.0, zo, rho, [0.0], terms="scattered")
+    G8 = ytf.closed_form_G(gc, 1, 20.0, zo, rho, [0.0], terms="scattered", precision="int8x3")
+    assert relerr(G8, G64) < 1e-6, relerr(G8, G64)
+    assert relerr(G8[..., 2, 2], G64[..., 2, 2]) < 1e-6
+
+
 def test_config1_gzz_1d_matches_oracle(ytf, oracle):
     """Vertical dipole 20 nm above the uniaxial film, real-axis GL panels to 20 k0."""
     st = config1_stack()

@@ -1,0 +1,357 @@
+// ytf_bessel_i8.cu -- the 1D Bessel synthesis contraction on the int8 tensor cores.
+//
+// closed_form_G for 1D caches (mod_ClosedFormField.jl:435-487) contracts, per Bessel order n,
+//   P_n[r][c] = Σ_k J_n(k_k ρ_r) C_n[c][k]
+// (C_n: the real and imaginary parts of the order's coefficient columns, k_coef1d). Both
+// operands are fixed point in three signed base-256 digits, as in the 2D lateral kernel:
+//   J: X = rint(8355000 J)            (|J_n| ≤ 1: one scale for every entry)
+//   C: Y = rint(8355000 C / max|C|)   per (node slice, column)
+// and the six digit products of weight ≥ 256² are summed exactly in INT32 in tensor memory.
+// Unlike the lateral kernel, both operands are prepared once per launch as the exact shared-
+// memory image of each 64-node stage (k_aimg_bessel evaluates J_n straight into digits; no
+// FP64 table), so the contraction kernel only streams images: warp 0 issues the two bulk
+// copies of a stage (one mbarrier, byte-counted), one thread of warp 1 issues the 12 MMAs
+// (6 digit products x 2 K-halves; M=128 radii, N ≤ 160 columns, K=32), warps 2-5 read the
+// accumulators at the end.
+// INT32 headroom: |level-2 sum| ≤ (127·128 + 128·128 + 128·127) K ≤ 48896 · 16384 < 2^30.
+#include "ytf_complex.cuh"
+#include "ytf_kernels.h"
+#include "ytf_tcgen05.cuh"
+
+namespace ytf {
+
+constexpr int BI_M = 128;
+constexpr int BI_NODES = 64;  // nodes per stage: one byte each, 64-byte rows (2 MMAs of K = 32)
+constexpr int BI_STAGES = 4;
+constexpr int BI_THREADS = 192;
+constexpr int BI_ACC_STRIDE = 160;
+constexpr int BI_TMEM_COLS = 512;
+constexpr long BI_WAIT_LIMIT = 1L << 22;
+constexpr double BI_SCALE = 8355000.0;
+
+size_t bessel_i8_stage_bytes_a() { return 3ul * BI_M * 64; }
+size_t bessel_i8_stage_bytes_b(int Np) { return 3ul * (size_t)Np * 64; }
+size_t bessel_i8_smem(int Np) {
+  return (size_t)BI_STAGES * (bessel_i8_stage_bytes_a() + bessel_i8_stage_bytes_b(Np)) + 128;
+}
+int bessel_i8_ctile(int N) {
+  int nt = (N + 159) / 160;
+  return (N + nt - 1) / nt;
+}
+
+// J_0, J_1 (the CUDA math library), J_2 by its power series below |x| = 1 (A&S 9.1.10; exact
+// 0 at x = 0) and the three-term recurrence above (A&S 9.1.27), as k_bessel
+__device__ __forceinline__ double bessel_j012(int order, double x) {
+  if (order == 0) return j0(x);
+  if (order == 1) return j1(x);
+  if (fabs(x) < 1.0) {
+    double h2 = 0.25 * x * x, t = 0.5 * h2, s = t;
+    for (int m = 0; m < 12; ++m) {
+      t *= -h2 / ((m + 1.0) * (m + 3.0));
+      s += t;
+    }
+    return s;
+  }
+  return (2.0 / x) * j1(x) - j0(x);
+}
+
+__device__ __forceinline__ void digits3b(int Y, uint32_t& d0, uint32_t& d1, uint32_t& d2) {
+  d2 = (uint32_t)Y & 255u;
+  d1 = (uint32_t)((Y + 128) >> 8) & 255u;
+  d0 = (uint32_t)((Y + 32896) >> 16) & 255u;
+}
+
+__device__ __forceinline__ double col_scale(unsigned long long bits) {
+  const double m = __longlong_as_double((long long)bits);
+  return (m > 0.0 && isfinite(m)) ? BI_SCALE / m : 0.0;
+}
+
+// per (slice, column) max |C| as IEEE bits (Inf for a non-finite entry)
+__global__ void k_bcolmax(BesselI8 p) {
+  const int col = blockIdx.x, z = blockIdx.y;
+  const long k0 = (long)z * p.kchunk, k1 = min(p.K, k0 + p.kchunk);
+  const double* c = p.C + (long)col * p.K;
+  double m = 0.0;
+  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    const double v = c[k];
+    m = isfinite(v) ? fmax(m, fabs(v)) : __longlong_as_double(0x7ff0000000000000LL);
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) p.colmax[(long)z * p.N + col] = (unsigned long long)__double_as_longlong(red[0]);
+}
+
+// one thread per (column tile, row slot, slice, 16-node group): 16 bytes of each digit plane
+__global__ void k_bimg_real(BesselI8 p) {
+  const long groups = p.kchunk / 16;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = (long)p.ntile_n * p.Np * p.nchunk * groups;
+  if (t >= total) return;
+  const long g = t % groups;
+  long rest = t / groups;
+  const int z = (int)(rest % p.nchunk);
+  rest /= p.nchunk;
+  const int slot = (int)(rest % p.Np);
+  const int ct = (int)(rest / p.Np);
+  const int col = ct * p.ctile + slot;
+  const bool cv = slot < p.ctile && col < p.N;
+  const double sB = cv ? col_scale(p.colmax[(long)z * p.N + col]) : 0.0;
+  uint32_t w[3][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t b[3][4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
+      const double v = (cv && k < p.K) ? p.C[(long)col * p.K + k] : 0.0;
+      uint32_t d0, d1, d2;
+      digits3b(__double2int_rn(v * sB), d0, d1, d2);
+      b[0][h] = d0; b[1][h] = d1; b[2][h] = d2;
+    }
+#pragma unroll
+    for (int pl = 0; pl < 3; ++pl) w[pl][q] = b[pl][0] | (b[pl][1] << 8) | (b[pl][2] << 16) | (b[pl][3] << 24);
+  }
+  const long nstage = p.kchunk / BI_NODES;
+  const int s = (int)(g / 4), kb = (int)(g % 4) * 16;
+  const size_t sbytes = 3ul * (size_t)p.Np * 64;
+  uint8_t* blk = p.Bimg + (((size_t)ct * p.nchunk + z) * nstage + s) * sbytes;
+#pragma unroll
+  for (int pl = 0; pl < 3; ++pl)
+    *reinterpret_cast<uint4*>(blk + (size_t)pl * p.Np * 64 + plane_off(slot, kb)) =
+        make_uint4(w[pl][0], w[pl][1], w[pl][2], w[pl][3]);
+}
+
+// one thread per (radius tile, row, slice, 16-node group): J_n(k ρ) straight into digits
+__global__ void k_aimg_bessel(BesselI8 p) {
+  const long groups = p.kchunk / 16;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = (long)p.ntile_m * BI_M * p.nchunk * groups;
+  if (t >= total) return;
+  const long g = t % groups;
+  long rest = t / groups;
+  const int z = (int)(rest % p.nchunk);
+  rest /= p.nchunk;
+  const int row = (int)(rest % BI_M);
+  const int mt = (int)(rest / BI_M);
+  const int r = mt * BI_M + row;
+  const bool rv = r < p.M;
+  const double rho = rv ? p.rho[r] : 0.0;
+  uint32_t w[3][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t b[3][4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
+      const double v = (rv && k < p.K) ? bessel_j012(p.order, p.kr[k] * rho) : 0.0;
+      uint32_t d0, d1, d2;
+      digits3b(__double2int_rn(v * BI_SCALE), d0, d1, d2);
+      b[0][h] = d0; b[1][h] = d1; b[2][h] = d2;
+    }
+#pragma unroll
+    for (int pl = 0; pl < 3; ++pl) w[pl][q] = b[pl][0] | (b[pl][1] << 8) | (b[pl][2] << 16) | (b[pl][3] << 24);
+  }
+  const long nstage = p.kchunk / BI_NODES;
+  const int s = (int)(g / 4), kb = (int)(g % 4) * 16;
+  const size_t sbytes = 3ul * BI_M * 64;
+  uint8_t* blk = p.Aimg + (((size_t)mt * p.nchunk + z) * nstage + s) * sbytes;
+#pragma unroll
+  for (int pl = 0; pl < 3; ++pl)
+    *reinterpret_cast<uint4*>(blk + (size_t)pl * BI_M * 64 + plane_off(row, kb)) =
+        make_uint4(w[pl][0], w[pl][1], w[pl][2], w[pl][3]);
+}
+
+struct BiShared {
+  uint64_t full[BI_STAGES], empty[BI_STAGES], done;
+  uint32_t tmem;
+  int abort_flag;
+};
+
+__device__ __forceinline__ bool bi_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, unsigned* err) {
+  for (long it = 0; it < BI_WAIT_LIMIT; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 255) == 255 && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  atomicOr(err, 1u);
+  return false;
+}
+__device__ __forceinline__ void bi_drain_wait(uint32_t bar, uint32_t parity) {
+  for (long it = 0; it < BI_WAIT_LIMIT; ++it)
+    if (mbar_try(bar, parity)) return;
+}
+
+__global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img(BesselI8 p) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int mt = blockIdx.x, ct = blockIdx.y, z = blockIdx.z;
+  const int c0 = ct * p.ctile;
+  const int nct = min(p.ctile, p.N - c0);
+  const long k0 = (long)z * p.kchunk, k1 = min(p.K, k0 + p.kchunk);
+  const int nst = k1 > k0 ? (int)((k1 - k0 + BI_NODES - 1) / BI_NODES) : 0;
+  const long nstage_chunk = p.kchunk / BI_NODES;
+  const uint32_t planeA = BI_M * 64u, planeB = (uint32_t)p.Np * 64u;
+  const uint32_t stageA = 3u * planeA, stageB = 3u * planeB;
+  uint8_t* smA = smem;
+  uint8_t* smB = smem + BI_STAGES * stageA;
+  BiShared* sh = reinterpret_cast<BiShared*>(smB + BI_STAGES * stageB);
+  volatile int* abort_flag = &sh->abort_flag;
+  if (tid == 0) {
+    for (int s = 0; s < BI_STAGES; ++s) {
+      mbar_init(smem_u32(&sh->full[s]), 1);
+      mbar_init(smem_u32(&sh->empty[s]), 1);
+    }
+    mbar_init(smem_u32(&sh->done), 1);
+    sh->abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem)),
+                 "r"(BI_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh->tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      const uint8_t* gA = p.Aimg + ((size_t)mt * p.nchunk + z) * nstage_chunk * stageA;
+      const uint8_t* gB = p.Bimg + ((size_t)ct * p.nchunk + z) * nstage_chunk * stageB;
+      int issued = 0;
+      for (int s = 0; s < nst; ++s) {
+        const int slot = s % BI_STAGES;
+        if (s >= BI_STAGES && !bi_wait(smem_u32(&sh->empty[slot]), ((s / BI_STAGES) - 1) & 1, abort_flag, p.err))
+          break;
+        const uint32_t bar = smem_u32(&sh->full[slot]);
+        mbar_arrive_tx(bar, stageA + stageB);
+        bulk_g2s(smem_u32(smA + slot * stageA), gA + (size_t)s * stageA, stageA, bar);
+        bulk_g2s(smem_u32(smB + slot * stageB), gB + (size_t)s * stageB, stageB, bar);
+        issued = s + 1;
+      }
+      for (int s = max(0, issued - BI_STAGES); s < issued; ++s)
+        bi_drain_wait(smem_u32(&sh->full[s % BI_STAGES]), (s / BI_STAGES) & 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc =
+          (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(p.Np >> 3) << 17) | ((uint32_t)(BI_M >> 4) << 24);
+      const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
+      for (int s = 0; s < nst; ++s) {
+        const int slot = s % BI_STAGES;
+        if (!bi_wait(smem_u32(&sh->full[slot]), (s / BI_STAGES) & 1, abort_flag, p.err)) break;
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(smA + slot * stageA), b0 = smem_u32(smB + slot * stageB);
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+#pragma unroll
+          for (int pr = 0; pr < 6; ++pr) {
+            const uint64_t ad = umma_desc(a0 + pa[pr] * planeA + t * 256u);
+            const uint64_t bd = umma_desc(b0 + pb[pr] * planeB + t * 256u);
+            const bool first = s == 0 && t == 0 && (pr == 0 || pr == 1 || pr == 3);
+            asm volatile(
+                "{\n\t.reg .pred PD;\n\t"
+                "setp.ne.b32 PD, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, PD;\n\t}" ::"r"(
+                    tmem + (uint32_t)((pa[pr] + pb[pr]) * BI_ACC_STRIDE)),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(first ? 0u : 1u)
+                : "memory");
+          }
+        tc_commit(smem_u32(&sh->empty[slot]));
+      }
+      tc_commit(smem_u32(&sh->done));
+      if (*abort_flag) bi_drain_wait(smem_u32(&sh->done), 0);
+    }
+  } else {
+    // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31 (rows of the radius tile)
+    bool ok = bi_wait(smem_u32(&sh->done), 0, abort_flag, p.err);
+    ok = __all_sync(0xffffffffu, ok) && !*abort_flag;
+    if (ok && nst > 0) {
+      tc_fence_after();
+      const int q = warp & 3;
+      const uint32_t lanebase = (uint32_t)(32 * q) << 16;
+      const int r = mt * BI_M + 32 * q + lane;
+      double* out = p.partial + (long)z * p.N * p.M;
+      const unsigned long long* cmax = p.colmax + (long)z * p.N;
+      for (int e0 = 0; e0 < p.Np; e0 += 8) {
+        uint32_t v0[8], v1[8], v2[8];
+        tmem_ld8(tmem + lanebase + e0, v0);
+        tmem_ld8(tmem + lanebase + BI_ACC_STRIDE + e0, v1);
+        tmem_ld8(tmem + lanebase + 2 * BI_ACC_STRIDE + e0, v2);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int cl = e0 + e;
+          if (cl < nct && r < p.M) {
+            const long long v = (long long)(int)v0[e] * 65536 + (long long)(int)v1[e] * 256 + (long long)(int)v2[e];
+            const unsigned long long bits = cmax[c0 + cl];
+            const double m = __longlong_as_double((long long)bits);
+            double f;
+            if (!isfinite(m)) f = __longlong_as_double(0x7ff8000000000000LL);
+            else f = m > 0.0 ? 65536.0 / (BI_SCALE * col_scale(bits)) : 0.0;
+            out[(long)(c0 + cl) * p.M + r] = (double)v * f;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BI_TMEM_COLS) : "memory");
+}
+
+// P[r][c] = Σ_z partial[z][c][r] through a 32 x 32 shared-memory transpose
+__global__ void k_reduce_transpose(int M, int N, int nz, const double* __restrict__ part, double* __restrict__ P) {
+  __shared__ double tile[32][33];
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int c = c0 + j, r = r0 + threadIdx.x;
+    double s = 0.0;
+    if (c < N && r < M)
+      for (int z = 0; z < nz; ++z) s += part[((long)z * N + c) * M + r];
+    tile[j][threadIdx.x] = s;
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = r0 + j, c = c0 + threadIdx.x;
+    if (r < M && c < N) P[(long)r * N + c] = tile[threadIdx.x][j];
+  }
+}
+
+cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s) {
+  if (p.M <= 0 || p.N <= 0 || p.K <= 0) return cudaSuccess;
+  if (p.kchunk % BI_NODES != 0 || p.kchunk > 16384 || p.Np % 16 != 0 || p.Np > BI_ACC_STRIDE || p.Np < p.ctile ||
+      (long)p.nchunk * p.kchunk < p.K)
+    return cudaErrorInvalidValue;
+  cudaError_t e;
+  k_bcolmax<<<dim3((unsigned)p.N, (unsigned)p.nchunk), 256, 0, s>>>(p);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  {
+    const long total = (long)p.ntile_n * p.Np * p.nchunk * (p.kchunk / 16);
+    k_bimg_real<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  {
+    const long total = (long)p.ntile_m * BI_M * p.nchunk * (p.kchunk / 16);
+    k_aimg_bessel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  const size_t sm = bessel_i8_smem(p.Np);
+  if ((e = cudaFuncSetAttribute(k_gemm_i8_img, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+    return e;
+  k_gemm_i8_img<<<dim3((unsigned)p.ntile_m, (unsigned)p.ntile_n, (unsigned)p.nchunk), BI_THREADS, sm, s>>>(p);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_reduce_transpose<<<dim3((unsigned)((p.M + 31) / 32), (unsigned)((p.N + 31) / 32)), dim3(32, 8), 0, s>>>(
+      p.M, p.N, p.nchunk, p.partial, P);
+  return cudaGetLastError();
+}
+
+}  // namespace ytf

@@ -1075,13 +1075,57 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
     WS(drmap, int, "g_rmap", npix);
     if ((rc = upload(ctx, drho, ur.data(), 8 * (size_t)nr))) return rc;
     if ((rc = upload(ctx, drmap, rmap.data(), 4 * (size_t)npix))) return rc;
-    WS(J, double, "g_J", 3 * (size_t)nr * nk);
     WS(C, double, "g_C", 26 * (size_t)nz * nk);
     WS(P, double, "g_P", 26 * (size_t)nz * nr);
-    double *J0 = J, *J1 = J + (size_t)nr * nk, *J2 = J + 2 * (size_t)nr * nk;
     double *C0 = C, *C1 = C + 10 * (size_t)nz * nk, *C2 = C + 18 * (size_t)nz * nk;
     double *P0 = P, *P1 = P + 10 * (size_t)nz * nr, *P2 = P + 18 * (size_t)nz * nr;
     CK(LAUNCH("k_coef1d", launch_coef1d(sp, C0, C1, C2, ctx->stream)));
+    if (precision == YTF_PREC_INT8X3) {
+      // int8 tensor cores: J_n(kρ) and the coefficient columns as fixed-point digit images,
+      // exact INT32 accumulation, FP64 sum of the node slices into P_n
+      const double* Cn8[3] = {C0, C1, C2};
+      double* Pn8[3] = {P0, P1, P2};
+      const int Nn8[3] = {10 * nz, 8 * nz, 8 * nz};
+      unsigned* err = gb ? gb->err : nullptr;
+      if (!err) {
+        WS(e1, unsigned, "g_tc_err", 1);
+        err = e1;
+        CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+      }
+      for (int o = 0; o < 3; ++o) {
+        BesselI8 bp;
+        std::memset(&bp, 0, sizeof(bp));
+        bp.M = nr; bp.N = Nn8[o]; bp.K = nk; bp.order = o;
+        bp.ctile = bessel_i8_ctile(bp.N);
+        bp.Np = ((bp.ctile + 15) / 16) * 16;
+        bp.ntile_n = (bp.N + bp.ctile - 1) / bp.ctile;
+        bp.ntile_m = (nr + 127) / 128;
+        const long tiles = (long)bp.ntile_m * bp.ntile_n;
+        const long want = std::max(1L, (long)nsm / tiles);
+        long kchunk = (nk + want - 1) / want;
+        kchunk = std::min(16384L, std::max(64L, ((kchunk + 63) / 64) * 64));
+        bp.kchunk = kchunk;
+        bp.nchunk = (int)((nk + kchunk - 1) / kchunk);
+        const size_t nst = (size_t)(kchunk / 64);
+        WS(Ai, uint8_t, "g_bi_a", (size_t)bp.ntile_m * bp.nchunk * nst * bessel_i8_stage_bytes_a());
+        WS(Bi, uint8_t, "g_bi_b", (size_t)bp.ntile_n * bp.nchunk * nst * bessel_i8_stage_bytes_b(bp.Np));
+        WS(cm, unsigned long long, "g_bi_cmax", (size_t)bp.nchunk * bp.N);
+        WS(pt, double, "g_bi_part", (size_t)bp.nchunk * bp.N * nr);
+        bp.kr = c->d_kr; bp.rho = drho; bp.C = Cn8[o];
+        bp.Aimg = Ai; bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
+        CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pn8[o], ctx->stream)));
+      }
+      if (!gb) {
+        unsigned herr = 0;
+        CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
+      }
+      CK(LAUNCH("k_assemble1d", launch_assemble1d(nx, ny, nz, dxs, dys, drmap, nr, P0, P1, P2, G, ctx->stream)));
+      goto synthesis_done;
+    }
+    WS(J, double, "g_J", 3 * (size_t)nr * nk);
+    double *J0 = J, *J1 = J + (size_t)nr * nk, *J2 = J + 2 * (size_t)nr * nk;
     CK(LAUNCH("k_bessel", launch_bessel(c->d_kr, nk, drho, nr, J0, J1, J2, ctx->stream)));
     auto splits_for = [&](int M, int N) {
       long tiles = (long)((M + 127) / 128) * ((N + 127) / 128);
@@ -1196,6 +1240,7 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
       }
     }
   }
+synthesis_done:
   if (!out_is_device) CK(cudaMemcpyAsync(out, G, sizeof(double2) * nout, cudaMemcpyDeviceToHost, ctx->stream));
   if (!gb) {
     CK(cudaStreamSynchronize(ctx->stream));

@@ -167,6 +167,30 @@ cudaError_t launch_lateral_i8(const LateralI8& p, cudaStream_t s);
 cudaError_t launch_phase_tables_pad(const CacheView& c, int nx, int ny, const double* xs, const double* ys, long n_pad,
                                     float2* Px, float2* Py, cudaStream_t s);
 
+// 1D Bessel synthesis contraction on the int8 tensor cores: P[r][c] = Σ_k J_order(k ρ_r) C[c][k]
+struct BesselI8 {
+  int M, N;          // radii, real coefficient columns
+  long K;            // nodes
+  int order;         // Bessel order 0, 1 or 2
+  int ctile, Np;     // columns per tile, ctile rounded up to 16 (MMA N ≤ 160)
+  int ntile_m, ntile_n;
+  long kchunk;       // nodes per slice: a multiple of 64, ≤ 16384
+  int nchunk;
+  const double* kr;  // [K]
+  const double* rho; // [M]
+  const double* C;   // [N][K]
+  uint8_t* Aimg;     // [ntile_m][nchunk][kchunk/64][3][128 x 64 B]
+  uint8_t* Bimg;     // [ntile_n][nchunk][kchunk/64][3][Np x 64 B]
+  unsigned long long* colmax;  // [nchunk][N]
+  double* partial;   // [nchunk][N][M]
+  unsigned* err;
+};
+size_t bessel_i8_stage_bytes_a();
+size_t bessel_i8_stage_bytes_b(int Np);
+size_t bessel_i8_smem(int Np);
+int bessel_i8_ctile(int N);
+cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s);
+
 // Gauss-Legendre panels -> nodes/weights, bit-exact with the CPU restatement
 cudaError_t launch_gl_nodes(int npanels, const double* pa, const double* pb, const int* sing_side, const double* xi,
                             const double* wx, int order, double* nodes, double* wts, cudaStream_t s);
