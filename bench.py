@@ -597,6 +597,79 @@ def run_learned(args):
     return 0
 
 
+def run_bessel(args):
+    """The Bessel synthesis at scale (one GPU): a film stack's 1D cache of 65536 nodes, G on
+    4096 radii log-spaced over 0.001-10 λ x 256 observer heights (9,437,184 entries), timed
+    for the contraction precision given and for FP64 beside it."""
+    import torch
+    from yellowthinfilms_b200 import api
+    from yellowthinfilms_b200.materials import FlatOpticalLayer, IsotropicMaterial, UniaxialMaterial
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    lam = 600.0
+    k0 = 2 * np.pi / lam
+    st = [FlatOpticalLayer(IsotropicMaterial(1.0), 200.0),
+          FlatOpticalLayer(UniaxialMaterial(-3.0 + 0.4j, 4.0 + 0.2j), 50.0),
+          FlatOpticalLayer(IsotropicMaterial(2.25), 100.0)]
+    stack = api.Stack(st, ctx)
+    npan = 65536 // ORDER
+    kx, wt = api.gl_rule([(20 * k0 * i / npan, 20 * k0 * (i + 1) / npan) for i in range(npan)], ORDER, ctx=ctx)
+    cache = api.build_cavity_transfer_1d(stack, k0, 1, kx, wt, obs_layers=[1])
+    rho = np.geomspace(0.001 * lam, 10 * lam, 4096)
+    zo = np.linspace(0.5, 199.5, 256)
+    prec = args.precision if args.precision != "split_bf16" else "int8x3"
+    out = torch.empty(4096 * 256 * 9, dtype=torch.complex128, device="cuda")
+
+    def run(p):
+        for _ in range(args.warmup):
+            api.closed_form_G(cache, 1, 20.0, zo, rho, [0.0], terms="scattered", precision=p, out=out)
+        torch.cuda.synchronize()
+        ctx.profile(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(0) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                api.closed_form_G(cache, 1, 20.0, zo, rho, [0.0], terms="scattered", precision=p, out=out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        return e0.elapsed_time(e1) / args.steps, prof, clk.summary(), out.cpu().numpy()
+
+    ms, prof, clocks, G = run(prec)
+    ms64, prof64, _, G64 = run("fp64")
+    entries = G.size
+    flops = 2.0 * 4096 * 65536 * 26 * 256  # 13 complex coefficient columns (26 real) per height
+    name = "k_bessel_i8" if prec == "int8x3" else "k_dgemm_nt"
+    t_k = prof[name][0] / prof[name][1] * 1e-3 if name in prof else None
+    peak, src = measured_peaks()["bf16_sustained"]
+    roof = {"kernel": name, "bound": "tensor" if prec == "int8x3" else "fp64",
+            "achieved": flops / 3 / t_k / 1e12 if t_k else None, "unit": "TFLOP/s",
+            "peak": peak if prec == "int8x3" else FP64_NOMINAL, "traffic": None,
+            "work": "2 x 4096 radii x 65536 nodes x 26 real columns x 256 heights = 3.57e12 flop over the 3 orders "
+                    "(one launch per order: a third each)",
+            "peak_source": src if prec == "int8x3" else "nominal FP64"}
+    if roof["achieved"]:
+        roof["frac"] = roof["achieved"] / roof["peak"]
+        if prec == "int8x3":
+            roof["executed_frac_of_int8_peak"] = 6 * roof["achieved"] / (2 * peak)
+    line = {"metric": METRIC, "value": entries / (ms * 1e-3), "unit": "entries/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": DTYPE[prec], "data": "synthetic (seeded)",
+            "config": {"workload": "Bessel synthesis: film stack, 65536 nodes, 4096 radii (0.001-10 λ) x 256 heights "
+                                   "x 9 components, scattered term", "entries_per_step": int(entries),
+                       "precision": prec},
+            "fp64_entries_per_s": entries / (ms64 * 1e-3), "speedup_vs_fp64": ms64 / ms,
+            "max_rel_err_vs_fp64": float(np.linalg.norm(G - G64) / np.linalg.norm(G64)),
+            "roofline": roof, "clocks": clocks,
+            "kernels_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items())},
+            "fp64_kernels_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof64.items())}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -604,9 +677,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-check", action="store_true")
-    ap.add_argument("--workload", default="gyro32", choices=["gyro32", "uneven", "learned"],
+    ap.add_argument("--workload", default="gyro32", choices=["gyro32", "uneven", "learned", "bessel"],
                     help="gyro32: the 8-layer stack at 32 wavelengths (default); uneven: 1024 uneven stacks; "
-                         "learned: learned adaptive quadrature vs the plain fixed rule")
+                         "learned: learned adaptive quadrature vs the plain fixed rule; bessel: the 1D Bessel synthesis at "
+                         "4096 radii x 65536 nodes x 256 heights")
     ap.add_argument("--per-call", action="store_true",
                     help="one build + synthesis call per wavelength instead of the batched calls")
     ap.add_argument("--precision", default="int8x3", choices=list(DTYPE),
@@ -619,6 +693,8 @@ def main():
         return run_uneven(args)
     if args.workload == "learned":
         return run_learned(args)
+    if args.workload == "bessel":
+        return run_bessel(args)
     return run_ours(args)
 
 
