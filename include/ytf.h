@@ -109,6 +109,24 @@ int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* cache, double* T, double* Qf
 int ytf_cavity_response(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer, long n,
                         const double* kr, double phi, double* out);
 
+/* build_cavity_transfer_1d on a deformed integration contour: complex nodes kρ = k_re + i k_im
+ * with complex weights (w_re + i w_im), e.g. kρ(t) = t - i h s(t) with s(0) = s(L) = 0 below
+ * the real axis. No counterpart in the reference, whose rules stay on the real axis
+ * (mod_KxGrid.jl:361-394); with lossy layers every pole and branch point lies above the real
+ * axis, so by Cauchy's theorem the contour integral equals the real-axis one with the same
+ * end points. Azimuthally symmetric (closed-form) stacks only, as the 1D path; the mode
+ * solve, S-matrices and projections are the analytic continuation in kρ (principal square
+ * roots: ω²ε - kρ² stays in the upper half plane below the axis). closed_form_G on such a
+ * cache uses complex J_n(kρ ρ) in an FP64 contraction (INT8X3 falls back to it). */
+int ytf_transfer_1d_contour(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer, int nk,
+                            const double* k_re, const double* k_im, const double* w_re, const double* w_im, int nobs,
+                            const int* obs_layers, ytf_cache** out);
+
+/* J_order(z) (order 0, 1, 2) at n complex points z = z_re + i z_im, evaluated by the device
+ * functions of the contour synthesis (power series, Miller recurrence, Hankel expansion). */
+int ytf_bessel_j(ytf_ctx* ctx, int order, long n, const double* z_re, const double* z_im, double* out_re,
+                 double* out_im);
+
 /* layer_light_lines(layer, ω, φ) (mod_KxGrid.jl:41-59) of one layer given as raw arrays
  * (column-major 3x3 ε and μ, interleaved re/im; mu NULL = identity): up to 2 values into
  * out (ascending), their count in *n. Host arithmetic; needs no context or GPU. */

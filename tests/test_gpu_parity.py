@@ -464,3 +464,62 @@ def test_uneven_batch_workload_shape(ytf, oracle):
         G = ytf.closed_form_G_batch([dict(y, cache=batch[i])])[0]
         Go = oracle.closed_form_G(oc, y["obs_layer"], y["zsrc_local"], y["z_obs"], y["xs"], y["ys"])
         assert relerr(G, Go) < 1e-9, (i, relerr(G, Go))
+
+
+def test_complex_bessel_matches_mpmath(ytf):
+    """J_0, J_1, J_2 of complex argument on the device (series, Miller recurrence, Hankel
+    expansion) against mpmath, |z| up to 700, -2 <= Im z <= 0.5: within 1e-12 of the
+    envelope sqrt(2/(π|z|)) e^{|Im z|} (1 below |z| = 1)."""
+    import mpmath
+    rng = np.random.default_rng(5)
+    r = np.exp(rng.uniform(np.log(1e-3), np.log(700.0), 400))
+    z = r * np.exp(1j * rng.uniform(-0.003, 0.0, 400)) + 1j * rng.uniform(-2.0, 0.5, 400)
+    z = np.concatenate([z, [8.0 - 0.1j, 8.0001 + 0.0j, 24.999 - 1.0j, 25.0, 1.0 - 0.5j, 0.999j * 0 + 0.999]])
+    env = np.where(np.abs(z) > 1, np.sqrt(2 / (np.pi * np.abs(z))) * np.exp(np.abs(z.imag)), np.exp(np.abs(z.imag)))
+    for n in (0, 1, 2):
+        g = ytf.bessel_j(n, z)
+        ref = np.array([complex(mpmath.besselj(n, complex(v))) for v in z])
+        err = np.abs(g - ref) / env
+        assert np.max(err) < 1e-12, (n, np.max(err), z[np.argmax(err)])
+
+
+def test_contour_with_zero_indentation_equals_real_axis_path(ytf):
+    """The complex-node path with zero imaginary parts reproduces the real-node path."""
+    st = config1_stack()
+    k0 = 2 * np.pi / 600.0
+    k, w = ytf.contour_rule(k0, npanels=64, h=0.0)
+    gc = ytf.build_cavity_transfer_1d_contour(st, k0, 1, k, w, obs_layers=[1])
+    gr = ytf.build_cavity_transfer_1d(st, k0, 1, k.real, w.real, obs_layers=[1])
+    rho = np.geomspace(6.0, 3000.0, 12)
+    zo = np.linspace(30.0, 190.0, 5)
+    Gc = ytf.closed_form_G(gc, 1, 20.0, zo, rho, [0.0])
+    Gr = ytf.closed_form_G(gr, 1, 20.0, zo, rho, [0.0])
+    assert relerr(Gc, Gr) < 1e-13, relerr(Gc, Gr)
+
+
+def test_config1_contour_matches_real_axis_oracle(ytf, oracle):
+    """Config 1: vertical dipole 20 nm above the uniaxial film; 4096 nodes (512 GL-8 panels)
+    on the contour kρ = t - 0.05 i k0 sin(π t / 20 k0), t in [0, 20 k0]. With the film's loss
+    every pole and branch point lies above the real axis, so by Cauchy's theorem the contour
+    integral equals the oracle's real-axis integral over [0, 20 k0] (dense rule: breaks at the
+    light lines, u² substitution at the half-space ones): G within 1e-6."""
+    st = config1_stack()
+    k0 = 2 * np.pi / 600.0
+    k, w = ytf.contour_rule(k0, npanels=512, order=8)
+    gc = ytf.build_cavity_transfer_1d_contour(st, k0, 1, k, w, obs_layers=[1])
+    rho = np.geomspace(6.0, 3000.0, 24)
+    zo = np.linspace(0.0, 200.0, 9)
+    Gc = ytf.closed_form_G(gc, 1, 20.0, zo, rho, [0.0])
+    lines = sorted({float(x) for L in st for x in oracle.light_lines(L, k0, 0.0) if 0 < x < 20 * k0})
+    sing = sorted({float(x) for L in (st[0], st[-1]) for x in oracle.light_lines(L, k0, 0.0)})
+    brk = [0.0] + lines + [20 * k0]
+    panels = []
+    for a, b in zip(brk[:-1], brk[1:]):
+        n = max(8, int(np.ceil(6000 * (b - a) / (20 * k0))))
+        e = np.linspace(a, b, n + 1)
+        panels += list(zip(e[:-1], e[1:]))
+    kr, wr = oracle.gl_rule(panels, 8, singular=sing)
+    oc = oracle.build_cavity_transfer_1d(st, k0, 1, kr, wr, obs_layers=[1])
+    Go = oracle.closed_form_G(oc, 1, 20.0, zo, rho, [0.0])
+    assert relerr(Gc, Go) < 1e-6, relerr(Gc, Go)
+    assert relerr(Gc[..., 2, 2], Go[..., 2, 2]) < 1e-6

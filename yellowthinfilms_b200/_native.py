@@ -87,6 +87,9 @@ SIGNATURES = {
     "ytf_nodes_from_poles": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams),
                                             ctypes.c_int, _d, _d, ctypes.c_long, _d, _d, ctypes.POINTER(ctypes.c_long),
                                             ctypes.POINTER(GridInfo)]),
+    "ytf_transfer_1d_contour": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _d, _d, _d, _d,
+                                               ctypes.c_int, _i, ctypes.POINTER(_vp)]),
+    "ytf_bessel_j": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_long, _d, _d, _d, _d]),
     "ytf_transfer_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(TransferDesc), ctypes.POINTER(_vp)]),
     "ytf_green_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(GreenDesc)]),
     "ytf_gauss_legendre": (ctypes.c_int, [ctypes.c_int, _d, _d]),

@@ -416,6 +416,49 @@ def grid_from_poles(stack, omega, source_layer, poles, h_min, rho_max=0.0, targe
     return _grid(stack, omega, source_layer, h_min, rho_max, target_decay, kr_cap, False, order, rtol, ctx, list(poles))
 
 
+def contour_rule(k0, npanels=512, order=8, L=None, h=None):
+    """Gauss–Legendre rule on the deformed path kρ(t) = t - i h sin(π t / L), t in [0, L]
+    (defaults L = 20 k0, h = 0.05 k0: below the real axis, back on it at both ends). Returns
+    complex nodes and weights (w = kρ'(t) w_t)."""
+    L = 20.0 * k0 if L is None else float(L)
+    h = 0.05 * k0 if h is None else float(h)
+    x, wx = gausslegendre(order)
+    edges = np.linspace(0.0, L, npanels + 1)
+    c = 0.5 * (edges[1:] + edges[:-1])
+    hw = 0.5 * np.diff(edges)
+    t = (c[:, None] + hw[:, None] * x[None, :]).ravel()
+    wt = (hw[:, None] * wx[None, :]).ravel()
+    k = t - 1j * h * np.sin(np.pi * t / L)
+    dk = 1.0 - 1j * h * (np.pi / L) * np.cos(np.pi * t / L)
+    return k, dk * wt
+
+
+def build_cavity_transfer_1d_contour(stack, omega, source_layer, k_nodes, w_nodes, obs_layers=None,
+                                     ctx: Optional[Context] = None) -> CavityTransferCache1D:
+    """build_cavity_transfer_1d on complex nodes of a deformed contour (ytf_transfer_1d_contour)."""
+    st = _as_stack(stack, ctx)
+    k = np.asarray(k_nodes, np.complex128)
+    w = np.asarray(w_nodes, np.complex128)
+    if len(k) != len(w):
+        raise YTFError("build_cavity_transfer_1d: kx_nodes/wt_nodes length mismatch")
+    kr, ki, wr, wi = (np.ascontiguousarray(a) for a in (k.real, k.imag, w.real, w.imag))
+    no, ob = _obs_arg(obs_layers)
+    h = ctypes.c_void_p()
+    st.ctx.check(lib().ytf_transfer_1d_contour(st.ctx.h, st.h, float(omega), int(source_layer), len(k), ptr(kr),
+                                               ptr(ki), ptr(wr), ptr(wi), no, ptr(ob, _i), ctypes.byref(h)))
+    return CavityTransferCache1D(h, st, omega, source_layer, k, w)
+
+
+def bessel_j(order, z, ctx: Optional[Context] = None):
+    """J_order(z) for complex z on the device (the contour synthesis's Bessel functions)."""
+    ctx = ctx or default_context()
+    z = np.atleast_1d(np.asarray(z, np.complex128))
+    zr, zi = np.ascontiguousarray(z.real), np.ascontiguousarray(z.imag)
+    outr, outi = np.zeros(len(z)), np.zeros(len(z))
+    ctx.check(lib().ytf_bessel_j(ctx.h, int(order), len(z), ptr(zr), ptr(zi), ptr(outr), ptr(outi)))
+    return outr + 1j * outi
+
+
 def build_cavity_transfer_batch(items, ctx: Optional[Context] = None):
     """Many caches in one call (ytf_transfer_batch): each item is a dict with the keyword
     arguments of build_cavity_transfer_1d (``kx_nodes``, ``wt_nodes``) or

@@ -64,9 +64,11 @@ struct ytf_cache {
   long n = 0;
   double omega = 0, d_src = 0;
   std::vector<double> kr, wr, phi, wphi, d_layer;
+  std::vector<double> kri, wri;  // imaginary parts of 1D nodes/weights on a deformed contour (else empty)
   void* block = nullptr;  // one device allocation for every array below
   size_t block_bytes = 0;
   double *d_kr = nullptr, *d_wr = nullptr, *d_phi = nullptr, *d_wphi = nullptr;
+  double *d_kri = nullptr, *d_wri = nullptr;
   uint8_t *d_status = nullptr, *d_valid = nullptr, *d_tvalid = nullptr;
   double2 *d_T = nullptr, *d_Qf = nullptr, *d_Qb = nullptr, *d_sf = nullptr, *d_sb = nullptr, *d_basis = nullptr;
   int oidx(int o) const {
@@ -209,6 +211,7 @@ int alloc_cache(ytf_ctx* ctx, ytf_cache* c, bool upload_nodes = true) {
   };
   size_t o_kr = take(8 * c->kr.size()), o_wr = take(8 * c->wr.size()), o_phi = take(8 * std::max<size_t>(1, c->phi.size())),
          o_wphi = take(8 * std::max<size_t>(1, c->wphi.size()));
+  size_t o_kri = take(8 * std::max<size_t>(1, c->kri.size())), o_wri = take(8 * std::max<size_t>(1, c->wri.size()));
   size_t o_status = take(n), o_valid = take(n), o_tvalid = take((size_t)n * c->nobs);
   size_t o_T = take(16 * 16 * (size_t)n * c->nobs), o_Qf = take(16 * 2 * (size_t)n), o_Qb = take(16 * 2 * (size_t)n);
   size_t o_sf = take(16 * 6 * (size_t)n), o_sb = take(16 * 6 * (size_t)n), o_basis = take(16 * 16 * (size_t)n * c->nobs);
@@ -224,6 +227,8 @@ int alloc_cache(ytf_ctx* ctx, ytf_cache* c, bool upload_nodes = true) {
   char* b = (char*)c->block;
   c->d_kr = (double*)(b + o_kr); c->d_wr = (double*)(b + o_wr);
   c->d_phi = (double*)(b + o_phi); c->d_wphi = (double*)(b + o_wphi);
+  c->d_kri = c->kri.empty() ? nullptr : (double*)(b + o_kri);
+  c->d_wri = c->wri.empty() ? nullptr : (double*)(b + o_wri);
   c->d_status = (uint8_t*)(b + o_status); c->d_valid = (uint8_t*)(b + o_valid); c->d_tvalid = (uint8_t*)(b + o_tvalid);
   c->d_T = (double2*)(b + o_T); c->d_Qf = (double2*)(b + o_Qf); c->d_Qb = (double2*)(b + o_Qb);
   c->d_sf = (double2*)(b + o_sf); c->d_sb = (double2*)(b + o_sb); c->d_basis = (double2*)(b + o_basis);
@@ -233,6 +238,10 @@ int alloc_cache(ytf_ctx* ctx, ytf_cache* c, bool upload_nodes = true) {
   if (!upload_nodes) return YTF_OK;
   if ((rc = upload(ctx, c->d_kr, c->kr.data(), 8 * c->kr.size()))) return rc;
   if ((rc = upload(ctx, c->d_wr, c->wr.data(), 8 * c->wr.size()))) return rc;
+  if (!c->kri.empty()) {
+    if ((rc = upload(ctx, c->d_kri, c->kri.data(), 8 * c->kri.size()))) return rc;
+    if ((rc = upload(ctx, c->d_wri, c->wri.data(), 8 * c->wri.size()))) return rc;
+  }
   if (!c->phi.empty()) {
     if ((rc = upload(ctx, c->d_phi, c->phi.data(), 8 * c->phi.size()))) return rc;
     if ((rc = upload(ctx, c->d_wphi, c->wphi.data(), 8 * c->wphi.size()))) return rc;
@@ -758,6 +767,51 @@ int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* st, double omega, int so
   return nodes_1d_impl(ctx, st, omega, source_layer, prm, npoles, q, G, cap, k, w, n, info);
 }
 
+int ytf_transfer_1d_contour(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, int nk,
+                            const double* k_re, const double* k_im, const double* w_re, const double* w_im, int nobs,
+                            const int* obs_layers, ytf_cache** out) {
+  if (!ctx || !out) return YTF_ERR_ARG;
+  *out = nullptr;
+  if (nk > 0 && (!k_im || !w_im))
+    return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_1d: contour nodes need imaginary parts");
+  ytf_cache* c;
+  bool rot;
+  int rc = prepare_cache(ctx, st, false, omega, source_layer, nk, k_re, w_re, 0, nullptr, nullptr, nobs, obs_layers, 1,
+                         YTF_ROT_OFF, false, &c, &rot);
+  if (rc) return rc;
+  // the cache block was laid out before the imaginary parts were known: lay it out again
+  c->kri.assign(k_im, k_im + nk);
+  c->wri.assign(w_im, w_im + nk);
+  if (c->block) {
+    cudaStreamSynchronize(ctx->stream);
+    ctx->pool.emplace(c->block_bytes, c->block);
+    c->block = nullptr;
+  }
+  if ((rc = alloc_cache(ctx, c, true))) { ytf_cache_destroy(c); return rc; }
+  TransferParams p;
+  fill_params(p, st, c);
+  p.mode = 0;
+  p.nout = c->n;
+  p.kr_im = c->d_kri;
+  if (c->n > 0 && (rc = run_transfer(ctx, p, c->n))) { ytf_cache_destroy(c); return rc; }
+  return finish_build(ctx, c, out);
+}
+
+int ytf_bessel_j(ytf_ctx* ctx, int order, long n, const double* z_re, const double* z_im, double* out_re,
+                 double* out_im) {
+  if (!ctx || order < 0 || order > 2 || n < 0 || (n > 0 && (!z_re || !z_im || !out_re || !out_im))) return YTF_ERR_ARG;
+  if (n == 0) return YTF_OK;
+  CK(cudaSetDevice(ctx->device));
+  WS(buf, double, "bj_buf", 4 * (size_t)n);
+  int rc;
+  if ((rc = upload(ctx, buf, z_re, 8 * (size_t)n)) || (rc = upload(ctx, buf + n, z_im, 8 * (size_t)n))) return rc;
+  CK(LAUNCH("k_bessel_eval", launch_bessel_eval(n, order, buf, buf + n, buf + 2 * n, buf + 3 * n, ctx->stream)));
+  CK(cudaMemcpyAsync(out_re, buf + 2 * n, 8 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(out_im, buf + 3 * n, 8 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return YTF_OK;
+}
+
 int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cache** out) {
   if (!ctx || nb < 0 || (nb > 0 && (!d || !out))) return YTF_ERR_ARG;
   for (int i = 0; i < nb; ++i) out[i] = nullptr;
@@ -1012,6 +1066,7 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
   CacheView& v = sp.c;
   v.n = c->n; v.Nk = c->Nk; v.Np = c->Np; v.src = c->src; v.d_src = c->d_src;
   v.kr = c->d_kr; v.wr = c->d_wr; v.phi = c->d_phi; v.wphi = c->d_wphi;
+  v.kri = c->d_kri; v.wri = c->d_wri;
   v.valid = c->d_valid;
   v.tvalid = c->d_tvalid + (size_t)oi * c->n;
   v.T = c->d_T + (size_t)oi * 16 * c->n;
@@ -1080,6 +1135,32 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
     double *C0 = C, *C1 = C + 10 * (size_t)nz * nk, *C2 = C + 18 * (size_t)nz * nk;
     double *P0 = P, *P1 = P + 10 * (size_t)nz * nr, *P2 = P + 18 * (size_t)nz * nr;
     CK(LAUNCH("k_coef1d", launch_coef1d(sp, C0, C1, C2, ctx->stream)));
+    if (c->d_kri) {
+      // nodes on a deformed contour: complex J_n(kρ ρ) tables, two FP64 GEMMs per order
+      // (Re J and Im J against the real/imaginary coefficient columns), then the complex combine
+      WS(Jc, double, "g_Jc", 6 * (size_t)nr * nk);
+      CK(LAUNCH("k_bessel_c", launch_bessel_c(c->d_kr, c->d_kri, nk, drho, nr, Jc, ctx->stream)));
+      const double* Cn[3] = {C0, C1, C2};
+      double* Pn[3] = {P0, P1, P2};
+      const int Nn[3] = {10 * nz, 8 * nz, 8 * nz};
+      WS(Pab, double, "g_Pab", 2 * (size_t)nr * 10 * nz);
+      for (int o = 0; o < 3; ++o) {
+        long tiles = (long)((nr + 127) / 128) * ((Nn[o] + 127) / 128);
+        long want = (2L * nsm + tiles - 1) / tiles;
+        int sp0 = dgemm_splits((int)nk, (int)std::max(1L, std::min(want, std::max(1L, nk / 256))));
+        WS(Pp, double, "g_partial", (size_t)sp0 * nr * Nn[o]);
+        for (int part = 0; part < 2; ++part) {
+          const double* Jp = Jc + (size_t)(2 * o + part) * nr * nk;
+          CK(LAUNCH("k_dgemm_nt", launch_dgemm_nt(nr, Nn[o], (int)nk, Jp, Cn[o], Pp, sp0, ctx->stream)));
+          CK(LAUNCH("k_reduce_splits", launch_reduce_splits((long)nr * Nn[o], sp0, Pp,
+                                                            Pab + (size_t)part * nr * 10 * nz, ctx->stream)));
+        }
+        CK(LAUNCH("k_combine_complex", launch_combine_complex(nr, Nn[o], Pab, Pab + (size_t)nr * 10 * nz, Pn[o],
+                                                              ctx->stream)));
+      }
+      CK(LAUNCH("k_assemble1d", launch_assemble1d(nx, ny, nz, dxs, dys, drmap, nr, P0, P1, P2, G, ctx->stream)));
+      goto synthesis_done;
+    }
     if (precision == YTF_PREC_INT8X3) {
       // int8 tensor cores: J_n(kρ) and the coefficient columns as fixed-point digit images,
       // exact INT32 accumulation, FP64 sum of the node slices into P_n
@@ -1436,6 +1517,7 @@ extern "C" int ytf_green_noalloc(ytf_ctx* ctx, const ytf_cache* c, int obs_layer
   CacheView& v = sp.c;
   v.n = n; v.Nk = c->Nk; v.Np = c->Np; v.src = c->src; v.d_src = c->d_src;
   v.kr = c->d_kr; v.wr = c->d_wr; v.phi = c->d_phi; v.wphi = c->d_wphi;
+  v.kri = c->d_kri; v.wri = c->d_wri;
   v.valid = c->d_valid;
   v.tvalid = c->d_tvalid + (size_t)oi * n;
   v.T = c->d_T + (size_t)oi * 16 * n;

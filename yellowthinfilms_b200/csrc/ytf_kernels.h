@@ -38,6 +38,7 @@ struct TransferParams {
   long nout;               // nodes of the output cache (== n except the rotation fill)
   int Nk, Np;
   const double* kr;        // 1D: kx nodes; 2D: kρ nodes
+  const double* kr_im;     // 1D nodes on a deformed contour: imaginary parts (else NULL)
   const double* phi;       // 2D: φ nodes
   // scratch
   double2* modes;          // [nL][20][n]
@@ -80,6 +81,8 @@ struct CacheView {
   double d_src;
   const double* kr;    // [Nk]
   const double* wr;    // [Nk]
+  const double* kri;   // [Nk] imaginary parts of complex 1D nodes (deformed contour), else NULL
+  const double* wri;   // [Nk] imaginary parts of their weights
   const double* phi;   // [Np]
   const double* wphi;  // [Np]
   const uint8_t* valid;
@@ -105,6 +108,11 @@ struct SynthParams {
 
 // 1D Jacobi-Anger synthesis
 cudaError_t launch_coef1d(const SynthParams& p, double* C0, double* C1, double* C2, cudaStream_t s);
+cudaError_t launch_bessel_c(const double* kr, const double* kri, long nk, const double* rho, int nr, double* J,
+                            cudaStream_t s);
+cudaError_t launch_combine_complex(long M, int N2, const double* A, const double* B, double* P, cudaStream_t s);
+cudaError_t launch_bessel_eval(long n, int order, const double* zr, const double* zi, double* outr, double* outi,
+                               cudaStream_t s);
 cudaError_t launch_bessel(const double* kr, long nk, const double* rho, int nr, double* J0, double* J1, double* J2,
                           cudaStream_t s);
 int dgemm_splits(int K, int splits);  // effective split count of launch_dgemm_nt

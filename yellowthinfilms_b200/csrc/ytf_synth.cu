@@ -16,6 +16,7 @@
 // whose A operand is generated in shared memory from the node's (kx, ky).
 #include "ytf_complex.cuh"
 #include "ytf_kernels.h"
+#include "ytf_bessel.cuh"
 
 #include <algorithm>
 
@@ -103,8 +104,9 @@ __global__ void __launch_bounds__(128) k_coef1d(SynthParams p, double* C0, doubl
   cd Af[2][3], Ab[2][3];
   reflected_amp(p, k, Af, Ab);
   const double z = p.zo[zi];
-  const cd W{0.0, c.wr[k] / (2.0 * 3.14159265358979323846)};
-  const double kx = c.kr[k];
+  // i w / (2π) with a complex weight and node on a deformed contour (kri, wri), real otherwise
+  const cd W = cd{0.0, 1.0 / (2.0 * 3.14159265358979323846)} * cd{c.wr[k], c.wri ? c.wri[k] : 0.0};
+  const cd kx{c.kr[k], c.kri ? c.kri[k] : 0.0};
   cd c0[5], c1[4], c2[4];
   for (int i = 0; i < 5; ++i) c0[i] = cd{0, 0};
   for (int i = 0; i < 4; ++i) { c1[i] = cd{0, 0}; c2[i] = cd{0, 0}; }
@@ -120,8 +122,8 @@ __global__ void __launch_bounds__(128) k_coef1d(SynthParams p, double* C0, doubl
         af[q] = fin0(W * (Afd[m][q] + Af[m][q] * pf));
         ab[q] = fin0(W * (Abd[m][q] + Ab[m][q] * pb));
       }
-      gf = cd{kx, 0.0};
-      gb = cd{kx, 0.0};
+      gf = kx;
+      gb = kx;
     } else {
       for (int q = 0; q < 3; ++q) { af[q] = fin0(W * Af[m][q]); ab[q] = fin0(W * Ab[m][q]); }
       gf = phase_cl(kzf, z) * kx;
@@ -194,6 +196,73 @@ __global__ void k_bessel(const double* kr, long nk, const double* rho, int nr, d
   J0[o] = a0;
   J1[o] = a1;
   J2[o] = a2;
+}
+
+// J_n(kρ ρ) of complex nodes (deformed contour): real and imaginary tables of each order
+__global__ void k_bessel_c(const double* kr, const double* kri, long nk, const double* rho, int nr, double* J) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (k >= nk) return;
+  const cd z = cd{kr[k], kri[k]} * rho[r];
+  cd a0, a1, a2;
+  if (z.x == 0.0 && z.y == 0.0) {
+    a0 = cd{1.0, 0.0}; a1 = cd{0.0, 0.0}; a2 = cd{0.0, 0.0};
+  } else {
+    bessel_j012_c(z, a0, a1, a2);
+  }
+  const long o = (long)r * nk + k, plane = (long)nr * nk;
+  J[o] = a0.x; J[plane + o] = a0.y;
+  J[2 * plane + o] = a1.x; J[3 * plane + o] = a1.y;
+  J[4 * plane + o] = a2.x; J[5 * plane + o] = a2.y;
+}
+
+cudaError_t launch_bessel_c(const double* kr, const double* kri, long nk, const double* rho, int nr, double* J,
+                            cudaStream_t s) {
+  if (nk <= 0 || nr <= 0) return cudaSuccess;
+  dim3 grid((unsigned)((nk + 127) / 128), (unsigned)nr);
+  k_bessel_c<<<grid, 128, 0, s>>>(kr, kri, nk, rho, nr, J);
+  return cudaGetLastError();
+}
+
+// complex J times the real/imag column pairs: P[r][2c] = A[2c] - B[2c+1], P[r][2c+1] = A[2c+1] + B[2c]
+// with A = Re J · C^T and B = Im J · C^T
+__global__ void k_combine_complex(long M, int N2, const double* A, const double* B, double* P) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= M * (N2 / 2)) return;
+  const long r = t / (N2 / 2), c = t % (N2 / 2);
+  const long o = r * N2 + 2 * c;
+  P[o] = A[o] - B[o + 1];
+  P[o + 1] = A[o + 1] + B[o];
+}
+
+cudaError_t launch_combine_complex(long M, int N2, const double* A, const double* B, double* P, cudaStream_t s) {
+  const long tot = M * (N2 / 2);
+  if (tot <= 0) return cudaSuccess;
+  k_combine_complex<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(M, N2, A, B, P);
+  return cudaGetLastError();
+}
+
+// one complex J_n evaluation per thread (the device Bessel functions, exposed for testing)
+__global__ void k_bessel_eval(long n, int order, const double* zr, const double* zi, double* outr, double* outi) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  cd a0, a1, a2;
+  const cd z{zr[t], zi[t]};
+  if (z.x == 0.0 && z.y == 0.0) {
+    a0 = cd{1.0, 0.0}; a1 = cd{0.0, 0.0}; a2 = cd{0.0, 0.0};
+  } else {
+    bessel_j012_c(z, a0, a1, a2);
+  }
+  const cd v = order == 0 ? a0 : (order == 1 ? a1 : a2);
+  outr[t] = v.x;
+  outi[t] = v.y;
+}
+
+cudaError_t launch_bessel_eval(long n, int order, const double* zr, const double* zi, double* outr, double* outi,
+                               cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_bessel_eval<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(n, order, zr, zi, outr, outi);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_bessel(const double* kr, long nk, const double* rho, int nr, double* J0, double* J1, double* J2,

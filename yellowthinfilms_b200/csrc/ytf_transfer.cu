@@ -42,31 +42,34 @@ __device__ __forceinline__ void st(double2* base, long elem, long n, long node, 
 __device__ __forceinline__ const cd& E(const LayerDev& L, int i, int j) { return *reinterpret_cast<const cd*>(&L.eps[2 * ((i - 1) + 3 * (j - 1))]); }
 __device__ __forceinline__ const cd& U(const LayerDev& L, int i, int j) { return *reinterpret_cast<const cd*>(&L.mu[2 * ((i - 1) + 3 * (j - 1))]); }
 
-__device__ __forceinline__ void node_k(const TransferParams& p, long node, double& kx, double& ky) {
+// in-plane wave vector of a node: real except for 1D nodes on a deformed contour (kr_im)
+__device__ __forceinline__ void node_k(const TransferParams& p, long node, cd& kx, cd& ky) {
   if (p.mode == 0) {  // 1D radial nodes kt = (kx, 0)
-    kx = p.kr[node];
-    ky = 0.0;
+    kx = cd{p.kr[node], p.kr_im ? p.kr_im[node] : 0.0};
+    ky = cd{0.0, 0.0};
   } else if (p.mode == 1) {  // full 2D solve, node = k + Nk * q
     long k = node % p.Nk, q = node / p.Nk;
     double s, c;
     sincos(p.phi[q], &s, &c);
-    kx = p.kr[k] * c;
-    ky = p.kr[k] * s;
+    kx = cd{p.kr[k] * c, 0.0};
+    ky = cd{p.kr[k] * s, 0.0};
   } else {  // rotation base: φ = 0
-    kx = p.kr[node] * 1.0;
-    ky = p.kr[node] * 0.0;
+    kx = cd{p.kr[node] * 1.0, 0.0};
+    ky = cd{p.kr[node] * 0.0, 0.0};
   }
 }
 
 // ------------------------------------------------------------------------------------
 // Berreman matrix (mod_ModeSolver.jl:122-193), real in-plane wavevector
 // ------------------------------------------------------------------------------------
-__device__ void berreman(const LayerDev& L, double w, double kx, double ky, cd B[4][4]) {
+// kt enters as a complex pair: real on the real axis; on a deformed contour the matrix is the
+// analytic continuation (no conjugation of kt anywhere, which changes nothing for real kt)
+__device__ void berreman(const LayerDev& L, double w, cd kx, cd ky, cd B[4][4]) {
   cd e11 = E(L, 1, 1), e12 = E(L, 1, 2), e21 = E(L, 2, 1), e22 = E(L, 2, 2);
   cd e13 = E(L, 1, 3), e23 = E(L, 2, 3), e31 = E(L, 3, 1), e32 = E(L, 3, 2), e33 = E(L, 3, 3);
   cd m11 = U(L, 1, 1), m12 = U(L, 1, 2), m21 = U(L, 2, 1), m22 = U(L, 2, 2);
   cd m13 = U(L, 1, 3), m23 = U(L, 2, 3), m31 = U(L, 3, 1), m32 = U(L, 3, 2), m33 = U(L, 3, 3);
-  cd k1{kx, 0.0}, k2{ky, 0.0};
+  const cd k1 = kx, k2 = ky;
   cd de = recip(e33), dm = recip(m33);
   cd iw{1.0 / w, 0.0};
   cd Se11 = e11 - e13 * de * e31, Se12 = e12 - e13 * de * e32;
@@ -75,7 +78,7 @@ __device__ void berreman(const LayerDev& L, double w, double kx, double ky, cd B
   cd Sm21 = m21 - m23 * dm * m31, Sm22 = m22 - m23 * dm * m32;
   cd re1 = de * e31, re2 = de * e32, se1 = e13 * de, se2 = e23 * de;
   cd rm1 = dm * m31, rm2 = dm * m32, sm1 = m13 * dm, sm2 = m23 * dm;
-  cd t21 = -conj(k2), t22 = conj(k1);
+  cd t21 = -k2, t22 = k1;
   cd t31 = iw * k1, t32 = iw * k2;
   cd Rsm1 = sm2, Rsm2 = -sm1, Rse1 = se2, Rse2 = -se1;
   B[0][0] = Rsm1 * t21 - k1 * re1; B[0][1] = Rsm1 * t22 - k1 * re2;
@@ -302,15 +305,23 @@ __device__ bool eig4(cd A[4][4], cd lam[4], cd V[4][4]) {
 }
 
 // closed-form TE/TM modes (mod_ModeSolver.jl:243-265)
-__device__ void closed_modes(const LayerDev& L, double w, double kx, double ky, cd Q[4], cd V[4][4]) {
+__device__ void closed_modes(const LayerDev& L, double w, cd kx, cd ky, cd Q[4], cd V[4][4]) {
   cd et = E(L, 1, 1), ez = E(L, 3, 3), mr = U(L, 1, 1);
   cd wc{w, 0.0};
-  double kr = hypot(kx, ky);
-  double phi = kr == 0 ? 0.0 : atan2(ky, kx);
   double s, c;
-  sincos(phi, &s, &c);
-  cd kzo = csqrt(wc * wc * et * mr - cd{kr * kr, 0.0});
-  cd kze = csqrt(et * (wc * wc * mr - cd{kr * kr, 0.0} / ez));
+  cd kr2;
+  if (kx.y == 0.0 && ky.y == 0.0) {
+    const double kr = hypot(kx.x, ky.x);
+    const double phi = kr == 0 ? 0.0 : atan2(ky.x, kx.x);
+    sincos(phi, &s, &c);
+    kr2 = cd{kr * kr, 0.0};
+  } else {  // complex 1D node on a deformed contour: direction (1, 0), kt² = kx²
+    s = 0.0;
+    c = 1.0;
+    kr2 = kx * kx + ky * ky;
+  }
+  cd kzo = csqrt(wc * wc * et * mr - kr2);
+  cd kze = csqrt(et * (wc * wc * mr - kr2 / ez));
   cd A = recip(wc * mr), Bn = recip(wc * et);
   cd mA = -A, mB = -Bn;
   V[0][0] = cd{-s, 0}; V[1][0] = cd{c, 0}; V[2][0] = mA * kzo * c; V[3][0] = mA * kzo * s;
@@ -333,7 +344,7 @@ __device__ __forceinline__ bool no_z_coupling(const LayerDev& L) {
          iszero(U(L, 2, 3)) && iszero(U(L, 3, 1)) && iszero(U(L, 3, 2));
 }
 
-__device__ bool block_modes(const LayerDev& L, double w, double kx, double ky, cd Q[4], cd V[4][4]) {
+__device__ bool block_modes(const LayerDev& L, double w, cd kx, cd ky, cd Q[4], cd V[4][4]) {
   cd B[4][4];
   berreman(L, w, kx, ky, B);
   // M = B12 B21 (B12 = rows 0-1, cols 2-3; B21 = rows 2-3, cols 0-1)
@@ -449,7 +460,7 @@ constexpr uint8_t ST_NEED_QR = 128;  // internal: this (node, layer) awaits the 
 // flagged for k_layer_modes_qr. Layer-major indexing: one layer, one material kind per warp.
 __device__ __forceinline__ void layer_modes_body(const TransferParams& p, int layer, long node) {
   const long n = p.n;
-  double kx, ky;
+  cd kx, ky;
   node_k(p, p.off + node, kx, ky);
   const LayerDev& L = p.layers[layer];
   cd Q[4], V[4][4];
@@ -473,7 +484,7 @@ __global__ void __launch_bounds__(128) k_layer_modes(TransferParams p) {
 __device__ __forceinline__ void layer_modes_qr_body(const TransferParams& p, int layer, long node) {
   const long n = p.n;
   if (p.lstat[(long)layer * n + node] != ST_NEED_QR) return;
-  double kx, ky;
+  cd kx, ky;
   node_k(p, p.off + node, kx, ky);
   const LayerDev& L = p.layers[layer];
   cd Q[4], V[4][4], B[4][4];
@@ -629,7 +640,7 @@ __device__ __forceinline__ S4 ld_s4(const double2* base, long slot, long n, long
 }
 
 // Source_projection_Berreman_xyz (mod_SourceProj.jl:34-60); returns (sif, sib) 2x3 each
-__device__ bool source_projection(double kx, double ky, double w, const LayerDev& L, const Mode4& M, cd sif[2][3], cd sib[2][3]) {
+__device__ bool source_projection(cd kx, cd ky, double w, const LayerDev& L, const Mode4& M, cd sif[2][3], cd sib[2][3]) {
   cd etz1 = E(L, 1, 3), etz2 = E(L, 2, 3), ezz = E(L, 3, 3);
   cd jw{0.0, -w};
   cd J[4][3];
@@ -637,8 +648,8 @@ __device__ bool source_projection(double kx, double ky, double w, const LayerDev
   cd jz = jw;  // (-iω)·ẑ column only
   for (int q = 0; q < 3; ++q) {
     cd z = q == 2 ? jz : cd{0.0, 0.0} * jw;
-    J[0][q] = cd{kx, 0.0} * z / ezw;
-    J[1][q] = cd{ky, 0.0} * z / ezw;
+    J[0][q] = kx * z / ezw;
+    J[1][q] = ky * z / ezw;
     cd jtx = q == 0 ? jw : cd{0.0, 0.0}, jty = q == 1 ? jw : cd{0.0, 0.0};
     J[2][q] = jty - etz2 * z / ezz;
     J[3][q] = -jtx - (-etz1) * z / ezz;
@@ -673,15 +684,15 @@ __device__ bool source_projection(double kx, double ky, double w, const LayerDev
 
 // mode field basis of one obs layer (mod_CavityTransfer.jl:87-130)
 __device__ void write_basis(const TransferParams& p, int oi, long node, long nout, const LayerDev& L, const Mode4& M,
-                            double kx, double ky) {
+                            cd kx, cd ky) {
   cd ezt1 = E(L, 3, 1), ezt2 = E(L, 3, 2), ezz = E(L, 3, 3);
   double iw = 1.0 / p.omega;
   double2* b = p.basis + (long)oi * 16 * nout;
   for (int m = 0; m < 2; ++m) {
     cd exf = M.vf[0][m], eyf = M.vf[1][m];
-    cd ezf = -(ezt1 * M.vf[0][m] + ezt2 * M.vf[1][m] + iw * (cd{kx, 0} * M.vf[3][m] - cd{ky, 0} * M.vf[2][m])) / ezz;
+    cd ezf = -(ezt1 * M.vf[0][m] + ezt2 * M.vf[1][m] + iw * (kx * M.vf[3][m] - ky * M.vf[2][m])) / ezz;
     cd exb = M.vb[0][m], eyb = M.vb[1][m];
-    cd ezb = -(ezt1 * M.vb[0][m] + ezt2 * M.vb[1][m] + iw * (cd{kx, 0} * M.vb[3][m] - cd{ky, 0} * M.vb[2][m])) / ezz;
+    cd ezb = -(ezt1 * M.vb[0][m] + ezt2 * M.vb[1][m] + iw * (kx * M.vb[3][m] - ky * M.vb[2][m])) / ezz;
     cd kzf = M.qf[m], kzb = M.qb[m];
     bool ok = isfin(exf) && isfin(eyf) && isfin(ezf) && isfin(exb) && isfin(eyb) && isfin(ezb) && isfin(kzf) && isfin(kzb);
     cd z{0, 0};
@@ -742,7 +753,7 @@ __device__ __forceinline__ void chain_body(const TransferParams& p, long node) {
   const long gnode = base ? node : p.off + node;  // index into the outputs
   uint8_t stat = 0;
   for (int l = 0; l < N; ++l) stat |= p.lstat[(long)l * n + node];
-  double kx, ky;
+  cd kx, ky;
   node_k(p, p.off + node, kx, ky);
   const cd z{0.0, 0.0};
   // outputs default to "invalid"
@@ -997,7 +1008,7 @@ __device__ __forceinline__ void chain_src_body(const TransferParams& p, long nod
   const long gnode = base ? node : p.off + node;
   uint8_t stat = 0;
   for (int l = 0; l < N; ++l) stat |= p.lstat[(long)l * n + node];
-  double kx, ky;
+  cd kx, ky;
   node_k(p, p.off + node, kx, ky);
   const cd z{0.0, 0.0};
   if (!p.resp) {  // response mode writes status and resp only
@@ -1205,7 +1216,7 @@ __global__ void __launch_bounds__(128) k_rotate_fill(TransferParams p, const uin
   long k = idx % p.Nk, q = idx / p.Nk;
   double s, c;
   sincos(p.phi[q], &s, &c);
-  double kx = p.kr[k] * c, ky = p.kr[k] * s;
+  const cd kx{p.kr[k] * c, 0.0}, ky{p.kr[k] * s, 0.0};
   p.valid[idx] = 0;
   for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * nout + idx] = 0;
   uint8_t bst = base_status[k];
