@@ -670,6 +670,58 @@ def run_bessel(args):
     return 0
 
 
+def run_contour(args):
+    """The config-1 path: vertical dipole 20 nm above the uniaxial film, 4096 nodes on the
+    deformed contour (512 GL-8 panels, indentation 0.05 k0) to 20 k0, G at 256 radii
+    (6-3000 nm, log) x 64 heights (0-200 nm); one step = transfer build + closed_form_G."""
+    import torch
+    from yellowthinfilms_b200 import api
+    from yellowthinfilms_b200.materials import FlatOpticalLayer, IsotropicMaterial, UniaxialMaterial
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    lam = 600.0
+    k0 = 2 * np.pi / lam
+    layers = [FlatOpticalLayer(IsotropicMaterial(1.0), 200.0),
+              FlatOpticalLayer(UniaxialMaterial(-3.0 + 0.4j, 4.0 + 0.2j), 50.0),
+              FlatOpticalLayer(IsotropicMaterial(2.25), 100.0)]
+    st = api.Stack(layers, ctx)
+    k, w = api.contour_rule(k0, npanels=512, order=8)
+    rho = np.geomspace(6.0, 3000.0, 256)
+    zo = np.linspace(0.0, 200.0, 64)
+    out = torch.empty(256 * 64 * 9, dtype=torch.complex128, device="cuda")
+
+    def step():
+        c = api.build_cavity_transfer_1d_contour(st, k0, 1, k, w, obs_layers=[1])
+        api.closed_form_G(c, 1, 20.0, zo, rho, [0.0], out=out)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    prof = ctx.profile_read()
+    line = {"metric": METRIC, "value": 256 * 64 * 9 / (ms * 1e-3), "unit": "entries/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128 (complex nodes, complex J_n)",
+            "data": "synthetic (the config-1 stack)",
+            "config": {"workload": "vertical dipole 20 nm above a uniaxial film (εo = -3+0.4i, εe = 4+0.2i, 50 nm) on "
+                                   "glass, λ = 600 nm; 4096 nodes on kρ = t - 0.05 i k0 sin(π t / 20 k0); 256 ρ x 64 z",
+                       "entries_per_step": 256 * 64 * 9, "gzz_entries_per_step": 256 * 64},
+            "gzz_entries_per_s": 256 * 64 / (ms * 1e-3), "clocks": clk.summary(),
+            "kernels_ms_per_step": {kk: round(v[0] / args.steps, 4) for kk, v in sorted(prof.items())}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -677,10 +729,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-check", action="store_true")
-    ap.add_argument("--workload", default="gyro32", choices=["gyro32", "uneven", "learned", "bessel"],
+    ap.add_argument("--workload", default="gyro32", choices=["gyro32", "uneven", "learned", "bessel", "contour"],
                     help="gyro32: the 8-layer stack at 32 wavelengths (default); uneven: 1024 uneven stacks; "
                          "learned: learned adaptive quadrature vs the plain fixed rule; bessel: the 1D Bessel synthesis at "
-                         "4096 radii x 65536 nodes x 256 heights")
+                         "4096 radii x 65536 nodes x 256 heights; contour: the config-1 path on the deformed contour")
     ap.add_argument("--per-call", action="store_true",
                     help="one build + synthesis call per wavelength instead of the batched calls")
     ap.add_argument("--precision", default="int8x3", choices=list(DTYPE),
@@ -695,6 +747,8 @@ def main():
         return run_learned(args)
     if args.workload == "bessel":
         return run_bessel(args)
+    if args.workload == "contour":
+        return run_contour(args)
     return run_ours(args)
 
 
