@@ -264,22 +264,25 @@ def measured_peaks():
 
 
 # FP64 operations per node of the per-node solve kernels on this workload, from one ncu count
-# of their DFMA/DADD/DMUL instructions (2 per DFMA); None until captured
-FP64_OPS_PER_NODE = {"k_chain_src": 31.7e3}  # 7.95e8 DFMA + 1.80e8 DADD + 3.10e8 DMUL per 65536-node launch
+# of their DFMA/DADD/DMUL instructions (2 per DFMA); absent until captured
+FP64_OPS_PER_NODE = {"k_iface": 12.4e3,  # 3.16e8 DFMA + 0.74e8 DADD + 1.08e8 DMUL per 65536 nodes
+                     "k_scan": 14.2e3}  # 3.65e8 DFMA + 0.62e8 DADD + 1.40e8 DMUL per 65536 nodes
 FP64_NOMINAL = 37.2  # TFLOP/s: 148 SM x 64 FP64 FMA/clk x 2 x 1.965 GHz (no measured FP64 peak)
 
 
-def roofline(name, prof):
-    """Roofline entry of one kernel from its CUDA-event time in the timed region."""
+def roofline(name, prof, steps=1):
+    """Roofline entry of one kernel from its CUDA-event time in the timed region; every
+    step covers N_LAMBDA x 65536 nodes, in one launch per kernel (batched calls) or one per
+    wavelength."""
     roof = {"kernel": name, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None,
             "traffic": TRAFFIC.get(name)}
     if name is None or name not in prof or not prof[name][1]:
         return roof
     tot_ms, nl = prof[name]
     t = tot_ms / nl * 1e-3  # seconds per launch
-    nodes = N_PANELS * ORDER * N_PHI
+    nodes = N_PANELS * ORDER * N_PHI * N_LAMBDA * steps // nl  # nodes per launch
     cmacs = float(NXY * NXY * nodes * NZ * 9)  # complex multiply-adds of one lateral contraction
-    work = "8 flop per complex multiply-add x 1024 pixels x 65536 nodes x 72 columns per launch"
+    work = f"8 flop per complex multiply-add x 1024 pixels x {nodes} nodes x 72 columns per launch"
     peaks = measured_peaks()
     if name in ("k_lateral_tc", "k_lateral_i8"):
         achieved = 8.0 * cmacs / t / 1e12
@@ -400,9 +403,11 @@ def run_ours(args):
     # profile of the timed region
     top = max(prof.items(), key=lambda kv: kv[1][0])[0] if prof else None
     lateral = next((k for k in ("k_lateral_i8", "k_lateral_tc", "k_lateral") if k in prof), None)
-    roof = roofline(top, prof)
+    roof = roofline(top, prof, args.steps)
     if lateral and lateral != top:
-        roof["lateral"] = roofline(lateral, prof)
+        roof["lateral"] = roofline(lateral, prof, args.steps)
+    if "k_scan" in prof and top != "k_scan":
+        roof["solve"] = roofline("k_scan", prof, args.steps)
     launches = int(sum(v[1] for v in prof.values()))
     line = {"metric": METRIC, "value": value, "unit": "entries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

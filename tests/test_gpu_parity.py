@@ -4,7 +4,7 @@ the per-node cache to 1e-9; k-grid construction bit-exact."""
 import numpy as np
 import pytest
 
-from helpers import (FOUNDATION_STACKS, e_free, krho_grid, lay, m_bi, m_gl, m_gyr, m_gyr4, m_uni, m_vac, relerr,
+from helpers import (FOUNDATION_STACKS, e_free, krho_grid, lay, m_bi, m_biT, m_gl, m_gyr, m_gyr4, m_uni, m_vac, relerr,
                      uniform_phi)
 from yellowthinfilms_b200.materials import IsotropicMaterial, UniaxialMaterial
 
@@ -80,6 +80,39 @@ def test_source_only_chain_matches_general_chain(ytf, oracle, idx):
         for key in ("Qf", "Qb", "sf", "sb"):
             assert relerr(gf[key], gg[key]) < 1e-13, (src, key)
         assert relerr(gf["basis"][0], gg["basis"][i]) < 1e-13, src
+        assert np.array_equal(fast.status()[0], full.status()[0])
+        _cmp_cache(fast, oc)
+
+
+def deep_stack(n_layers=24):
+    """Vacuum / alternating gyrotropic, transposed-biaxial, uniaxial and glass films / vacuum:
+    more than 16 layers, so the mode-matching swaps of layers 16 and up sit past bit 31 of
+    the per-node swap mask."""
+    films = [m_gyr4, m_biT, m_uni, m_gl]
+    st = [lay(m_vac, 0.5)]
+    for i in range(n_layers - 2):
+        st.append(lay(films[i % 4], 0.12 + 0.01 * (i % 3)))
+    st.append(lay(m_vac, 0.5))
+    return st
+
+
+@pytest.mark.gpu
+def test_source_only_chain_deep_stack(ytf, oracle):
+    """24-layer stack, source layers on both sides of layer 16: the forward-only chain agrees
+    with the general chain and with the oracle."""
+    st = deep_stack(24)
+    kr, wr = krho_grid(st, W, kmax=5.0, width=1.0, order=6)
+    ph, wp = uniform_phi(3)
+    N = len(st)
+    for src in (3, 18, N - 1):
+        fast = ytf.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp, obs_layers=[src])
+        full = ytf.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp, obs_layers=list(range(1, N + 1)))
+        oc = oracle.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp, obs_layers=[src])
+        gf, gg = fast.export(), full.export()
+        i = full.obs_layers.index(src)
+        assert relerr(gf["T"][0], gg["T"][i]) < 1e-10, src
+        for key in ("Qf", "Qb", "sf", "sb"):
+            assert relerr(gf[key], gg[key]) < 1e-12, (src, key)
         assert np.array_equal(fast.status()[0], full.status()[0])
         _cmp_cache(fast, oc)
 

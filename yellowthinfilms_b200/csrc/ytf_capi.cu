@@ -316,6 +316,15 @@ void fill_params(TransferParams& p, const ytf_stack* st, const ytf_cache* c) {
   p.basis = c->d_basis;
 }
 
+// the forward-only chain (every observation layer is the source layer)
+int launch_forward_chain(ytf_ctx* ctx, const TransferParams& p) {
+  CK(LAUNCH("k_match", launch_chain_part(0, p, ctx->stream)));
+  CK(LAUNCH("k_seeds", launch_chain_part(1, p, ctx->stream)));
+  CK(LAUNCH("k_iface", launch_chain_part(2, p, ctx->stream)));
+  CK(LAUNCH("k_scan", launch_chain_part(3, p, ctx->stream)));
+  return YTF_OK;
+}
+
 // per-node scratch bytes of the transfer kernels
 size_t scratch_per_node(int N, uint32_t needL, uint32_t needR) {
   size_t b = (size_t)N * 20 * 16 + (size_t)std::max(N - 1, 1) * 16 * 16 + (size_t)N;
@@ -334,6 +343,7 @@ int run_transfer(ytf_ctx* ctx, TransferParams p, long total) {
   WS(modes, double2, "tr_modes", (size_t)N * 20 * chunk);
   WS(lstat, uint8_t, "tr_lstat", (size_t)N * chunk);
   WS(sint, double2, "tr_sint", (size_t)std::max(N - 1, 1) * 16 * chunk);
+  WS(swaps, uint64_t, "tr_swaps", (size_t)chunk);
   double2* sleft = nullptr;
   double2* sright = nullptr;
   if (p.needL) { WS(sl, double2, "tr_sleft", (size_t)N * 16 * chunk); sleft = sl; }
@@ -341,6 +351,7 @@ int run_transfer(ytf_ctx* ctx, TransferParams p, long total) {
   p.modes = modes;
   p.lstat = lstat;
   p.sint = sint;
+  p.swaps = swaps;
   p.sleft = sleft;
   p.sright = sright;
   for (long off = 0; off < total; off += chunk) {
@@ -348,7 +359,9 @@ int run_transfer(ytf_ctx* ctx, TransferParams p, long total) {
     p.n = std::min(chunk, total - off);
     CK(LAUNCH("k_layer_modes", launch_layer_modes(p, ctx->stream)));
     CK(LAUNCH("k_layer_modes_qr", launch_layer_modes_qr(p, ctx->stream)));
-    if (only_source_observed(p)) CK(LAUNCH("k_chain_src", launch_chain_src(p, ctx->stream)));
+    if (only_source_observed(p)) {
+      if (int rc = launch_forward_chain(ctx, p)) return rc;
+    }
     else CK(LAUNCH("k_chain", launch_chain(p, ctx->stream)));
   }
   return YTF_OK;
@@ -562,6 +575,8 @@ int solve_rotation(ytf_ctx* ctx, const ytf_stack* st, ytf_cache* c, const Transf
   b.modes = modes;
   b.lstat = lstat;
   b.sint = sint;
+  WS(bsw, uint64_t, "tr_swaps", (size_t)nb);
+  b.swaps = bsw;
   if (b.needL) { WS(sl, double2, "tr_sleft", (size_t)N * 16 * nb); b.sleft = sl; }
   if (b.needR) { WS(sr, double2, "tr_sright", (size_t)N * 16 * nb); b.sright = sr; }
   b.status = bstat;
@@ -569,7 +584,9 @@ int solve_rotation(ytf_ctx* ctx, const ytf_stack* st, ytf_cache* c, const Transf
   b.Tout = bT;
   CK(LAUNCH("k_layer_modes", launch_layer_modes(b, ctx->stream)));
   CK(LAUNCH("k_layer_modes_qr", launch_layer_modes_qr(b, ctx->stream)));
-  if (only_source_observed(b)) CK(LAUNCH("k_chain_src", launch_chain_src(b, ctx->stream)));
+  if (only_source_observed(b)) {
+    if (int rc = launch_forward_chain(ctx, b)) return rc;
+  }
   else CK(LAUNCH("k_chain", launch_chain(b, ctx->stream)));
   TransferParams f = p;
   f.mode = 1;
@@ -854,11 +871,12 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
     const int N = ps[i].nL;
     const bool fast = only_source_observed(ps[i]);
     size_t per = (size_t)N * 20 * 16 + (size_t)N;
+    if (fast) per += (size_t)std::max(N - 1, 1) * 16 * 16 + 8;
     if (!fast) per = scratch_per_node(N, ps[i].needL, ps[i].needR);
-    scratch[i] = per * (size_t)cs[i]->n + 4 * 256;
+    scratch[i] = per * (size_t)cs[i]->n + 5 * 256;
   }
   // per pass: every item's block, then the forward-only and general subsets, 3 offset arrays
-  size_t pbytes = 2 * (size_t)nb * sizeof(TransferParams) + 3 * (size_t)(nb + 1) * sizeof(long);
+  size_t pbytes = 2 * (size_t)nb * sizeof(TransferParams) + 4 * (size_t)(nb + 1) * sizeof(long);
   char* h = (char*)pinned_staging(ctx, 8 * std::max<size_t>(stage, 1) + pbytes + 64);
   if (!h) return abort_all(fail(ctx, YTF_ERR_NOMEM, "build_cavity_transfer: page-locked staging allocation failed"));
   {
@@ -911,6 +929,7 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
     long* offm = (long*)(hp + m);
     long* offs = offm + (m + 1);
     long* offg = offs + (m + 1);
+    long* offi = offg + (m + 1);
     std::vector<int> fast_ids, gen_ids;
     offm[0] = 0;
     for (int j = 0; j < m; ++j) {
@@ -920,6 +939,8 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
       q.modes = (double2*)carve((size_t)N * 20 * 16 * n);
       q.lstat = (uint8_t*)carve((size_t)N * n);
       if (only_source_observed(q)) {
+        q.sint = (double2*)carve((size_t)std::max(N - 1, 1) * 16 * 16 * n);
+        q.swaps = (uint64_t*)carve((size_t)8 * n);
         fast_ids.push_back(j);
       } else {
         q.sint = (double2*)carve((size_t)std::max(N - 1, 1) * 16 * 16 * n);
@@ -936,10 +957,16 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
     std::memcpy(hp, all.data(), sizeof(TransferParams) * m);
     offs[0] = 0;
     offg[0] = 0;
+    offi[0] = 0;
     std::vector<TransferParams> pf, pg;
-    for (int j = 0; j < nf; ++j) { pf.push_back(all[fast_ids[j]]); offs[j + 1] = offs[j] + all[fast_ids[j]].n; }
+    for (int j = 0; j < nf; ++j) {
+      const TransferParams& q = all[fast_ids[j]];
+      pf.push_back(q);
+      offs[j + 1] = offs[j] + q.n;
+      offi[j + 1] = offi[j] + (long)(q.nL - 1) * q.n;
+    }
     for (int j = 0; j < ng; ++j) { pg.push_back(all[gen_ids[j]]); offg[j + 1] = offg[j] + all[gen_ids[j]].n; }
-    const size_t blk = sizeof(TransferParams) * m + 3 * sizeof(long) * (m + 1);
+    const size_t blk = sizeof(TransferParams) * m + 4 * sizeof(long) * (m + 1);
     TransferParams* hpf = (TransferParams*)(h + blk);
     TransferParams* hpg = hpf + nf;
     if (nf) std::memcpy(hpf, pf.data(), sizeof(TransferParams) * nf);
@@ -951,11 +978,17 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
     const long* doffm = (const long*)(dp + m);
     const long* doffs = doffm + (m + 1);
     const long* doffg = doffs + (m + 1);
+    const long* doffi = doffg + (m + 1);
     const TransferParams* dpf = (const TransferParams*)(dpar + blk);
     const TransferParams* dpg = dpf + nf;
     CK(LAUNCH("k_layer_modes", launch_transfer_batch(0, dp, doffm, m, offm[m], ctx->stream)));
     CK(LAUNCH("k_layer_modes_qr", launch_transfer_batch(1, dp, doffm, m, offm[m], ctx->stream)));
-    if (nf) CK(LAUNCH("k_chain_src", launch_transfer_batch(2, dpf, doffs, nf, offs[nf], ctx->stream)));
+    if (nf) {
+      CK(LAUNCH("k_match", launch_transfer_batch(4, dpf, doffs, nf, offs[nf], ctx->stream)));
+      CK(LAUNCH("k_seeds", launch_transfer_batch(5, dpf, doffs, nf, offs[nf], ctx->stream)));
+      if (offi[nf]) CK(LAUNCH("k_iface", launch_transfer_batch(6, dpf, doffi, nf, offi[nf], ctx->stream)));
+      CK(LAUNCH("k_scan", launch_transfer_batch(7, dpf, doffs, nf, offs[nf], ctx->stream)));
+    }
     if (ng) CK(LAUNCH("k_chain", launch_transfer_batch(3, dpg, doffg, ng, offg[ng], ctx->stream)));
     // the staging block is reused by the next pass: let this pass's upload land first
     if (first < nb) CK(cudaStreamSynchronize(ctx->stream));

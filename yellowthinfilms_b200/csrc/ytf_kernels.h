@@ -46,6 +46,7 @@ struct TransferParams {
   double2* sint;           // [nL-1][16][n]
   double2* sleft;          // [nL][16][n]
   double2* sright;         // [nL][16][n]
+  uint64_t* swaps;         // [n] matching swaps per node, 2 bits per layer (split forward-only chain)
   // outputs
   uint8_t* status;         // [nout] (rotation base: [n])
   uint8_t* valid;          // [nout]
@@ -56,7 +57,7 @@ struct TransferParams {
   double2* sf;             // [6][nout], column-major 2x3
   double2* sb;             // [6][nout]
   double2* basis;          // [nobs][16][nout]: exf0 exf1 eyf0 eyf1 ezf0 ezf1 exb.. eyb.. ezb.. kzf0 kzf1 kzb0 kzb1
-  // response mode of the forward-only chain (_cavity_response): when set, k_chain_src writes
+  // response mode of the forward-only chain (_cavity_response): when set, k_scan writes
   // resp[node] and the status only (no T^o, seeds, basis, valid flags)
   double* resp;            // [nout]
 };
@@ -64,10 +65,12 @@ struct TransferParams {
 cudaError_t launch_layer_modes(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_layer_modes_qr(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream);
-// k_chain when every observation layer is the source layer
-cudaError_t launch_chain_src(const TransferParams& p, cudaStream_t stream);
+// k_chain when every observation layer is the source layer, as four kernels: part 0..3 =
+// k_match, k_seeds, k_iface, k_scan, launched in that order (needs the sint and swaps scratch)
+cudaError_t launch_chain_part(int part, const TransferParams& p, cudaStream_t stream);
 // batched transfer kernels over nb problems (device arrays probs[nb], off[nb + 1]; total =
-// off[nb]): kernel 0 = layer modes, 1 = general QR pass, 2 = forward-only chain, 3 = chain
+// off[nb]): kernel 0 = layer modes, 1 = general QR pass, 3 = chain, 4-7 = the forward-only
+// chain (match, seeds, iface (off over (nL - 1) n interface-node pairs), scan)
 cudaError_t launch_transfer_batch(int kernel, const TransferParams* probs, const long* off, int nb, long total,
                                   cudaStream_t stream);
 cudaError_t launch_rotate_fill(const TransferParams& p, const uint8_t* base_status, const uint8_t* base_tvalid,

@@ -937,12 +937,21 @@ __device__ __forceinline__ void chain_body(const TransferParams& p, long node) {
 // K2': the same solve when every observation layer is the source layer (needL = needR = 0):
 // no walk to other layers, so SRight is needed at the source layer only. The Redheffer
 // product is associative, so SRight[src] = eff_src ⋆ eff_src+1 ⋆ … ⋆ eff_N-1 accumulates in
-// the forward sweep (left to right) instead of a backward scan over stored interface
-// matrices: N-1 star products instead of N-1 + (N-src), and no interface, SRight or
-// matched-mode records written. One S4 register set serves as the SLeft prefix up to the
-// source layer and as the SRight product after it. The mode vectors of a layer are read
-// from the (read-only) mode records with its matching swaps applied instead of being held
-// across iterations.
+// a forward sweep (left to right) instead of a backward scan: N-1 star products instead of
+// N-1 + (N-src), and no SLeft, SRight or matched-mode records. One S4 register set serves as
+// the SLeft prefix up to the source layer and as the SRight product after it. The solve runs
+// as four kernels with short code, so that more warps stay resident than in one fused
+// kernel (255 registers with spills):
+//   k_match  (per node)             mode matching down the stack -> a 64-bit swap mask
+//   k_seeds  (per node)             source projection and mode basis of the source layer
+//   k_iface  (per node, interface)  the interface matrix (4x4 LU); past the source layer the
+//                                   propagation of the layer on its left folded in:
+//                                   X_j = diag(e^{iQf d}, e^{-iQb d}) ⋆ Sint_j
+//   k_scan   (per node)             acc = acc ⋆ X_j over the interfaces, cavity, T^o
+// The interface matrices live in the `sint` scratch, the swap masks in `swaps`; the LU
+// failures and the projection's status travel in the layer status bytes, which k_scan reads
+// and translates. The mode vectors are read from the read-only mode records with the
+// matching swaps applied.
 // ------------------------------------------------------------------------------------
 // largest singular value of a 2x2 complex matrix: √ of the larger eigenvalue of A^H A
 __device__ __forceinline__ double sigma_max2(const M2& A) {
@@ -956,7 +965,7 @@ struct ModeV {  // one layer's mode vectors: Vf, Vb (4x2)
   cd vf[4][2], vb[4][2];
 };
 
-__device__ __forceinline__ void load_v(const TransferParams& p, int layer, long node, uint32_t swaps, ModeV& M) {
+__device__ __forceinline__ void load_v(const TransferParams& p, int layer, long node, uint64_t swaps, ModeV& M) {
   const double2* rec = p.modes + (long)layer * 20 * p.n;
   const int sf = (swaps >> (2 * layer)) & 1, sb = (swaps >> (2 * layer + 1)) & 1;
 #pragma unroll
@@ -967,7 +976,7 @@ __device__ __forceinline__ void load_v(const TransferParams& p, int layer, long 
       M.vb[i][m] = ld(rec, 8 + i + 4 * (m ^ sb), p.n, node);
     }
 }
-__device__ __forceinline__ void load_q(const TransferParams& p, int layer, long node, uint32_t swaps, cd qf[2], cd qb[2]) {
+__device__ __forceinline__ void load_q(const TransferParams& p, int layer, long node, uint64_t swaps, cd qf[2], cd qb[2]) {
   const double2* rec = p.modes + (long)layer * 20 * p.n;
   const int sf = (swaps >> (2 * layer)) & 1, sb = (swaps >> (2 * layer + 1)) & 1;
 #pragma unroll
@@ -976,7 +985,7 @@ __device__ __forceinline__ void load_q(const TransferParams& p, int layer, long 
     qb[m] = ld(rec, 18 + (m ^ sb), p.n, node);
   }
 }
-__device__ __forceinline__ void load_matched(const TransferParams& p, int layer, long node, uint32_t swaps, Mode4& M) {
+__device__ __forceinline__ void load_matched(const TransferParams& p, int layer, long node, uint64_t swaps, Mode4& M) {
   ModeV v;
   load_v(p, layer, node, swaps, v);
 #pragma unroll
@@ -1000,18 +1009,86 @@ __device__ __forceinline__ bool match_swap(const cd va[4][2], const cd vb[4][2])
   return norm2(C[0][1]) + norm2(C[1][0]) > norm2(C[0][0]) + norm2(C[1][1]);
 }
 
-__device__ __forceinline__ void chain_src_body(const TransferParams& p, long node) {
+constexpr uint8_t ST_PROJ_SINGULAR = 64;  // internal: the source projection's 4x4 solve failed
+
+__device__ __forceinline__ uint8_t node_status(const TransferParams& p, long node) {
+  uint8_t stat = 0;
+  for (int l = 0; l < p.nL; ++l) stat |= p.lstat[(long)l * p.n + node];
+  return stat;
+}
+
+__device__ __forceinline__ void match_body(const TransferParams& p, long node) {
+  const uint8_t stat = node_status(p, node);
+  uint64_t swaps = 0;
+  if (!(stat & (ST_EIGEN | ST_SORT)))
+    for (int j = 2; j <= p.nL; ++j) {
+      ModeV va, vb;
+      load_v(p, j - 2, node, swaps, va);
+      load_v(p, j - 1, node, 0, vb);
+      const bool sf = match_swap(va.vf, vb.vf), sb = match_swap(va.vb, vb.vb);
+      swaps |= (uint64_t)(sf ? 1 : 0) << (2 * (j - 1)) | (uint64_t)(sb ? 1 : 0) << (2 * (j - 1) + 1);
+    }
+  p.swaps[node] = swaps;
+}
+
+__device__ __forceinline__ void seeds_body(const TransferParams& p, long node) {
+  if (p.mode == 2 || p.resp) return;
+  if (node_status(p, node) & (ST_EIGEN | ST_SORT)) return;
+  const long gnode = p.off + node;
+  const int layer = p.src - 1;
+  cd kx, ky;
+  node_k(p, p.off + node, kx, ky);
+  Mode4 M;
+  load_matched(p, layer, node, p.swaps[node], M);
+  cd sif[2][3], sib[2][3];
+  const bool ok = source_projection(kx, ky, p.omega, p.layers[layer], M, sif, sib);
+  bool fin = true;
+  for (int m = 0; m < 2; ++m)
+    for (int q = 0; q < 3; ++q) fin = fin && isfin(sif[m][q]) && isfin(sib[m][q]);
+  write_seeds(p, gnode, p.nout, M, sif, sib);
+  for (int oi = 0; oi < p.nobs; ++oi) write_basis(p, oi, gnode, p.nout, p.layers[layer], M, kx, ky);
+  uint8_t f = 0;
+  if (!ok) f |= ST_PROJ_SINGULAR;
+  if (!(ok && fin)) f |= ST_SEEDS;
+  if (f) p.lstat[(long)layer * p.n + node] |= f;
+}
+
+__device__ __forceinline__ void iface_body(const TransferParams& p, int j, long node) {
+  const uint64_t swaps = p.swaps[node];
+  const int a = j - 2, b = j - 1;
+  S4 X;
+  {
+    ModeV va, vb;
+    load_v(p, a, node, swaps, va);
+    load_v(p, b, node, swaps, vb);
+    Mode4 A, B;
+    for (int i = 0; i < 4; ++i)
+      for (int m = 0; m < 2; ++m) {
+        A.vf[i][m] = va.vf[i][m]; A.vb[i][m] = va.vb[i][m];
+        B.vf[i][m] = vb.vf[i][m]; B.vb[i][m] = vb.vb[i][m];
+      }
+    if (!interface_matrix(A, B, X)) p.lstat[(long)b * p.n + node] |= ST_SINGULAR;
+  }
+  if (j > p.src) {
+    cd qf[2], qb[2];
+    load_q(p, a, node, swaps, qf, qb);
+    const double d = p.layers[a].d;
+    X = redheffer_diag_left(expi(qf[0], d), expi(qf[1], d), expi(-qb[0], d), expi(-qb[1], d), X);
+  }
+  st_s4(p.sint, j - 2, p.n, node, X);
+}
+
+__device__ __forceinline__ void scan_body(const TransferParams& p, long node) {
   const long n = p.n;
   const int N = p.nL, src = p.src;
   const bool base = p.mode == 2;
   const long nT = base ? n : p.nout;
   const long gnode = base ? node : p.off + node;
-  uint8_t stat = 0;
-  for (int l = 0; l < N; ++l) stat |= p.lstat[(long)l * n + node];
-  cd kx, ky;
-  node_k(p, p.off + node, kx, ky);
+  uint8_t stat = node_status(p, node);
+  const bool seeds_ok = !(stat & ST_PROJ_SINGULAR), seeds_fin = !(stat & ST_SEEDS);
+  stat &= (uint8_t)~(ST_PROJ_SINGULAR | ST_SEEDS);
   const cd z{0.0, 0.0};
-  if (!p.resp) {  // response mode writes status and resp only
+  if (!p.resp) {
     if (!base) p.valid[gnode] = 0;
     for (int oi = 0; oi < p.nobs; ++oi) p.tvalid[(long)oi * nT + gnode] = 0;
   }
@@ -1020,25 +1097,13 @@ __device__ __forceinline__ void chain_src_body(const TransferParams& p, long nod
     if (p.resp) p.resp[gnode] = 0.0;
     return;
   }
-  uint32_t swaps = 0;  // bit 2l: forward columns of layer l swapped by matching, bit 2l+1: backward
-  bool seeds_ok = true, seeds_fin = true;
-  auto seeds_and_basis = [&](int layer) {  // layer 0-based, the source layer
-    if (base || p.resp) return;
-    Mode4 M;
-    load_matched(p, layer, node, swaps, M);
-    cd sif[2][3], sib[2][3];
-    seeds_ok = source_projection(kx, ky, p.omega, p.layers[layer], M, sif, sib);
-    for (int m = 0; m < 2; ++m)
-      for (int q = 0; q < 3; ++q) seeds_fin = seeds_fin && isfin(sif[m][q]) && isfin(sib[m][q]);
-    write_seeds(p, gnode, p.nout, M, sif, sib);
-    for (int oi = 0; oi < p.nobs; ++oi) write_basis(p, oi, gnode, p.nout, p.layers[layer], M, kx, ky);
-  };
-  cd Qs[4];  // Qf0 Qf1 Qb0 Qb1 of the source layer
+  const uint64_t swaps = p.swaps[node];
+  cd Qs[4];
   M2 RL = M2{z, z, z, z};
   S4 acc;
   {
     cd qf[2], qb[2];
-    load_q(p, 0, node, 0u, qf, qb);
+    load_q(p, 0, node, 0, qf, qb);
     const double d0 = p.layers[0].d;
     if (src == 1) {
       Qs[0] = qf[0]; Qs[1] = qf[1]; Qs[2] = qb[0]; Qs[3] = qb[1];
@@ -1047,47 +1112,28 @@ __device__ __forceinline__ void chain_src_body(const TransferParams& p, long nod
       acc = s4_diag(expi(qf[0], d0), expi(qf[1], d0), expi(-qb[0], d0), expi(-qb[1], d0));
     }
   }
-  // one star product per interface: up to the source layer acc = SLeft ⋆ Sint, then the
-  // propagation of the next layer on the right; after it acc ⋆ (diag(prop of layer j-1) ⋆ Sint)
   for (int j = 2; j <= N; ++j) {
-    const int a = j - 2, b = j - 1;  // 0-based layers on either side of interface j-1|j
-    S4 X;
-    {
-      ModeV va, vb;
-      load_v(p, a, node, swaps, va);
-      load_v(p, b, node, 0u, vb);
-      const bool sf = match_swap(va.vf, vb.vf), sb = match_swap(va.vb, vb.vb);
-      swaps |= (sf ? 1u : 0u) << (2 * b) | (sb ? 1u : 0u) << (2 * b + 1);
-      Mode4 A, B;
-      for (int i = 0; i < 4; ++i)
-        for (int m = 0; m < 2; ++m) {
-          A.vf[i][m] = va.vf[i][m]; A.vb[i][m] = va.vb[i][m];
-          B.vf[i][m] = sf ? vb.vf[i][1 - m] : vb.vf[i][m];
-          B.vb[i][m] = sb ? vb.vb[i][1 - m] : vb.vb[i][m];
-        }
-      if (!interface_matrix(A, B, X)) stat |= ST_SINGULAR;
-    }
-    const bool left = j <= src;
-    cd qf[2], qb[2];
-    load_q(p, left ? b : a, node, swaps, qf, qb);
-    const double d = p.layers[left ? b : a].d;
-    const cd pf0 = expi(qf[0], d), pf1 = expi(qf[1], d), pb0 = expi(-qb[0], d), pb1 = expi(-qb[1], d);
-    if (!left) X = redheffer_diag_left(pf0, pf1, pb0, pb1, X);
+    const S4 X = ld_s4(p.sint, j - 2, n, node);
     const S4 R = redheffer(acc, X);
-    if (!left) {
+    if (j > src) {
       acc = R;
-    } else if (j == src) {
-      RL = R.b12;
-      Qs[0] = qf[0]; Qs[1] = qf[1]; Qs[2] = qb[0]; Qs[3] = qb[1];
-      acc = s4_identity();
     } else {
-      acc.b11 = dl(pf0, pf1, R.b11);
-      acc.b12 = dl(pf0, pf1, dr(R.b12, pb0, pb1));
-      acc.b21 = R.b21;
-      acc.b22 = dr(R.b22, pb0, pb1);
+      cd qf[2], qb[2];
+      load_q(p, j - 1, node, swaps, qf, qb);
+      if (j == src) {
+        RL = R.b12;
+        Qs[0] = qf[0]; Qs[1] = qf[1]; Qs[2] = qb[0]; Qs[3] = qb[1];
+        acc = s4_identity();
+      } else {
+        const double d = p.layers[j - 1].d;
+        const cd pf0 = expi(qf[0], d), pf1 = expi(qf[1], d), pb0 = expi(-qb[0], d), pb1 = expi(-qb[1], d);
+        acc.b11 = dl(pf0, pf1, R.b11);
+        acc.b12 = dl(pf0, pf1, dr(R.b12, pb0, pb1));
+        acc.b21 = R.b21;
+        acc.b22 = dr(R.b22, pb0, pb1);
+      }
     }
   }
-  seeds_and_basis(src - 1);
   if (stat & ST_SINGULAR) {
     p.status[gnode] = stat;
     if (p.resp) p.resp[gnode] = 0.0;
@@ -1146,13 +1192,29 @@ __device__ __forceinline__ void chain_src_body(const TransferParams& p, long nod
   p.status[gnode] = stat;
 }
 
+__global__ void __launch_bounds__(128) k_match(TransferParams p) {
+  const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (node < p.n) match_body(p, node);
+}
+__global__ void __launch_bounds__(128) k_seeds(TransferParams p) {
+  const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (node < p.n) seeds_body(p, node);
+}
+__global__ void __launch_bounds__(128) k_iface(TransferParams p) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long n = p.n;
+  if (t >= n * (p.nL - 1)) return;
+  const int j = (int)(t / n) + 2;
+  iface_body(p, j, t - (long)(j - 2) * n);
+}
+__global__ void __launch_bounds__(128) k_scan(TransferParams p) {
+  const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (node < p.n) scan_body(p, node);
+}
+
 __global__ void __launch_bounds__(128) k_chain(TransferParams p) {
   const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (node < p.n) chain_body(p, node);
-}
-__global__ void __launch_bounds__(128) k_chain_src(TransferParams p) {
-  const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (node < p.n) chain_src_body(p, node);
 }
 
 // ------------------------------------------------------------------------------------
@@ -1196,13 +1258,6 @@ __global__ void __launch_bounds__(128) k_chain_batch(const TransferParams* __res
   if (t >= off[nb]) return;
   const int i = find_problem(off, nb, t);
   chain_body(probs[i], t - off[i]);
-}
-__global__ void __launch_bounds__(128) k_chain_src_batch(const TransferParams* __restrict__ probs,
-                                                         const long* __restrict__ off, int nb) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= off[nb]) return;
-  const int i = find_problem(off, nb, t);
-  chain_src_body(probs[i], t - off[i]);
 }
 
 // ------------------------------------------------------------------------------------
@@ -1275,15 +1330,56 @@ cudaError_t launch_layer_modes_qr(const TransferParams& p, cudaStream_t stream) 
   return cudaGetLastError();
 }
 
-cudaError_t launch_chain_src(const TransferParams& p, cudaStream_t stream) {
-  if (p.n <= 0) return cudaSuccess;
-  k_chain_src<<<(unsigned)((p.n + 127) / 128), 128, 0, stream>>>(p);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream) {
   if (p.n <= 0) return cudaSuccess;
   k_chain<<<(unsigned)((p.n + 127) / 128), 128, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(128) k_match_batch(const TransferParams* __restrict__ probs, const long* __restrict__ off,
+                                                     int nb) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= off[nb]) return;
+  const int i = find_problem(off, nb, t);
+  match_body(probs[i], t - off[i]);
+}
+__global__ void __launch_bounds__(128) k_seeds_batch(const TransferParams* __restrict__ probs, const long* __restrict__ off,
+                                                     int nb) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= off[nb]) return;
+  const int i = find_problem(off, nb, t);
+  seeds_body(probs[i], t - off[i]);
+}
+// off: per-item (nL - 1) x n interface-node pairs
+__global__ void __launch_bounds__(128) k_iface_batch(const TransferParams* __restrict__ probs, const long* __restrict__ off,
+                                                     int nb) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= off[nb]) return;
+  const int i = find_problem(off, nb, t);
+  const TransferParams& p = probs[i];
+  const long lt = t - off[i];
+  const int j = (int)(lt / p.n) + 2;
+  iface_body(p, j, lt - (long)(j - 2) * p.n);
+}
+__global__ void __launch_bounds__(128) k_scan_batch(const TransferParams* __restrict__ probs, const long* __restrict__ off,
+                                                    int nb) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= off[nb]) return;
+  const int i = find_problem(off, nb, t);
+  scan_body(probs[i], t - off[i]);
+}
+
+cudaError_t launch_chain_part(int part, const TransferParams& p, cudaStream_t stream) {
+  if (p.n <= 0) return cudaSuccess;
+  const unsigned g = (unsigned)((p.n + 127) / 128);
+  switch (part) {
+    case 0: k_match<<<g, 128, 0, stream>>>(p); break;
+    case 1: k_seeds<<<g, 128, 0, stream>>>(p); break;
+    case 2:
+      if (p.nL > 1) k_iface<<<(unsigned)((p.n * (p.nL - 1) + 127) / 128), 128, 0, stream>>>(p);
+      break;
+    default: k_scan<<<g, 128, 0, stream>>>(p); break;
+  }
   return cudaGetLastError();
 }
 
@@ -1294,7 +1390,10 @@ cudaError_t launch_transfer_batch(int kernel, const TransferParams* probs, const
   switch (kernel) {
     case 0: k_layer_modes_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
     case 1: k_layer_modes_qr_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
-    case 2: k_chain_src_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
+    case 4: k_match_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
+    case 5: k_seeds_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
+    case 6: k_iface_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
+    case 7: k_scan_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
     default: k_chain_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
   }
   return cudaGetLastError();
