@@ -40,7 +40,16 @@ __host__ __device__ __forceinline__ cd operator/(cd a, cd b) {
   return cd{(a.x * r + a.y) / den, (a.y * r - a.x) / den};
 }
 __host__ __device__ __forceinline__ cd operator/(cd a, double s) { return cd{a.x / s, a.y / s}; }
-__host__ __device__ __forceinline__ cd recip(cd b) { return cd{1.0, 0.0} / b; }
+// 1 / b by Smith's scaling with two real divisions
+__host__ __device__ __forceinline__ cd recip(cd b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    if (b.x == 0.0 && b.y == 0.0) return cd{1.0 / b.x, 0.0 / b.x};
+    const double r = b.y / b.x, t = 1.0 / (b.x + b.y * r);
+    return cd{t, -r * t};
+  }
+  const double r = b.x / b.y, t = 1.0 / (b.x * r + b.y);
+  return cd{r * t, -t};
+}
 
 // principal square root, signed-zero aware (branch cut on the negative real axis)
 __host__ __device__ __forceinline__ cd csqrt(cd z) {
@@ -76,15 +85,15 @@ __host__ __device__ __forceinline__ M2 imin(const M2& A) {  // I - A
   return M2{cd{1.0 - A.a00.x, -A.a00.y}, -A.a01, -A.a10, cd{1.0 - A.a11.x, -A.a11.y}};
 }
 __host__ __device__ __forceinline__ cd det(const M2& A) { return A.a00 * A.a11 - A.a01 * A.a10; }
-// A \ B by Cramer's rule
+// A \ B by Cramer's rule (one reciprocal of the determinant)
 __host__ __device__ __forceinline__ M2 solve(const M2& A, const M2& B) {
-  cd d = det(A);
-  return M2{(A.a11 * B.a00 - A.a01 * B.a10) / d, (A.a11 * B.a01 - A.a01 * B.a11) / d,
-            (A.a00 * B.a10 - A.a10 * B.a00) / d, (A.a00 * B.a11 - A.a10 * B.a01) / d};
+  const cd r = recip(det(A));
+  return M2{(A.a11 * B.a00 - A.a01 * B.a10) * r, (A.a11 * B.a01 - A.a01 * B.a11) * r,
+            (A.a00 * B.a10 - A.a10 * B.a00) * r, (A.a00 * B.a11 - A.a10 * B.a01) * r};
 }
 __host__ __device__ __forceinline__ M2 inv(const M2& A) {
-  cd d = det(A);
-  return M2{A.a11 / d, -A.a01 / d, -A.a10 / d, A.a00 / d};
+  const cd r = recip(det(A));
+  return M2{A.a11 * r, -(A.a01 * r), -(A.a10 * r), A.a00 * r};
 }
 // diag(p) * A and A * diag(p)
 __host__ __device__ __forceinline__ M2 dl(cd p0, cd p1, const M2& A) { return M2{p0 * A.a00, p0 * A.a01, p1 * A.a10, p1 * A.a11}; }
@@ -103,15 +112,18 @@ __host__ __device__ __forceinline__ S4 s4_diag(cd p0, cd p1, cd p2, cd p3) {
   return S4{M2{p0, z, z, p1}, M2{z, z, z, z}, M2{z, z, z, z}, M2{p2, z, z, p3}};
 }
 
-// Redheffer star product (mod_ScatteringMatrix.jl:65-85)
+// Redheffer star product (mod_ScatteringMatrix.jl:65-85), regrouped around the two 2x2
+// inverses: E = B11 (I - A12 B21)^-1, F = A22 (I - B21 A12)^-1, then
+//   S11 = E A11, S12 = B12 + E A12 B22, S21 = A21 + F B21 A11, S22 = F B22
+// (two complex reciprocals instead of sixteen complex divisions)
 __host__ __device__ __forceinline__ S4 redheffer(const S4& A, const S4& B) {
-  M2 D1 = imin(mul(A.b12, B.b21));
-  M2 D2 = imin(mul(B.b21, A.b12));
+  const M2 E = mul(B.b11, inv(imin(mul(A.b12, B.b21))));
+  const M2 F = mul(A.b22, inv(imin(mul(B.b21, A.b12))));
   S4 o;
-  o.b11 = mul(B.b11, solve(D1, A.b11));
-  o.b12 = add(B.b12, mul(B.b11, mul(solve(D1, A.b12), B.b22)));
-  o.b21 = add(A.b21, mul(A.b22, mul(solve(D2, B.b21), A.b11)));
-  o.b22 = mul(A.b22, solve(D2, B.b22));
+  o.b11 = mul(E, A.b11);
+  o.b12 = add(B.b12, mul(mul(E, A.b12), B.b22));
+  o.b21 = add(A.b21, mul(mul(F, B.b21), A.b11));
+  o.b22 = mul(F, B.b22);
   return o;
 }
 // Redheffer with a diagonal left factor diag(p0,p1,p2,p3) (blocks 12 = 21 = 0)

@@ -562,6 +562,7 @@ __device__ __forceinline__ void match_dir(const cd wa_src[4][2], cd vb[4][2], cd
 template <int NR>
 __device__ __forceinline__ bool lu_solve4(cd A[4][4], cd B[4][NR]) {
   bool ok = true;
+  cd rp[4];  // reciprocal pivots, reused by the back substitution
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     int pv = k;
@@ -589,6 +590,7 @@ __device__ __forceinline__ bool lu_solve4(cd A[4][4], cd B[4][NR]) {
       }
     }
     const cd piv = recip(A[k][k]);
+    rp[k] = piv;
 #pragma unroll
     for (int i = k + 1; i < 4; ++i) {
       const cd l = A[i][k] * piv;
@@ -606,7 +608,7 @@ __device__ __forceinline__ bool lu_solve4(cd A[4][4], cd B[4][NR]) {
       cd s = B[i][j];
 #pragma unroll
       for (int k = i + 1; k < 4; ++k) s -= A[i][k] * B[k][j];
-      B[i][j] = s / A[i][i];
+      B[i][j] = s * rp[i];
     }
   return true;
 }
