@@ -426,9 +426,13 @@ def run_ours(args):
 
 
 def run_uneven(args):
-    """The uneven-batch workload through ytf_transfer_batch + ytf_green_batch, one GPU."""
+    """The uneven-batch workload as one autotuned plan (BatchPlan: the whole step is one CUDA
+    graph: upload, persistent node-solve kernels, batched synthesis, download), one GPU. The
+    tuning (coordinate descent over the plan's tiles, persisted per (GPU, batch class)) runs
+    before the timed region; the per-item call path (ytf_transfer_batch + ytf_green_batch) is
+    timed beside it for one step."""
     import torch
-    from yellowthinfilms_b200 import api
+    from yellowthinfilms_b200 import api, autotune
     torch.cuda.set_device(0)
     ctx = api.Context(0)
     stream = torch.cuda.current_stream()
@@ -436,29 +440,41 @@ def run_uneven(args):
     tr, syn = uneven_batch()
     stacks = [api.Stack(t["stack"], ctx) for t in tr]
     items = [dict(t, stack=s) for t, s in zip(tr, stacks)]
-    prec = args.precision if args.precision != "int8x3" else "fp64"  # 4 x 4 pixels: the FP64 contraction
-
-    def step():
-        caches = api.build_cavity_transfer_batch(items, ctx=ctx)
-        out = api.closed_form_G_batch([dict(y, cache=c, precision=prec) for y, c in zip(syn, caches)])
-        del caches
-        return out
-
+    t0 = time.perf_counter()
+    plan, rec = autotune.tuned_plan(items, syn, ctx=ctx, force=args.retune, reps=1)
+    tune_s = time.perf_counter() - t0
+    info = plan.info()
     for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
+        plan.run()
+        plan.wait()
     ctx.profile(True)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dev = []
     with Clocks(0) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            G = step()
-        e1.record(stream)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            plan.run()
+            dev.append(plan.wait())
+        wall_ms = (time.perf_counter() - w0) * 1e3 / max(args.steps, 1)
     prof = ctx.profile_read()
+    ms = float(np.mean(dev)) if dev else 0.0
+    G = plan.results()
     entries = sum(g.size for g in G)
-    nodes = sum(len(t.get("kx_nodes", ())) or len(t["kr_nodes"]) * len(t["phi_nodes"]) for t in tr)
+    nodes = info["nodes"]
+    # the per-item call path, one step after one warm-up
+    prec = "fp64"
+
+    def calls_step():
+        caches = api.build_cavity_transfer_batch([dict(t, rotation=False) for t in items], ctx=ctx)
+        return api.closed_form_G_batch([dict(y, cache=c, precision=prec) for y, c in zip(syn, caches)])
+
+    calls_step()
+    torch.cuda.synchronize()
+    c0 = time.perf_counter()
+    Gc = calls_step()
+    torch.cuda.synchronize()
+    calls_ms = (time.perf_counter() - c0) * 1e3
+    err_calls = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)) for a, b in zip(G, Gc))
     err = None
     if not args.no_check:  # two items against the oracle on identical nodes
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -486,10 +502,17 @@ def run_uneven(args):
                                    "gyrotropic), node counts log-uniform in [1024, 32768] (1D kx or 2D kρ x 8 φ), "
                                    "4 z rows x 4x4 lateral offsets each", "stacks": len(tr), "nodes_per_step": nodes,
                        "entries_per_step": int(entries), "precision": prec,
-                       "calls": "ytf_transfer_batch + ytf_green_batch"},
-            "max_rel_err_vs_oracle": err, "clocks": clk.summary(),
+                       "calls": "ytf_plan_run + ytf_plan_wait: one CUDA graph per step (H2D of nodes and "
+                                "coordinates, persistent node-solve kernels, batched synthesis, D2H of G)",
+                       "tune": rec["tune"], "tune_class": autotune.config_class(items, syn),
+                       "tuning_s": round(tune_s, 2), "tune_measured": rec.get("measured"),
+                       "default_tune_ms": rec.get("default_ms"), "node_solve_passes": info["passes"]},
+            "max_rel_err_vs_oracle": err, "max_rel_diff_vs_per_item_calls": err_calls,
+            "e2e": {"value": entries / (wall_ms * 1e-3), "unit": "entries/s", "h2d_bytes_per_step": info["h2d_bytes"],
+                    "d2h_bytes_per_step": info["d2h_bytes"], "ms_per_step": wall_ms},
+            "per_item_calls_ms_per_step": calls_ms, "clocks": clk.summary(),
             "nodes_per_s": nodes / (ms * 1e-3),
-            "kernels_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in sorted(prof.items())},
+            "kernels_per_step": {k: v[1] // max(args.steps, 1) for k, v in sorted(prof.items())},
             "gpu_launches": int(sum(v[1] for v in prof.values()))}
     print(json.dumps(line), flush=True)
     return 0
@@ -738,6 +761,8 @@ def main():
                     help="gyro32: the 8-layer stack at 32 wavelengths (default); uneven: 1024 uneven stacks; "
                          "learned: learned adaptive quadrature vs the plain fixed rule; bessel: the 1D Bessel synthesis at "
                          "4096 radii x 65536 nodes x 256 heights; contour: the config-1 path on the deformed contour")
+    ap.add_argument("--retune", action="store_true",
+                    help="uneven workload: tune the plan again even if the tuning database has its class")
     ap.add_argument("--per-call", action="store_true",
                     help="one build + synthesis call per wavelength instead of the batched calls")
     ap.add_argument("--precision", default="int8x3", choices=list(DTYPE),

@@ -267,6 +267,50 @@ int ytf_green_noalloc(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, doubl
                       double* out_dev);
 
 /* ---------------------------------------------------------------------------------------
+ * Uneven-batch plans. No counterpart in the reference, whose callers loop over stacks,
+ * frequencies and grids, one build_cavity_transfer_1d/2d and one closed_form_G per item
+ * (mod_CavityTransfer.jl:224, :330; mod_ClosedFormField.jl:435, :711; e.g. chunked_2d,
+ * mod_ClosedFormGrid.jl:457-467). A plan takes nb (transfer, green) item pairs, allocates
+ * everything once and records the whole computation as one CUDA graph: the upload of every
+ * item's nodes and coordinates, the node solve as persistent kernels that pull tiles of
+ * (item, nodes) from a device counter (scratch reused pass by pass under 6 GiB), the
+ * synthesis of every item's G (FP64, node chunks of all items as the work units of one
+ * persistent kernel), and the download of the host outputs. ytf_plan_run stages the inputs
+ * and launches the graph; ytf_plan_wait synchronises and delivers the host outputs.
+ *
+ * Item i: tr[i] as for ytf_transfer_batch (rotation is ignored: 2D items take the full (kρ, φ)
+ * solve, which the rotation reproduces to rounding) and gr[i] as for ytf_green_batch, where
+ * gr[i].cache is ignored (item i synthesises from the cache of tr[i]) and precision must be
+ * YTF_PREC_FP64. Limits per item: nz <= 8; 2D: nx*ny <= 64; 1D: at most 32 distinct radii
+ * and 13*nz*(distinct radii) <= 2304; 1D nodes real (no deformed contour). The descriptors'
+ * host arrays are read again by every ytf_plan_run (their sizes, and for 1D items the
+ * pattern of equal radii, are fixed at creation) and gr[i].out receives G at ytf_plan_wait
+ * (or, with out_is_device, from the graph itself). Results: the caches equal
+ * ytf_transfer_batch's bit for bit; G equals ytf_green_batch's FP64 result to rounding (the
+ * node sums run in another order). */
+typedef struct ytf_plan ytf_plan;
+typedef struct {
+  int block;             /* threads per CTA of the persistent node-solve kernels: 128 or 256 */
+  int ctas_per_sm;       /* node-solve grid: ctas_per_sm x SM count (1..32) */
+  int tile;              /* units per node-solve tile (nodes; (node, layer) pairs for the mode solve) */
+  int chunk;             /* nodes per synthesis work unit (multiple of 16) */
+  int synth_ctas_per_sm; /* synthesis grid: synth_ctas_per_sm x SM count (1..8) */
+} ytf_tune;
+/* tune NULL: block 128, 4 CTAs per SM, tile 1024, chunk 2048, 2 synthesis CTAs per SM */
+int ytf_plan_create(ytf_ctx* ctx, int nb, const ytf_transfer_desc* tr, const ytf_green_desc* gr,
+                    const ytf_tune* tune, ytf_plan** out);
+/* re-record the graph with other tiles (the caches, scratch and staging are kept) */
+int ytf_plan_retune(ytf_plan* plan, const ytf_tune* tune);
+int ytf_plan_run(ytf_plan* plan);
+/* device_ms (optional): CUDA-event time of the last run's graph on the context's stream */
+int ytf_plan_wait(ytf_plan* plan, float* device_ms);
+/* the cache of item i (owned by the plan, valid until ytf_plan_destroy; do not destroy it) */
+int ytf_plan_cache(const ytf_plan* plan, int item, const ytf_cache** out);
+/* nodes of all items, node-solve passes, kernel launches per run, bytes staged in and out */
+int ytf_plan_info(const ytf_plan* plan, long* nodes, int* passes, int* kernels, long* h2d_bytes, long* d2h_bytes);
+int ytf_plan_destroy(ytf_plan* plan);
+
+/* ---------------------------------------------------------------------------------------
  * The small MLP of the learned node placement. No counterpart in the reference: the
  * reference places quadrature nodes from a pole scan of solved responses
  * (mod_KSpaceFeatures.jl:151-204); this network predicts the scanned quantity (the log

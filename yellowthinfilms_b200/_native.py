@@ -31,6 +31,12 @@ class GreenDesc(ctypes.Structure):
                 ("terms", ctypes.c_int), ("precision", ctypes.c_int), ("out", _vp), ("out_is_device", ctypes.c_int)]
 
 
+class Tune(ctypes.Structure):
+    """ytf_tune (include/ytf.h)."""
+    _fields_ = [("block", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("tile", ctypes.c_int), ("chunk", ctypes.c_int),
+                ("synth_ctas_per_sm", ctypes.c_int)]
+
+
 class GridParams(ctypes.Structure):
     """ytf_grid_params (include/ytf.h)."""
     _fields_ = [("h_min", ctypes.c_double), ("rho_max", ctypes.c_double), ("target_decay", ctypes.c_double),
@@ -92,6 +98,16 @@ SIGNATURES = {
     "ytf_bessel_j": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_long, _d, _d, _d, _d]),
     "ytf_transfer_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(TransferDesc), ctypes.POINTER(_vp)]),
     "ytf_green_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(GreenDesc)]),
+    "ytf_plan_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(TransferDesc), ctypes.POINTER(GreenDesc),
+                                       ctypes.POINTER(Tune), ctypes.POINTER(_vp)]),
+    "ytf_plan_retune": (ctypes.c_int, [_vp, ctypes.POINTER(Tune)]),
+    "ytf_plan_run": (ctypes.c_int, [_vp]),
+    "ytf_plan_wait": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "ytf_plan_cache": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "ytf_plan_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_long),
+                                     ctypes.POINTER(ctypes.c_long)]),
+    "ytf_plan_destroy": (ctypes.c_int, [_vp]),
     "ytf_gauss_legendre": (ctypes.c_int, [ctypes.c_int, _d, _d]),
     "ytf_gl_rule": (ctypes.c_int, [_vp, ctypes.c_int, _d, _d, ctypes.c_int, ctypes.c_int, _d, _d, _d]),
 }

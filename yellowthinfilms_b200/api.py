@@ -142,9 +142,10 @@ class _Cache:
         self.d_obs = {o: float(stack.layers[o - 1].d) for o in self.obs_layers}
 
     def __del__(self):
-        if getattr(self, "h", None) is not None and _native._lib is not None:
+        # a cache lent by a BatchPlan (_plan set) belongs to the plan
+        if getattr(self, "h", None) is not None and _native._lib is not None and getattr(self, "_plan", None) is None:
             _native._lib.ytf_cache_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def status(self):
         """(valid[n], Tvalid[n_obs, n], status bits[n]) as numpy arrays."""
@@ -557,6 +558,159 @@ def closed_form_G_batch(items, precision: str = "fp64"):
         else:
             res.append(o)
     return res
+
+
+class BatchPlan:
+    """An uneven batch prepared once and replayed as one CUDA graph (ytf_plan_*; no
+    counterpart in the reference, whose callers loop build_cavity_transfer_* and
+    closed_form_G per item). ``transfer_items`` as build_cavity_transfer_batch (``rotation``
+    is ignored: 2D items take the full (kρ, φ) solve); ``green_items`` as closed_form_G_batch
+    without ``cache`` (item i synthesises from the cache of transfer item i), FP64 only.
+    ``tune``: dict of ytf_tune fields (block, ctas_per_sm, tile, chunk, synth_ctas_per_sm)
+    or None for the defaults. Every ``run`` re-reads the node, weight and coordinate arrays
+    held by the plan (``inputs(i)`` returns them for in-place updates of the same sizes)."""
+
+    def __init__(self, transfer_items, green_items, tune=None, ctx: Optional[Context] = None):
+        from ._native import GreenDesc, TransferDesc
+        if len(transfer_items) != len(green_items):
+            raise YTFError("BatchPlan: transfer_items and green_items differ in length")
+        nb = len(transfer_items)
+        self._td = (TransferDesc * max(1, nb))()
+        self._gd = (GreenDesc * max(1, nb))()
+        self._keep, self._inputs, self._outs, self._meta = [], [], [], []
+        for i, (it, g) in enumerate(zip(transfer_items, green_items)):
+            st = _as_stack(it["stack"], ctx)
+            ctx = ctx or st.ctx
+            is2d = "kr_nodes" in it
+            if is2d:
+                k, w = _f64(it["kr_nodes"]), _f64(it["kr_weights"])
+                ph, wp = _f64(it["phi_nodes"]), _f64(it["phi_weights"])
+            else:
+                k, w = _f64(it["kx_nodes"]), _f64(it["wt_nodes"])
+                ph = wp = np.zeros(0)
+            if len(k) != len(w) or len(ph) != len(wp):
+                raise YTFError("BatchPlan: node/weight length mismatch (item %d)" % i)
+            no, ob = _obs_arg(it.get("obs_layers"))
+            d = self._td[i]
+            d.stack, d.omega, d.source_layer = st.h, float(it["omega"]), int(it["source_layer"])
+            d.nk, d.k_nodes, d.k_weights = len(k), ptr(k), ptr(w)
+            d.nphi, d.phi_nodes, d.phi_weights = len(ph), ptr(ph), ptr(wp)
+            d.nobs, d.obs_layers = no, ptr(ob, _i)
+            d.check_symmetry = int(bool(it.get("check_symmetry", True)))
+            d.rotation = 0
+            d.is2d = int(is2d)
+            if not isinstance(g, dict):
+                g = dict(zip(("obs_layer", "zsrc_local", "z_obs", "xs", "ys"), g))
+            terms = g.get("terms", "all")
+            if terms not in TERMS:
+                raise YTFError(f"closed_form_G: terms must be :all, :direct, :scattered, :toeplitz or :hankel (got :{terms})")
+            if g.get("precision", "fp64") != "fp64":
+                raise YTFError("BatchPlan: the plan's synthesis is FP64 (precision must be 'fp64')")
+            zo, x, y = _f64(g["z_obs"]), _f64(g["xs"]), _f64(g["ys"])
+            nx, ny, nz = len(x), len(y), len(zo)
+            out = g.get("out")
+            e = self._gd[i]
+            if out is not None:
+                if out.numel() != nx * ny * nz * 9:
+                    raise YTFError("closed_form_G: out has the wrong size")
+                e.out, e.out_is_device = out.data_ptr(), int(bool(getattr(out, "is_cuda", False)))
+                self._outs.append(out)
+            else:
+                G = np.zeros(2 * 9 * max(nz * nx * ny, 1))
+                e.out, e.out_is_device = G.ctypes.data, 0
+                self._outs.append((G, nx, ny, nz))
+            e.cache, e.obs_layer, e.zsrc_local = None, int(g["obs_layer"]), float(g["zsrc_local"])
+            e.nz, e.z_obs, e.nx, e.xs, e.ny, e.ys = nz, ptr(zo), nx, ptr(x), ny, ptr(y)
+            e.terms, e.precision = TERMS[terms], PRECISION["fp64"]
+            self._keep += [k, w, ph, wp, ob, zo, x, y]
+            self._inputs.append(dict(k=k, w=w, phi=ph, wphi=wp, z=zo, x=x, y=y))
+            self._meta.append((st, is2d, it))
+        self.ctx = ctx or default_context()
+        self.n_items = nb
+        self.h = None
+        h = ctypes.c_void_p()
+        tp = self._tune_struct(tune)
+        self.ctx.check(lib().ytf_plan_create(self.ctx.h, nb, self._td, self._gd, tp, ctypes.byref(h)))
+        self.h = h
+        self.tune = self._tune_dict(tune)
+
+    @staticmethod
+    def _tune_dict(tune):
+        t = dict(block=128, ctas_per_sm=4, tile=1024, chunk=2048, synth_ctas_per_sm=2)
+        t.update(tune or {})
+        return t
+
+    def _tune_struct(self, tune):
+        from ._native import Tune
+        if tune is None:
+            return None
+        t = self._tune_dict(tune)
+        self._tune_c = Tune(t["block"], t["ctas_per_sm"], t["tile"], t["chunk"], t["synth_ctas_per_sm"])
+        return ctypes.byref(self._tune_c)
+
+    def retune(self, tune):
+        """Re-record the graph with other tiles (caches, scratch and staging are kept)."""
+        self.ctx.check(lib().ytf_plan_retune(self.h, self._tune_struct(tune or {})))
+        self.tune = self._tune_dict(tune)
+
+    def inputs(self, i: int) -> dict:
+        """The arrays item i is read from at every run (k, w, phi, wphi, z, x, y)."""
+        return self._inputs[i]
+
+    def run(self):
+        """Stage the inputs and launch the graph on the context's stream (asynchronous)."""
+        self.ctx.check(lib().ytf_plan_run(self.h))
+
+    def wait(self) -> float:
+        """Synchronise, deliver the host outputs; returns the graph's device time in ms."""
+        ms = ctypes.c_float()
+        self.ctx.check(lib().ytf_plan_wait(self.h, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def __call__(self):
+        self.run()
+        self.wait()
+        return self.results()
+
+    def results(self):
+        """G of every item, as closed_form_G returns it (views of the plan's host buffers, or
+        the ``out`` tensors)."""
+        res = []
+        for o in self._outs:
+            if isinstance(o, tuple):
+                G, nx, ny, nz = o
+                res.append(G[:2 * 9 * nz * nx * ny].view(np.complex128).reshape(3, 3, nz, ny, nx).transpose(4, 3, 2, 1, 0))
+            else:
+                res.append(o)
+        return res
+
+    def cache(self, i: int):
+        """The cache of item i (owned by the plan)."""
+        h = ctypes.c_void_p()
+        self.ctx.check(lib().ytf_plan_cache(self.h, int(i), ctypes.byref(h)))
+        st, is2d, it = self._meta[i]
+        inp = self._inputs[i]
+        if is2d:
+            c = CavityTransferCache2D(h, st, it["omega"], it["source_layer"], inp["k"], inp["w"], inp["phi"], inp["wphi"])
+        else:
+            c = CavityTransferCache1D(h, st, it["omega"], it["source_layer"], inp["k"], inp["w"])
+        c._plan = self
+        return c
+
+    def info(self) -> dict:
+        n, p, k, hi, ho = ctypes.c_long(), ctypes.c_int(), ctypes.c_int(), ctypes.c_long(), ctypes.c_long()
+        self.ctx.check(lib().ytf_plan_info(self.h, ctypes.byref(n), ctypes.byref(p), ctypes.byref(k), ctypes.byref(hi),
+                                           ctypes.byref(ho)))
+        return dict(nodes=int(n.value), passes=int(p.value), kernels=int(k.value), h2d_bytes=int(hi.value),
+                    d2h_bytes=int(ho.value))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and _native._lib is not None:
+            _native._lib.ytf_plan_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def gausslegendre(n: int):

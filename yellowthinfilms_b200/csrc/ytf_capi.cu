@@ -1067,11 +1067,10 @@ int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* c, double* T, double* Qf, do
   return YTF_OK;
 }
 
-static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local, int nz, const double* z_obs,
-                      int nx, const double* xs, int ny, const double* ys, int terms, int precision, double* out,
-                      int out_is_device, const GreenBatch* gb) {
-  if (!ctx || !c || !out) return YTF_ERR_ARG;
-  if (c->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "closed_form_G: cache belongs to another context");
+// the synthesis parameters of closed_form_G(cache, obs_layer, zsrc_local, ...; terms) with
+// its argument checks (z rows left unset)
+static int synth_setup(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local, int terms, int nz,
+                       SynthParams& sp) {
   int oi = c->oidx(obs_layer);
   if (oi < 0)
     return fail(ctx, YTF_ERR_ARG, "amplitude_at: obs_layer=" + std::to_string(obs_layer) +
@@ -1082,19 +1081,11 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
   if ((terms == YTF_TERMS_TOEPLITZ || terms == YTF_TERMS_HANKEL || terms == YTF_TERMS_DIRECT) && !same)
     return fail(ctx, YTF_ERR_ARG, "closed_form_G: terms needs obs_layer == source_layer (" + std::to_string(c->src) +
                                       "), got " + std::to_string(obs_layer));
-  if (precision != YTF_PREC_FP64 && precision != YTF_PREC_SPLIT_BF16 && precision != YTF_PREC_INT8X3)
-    return fail(ctx, YTF_ERR_ARG, "closed_form_G: unknown precision mode");
   double zpos = c->src == 1 ? c->d_src - zsrc_local : zsrc_local;
   const double se = 1.4901161193847656e-08;
   if (!(-se <= zpos && zpos <= c->d_src + se))
     return fail(ctx, YTF_ERR_ARG, "amplitude_at: zsrc_local=" + std::to_string(zsrc_local) + " outside [0," +
                                       std::to_string(c->d_src) + "]");
-  if (nz < 0 || nx < 0 || ny < 0) return fail(ctx, YTF_ERR_ARG, "closed_form_G: negative grid size");
-  CK(cudaSetDevice(ctx->device));
-  long npix = (long)nx * ny;
-  long nout = npix * nz * 9;
-  if (nout == 0) return YTF_OK;
-  SynthParams sp;
   std::memset(&sp, 0, sizeof(sp));
   CacheView& v = sp.c;
   v.n = c->n; v.Nk = c->Nk; v.Np = c->Np; v.src = c->src; v.d_src = c->d_src;
@@ -1116,6 +1107,27 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
   sp.zpos = zpos;
   sp.d_obs = c->d_layer[obs_layer - 1];
   sp.nz = nz;
+  return YTF_OK;
+}
+
+static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local, int nz, const double* z_obs,
+                      int nx, const double* xs, int ny, const double* ys, int terms, int precision, double* out,
+                      int out_is_device, const GreenBatch* gb) {
+  if (!ctx || !c || !out) return YTF_ERR_ARG;
+  if (c->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "closed_form_G: cache belongs to another context");
+  SynthParams sp;
+  {
+    int rc0 = synth_setup(ctx, c, obs_layer, zsrc_local, terms, nz, sp);
+    if (rc0) return rc0;
+  }
+  if (precision != YTF_PREC_FP64 && precision != YTF_PREC_SPLIT_BF16 && precision != YTF_PREC_INT8X3)
+    return fail(ctx, YTF_ERR_ARG, "closed_form_G: unknown precision mode");
+  if (nz < 0 || nx < 0 || ny < 0) return fail(ctx, YTF_ERR_ARG, "closed_form_G: negative grid size");
+  CK(cudaSetDevice(ctx->device));
+  long npix = (long)nx * ny;
+  long nout = npix * nz * 9;
+  if (nout == 0) return YTF_OK;
+  CacheView& v = sp.c;
   const double *dzo, *dxs, *dys;
   int rc;
   if (gb) {
@@ -1465,6 +1477,564 @@ int ytf_gl_rule(ytf_ctx* ctx, int npanels, const double* pa, const double* pb, i
 }
 
 }  // extern "C"
+
+// =====================================================================================
+// Uneven-batch plans (no counterpart in the reference; the contract is in ytf.h). Creation
+// validates every item, creates the caches, lays out one staging block of inputs (nodes,
+// weights, coordinates, 1D radii) and one of host outputs, and groups the node solves into
+// passes that share one scratch arena; ytf_plan_retune builds the tile tables and records
+// the graph: H2D of the inputs, counter reset, per pass the persistent stage kernels
+// (modes, QR pass, forward-only match/seeds/iface/scan or the general chain), the batched
+// synthesis and its chunk sums, D2H of the host outputs.
+// =====================================================================================
+struct ytf_plan {
+  ytf_ctx* ctx = nullptr;
+  int nb = 0;
+  std::vector<ytf_transfer_desc> tr;
+  std::vector<ytf_green_desc> gr;
+  std::vector<ytf_cache*> cs;
+  std::vector<TransferParams> ps;      // per item, scratch pointers into the arena
+  std::vector<std::vector<int>> passes;
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  std::vector<size_t> in_node, in_coord;  // per item offsets into the input staging (doubles)
+  size_t in_count = 0;
+  double* h_in = nullptr;
+  double* d_in = nullptr;
+  std::vector<std::vector<int>> rmap;  // 1D items: pixel -> distinct radius (first occurrence)
+  std::vector<int> nr;
+  std::vector<size_t> rmap_off;
+  int* d_rmap = nullptr;
+  std::vector<long> g_off;             // host-output items: offset into h_G / d_G (complex); else -1
+  size_t g_count = 0;
+  double2* h_G = nullptr;
+  double2* d_G = nullptr;
+  std::vector<SynthParams> sps;
+  std::vector<long> nout_syn;          // per item: partial outputs per chunk (0: no synthesis)
+  ytf_tune tune{};
+  char* tb = nullptr;
+  size_t tb_bytes = 0;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  bool pending = false;
+  std::map<std::string, long> kcount;  // kernels per run, by name
+  long nodes = 0;
+  int nsm = 148;
+};
+
+namespace {
+
+void plan_release_graph(ytf_plan* P) {
+  if (P->exec) cudaGraphExecDestroy(P->exec);
+  if (P->graph) cudaGraphDestroy(P->graph);
+  if (P->tb) cudaFree(P->tb);
+  P->exec = nullptr;
+  P->graph = nullptr;
+  P->tb = nullptr;
+  P->tb_bytes = 0;
+  P->kcount.clear();
+}
+
+void plan_free(ytf_plan* P) {
+  if (!P) return;
+  cudaSetDevice(P->ctx->device);
+  cudaStreamSynchronize(P->ctx->stream);
+  if (P->cap) cudaStreamSynchronize(P->cap);
+  plan_release_graph(P);
+  if (P->cap) cudaStreamDestroy(P->cap);
+  if (P->e0) cudaEventDestroy(P->e0);
+  if (P->e1) cudaEventDestroy(P->e1);
+  if (P->arena) cudaFree(P->arena);
+  if (P->d_in) cudaFree(P->d_in);
+  if (P->d_rmap) cudaFree(P->d_rmap);
+  if (P->d_G) cudaFree(P->d_G);
+  if (P->h_in) cudaFreeHost(P->h_in);
+  if (P->h_G) cudaFreeHost(P->h_G);
+  for (auto c : P->cs)
+    if (c) ytf_cache_destroy(c);
+  delete P;
+}
+
+// distinct radii of a pixel set in first-occurrence order over (i fastest, j), as the 1D
+// synthesis of closed_form_G
+void radius_map(int nx, int ny, const double* xs, const double* ys, std::vector<double>& ur, std::vector<int>& rm) {
+  ur.clear();
+  rm.assign((size_t)nx * ny, 0);
+  std::unordered_map<double, int> idx;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const double r = std::hypot(xs[i], ys[j]);
+      auto it = idx.find(r);
+      if (it == idx.end()) {
+        idx.emplace(r, (int)ur.size());
+        rm[i + (size_t)nx * j] = (int)ur.size();
+        ur.push_back(r);
+      } else {
+        rm[i + (size_t)nx * j] = it->second;
+      }
+    }
+}
+
+int plan_fail(ytf_ctx* ctx, int rc, int item) {
+  ctx->err += " (plan item " + std::to_string(item) + ")";
+  return rc;
+}
+
+// validation, caches, staging, outputs and passes (everything the tiles do not change)
+int plan_build(ytf_plan* P) {
+  ytf_ctx* ctx = P->ctx;
+  const int nb = P->nb;
+  P->cs.assign(nb, nullptr);
+  P->ps.resize(nb);
+  P->sps.resize(nb);
+  P->rmap.resize(nb);
+  P->nr.assign(nb, 0);
+  P->rmap_off.assign(nb, 0);
+  P->g_off.assign(nb, -1);
+  P->nout_syn.assign(nb, 0);
+  P->in_node.assign(nb, 0);
+  P->in_coord.assign(nb, 0);
+  size_t rmap_count = 0;
+  for (int i = 0; i < nb; ++i) {
+    const ytf_transfer_desc& d = P->tr[i];
+    const ytf_green_desc& g = P->gr[i];
+    const bool is2d = d.nphi > 0 || d.is2d;
+    bool rot = false;
+    int rc = prepare_cache(ctx, d.stack, is2d, d.omega, d.source_layer, d.nk, d.k_nodes, d.k_weights, d.nphi,
+                           d.phi_nodes, d.phi_weights, d.nobs, d.obs_layers, d.check_symmetry, YTF_ROT_OFF, false,
+                           &P->cs[i], &rot);
+    if (rc) return plan_fail(ctx, rc, i);
+    ytf_cache* c = P->cs[i];
+    P->nodes += c->n;
+    if (g.nz < 0 || g.nx < 0 || g.ny < 0) return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "closed_form_G: negative grid size"), i);
+    if (g.precision != YTF_PREC_FP64)
+      return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: the plan's synthesis is FP64 (precision must be YTF_PREC_FP64)"), i);
+    if (g.nz > SYN_MAXZ)
+      return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: at most " + std::to_string(SYN_MAXZ) + " z rows per item"), i);
+    if ((g.nz && !g.z_obs) || (g.nx && !g.xs) || (g.ny && !g.ys) || !g.out)
+      return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: NULL coordinate or output array"), i);
+    if ((rc = synth_setup(ctx, c, g.obs_layer, g.zsrc_local, g.terms, g.nz, P->sps[i]))) return plan_fail(ctx, rc, i);
+    const long npix = (long)g.nx * g.ny;
+    if (is2d) {
+      if (npix > SYN_MAXPIX || npix * 9 * g.nz > SYN_MAXOUT)
+        return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: 2D items need nx*ny <= " + std::to_string(SYN_MAXPIX) +
+                                                         " and 9*nz*nx*ny <= " + std::to_string(SYN_MAXOUT)), i);
+      P->nout_syn[i] = npix * 9 * g.nz;
+    } else {
+      std::vector<double> ur;
+      radius_map(g.nx, g.ny, g.xs, g.ys, ur, P->rmap[i]);
+      P->nr[i] = (int)ur.size();
+      if (P->nr[i] > SYN_MAXR || (long)P->nr[i] * 13 * g.nz > SYN_MAXOUT)
+        return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: 1D items need at most " + std::to_string(SYN_MAXR) +
+                                                         " distinct radii and 13*nz*radii <= " + std::to_string(SYN_MAXOUT)), i);
+      P->nout_syn[i] = (long)P->nr[i] * 13 * g.nz;
+      P->rmap_off[i] = rmap_count;
+      rmap_count += (size_t)npix;
+    }
+    if (npix * g.nz == 0) P->nout_syn[i] = 0;
+    // input staging: nodes, weights, φ nodes and weights, then z rows, x, y, 1D radii
+    P->in_node[i] = P->in_count;
+    P->in_count += 2 * c->kr.size() + 2 * c->phi.size();
+    P->in_coord[i] = P->in_count;
+    P->in_count += (size_t)g.nz + g.nx + g.ny + P->nr[i];
+    if (!g.out_is_device && npix * g.nz > 0) {
+      P->g_off[i] = (long)P->g_count;
+      P->g_count += (size_t)npix * g.nz * 9;
+    }
+  }
+  CK(cudaHostAlloc(&P->h_in, 8 * std::max<size_t>(P->in_count, 1), cudaHostAllocDefault));
+  CK(cudaMalloc(&P->d_in, 8 * std::max<size_t>(P->in_count, 1)));
+  if (P->g_count) {
+    CK(cudaHostAlloc(&P->h_G, 16 * P->g_count, cudaHostAllocDefault));
+    CK(cudaMalloc(&P->d_G, 16 * P->g_count));
+  }
+  if (rmap_count) {
+    std::vector<int> all(rmap_count);
+    for (int i = 0; i < nb; ++i)
+      if (!P->rmap[i].empty()) std::copy(P->rmap[i].begin(), P->rmap[i].end(), all.begin() + P->rmap_off[i]);
+    CK(cudaMalloc(&P->d_rmap, 4 * rmap_count));
+    CK(cudaMemcpy(P->d_rmap, all.data(), 4 * rmap_count, cudaMemcpyHostToDevice));
+  }
+  // the caches read their nodes from the device copy of the staging; the synthesis its rows
+  for (int i = 0; i < nb; ++i) {
+    ytf_cache* c = P->cs[i];
+    double* b = P->d_in + P->in_node[i];
+    const size_t nk = c->kr.size(), np = c->phi.size();
+    c->d_kr = b;
+    c->d_wr = b + nk;
+    if (np) {
+      c->d_phi = b + 2 * nk;
+      c->d_wphi = b + 2 * nk + np;
+    }
+    const int oi = c->oidx(P->gr[i].obs_layer);
+    SynthParams& sp = P->sps[i];
+    sp.c.kr = c->d_kr; sp.c.wr = c->d_wr; sp.c.phi = c->d_phi; sp.c.wphi = c->d_wphi;
+    (void)oi;
+    sp.zo = P->d_in + P->in_coord[i];
+  }
+  // node-solve passes under the scratch budget, items in order
+  const size_t budget = (size_t)6 << 30;
+  std::vector<size_t> need(nb, 0);
+  for (int i = 0; i < nb; ++i) {
+    ytf_cache* c = P->cs[i];
+    TransferParams& q = P->ps[i];
+    fill_params(q, P->tr[i].stack, c);
+    q.mode = c->is2d ? 1 : 0;
+    q.n = c->n;
+    q.off = 0;
+    q.nout = c->n;
+    if (c->n == 0) continue;
+    const int N = q.nL;
+    const long n = q.n;
+    auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
+    size_t b = r256((size_t)N * 20 * 16 * n) + r256((size_t)N * n) + r256((size_t)std::max(N - 1, 1) * 16 * 16 * n);
+    if (only_source_observed(q)) b += r256((size_t)8 * n);
+    else b += (q.needL ? r256((size_t)N * 16 * 16 * n) : 0) + (q.needR ? r256((size_t)N * 16 * 16 * n) : 0);
+    need[i] = b;
+  }
+  {
+    std::vector<int> cur;
+    size_t used = 0;
+    for (int i = 0; i < nb; ++i) {
+      if (!need[i]) continue;
+      if (!cur.empty() && used + need[i] > budget) {
+        P->passes.push_back(cur);
+        P->arena_bytes = std::max(P->arena_bytes, used);
+        cur.clear();
+        used = 0;
+      }
+      cur.push_back(i);
+      used += need[i];
+    }
+    if (!cur.empty()) {
+      P->passes.push_back(cur);
+      P->arena_bytes = std::max(P->arena_bytes, used);
+    }
+  }
+  if (P->arena_bytes) CK(cudaMalloc(&P->arena, P->arena_bytes));
+  for (auto& pass : P->passes) {
+    size_t o = 0;
+    auto carve = [&](size_t bytes) {
+      char* q = P->arena + o;
+      o += (bytes + 255) & ~size_t(255);
+      return q;
+    };
+    for (int i : pass) {
+      TransferParams& q = P->ps[i];
+      const int N = q.nL;
+      const long n = q.n;
+      q.modes = (double2*)carve((size_t)N * 20 * 16 * n);
+      q.lstat = (uint8_t*)carve((size_t)N * n);
+      q.sint = (double2*)carve((size_t)std::max(N - 1, 1) * 16 * 16 * n);
+      if (only_source_observed(q)) {
+        q.swaps = (uint64_t*)carve((size_t)8 * n);
+      } else {
+        q.sleft = q.needL ? (double2*)carve((size_t)N * 16 * 16 * n) : nullptr;
+        q.sright = q.needR ? (double2*)carve((size_t)N * 16 * 16 * n) : nullptr;
+      }
+    }
+  }
+  CK(cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&P->e0));
+  CK(cudaEventCreate(&P->e1));
+  CK(synth_small_init());
+  CK(cudaStreamSynchronize(ctx->stream));  // cache blocks cleared before the first run
+  return YTF_OK;
+}
+
+}  // namespace
+
+extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
+  if (!P) return YTF_ERR_ARG;
+  ytf_ctx* ctx = P->ctx;
+  ytf_tune t{128, 4, 1024, 2048, 2};
+  if (tune_in) t = *tune_in;
+  if (!(t.block == 128 || t.block == 256) || t.ctas_per_sm < 1 || t.ctas_per_sm > 32 || t.tile < 1 || t.chunk < 16 ||
+      t.chunk % 16 != 0 || t.synth_ctas_per_sm < 1 || t.synth_ctas_per_sm > 8)
+    return fail(ctx, YTF_ERR_ARG, "ytf_plan_retune: block 128|256, ctas_per_sm 1..32, tile >= 1, chunk a positive "
+                                  "multiple of 16, synth_ctas_per_sm 1..8");
+  CK(cudaSetDevice(ctx->device));
+  if (P->pending) {
+    CK(cudaEventSynchronize(P->e1));
+    P->pending = false;
+  }
+  plan_release_graph(P);
+  P->tune = t;
+  const int nb = P->nb;
+  // host image of the tile-dependent block: per pass the parameter array and its tile
+  // tables per stage, the synthesis items with their offsets, then the counters and partials
+  struct Launch {
+    int stage;
+    size_t params;  // byte offset of the pass's TransferParams array
+    size_t prob, start, end;
+    int ntiles;
+    int counter;
+  };
+  std::vector<char> hb;
+  auto put = [&](const void* src, size_t bytes) {  // src NULL: zero bytes
+    size_t o = (hb.size() + 255) & ~size_t(255);
+    hb.resize(o + bytes, 0);
+    if (bytes && src) std::memcpy(hb.data() + o, src, bytes);
+    return o;
+  };
+  std::vector<Launch> launches;
+  int ncounter = 0;
+  for (auto& pass : P->passes) {
+    std::vector<TransferParams> pp;
+    for (int i : pass) pp.push_back(P->ps[i]);
+    const size_t po = put(pp.data(), sizeof(TransferParams) * pp.size());
+    const int stages[] = {0, 1, 4, 5, 6, 7, 3};
+    for (int st : stages) {
+      std::vector<int> prob;
+      std::vector<long> a, b;
+      for (int j = 0; j < (int)pass.size(); ++j) {
+        const TransferParams& q = pp[j];
+        const bool fast = only_source_observed(q);
+        long units;
+        if (st == 0 || st == 1) units = (long)q.nL * q.n;
+        else if (st == 3) units = fast ? 0 : q.n;
+        else if (st == 6) units = fast ? (long)(q.nL - 1) * q.n : 0;
+        else units = fast ? q.n : 0;
+        for (long u = 0; u < units; u += t.tile) {
+          prob.push_back(j);
+          a.push_back(u);
+          b.push_back(std::min(units, u + (long)t.tile));
+        }
+      }
+      if (prob.empty()) continue;
+      Launch L;
+      L.stage = st;
+      L.params = po;
+      L.prob = put(prob.data(), 4 * prob.size());
+      L.start = put(a.data(), 8 * a.size());
+      L.end = put(b.data(), 8 * b.size());
+      L.ntiles = (int)prob.size();
+      L.counter = ncounter++;
+      launches.push_back(L);
+    }
+  }
+  // synthesis items (those with outputs), chunk and finish offsets
+  std::vector<SynthItem> items;
+  std::vector<long> woff{0}, foff{0};
+  std::vector<int> item_of;
+  size_t npart = 0;
+  for (int i = 0; i < nb; ++i) {
+    const ytf_green_desc& g = P->gr[i];
+    const long npix = (long)g.nx * g.ny;
+    if (npix * g.nz == 0) continue;
+    SynthItem it;
+    std::memset(&it, 0, sizeof(it));
+    it.sp = P->sps[i];
+    const double* co = P->d_in + P->in_coord[i];
+    it.xs = co + g.nz;
+    it.ys = co + g.nz + g.nx;
+    it.nx = g.nx;
+    it.ny = g.ny;
+    it.is2d = P->cs[i]->is2d ? 1 : 0;
+    it.rho = co + g.nz + g.nx + g.ny;
+    it.rmap = it.is2d ? nullptr : P->d_rmap + P->rmap_off[i];
+    it.nr = P->nr[i];
+    const long n = P->cs[i]->n;
+    it.nw = (int)((n + t.chunk - 1) / t.chunk);
+    it.G = P->g_off[i] >= 0 ? P->d_G + P->g_off[i] : (double2*)g.out;
+    items.push_back(it);
+    item_of.push_back(i);
+    npart += (size_t)it.nw * P->nout_syn[i];
+    woff.push_back(woff.back() + it.nw);
+    foff.push_back(foff.back() + (it.is2d ? npix * 9 * g.nz : npix * g.nz));
+  }
+  const int synth_counter = ncounter++;
+  size_t o_items = 0, o_woff = 0, o_foff = 0;
+  if (!items.empty()) {
+    o_items = put(items.data(), sizeof(SynthItem) * items.size());
+    o_woff = put(woff.data(), 8 * woff.size());
+    o_foff = put(foff.data(), 8 * foff.size());
+  }
+  const size_t o_ctr = put(nullptr, 4 * (size_t)ncounter);
+  const size_t o_part = (hb.size() + 255) & ~size_t(255);  // partial sums: device only
+  P->tb_bytes = o_part + 16 * std::max<size_t>(npart, 1);
+  CK(cudaMalloc(&P->tb, P->tb_bytes));
+  // partial-sum pointers of the synthesis items, now that the block's address is known
+  {
+    size_t po = 0;
+    for (size_t k = 0; k < items.size(); ++k) {
+      SynthItem* it = reinterpret_cast<SynthItem*>(hb.data() + o_items) + k;
+      it->partial = reinterpret_cast<double2*>(P->tb + o_part) + po;
+      po += (size_t)it->nw * P->nout_syn[item_of[k]];
+    }
+  }
+  CK(cudaMemcpy(P->tb, hb.data(), hb.size(), cudaMemcpyHostToDevice));
+  // record the graph
+  unsigned* ctr = reinterpret_cast<unsigned*>(P->tb + o_ctr);
+  const int nsm = P->nsm;
+  cudaStream_t s = P->cap;
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  auto step = [&](cudaError_t r) {
+    if (e == cudaSuccess && r != cudaSuccess) e = r;
+  };
+  if (P->in_count) step(cudaMemcpyAsync(P->d_in, P->h_in, 8 * P->in_count, cudaMemcpyHostToDevice, s));
+  step(cudaMemsetAsync(ctr, 0, 4 * (size_t)ncounter, s));
+  static const char* names[] = {"k_persist_modes", "k_persist_qr", "", "k_persist_chain", "k_persist_match",
+                                "k_persist_seeds", "k_persist_iface", "k_persist_scan"};
+  for (auto& L : launches) {
+    TileQueue q;
+    q.prob = reinterpret_cast<const int*>(P->tb + L.prob);
+    q.start = reinterpret_cast<const long*>(P->tb + L.start);
+    q.end = reinterpret_cast<const long*>(P->tb + L.end);
+    q.ntiles = L.ntiles;
+    q.counter = ctr + L.counter;
+    const int grid = std::min(L.ntiles, t.ctas_per_sm * nsm);
+    step(launch_persist(L.stage, t.block, grid, reinterpret_cast<const TransferParams*>(P->tb + L.params), q, s));
+    P->kcount[names[L.stage]] += 1;
+  }
+  if (!items.empty()) {
+    const SynthItem* di = reinterpret_cast<const SynthItem*>(P->tb + o_items);
+    const long* dw = reinterpret_cast<const long*>(P->tb + o_woff);
+    const long* df = reinterpret_cast<const long*>(P->tb + o_foff);
+    if (woff.back() > 0) {
+      const int grid = (int)std::min<long>(woff.back(), (long)t.synth_ctas_per_sm * nsm);
+      step(launch_synth_small(di, (int)items.size(), dw, woff.back(), ctr + synth_counter, t.chunk, grid, s));
+      P->kcount["k_synth_small"] += 1;
+    }
+    step(launch_synth_finish(di, (int)items.size(), df, foff.back(), s));
+    P->kcount["k_synth_finish"] += 1;
+  }
+  if (P->g_count) step(cudaMemcpyAsync(P->h_G, P->d_G, 16 * P->g_count, cudaMemcpyDeviceToHost, s));
+  cudaError_t ee = cudaStreamEndCapture(s, &P->graph);
+  if (e == cudaSuccess) e = ee;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&P->exec, P->graph, 0);
+  if (e != cudaSuccess) {
+    plan_release_graph(P);
+    return fail(ctx, YTF_ERR_CUDA, std::string("ytf_plan_retune: graph capture: ") + cudaGetErrorString(e));
+  }
+  return YTF_OK;
+}
+
+extern "C" int ytf_plan_create(ytf_ctx* ctx, int nb, const ytf_transfer_desc* tr, const ytf_green_desc* gr,
+                               const ytf_tune* tune, ytf_plan** out) {
+  if (!ctx || !out || nb < 0 || (nb > 0 && (!tr || !gr))) return YTF_ERR_ARG;
+  *out = nullptr;
+  CK(cudaSetDevice(ctx->device));
+  ytf_plan* P = new ytf_plan();
+  P->ctx = ctx;
+  P->nb = nb;
+  P->tr.assign(tr, tr + nb);
+  P->gr.assign(gr, gr + nb);
+  cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+  int rc = plan_build(P);
+  if (!rc) rc = ytf_plan_retune(P, tune);
+  if (rc) {
+    std::string m = ctx->err;
+    plan_free(P);
+    ctx->err = m;
+    return rc;
+  }
+  *out = P;
+  return YTF_OK;
+}
+
+extern "C" int ytf_plan_run(ytf_plan* P) {
+  if (!P || !P->exec) return YTF_ERR_ARG;
+  ytf_ctx* ctx = P->ctx;
+  CK(cudaSetDevice(ctx->device));
+  if (P->pending) {  // the staging is read by the previous run's copy
+    CK(cudaEventSynchronize(P->e1));
+    P->pending = false;
+  }
+  for (int i = 0; i < P->nb; ++i) {
+    const ytf_transfer_desc& d = P->tr[i];
+    const ytf_green_desc& g = P->gr[i];
+    const ytf_cache* c = P->cs[i];
+    double* h = P->h_in + P->in_node[i];
+    const size_t nk = c->kr.size(), np = c->phi.size();
+    if (nk) {
+      std::memcpy(h, d.k_nodes, 8 * nk);
+      std::memcpy(h + nk, d.k_weights, 8 * nk);
+    }
+    if (np) {
+      std::memcpy(h + 2 * nk, d.phi_nodes, 8 * np);
+      std::memcpy(h + 2 * nk + np, d.phi_weights, 8 * np);
+    }
+    double* hc = P->h_in + P->in_coord[i];
+    if (g.nz) std::memcpy(hc, g.z_obs, 8 * (size_t)g.nz);
+    if (g.nx) std::memcpy(hc + g.nz, g.xs, 8 * (size_t)g.nx);
+    if (g.ny) std::memcpy(hc + g.nz + g.nx, g.ys, 8 * (size_t)g.ny);
+    if (!c->is2d && P->nr[i]) {
+      std::vector<double> ur;
+      std::vector<int> rm;
+      radius_map(g.nx, g.ny, g.xs, g.ys, ur, rm);
+      if (rm != P->rmap[i]) return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_run: the pattern of equal radii changed"), i);
+      std::memcpy(hc + g.nz + g.nx + g.ny, ur.data(), 8 * ur.size());
+    }
+  }
+  CK(cudaEventRecord(P->e0, ctx->stream));
+  if (ctx->prof) {
+    ProfSpan sp{"ytf_plan_graph", take_event(ctx), take_event(ctx)};
+    CK(cudaEventRecord(sp.a, ctx->stream));
+    CK(cudaGraphLaunch(P->exec, ctx->stream));
+    CK(cudaEventRecord(sp.b, ctx->stream));
+    ctx->spans.push_back(sp);
+  } else {
+    CK(cudaGraphLaunch(P->exec, ctx->stream));
+  }
+  CK(cudaEventRecord(P->e1, ctx->stream));
+  for (auto& kv : P->kcount) ctx->klaunch[kv.first] += kv.second;
+  P->pending = true;
+  return YTF_OK;
+}
+
+extern "C" int ytf_plan_wait(ytf_plan* P, float* device_ms) {
+  if (!P) return YTF_ERR_ARG;
+  ytf_ctx* ctx = P->ctx;
+  CK(cudaSetDevice(ctx->device));
+  if (!P->pending) {
+    if (device_ms) *device_ms = 0.f;
+    return YTF_OK;
+  }
+  CK(cudaEventSynchronize(P->e1));
+  P->pending = false;
+  for (int i = 0; i < P->nb; ++i)
+    if (P->g_off[i] >= 0) {
+      const ytf_green_desc& g = P->gr[i];
+      std::memcpy(g.out, P->h_G + P->g_off[i], 16 * (size_t)g.nx * g.ny * g.nz * 9);
+    }
+  if (device_ms) CK(cudaEventElapsedTime(device_ms, P->e0, P->e1));
+  if (ctx->prof) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    prof_collect(ctx);
+  }
+  return YTF_OK;
+}
+
+extern "C" int ytf_plan_cache(const ytf_plan* P, int item, const ytf_cache** out) {
+  if (!P || !out || item < 0 || item >= P->nb) return YTF_ERR_ARG;
+  *out = P->cs[item];
+  return YTF_OK;
+}
+
+extern "C" int ytf_plan_info(const ytf_plan* P, long* nodes, int* passes, int* kernels, long* h2d_bytes,
+                             long* d2h_bytes) {
+  if (!P) return YTF_ERR_ARG;
+  if (nodes) *nodes = P->nodes;
+  if (passes) *passes = (int)P->passes.size();
+  if (kernels) {
+    long k = 0;
+    for (auto& kv : P->kcount) k += kv.second;
+    *kernels = (int)k;
+  }
+  if (h2d_bytes) *h2d_bytes = 8 * (long)P->in_count;
+  if (d2h_bytes) *d2h_bytes = 16 * (long)P->g_count;
+  return YTF_OK;
+}
+
+extern "C" int ytf_plan_destroy(ytf_plan* P) {
+  if (!P) return YTF_OK;
+  plan_free(P);
+  return YTF_OK;
+}
 
 // =====================================================================================
 // Allocation-free 2D synthesis (ytf_green_noalloc)

@@ -76,6 +76,19 @@ cudaError_t launch_transfer_batch(int kernel, const TransferParams* probs, const
 cudaError_t launch_rotate_fill(const TransferParams& p, const uint8_t* base_status, const uint8_t* base_tvalid,
                                const double2* Tbase, cudaStream_t stream);
 
+// persistent transfer kernels: tiles of units of one problem each, pulled from a counter
+struct TileQueue {
+  const int* prob;    // [ntiles] problem index into the parameter array
+  const long* start;  // [ntiles] first unit of the tile
+  const long* end;    // [ntiles] one past its last unit
+  int ntiles;
+  unsigned* counter;  // next tile; zero before the launch
+};
+// stage: 0 modes, 1 QR pass, 3 general chain, 4 match, 5 seeds, 6 iface, 7 scan (units as the
+// batched kernels); block 128 or 256 threads; grid CTAs (persistent)
+cudaError_t launch_persist(int stage, int block, int grid, const TransferParams* probs, const TileQueue& q,
+                           cudaStream_t s);
+
 // read-only view of a device transfer cache for the synthesis kernels
 struct CacheView {
   long n;
@@ -132,6 +145,33 @@ int lateral_splits(long n, int splits);  // effective split count of launch_late
 cudaError_t launch_lateral(const CacheView& c, int nx, int ny, const double* xs, const double* ys, int ncol, const double2* S,
                            double2* partial, int splits, cudaStream_t s);
 cudaError_t launch_reduce_splits2(long len, int splits, const double2* partial, double2* G, cudaStream_t s);
+
+// batched synthesis of small observation sets (uneven batches): per item the partial sums
+// of each node chunk, then a per-output sum over the chunks (2D) or sum and pixel assembly (1D)
+constexpr int SYN_MAXOUT = 2304;  // partial outputs per item: 2D nx ny 9 nz, 1D nr 13 nz
+constexpr int SYN_MAXPIX = 64;    // 2D pixels per item
+constexpr int SYN_MAXR = 32;      // 1D distinct radii per item
+constexpr int SYN_MAXZ = 8;       // z rows per item
+struct SynthItem {
+  SynthParams sp;          // cache view, term masks, source position, z rows (device)
+  const double* xs;        // [nx] device
+  const double* ys;        // [ny] device
+  int nx, ny;
+  int is2d;
+  const double* rho;       // 1D: [nr] distinct radii (device)
+  const int* rmap;         // 1D: [nx ny] pixel -> radius (device)
+  int nr;
+  int nw;                  // node chunks of this item
+  double2* partial;        // [nw][outputs]
+  double2* G;              // [nx ny nz 9] Julia layout (device)
+};
+size_t synth_small_smem();
+cudaError_t synth_small_init();  // shared-memory attribute of k_synth_small (before any capture)
+// w_off[nitems + 1]: prefix of the items' chunk counts; counter zeroed before the launch
+cudaError_t launch_synth_small(const SynthItem* items, int nitems, const long* w_off, long nwork, unsigned* counter,
+                               int chunk, int grid, cudaStream_t s);
+// f_off[nitems + 1]: prefix of the items' finish units (2D: nx ny 9 nz, 1D: nx ny nz)
+cudaError_t launch_synth_finish(const SynthItem* items, int nitems, const long* f_off, long nfin, cudaStream_t s);
 
 // 2D lateral synthesis on the tensor cores (split-BF16, FP32 accumulation)
 struct LateralTC {

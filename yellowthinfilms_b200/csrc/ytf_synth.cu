@@ -95,19 +95,16 @@ __device__ __forceinline__ void direct_amp(const SynthParams& p, long k, double 
 // 1D coefficients. Columns per z-row: order 0: xx yx xy yy zz; order 1: zx zy xz yz;
 // order 2: xx yx xy yy (c q). Output rows are real: row 2*(zi*ncol + col) + part, node fastest.
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_coef1d(SynthParams p, double* C0, double* C1, double* C2) {
-  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  int zi = blockIdx.y;
+// the 13 coefficient columns of one (node, z row) (_integrate_pixel_1d's integrand,
+// mod_ClosedFormField.jl:435-487): order 0: xx yx xy yy zz; order 1: zx zy xz yz; order 2:
+// xx yx xy yy
+__device__ __forceinline__ void coef1d_row(const SynthParams& p, long k, double z, const cd Af[2][3], const cd Ab[2][3],
+                                           cd c0[5], cd c1[4], cd c2[4]) {
   const CacheView& c = p.c;
-  if (k >= c.n) return;
   const long n = c.n;
-  cd Af[2][3], Ab[2][3];
-  reflected_amp(p, k, Af, Ab);
-  const double z = p.zo[zi];
   // i w / (2π) with a complex weight and node on a deformed contour (kri, wri), real otherwise
   const cd W = cd{0.0, 1.0 / (2.0 * 3.14159265358979323846)} * cd{c.wr[k], c.wri ? c.wri[k] : 0.0};
   const cd kx{c.kr[k], c.kri ? c.kri[k] : 0.0};
-  cd c0[5], c1[4], c2[4];
   for (int i = 0; i < 5; ++i) c0[i] = cd{0, 0};
   for (int i = 0; i < 4; ++i) { c1[i] = cd{0, 0}; c2[i] = cd{0, 0}; }
   cd Afd[2][3], Abd[2][3];
@@ -154,6 +151,18 @@ __global__ void __launch_bounds__(128) k_coef1d(SynthParams p, double* C0, doubl
       c0[4] += cd{0.0, -1.0} * (az * ez);        // zz
     }
   }
+}
+
+__global__ void __launch_bounds__(128) k_coef1d(SynthParams p, double* C0, double* C1, double* C2) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int zi = blockIdx.y;
+  const CacheView& c = p.c;
+  if (k >= c.n) return;
+  const long n = c.n;
+  cd Af[2][3], Ab[2][3];
+  reflected_amp(p, k, Af, Ab);
+  cd c0[5], c1[4], c2[4];
+  coef1d_row(p, k, p.zo[zi], Af, Ab, c0, c1, c2);
   for (int i = 0; i < 5; ++i) {
     long r = 2L * (zi * 5 + i);
     C0[r * n + k] = c0[i].x;
@@ -174,14 +183,11 @@ cudaError_t launch_coef1d(const SynthParams& p, double* C0, double* C1, double* 
   return cudaGetLastError();
 }
 
-// Bessel tables J_n(k ρ), n = 0, 1, 2; row r = radius, k contiguous
-__global__ void k_bessel(const double* kr, long nk, const double* rho, int nr, double* J0, double* J1, double* J2) {
-  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  int r = blockIdx.y;
-  if (k >= nk) return;
-  double x = kr[k] * rho[r];
-  long o = (long)r * nk + k;
-  double a0 = j0(x), a1 = j1(x), a2;
+// J_0, J_1, J_2 of a real argument: CUDA's j0/j1, J2 by its power series below |x| = 1 and the
+// three-term recurrence above
+__device__ __forceinline__ void bessel_j012(double x, double& a0, double& a1, double& a2) {
+  a0 = j0(x);
+  a1 = j1(x);
   if (fabs(x) < 1.0) {
     // J2(x) = Σ_m (-1)^m (x/2)^{2m+2} / (m! (m+2)!)  (A&S 9.1.10); exact 0 at x = 0
     double h2 = 0.25 * x * x, t = 0.5 * h2, s = t;
@@ -193,6 +199,17 @@ __global__ void k_bessel(const double* kr, long nk, const double* rho, int nr, d
   } else {
     a2 = (2.0 / x) * a1 - a0;  // three-term recurrence (A&S 9.1.27)
   }
+}
+
+// Bessel tables J_n(k ρ), n = 0, 1, 2; row r = radius, k contiguous
+__global__ void k_bessel(const double* kr, long nk, const double* rho, int nr, double* J0, double* J1, double* J2) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (k >= nk) return;
+  double x = kr[k] * rho[r];
+  long o = (long)r * nk + k;
+  double a0, a1, a2;
+  bessel_j012(x, a0, a1, a2);
   J0[o] = a0;
   J1[o] = a1;
   J2[o] = a2;
@@ -363,31 +380,64 @@ cudaError_t launch_reduce_splits(long len, int splits, const double* partial, do
 
 // ------------------------------------------------------------------------------------
 // 1D assembly: combine orders, rotate per pixel, Julia layout (Nx, Ny, Nz, 3, 3)
+// obs-layer basis of one node: kz and the field components (E_f, E_b) of the two modes
+__device__ __forceinline__ void load_obs_basis(const CacheView& c, long node, cd kzf[2], cd kzb[2], cd ef[2][3],
+                                               cd eb[2][3]) {
+  const long n = c.n;
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    kzf[m] = ldc(c.basis, 12 + m, n, node);
+    kzb[m] = ldc(c.basis, 14 + m, n, node);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      ef[m][a] = ldc(c.basis, 2 * a + m, n, node);
+      eb[m][a] = ldc(c.basis, 6 + 2 * a + m, n, node);
+    }
+  }
+}
+
+// the nine strengths of one (node, z row) (_strengths_row!, mod_ClosedFormField.jl:616-659):
+// s[a][q] = Σ_m E_f[m][a] w (A_f[m][q] e^{i kzf z} + direct) + E_b[m][a] w (A_b ... )
+__device__ __forceinline__ void strengths_row(const SynthParams& p, long node, double z, cd W, const cd Af[2][3],
+                                              const cd Ab[2][3], const cd kzf[2], const cd kzb[2], const cd ef[2][3],
+                                              const cd eb[2][3], cd s[3][3]) {
+  cd Afd[2][3], Abd[2][3];
+  if (p.with_direct) direct_amp(p, node, z, Afd, Abd);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) s[a][b] = cd{0, 0};
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    const cd pf = phase_cl(kzf[m], z);
+    const cd pb = phase_cl(kzb[m], z - p.d_obs);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      cd tf = Af[m][q] * pf, tb = Ab[m][q] * pb;
+      if (p.with_direct) { tf += Afd[m][q]; tb += Abd[m][q]; }
+      const cd af = fin0(W * tf), ab = fin0(W * tb);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) s[a][q] += ef[m][a] * af + eb[m][a] * ab;
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------------
-__global__ void k_assemble1d(int nx, int ny, int nz, const double* xs, const double* ys, const int* rmap, int nr,
-                             const double* P0, const double* P1, const double* P2, double2* G) {
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long npix = (long)nx * ny;
-  if (t >= npix * nz) return;
-  long pix = t % npix;
-  int zi = (int)(t / npix);
-  int i = (int)(pix % nx), j = (int)(pix / nx);
-  int r = rmap[pix];
-  const long n0 = 10L * nz, n1 = 8L * nz;
-  auto g0 = [&](int col) { long o = (long)r * n0 + 2L * (zi * 5 + col); return cd{P0[o], P0[o + 1]}; };
-  auto g1 = [&](int col) { long o = (long)r * n1 + 2L * (zi * 4 + col); return cd{P1[o], P1[o + 1]}; };
-  auto g2 = [&](int col) { long o = (long)r * n1 + 2L * (zi * 4 + col); return cd{P2[o], P2[o + 1]}; };
+// one pixel of the 1D assembly: the order sums g0[5], g1[4], g2[4] of its radius combined
+// into the 3x3 dyadic of the frame along the pixel's azimuth, then rotated to (x, y):
+// G = Rot R Rotᵀ, written at pix + npix (zi + nz (cc + 3 q))
+__device__ __forceinline__ void assemble1d_pixel(double x, double y, const cd g0[5], const cd g1[4], const cd g2[4],
+                                                 long pix, long npix, int zi, int nz, double2* G) {
   cd R[3][3];
-  R[0][0] = g0(0) + g2(0);
-  R[1][0] = g0(1) + g2(1);
-  R[2][0] = g1(0);
-  R[0][1] = g0(2) + g2(2);
-  R[1][1] = g0(3) + g2(3);
-  R[2][1] = g1(1);
-  R[0][2] = g1(2);
-  R[1][2] = g1(3);
-  R[2][2] = g0(4);
-  double x = xs[i], y = ys[j];
+  R[0][0] = g0[0] + g2[0];
+  R[1][0] = g0[1] + g2[1];
+  R[2][0] = g1[0];
+  R[0][1] = g0[2] + g2[2];
+  R[1][1] = g0[3] + g2[3];
+  R[2][1] = g1[1];
+  R[0][2] = g1[2];
+  R[1][2] = g1[3];
+  R[2][2] = g0[4];
   double rho = hypot(x, y);
   double cp = rho == 0.0 ? 1.0 : x / rho, sp = rho == 0.0 ? 0.0 : y / rho;
   double Rot[3][3] = {{cp, -sp, 0.0}, {sp, cp, 0.0}, {0.0, 0.0, 1.0}};
@@ -400,6 +450,26 @@ __global__ void k_assemble1d(int nx, int ny, int nz, const double* xs, const dou
       }
       G[pix + npix * (zi + (long)nz * (cc + 3 * q))] = make_double2(s.x, s.y);
     }
+}
+
+__global__ void k_assemble1d(int nx, int ny, int nz, const double* xs, const double* ys, const int* rmap, int nr,
+                             const double* P0, const double* P1, const double* P2, double2* G) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long npix = (long)nx * ny;
+  if (t >= npix * nz) return;
+  long pix = t % npix;
+  int zi = (int)(t / npix);
+  int i = (int)(pix % nx), j = (int)(pix / nx);
+  int r = rmap[pix];
+  const long n0 = 10L * nz, n1 = 8L * nz;
+  cd g0[5], g1[4], g2[4];
+  for (int col = 0; col < 5; ++col) { long o = (long)r * n0 + 2L * (zi * 5 + col); g0[col] = cd{P0[o], P0[o + 1]}; }
+  for (int col = 0; col < 4; ++col) {
+    long o = (long)r * n1 + 2L * (zi * 4 + col);
+    g1[col] = cd{P1[o], P1[o + 1]};
+    g2[col] = cd{P2[o], P2[o + 1]};
+  }
+  assemble1d_pixel(xs[i], ys[j], g0, g1, g2, pix, npix, zi, nz, G);
 }
 
 cudaError_t launch_assemble1d(int nx, int ny, int nz, const double* xs, const double* ys, const int* rmap, int nr,
@@ -432,39 +502,11 @@ __global__ void __launch_bounds__(128) k_strengths2d(SynthParams p, double2* S, 
   cd Af[2][3], Ab[2][3];
   reflected_amp(p, node, Af, Ab);
   cd kzf[2], kzb[2], ef[2][3], eb[2][3];
-#pragma unroll
-  for (int m = 0; m < 2; ++m) {
-    kzf[m] = ldc(c.basis, 12 + m, n, node);
-    kzb[m] = ldc(c.basis, 14 + m, n, node);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      ef[m][a] = ldc(c.basis, 2 * a + m, n, node);
-      eb[m][a] = ldc(c.basis, 6 + 2 * a + m, n, node);
-    }
-  }
+  load_obs_basis(c, node, kzf, kzb, ef, eb);
   const int z0 = blockIdx.y * SG_Z, z1 = min(p.nz, z0 + SG_Z);
   for (int zi = z0; zi < z1; ++zi) {
-    const double z = p.zo[zi];
-    cd Afd[2][3], Abd[2][3];
-    if (p.with_direct) direct_amp(p, node, z, Afd, Abd);
     cd s[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) s[a][b] = cd{0, 0};
-#pragma unroll
-    for (int m = 0; m < 2; ++m) {
-      const cd pf = phase_cl(kzf[m], z);
-      const cd pb = phase_cl(kzb[m], z - p.d_obs);
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        cd tf = Af[m][q] * pf, tb = Ab[m][q] * pb;
-        if (p.with_direct) { tf += Afd[m][q]; tb += Abd[m][q]; }
-        const cd af = fin0(W * tf), ab = fin0(W * tb);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) s[a][q] += ef[m][a] * af + eb[m][a] * ab;
-      }
-    }
+    strengths_row(p, node, p.zo[zi], W, Af, Ab, kzf, kzb, ef, eb, s);
 #pragma unroll
     for (int q = 0; q < 3; ++q)
 #pragma unroll
@@ -646,6 +688,218 @@ cudaError_t launch_gl_nodes(int npanels, const double* pa, const double* pb, con
   long tot = (long)npanels * order;
   if (tot == 0) return cudaSuccess;
   k_gl_nodes<<<(unsigned)((tot + 127) / 128), 128, 0, s>>>(npanels, pa, pb, sing_side, xi, wx, order, nodes, wts);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// Batched synthesis of many small observation sets (uneven batches, one graph launch).
+// Work unit = (item, chunk of nodes), pulled by persistent CTAs from a counter. Per
+// sub-batch of SYN_SB nodes the CTA forms in shared memory
+//   2D: the strengths S[node][col] (col = zi + nz (cc + 3 q)) and the phases
+//       P[node][pix] = e^{i (kx x + ky y)};
+//   1D: the coefficient columns C[node][zi 13 + m] (m: 5 of order 0, 4 of order 1, 4 of
+//       order 2) and the tables J_n(kρ ρ_r), n = 0, 1, 2;
+// and the threads accumulate the outputs o = row + nrow col of the item's partial sum (2D
+// rows: pixels; 1D rows: distinct radii) in shared memory, a strided set of outputs each,
+// over the sub-batch's nodes in registers. k_synth_finish sums the
+// chunks of each output in chunk order (2D) or sums them and assembles the pixel (1D).
+// ------------------------------------------------------------------------------------
+constexpr int SYN_SB = 16;
+
+size_t synth_small_smem() {
+  const size_t s2 = (size_t)SYN_SB * SYN_MAXPIX * 16 + (size_t)SYN_SB * 9 * SYN_MAXZ * 16;
+  const size_t s1 = (size_t)SYN_SB * 3 * SYN_MAXR * 8 + (size_t)SYN_SB * 13 * SYN_MAXZ * 16;
+  return (size_t)SYN_MAXOUT * 16 + (s1 > s2 ? s1 : s2);
+}
+
+__device__ __forceinline__ int find_item(const long* __restrict__ off, int nb, long t) {
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(128) k_synth_small(const SynthItem* __restrict__ items, int nitems,
+                                                      const long* __restrict__ w_off, long nwork, unsigned* counter,
+                                                      int chunk) {
+  extern __shared__ __align__(16) unsigned char syn_smem[];
+  __shared__ long wsh;
+  __shared__ double kxs[SYN_SB], kys[SYN_SB], wts[SYN_SB];
+  __shared__ cd amp[SYN_SB][12];
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) wsh = (long)atomicAdd(counter, 1u);
+    __syncthreads();
+    const long w = wsh;
+    __syncthreads();
+    if (w >= nwork) return;
+    const int it = find_item(w_off, nitems, w);
+    const SynthItem& I = items[it];
+    const SynthParams& p = I.sp;
+    const CacheView& c = p.c;
+    const long cid = w - w_off[it];
+    const long k0 = cid * chunk, k1 = min(c.n, k0 + chunk);
+    const int nz = p.nz, npix = I.nx * I.ny;
+    const bool two = I.is2d != 0;
+    const int ncol = two ? 9 * nz : 13 * nz;
+    const int nrow = two ? npix : I.nr;
+    const int nout = nrow * ncol;
+    cd* acc = reinterpret_cast<cd*>(syn_smem);                        // [nout]
+    cd* Ps = acc + SYN_MAXOUT;                                        // 2D [SB][SYN_MAXPIX]
+    cd* Ss = Ps + SYN_SB * SYN_MAXPIX;                                // 2D [SB][ncol]
+    double* Js = reinterpret_cast<double*>(acc + SYN_MAXOUT);         // 1D [SB][3][SYN_MAXR]
+    cd* Cs = reinterpret_cast<cd*>(Js + SYN_SB * 3 * SYN_MAXR);       // 1D [SB][ncol]
+    for (int o = tid; o < nout; o += 128) acc[o] = cd{0.0, 0.0};
+    for (long b0 = k0; b0 < k1; b0 += SYN_SB) {
+      const int nb = (int)min((long)SYN_SB, k1 - b0);
+      if (tid < nb) {
+        const long node = b0 + tid;
+        cd Af[2][3], Ab[2][3];
+        reflected_amp(p, node, Af, Ab);
+        for (int m = 0; m < 2; ++m)
+          for (int q = 0; q < 3; ++q) { amp[tid][3 * m + q] = Af[m][q]; amp[tid][6 + 3 * m + q] = Ab[m][q]; }
+        if (two) {
+          const long k = node % c.Nk, pp = node / c.Nk;
+          double sn, cs;
+          sincos(c.phi[pp], &sn, &cs);
+          kxs[tid] = c.kr[k] * cs;
+          kys[tid] = c.kr[k] * sn;
+          wts[tid] = c.kr[k] * c.wr[k] * c.wphi[pp] / (4.0 * 3.14159265358979323846 * 3.14159265358979323846);
+        } else {
+          kxs[tid] = c.kr[node];
+        }
+      }
+      __syncthreads();
+      for (int e = tid; e < SYN_SB * nz; e += 128) {
+        const int j = e % SYN_SB, zi = e / SYN_SB;
+        if (j >= nb) continue;
+        const long node = b0 + j;
+        cd Af[2][3], Ab[2][3];
+        for (int m = 0; m < 2; ++m)
+          for (int q = 0; q < 3; ++q) { Af[m][q] = amp[j][3 * m + q]; Ab[m][q] = amp[j][6 + 3 * m + q]; }
+        if (two) {
+          cd kzf[2], kzb[2], ef[2][3], eb[2][3], sv[3][3];
+          load_obs_basis(c, node, kzf, kzb, ef, eb);
+          strengths_row(p, node, p.zo[zi], cd{wts[j], 0.0}, Af, Ab, kzf, kzb, ef, eb, sv);
+          for (int q = 0; q < 3; ++q)
+            for (int cc = 0; cc < 3; ++cc) Ss[j * ncol + zi + nz * (cc + 3 * q)] = sv[cc][q];
+        } else {
+          cd c0[5], c1[4], c2[4];
+          coef1d_row(p, node, p.zo[zi], Af, Ab, c0, c1, c2);
+          cd* dst = Cs + j * ncol + 13 * zi;
+          for (int m = 0; m < 5; ++m) dst[m] = c0[m];
+          for (int m = 0; m < 4; ++m) { dst[5 + m] = c1[m]; dst[9 + m] = c2[m]; }
+        }
+      }
+      if (two) {
+        for (int e = tid; e < nb * npix; e += 128) {
+          const int j = e / npix, px = e - j * npix;
+          const int i = px % I.nx, jj = px / I.nx;
+          double sx, cx, sy, cy;
+          sincos(kxs[j] * I.xs[i], &sx, &cx);
+          sincos(kys[j] * I.ys[jj], &sy, &cy);
+          Ps[j * SYN_MAXPIX + px] = cd{cx * cy - sx * sy, cx * sy + sx * cy};
+        }
+      } else {
+        for (int e = tid; e < nb * I.nr; e += 128) {
+          const int j = e / I.nr, r = e - j * I.nr;
+          double a0, a1, a2;
+          bessel_j012(kxs[j] * I.rho[r], a0, a1, a2);
+          double* dst = Js + j * 3 * SYN_MAXR + r;
+          dst[0] = a0;
+          dst[SYN_MAXR] = a1;
+          dst[2 * SYN_MAXR] = a2;
+        }
+      }
+      __syncthreads();
+      for (int o = tid; o < nout; o += 128) {
+        {
+          const int row = o % nrow, col = o / nrow;
+          cd a = acc[o];
+          if (two) {
+            for (int t = 0; t < nb; ++t) {
+              const cd pv = Ps[t * SYN_MAXPIX + row], sv = Ss[t * ncol + col];
+              a.x = fma(pv.x, sv.x, fma(-pv.y, sv.y, a.x));
+              a.y = fma(pv.x, sv.y, fma(pv.y, sv.x, a.y));
+            }
+          } else {
+            const int m = col % 13;
+            const int ord = m < 5 ? 0 : (m < 9 ? 1 : 2);
+            for (int t = 0; t < nb; ++t) {
+              const double jv = Js[t * 3 * SYN_MAXR + ord * SYN_MAXR + row];
+              const cd cv = Cs[t * ncol + col];
+              a.x = fma(jv, cv.x, a.x);
+              a.y = fma(jv, cv.y, a.y);
+            }
+          }
+          acc[o] = a;
+        }
+      }
+      __syncthreads();
+    }
+    double2* out = I.partial + cid * (long)nout;
+    for (int o = tid; o < nout; o += 128) out[o] = make_double2(acc[o].x, acc[o].y);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(128) k_synth_finish(const SynthItem* __restrict__ items, int nitems,
+                                                       const long* __restrict__ f_off, long nfin) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nfin) return;
+  const int it = find_item(f_off, nitems, t);
+  const SynthItem& I = items[it];
+  const long u = t - f_off[it];
+  const int nz = I.sp.nz;
+  const long npix = (long)I.nx * I.ny;
+  if (I.is2d) {
+    const long nout = npix * 9 * nz;
+    double2 s = make_double2(0.0, 0.0);
+    for (int k = 0; k < I.nw; ++k) {
+      const double2 v = I.partial[(long)k * nout + u];
+      s.x += v.x;
+      s.y += v.y;
+    }
+    I.G[u] = s;
+    return;
+  }
+  const long pix = u % npix;
+  const int zi = (int)(u / npix);
+  const int r = I.rmap[pix];
+  const long nout = (long)I.nr * 13 * nz;
+  cd g[13];
+  for (int m = 0; m < 13; ++m) {
+    cd s{0.0, 0.0};
+    const long o = r + (long)I.nr * (13 * zi + m);
+    for (int k = 0; k < I.nw; ++k) {
+      const double2 v = I.partial[(long)k * nout + o];
+      s.x += v.x;
+      s.y += v.y;
+    }
+    g[m] = s;
+  }
+  const int i = (int)(pix % I.nx), j = (int)(pix / I.nx);
+  assemble1d_pixel(I.xs[i], I.ys[j], g, g + 5, g + 9, pix, npix, zi, nz, I.G);
+}
+
+cudaError_t synth_small_init() {
+  return cudaFuncSetAttribute(k_synth_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)synth_small_smem());
+}
+
+cudaError_t launch_synth_small(const SynthItem* items, int nitems, const long* w_off, long nwork, unsigned* counter,
+                               int chunk, int grid, cudaStream_t s) {
+  if (nwork <= 0) return cudaSuccess;
+  if (grid <= 0 || chunk <= 0) return cudaErrorInvalidValue;
+  k_synth_small<<<grid, 128, synth_small_smem(), s>>>(items, nitems, w_off, nwork, counter, chunk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_synth_finish(const SynthItem* items, int nitems, const long* f_off, long nfin, cudaStream_t s) {
+  if (nfin <= 0) return cudaSuccess;
+  k_synth_finish<<<(unsigned)((nfin + 127) / 128), 128, 0, s>>>(items, nitems, f_off, nfin);
   return cudaGetLastError();
 }
 

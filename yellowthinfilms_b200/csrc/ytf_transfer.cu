@@ -371,7 +371,8 @@ __device__ bool block_modes(const LayerDev& L, double w, cd kx, cd ky, cd Q[4], 
     cd q = csqrt(mu[i]);
     if (!(cabs(q) > 1e-12 * sqrt(scale))) return false;
     // b = B21 a / q
-    cd bx = (B[2][0] * ax + B[2][1] * ay) / q, by = (B[3][0] * ax + B[3][1] * ay) / q;
+    const cd rq = recip(q);
+    cd bx = (B[2][0] * ax + B[2][1] * ay) * rq, by = (B[3][0] * ax + B[3][1] * ay) * rq;
 #pragma unroll
     for (int sgn = 0; sgn < 2; ++sgn) {
       cd v[4] = {ax, ay, sgn ? -bx : bx, sgn ? -by : by};
@@ -646,15 +647,15 @@ __device__ bool source_projection(cd kx, cd ky, double w, const LayerDev& L, con
   cd etz1 = E(L, 1, 3), etz2 = E(L, 2, 3), ezz = E(L, 3, 3);
   cd jw{0.0, -w};
   cd J[4][3];
-  cd ezw = ezz * w;
+  const cd rezw = recip(ezz * w), rezz = recip(ezz);
   cd jz = jw;  // (-iω)·ẑ column only
   for (int q = 0; q < 3; ++q) {
     cd z = q == 2 ? jz : cd{0.0, 0.0} * jw;
-    J[0][q] = kx * z / ezw;
-    J[1][q] = ky * z / ezw;
+    J[0][q] = kx * z * rezw;
+    J[1][q] = ky * z * rezw;
     cd jtx = q == 0 ? jw : cd{0.0, 0.0}, jty = q == 1 ? jw : cd{0.0, 0.0};
-    J[2][q] = jty - etz2 * z / ezz;
-    J[3][q] = -jtx - (-etz1) * z / ezz;
+    J[2][q] = jty - etz2 * z * rezz;
+    J[3][q] = -jtx - (-etz1) * z * rezz;
   }
   cd V[4][4], W[4][4];
   for (int i = 0; i < 4; ++i) {
@@ -689,12 +690,13 @@ __device__ void write_basis(const TransferParams& p, int oi, long node, long nou
                             cd kx, cd ky) {
   cd ezt1 = E(L, 3, 1), ezt2 = E(L, 3, 2), ezz = E(L, 3, 3);
   double iw = 1.0 / p.omega;
+  const cd rezz = recip(ezz);
   double2* b = p.basis + (long)oi * 16 * nout;
   for (int m = 0; m < 2; ++m) {
     cd exf = M.vf[0][m], eyf = M.vf[1][m];
-    cd ezf = -(ezt1 * M.vf[0][m] + ezt2 * M.vf[1][m] + iw * (kx * M.vf[3][m] - ky * M.vf[2][m])) / ezz;
+    cd ezf = -(ezt1 * M.vf[0][m] + ezt2 * M.vf[1][m] + iw * (kx * M.vf[3][m] - ky * M.vf[2][m])) * rezz;
     cd exb = M.vb[0][m], eyb = M.vb[1][m];
-    cd ezb = -(ezt1 * M.vb[0][m] + ezt2 * M.vb[1][m] + iw * (kx * M.vb[3][m] - ky * M.vb[2][m])) / ezz;
+    cd ezb = -(ezt1 * M.vb[0][m] + ezt2 * M.vb[1][m] + iw * (kx * M.vb[3][m] - ky * M.vb[2][m])) * rezz;
     cd kzf = M.qf[m], kzb = M.qb[m];
     bool ok = isfin(exf) && isfin(eyf) && isfin(ezf) && isfin(exb) && isfin(eyb) && isfin(ezb) && isfin(kzf) && isfin(kzb);
     cd z{0, 0};
@@ -1260,6 +1262,74 @@ __global__ void __launch_bounds__(128) k_chain_batch(const TransferParams* __res
   if (t >= off[nb]) return;
   const int i = find_problem(off, nb, t);
   chain_body(probs[i], t - off[i]);
+}
+
+// ------------------------------------------------------------------------------------
+// Persistent forms of the batched transfer kernels (uneven batches replayed as one CUDA
+// graph): a fixed grid of CTAs pulls tiles (problem, unit range) from a device counter until
+// the queue is empty, so CTAs that drew short problems take more tiles instead of idling
+// behind the longest one; a tile's units go to the CTA's threads in a block-stride loop.
+// Units per stage: 0 modes and 1 QR = (layer, node) pairs, layer-major; 3 chain, 4 match,
+// 5 seeds, 7 scan = nodes; 6 iface = (interface, node) pairs. The counter is zeroed before
+// each launch (a memset node of the same graph). No CTA waits on another.
+// ------------------------------------------------------------------------------------
+template <int STAGE>
+__device__ __forceinline__ void stage_unit(const TransferParams& p, long u) {
+  if constexpr (STAGE == 0 || STAGE == 1) {
+    const int layer = (int)(u / p.n);
+    if constexpr (STAGE == 0) layer_modes_body(p, layer, u - (long)layer * p.n);
+    else layer_modes_qr_body(p, layer, u - (long)layer * p.n);
+  } else if constexpr (STAGE == 3) {
+    chain_body(p, u);
+  } else if constexpr (STAGE == 4) {
+    match_body(p, u);
+  } else if constexpr (STAGE == 5) {
+    seeds_body(p, u);
+  } else if constexpr (STAGE == 6) {
+    const int j = (int)(u / p.n) + 2;
+    iface_body(p, j, u - (long)(j - 2) * p.n);
+  } else {
+    scan_body(p, u);
+  }
+}
+
+template <int STAGE, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_persist(const TransferParams* __restrict__ probs, TileQueue q) {
+  __shared__ int tile;
+  for (;;) {
+    if (threadIdx.x == 0) tile = (int)atomicAdd(q.counter, 1u);
+    __syncthreads();
+    const int t = tile;
+    __syncthreads();
+    if (t >= q.ntiles) return;
+    const TransferParams& p = probs[q.prob[t]];
+    const long e = q.end[t];
+    for (long u = q.start[t] + threadIdx.x; u < e; u += BLOCK) stage_unit<STAGE>(p, u);
+  }
+}
+
+template <int BLOCK>
+cudaError_t launch_persist_b(int stage, int grid, const TransferParams* probs, const TileQueue& q, cudaStream_t s) {
+  switch (stage) {
+    case 0: k_persist<0, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
+    case 1: k_persist<1, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
+    case 3: k_persist<3, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
+    case 4: k_persist<4, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
+    case 5: k_persist<5, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
+    case 6: k_persist<6, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
+    case 7: k_persist<7, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_persist(int stage, int block, int grid, const TransferParams* probs, const TileQueue& q,
+                           cudaStream_t s) {
+  if (q.ntiles <= 0) return cudaSuccess;
+  if (grid <= 0) return cudaErrorInvalidValue;
+  if (block == 128) return launch_persist_b<128>(stage, grid, probs, q, s);
+  if (block == 256) return launch_persist_b<256>(stage, grid, probs, q, s);
+  return cudaErrorInvalidValue;
 }
 
 // ------------------------------------------------------------------------------------
