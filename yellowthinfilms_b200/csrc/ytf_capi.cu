@@ -1819,7 +1819,7 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
   std::vector<SynthItem> items;
   std::vector<long> woff{0}, foff{0};
   std::vector<int> item_of;
-  size_t npart = 0;
+  size_t npart = 0, syn_smem = 0;
   for (int i = 0; i < nb; ++i) {
     const ytf_green_desc& g = P->gr[i];
     const long npix = (long)g.nx * g.ny;
@@ -1841,6 +1841,7 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
     it.G = P->g_off[i] >= 0 ? P->d_G + P->g_off[i] : (double2*)g.out;
     items.push_back(it);
     item_of.push_back(i);
+    syn_smem = std::max(syn_smem, synth_small_smem(it.is2d, (int)npix, it.nr, g.nz));
     npart += (size_t)it.nw * P->nout_syn[i];
     woff.push_back(woff.back() + it.nw);
     foff.push_back(foff.back() + (it.is2d ? npix * 9 * g.nz : npix * g.nz));
@@ -1896,7 +1897,7 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
     const long* df = reinterpret_cast<const long*>(P->tb + o_foff);
     if (woff.back() > 0) {
       const int grid = (int)std::min<long>(woff.back(), (long)t.synth_ctas_per_sm * nsm);
-      step(launch_synth_small(di, (int)items.size(), dw, woff.back(), ctr + synth_counter, t.chunk, grid, s));
+      step(launch_synth_small(di, (int)items.size(), dw, woff.back(), ctr + synth_counter, t.chunk, grid, syn_smem, s));
       P->kcount["k_synth_small"] += 1;
     }
     step(launch_synth_finish(di, (int)items.size(), df, foff.back(), s));

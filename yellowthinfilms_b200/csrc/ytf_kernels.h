@@ -165,11 +165,13 @@ struct SynthItem {
   double2* partial;        // [nw][outputs]
   double2* G;              // [nx ny nz 9] Julia layout (device)
 };
-size_t synth_small_smem();
+size_t synth_small_smem();                                      // the largest item's
+size_t synth_small_smem(int is2d, int npix, int nr, int nz);    // one item's
 cudaError_t synth_small_init();  // shared-memory attribute of k_synth_small (before any capture)
-// w_off[nitems + 1]: prefix of the items' chunk counts; counter zeroed before the launch
+// w_off[nitems + 1]: prefix of the items' chunk counts; counter zeroed before the launch;
+// smem: the largest synth_small_smem(item) of the batch
 cudaError_t launch_synth_small(const SynthItem* items, int nitems, const long* w_off, long nwork, unsigned* counter,
-                               int chunk, int grid, cudaStream_t s);
+                               int chunk, int grid, size_t smem, cudaStream_t s);
 // f_off[nitems + 1]: prefix of the items' finish units (2D: nx ny 9 nz, 1D: nx ny nz)
 cudaError_t launch_synth_finish(const SynthItem* items, int nitems, const long* f_off, long nfin, cudaStream_t s);
 

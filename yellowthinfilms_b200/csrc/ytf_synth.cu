@@ -401,8 +401,11 @@ __device__ __forceinline__ void load_obs_basis(const CacheView& c, long node, cd
 __device__ __forceinline__ void strengths_row(const SynthParams& p, long node, double z, cd W, const cd Af[2][3],
                                               const cd Ab[2][3], const cd kzf[2], const cd kzb[2], const cd ef[2][3],
                                               const cd eb[2][3], cd s[3][3]) {
-  cd Afd[2][3], Abd[2][3];
-  if (p.with_direct) direct_amp(p, node, z, Afd, Abd);
+  // the direct term (direct_amp) is formed per mode inline: sf[m][q] e^{i Qf zeta} above the
+  // source, sb[m][q] e^{i Qb zeta} below it, exact zeros elsewhere (as direct_amp's arrays)
+  const CacheView& c = p.c;
+  const double zeta = z - p.zpos;
+  const bool dir = p.with_direct && c.valid[node];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -411,10 +414,17 @@ __device__ __forceinline__ void strengths_row(const SynthParams& p, long node, d
   for (int m = 0; m < 2; ++m) {
     const cd pf = phase_cl(kzf[m], z);
     const cd pb = phase_cl(kzb[m], z - p.d_obs);
+    cd edf{0.0, 0.0}, edb{0.0, 0.0};
+    const bool up = dir && zeta > 0, dn = dir && zeta < 0;
+    if (up) edf = phase_cl(ldc(c.Qf, m, c.n, node), zeta);
+    if (dn) edb = phase_cl(ldc(c.Qb, m, c.n, node), zeta);
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       cd tf = Af[m][q] * pf, tb = Ab[m][q] * pb;
-      if (p.with_direct) { tf += Afd[m][q]; tb += Abd[m][q]; }
+      if (p.with_direct) {
+        tf += up ? ldc(c.sf, m + 2 * q, c.n, node) * edf : cd{0.0, 0.0};
+        tb += dn ? ldc(c.sb, m + 2 * q, c.n, node) * edb : cd{0.0, 0.0};
+      }
       const cd af = fin0(W * tf), ab = fin0(W * tb);
 #pragma unroll
       for (int a = 0; a < 3; ++a) s[a][q] += ef[m][a] * af + eb[m][a] * ab;
@@ -488,7 +498,7 @@ cudaError_t launch_assemble1d(int nx, int ny, int nz, const double* xs, const do
 // the IEEE bits, which order like the values for non-negative doubles (Inf/NaN sort above
 // every finite value, so a non-finite strength shows in the slice's maximum).
 // ------------------------------------------------------------------------------------
-constexpr int SG_Z = 2;  // z-rows per thread
+constexpr int SG_Z = 8;  // z-rows per thread
 
 __global__ void __launch_bounds__(128) k_strengths2d(SynthParams p, double2* S, unsigned long long* colmax, long kchunk) {
   const long nidx = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -694,22 +704,33 @@ cudaError_t launch_gl_nodes(int npanels, const double* pa, const double* pb, con
 // ------------------------------------------------------------------------------------
 // Batched synthesis of many small observation sets (uneven batches, one graph launch).
 // Work unit = (item, chunk of nodes), pulled by persistent CTAs from a counter. Per
-// sub-batch of SYN_SB nodes the CTA forms in shared memory
-//   2D: the strengths S[node][col] (col = zi + nz (cc + 3 q)) and the phases
-//       P[node][pix] = e^{i (kx x + ky y)};
-//   1D: the coefficient columns C[node][zi 13 + m] (m: 5 of order 0, 4 of order 1, 4 of
-//       order 2) and the tables J_n(kρ ρ_r), n = 0, 1, 2;
-// and the threads accumulate the outputs o = row + nrow col of the item's partial sum (2D
+// sub-batch of SYN_SB = 64 nodes, threads 0-63 take one node each and form in shared memory
+//   2D: its strengths S[node][col] (col = zi + nz (cc + 3 q)), reflected amplitudes first;
+//   1D: its coefficient columns C[node][zi 13 + m] (m: 5 of order 0, 4 of order 1, 4 of
+//       order 2);
+// while threads 64-127 form for the same nodes
+//   2D: the phases P[node][pix] = e^{i kx x} e^{i ky y} (one sincos per x and per y);
+//   1D: the tables J_n(kρ ρ_r), n = 0, 1, 2;
+// then all threads accumulate the outputs o = row + nrow col of the item's partial sum (2D
 // rows: pixels; 1D rows: distinct radii) in shared memory, a strided set of outputs each,
-// over the sub-batch's nodes in registers. k_synth_finish sums the
-// chunks of each output in chunk order (2D) or sums them and assembles the pixel (1D).
+// over the sub-batch's nodes in registers. The shared arrays are laid out with the item's own
+// sizes. k_synth_finish sums the chunks of each output in chunk order (2D) or sums them and
+// assembles the pixel (1D).
 // ------------------------------------------------------------------------------------
-constexpr int SYN_SB = 16;
+constexpr int SYN_SB = 64;
+
+// shared bytes of one item's work unit
+__host__ __device__ __forceinline__ size_t synth_item_smem(int is2d, int npix, int nr, int nz) {
+  const size_t nout = is2d ? (size_t)npix * 9 * nz : (size_t)nr * 13 * nz;
+  if (is2d) return 16 * nout + (size_t)SYN_SB * (npix + 9 * nz) * 16;
+  return 16 * nout + (size_t)SYN_SB * 3 * nr * 8 + (size_t)SYN_SB * 13 * nz * 16;
+}
+
+size_t synth_small_smem(int is2d, int npix, int nr, int nz) { return synth_item_smem(is2d, npix, nr, nz); }
 
 size_t synth_small_smem() {
-  const size_t s2 = (size_t)SYN_SB * SYN_MAXPIX * 16 + (size_t)SYN_SB * 9 * SYN_MAXZ * 16;
-  const size_t s1 = (size_t)SYN_SB * 3 * SYN_MAXR * 8 + (size_t)SYN_SB * 13 * SYN_MAXZ * 16;
-  return (size_t)SYN_MAXOUT * 16 + (s1 > s2 ? s1 : s2);
+  const size_t a = synth_item_smem(1, SYN_MAXPIX, 0, SYN_MAXZ), b = synth_item_smem(0, 0, SYN_MAXR, SYN_MAXZ);
+  return a > b ? a : b;
 }
 
 __device__ __forceinline__ int find_item(const long* __restrict__ off, int nb, long t) {
@@ -727,8 +748,6 @@ __global__ void __launch_bounds__(128) k_synth_small(const SynthItem* __restrict
                                                       int chunk) {
   extern __shared__ __align__(16) unsigned char syn_smem[];
   __shared__ long wsh;
-  __shared__ double kxs[SYN_SB], kys[SYN_SB], wts[SYN_SB];
-  __shared__ cd amp[SYN_SB][12];
   const int tid = threadIdx.x;
   for (;;) {
     if (tid == 0) wsh = (long)atomicAdd(counter, 1u);
@@ -747,96 +766,95 @@ __global__ void __launch_bounds__(128) k_synth_small(const SynthItem* __restrict
     const int ncol = two ? 9 * nz : 13 * nz;
     const int nrow = two ? npix : I.nr;
     const int nout = nrow * ncol;
-    cd* acc = reinterpret_cast<cd*>(syn_smem);                        // [nout]
-    cd* Ps = acc + SYN_MAXOUT;                                        // 2D [SB][SYN_MAXPIX]
-    cd* Ss = Ps + SYN_SB * SYN_MAXPIX;                                // 2D [SB][ncol]
-    double* Js = reinterpret_cast<double*>(acc + SYN_MAXOUT);         // 1D [SB][3][SYN_MAXR]
-    cd* Cs = reinterpret_cast<cd*>(Js + SYN_SB * 3 * SYN_MAXR);       // 1D [SB][ncol]
+    cd* acc = reinterpret_cast<cd*>(syn_smem);                      // [nout]
+    cd* Ss = acc + nout;                                            // 2D [SB][ncol]
+    cd* Ps = Ss + SYN_SB * ncol;                                    // 2D [SB][npix]
+    cd* Cs = acc + nout;                                            // 1D [SB][ncol]
+    double* Js = reinterpret_cast<double*>(Cs + SYN_SB * ncol);     // 1D [SB][3][nr]
     for (int o = tid; o < nout; o += 128) acc[o] = cd{0.0, 0.0};
     for (long b0 = k0; b0 < k1; b0 += SYN_SB) {
       const int nb = (int)min((long)SYN_SB, k1 - b0);
-      if (tid < nb) {
-        const long node = b0 + tid;
-        cd Af[2][3], Ab[2][3];
-        reflected_amp(p, node, Af, Ab);
-        for (int m = 0; m < 2; ++m)
-          for (int q = 0; q < 3; ++q) { amp[tid][3 * m + q] = Af[m][q]; amp[tid][6 + 3 * m + q] = Ab[m][q]; }
-        if (two) {
+      const int j = tid & (SYN_SB - 1);
+      const long node = b0 + j;
+      if (j < nb) {
+        if (tid < SYN_SB) {
+          cd Af[2][3], Ab[2][3];
+          reflected_amp(p, node, Af, Ab);
+          if (two) {
+            const long k = node % c.Nk, pp = node / c.Nk;
+            const double wt = c.kr[k] * c.wr[k] * c.wphi[pp] / (4.0 * 3.14159265358979323846 * 3.14159265358979323846);
+            cd kzf[2], kzb[2], ef[2][3], eb[2][3];
+            load_obs_basis(c, node, kzf, kzb, ef, eb);
+            for (int zi = 0; zi < nz; ++zi) {
+              cd sv[3][3];
+              strengths_row(p, node, p.zo[zi], cd{wt, 0.0}, Af, Ab, kzf, kzb, ef, eb, sv);
+              for (int q = 0; q < 3; ++q)
+                for (int cc = 0; cc < 3; ++cc) Ss[j * ncol + zi + nz * (cc + 3 * q)] = sv[cc][q];
+            }
+          } else {
+            for (int zi = 0; zi < nz; ++zi) {
+              cd c0[5], c1[4], c2[4];
+              coef1d_row(p, node, p.zo[zi], Af, Ab, c0, c1, c2);
+              cd* dst = Cs + j * ncol + 13 * zi;
+              for (int m = 0; m < 5; ++m) dst[m] = c0[m];
+              for (int m = 0; m < 4; ++m) { dst[5 + m] = c1[m]; dst[9 + m] = c2[m]; }
+            }
+          }
+        } else if (two) {
           const long k = node % c.Nk, pp = node / c.Nk;
           double sn, cs;
           sincos(c.phi[pp], &sn, &cs);
-          kxs[tid] = c.kr[k] * cs;
-          kys[tid] = c.kr[k] * sn;
-          wts[tid] = c.kr[k] * c.wr[k] * c.wphi[pp] / (4.0 * 3.14159265358979323846 * 3.14159265358979323846);
+          const double kx = c.kr[k] * cs, ky = c.kr[k] * sn;
+          double sy[8], cy[8];
+          const int ny8 = min(I.ny, 8);
+          for (int jj = 0; jj < ny8; ++jj) sincos(ky * I.ys[jj], &sy[jj], &cy[jj]);
+          for (int i = 0; i < I.nx; ++i) {
+            double sx, cx;
+            sincos(kx * I.xs[i], &sx, &cx);
+            for (int jj = 0; jj < I.ny; ++jj) {
+              double s2, c2;
+              if (jj < 8) { s2 = sy[jj]; c2 = cy[jj]; }
+              else sincos(ky * I.ys[jj], &s2, &c2);
+              Ps[j * npix + i + I.nx * jj] = cd{cx * c2 - sx * s2, cx * s2 + sx * c2};
+            }
+          }
         } else {
-          kxs[tid] = c.kr[node];
-        }
-      }
-      __syncthreads();
-      for (int e = tid; e < SYN_SB * nz; e += 128) {
-        const int j = e % SYN_SB, zi = e / SYN_SB;
-        if (j >= nb) continue;
-        const long node = b0 + j;
-        cd Af[2][3], Ab[2][3];
-        for (int m = 0; m < 2; ++m)
-          for (int q = 0; q < 3; ++q) { Af[m][q] = amp[j][3 * m + q]; Ab[m][q] = amp[j][6 + 3 * m + q]; }
-        if (two) {
-          cd kzf[2], kzb[2], ef[2][3], eb[2][3], sv[3][3];
-          load_obs_basis(c, node, kzf, kzb, ef, eb);
-          strengths_row(p, node, p.zo[zi], cd{wts[j], 0.0}, Af, Ab, kzf, kzb, ef, eb, sv);
-          for (int q = 0; q < 3; ++q)
-            for (int cc = 0; cc < 3; ++cc) Ss[j * ncol + zi + nz * (cc + 3 * q)] = sv[cc][q];
-        } else {
-          cd c0[5], c1[4], c2[4];
-          coef1d_row(p, node, p.zo[zi], Af, Ab, c0, c1, c2);
-          cd* dst = Cs + j * ncol + 13 * zi;
-          for (int m = 0; m < 5; ++m) dst[m] = c0[m];
-          for (int m = 0; m < 4; ++m) { dst[5 + m] = c1[m]; dst[9 + m] = c2[m]; }
-        }
-      }
-      if (two) {
-        for (int e = tid; e < nb * npix; e += 128) {
-          const int j = e / npix, px = e - j * npix;
-          const int i = px % I.nx, jj = px / I.nx;
-          double sx, cx, sy, cy;
-          sincos(kxs[j] * I.xs[i], &sx, &cx);
-          sincos(kys[j] * I.ys[jj], &sy, &cy);
-          Ps[j * SYN_MAXPIX + px] = cd{cx * cy - sx * sy, cx * sy + sx * cy};
-        }
-      } else {
-        for (int e = tid; e < nb * I.nr; e += 128) {
-          const int j = e / I.nr, r = e - j * I.nr;
-          double a0, a1, a2;
-          bessel_j012(kxs[j] * I.rho[r], a0, a1, a2);
-          double* dst = Js + j * 3 * SYN_MAXR + r;
-          dst[0] = a0;
-          dst[SYN_MAXR] = a1;
-          dst[2 * SYN_MAXR] = a2;
+          const double kx = c.kr[node];
+          double* dst = Js + j * 3 * I.nr;
+          for (int r = 0; r < I.nr; ++r) {
+            double a0, a1, a2;
+            bessel_j012(kx * I.rho[r], a0, a1, a2);
+            dst[r] = a0;
+            dst[I.nr + r] = a1;
+            dst[2 * I.nr + r] = a2;
+          }
         }
       }
       __syncthreads();
       for (int o = tid; o < nout; o += 128) {
-        {
-          const int row = o % nrow, col = o / nrow;
-          cd a = acc[o];
-          if (two) {
-            for (int t = 0; t < nb; ++t) {
-              const cd pv = Ps[t * SYN_MAXPIX + row], sv = Ss[t * ncol + col];
-              a.x = fma(pv.x, sv.x, fma(-pv.y, sv.y, a.x));
-              a.y = fma(pv.x, sv.y, fma(pv.y, sv.x, a.y));
-            }
-          } else {
-            const int m = col % 13;
-            const int ord = m < 5 ? 0 : (m < 9 ? 1 : 2);
-            for (int t = 0; t < nb; ++t) {
-              const double jv = Js[t * 3 * SYN_MAXR + ord * SYN_MAXR + row];
-              const cd cv = Cs[t * ncol + col];
-              a.x = fma(jv, cv.x, a.x);
-              a.y = fma(jv, cv.y, a.y);
-            }
+        const int row = o % nrow, cidx = o / nrow;
+        cd a = acc[o];
+        if (two) {
+          const cd* pp = Ps + row;
+          const cd* sp = Ss + cidx;
+          for (int t = 0; t < nb; ++t) {
+            const cd pv = pp[t * npix], sv = sp[t * ncol];
+            a.x = fma(pv.x, sv.x, fma(-pv.y, sv.y, a.x));
+            a.y = fma(pv.x, sv.y, fma(pv.y, sv.x, a.y));
           }
-          acc[o] = a;
+        } else {
+          const int m = cidx % 13;
+          const int ord = m < 5 ? 0 : (m < 9 ? 1 : 2);
+          const double* jp = Js + ord * I.nr + row;
+          const cd* cp = Cs + cidx;
+          for (int t = 0; t < nb; ++t) {
+            const double jv = jp[t * 3 * I.nr];
+            const cd cv = cp[t * ncol];
+            a.x = fma(jv, cv.x, a.x);
+            a.y = fma(jv, cv.y, a.y);
+          }
         }
+        acc[o] = a;
       }
       __syncthreads();
     }
@@ -890,10 +908,10 @@ cudaError_t synth_small_init() {
 }
 
 cudaError_t launch_synth_small(const SynthItem* items, int nitems, const long* w_off, long nwork, unsigned* counter,
-                               int chunk, int grid, cudaStream_t s) {
+                               int chunk, int grid, size_t smem, cudaStream_t s) {
   if (nwork <= 0) return cudaSuccess;
-  if (grid <= 0 || chunk <= 0) return cudaErrorInvalidValue;
-  k_synth_small<<<grid, 128, synth_small_smem(), s>>>(items, nitems, w_off, nwork, counter, chunk);
+  if (grid <= 0 || chunk <= 0 || smem > synth_small_smem()) return cudaErrorInvalidValue;
+  k_synth_small<<<grid, 128, smem, s>>>(items, nitems, w_off, nwork, counter, chunk);
   return cudaGetLastError();
 }
 
