@@ -218,6 +218,33 @@ def test_transfer_2d_full_solve_matches_oracle(ytf, oracle, idx):
             assert relerr(G, Go) < 1e-9, (src, obs, relerr(G, Go))
 
 
+@pytest.mark.parametrize("nz", [3, 6, 8, 11])
+def test_green_2d_even_rows_match_oracle(ytf, oracle, nz):
+    """Evenly spaced z rows (the strength kernel steps the phases e^{i kz z} by recurrence
+    where no row's exponent nears the clamp) on both sides of the source and in the other
+    layers, with nodes far into the evanescent range (kρ up to 150 k0: exponents -Im(kz) z
+    beyond 690, where the per-row clamped phase takes over): every precision agrees with the
+    oracle as on unevenly spaced rows."""
+    _, st = FOUNDATION_STACKS[4]
+    kr, wr = krho_grid(st, W, kmax=150.0 * W, width=6.0)
+    ph, wp = uniform_phi(6)
+    src = 2
+    gc = ytf.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp)
+    oc = oracle.build_cavity_transfer_2d(st, W, src, kr, wr, ph, wp)
+    xs = np.array([-0.2, 0.0, 0.3])
+    zs = 0.45 * st[src - 1].d
+    for obs in (src, 1, 3):
+        d = st[obs - 1].d
+        zo = np.linspace(0.05 * d, 0.95 * d, nz)
+        Go = oracle.closed_form_G(oc, obs, zs, zo, xs, xs)
+        assert relerr(ytf.closed_form_G(gc, obs, zs, zo, xs, xs), Go) < 1e-10, obs
+        assert relerr(ytf.closed_form_G(gc, obs, zs, zo, xs, xs, precision="int8x3"), Go) < 1e-6, obs
+        if obs == src:
+            for terms in ("direct", "scattered", "toeplitz", "hankel"):
+                Gt = ytf.closed_form_G(gc, obs, zs, zo, xs, xs, terms=terms)
+                assert relerr(Gt, oracle.closed_form_G(oc, obs, zs, zo, xs, xs, terms=terms)) < 1e-10, terms
+
+
 def test_transfer_2d_rotation_fill_matches_oracle(ytf, oracle):
     st = [lay(m_vac, 1.0), lay(m_uni, 0.8), lay(m_gl, 0.5), lay(m_vac, 1.0)]
     kr, wr = krho_grid(st, W, kmax=12.0, width=1.0)

@@ -1275,6 +1275,7 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
   } else {
     int ncol = 9 * nz;
     WS(S, double2, "g_S", (size_t)ncol * c->n);
+    WS(amp, double2, "g_amp", (size_t)12 * c->n);
     if (precision == YTF_PREC_INT8X3) {
       // int8 tensor cores: FP32 phase tables, fixed-point digits, exact INT32 accumulation,
       // FP64 reduction of the node slices
@@ -1301,7 +1302,7 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
       WS(Bq, uint8_t, "g_i8_b", (size_t)lp.ntile * lp.nchunk * (kchunk / 32) * lateral_i8_stage_bytes(lp.Np));
       WS(cmax, unsigned long long, "g_i8_cmax", (size_t)lp.nchunk * ncol);
       CK(cudaMemsetAsync(cmax, 0, sizeof(unsigned long long) * lp.nchunk * ncol, ctx->stream));
-      CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream, cmax, kchunk)));
+      CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream, cmax, kchunk, amp)));
       WS(Gp, double2, "g_partial2", (size_t)lp.nchunk * npix * ncol);
       unsigned* err = gb ? gb->err : nullptr;
       if (!err) {
@@ -1319,7 +1320,7 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
         if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
       }
     } else {
-      CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream)));
+      CK(LAUNCH("k_strengths2d", launch_strengths2d(sp, S, ctx->stream, nullptr, 0, amp)));
       if (precision == YTF_PREC_SPLIT_BF16) {
         // tensor cores: FP32 phase tables, split-BF16 contraction, FP64 reduction of the slices
         WS(Px, float2, "g_px", (size_t)c->n * nx);

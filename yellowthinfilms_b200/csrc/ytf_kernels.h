@@ -138,9 +138,10 @@ cudaError_t launch_reduce_splits(long len, int splits, const double* partial, do
 cudaError_t launch_assemble1d(int nx, int ny, int nz, const double* xs, const double* ys, const int* rmap, int nr,
                               const double* P0, const double* P1, const double* P2, double2* G, cudaStream_t s);
 // 2D direct lateral synthesis
-// colmax (optional, zeroed by the caller): [n / kchunk][9 nz] IEEE bits of max(|Re|, |Im|)
+// colmax (optional, zeroed by the caller): [n / kchunk][9 nz] IEEE bits of max(|Re|, |Im|);
+// amp (optional scratch, [12][n] complex): the two-kernel form (k_reflect2d, k_strengths_rows)
 cudaError_t launch_strengths2d(const SynthParams& p, double2* S, cudaStream_t s, unsigned long long* colmax = nullptr,
-                               long kchunk = 0);
+                               long kchunk = 0, double2* amp = nullptr);
 int lateral_splits(long n, int splits);  // effective split count of launch_lateral
 cudaError_t launch_lateral(const CacheView& c, int nx, int ny, const double* xs, const double* ys, int ncol, const double2* S,
                            double2* partial, int splits, cudaStream_t s);

@@ -536,9 +536,122 @@ __global__ void __launch_bounds__(128) k_strengths2d(SynthParams p, double2* S, 
   }
 }
 
-cudaError_t launch_strengths2d(const SynthParams& p, double2* S, cudaStream_t s, unsigned long long* colmax, long kchunk) {
+// ------------------------------------------------------------------------------------
+// The same strengths in two kernels, for callers that give a scratch array `amp`:
+// k_reflect2d writes each node's reflected amplitudes (A_f, A_b: 12 complex, node fastest)
+// once; k_strengths_rows stages 32 nodes' amplitudes, basis, seeds and q's in shared memory
+// (coalesced, once per block), then each of its 4 warps takes every fourth z row of the 32
+// nodes, one node per lane. The arithmetic per row is strengths_row's, in the same order.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_reflect2d(SynthParams p, double2* __restrict__ amp) {
+  const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long n = p.c.n;
+  if (node >= n) return;
+  cd Af[2][3], Ab[2][3];
+  reflected_amp(p, node, Af, Ab);
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      amp[(long)(3 * m + q) * n + node] = make_double2(Af[m][q].x, Af[m][q].y);
+      amp[(long)(6 + 3 * m + q) * n + node] = make_double2(Ab[m][q].x, Ab[m][q].y);
+    }
+}
+
+// per node of a k_strengths_rows block: 12 amplitudes, the obs-layer basis (16), sf, sb (6 each),
+// Qf, Qb (2 each)
+constexpr int SR_F = 44;
+__global__ void __launch_bounds__(128) k_strengths_rows(SynthParams p, const double2* __restrict__ amp,
+                                                         double2* __restrict__ S, unsigned long long* colmax,
+                                                         long kchunk) {
+  __shared__ double2 sh[SR_F][32];
+  __shared__ double wsh[32];
+  __shared__ int vsh[32];
+  const CacheView& c = p.c;
+  const long n = c.n;
+  const long node0 = (long)blockIdx.x * 32;
+  const int tid = threadIdx.x, lane = tid & 31;
+  // stage the 32 nodes' inputs: field f of node node0 + j at sh[f][j] (coalesced over j)
+  for (int e = tid; e < SR_F * 32; e += 128) {
+    const int j = e & 31, f = e >> 5;
+    const long node = min(node0 + j, n - 1);
+    const double2* src;
+    long fe;
+    if (f < 12) { src = amp; fe = f; }
+    else if (f < 28) { src = c.basis; fe = f - 12; }
+    else if (f < 34) { src = c.sf; fe = f - 28; }
+    else if (f < 40) { src = c.sb; fe = f - 34; }
+    else if (f < 42) { src = c.Qf; fe = f - 40; }
+    else { src = c.Qb; fe = f - 42; }
+    sh[f][j] = src[fe * n + node];
+  }
+  if (tid < 32) {
+    const long node = min(node0 + tid, n - 1);
+    const long k = node % c.Nk, pp = node / c.Nk;
+    wsh[tid] = c.kr[k] * c.wr[k] * c.wphi[pp] / (4.0 * 3.14159265358979323846 * 3.14159265358979323846);
+    vsh[tid] = c.valid[node];
+  }
+  __syncthreads();
+  const long nidx = node0 + lane;
+  const bool live = nidx < n;
+  auto g = [&](int f) { const double2 v = sh[f][lane]; return cd{v.x, v.y}; };
+  const cd W{wsh[lane], 0.0};
+  const bool dir = p.with_direct && vsh[lane];
+  for (int zi = tid >> 5; zi < p.nz; zi += 4) {
+    const double z = p.zo[zi];
+    const double zeta = z - p.zpos;
+    cd s[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) s[a][b] = cd{0, 0};
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const cd pf = phase_cl(g(24 + m), z);            // basis element 12 + m: kzf
+      const cd pb = phase_cl(g(26 + m), z - p.d_obs);  // basis element 14 + m: kzb
+      cd edf{0.0, 0.0}, edb{0.0, 0.0};
+      const bool up = dir && zeta > 0, dn = dir && zeta < 0;
+      if (up) edf = phase_cl(g(40 + m), zeta);
+      if (dn) edb = phase_cl(g(42 + m), zeta);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        cd tf = g(3 * m + q) * pf, tb = g(6 + 3 * m + q) * pb;
+        if (p.with_direct) {
+          tf += up ? g(28 + m + 2 * q) * edf : cd{0.0, 0.0};
+          tb += dn ? g(34 + m + 2 * q) * edb : cd{0.0, 0.0};
+        }
+        const cd af = fin0(W * tf), ab = fin0(W * tb);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) s[a][q] += g(12 + 2 * a + m) * af + g(18 + 2 * a + m) * ab;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        const long col = zi + (long)p.nz * (cc + 3 * q);
+        if (live) S[col * n + nidx] = make_double2(s[cc][q].x, s[cc][q].y);
+        if (colmax) {
+          double mx = live ? fmax(fabs(s[cc][q].x), fabs(s[cc][q].y)) : 0.0;
+          if (live && !(isfinite(s[cc][q].x) && isfinite(s[cc][q].y))) mx = __longlong_as_double(0x7ff0000000000000LL);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+          if (lane == 0 && live)
+            atomicMax(colmax + (nidx / kchunk) * (long)(9 * p.nz) + col, (unsigned long long)__double_as_longlong(mx));
+        }
+      }
+  }
+}
+
+cudaError_t launch_strengths2d(const SynthParams& p, double2* S, cudaStream_t s, unsigned long long* colmax, long kchunk,
+                               double2* amp) {
   if (p.c.n <= 0) return cudaSuccess;
   if (colmax && (kchunk <= 0 || kchunk % 32 != 0)) return cudaErrorInvalidValue;
+  if (amp) {
+    k_reflect2d<<<(unsigned)((p.c.n + 127) / 128), 128, 0, s>>>(p, amp);
+    k_strengths_rows<<<(unsigned)((p.c.n + 31) / 32), 128, 0, s>>>(p, amp, S, colmax, kchunk);
+    return cudaGetLastError();
+  }
   dim3 grid((unsigned)((p.c.n + 127) / 128), (unsigned)((p.nz + SG_Z - 1) / SG_Z));
   k_strengths2d<<<grid, 128, 0, s>>>(p, S, colmax, kchunk);
   return cudaGetLastError();
