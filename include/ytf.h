@@ -280,14 +280,17 @@ int ytf_green_noalloc(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, doubl
  *
  * Item i: tr[i] as for ytf_transfer_batch (rotation is ignored: 2D items take the full (kρ, φ)
  * solve, which the rotation reproduces to rounding) and gr[i] as for ytf_green_batch, where
- * gr[i].cache is ignored (item i synthesises from the cache of tr[i]) and precision must be
- * YTF_PREC_FP64. Limits per item: nz <= 8; 2D: nx*ny <= 64; 1D: at most 32 distinct radii
- * and 13*nz*(distinct radii) <= 2304; 1D nodes real (no deformed contour). The descriptors'
- * host arrays are read again by every ytf_plan_run (their sizes, and for 1D items the
- * pattern of equal radii, are fixed at creation) and gr[i].out receives G at ytf_plan_wait
- * (or, with out_is_device, from the graph itself). Results: the caches equal
- * ytf_transfer_batch's bit for bit; G equals ytf_green_batch's FP64 result to rounding (the
- * node sums run in another order). */
+ * gr[i].cache is ignored (item i synthesises from the cache of tr[i]). Small observation sets
+ * (nz <= 8, 2D nx*ny <= 64 and 9*nz*nx*ny <= 2304, FP64) share one batched synthesis kernel;
+ * other 2D items run closed_form_G's own kernels (any precision) inside the same graph, from
+ * workspaces the plan owns (sized by one eager pass at creation). 1D items must be small
+ * sets: FP64, nz <= 8, at most 32 distinct radii and 13*nz*(distinct radii) <= 2304, real
+ * nodes. The descriptors' host arrays are read again by every ytf_plan_run (their sizes, and
+ * for 1D items the pattern of equal radii, are fixed at creation) and gr[i].out receives G at
+ * ytf_plan_wait (from the graph itself when it is device memory (out_is_device) or page-locked
+ * host memory). Results: the caches equal
+ * ytf_transfer_batch's bit for bit; G equals ytf_green_batch's bit for bit for the large 2D
+ * items and to rounding for the small sets (the node sums run in another order). */
 typedef struct ytf_plan ytf_plan;
 typedef struct {
   int block;             /* threads per CTA of the persistent node-solve kernels: 128 or 256 */

@@ -168,22 +168,66 @@ def test_plan_reads_updated_inputs_and_device_outputs():
 @pytest.mark.gpu
 def test_plan_argument_errors():
     from yellowthinfilms_b200 import api
-    tr, syn = _small_uneven(3)
-    with pytest.raises(api.YTFError, match="FP64"):
-        api.BatchPlan(tr, [dict(s, precision="int8x3") for s in syn])
-    big = dict(syn[1], xs=np.linspace(-1, 1, 9), ys=np.linspace(-1, 1, 9))
-    two = next(i for i, t in enumerate(tr) if "kr_nodes" in t) if any("kr_nodes" in t for t in tr) else None
-    if two is not None:
-        bad = list(syn)
-        bad[two] = dict(big, obs_layer=syn[two]["obs_layer"], zsrc_local=syn[two]["zsrc_local"])
-        with pytest.raises(api.YTFError, match="plan item %d" % two):
-            api.BatchPlan(tr, bad)
+    tr, syn = _small_uneven(12)
+    one = next(i for i, t in enumerate(tr) if "kx_nodes" in t)
+    bad = list(syn)
+    bad[one] = dict(syn[one], precision="int8x3")
+    with pytest.raises(api.YTFError, match="plan item %d" % one):
+        api.BatchPlan(tr, bad)
+    bad = list(syn)
+    bad[one] = dict(syn[one], xs=np.linspace(0.1, 3.0, 9) * 50, ys=np.linspace(0.2, 2.0, 9) * 50)
+    with pytest.raises(api.YTFError, match="distinct radii"):
+        api.BatchPlan(tr, bad)
+    bad = list(syn)
+    bad[one] = dict(syn[one], z_obs=np.linspace(0.1, 0.2, 9) * syn[one]["zsrc_local"])
     with pytest.raises(api.YTFError, match="z rows"):
-        api.BatchPlan(tr, [dict(s, z_obs=np.linspace(0.1, 0.2, 9) * s["zsrc_local"]) for s in syn])
+        api.BatchPlan(tr, bad)
     p = api.BatchPlan(tr, syn)
     with pytest.raises(api.YTFError, match="multiple of 16"):
         p.retune(dict(chunk=100))
-    assert len(p()) == 3  # the plan still runs after a refused retune... with its last graph
+    assert len(p()) == 12  # a refused retune keeps the last graph
+
+
+@pytest.mark.gpu
+def test_plan_large_2d_sets_in_the_graph():
+    """2D items beyond the small-set limits (32x32 pixels, 8 z rows) or in a tensor-core
+    precision run closed_form_G's own kernels inside the plan's graph, from the plan's own
+    workspaces: G equals ytf_green_batch's bit for bit, on pageable, page-locked and device
+    outputs, over
+    repeated runs and after a retune; small items of the same plan keep the batched kernel."""
+    import torch
+    from yellowthinfilms_b200 import api
+    tr, syn = _small_uneven(10)
+    two = [i for i, t in enumerate(tr) if "kr_nodes" in t]
+    assert len(two) >= 3
+    syn = list(syn)
+    xy = np.linspace(-60.0, 60.0, 32)
+    precs = ["int8x3", "fp64", "split_bf16"]
+    outs = {}
+    for k, i in enumerate(two[:3]):
+        zs = syn[i]["zsrc_local"]
+        syn[i] = dict(syn[i], xs=xy, ys=xy, z_obs=np.linspace(0.2, 1.8, 8) * zs, precision=precs[k])
+    dev, pin = two[1], two[0]
+    outs[dev] = torch.zeros(32 * 32 * 8 * 9, dtype=torch.complex128, device="cuda:0")
+    outs[pin] = torch.zeros(32 * 32 * 8 * 9, dtype=torch.complex128, pin_memory=True)  # copied into directly
+    syn[dev] = dict(syn[dev], out=outs[dev])
+    syn[pin] = dict(syn[pin], out=outs[pin])
+    plan = api.BatchPlan(tr, syn)
+    caches = api.build_cavity_transfer_batch([dict(t, rotation=False) for t in tr])
+    ref = api.closed_form_G_batch([dict({k: v for k, v in y.items() if k != "out"}, cache=c) for y, c in zip(syn, caches)])
+    for rep in range(3):
+        if rep == 2:
+            plan.retune(dict(ctas_per_sm=2, tile=512, chunk=1024))
+        G = plan()
+        for i in range(len(tr)):
+            if i in (dev, pin):
+                g = outs[i].cpu().numpy().reshape(3, 3, 8, 32, 32).transpose(4, 3, 2, 1, 0)
+            else:
+                g = G[i]
+            if i in two[:3]:
+                assert np.array_equal(g, ref[i]), (rep, i)
+            else:
+                assert relerr(g, ref[i]) < 1e-12, (rep, i)
 
 
 @pytest.mark.gpu

@@ -565,7 +565,9 @@ class BatchPlan:
     counterpart in the reference, whose callers loop build_cavity_transfer_* and
     closed_form_G per item). ``transfer_items`` as build_cavity_transfer_batch (``rotation``
     is ignored: 2D items take the full (kρ, φ) solve); ``green_items`` as closed_form_G_batch
-    without ``cache`` (item i synthesises from the cache of transfer item i), FP64 only.
+    without ``cache`` (item i synthesises from the cache of transfer item i). Small
+    observation sets share one batched FP64 synthesis kernel; larger 2D sets (or another
+    precision) run closed_form_G's own kernels inside the same graph; 1D items are FP64.
     ``tune``: dict of ytf_tune fields (block, ctas_per_sm, tile, chunk, synth_ctas_per_sm)
     or None for the defaults. Every ``run`` re-reads the node, weight and coordinate arrays
     held by the plan (``inputs(i)`` returns them for in-place updates of the same sizes)."""
@@ -604,8 +606,9 @@ class BatchPlan:
             terms = g.get("terms", "all")
             if terms not in TERMS:
                 raise YTFError(f"closed_form_G: terms must be :all, :direct, :scattered, :toeplitz or :hankel (got :{terms})")
-            if g.get("precision", "fp64") != "fp64":
-                raise YTFError("BatchPlan: the plan's synthesis is FP64 (precision must be 'fp64')")
+            prec = g.get("precision", "fp64")
+            if prec not in PRECISION:
+                raise YTFError(f"closed_form_G: unknown precision {prec!r}")
             zo, x, y = _f64(g["z_obs"]), _f64(g["xs"]), _f64(g["ys"])
             nx, ny, nz = len(x), len(y), len(zo)
             out = g.get("out")
@@ -621,7 +624,7 @@ class BatchPlan:
                 self._outs.append((G, nx, ny, nz))
             e.cache, e.obs_layer, e.zsrc_local = None, int(g["obs_layer"]), float(g["zsrc_local"])
             e.nz, e.z_obs, e.nx, e.xs, e.ny, e.ys = nz, ptr(zo), nx, ptr(x), ny, ptr(y)
-            e.terms, e.precision = TERMS[terms], PRECISION["fp64"]
+            e.terms, e.precision = TERMS[terms], PRECISION[prec]
             self._keep += [k, w, ph, wp, ob, zo, x, y]
             self._inputs.append(dict(k=k, w=w, phi=ph, wphi=wp, z=zo, x=x, y=y))
             self._meta.append((st, is2d, it))

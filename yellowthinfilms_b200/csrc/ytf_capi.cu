@@ -38,7 +38,13 @@ struct ytf_ctx {
   std::map<std::string, long> klaunch;                   // name -> launches
   void* pinned = nullptr;                                // page-locked staging of batched uploads
   size_t pinned_bytes = 0;
+  cudaEvent_t stage_ev = nullptr;                        // last copy out of the staging block
+  // plan recording: the first (eager) pass notes every workspace request's largest size by
+  // name; the captured pass is served from the plan's own buffers of those sizes
+  std::map<std::string, size_t>* ws_record = nullptr;
+  std::map<std::string, std::pair<void*, size_t>>* ws_override = nullptr;
   ~ytf_ctx() {
+    if (stage_ev) cudaEventDestroy(stage_ev);
     if (pinned) cudaFreeHost(pinned);
     for (auto& kv : ws) cudaFree(kv.second.first);
     for (auto& kv : pool) cudaFree(kv.second);
@@ -139,6 +145,18 @@ void ctx_release(ytf_ctx* ctx) {
 void* ws_get(ytf_ctx* ctx, const char* name, size_t bytes, cudaError_t* e) {
   *e = cudaSuccess;
   if (bytes == 0) bytes = 16;
+  if (ctx->ws_override) {
+    auto o = ctx->ws_override->find(name);
+    if (o == ctx->ws_override->end() || o->second.second < bytes) {
+      *e = cudaErrorMemoryAllocation;
+      return nullptr;
+    }
+    return o->second.first;
+  }
+  if (ctx->ws_record) {
+    size_t& r = (*ctx->ws_record)[name];
+    r = std::max(r, bytes);
+  }
   auto it = ctx->ws.find(name);
   if (it != ctx->ws.end() && it->second.second >= bytes) return it->second.first;
   if (it != ctx->ws.end()) {
@@ -905,6 +923,7 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
     if (rc) return abort_all(rc);
   }
   int first = 0;
+  bool staged = false;
   while (first < nb) {
     std::vector<int> items;
     size_t used = 0;
@@ -925,6 +944,9 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
       return q;
     };
     const int m = (int)items.size();
+    // the previous pass's parameter upload reads the same staging bytes: wait for that copy
+    // only (its kernels keep running)
+    if (staged) CK(cudaEventSynchronize(ctx->stage_ev));
     TransferParams* hp = (TransferParams*)h;
     long* offm = (long*)(hp + m);
     long* offs = offm + (m + 1);
@@ -974,6 +996,9 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
     const size_t tot = blk + sizeof(TransferParams) * (nf + ng);
     WS(dpar, char, "tb_params", tot);
     CK(cudaMemcpyAsync(dpar, h, tot, cudaMemcpyHostToDevice, ctx->stream));
+    if (!ctx->stage_ev) CK(cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ctx->stage_ev, ctx->stream));
+    staged = true;
     const TransferParams* dp = (const TransferParams*)dpar;
     const long* doffm = (const long*)(dp + m);
     const long* doffs = doffm + (m + 1);
@@ -990,8 +1015,6 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
       CK(LAUNCH("k_scan", launch_transfer_batch(7, dpf, doffs, nf, offs[nf], ctx->stream)));
     }
     if (ng) CK(LAUNCH("k_chain", launch_transfer_batch(3, dpg, doffg, ng, offg[ng], ctx->stream)));
-    // the staging block is reused by the next pass: let this pass's upload land first
-    if (first < nb) CK(cudaStreamSynchronize(ctx->stream));
   }
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return abort_all(fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e)));
@@ -1507,11 +1530,17 @@ struct ytf_plan {
   std::vector<size_t> rmap_off;
   int* d_rmap = nullptr;
   std::vector<long> g_off;             // host-output items: offset into h_G / d_G (complex); else -1
+  std::vector<char> direct;            // host output page-locked: the graph copies G straight into it
   size_t g_count = 0;
   double2* h_G = nullptr;
   double2* d_G = nullptr;
   std::vector<SynthParams> sps;
   std::vector<long> nout_syn;          // per item: partial outputs per chunk (0: no synthesis)
+  std::vector<char> large;             // 2D items beyond the small-set limits (or not FP64): their
+                                       // synthesis is closed_form_G's own kernels in the graph
+  std::map<std::string, std::pair<void*, size_t>> wsbufs;  // those kernels' workspaces
+  unsigned* d_err = nullptr;           // tensor-core wait-timeout word of those kernels
+  unsigned* h_err = nullptr;
   ytf_tune tune{};
   char* tb = nullptr;
   size_t tb_bytes = 0;
@@ -1553,6 +1582,9 @@ void plan_free(ytf_plan* P) {
   if (P->d_G) cudaFree(P->d_G);
   if (P->h_in) cudaFreeHost(P->h_in);
   if (P->h_G) cudaFreeHost(P->h_G);
+  if (P->d_err) cudaFree(P->d_err);
+  if (P->h_err) cudaFreeHost(P->h_err);
+  for (auto& kv : P->wsbufs) cudaFree(kv.second.first);
   for (auto c : P->cs)
     if (c) ytf_cache_destroy(c);
   delete P;
@@ -1583,6 +1615,45 @@ int plan_fail(ytf_ctx* ctx, int rc, int item) {
   return rc;
 }
 
+// the synthesis of the large 2D items through closed_form_G's own path, on the plan's stream
+// with the coordinates of the device staging, outputs into the plan's buffers: recording the
+// workspace sizes (rec) or from the plan's workspaces (ovr, inside the capture). Profiling is
+// off meanwhile; the launch counts it adds go to the plan's per-run counts (captured pass).
+int plan_large_synthesis(ytf_plan* P, std::map<std::string, size_t>* rec,
+                         std::map<std::string, std::pair<void*, size_t>>* ovr) {
+  ytf_ctx* ctx = P->ctx;
+  const cudaStream_t saved = ctx->stream;
+  const bool prof = ctx->prof;
+  const auto klaunch = ctx->klaunch;
+  ctx->stream = P->cap;
+  ctx->prof = false;
+  ctx->ws_record = rec;
+  ctx->ws_override = ovr;
+  int rc = YTF_OK;
+  for (int i = 0; i < P->nb && !rc; ++i) {
+    if (!P->large[i]) continue;
+    const ytf_green_desc& g = P->gr[i];
+    const double* co = P->d_in + P->in_coord[i];
+    GreenBatch gb{co, co + g.nz, co + g.nz + g.nx, P->d_err};
+    double* out = P->g_off[i] >= 0 ? (double*)(P->d_G + P->g_off[i]) : g.out;
+    rc = green_impl(ctx, P->cs[i], g.obs_layer, g.zsrc_local, g.nz, g.z_obs, g.nx, g.xs, g.ny, g.ys, g.terms,
+                    g.precision, out, 1, &gb);
+    if (rc) rc = plan_fail(ctx, rc, i);
+  }
+  if (ovr)
+    for (auto& kv : ctx->klaunch) {
+      auto it = klaunch.find(kv.first);
+      const long d = kv.second - (it == klaunch.end() ? 0 : it->second);
+      if (d > 0) P->kcount[kv.first] += d;
+    }
+  ctx->klaunch = klaunch;
+  ctx->ws_record = nullptr;
+  ctx->ws_override = nullptr;
+  ctx->stream = saved;
+  ctx->prof = prof;
+  return rc;
+}
+
 // validation, caches, staging, outputs and passes (everything the tiles do not change)
 int plan_build(ytf_plan* P) {
   ytf_ctx* ctx = P->ctx;
@@ -1595,6 +1666,8 @@ int plan_build(ytf_plan* P) {
   P->rmap_off.assign(nb, 0);
   P->g_off.assign(nb, -1);
   P->nout_syn.assign(nb, 0);
+  P->large.assign(nb, 0);
+  P->direct.assign(nb, 0);
   P->in_node.assign(nb, 0);
   P->in_coord.assign(nb, 0);
   size_t rmap_count = 0;
@@ -1610,19 +1683,19 @@ int plan_build(ytf_plan* P) {
     ytf_cache* c = P->cs[i];
     P->nodes += c->n;
     if (g.nz < 0 || g.nx < 0 || g.ny < 0) return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "closed_form_G: negative grid size"), i);
-    if (g.precision != YTF_PREC_FP64)
-      return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: the plan's synthesis is FP64 (precision must be YTF_PREC_FP64)"), i);
-    if (g.nz > SYN_MAXZ)
-      return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: at most " + std::to_string(SYN_MAXZ) + " z rows per item"), i);
+    const long npix0 = (long)g.nx * g.ny;
+    P->large[i] = is2d && (g.precision != YTF_PREC_FP64 || g.nz > SYN_MAXZ || npix0 > SYN_MAXPIX ||
+                           npix0 * 9 * g.nz > SYN_MAXOUT);
+    if (!is2d && g.precision != YTF_PREC_FP64)
+      return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: a plan's 1D synthesis is FP64 (precision must be YTF_PREC_FP64)"), i);
+    if (!is2d && g.nz > SYN_MAXZ)
+      return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: at most " + std::to_string(SYN_MAXZ) + " z rows per 1D item"), i);
     if ((g.nz && !g.z_obs) || (g.nx && !g.xs) || (g.ny && !g.ys) || !g.out)
       return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: NULL coordinate or output array"), i);
     if ((rc = synth_setup(ctx, c, g.obs_layer, g.zsrc_local, g.terms, g.nz, P->sps[i]))) return plan_fail(ctx, rc, i);
     const long npix = (long)g.nx * g.ny;
     if (is2d) {
-      if (npix > SYN_MAXPIX || npix * 9 * g.nz > SYN_MAXOUT)
-        return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: 2D items need nx*ny <= " + std::to_string(SYN_MAXPIX) +
-                                                         " and 9*nz*nx*ny <= " + std::to_string(SYN_MAXOUT)), i);
-      P->nout_syn[i] = npix * 9 * g.nz;
+      P->nout_syn[i] = P->large[i] ? 0 : npix * 9 * g.nz;
     } else {
       std::vector<double> ur;
       radius_map(g.nx, g.ny, g.xs, g.ys, ur, P->rmap[i]);
@@ -1643,10 +1716,18 @@ int plan_build(ytf_plan* P) {
     if (!g.out_is_device && npix * g.nz > 0) {
       P->g_off[i] = (long)P->g_count;
       P->g_count += (size_t)npix * g.nz * 9;
+      cudaPointerAttributes at;
+      if (cudaPointerGetAttributes(&at, g.out) == cudaSuccess && at.type == cudaMemoryTypeHost) P->direct[i] = 1;
+      cudaGetLastError();
     }
   }
   CK(cudaHostAlloc(&P->h_in, 8 * std::max<size_t>(P->in_count, 1), cudaHostAllocDefault));
   CK(cudaMalloc(&P->d_in, 8 * std::max<size_t>(P->in_count, 1)));
+  CK(cudaMemset(P->d_in, 0, 8 * std::max<size_t>(P->in_count, 1)));
+  CK(cudaMalloc(&P->d_err, sizeof(unsigned)));
+  CK(cudaMemset(P->d_err, 0, sizeof(unsigned)));
+  CK(cudaHostAlloc(&P->h_err, sizeof(unsigned), cudaHostAllocDefault));
+  *P->h_err = 0;
   if (P->g_count) {
     CK(cudaHostAlloc(&P->h_G, 16 * P->g_count, cudaHostAllocDefault));
     CK(cudaMalloc(&P->d_G, 16 * P->g_count));
@@ -1742,6 +1823,17 @@ int plan_build(ytf_plan* P) {
   CK(cudaEventCreate(&P->e1));
   CK(synth_small_init());
   CK(cudaStreamSynchronize(ctx->stream));  // cache blocks cleared before the first run
+  // one eager pass of the large items' synthesis (on the zeroed inputs) records the largest
+  // size of each workspace it asks for; the plan then owns buffers of those sizes
+  std::map<std::string, size_t> rec;
+  int rc = plan_large_synthesis(P, &rec, nullptr);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(P->cap));
+  for (auto& kv : rec) {
+    void* b = nullptr;
+    CK(cudaMalloc(&b, kv.second));
+    P->wsbufs[kv.first] = {b, kv.second};
+  }
   return YTF_OK;
 }
 
@@ -1824,7 +1916,7 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
   for (int i = 0; i < nb; ++i) {
     const ytf_green_desc& g = P->gr[i];
     const long npix = (long)g.nx * g.ny;
-    if (npix * g.nz == 0) continue;
+    if (npix * g.nz == 0 || P->large[i]) continue;
     SynthItem it;
     std::memset(&it, 0, sizeof(it));
     it.sp = P->sps[i];
@@ -1879,6 +1971,7 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
   };
   if (P->in_count) step(cudaMemcpyAsync(P->d_in, P->h_in, 8 * P->in_count, cudaMemcpyHostToDevice, s));
   step(cudaMemsetAsync(ctr, 0, 4 * (size_t)ncounter, s));
+  step(cudaMemsetAsync(P->d_err, 0, sizeof(unsigned), s));
   static const char* names[] = {"k_persist_modes", "k_persist_qr", "", "k_persist_chain", "k_persist_match",
                                 "k_persist_seeds", "k_persist_iface", "k_persist_scan"};
   for (auto& L : launches) {
@@ -1904,8 +1997,35 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
     step(launch_synth_finish(di, (int)items.size(), df, foff.back(), s));
     P->kcount["k_synth_finish"] += 1;
   }
-  if (P->g_count) step(cudaMemcpyAsync(P->h_G, P->d_G, 16 * P->g_count, cudaMemcpyDeviceToHost, s));
+  int lrc = YTF_OK;
+  if (e == cudaSuccess) lrc = plan_large_synthesis(P, nullptr, &P->wsbufs);
+  // host outputs: page-locked ones straight from the device buffer, the rest in one copy to
+  // the plan's staging (delivered by ytf_plan_wait)
+  {
+    size_t lo = 0, hi = 0;
+    bool any = false;
+    for (int i = 0; i < nb; ++i) {
+      if (P->g_off[i] < 0) continue;
+      const ytf_green_desc& g = P->gr[i];
+      const size_t cnt = (size_t)g.nx * g.ny * g.nz * 9;
+      if (P->direct[i]) {
+        step(cudaMemcpyAsync(g.out, P->d_G + P->g_off[i], 16 * cnt, cudaMemcpyDeviceToHost, s));
+      } else {
+        if (!any) lo = P->g_off[i];
+        any = true;
+        hi = P->g_off[i] + cnt;
+      }
+    }
+    if (any) step(cudaMemcpyAsync(P->h_G + lo, P->d_G + lo, 16 * (hi - lo), cudaMemcpyDeviceToHost, s));
+  }
+  step(cudaMemcpyAsync(P->h_err, P->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   cudaError_t ee = cudaStreamEndCapture(s, &P->graph);
+  if (lrc) {
+    if (P->graph) cudaGraphDestroy(P->graph);
+    P->graph = nullptr;
+    plan_release_graph(P);
+    return lrc;
+  }
   if (e == cudaSuccess) e = ee;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&P->exec, P->graph, 0);
   if (e != cudaSuccess) {
@@ -1998,8 +2118,9 @@ extern "C" int ytf_plan_wait(ytf_plan* P, float* device_ms) {
   }
   CK(cudaEventSynchronize(P->e1));
   P->pending = false;
+  if (*P->h_err) return fail(ctx, YTF_ERR_CUDA, "ytf_plan_wait: a tensor-core pipeline wait timed out");
   for (int i = 0; i < P->nb; ++i)
-    if (P->g_off[i] >= 0) {
+    if (P->g_off[i] >= 0 && !P->direct[i]) {
       const ytf_green_desc& g = P->gr[i];
       std::memcpy(g.out, P->h_G + P->g_off[i], 16 * (size_t)g.nx * g.ny * g.nz * 9);
     }
