@@ -245,6 +245,26 @@ def test_green_2d_even_rows_match_oracle(ytf, oracle, nz):
                 assert relerr(Gt, oracle.closed_form_G(oc, obs, zs, zo, xs, xs, terms=terms)) < 1e-10, terms
 
 
+@pytest.mark.parametrize("shape", [(8, 6), (1, 5), (33, 2)])
+def test_green_2d_int8_even_pixels_match_oracle(ytf, oracle, shape):
+    """Evenly spaced pixel coordinates (the int8 path's phase tables are then stepped along each
+    row by recurrence): int8x3 and split-BF16 G within 1e-6 of the oracle, like uneven pixels."""
+    _, st = FOUNDATION_STACKS[3]
+    kr, wr = krho_grid(st, W, kmax=12.0, width=1.0)
+    ph, wp = uniform_phi(8)
+    gc = ytf.build_cavity_transfer_2d(st, W, 2, kr, wr, ph, wp, obs_layers=[2])
+    oc = oracle.build_cavity_transfer_2d(st, W, 2, kr, wr, ph, wp, obs_layers=[2])
+    nx, ny = shape
+    xs = np.linspace(-0.4, 0.35, nx) if nx > 1 else np.array([0.15])
+    ys = np.linspace(0.3, -0.25, ny)
+    d = st[1].d
+    zo = [0.2 * d, 0.6 * d]
+    Go = oracle.closed_form_G(oc, 2, 0.4 * d, zo, xs, ys)
+    for prec in ("int8x3", "split_bf16"):
+        G = ytf.closed_form_G(gc, 2, 0.4 * d, zo, xs, ys, precision=prec)
+        assert relerr(G, Go) < 1e-6, (prec, relerr(G, Go))
+
+
 def test_transfer_2d_rotation_fill_matches_oracle(ytf, oracle):
     st = [lay(m_vac, 1.0), lay(m_uni, 0.8), lay(m_gl, 0.5), lay(m_vac, 1.0)]
     kr, wr = krho_grid(st, W, kmax=12.0, width=1.0)

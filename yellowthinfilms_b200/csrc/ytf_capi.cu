@@ -1320,7 +1320,20 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
       lp.n_pad = (long)lp.nchunk * kchunk;
       WS(Px, float2, "g_px", (size_t)lp.n_pad * nx);
       WS(Py, float2, "g_py", (size_t)lp.n_pad * ny);
-      CK(LAUNCH("k_phase_tables", launch_phase_tables_pad(v, nx, ny, dxs, dys, lp.n_pad, Px, Py, ctx->stream)));
+      // evenly spaced x and y (to 4 ulp of the progression): the tables by recurrence
+      double ev[4];
+      bool even = xs && ys && nx >= 1 && ny >= 1;
+      auto spaced = [&](const double* v, int m, double& a0, double& d) {
+        a0 = v[0];
+        d = m > 1 ? (v[m - 1] - v[0]) / (m - 1) : 0.0;
+        const double tol = 4 * 2.220446049250313e-16 * std::max(std::fabs(v[0]), std::fabs(v[m - 1]));
+        bool ok = std::isfinite(d);
+        for (int r = 0; r < m && ok; ++r) ok = std::fabs(v[r] - (v[0] + r * d)) <= tol;
+        return ok;
+      };
+      if (even) even = spaced(xs, nx, ev[0], ev[1]) && spaced(ys, ny, ev[2], ev[3]);
+      CK(LAUNCH("k_phase_tables", launch_phase_tables_pad(v, nx, ny, dxs, dys, lp.n_pad, Px, Py, ctx->stream,
+                                                          even ? ev : nullptr)));
       lp.Px = Px; lp.Py = Py;
       WS(Bq, uint8_t, "g_i8_b", (size_t)lp.ntile * lp.nchunk * (kchunk / 32) * lateral_i8_stage_bytes(lp.Np));
       WS(cmax, unsigned long long, "g_i8_cmax", (size_t)lp.nchunk * ncol);

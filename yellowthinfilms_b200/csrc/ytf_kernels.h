@@ -218,8 +218,10 @@ size_t lateral_i8_stage_bytes(int Np);
 size_t lateral_i8_smem(int Np);
 int lateral_i8_ctile(int ncol);
 cudaError_t launch_lateral_i8(const LateralI8& p, cudaStream_t s);
+// even (optional, host): {x_0, dx, y_0, dy} of evenly spaced pixel coordinates: the tables by
+// recurrence along each row
 cudaError_t launch_phase_tables_pad(const CacheView& c, int nx, int ny, const double* xs, const double* ys, long n_pad,
-                                    float2* Px, float2* Py, cudaStream_t s);
+                                    float2* Px, float2* Py, cudaStream_t s, const double* even = nullptr);
 
 // 1D Bessel synthesis contraction on the int8 tensor cores: P[r][c] = Σ_k J_order(k ρ_r) C[c][k]
 struct BesselI8 {

@@ -63,33 +63,113 @@ int lateral_i8_ctile(int ncol) {
 }
 
 // ------------------------------------------------------------------------------------
-// FP32 phase tables Px[n][i] = e^{i kx_n x_i}, Py[n][j] = e^{i ky_n y_j} (computed in FP64),
-// zero for the padding nodes n <= node < n_pad
+// FP32 phase tables Px[n][i] = e^{i kx_n x_i}, Py[n][j] = e^{i ky_n y_j}, zero for the padding
+// nodes n <= node < n_pad. The arguments are formed and reduced to [-π, π] in FP64 (2π as a
+// double plus its remainder; the FMAs subtract k·2π with one rounding each, so the reduced
+// argument is good to a few FP64 ulp of the argument), then FP32 sincosf of the reduced
+// argument: the FP32 values the int8 digits are made from, within ~1 FP32 ulp. The block's
+// nodes get their cos φ, sin φ once, in shared memory.
 // ------------------------------------------------------------------------------------
-__global__ void k_phase_tables_pad(CacheView c, int nx, int ny, const double* xs, const double* ys, long n_pad,
-                                   float2* Px, float2* Py) {
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_phase_tables_pad(CacheView c, int nx, int ny, const double* xs,
+                                                          const double* ys, long n_pad, float2* Px, float2* Py) {
+  __shared__ double kxs[256], kys[256];
   const int m = nx + ny;
-  if (t >= n_pad * (long)m) return;
-  const long nn = t / m;
-  const int e = (int)(t % m);
+  const long t0 = (long)blockIdx.x * blockDim.x;
+  const long tot = n_pad * (long)m;
+  const long nn0 = tot <= 0x7fffffffL ? (long)((unsigned)t0 / (unsigned)m) : t0 / m;
+  const long last = min(tot, t0 + (long)blockDim.x) - 1;
+  const int nodes = (int)(last / m - nn0 + 1);
+  if ((int)threadIdx.x < nodes) {
+    const long nn = nn0 + threadIdx.x;
+    double kx = 0.0, ky = 0.0;
+    if (nn < c.n) {
+      const long k = nn % c.Nk, q = nn / c.Nk;
+      double s, co;
+      sincos(c.phi[q], &s, &co);
+      kx = c.kr[k] * co;
+      ky = c.kr[k] * s;
+    }
+    kxs[threadIdx.x] = kx;
+    kys[threadIdx.x] = ky;
+  }
+  __syncthreads();
+  const long t = t0 + threadIdx.x;
+  if (t >= tot) return;
+  // 32-bit division when the table fits (a 64-bit one costs tens of instructions)
+  const long nn = tot <= 0x7fffffffL ? (long)((unsigned)t / (unsigned)m) : t / m;
+  const int e = (int)(t - nn * m);
   float2 v = make_float2(0.f, 0.f);
   if (nn < c.n) {
-    const long k = nn % c.Nk, q = nn / c.Nk;
-    double s, co, sn, cs;
-    sincos(c.phi[q], &s, &co);
-    if (e < nx) sincos(c.kr[k] * co * xs[e], &sn, &cs);
-    else sincos(c.kr[k] * s * ys[e - nx], &sn, &cs);
-    v = make_float2((float)cs, (float)sn);
+    const int b = (int)(nn - nn0);
+    const double arg = e < nx ? kxs[b] * xs[e] : kys[b] * ys[e - nx];
+    // arg - 2π rint(arg / 2π), 2π = TWO_PI_HI + TWO_PI_LO
+    const double TWO_PI_HI = 6.28318530717958623200e+00, TWO_PI_LO = 2.44929359829470635445e-16;
+    const double kq = rint(arg * 0.15915494309189533577);
+    const double r = fma(-kq, TWO_PI_LO, fma(-kq, TWO_PI_HI, arg));
+    float sn, cs;
+    sincosf((float)r, &sn, &cs);
+    v = make_float2(cs, sn);
   }
   if (e < nx) Px[nn * nx + e] = v;
   else Py[nn * ny + (e - nx)] = v;
 }
 
+// The same tables when the pixel coordinates are evenly spaced (x_i = x_0 + i dx, y_j = y_0 +
+// j dy): one thread per (node, axis) forms e^{i k x_0} and e^{i k dx} in FP64 and steps along
+// the row, e(x + dx) = e(x) e^{i k dx} (unit-modulus factors: a few FP64 ulp after a row of
+// 64, far below the FP32 rounding of the stored value); rows go through shared memory so the
+// stores are coalesced.
+__global__ void __launch_bounds__(128) k_phase_tables_even(CacheView c, int nx, int ny, double x0, double dx, double y0,
+                                                           double dy, long n_pad, float2* Px, float2* Py) {
+  // 64 nodes per block: threads 0-63 step their node's x row, 64-127 its y row, into shared
+  // memory (32 entries of each row per pass), then the block writes them coalesced
+  __shared__ float2 rows[2][64][33];
+  const long nb0 = (long)blockIdx.x * 64;
+  const int tid = threadIdx.x, ax = tid >> 6, r = tid & 63;
+  const int cnt = ax ? ny : nx;
+  const long nn = nb0 + r;
+  double er = 0.0, ei = 0.0, cd_ = 1.0, sd = 0.0;
+  if (nn < c.n) {
+    const long k = nn % c.Nk, q = nn / c.Nk;
+    double sp, cp;
+    sincos(c.phi[q], &sp, &cp);
+    const double kk = c.kr[k] * (ax ? sp : cp);
+    sincos(kk * (ax ? y0 : x0), &ei, &er);
+    sincos(kk * (ax ? dy : dx), &sd, &cd_);
+  }
+  const long nrows = min(64L, n_pad - nb0);
+  for (int base = 0; base < max(nx, ny); base += 32) {
+    const int m = min(32, cnt - base);
+    for (int i = 0; i < m; ++i) {
+      rows[ax][r][i] = nn < c.n ? make_float2((float)er, (float)ei) : make_float2(0.f, 0.f);
+      const double nr = er * cd_ - ei * sd, ni = er * sd + ei * cd_;
+      er = nr;
+      ei = ni;
+    }
+    __syncthreads();
+    for (int a = 0; a < 2; ++a) {
+      const int ca = a ? ny : nx;
+      const int ma = min(32, ca - base);
+      if (ma <= 0) continue;
+      float2* out = a ? Py : Px;
+      for (int e = tid; e < nrows * ma; e += 128) {
+        const int rr = e / ma, i = e - rr * ma;
+        out[(nb0 + rr) * ca + base + i] = rows[a][rr][i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 cudaError_t launch_phase_tables_pad(const CacheView& c, int nx, int ny, const double* xs, const double* ys, long n_pad,
-                                    float2* Px, float2* Py, cudaStream_t s) {
+                                    float2* Px, float2* Py, cudaStream_t s, const double* even) {
   long tot = n_pad * (long)(nx + ny);
   if (tot <= 0) return cudaSuccess;
+  if (even) {
+    k_phase_tables_even<<<(unsigned)((n_pad + 63) / 64), 128, 0, s>>>(c, nx, ny, even[0], even[1], even[2], even[3],
+                                                                     n_pad, Px, Py);
+    return cudaGetLastError();
+  }
   k_phase_tables_pad<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(c, nx, ny, xs, ys, n_pad, Px, Py);
   return cudaGetLastError();
 }
