@@ -581,58 +581,48 @@ def run_learned(args):
         torch.cuda.synchronize()
         return r, a.elapsed_time(b) * 1e-3
 
-    res = {}
-    for rw in (0.2, 5.0):
-        res[rw] = dict(entries=0, t_plain=0.0, t_learned=0.0, n_plain=[], n_learned=[], accepted=0, err=0.0)
+    # held-out problems: every stack at a near-field and a 5 λ observation set; the G
+    # evaluations of both methods are batched over all problems of a regime
+    ctx = api.Context(0)
+    stacks = []
     for _ in range(n_test):
         st, lam = L.film_stack(rng)
-        k0 = 2 * np.pi / lam
-        for rw in (0.2, 5.0):
-            rho = np.exp(np.linspace(np.log(0.01 * lam), np.log(rw * lam), 16))
-            z = np.linspace(60.0, 200.0, 6)
-
-            def G(k, w):
-                c = api.build_cavity_transfer_1d(st, k0, 1, k, w, obs_layers=[1])
-                return api.closed_form_G(c, 1, 20.0, z, rho, [0.0], terms="scattered")
-            kr, wr, ir = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rw * lam, rtol=1e-10)
-            Gref = G(*L.halved(st, k0, ir["panels"], 8))
-
-            def plain():
-                k, w, info = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rw * lam, scan=False)
-                panels = info["panels"]
-                sing = sorted(set(api.layer_light_lines(st[0], k0)) | set(api.layer_light_lines(st[-1], k0)))
-                Gk = G(k, w)
-                for _ in range(8):
-                    panels = api.halve_panels([tuple(p) for p in panels])
-                    kh, wh = api.gl_rule(panels, 8, singular=sing)
-                    Gh = G(kh, wh)
-                    if np.linalg.norm(Gk - Gh) <= 1e-6 * np.linalg.norm(Gh):
-                        return Gk, len(k)
-                    k, w, Gk = kh, wh, Gh
-                return Gk, len(k)
-
-            def learned():
-                k, w, info = L.learned_rule(net, st, k0, 1, h_min=80.0, rho_max=rw * lam, check=G)
-                return info["G"], len(k), info["learned"]
-
-            (Gp, npl), tp = timed(plain)
-            (Gl, nle, acc), tl = timed(learned)
-            r = res[rw]
-            r["entries"] += Gref.size
-            r["t_plain"] += tp
-            r["t_learned"] += tl
-            r["n_plain"].append(npl)
-            r["n_learned"].append(nle)
-            r["accepted"] += int(acc)
-            r["err"] = max(r["err"], float(np.linalg.norm(Gl - Gref) / np.linalg.norm(Gref)),
-                           float(np.linalg.norm(Gp - Gref) / np.linalg.norm(Gref)))
+        stacks.append((st, lam, api.Stack(st, ctx)))
+    res = {}
+    for rw in (0.2, 5.0):
+        probs = []
+        for st, lam, sto in stacks:
+            probs.append(dict(stack=sto, layers=st, k0=2 * np.pi / lam, source_layer=1, zsrc_local=20.0,
+                              z=np.linspace(60.0, 200.0, 6), rho=np.exp(np.linspace(np.log(0.01 * lam), np.log(rw * lam), 16)),
+                              terms="scattered", h_min=80.0, rho_max=rw * lam))
+        # converged references: the scanned rule at rtol 1e-10, halved (untimed)
+        refs = []
+        for P in probs:
+            kr, wr, ir = api.point_kx_grid(P["stack"], P["k0"], 1, h_min=80.0, rho_max=P["rho_max"], rtol=1e-10, ctx=ctx)
+            refs.append(L.halved(P["layers"], P["k0"], ir["panels"], 8))
+        Gref = L.batch_G(probs, refs, ctx=ctx)
+        L.plain_rules_batch(probs, ctx=ctx)  # warm-up of both paths
+        L.learned_rules_batch(net, probs, ctx=ctx)
+        outp, tp = timed(lambda: L.plain_rules_batch(probs, ctx=ctx))
+        outl, tl = timed(lambda: L.learned_rules_batch(net, probs, ctx=ctx))
+        err = 0.0
+        for (gp, kp, _, _, _), (gl, kl, _, _, _), gr in zip(outp, outl, Gref):
+            nr = np.linalg.norm(gr)
+            err = max(err, float(np.linalg.norm(gp - gr) / nr), float(np.linalg.norm(gl - gr) / nr))
+        res[rw] = dict(entries=sum(g.size for g in Gref), t_plain=tp, t_learned=tl,
+                       n_plain=[len(o[1]) for o in outp], n_learned=[len(o[1]) for o in outl],
+                       accepted=sum(int(o[3]) for o in outl), err=err,
+                       halvings_plain=float(np.mean([o[3] for o in outp])),
+                       halvings_learned=float(np.mean([o[4] for o in outl])))
     near = res[0.2]
     line = {"metric": METRIC, "value": near["entries"] / near["t_learned"], "unit": "entries/s", "n_gpus": 1,
             "steps": n_test, "warmup": 0, "ms_per_step": 1e3 * near["t_learned"] / n_test, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve and synthesis; MLP bf16 weights, fp32 accum",
             "data": "synthetic (seeded)", "impl": "learned-adaptive",
             "config": {"workload": "learned adaptive quadrature: air / uniaxial film / substrate stacks, vertical dipole "
-                                   "20 nm above the film, 16 ρ x 6 heights (60-200 nm) x 9 components, scattered term",
+                                   "20 nm above the film, 16 ρ x 6 heights (60-200 nm) x 9 components, scattered term; "
+                                   "each method's G evaluations batched over the held-out stacks (one batched build "
+                                   "and synthesis per refinement level)",
                        "train_samples": n_train * n_k, "train_steps": steps, "batch": batch, "held_out_stacks": n_test,
                        "tolerance": 1e-6},
             "plain_entries_per_s": near["entries"] / near["t_plain"],
@@ -643,6 +633,8 @@ def run_learned(args):
                                                 "learned_vs_plain": r["t_plain"] / r["t_learned"],
                                                 "mean_nodes_learned": float(np.mean(r["n_learned"])),
                                                 "mean_nodes_plain": float(np.mean(r["n_plain"])),
+                                                "mean_halvings_plain": r["halvings_plain"],
+                                                "mean_refinements_learned": r["halvings_learned"],
                                                 "accepted": r["accepted"], "stacks": n_test}
                         for rw, r in res.items()},
             "training": {"data_s": t_data, "train_s": t_train, "first_loss": float(losses[0]),

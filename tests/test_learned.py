@@ -157,3 +157,35 @@ def test_untrained_network_falls_back_to_the_plain_method(L):
     assert np.linalg.norm(info["G"] - Gref) <= 2e-6 * np.linalg.norm(Gref)
     if not info["learned"]:
         assert info["halvings"] >= 1
+
+
+def test_batched_rules_equal_per_stack_rules(L):
+    """learned_rules_batch and plain_rules_batch (G evaluations batched over problems) give,
+    problem by problem, the rules and G of learned_rule and of the per-stack plain halving,
+    bit for bit (batched builds and syntheses equal single ones bit for bit)."""
+    from yellowthinfilms_b200 import api
+    net = _random_net(L, 7)
+    rng = np.random.default_rng(31)
+    probs = []
+    for _ in range(3):
+        st, lam = L.film_stack(rng)
+        k0 = 2 * np.pi / lam
+        for rw in (0.2, 5.0):
+            probs.append(dict(stack=api.Stack(st), layers=st, k0=k0, source_layer=1, zsrc_local=20.0,
+                              z=np.linspace(60.0, 200.0, 6), rho=np.exp(np.linspace(np.log(0.01 * lam), np.log(rw * lam), 16)),
+                              terms="scattered", h_min=80.0, rho_max=rw * lam))
+    outl = L.learned_rules_batch(net, probs)
+    outp = L.plain_rules_batch(probs)
+    for P, (gl, kl, wl, acc, h), (gp, kp, wp, hp, conv) in zip(probs, outl, outp):
+        def G(k, w):
+            c = api.build_cavity_transfer_1d(P["stack"], P["k0"], 1, k, w, obs_layers=[1])
+            return api.closed_form_G(c, 1, 20.0, P["z"], P["rho"], [0.0], terms="scattered")
+        k, w, info = L.learned_rule(net, P["stack"], P["k0"], 1, h_min=80.0, rho_max=P["rho_max"], check=G)
+        assert np.array_equal(k, kl) and np.array_equal(info["G"], gl) and bool(info["learned"]) == bool(acc)
+        k2, w2, inf2 = api.point_kx_grid(P["stack"], P["k0"], 1, h_min=80.0, rho_max=P["rho_max"], scan=False)
+        panels, Gk = inf2["panels"], G(k2, w2)
+        for _ in range(hp):
+            panels = api.halve_panels([tuple(p) for p in panels])
+            k2, w2 = api.gl_rule(panels, 8, singular=L._sing(P))
+            Gk = G(k2, w2)
+        assert np.array_equal(k2, kp) and np.array_equal(Gk, gp)

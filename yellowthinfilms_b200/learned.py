@@ -61,9 +61,10 @@ def features(stack, k0, ks):
         row[19 * l + 9:19 * l + 18] = eps[l].imag / 10.0
         row[19 * l + 18] = d[l] * k0 / (2 * np.pi)
     row[-2] = k0 * LAMBDA_REF / (2 * np.pi)
-    X = np.repeat(row[None, :], len(ks), axis=0)
-    X[:, -1] = np.asarray(ks) / (K_HI * k0)
-    return X.astype(np.float32)
+    X = np.empty((len(ks), N_FEATURES), np.float32)
+    X[:] = row.astype(np.float32)
+    X[:, -1] = (np.asarray(ks) / (K_HI * k0)).astype(np.float32)
+    return X
 
 
 def peaks(ks, logR, prominence=np.log(1.05), floor_rel=1e-6):
@@ -79,9 +80,10 @@ def peaks(ks, logR, prominence=np.log(1.05), floor_rel=1e-6):
     step = lk[1] - lk[0]
     W = int(np.ceil(np.log(4.0) / step))
     out = []
-    for i in range(1, n - 1):
-        if not (y[i] > y[i - 1] and y[i] >= y[i + 1] and y[i] >= ymin):
-            continue
+    # local maxima above the floor (vectorised), then each candidate in order
+    cand = np.nonzero((y[1:-1] > y[:-2]) & (y[1:-1] >= y[2:]) & (y[1:-1] >= ymin))[0] + 1
+    for i in cand:
+        i = int(i)
         lo, hi = max(0, i - W), min(n - 1, i + W)
         jl = i
         while jl > lo and y[jl - 1] <= y[i]:
@@ -150,18 +152,25 @@ def train(net, X, T, steps, batch=4096, lr=1e-3, seed=1):
     return losses
 
 
+def _score_candidates(ks, logit, cand):
+    """cand plus the local maxima of the pole score σ(logit) above 0.3 that lie more than 2Γ
+    from every candidate so far (in increasing k), each with Γ = 2e-3 k."""
+    sc = 1.0 / (1.0 + np.exp(-np.asarray(logit, np.float64)))
+    idx = np.nonzero((sc[1:-1] > 0.3) & (sc[1:-1] >= sc[:-2]) & (sc[1:-1] > sc[2:]))[0] + 1
+    cand = list(cand)
+    for i in idx:
+        if all(abs(ks[i] - q) > 2 * G for q, G in cand):
+            cand.append((float(ks[i]), float(ks[i] * 2e-3)))
+    return cand
+
+
 def propose_poles(net, stack, k0, n_k=4096):
     """Candidate real-axis poles (q, Γ) from the network: peaks of its predicted response and
     maxima of its pole score (> 0.3) on a fine log grid."""
     ks = scan_grid(k0, n_k)
     out = net.forward(features(stack, k0, ks)).astype(np.float64)
     cand = peaks(ks, out[:, 0] * LOG_SCALE)
-    s = 1.0 / (1.0 + np.exp(-out[:, 1]))
-    for i in range(1, len(ks) - 1):
-        if s[i] > 0.3 and s[i] >= s[i - 1] and s[i] > s[i + 1]:
-            if all(abs(ks[i] - q) > 2 * G for q, G in cand):
-                cand.append((float(ks[i]), float(ks[i] * 2e-3)))
-    return sorted(cand)
+    return sorted(_score_candidates(ks, out[:, 1], cand))
 
 
 def refine_poles(stack, k0, source_layer, cand, n_local=129, ctx=None):
@@ -230,6 +239,105 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
                                     ctx=ctx)
     info.update(info2, learned=False, halvings=max_halvings + 1, G=check(k, w))
     return k, w, info
+
+
+# ------------------------------------------------------------------------------------
+# Batched forms: many problems (stack, k0, observation set) at once. Rules are built per
+# problem; every G evaluation of a refinement level is ONE batched build and ONE batched
+# synthesis over the problems still open (ytf_transfer_batch + ytf_green_batch), so the
+# time follows the nodes solved rather than per-call latency.
+# ------------------------------------------------------------------------------------
+def batch_G(problems, rules, ctx=None):
+    """G on each problem's rule: problems are dicts with stack (api.Stack or layers), k0,
+    source_layer, zsrc_local, z (rows), rho (radii, on the x axis), terms; rules (k, w)."""
+    if not problems:
+        return []
+    caches = api.build_cavity_transfer_batch(
+        [dict(stack=P["stack"], omega=P["k0"], source_layer=P["source_layer"], kx_nodes=k, wt_nodes=w,
+              obs_layers=[P["source_layer"]]) for P, (k, w) in zip(problems, rules)], ctx=ctx)
+    return api.closed_form_G_batch(
+        [dict(cache=c, obs_layer=P["source_layer"], zsrc_local=P["zsrc_local"], z_obs=P["z"], xs=P["rho"],
+              ys=[0.0], terms=P.get("terms", "all")) for P, c in zip(problems, caches)])
+
+
+def _sing(P):
+    st = P["layers"]
+    return sorted(set(api.layer_light_lines(st[0], P["k0"])) | set(api.layer_light_lines(st[-1], P["k0"])))
+
+
+def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, ctx, out):
+    """Halve the open problems' rules until G agrees with G on the halved rule (the plain
+    method's own check), all open problems per batched level; fills out[i] = (G, k, w,
+    halvings, converged)."""
+    open_ = list(idx)
+    for h in range(max_halvings + 1):
+        if not open_:
+            break
+        halv = {}
+        for i in open_:
+            p2 = api.halve_panels([tuple(p) for p in panels[i]])
+            halv[i] = (p2, api.gl_rule(p2, order, singular=_sing(problems[i]), ctx=ctx))
+        Gh = batch_G([problems[i] for i in open_], [halv[i][1] for i in open_], ctx=ctx)
+        still = []
+        for i, g in zip(open_, Gh):
+            if np.linalg.norm(G[i] - g) <= rtol * np.linalg.norm(g):
+                out[i] = (G[i], rules[i][0], rules[i][1], h, True)
+            else:
+                panels[i], rules[i], G[i] = halv[i][0], halv[i][1], g
+                still.append(i)
+        open_ = still
+    for i in open_:
+        out[i] = (G[i], rules[i][0], rules[i][1], max_halvings + 1, False)
+
+
+def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None):
+    """The plain fixed rule (no pole knowledge: light-line breaks, u² substitution) of every
+    problem, halved until two levels agree. Returns [(G, k, w, halvings, converged)]."""
+    rules, panels = [], []
+    for P in problems:
+        k, w, info = api.point_kx_grid(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
+                                       rho_max=P["rho_max"], scan=False, order=order, ctx=ctx)
+        rules.append((k, w))
+        panels.append(info["panels"])
+    G = batch_G(problems, rules, ctx=ctx)
+    out = [None] * len(problems)
+    _refine_levels(problems, range(len(problems)), rules, panels, G, rtol, max_halvings, order, ctx, out)
+    return out
+
+
+def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=None):
+    """learned_rule for every problem: one network forward over all problems' scan grids,
+    the exact window sampling and fixed_kρ_rule per problem, then the acceptance check and any
+    plain refinement in batched levels; a problem that never converges falls back to the
+    scanned rule. Returns [(G, k, w, accepted, halvings)]."""
+    n_k = 4096
+    feats = [features(P["layers"], P["k0"], scan_grid(P["k0"], n_k)) for P in problems]
+    pred = net.forward(np.concatenate(feats)).astype(np.float64) if problems else np.zeros((0, 2))
+    rules, panels = [], []
+    for j, P in enumerate(problems):
+        ks = scan_grid(P["k0"], n_k)
+        o = pred[j * n_k:(j + 1) * n_k]
+        cand = _score_candidates(ks, o[:, 1], peaks(ks, o[:, 0] * LOG_SCALE))
+        poles = refine_poles(P["stack"], P["k0"], P["source_layer"], sorted(cand), ctx=ctx)
+        k, w, info = api.grid_from_poles(P["stack"], P["k0"], P["source_layer"], poles, h_min=P["h_min"],
+                                         rho_max=P["rho_max"], order=order, rtol=rtol, ctx=ctx)
+        rules.append((k, w))
+        panels.append(info["panels"])
+    G = batch_G(problems, rules, ctx=ctx)
+    out = [None] * len(problems)
+    _refine_levels(problems, range(len(problems)), rules, panels, G, rtol, max_halvings, order, ctx, out)
+    fall = [i for i, r in enumerate(out) if not r[4]]
+    if fall:
+        fr = []
+        for i in fall:
+            P = problems[i]
+            k, w, _ = api.point_kx_grid(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
+                                        rho_max=P["rho_max"], order=order, rtol=rtol, ctx=ctx)
+            fr.append((k, w))
+        Gf = batch_G([problems[i] for i in fall], fr, ctx=ctx)
+        for i, (k, w), g in zip(fall, fr, Gf):
+            out[i] = (g, k, w, out[i][3], False)
+    return [(g, k, w, conv and h == 0, h) for (g, k, w, h, conv) in out]
 
 
 def uniform_rule(k0, kmax, npanels, order=8):
