@@ -336,10 +336,9 @@ void fill_params(TransferParams& p, const ytf_stack* st, const ytf_cache* c) {
 
 // the forward-only chain (every observation layer is the source layer)
 int launch_forward_chain(ytf_ctx* ctx, const TransferParams& p) {
-  CK(LAUNCH("k_match", launch_chain_part(0, p, ctx->stream)));
+  CK(LAUNCH("k_iface", launch_chain_part(0, p, ctx->stream)));
   CK(LAUNCH("k_seeds", launch_chain_part(1, p, ctx->stream)));
-  CK(LAUNCH("k_iface", launch_chain_part(2, p, ctx->stream)));
-  CK(LAUNCH("k_scan", launch_chain_part(3, p, ctx->stream)));
+  CK(LAUNCH("k_scan", launch_chain_part(2, p, ctx->stream)));
   return YTF_OK;
 }
 
@@ -361,7 +360,7 @@ int run_transfer(ytf_ctx* ctx, TransferParams p, long total) {
   WS(modes, double2, "tr_modes", (size_t)N * 20 * chunk);
   WS(lstat, uint8_t, "tr_lstat", (size_t)N * chunk);
   WS(sint, double2, "tr_sint", (size_t)std::max(N - 1, 1) * 16 * chunk);
-  WS(swaps, uint64_t, "tr_swaps", (size_t)chunk);
+  WS(dec, uint8_t, "tr_dec", (size_t)std::max(N - 1, 1) * chunk);
   double2* sleft = nullptr;
   double2* sright = nullptr;
   if (p.needL) { WS(sl, double2, "tr_sleft", (size_t)N * 16 * chunk); sleft = sl; }
@@ -369,7 +368,7 @@ int run_transfer(ytf_ctx* ctx, TransferParams p, long total) {
   p.modes = modes;
   p.lstat = lstat;
   p.sint = sint;
-  p.swaps = swaps;
+  p.dec = dec;
   p.sleft = sleft;
   p.sright = sright;
   for (long off = 0; off < total; off += chunk) {
@@ -593,8 +592,8 @@ int solve_rotation(ytf_ctx* ctx, const ytf_stack* st, ytf_cache* c, const Transf
   b.modes = modes;
   b.lstat = lstat;
   b.sint = sint;
-  WS(bsw, uint64_t, "tr_swaps", (size_t)nb);
-  b.swaps = bsw;
+  WS(bdec, uint8_t, "tr_dec", (size_t)std::max(N - 1, 1) * nb);
+  b.dec = bdec;
   if (b.needL) { WS(sl, double2, "tr_sleft", (size_t)N * 16 * nb); b.sleft = sl; }
   if (b.needR) { WS(sr, double2, "tr_sright", (size_t)N * 16 * nb); b.sright = sr; }
   b.status = bstat;
@@ -889,7 +888,7 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
     const int N = ps[i].nL;
     const bool fast = only_source_observed(ps[i]);
     size_t per = (size_t)N * 20 * 16 + (size_t)N;
-    if (fast) per += (size_t)std::max(N - 1, 1) * 16 * 16 + 8;
+    if (fast) per += (size_t)std::max(N - 1, 1) * (16 * 16 + 1);
     if (!fast) per = scratch_per_node(N, ps[i].needL, ps[i].needR);
     scratch[i] = per * (size_t)cs[i]->n + 5 * 256;
   }
@@ -962,7 +961,7 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
       q.lstat = (uint8_t*)carve((size_t)N * n);
       if (only_source_observed(q)) {
         q.sint = (double2*)carve((size_t)std::max(N - 1, 1) * 16 * 16 * n);
-        q.swaps = (uint64_t*)carve((size_t)8 * n);
+        q.dec = (uint8_t*)carve((size_t)std::max(N - 1, 1) * n);
         fast_ids.push_back(j);
       } else {
         q.sint = (double2*)carve((size_t)std::max(N - 1, 1) * 16 * 16 * n);
@@ -1009,9 +1008,8 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
     CK(LAUNCH("k_layer_modes", launch_transfer_batch(0, dp, doffm, m, offm[m], ctx->stream)));
     CK(LAUNCH("k_layer_modes_qr", launch_transfer_batch(1, dp, doffm, m, offm[m], ctx->stream)));
     if (nf) {
-      CK(LAUNCH("k_match", launch_transfer_batch(4, dpf, doffs, nf, offs[nf], ctx->stream)));
-      CK(LAUNCH("k_seeds", launch_transfer_batch(5, dpf, doffs, nf, offs[nf], ctx->stream)));
       if (offi[nf]) CK(LAUNCH("k_iface", launch_transfer_batch(6, dpf, doffi, nf, offi[nf], ctx->stream)));
+      CK(LAUNCH("k_seeds", launch_transfer_batch(5, dpf, doffs, nf, offs[nf], ctx->stream)));
       CK(LAUNCH("k_scan", launch_transfer_batch(7, dpf, doffs, nf, offs[nf], ctx->stream)));
     }
     if (ng) CK(LAUNCH("k_chain", launch_transfer_batch(3, dpg, doffg, ng, offg[ng], ctx->stream)));
@@ -1785,7 +1783,7 @@ int plan_build(ytf_plan* P) {
     const long n = q.n;
     auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
     size_t b = r256((size_t)N * 20 * 16 * n) + r256((size_t)N * n) + r256((size_t)std::max(N - 1, 1) * 16 * 16 * n);
-    if (only_source_observed(q)) b += r256((size_t)8 * n);
+    if (only_source_observed(q)) b += r256((size_t)std::max(N - 1, 1) * n);
     else b += (q.needL ? r256((size_t)N * 16 * 16 * n) : 0) + (q.needR ? r256((size_t)N * 16 * 16 * n) : 0);
     need[i] = b;
   }
@@ -1824,7 +1822,7 @@ int plan_build(ytf_plan* P) {
       q.lstat = (uint8_t*)carve((size_t)N * n);
       q.sint = (double2*)carve((size_t)std::max(N - 1, 1) * 16 * 16 * n);
       if (only_source_observed(q)) {
-        q.swaps = (uint64_t*)carve((size_t)8 * n);
+        q.dec = (uint8_t*)carve((size_t)std::max(N - 1, 1) * n);
       } else {
         q.sleft = q.needL ? (double2*)carve((size_t)N * 16 * 16 * n) : nullptr;
         q.sright = q.needR ? (double2*)carve((size_t)N * 16 * 16 * n) : nullptr;
@@ -1891,7 +1889,7 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
     std::vector<TransferParams> pp;
     for (int i : pass) pp.push_back(P->ps[i]);
     const size_t po = put(pp.data(), sizeof(TransferParams) * pp.size());
-    const int stages[] = {0, 1, 4, 5, 6, 7, 3};
+    const int stages[] = {0, 1, 6, 5, 7, 3};
     for (int st : stages) {
       std::vector<int> prob;
       std::vector<long> a, b;
@@ -1985,7 +1983,7 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
   if (P->in_count) step(cudaMemcpyAsync(P->d_in, P->h_in, 8 * P->in_count, cudaMemcpyHostToDevice, s));
   step(cudaMemsetAsync(ctr, 0, 4 * (size_t)ncounter, s));
   step(cudaMemsetAsync(P->d_err, 0, sizeof(unsigned), s));
-  static const char* names[] = {"k_persist_modes", "k_persist_qr", "", "k_persist_chain", "k_persist_match",
+  static const char* names[] = {"k_persist_modes", "k_persist_qr", "", "k_persist_chain", "",
                                 "k_persist_seeds", "k_persist_iface", "k_persist_scan"};
   for (auto& L : launches) {
     TileQueue q;

@@ -46,7 +46,7 @@ struct TransferParams {
   double2* sint;           // [nL-1][16][n]
   double2* sleft;          // [nL][16][n]
   double2* sright;         // [nL][16][n]
-  uint64_t* swaps;         // [n] matching swaps per node, 2 bits per layer (split forward-only chain)
+  uint8_t* dec;            // [nL-1][n] matching decisions per interface (forward-only chain)
   // outputs
   uint8_t* status;         // [nout] (rotation base: [n])
   uint8_t* valid;          // [nout]
@@ -65,12 +65,12 @@ struct TransferParams {
 cudaError_t launch_layer_modes(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_layer_modes_qr(const TransferParams& p, cudaStream_t stream);
 cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream);
-// k_chain when every observation layer is the source layer, as four kernels: part 0..3 =
-// k_match, k_seeds, k_iface, k_scan, launched in that order (needs the sint and swaps scratch)
+// k_chain when every observation layer is the source layer, as three kernels: part 0..2 =
+// k_iface, k_seeds, k_scan, launched in that order (needs the sint and dec scratch)
 cudaError_t launch_chain_part(int part, const TransferParams& p, cudaStream_t stream);
 // batched transfer kernels over nb problems (device arrays probs[nb], off[nb + 1]; total =
-// off[nb]): kernel 0 = layer modes, 1 = general QR pass, 3 = chain, 4-7 = the forward-only
-// chain (match, seeds, iface (off over (nL - 1) n interface-node pairs), scan)
+// off[nb]): kernel 0 = layer modes, 1 = general QR pass, 3 = chain, 5-7 = the forward-only
+// chain (seeds, iface (off over (nL - 1) n interface-node pairs), scan; iface first)
 cudaError_t launch_transfer_batch(int kernel, const TransferParams* probs, const long* off, int nb, long total,
                                   cudaStream_t stream);
 cudaError_t launch_rotate_fill(const TransferParams& p, const uint8_t* base_status, const uint8_t* base_tvalid,
@@ -84,8 +84,8 @@ struct TileQueue {
   int ntiles;
   unsigned* counter;  // next tile; zero before the launch
 };
-// stage: 0 modes, 1 QR pass, 3 general chain, 4 match, 5 seeds, 6 iface, 7 scan (units as the
-// batched kernels); block 128 or 256 threads; grid CTAs (persistent)
+// stage: 0 modes, 1 QR pass, 3 general chain, 6 iface, 5 seeds, 7 scan (units as the batched
+// kernels, iface before seeds); block 128 or 256 threads; grid CTAs (persistent)
 cudaError_t launch_persist(int stage, int block, int grid, const TransferParams* probs, const TileQueue& q,
                            cudaStream_t s);
 

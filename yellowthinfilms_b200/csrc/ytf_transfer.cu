@@ -944,18 +944,21 @@ __device__ __forceinline__ void chain_body(const TransferParams& p, long node) {
 // a forward sweep (left to right) instead of a backward scan: N-1 star products instead of
 // N-1 + (N-src), and no SLeft, SRight or matched-mode records. One S4 register set serves as
 // the SLeft prefix up to the source layer and as the SRight product after it. The solve runs
-// as four kernels with short code, so that more warps stay resident than in one fused
+// as three kernels with short code, so that more warps stay resident than in one fused
 // kernel (255 registers with spills):
-//   k_match  (per node)             mode matching down the stack -> a 64-bit swap mask
-//   k_seeds  (per node)             source projection and mode basis of the source layer
-//   k_iface  (per node, interface)  the interface matrix (4x4 LU); past the source layer the
-//                                   propagation of the layer on its left folded in:
-//                                   X_j = diag(e^{iQf d}, e^{-iQb d}) ⋆ Sint_j
-//   k_scan   (per node)             acc = acc ⋆ X_j over the interfaces, cavity, T^o
-// The interface matrices live in the `sint` scratch, the swap masks in `swaps`; the LU
-// failures and the projection's status travel in the layer status bytes, which k_scan reads
-// and translates. The mode vectors are read from the read-only mode records with the
-// matching swaps applied.
+//   k_iface  (per node, interface)  the interface matrix (4x4 LU) of the two layers' RAW mode
+//                                   columns and the two matching decisions (match_decision);
+//                                   past the source layer the propagation of the layer on its
+//                                   left folded in: X_j = diag(e^{iQf d}, e^{-iQb d}) ⋆ Sint_j
+//   k_seeds  (per node)             the swap mask up to the source layer from the decisions,
+//                                   source projection and mode basis of the source layer
+//   k_scan   (per node)             the swap mask of the stack, then acc = acc ⋆ X_j over the
+//                                   interfaces (each X_j relabelled to the matched columns),
+//                                   cavity, T^o
+// Relabelling is exact; only the LU's pivot order differs from a solve on matched columns.
+// The interface matrices live in the `sint` scratch, the decisions in `dec`; the LU failures
+// and the projection's status travel in the layer status bytes, which k_scan reads and
+// translates.
 // ------------------------------------------------------------------------------------
 // largest singular value of a 2x2 complex matrix: √ of the larger eigenvalue of A^H A
 __device__ __forceinline__ double sigma_max2(const M2& A) {
@@ -998,8 +1001,13 @@ __device__ __forceinline__ void load_matched(const TransferParams& p, int layer,
     for (int m = 0; m < 2; ++m) { M.vf[i][m] = v.vf[i][m]; M.vb[i][m] = v.vb[i][m]; }
   load_q(p, layer, node, swaps, M.qf, M.qb);
 }
-// _match_modes (mod_ModeSolver.jl:333-349) for one direction: true if b's columns swap
-__device__ __forceinline__ bool match_swap(const cd va[4][2], const cd vb[4][2]) {
+// _match_modes (mod_ModeSolver.jl:333-349) for one direction, on the RAW columns of both
+// layers: the overlaps C[a][b] = <W(va)_a, vb_b>, X = |C01|² + |C10|², Y = |C00|² + |C11|².
+// b's columns swap when X > Y if a's columns stand as computed, and when Y > X if a's columns
+// were themselves swapped by the matching above them (swapping a's columns swaps C's rows, so
+// X and Y trade places, sums of the same two terms; on a tie neither swaps). Returns
+// (X > Y) | (Y > X) << 1.
+__device__ __forceinline__ uint32_t match_decision(const cd va[4][2], const cd vb[4][2]) {
   cd C[2][2];
 #pragma unroll
   for (int a = 0; a < 2; ++a)
@@ -1010,7 +1018,36 @@ __device__ __forceinline__ bool match_swap(const cd va[4][2], const cd vb[4][2])
       for (int i = 1; i < 4; ++i) s += conj(Wof(va, i, a)) * vb[i][b];
       C[a][b] = s;
     }
-  return norm2(C[0][1]) + norm2(C[1][0]) > norm2(C[0][0]) + norm2(C[1][1]);
+  const double X = norm2(C[0][1]) + norm2(C[1][0]), Y = norm2(C[0][0]) + norm2(C[1][1]);
+  return (X > Y ? 1u : 0u) | (Y > X ? 2u : 0u);
+}
+
+// the matching swap mask of layers 0 .. nlayers-1 (bit 2l: forward columns of layer l swapped,
+// bit 2l+1: backward) from the per-interface decisions k_iface stored
+__device__ __forceinline__ uint64_t swaps_upto(const TransferParams& p, long node, int nlayers) {
+  uint64_t s = 0;
+  for (int j = 2; j <= nlayers; ++j) {
+    const int a = j - 2, b = j - 1;
+    const uint32_t d = p.dec[(long)a * p.n + node];
+    const uint32_t saf = (uint32_t)(s >> (2 * a)) & 1u, sab = (uint32_t)(s >> (2 * a + 1)) & 1u;
+    const uint64_t sf = (d >> (saf ? 1 : 0)) & 1u, sb = (d >> (sab ? 3 : 2)) & 1u;
+    s |= sf << (2 * b) | sb << (2 * b + 1);
+  }
+  return s;
+}
+
+// relabel an interface S-matrix formed on raw mode columns to the matched columns: rows of
+// b11, b12 follow layer b's forward swap, rows of b21, b22 layer a's backward swap; columns of
+// b11, b21 layer a's forward swap, of b12, b22 layer b's backward swap
+__device__ __forceinline__ M2 m2_swap_rows(const M2& A, bool s) { return s ? M2{A.a10, A.a11, A.a00, A.a01} : A; }
+__device__ __forceinline__ M2 m2_swap_cols(const M2& A, bool s) { return s ? M2{A.a01, A.a00, A.a11, A.a10} : A; }
+__device__ __forceinline__ S4 relabel(const S4& X, bool saf, bool sab, bool sbf, bool sbb) {
+  S4 o;
+  o.b11 = m2_swap_cols(m2_swap_rows(X.b11, sbf), saf);
+  o.b12 = m2_swap_cols(m2_swap_rows(X.b12, sbf), sbb);
+  o.b21 = m2_swap_cols(m2_swap_rows(X.b21, sab), saf);
+  o.b22 = m2_swap_cols(m2_swap_rows(X.b22, sab), sbb);
+  return o;
 }
 
 constexpr uint8_t ST_PROJ_SINGULAR = 64;  // internal: the source projection's 4x4 solve failed
@@ -1021,20 +1058,6 @@ __device__ __forceinline__ uint8_t node_status(const TransferParams& p, long nod
   return stat;
 }
 
-__device__ __forceinline__ void match_body(const TransferParams& p, long node) {
-  const uint8_t stat = node_status(p, node);
-  uint64_t swaps = 0;
-  if (!(stat & (ST_EIGEN | ST_SORT)))
-    for (int j = 2; j <= p.nL; ++j) {
-      ModeV va, vb;
-      load_v(p, j - 2, node, swaps, va);
-      load_v(p, j - 1, node, 0, vb);
-      const bool sf = match_swap(va.vf, vb.vf), sb = match_swap(va.vb, vb.vb);
-      swaps |= (uint64_t)(sf ? 1 : 0) << (2 * (j - 1)) | (uint64_t)(sb ? 1 : 0) << (2 * (j - 1) + 1);
-    }
-  p.swaps[node] = swaps;
-}
-
 __device__ __forceinline__ void seeds_body(const TransferParams& p, long node) {
   if (p.mode == 2 || p.resp) return;
   if (node_status(p, node) & (ST_EIGEN | ST_SORT)) return;
@@ -1043,7 +1066,7 @@ __device__ __forceinline__ void seeds_body(const TransferParams& p, long node) {
   cd kx, ky;
   node_k(p, p.off + node, kx, ky);
   Mode4 M;
-  load_matched(p, layer, node, p.swaps[node], M);
+  load_matched(p, layer, node, swaps_upto(p, node, p.src), M);
   cd sif[2][3], sib[2][3];
   const bool ok = source_projection(kx, ky, p.omega, p.layers[layer], M, sif, sib);
   bool fin = true;
@@ -1058,13 +1081,13 @@ __device__ __forceinline__ void seeds_body(const TransferParams& p, long node) {
 }
 
 __device__ __forceinline__ void iface_body(const TransferParams& p, int j, long node) {
-  const uint64_t swaps = p.swaps[node];
   const int a = j - 2, b = j - 1;
   S4 X;
   {
     ModeV va, vb;
-    load_v(p, a, node, swaps, va);
-    load_v(p, b, node, swaps, vb);
+    load_v(p, a, node, 0, va);
+    load_v(p, b, node, 0, vb);
+    p.dec[(long)a * p.n + node] = (uint8_t)(match_decision(va.vf, vb.vf) | match_decision(va.vb, vb.vb) << 2);
     Mode4 A, B;
     for (int i = 0; i < 4; ++i)
       for (int m = 0; m < 2; ++m) {
@@ -1073,9 +1096,9 @@ __device__ __forceinline__ void iface_body(const TransferParams& p, int j, long 
       }
     if (!interface_matrix(A, B, X)) p.lstat[(long)b * p.n + node] |= ST_SINGULAR;
   }
-  if (j > p.src) {
+  if (j > p.src) {  // layer a's propagation, in its raw column order as X
     cd qf[2], qb[2];
-    load_q(p, a, node, swaps, qf, qb);
+    load_q(p, a, node, 0, qf, qb);
     const double d = p.layers[a].d;
     X = redheffer_diag_left(expi(qf[0], d), expi(qf[1], d), expi(-qb[0], d), expi(-qb[1], d), X);
   }
@@ -1101,7 +1124,7 @@ __device__ __forceinline__ void scan_body(const TransferParams& p, long node) {
     if (p.resp) p.resp[gnode] = 0.0;
     return;
   }
-  const uint64_t swaps = p.swaps[node];
+  const uint64_t swaps = swaps_upto(p, node, N);
   cd Qs[4];
   M2 RL = M2{z, z, z, z};
   S4 acc;
@@ -1117,7 +1140,9 @@ __device__ __forceinline__ void scan_body(const TransferParams& p, long node) {
     }
   }
   for (int j = 2; j <= N; ++j) {
-    const S4 X = ld_s4(p.sint, j - 2, n, node);
+    const int la = j - 2, lb = j - 1;
+    const S4 X = relabel(ld_s4(p.sint, j - 2, n, node), (swaps >> (2 * la)) & 1, (swaps >> (2 * la + 1)) & 1,
+                         (swaps >> (2 * lb)) & 1, (swaps >> (2 * lb + 1)) & 1);
     const S4 R = redheffer(acc, X);
     if (j > src) {
       acc = R;
@@ -1196,10 +1221,6 @@ __device__ __forceinline__ void scan_body(const TransferParams& p, long node) {
   p.status[gnode] = stat;
 }
 
-__global__ void __launch_bounds__(128) k_match(TransferParams p) {
-  const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (node < p.n) match_body(p, node);
-}
 __global__ void __launch_bounds__(128) k_seeds(TransferParams p) {
   const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (node < p.n) seeds_body(p, node);
@@ -1281,8 +1302,6 @@ __device__ __forceinline__ void stage_unit(const TransferParams& p, long u) {
     else layer_modes_qr_body(p, layer, u - (long)layer * p.n);
   } else if constexpr (STAGE == 3) {
     chain_body(p, u);
-  } else if constexpr (STAGE == 4) {
-    match_body(p, u);
   } else if constexpr (STAGE == 5) {
     seeds_body(p, u);
   } else if constexpr (STAGE == 6) {
@@ -1314,7 +1333,6 @@ cudaError_t launch_persist_b(int stage, int grid, const TransferParams* probs, c
     case 0: k_persist<0, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
     case 1: k_persist<1, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
     case 3: k_persist<3, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
-    case 4: k_persist<4, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
     case 5: k_persist<5, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
     case 6: k_persist<6, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
     case 7: k_persist<7, BLOCK><<<grid, BLOCK, 0, s>>>(probs, q); break;
@@ -1408,13 +1426,6 @@ cudaError_t launch_chain(const TransferParams& p, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-__global__ void __launch_bounds__(128) k_match_batch(const TransferParams* __restrict__ probs, const long* __restrict__ off,
-                                                     int nb) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= off[nb]) return;
-  const int i = find_problem(off, nb, t);
-  match_body(probs[i], t - off[i]);
-}
 __global__ void __launch_bounds__(128) k_seeds_batch(const TransferParams* __restrict__ probs, const long* __restrict__ off,
                                                      int nb) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1445,11 +1456,10 @@ cudaError_t launch_chain_part(int part, const TransferParams& p, cudaStream_t st
   if (p.n <= 0) return cudaSuccess;
   const unsigned g = (unsigned)((p.n + 127) / 128);
   switch (part) {
-    case 0: k_match<<<g, 128, 0, stream>>>(p); break;
-    case 1: k_seeds<<<g, 128, 0, stream>>>(p); break;
-    case 2:
+    case 0:
       if (p.nL > 1) k_iface<<<(unsigned)((p.n * (p.nL - 1) + 127) / 128), 128, 0, stream>>>(p);
       break;
+    case 1: k_seeds<<<g, 128, 0, stream>>>(p); break;
     default: k_scan<<<g, 128, 0, stream>>>(p); break;
   }
   return cudaGetLastError();
@@ -1462,7 +1472,6 @@ cudaError_t launch_transfer_batch(int kernel, const TransferParams* probs, const
   switch (kernel) {
     case 0: k_layer_modes_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
     case 1: k_layer_modes_qr_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
-    case 4: k_match_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
     case 5: k_seeds_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
     case 6: k_iface_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
     case 7: k_scan_batch<<<grid, 128, 0, stream>>>(probs, off, nb); break;
