@@ -1225,7 +1225,8 @@ __global__ void __launch_bounds__(128) k_seeds(TransferParams p) {
   const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (node < p.n) seeds_body(p, node);
 }
-__global__ void __launch_bounds__(128) k_iface(TransferParams p) {
+// at most 170 registers: three 128-thread CTAs per SM (16 B of spills)
+__global__ void __launch_bounds__(128, 3) k_iface(TransferParams p) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long n = p.n;
   if (t >= n * (p.nL - 1)) return;
@@ -1312,8 +1313,9 @@ __device__ __forceinline__ void stage_unit(const TransferParams& p, long u) {
   }
 }
 
+// the interface stage at three 128-thread CTAs per SM, as k_iface
 template <int STAGE, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_persist(const TransferParams* __restrict__ probs, TileQueue q) {
+__global__ void __launch_bounds__(BLOCK, (STAGE == 6 && BLOCK == 128) ? 3 : 1) k_persist(const TransferParams* __restrict__ probs, TileQueue q) {
   __shared__ int tile;
   for (;;) {
     if (threadIdx.x == 0) tile = (int)atomicAdd(q.counter, 1u);
@@ -1434,7 +1436,7 @@ __global__ void __launch_bounds__(128) k_seeds_batch(const TransferParams* __res
   seeds_body(probs[i], t - off[i]);
 }
 // off: per-item (nL - 1) x n interface-node pairs
-__global__ void __launch_bounds__(128) k_iface_batch(const TransferParams* __restrict__ probs, const long* __restrict__ off,
+__global__ void __launch_bounds__(128, 3) k_iface_batch(const TransferParams* __restrict__ probs, const long* __restrict__ off,
                                                      int nb) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= off[nb]) return;
