@@ -265,10 +265,10 @@ def measured_peaks():
 
 # FP64 operations per node of the per-node solve kernels on this workload, from one ncu count
 # of their DFMA/DADD/DMUL instructions (2 per DFMA); absent until captured
-FP64_OPS_PER_NODE = {"k_iface": 7.11e3,  # 1.464e8 DFMA + 0.731e8 DADD + 1.000e8 DMUL per 65536 nodes
-                     "k_scan": 7.43e3,  # 1.587e8 DFMA + 0.574e8 DADD + 1.119e8 DMUL per 65536 nodes
-                     "k_layer_modes": 9.46e3,  # 1.982e8 DFMA + 0.594e8 DADD + 1.641e8 DMUL (8 layers)
-                     "k_strengths2d": 8.04e3}  # 1.832e8 DFMA + 0.596e8 DADD + 1.009e8 DMUL (8 z rows)
+FP64_OPS_PER_NODE = {"k_iface": 8.99e3,  # 1.79e8 DFMA + 0.97e8 DADD + 1.33e8 DMUL per 65536 nodes
+                     "k_scan": 7.43e3,  # 1.59e8 DFMA + 0.57e8 DADD + 1.12e8 DMUL per 65536 nodes
+                     "k_layer_modes": 9.46e3,  # 1.98e8 DFMA + 0.59e8 DADD + 1.64e8 DMUL (8 layers)
+                     "k_strengths2d": 8.04e3}  # k_reflect2d + k_strengths_rows (8 z rows)  # 1.832e8 DFMA + 0.596e8 DADD + 1.009e8 DMUL (8 z rows)
 FP64_NOMINAL = 37.2  # TFLOP/s: 148 SM x 64 FP64 FMA/clk x 2 x 1.965 GHz (no measured FP64 peak)
 
 
