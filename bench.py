@@ -201,9 +201,34 @@ def cpu_sample(stack, lam, phi_take=4):
     return dt, len(kr) * len(phi), N_PHI / len(phi)
 
 
+# --------------------------------------------------------------------------------------
+# ranks (one process per GPU under torchrun): every rank takes the same collective steps in
+# the same order; no data-path collective, only the timing's barrier and max
+# --------------------------------------------------------------------------------------
+def rank_env():
+    """(rank, world size, local rank) from the torchrun environment (1 process: 0, 1, 0)."""
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def max_over_ranks(ms, dist=None, device="cpu"):
+    """The largest per-rank time: every rank calls it once per timed quantity, in order."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, ms):
+    """Whole-job throughput of a weak-scaling run: every rank processes units_per_rank in
+    (at most) ms milliseconds."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    rank = rank_env()[0]
+    if rank != 0:  # the reference arm runs on rank 0's host cores only
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ytf_oracle as oracle
@@ -313,9 +338,7 @@ def roofline(name, prof, steps=1):
 
 def run_ours(args):
     import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = rank_env()
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -388,10 +411,7 @@ def run_ours(args):
             torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
         prof = ctx.profile_read()
-        if dist is not None:
-            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist, f"cuda:{local}")
         return ms, prof, clk.summary()
 
     # value and e2e without the per-kernel events; the kernel split from a third, profiled pass
@@ -401,8 +421,8 @@ def run_ours(args):
     ms_e2e, _, _ = timed(True, False)
     _, prof, _ = timed(False, True, "batched" if args.calls == "plan" else None)
     entries = ENTRIES_PER_LAMBDA * N_LAMBDA
-    value = world * entries / (ms * 1e-3)
-    e2e = world * entries / (ms_e2e * 1e-3)
+    value = job_rate(entries, world, ms)
+    e2e = job_rate(entries, world, ms_e2e)
     h2d = sum(8 * (len(g[1]) * 2 + len(g[3]) * 2) + 8 * (len(o[1]) + len(o[2]) + len(o[3])) for g, o in per)
     d2h = entries * 16
 
