@@ -199,19 +199,14 @@ __device__ __forceinline__ void digits3(int Y, uint32_t& d0, uint32_t& d1, uint3
 }
 
 // one thread per (column tile, column slot, node slice, 8-node group): 16 bytes of each of
-// the two rows of the column in each of the three digit planes
-__global__ void k_bslice(LateralI8 p) {
-  const long groups = p.kchunk / 8;
-  const int slots = p.Np / 2;
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long total = (long)p.ntile * slots * p.nchunk * groups;
-  if (t >= total) return;
-  const long g = t % groups;
-  long rest = t / groups;
-  const int z = (int)(rest % p.nchunk);
-  rest /= p.nchunk;
-  const int cl = (int)(rest % slots);
-  const int ct = (int)(rest / slots);
+// the two rows of the column in each of the three digit planes. Grid: x over the slice's
+// 8-node groups, y = column slot, z = column tile x node slice (no index division).
+__global__ void __launch_bounds__(256) k_bslice(LateralI8 p) {
+  const int groups = (int)(p.kchunk / 8);
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= groups) return;
+  const int cl = blockIdx.y;
+  const int z = (int)(blockIdx.z % (unsigned)p.nchunk), ct = (int)(blockIdx.z / (unsigned)p.nchunk);
   const int col = ct * p.ctile + cl;
   const bool cv = cl < p.ctile && col < p.ncol;
   const long o = (long)z * p.ncol + (cv ? col : 0);
@@ -501,8 +496,8 @@ cudaError_t launch_lateral_i8(const LateralI8& p, cudaStream_t s) {
       p.n_pad != (long)p.nchunk * p.kchunk || p.n_pad < p.n)
     return cudaErrorInvalidValue;
   {
-    const long total = (long)p.ntile * (p.Np / 2) * p.nchunk * (p.kchunk / 8);
-    k_bslice<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p);
+    const dim3 grid((unsigned)((p.kchunk / 8 + 255) / 256), (unsigned)(p.Np / 2), (unsigned)(p.ntile * p.nchunk));
+    k_bslice<<<grid, 256, 0, s>>>(p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
