@@ -1556,6 +1556,9 @@ struct ytf_plan {
   char* tb = nullptr;
   size_t tb_bytes = 0;
   cudaStream_t cap = nullptr;
+  cudaStream_t copy = nullptr;          // captured side branch: the large items' output copies
+  std::vector<cudaEvent_t> fork_ev;     // one per large item with a page-locked host output, + join
+  std::vector<char> copied;             // output copied on the side branch in the current graph
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1576,6 +1579,8 @@ void plan_release_graph(ytf_plan* P) {
   P->tb = nullptr;
   P->tb_bytes = 0;
   P->kcount.clear();
+  for (auto e : P->fork_ev) cudaEventDestroy(e);
+  P->fork_ev.clear();
 }
 
 void plan_free(ytf_plan* P) {
@@ -1585,6 +1590,7 @@ void plan_free(ytf_plan* P) {
   if (P->cap) cudaStreamSynchronize(P->cap);
   plan_release_graph(P);
   if (P->cap) cudaStreamDestroy(P->cap);
+  if (P->copy) cudaStreamDestroy(P->copy);
   if (P->e0) cudaEventDestroy(P->e0);
   if (P->e1) cudaEventDestroy(P->e1);
   if (P->arena) cudaFree(P->arena);
@@ -1641,6 +1647,7 @@ int plan_large_synthesis(ytf_plan* P, std::map<std::string, size_t>* rec,
   ctx->ws_record = rec;
   ctx->ws_override = ovr;
   int rc = YTF_OK;
+  size_t nfork = 0;
   for (int i = 0; i < P->nb && !rc; ++i) {
     if (!P->large[i]) continue;
     const ytf_green_desc& g = P->gr[i];
@@ -1650,6 +1657,25 @@ int plan_large_synthesis(ytf_plan* P, std::map<std::string, size_t>* rec,
     rc = green_impl(ctx, P->cs[i], g.obs_layer, g.zsrc_local, g.nz, g.z_obs, g.nx, g.xs, g.ny, g.ys, g.terms,
                     g.precision, out, 1, &gb);
     if (rc) rc = plan_fail(ctx, rc, i);
+    // captured pass: a page-locked host output is copied on the side branch as soon as its
+    // item is done, overlapping the next items' kernels
+    if (!rc && ovr && P->direct[i] && P->g_off[i] >= 0 && nfork < P->fork_ev.size()) {
+      cudaEvent_t ev = P->fork_ev[nfork++];
+      cudaError_t e = cudaEventRecord(ev, P->cap);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(P->copy, ev, 0);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(g.out, P->d_G + P->g_off[i], 16 * (size_t)g.nx * g.ny * g.nz * 9, cudaMemcpyDeviceToHost,
+                            P->copy);
+      if (e != cudaSuccess) rc = fail(ctx, YTF_ERR_CUDA, std::string("ytf_plan: output copy: ") + cudaGetErrorString(e));
+      else P->copied[i] = 1;
+    }
+  }
+  // join the side branch back into the captured stream
+  if (!rc && ovr && nfork > 0) {
+    cudaEvent_t join = P->fork_ev.back();
+    cudaError_t e = cudaEventRecord(join, P->copy);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(P->cap, join, 0);
+    if (e != cudaSuccess) rc = fail(ctx, YTF_ERR_CUDA, std::string("ytf_plan: output copy join: ") + cudaGetErrorString(e));
   }
   if (ovr)
     for (auto& kv : ctx->klaunch) {
@@ -1830,6 +1856,7 @@ int plan_build(ytf_plan* P) {
     }
   }
   CK(cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&P->copy, cudaStreamNonBlocking));
   CK(cudaEventCreate(&P->e0));
   CK(cudaEventCreate(&P->e1));
   CK(synth_small_init());
@@ -1971,6 +1998,18 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
     }
   }
   CK(cudaMemcpy(P->tb, hb.data(), hb.size(), cudaMemcpyHostToDevice));
+  // side-branch events of the large items' page-locked outputs (+ one to join), made before
+  // the capture
+  P->copied.assign(nb, 0);
+  {
+    int nd = 0;
+    for (int i = 0; i < nb; ++i) nd += P->large[i] && P->direct[i] && P->g_off[i] >= 0;
+    for (int k = 0; k < nd + (nd > 0); ++k) {
+      cudaEvent_t ev;
+      CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      P->fork_ev.push_back(ev);
+    }
+  }
   // record the graph
   unsigned* ctr = reinterpret_cast<unsigned*>(P->tb + o_ctr);
   const int nsm = P->nsm;
@@ -2020,7 +2059,7 @@ extern "C" int ytf_plan_retune(ytf_plan* P, const ytf_tune* tune_in) {
       const ytf_green_desc& g = P->gr[i];
       const size_t cnt = (size_t)g.nx * g.ny * g.nz * 9;
       if (P->direct[i]) {
-        step(cudaMemcpyAsync(g.out, P->d_G + P->g_off[i], 16 * cnt, cudaMemcpyDeviceToHost, s));
+        if (!P->copied[i]) step(cudaMemcpyAsync(g.out, P->d_G + P->g_off[i], 16 * cnt, cudaMemcpyDeviceToHost, s));
       } else {
         if (!any) lo = P->g_off[i];
         any = true;
