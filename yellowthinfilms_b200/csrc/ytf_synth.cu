@@ -561,7 +561,8 @@ __global__ void __launch_bounds__(128) k_reflect2d(SynthParams p, double2* __res
 // per node of a k_strengths_rows block: 12 amplitudes, the obs-layer basis (16), sf, sb (6 each),
 // Qf, Qb (2 each)
 constexpr int SR_F = 44;
-__global__ void __launch_bounds__(128) k_strengths_rows(SynthParams p, const double2* __restrict__ amp,
+// at most 128 registers: four CTAs per SM (no spills)
+__global__ void __launch_bounds__(128, 4) k_strengths_rows(SynthParams p, const double2* __restrict__ amp,
                                                          double2* __restrict__ S, unsigned long long* colmax,
                                                          long kchunk) {
   __shared__ double2 sh[SR_F][32];
