@@ -543,7 +543,7 @@ __global__ void __launch_bounds__(128) k_strengths2d(SynthParams p, double2* S, 
 // (coalesced, once per block), then each of its 4 warps takes every fourth z row of the 32
 // nodes, one node per lane. The arithmetic per row is strengths_row's, in the same order.
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_reflect2d(SynthParams p, double2* __restrict__ amp) {
+__global__ void __launch_bounds__(128, 4) k_reflect2d(SynthParams p, double2* __restrict__ amp) {
   const long node = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long n = p.c.n;
   if (node >= n) return;
@@ -857,7 +857,7 @@ __device__ __forceinline__ int find_item(const long* __restrict__ off, int nb, l
   return lo;
 }
 
-__global__ void __launch_bounds__(128) k_synth_small(const SynthItem* __restrict__ items, int nitems,
+__global__ void __launch_bounds__(128, 3) k_synth_small(const SynthItem* __restrict__ items, int nitems,
                                                       const long* __restrict__ w_off, long nwork, unsigned* counter,
                                                       int chunk) {
   extern __shared__ __align__(16) unsigned char syn_smem[];
