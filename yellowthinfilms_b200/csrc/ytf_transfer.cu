@@ -1313,9 +1313,11 @@ __device__ __forceinline__ void stage_unit(const TransferParams& p, long u) {
   }
 }
 
-// the interface stage at three 128-thread CTAs per SM, as k_iface
+// the interface stage at three 128-thread CTAs per SM (as k_iface), the mode stage at four
+// (128 registers, no spills)
 template <int STAGE, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, (STAGE == 6 && BLOCK == 128) ? 3 : 1) k_persist(const TransferParams* __restrict__ probs, TileQueue q) {
+__global__ void __launch_bounds__(BLOCK, (STAGE == 6 && BLOCK == 128) ? 3 : ((STAGE == 0 && BLOCK == 128) ? 4 : 1))
+    k_persist(const TransferParams* __restrict__ probs, TileQueue q) {
   __shared__ int tile;
   for (;;) {
     if (threadIdx.x == 0) tile = (int)atomicAdd(q.counter, 1u);
