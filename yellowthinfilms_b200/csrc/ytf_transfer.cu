@@ -498,6 +498,7 @@ __device__ __forceinline__ void layer_modes_qr_body(const TransferParams& p, int
 __global__ void __launch_bounds__(128) k_layer_modes_qr(TransferParams p) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= p.n * p.nL) return;
+  if (p.lstat[t] != ST_NEED_QR) return;  // units are layer-major: t = layer n + node
   const int layer = (int)(t / p.n);
   layer_modes_qr_body(p, layer, t - (long)layer * p.n);
 }
@@ -1275,6 +1276,7 @@ __global__ void __launch_bounds__(128) k_layer_modes_qr_batch(const TransferPara
   const int i = find_problem(off, nb, t);
   const TransferParams& p = probs[i];
   const long lt = t - off[i];
+  if (p.lstat[lt] != ST_NEED_QR) return;  // the status byte of unit lt, before any division
   const int layer = (int)(lt / p.n);
   layer_modes_qr_body(p, layer, lt - (long)layer * p.n);
 }
@@ -1298,6 +1300,8 @@ __global__ void __launch_bounds__(128) k_chain_batch(const TransferParams* __res
 template <int STAGE>
 __device__ __forceinline__ void stage_unit(const TransferParams& p, long u) {
   if constexpr (STAGE == 0 || STAGE == 1) {
+    if constexpr (STAGE == 1)
+      if (p.lstat[u] != ST_NEED_QR) return;  // most units: one status byte, no division
     const int layer = (int)(u / p.n);
     if constexpr (STAGE == 0) layer_modes_body(p, layer, u - (long)layer * p.n);
     else layer_modes_qr_body(p, layer, u - (long)layer * p.n);
