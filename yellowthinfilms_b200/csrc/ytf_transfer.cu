@@ -286,8 +286,8 @@ __device__ bool eig4(cd A[4][4], cd lam[4], cd V[4][4]) {
       nn += a2;
       if (a2 > best) { best = a2; vb = v[i]; }
     }
-    const double inv = 1.0 / sqrt(nn);
-    const cd ph = conj(vb) * (1.0 / sqrt(best));
+    const double inv = rsqrt(nn);
+    const cd ph = conj(vb) * rsqrt(best);
 #pragma unroll
     for (int i = 0; i < 4; ++i) V[i][k] = (v[i] * ph) * inv;
   }
@@ -384,8 +384,8 @@ __device__ bool block_modes(const LayerDev& L, double w, cd kx, cd ky, cd Q[4], 
         nn += a2;
         if (a2 > best) { best = a2; vb = v[r]; }
       }
-      const double inv = 1.0 / sqrt(nn);
-      const cd ph = conj(vb) * (1.0 / sqrt(best));
+      const double inv = rsqrt(nn);  // unit 2-norm, largest component real (ZGEEVX)
+      const cd ph = conj(vb) * rsqrt(best);
 #pragma unroll
       for (int r = 0; r < 4; ++r) V[r][col] = (v[r] * ph) * inv;
       Q[col] = sgn ? -q : q;
