@@ -1787,10 +1787,8 @@ int plan_build(ytf_plan* P) {
       c->d_phi = b + 2 * nk;
       c->d_wphi = b + 2 * nk + np;
     }
-    const int oi = c->oidx(P->gr[i].obs_layer);
     SynthParams& sp = P->sps[i];
     sp.c.kr = c->d_kr; sp.c.wr = c->d_wr; sp.c.phi = c->d_phi; sp.c.wphi = c->d_wphi;
-    (void)oi;
     sp.zo = P->d_in + P->in_coord[i];
   }
   // node-solve passes under the scratch budget, items in order
