@@ -1200,7 +1200,8 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
     WS(P, double, "g_P", 26 * (size_t)nz * nr);
     double *C0 = C, *C1 = C + 10 * (size_t)nz * nk, *C2 = C + 18 * (size_t)nz * nk;
     double *P0 = P, *P1 = P + 10 * (size_t)nz * nr, *P2 = P + 18 * (size_t)nz * nr;
-    CK(LAUNCH("k_coef1d", launch_coef1d(sp, C0, C1, C2, ctx->stream)));
+    WS(amp1, double2, "g_amp", (size_t)12 * nk);
+    CK(LAUNCH("k_coef1d", launch_coef1d_amp(sp, amp1, C0, C1, C2, ctx->stream)));
     if (c->d_kri) {
       // nodes on a deformed contour: complex J_n(kρ ρ) tables, two FP64 GEMMs per order
       // (Re J and Im J against the real/imaginary coefficient columns), then the complex combine
@@ -1239,6 +1240,23 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
         err = e1;
         CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
       }
+      // one node slicing for the three orders (that of order 0, the widest), so the J_n
+      // digit images of all three come from one Bessel evaluation per (ρ, k)
+      long kchunk;
+      {
+        const int ct0 = bessel_i8_ctile(Nn8[0]);
+        const long tiles = (long)((nr + 127) / 128) * ((Nn8[0] + ct0 - 1) / ct0);
+        const long want = std::max(1L, (long)nsm / tiles);
+        kchunk = (nk + want - 1) / want;
+        kchunk = std::min(16384L, std::max(64L, ((kchunk + 63) / 64) * 64));
+      }
+      const int nchunk = (int)((nk + kchunk - 1) / kchunk);
+      const size_t nst = (size_t)(kchunk / 64);
+      const size_t abytes = (size_t)((nr + 127) / 128) * nchunk * nst * bessel_i8_stage_bytes_a();
+      WS(A0i, uint8_t, "g_bi_a0", abytes);
+      WS(A1i, uint8_t, "g_bi_a1", abytes);
+      WS(A2i, uint8_t, "g_bi_a2", abytes);
+      uint8_t* Aord[3] = {A0i, A1i, A2i};
       for (int o = 0; o < 3; ++o) {
         BesselI8 bp;
         std::memset(&bp, 0, sizeof(bp));
@@ -1247,19 +1265,15 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
         bp.Np = ((bp.ctile + 15) / 16) * 16;
         bp.ntile_n = (bp.N + bp.ctile - 1) / bp.ctile;
         bp.ntile_m = (nr + 127) / 128;
-        const long tiles = (long)bp.ntile_m * bp.ntile_n;
-        const long want = std::max(1L, (long)nsm / tiles);
-        long kchunk = (nk + want - 1) / want;
-        kchunk = std::min(16384L, std::max(64L, ((kchunk + 63) / 64) * 64));
         bp.kchunk = kchunk;
-        bp.nchunk = (int)((nk + kchunk - 1) / kchunk);
-        const size_t nst = (size_t)(kchunk / 64);
-        WS(Ai, uint8_t, "g_bi_a", (size_t)bp.ntile_m * bp.nchunk * nst * bessel_i8_stage_bytes_a());
+        bp.nchunk = nchunk;
         WS(Bi, uint8_t, "g_bi_b", (size_t)bp.ntile_n * bp.nchunk * nst * bessel_i8_stage_bytes_b(bp.Np));
         WS(cm, unsigned long long, "g_bi_cmax", (size_t)bp.nchunk * bp.N);
         WS(pt, double, "g_bi_part", (size_t)bp.nchunk * bp.N * nr);
         bp.kr = c->d_kr; bp.rho = drho; bp.C = Cn8[o];
-        bp.Aimg = Ai; bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
+        bp.Aimg = Aord[o]; bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
+        if (o == 0) CK(LAUNCH("k_bessel_i8", launch_bessel_i8_aimg3(bp, A0i, A1i, A2i, ctx->stream)));
+        bp.aimg_ready = 1;
         CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pn8[o], ctx->stream)));
       }
       if (!gb) {

@@ -124,6 +124,8 @@ struct SynthParams {
 
 // 1D Jacobi-Anger synthesis
 cudaError_t launch_coef1d(const SynthParams& p, double* C0, double* C1, double* C2, cudaStream_t s);
+// the same through per-node reflected amplitudes in amp ([12][n] complex scratch)
+cudaError_t launch_coef1d_amp(const SynthParams& p, double2* amp, double* C0, double* C1, double* C2, cudaStream_t s);
 cudaError_t launch_bessel_c(const double* kr, const double* kri, long nk, const double* rho, int nr, double* J,
                             cudaStream_t s);
 cudaError_t launch_combine_complex(long M, int N2, const double* A, const double* B, double* P, cudaStream_t s);
@@ -240,7 +242,11 @@ struct BesselI8 {
   unsigned long long* colmax;  // [nchunk][N]
   double* partial;   // [nchunk][N][M]
   unsigned* err;
+  int aimg_ready;    // Aimg already holds this order's J_n digits (launch_bessel_i8_aimg3)
 };
+// the J_0, J_1, J_2 digit images of all three orders in one pass (one Bessel evaluation per
+// (ρ, k)); p gives the shared layout (M, K, ntile_m, kchunk, nchunk, kr, rho)
+cudaError_t launch_bessel_i8_aimg3(const BesselI8& p, uint8_t* A0, uint8_t* A1, uint8_t* A2, cudaStream_t s);
 size_t bessel_i8_stage_bytes_a();
 size_t bessel_i8_stage_bytes_b(int Np);
 size_t bessel_i8_smem(int Np);
