@@ -573,7 +573,7 @@ def run_learned(args):
     from yellowthinfilms_b200 import api
     from yellowthinfilms_b200 import learned as L
     torch.cuda.set_device(0)
-    n_train, n_k, n_test = 4883, 2048, int(os.environ.get("YTF_LEARNED_TEST_STACKS", "48"))
+    n_train, n_k, n_test = 4883, 2048, int(os.environ.get("YTF_LEARNED_TEST_STACKS", "4096"))
     t = time.perf_counter()
     X, T = L.training_set(n_train, n_k=n_k, seed=SEED)
     t_data = time.perf_counter() - t
@@ -601,61 +601,91 @@ def run_learned(args):
         torch.cuda.synchronize()
         return r, a.elapsed_time(b) * 1e-3
 
-    # held-out problems: every stack at a near-field and a 5 λ observation set; the G
-    # evaluations of both methods are batched over all problems of a regime
+    # held-out problems: every stack at the config-1 observation grid (256 ρ log-spaced over
+    # 0.01 λ to 5 λ x 64 heights) and at the same grid squeezed into the near field (ρ ≤ 0.2 λ);
+    # both methods solve the same problems, chunk by chunk, each method's G evaluations
+    # batched over a chunk's problems still open; G and the acceptance checks stay in HBM
+    chunk = int(os.environ.get("YTF_LEARNED_CHUNK", "256"))
+    n_ref = min(n_test, int(os.environ.get("YTF_LEARNED_REF_STACKS", "64")))
+    prec = args.precision if args.precision != "split_bf16" else "int8x3"
     ctx = api.Context(0)
     stacks = []
     for _ in range(n_test):
         st, lam = L.film_stack(rng)
         stacks.append((st, lam, api.Stack(st, ctx)))
+    n_rho, n_z = 256, 64
     res = {}
-    for rw in (0.2, 5.0):
+    for rw in (5.0, 0.2):
         probs = []
         for st, lam, sto in stacks:
             probs.append(dict(stack=sto, layers=st, k0=2 * np.pi / lam, source_layer=1, zsrc_local=20.0,
-                              z=np.linspace(60.0, 200.0, 6), rho=np.exp(np.linspace(np.log(0.01 * lam), np.log(rw * lam), 16)),
-                              terms="scattered", h_min=80.0, rho_max=rw * lam))
-        # converged references: the scanned rule at rtol 1e-10, halved (untimed)
+                              z=np.linspace(60.0, 200.0, n_z),
+                              rho=np.exp(np.linspace(np.log(0.01 * lam), np.log(rw * lam), n_rho)),
+                              terms="scattered", h_min=80.0, rho_max=rw * lam, precision=prec))
+        # converged references on the first n_ref problems: the scanned rule at rtol 1e-10,
+        # halved, FP64 synthesis (untimed)
         refs = []
-        for P in probs:
+        for P in probs[:n_ref]:
             kr, wr, ir = api.point_kx_grid(P["stack"], P["k0"], 1, h_min=80.0, rho_max=P["rho_max"], rtol=1e-10, ctx=ctx)
             refs.append(L.halved(P["layers"], P["k0"], ir["panels"], 8))
-        Gref = L.batch_G(probs, refs, ctx=ctx)
-        L.plain_rules_batch(probs, ctx=ctx)  # warm-up of both paths
-        L.learned_rules_batch(net, probs, ctx=ctx)
-        outp, tp = timed(lambda: L.plain_rules_batch(probs, ctx=ctx))
-        outl, tl = timed(lambda: L.learned_rules_batch(net, probs, ctx=ctx))
-        err = 0.0
-        for (gp, kp, _, _, _), (gl, kl, _, _, _), gr in zip(outp, outl, Gref):
-            nr = np.linalg.norm(gr)
-            err = max(err, float(np.linalg.norm(gp - gr) / nr), float(np.linalg.norm(gl - gr) / nr))
-        res[rw] = dict(entries=sum(g.size for g in Gref), t_plain=tp, t_learned=tl,
-                       n_plain=[len(o[1]) for o in outp], n_learned=[len(o[1]) for o in outl],
-                       accepted=sum(int(o[3]) for o in outl), err=err,
-                       halvings_plain=float(np.mean([o[3] for o in outp])),
-                       halvings_learned=float(np.mean([o[4] for o in outl])))
-    near = res[0.2]
-    line = {"metric": METRIC, "value": near["entries"] / near["t_learned"], "unit": "entries/s", "n_gpus": 1,
-            "steps": n_test, "warmup": 0, "ms_per_step": 1e3 * near["t_learned"] / n_test, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve and synthesis; MLP bf16 weights, fp32 accum",
+        Gref = L.batch_G([dict(P, precision="fp64") for P in probs[:n_ref]], refs, ctx=ctx)
+        warm = probs[:min(chunk, n_test)]
+        L.plain_rules_batch(warm, ctx=ctx, device=True)  # warm-up of both paths (one chunk)
+        L.learned_rules_batch(net, warm, ctx=ctx, device=True)
+        tp = tl = 0.0
+        entries, n_plain, n_learned, acc, hp, hl = 0, [], [], 0, [], []
+        err, mutual = 0.0, 0.0
+        for c0 in range(0, n_test, chunk):
+            part = probs[c0:c0 + chunk]
+            outp, t1 = timed(lambda: L.plain_rules_batch(part, ctx=ctx, device=True))
+            outl, t2 = timed(lambda: L.learned_rules_batch(net, part, ctx=ctx, device=True))
+            tp, tl = tp + t1, tl + t2
+            for j, (op, ol) in enumerate(zip(outp, outl)):
+                gp, gl = op[0], ol[0]
+                entries += gp.numel()
+                n_plain.append(len(op[1]))
+                n_learned.append(len(ol[1]))
+                acc += int(ol[3])
+                hp.append(op[3])
+                hl.append(ol[4])
+                mutual = max(mutual, float(torch.linalg.vector_norm(gp - gl) / torch.linalg.vector_norm(gp)))
+                if c0 + j < n_ref:
+                    gp, gl = gp.cpu().numpy(), gl.cpu().numpy()
+                    gr = Gref[c0 + j]
+                    nr = np.linalg.norm(gr)
+                    err = max(err, float(np.linalg.norm(gp - gr) / nr), float(np.linalg.norm(gl - gr) / nr))
+            del outp, outl
+        res[rw] = dict(entries=entries, t_plain=tp, t_learned=tl, n_plain=n_plain, n_learned=n_learned,
+                       accepted=acc, err=err, mutual=mutual, halvings_plain=float(np.mean(hp)),
+                       halvings_learned=float(np.mean(hl)))
+        del probs, Gref
+    head = res[5.0]
+    line = {"metric": METRIC, "value": head["entries"] / head["t_learned"], "unit": "entries/s", "n_gpus": 1,
+            "steps": n_test, "warmup": 0, "ms_per_step": 1e3 * head["t_learned"] / n_test, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": f"f64 solve, {prec} synthesis; MLP bf16 weights, fp32 accum",
             "data": "synthetic (seeded)", "impl": "learned-adaptive",
-            "config": {"workload": "learned adaptive quadrature: air / uniaxial film / substrate stacks, vertical dipole "
-                                   "20 nm above the film, 16 ρ x 6 heights (60-200 nm) x 9 components, scattered term; "
-                                   "each method's G evaluations batched over the held-out stacks (one batched build "
-                                   "and synthesis per refinement level)",
+            "config": {"workload": f"learned adaptive quadrature: {n_test} held-out air / uniaxial film / substrate "
+                                   f"stacks, vertical dipole 20 nm above the film, {n_rho} ρ log-spaced over "
+                                   f"0.01-5 λ x {n_z} heights (60-200 nm) x 9 components, scattered term; each "
+                                   f"method's G evaluations batched over chunks of {chunk} stacks (one batched "
+                                   "build and synthesis per refinement level), G and the acceptance checks in HBM",
                        "train_samples": n_train * n_k, "train_steps": steps, "batch": batch, "held_out_stacks": n_test,
-                       "tolerance": 1e-6},
-            "plain_entries_per_s": near["entries"] / near["t_plain"],
-            "learned_vs_plain": near["t_plain"] / near["t_learned"],
+                       "tolerance": 1e-6, "synthesis": prec, "reference_checked_stacks": n_ref},
+            "plain_entries_per_s": head["entries"] / head["t_plain"],
+            "learned_vs_plain": head["t_plain"] / head["t_learned"],
             "max_rel_err_vs_reference": max(r["err"] for r in res.values()),
+            "max_rel_diff_learned_vs_plain": max(r["mutual"] for r in res.values()),
             "regimes": {f"rho_max {rw} lambda": {"learned_entries_per_s": r["entries"] / r["t_learned"],
                                                 "plain_entries_per_s": r["entries"] / r["t_plain"],
                                                 "learned_vs_plain": r["t_plain"] / r["t_learned"],
+                                                "t_learned_s": r["t_learned"], "t_plain_s": r["t_plain"],
                                                 "mean_nodes_learned": float(np.mean(r["n_learned"])),
                                                 "mean_nodes_plain": float(np.mean(r["n_plain"])),
                                                 "mean_halvings_plain": r["halvings_plain"],
                                                 "mean_refinements_learned": r["halvings_learned"],
-                                                "accepted": r["accepted"], "stacks": n_test}
+                                                "accepted": r["accepted"], "stacks": n_test,
+                                                "max_rel_err_vs_reference": r["err"]}
                         for rw, r in res.items()},
             "training": {"data_s": t_data, "train_s": t_train, "first_loss": float(losses[0]),
                          "last_loss": float(np.mean(losses[-50:]))}}

@@ -109,6 +109,14 @@ int ytf_cache_export(ytf_ctx* ctx, const ytf_cache* cache, double* T, double* Qf
 int ytf_cavity_response(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer, long n,
                         const double* kr, double phi, double* out);
 
+/* ytf_cavity_response for many (stack, ω, source layer) items with one synchronisation
+ * (_cavity_response, mod_KSpaceFeatures.jl:109-127, per item): item i's counts[i] kρ values
+ * are kr[o_i : o_i + counts[i]] with o_i = counts[0] + ... + counts[i-1]; its responses go to
+ * the same places of out. The exact window sampling of the learned node placement calls it
+ * once for all problems. An argument error names the item. */
+int ytf_cavity_response_batch(ytf_ctx* ctx, int nitems, const ytf_stack* const* stacks, const double* omega,
+                              const int* source_layer, const long* counts, const double* kr, double phi, double* out);
+
 /* build_cavity_transfer_1d on a deformed integration contour: complex nodes kρ = k_re + i k_im
  * with complex weights (w_re + i w_im), e.g. kρ(t) = t - i h s(t) with s(0) = s(L) = 0 below
  * the real axis. No counterpart in the reference, whose rules stay on the real axis

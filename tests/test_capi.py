@@ -64,3 +64,17 @@ def test_host_light_lines_bit_exact_with_oracle(oracle):
                     assert len(a) == len(b) and np.array_equal(a, b), (a, b)
                     n += 1
     assert n > 300
+
+
+def test_halve_panels_array_form_equals_pair_form():
+    """halve_panels on a [n, 2] array gives the pair form's panels bit for bit (the batched
+    refinement levels pass arrays); mod_KxGrid.jl:387-388."""
+    from yellowthinfilms_b200 import api
+    rng = np.random.default_rng(3)
+    e = np.sort(rng.uniform(0.0, 7.0, 41))
+    pairs = list(zip(e[:-1], e[1:]))
+    arr = api.halve_panels(np.array(pairs))
+    lst = api.halve_panels(pairs)
+    assert arr.shape == (80, 2)
+    assert np.array_equal(arr, np.array(lst))
+    assert np.array_equal(api.halve_panels(arr), np.array(api.halve_panels(lst)))

@@ -471,6 +471,41 @@ def test_green_batch_matches_single_calls(ytf):
         assert np.array_equal(got, ref), p
 
 
+def test_green_batch_all_1d_side_streams_match_single_calls(ytf):
+    """An all-1D ytf_green_batch (its items round-robin on side streams with their own
+    workspaces, radii maps pre-uploaded): item for item the same arrays as closed_form_G, bit
+    for bit, for several stacks, node counts, precisions, repeated radii, host and device
+    outputs and a deformed-contour cache."""
+    import torch
+    specs, caches = [], []
+    for idx, kmax, src in ((1, 12.0, 2), (0, 6.0, 1), (2, 9.0, 1), (1, 4.0, 1)):
+        _, st = FOUNDATION_STACKS[idx]
+        kx, wt = krho_grid(st, W, kmax=kmax)
+        caches.append(ytf.build_cavity_transfer_1d(st, W, src, kx, wt, obs_layers=[src]))
+    _, stc = FOUNDATION_STACKS[1]
+    kc, wc = ytf.contour_rule(W, npanels=64)
+    caches.append(ytf.build_cavity_transfer_1d_contour(stc, W, 1, kc, wc, obs_layers=[1]))
+    xs, ys = np.linspace(-0.3, 0.3, 9), np.linspace(-0.2, 0.25, 7)
+    rho = np.geomspace(0.01, 2.0, 40)
+    for j, c in enumerate(caches):
+        src = c.source_layer
+        for prec in (("fp64", "int8x3") if j < 4 else ("fp64",)):
+            specs.append((c, src, 0.3, [0.1, 0.4, 0.7], rho, [0.0], prec))
+            specs.append((c, src, 0.3, [0.2], xs, ys, prec))
+    items = [dict(cache=c, obs_layer=o, zsrc_local=z, z_obs=zo, xs=x, ys=y, precision=p)
+             for c, o, z, zo, x, y, p in specs]
+    for i in (1, 4, 7):
+        x, y, zo = items[i]["xs"], items[i]["ys"], items[i]["z_obs"]
+        items[i]["out"] = torch.empty(len(x) * len(y) * len(zo) * 9, dtype=torch.complex128, device="cuda")
+    for rep in range(2):  # the second pass reuses the slots' workspaces
+        res = ytf.closed_form_G_batch(items)
+        for (c, o, z, zo, x, y, p), r in zip(specs, res):
+            ref = ytf.closed_form_G(c, o, z, zo, x, y, precision=p)
+            if hasattr(r, "cpu"):
+                r = r.cpu().numpy().reshape(3, 3, len(zo), len(y), len(x)).transpose(4, 3, 2, 1, 0)
+            assert np.array_equal(r, ref), (p, len(x), len(y))
+
+
 @pytest.mark.parametrize("idx", [0, 1, 2])
 def test_cavity_response_matches_oracle(ytf, oracle, idx):
     """_cavity_response on the device (forward-only chain in response mode) against the

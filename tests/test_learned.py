@@ -189,3 +189,46 @@ def test_batched_rules_equal_per_stack_rules(L):
             k2, w2 = api.gl_rule(panels, 8, singular=L._sing(P))
             Gk = G(k2, w2)
         assert np.array_equal(k2, kp) and np.array_equal(Gk, gp)
+
+
+def test_cavity_response_batch_equals_single_calls(L):
+    """ytf_cavity_response_batch gives every item's responses bit for bit as its own
+    ytf_cavity_response call (empty items included); a bad item is named in the error."""
+    from yellowthinfilms_b200 import api
+    rng = np.random.default_rng(17)
+    items = []
+    for j in range(5):
+        st, lam = L.film_stack(rng)
+        k0 = 2 * np.pi / lam
+        n = 0 if j == 2 else int(rng.integers(1, 400))
+        items.append((api.Stack(st), k0, 1, k0 * rng.uniform(0.2, 20.0, n)))
+    got = api.cavity_response_batch(items)
+    assert len(got) == len(items)
+    for (st, k0, s, ks), R in zip(items, got):
+        assert len(R) == len(ks)
+        if len(ks):
+            assert np.array_equal(R, api.cavity_response(st, k0, s, ks))
+    bad = list(items)
+    bad[3] = (items[3][0], items[3][1], 3, items[3][3])
+    with pytest.raises(api.YTFError, match="item 3"):
+        api.cavity_response_batch(bad)
+
+
+def test_device_resident_rules_equal_host_rules(L):
+    """learned_rules_batch / plain_rules_batch with G and the acceptance checks in device
+    memory return the same rules and, bit for bit, the same G as the host-array form."""
+    from yellowthinfilms_b200 import api
+    net = _random_net(L, 7)
+    rng = np.random.default_rng(41)
+    probs = []
+    for _ in range(4):
+        st, lam = L.film_stack(rng)
+        k0 = 2 * np.pi / lam
+        probs.append(dict(stack=api.Stack(st), layers=st, k0=k0, source_layer=1, zsrc_local=20.0,
+                          z=np.linspace(60.0, 200.0, 12), rho=np.exp(np.linspace(np.log(0.01 * lam), np.log(5 * lam), 40)),
+                          terms="scattered", h_min=80.0, rho_max=5 * lam, precision="int8x3"))
+    for fn in (lambda d: L.plain_rules_batch(probs, device=d), lambda d: L.learned_rules_batch(net, probs, device=d)):
+        host, dev = fn(False), fn(True)
+        for a, b in zip(host, dev):
+            assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]) and a[3:] == b[3:]
+            assert np.array_equal(a[0], b[0].cpu().numpy())

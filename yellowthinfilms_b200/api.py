@@ -284,6 +284,27 @@ def cavity_response(stack, omega, s, kr, phi=0.0, ctx: Optional[Context] = None)
     return out
 
 
+def cavity_response_batch(items, phi=0.0, ctx: Optional[Context] = None):
+    """cavity_response for many (stack, omega, source_layer, kr) tuples with one device
+    synchronisation (ytf_cavity_response_batch). Returns one response array per item."""
+    items = list(items)
+    if not items:
+        return []
+    sts = [_as_stack(it[0], ctx) for it in items]
+    ctx = ctx or sts[0].ctx
+    ks = [_f64(np.atleast_1d(it[3])) for it in items]
+    counts = np.array([len(k) for k in ks], np.int64)
+    kall = _f64(np.concatenate(ks)) if counts.sum() else np.zeros(1)
+    out = np.zeros(max(1, int(counts.sum())))
+    hs = (ctypes.c_void_p * len(items))(*[st.h.value for st in sts])
+    om = _f64([it[1] for it in items])
+    src = np.array([int(it[2]) for it in items], np.int32)
+    ctx.check(lib().ytf_cavity_response_batch(ctx.h, len(items), hs, ptr(om), ptr(src, _i),
+                                              counts.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), ptr(kall),
+                                              float(phi), ptr(out)))
+    return np.split(out[:int(counts.sum())], np.cumsum(counts)[:-1])
+
+
 def layer_light_lines(layer, omega, phi=0.0):
     """layer_light_lines(layer, ω, φ) (mod_KxGrid.jl:41-59): host arithmetic of libytf."""
     from .materials import stack_arrays
@@ -727,8 +748,12 @@ def gausslegendre(n: int):
 def gl_rule(panels: Sequence, order: int = 8, singular=(), ctx: Optional[Context] = None):
     """Composite Gauss–Legendre rule on `panels` (mod_KxGrid.jl:361-384), on the device."""
     ctx = ctx or default_context()
-    pa = _f64([p[0] for p in panels]) if len(panels) else np.zeros(0)
-    pb = _f64([p[1] for p in panels]) if len(panels) else np.zeros(0)
+    if isinstance(panels, np.ndarray):
+        P = np.asarray(panels, np.float64).reshape(-1, 2)
+        pa, pb = np.ascontiguousarray(P[:, 0]), np.ascontiguousarray(P[:, 1])
+    else:
+        pa = _f64([p[0] for p in panels]) if len(panels) else np.zeros(0)
+        pb = _f64([p[1] for p in panels]) if len(panels) else np.zeros(0)
     s = _f64(list(singular)) if len(singular) else np.zeros(1)
     nodes = np.zeros(len(panels) * order)
     wts = np.zeros(len(panels) * order)
@@ -738,7 +763,15 @@ def gl_rule(panels: Sequence, order: int = 8, singular=(), ctx: Optional[Context
 
 
 def halve_panels(panels):
-    """`panels` with every panel split in two (mod_KxGrid.jl:387-388)."""
+    """`panels` with every panel split in two (mod_KxGrid.jl:387-388). A [n, 2] array gives a
+    [2n, 2] array (the same midpoints (a + b) / 2), a sequence of pairs a list of pairs."""
+    if isinstance(panels, np.ndarray):
+        P = np.asarray(panels, np.float64).reshape(-1, 2)
+        m = (P[:, 0] + P[:, 1]) / 2
+        out = np.empty((2 * len(P), 2))
+        out[0::2, 0], out[0::2, 1] = P[:, 0], m
+        out[1::2, 0], out[1::2, 1] = m, P[:, 1]
+        return out
     out = []
     for a, b in panels:
         m = (a + b) / 2

@@ -43,7 +43,14 @@ struct ytf_ctx {
   // name; the captured pass is served from the plan's own buffers of those sizes
   std::map<std::string, size_t>* ws_record = nullptr;
   std::map<std::string, std::pair<void*, size_t>>* ws_override = nullptr;
+  // side streams of ytf_green_batch: the items of an all-1D batch run round-robin on them,
+  // each slot with its own workspace (names suffixed "#<slot>" while ws_slot > 0)
+  std::vector<cudaStream_t> slot_streams;
+  std::vector<cudaEvent_t> slot_events;
+  int ws_slot = 0;
   ~ytf_ctx() {
+    for (auto s : slot_streams) cudaStreamDestroy(s);
+    for (auto e : slot_events) cudaEventDestroy(e);
     if (stage_ev) cudaEventDestroy(stage_ev);
     if (pinned) cudaFreeHost(pinned);
     for (auto& kv : ws) cudaFree(kv.second.first);
@@ -142,9 +149,10 @@ void ctx_release(ytf_ctx* ctx) {
   if (--ctx->refs <= 0 && ctx->closing) delete ctx;
 }
 
-void* ws_get(ytf_ctx* ctx, const char* name, size_t bytes, cudaError_t* e) {
+void* ws_get(ytf_ctx* ctx, const char* name_, size_t bytes, cudaError_t* e) {
   *e = cudaSuccess;
   if (bytes == 0) bytes = 16;
+  const std::string name = ctx->ws_slot > 0 ? std::string(name_) + "#" + std::to_string(ctx->ws_slot) : std::string(name_);
   if (ctx->ws_override) {
     auto o = ctx->ws_override->find(name);
     if (o == ctx->ws_override->end() || o->second.second < bytes) {
@@ -216,7 +224,26 @@ struct GreenBatch {
   const double* dxs;
   const double* dys;
   unsigned* err;
+  const double* drho = nullptr;  // 1D: the distinct radii (radii_map), pre-uploaded
+  const int* drmap = nullptr;    // 1D: pixel -> radius index
 };
+
+// distinct radii hypot(x_i, y_j) in first-occurrence order over (i fastest, j), as the
+// reference, and each pixel's index into them
+void radii_map(int nx, const double* xs, int ny, const double* ys, std::vector<double>& ur, std::vector<int>& rmap) {
+  const long npix = (long)nx * ny;
+  ur.clear();
+  rmap.assign(npix, 0);
+  std::unordered_map<double, int> idx;
+  idx.reserve(npix * 2);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      double r = std::hypot(xs[i], ys[j]);
+      auto it = idx.find(r);
+      if (it == idx.end()) { idx.emplace(r, (int)ur.size()); rmap[i + (long)nx * j] = (int)ur.size(); ur.push_back(r); }
+      else rmap[i + (long)nx * j] = it->second;
+    }
+}
 
 // allocate the cache's arrays in one block
 int alloc_cache(ytf_ctx* ctx, ytf_cache* c, bool upload_nodes = true) {
@@ -711,6 +738,62 @@ int ytf_cavity_response(ytf_ctx* ctx, const ytf_stack* st, double omega, int sou
   return YTF_OK;
 }
 
+int ytf_cavity_response_batch(ytf_ctx* ctx, int nitems, const ytf_stack* const* stacks, const double* omega,
+                              const int* source_layer, const long* counts, const double* kr, double phi, double* out) {
+  if (!ctx || nitems < 0 || (nitems > 0 && (!stacks || !omega || !source_layer || !counts))) return YTF_ERR_ARG;
+  long total = 0;
+  for (int i = 0; i < nitems; ++i) {
+    const ytf_stack* st = stacks[i];
+    const std::string at = "_cavity_response (item " + std::to_string(i) + "): ";
+    if (counts[i] < 0) return fail(ctx, YTF_ERR_ARG, at + "negative node count");
+    if (!st) return fail(ctx, YTF_ERR_ARG, at + "stack is NULL");
+    if (st->ctx != ctx) return fail(ctx, YTF_ERR_STATE, at + "stack belongs to another context");
+    if (!(1 <= source_layer[i] && source_layer[i] < st->nL))
+      return fail(ctx, YTF_ERR_ARG, at + "source layer " + std::to_string(source_layer[i]) + " outside 1:" +
+                                        std::to_string(st->nL - 1));
+    total += counts[i];
+  }
+  if (total == 0) return YTF_OK;
+  if (!kr || !out) return YTF_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  WS(dk, double, "crb_k", total);
+  WS(dphi, double, "crb_phi", 1);
+  WS(dresp, double, "crb_out", total);
+  WS(dstat, uint8_t, "crb_status", total);
+  int rc;
+  if ((rc = upload(ctx, dk, kr, 8 * (size_t)total))) return rc;
+  if ((rc = upload(ctx, dphi, &phi, 8))) return rc;
+  // each item is its own (kρ, φ) grid of counts[i] x 1 nodes, solved in stream order on the
+  // shared node scratch; one download and one synchronisation for all
+  long off = 0;
+  for (int i = 0; i < nitems; ++i) {
+    const long n = counts[i];
+    if (n == 0) continue;
+    TransferParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.layers = stacks[i]->dev;
+    p.nL = stacks[i]->nL;
+    p.src = source_layer[i];
+    p.nobs = 1;
+    p.obs[0] = source_layer[i];
+    p.omega = omega[i];
+    p.mode = 1;
+    p.Nk = (int)n;
+    p.Np = 1;
+    p.kr = dk + off;
+    p.phi = dphi;
+    p.nout = n;
+    p.status = dstat + off;
+    p.resp = dresp + off;
+    if ((rc = run_transfer(ctx, p, n))) return rc;
+    off += n;
+  }
+  CK(cudaMemcpyAsync(out, dresp, 8 * (size_t)total, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  prof_collect(ctx);
+  return YTF_OK;
+}
+
 int ytf_layer_light_lines(const double* eps, const double* mu, double omega, double phi, double* out, int* n) {
   if (!eps || !n) return YTF_ERR_ARG;
   static const double mu_one[18] = {1, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 1, 0};
@@ -1178,24 +1261,24 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
   if (c->n == 0) {  // an empty rule integrates to zero
     CK(cudaMemsetAsync(G, 0, sizeof(double2) * nout, ctx->stream));
   } else if (!c->is2d) {
-    // distinct radii in first-occurrence order over (i fastest, j), as the reference
     std::vector<double> ur;
-    std::vector<int> rmap(npix);
-    std::unordered_map<double, int> idx;
-    idx.reserve(npix * 2);
-    for (int j = 0; j < ny; ++j)
-      for (int i = 0; i < nx; ++i) {
-        double r = std::hypot(xs[i], ys[j]);
-        auto it = idx.find(r);
-        if (it == idx.end()) { idx.emplace(r, (int)ur.size()); rmap[i + (long)nx * j] = (int)ur.size(); ur.push_back(r); }
-        else rmap[i + (long)nx * j] = it->second;
-      }
+    std::vector<int> rmap;
+    radii_map(nx, xs, ny, ys, ur, rmap);
     int nr = (int)ur.size();
     long nk = c->n;
-    WS(drho, double, "g_rho", nr);
-    WS(drmap, int, "g_rmap", npix);
-    if ((rc = upload(ctx, drho, ur.data(), 8 * (size_t)nr))) return rc;
-    if ((rc = upload(ctx, drmap, rmap.data(), 4 * (size_t)npix))) return rc;
+    const double* drho;
+    const int* drmap;
+    if (gb && gb->drho) {
+      drho = gb->drho;
+      drmap = gb->drmap;
+    } else {
+      WS(urho, double, "g_rho", nr);
+      WS(urmap, int, "g_rmap", npix);
+      if ((rc = upload(ctx, urho, ur.data(), 8 * (size_t)nr))) return rc;
+      if ((rc = upload(ctx, urmap, rmap.data(), 4 * (size_t)npix))) return rc;
+      drho = urho;
+      drmap = urmap;
+    }
     WS(C, double, "g_C", 26 * (size_t)nz * nk);
     WS(P, double, "g_P", 26 * (size_t)nz * nr);
     double *C0 = C, *C1 = C + 10 * (size_t)nz * nk, *C2 = C + 18 * (size_t)nz * nk;
@@ -1434,14 +1517,31 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
   if (!ctx || nb < 0 || (nb > 0 && !d)) return YTF_ERR_ARG;
   if (nb == 0) return YTF_OK;
   CK(cudaSetDevice(ctx->device));
-  // every item's coordinates in one page-locked block, one upload
+  // every item's coordinates (and, for 1D items, its distinct radii and pixel -> radius map)
+  // in one page-locked block, one upload
   size_t tot = 0;
+  bool all1d = nb >= 2;
   for (int i = 0; i < nb; ++i) {
     if (d[i].nz < 0 || d[i].nx < 0 || d[i].ny < 0)
       return fail(ctx, YTF_ERR_ARG, "closed_form_G: negative grid size (batch item " + std::to_string(i) + ")");
     tot += (size_t)d[i].nz + d[i].nx + d[i].ny;
+    if (!d[i].cache || d[i].cache->is2d || d[i].cache->ctx != ctx) all1d = false;
   }
-  double* h = (double*)pinned_staging(ctx, 8 * std::max<size_t>(tot, 1));
+  std::vector<std::vector<double>> ur(nb);
+  std::vector<std::vector<int>> rmap(nb);
+  std::vector<size_t> orho(nb, 0), omap(nb, 0);
+  size_t tot_r = 0, tot_m = 0;
+  for (int i = 0; i < nb; ++i) {
+    if (!d[i].cache || d[i].cache->is2d || !d[i].xs || !d[i].ys) continue;
+    radii_map(d[i].nx, d[i].xs, d[i].ny, d[i].ys, ur[i], rmap[i]);
+    orho[i] = tot_r;
+    omap[i] = tot_m;
+    tot_r += ur[i].size();
+    tot_m += rmap[i].size();
+  }
+  const size_t nd = std::max<size_t>(tot + tot_r, 1);  // doubles, then the int maps
+  const size_t bytes = 8 * nd + 4 * tot_m;
+  double* h = (double*)pinned_staging(ctx, bytes);
   if (!h) return fail(ctx, YTF_ERR_NOMEM, "closed_form_G: page-locked staging allocation failed");
   std::vector<size_t> o(nb);
   size_t k = 0;
@@ -1454,18 +1554,57 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
     if (d[i].ny) std::memcpy(h + k, d[i].ys, 8 * (size_t)d[i].ny);
     k += d[i].ny;
   }
-  WS(dc, double, "gb_coords", std::max<size_t>(tot, 1));
-  WS(err, unsigned, "gb_tc_err", 1);
-  CK(cudaMemcpyAsync(dc, h, 8 * tot, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+  int* hm = (int*)(h + nd);
   for (int i = 0; i < nb; ++i) {
-    GreenBatch gb{dc + o[i], dc + o[i] + d[i].nz, dc + o[i] + d[i].nz + d[i].nx, err};
-    int rc = green_impl(ctx, d[i].cache, d[i].obs_layer, d[i].zsrc_local, d[i].nz, d[i].z_obs, d[i].nx, d[i].xs,
-                        d[i].ny, d[i].ys, d[i].terms, d[i].precision, d[i].out, d[i].out_is_device, &gb);
-    if (rc) {
-      cudaStreamSynchronize(ctx->stream);
-      return rc;
+    if (!ur[i].empty()) std::memcpy(h + tot + orho[i], ur[i].data(), 8 * ur[i].size());
+    if (!rmap[i].empty()) std::memcpy(hm + omap[i], rmap[i].data(), 4 * rmap[i].size());
+  }
+  WS(dc, double, "gb_coords", (bytes + 7) / 8);
+  WS(err, unsigned, "gb_tc_err", 1);
+  CK(cudaMemcpyAsync(dc, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+  const int* dm = (const int*)(dc + nd);
+  // an all-1D batch runs its items round-robin on kSlots side streams (each item is a chain
+  // of small dependent launches; independent items overlap), forked from and joined to the
+  // context's stream
+  constexpr int kSlots = 4;
+  const int nslot = all1d ? std::min(kSlots, nb) : 0;
+  if (nslot) {
+    while ((int)ctx->slot_streams.size() < kSlots) {
+      cudaStream_t s;
+      cudaEvent_t e;
+      CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ctx->slot_streams.push_back(s);
+      ctx->slot_events.push_back(e);
     }
+    CK(cudaEventRecord(ctx->slot_events[0], ctx->stream));
+    for (int s = 0; s < nslot; ++s) CK(cudaStreamWaitEvent(ctx->slot_streams[s], ctx->slot_events[0], 0));
+  }
+  cudaStream_t main = ctx->stream;
+  int rc = YTF_OK;
+  for (int i = 0; i < nb && !rc; ++i) {
+    GreenBatch gb{dc + o[i], dc + o[i] + d[i].nz, dc + o[i] + d[i].nz + d[i].nx, err};
+    if (!ur[i].empty()) {
+      gb.drho = dc + tot + orho[i];
+      gb.drmap = dm + omap[i];
+    }
+    if (nslot) {
+      ctx->stream = ctx->slot_streams[i % nslot];
+      ctx->ws_slot = 1 + i % nslot;
+    }
+    rc = green_impl(ctx, d[i].cache, d[i].obs_layer, d[i].zsrc_local, d[i].nz, d[i].z_obs, d[i].nx, d[i].xs,
+                    d[i].ny, d[i].ys, d[i].terms, d[i].precision, d[i].out, d[i].out_is_device, &gb);
+  }
+  ctx->stream = main;
+  ctx->ws_slot = 0;
+  for (int s = 0; s < nslot; ++s) {
+    cudaEventRecord(ctx->slot_events[s], ctx->slot_streams[s]);
+    cudaStreamWaitEvent(main, ctx->slot_events[s], 0);
+  }
+  if (rc) {
+    cudaStreamSynchronize(main);
+    return rc;
   }
   unsigned herr = 0;
   CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));

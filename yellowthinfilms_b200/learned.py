@@ -51,9 +51,9 @@ def scan_grid(k0, n):
     return k0 * np.exp(np.linspace(np.log(K_LO), np.log(K_HI), n))
 
 
-def features(stack, k0, ks):
-    """[len(ks), 154] float32: per layer (up to 8) Re and Im of the 9 ε entries / 10 and the
-    thickness in wavelengths; then λ_ref / λ and k / (K_HI k0)."""
+def feature_row(stack, k0):
+    """The k-independent part of a feature row (float32 [154], last entry 0): per layer (up
+    to 8) Re and Im of the 9 ε entries / 10 and the thickness in wavelengths; then λ_ref / λ."""
     _, _, eps, _, d = stack_arrays(stack)
     row = np.zeros(N_FEATURES)
     for l in range(min(len(stack), MAX_LAYERS)):
@@ -61,9 +61,19 @@ def features(stack, k0, ks):
         row[19 * l + 9:19 * l + 18] = eps[l].imag / 10.0
         row[19 * l + 18] = d[l] * k0 / (2 * np.pi)
     row[-2] = k0 * LAMBDA_REF / (2 * np.pi)
+    return row.astype(np.float32)
+
+
+def k_feature(k0, ks):
+    """The last feature column, k / (K_HI k0) (float32)."""
+    return (np.asarray(ks) / (K_HI * k0)).astype(np.float32)
+
+
+def features(stack, k0, ks):
+    """[len(ks), 154] float32: feature_row with k / (K_HI k0) as the last column."""
     X = np.empty((len(ks), N_FEATURES), np.float32)
-    X[:] = row.astype(np.float32)
-    X[:, -1] = (np.asarray(ks) / (K_HI * k0)).astype(np.float32)
+    X[:] = feature_row(stack, k0)
+    X[:, -1] = k_feature(k0, ks)
     return X
 
 
@@ -152,6 +162,22 @@ def train(net, X, T, steps, batch=4096, lr=1e-3, seed=1):
     return losses
 
 
+def predict_batch(net, stacks, n_k=4096, chunk=256):
+    """The network's outputs (float64 [len(stacks) n_k, 2]) on every (layers, k0) item's scan
+    grid: the feature rows are repeated over the grid on the device (the same float32 inputs
+    as features()), chunk items per forward."""
+    import torch
+    out = []
+    for c0 in range(0, len(stacks), chunk):
+        part = stacks[c0:c0 + chunk]
+        rows = torch.from_numpy(np.stack([feature_row(st, k0) for st, k0 in part])).cuda()
+        kf = torch.from_numpy(np.stack([k_feature(k0, scan_grid(k0, n_k)) for _, k0 in part])).cuda()
+        X = rows[:, None, :].repeat(1, n_k, 1)
+        X[:, :, -1] = kf
+        out.append(net.forward(X.view(-1, N_FEATURES)).cpu().numpy().astype(np.float64))
+    return np.concatenate(out) if out else np.zeros((0, 2))
+
+
 def _score_candidates(ks, logit, cand):
     """cand plus the local maxima of the pole score σ(logit) above 0.3 that lie more than 2Γ
     from every candidate so far (in increasing k), each with Γ = 2e-3 k."""
@@ -173,17 +199,41 @@ def propose_poles(net, stack, k0, n_k=4096):
     return sorted(_score_candidates(ks, out[:, 1], cand))
 
 
+def _windows(cand, n_local):
+    """The log windows (±6 max(Γ/q, 2e-3), n_local points) around the candidates."""
+    wins = []
+    for q, G in cand:
+        w = max(G / q, 2e-3)
+        wins.append(q * np.exp(np.linspace(-6 * w, 6 * w, n_local)))
+    return wins
+
+
 def refine_poles(stack, k0, source_layer, cand, n_local=129, ctx=None):
     """(q, Γ) of each candidate from the EXACT cavity response sampled on a small log window
     around it (±6 max(Γ/q, 2e-3)), all windows in one device call; candidates whose window
     shows no peak are dropped."""
     if not cand:
         return []
-    wins = []
-    for q, G in cand:
-        w = max(G / q, 2e-3)
-        wins.append(q * np.exp(np.linspace(-6 * w, 6 * w, n_local)))
+    wins = _windows(cand, n_local)
     R = api.cavity_response(stack, k0, source_layer, np.concatenate(wins), ctx=ctx)
+    return _poles_from_windows(wins, R, n_local)
+
+
+def refine_poles_batch(items, n_local=129, ctx=None):
+    """refine_poles for many (stack, k0, source_layer, cand) items: every window of every
+    item in ONE device call (ytf_cavity_response_batch). Returns the poles per item."""
+    wins = [_windows(c, n_local) for (_, _, _, c) in items]
+    idx = [i for i, w in enumerate(wins) if w]
+    Rs = api.cavity_response_batch([(items[i][0], items[i][1], items[i][2], np.concatenate(wins[i])) for i in idx],
+                                   ctx=ctx)
+    out = [[] for _ in items]
+    for i, R in zip(idx, Rs):
+        out[i] = _poles_from_windows(wins[i], R, n_local)
+    return out
+
+
+def _poles_from_windows(wins, R, n_local):
+    """Per window the strongest peak of the sampled response, merged across windows."""
     out = []
     for i, ks in enumerate(wins):
         y = np.log(np.maximum(R[i * n_local:(i + 1) * n_local], 1e-12))
@@ -247,17 +297,39 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
 # synthesis over the problems still open (ytf_transfer_batch + ytf_green_batch), so the
 # time follows the nodes solved rather than per-call latency.
 # ------------------------------------------------------------------------------------
-def batch_G(problems, rules, ctx=None):
+def batch_G(problems, rules, ctx=None, device=False):
     """G on each problem's rule: problems are dicts with stack (api.Stack or layers), k0,
-    source_layer, zsrc_local, z (rows), rho (radii, on the x axis), terms; rules (k, w)."""
+    source_layer, zsrc_local, z (rows), rho (radii, on the x axis), terms and optionally the
+    synthesis precision ("fp64" by default, "int8x3"); rules (k, w). With ``device`` the G
+    arrays stay in device memory (complex128 CUDA tensors of the same (ρ, 1, z, 3, 3) shape)."""
     if not problems:
         return []
     caches = api.build_cavity_transfer_batch(
         [dict(stack=P["stack"], omega=P["k0"], source_layer=P["source_layer"], kx_nodes=k, wt_nodes=w,
               obs_layers=[P["source_layer"]]) for P, (k, w) in zip(problems, rules)], ctx=ctx)
-    return api.closed_form_G_batch(
-        [dict(cache=c, obs_layer=P["source_layer"], zsrc_local=P["zsrc_local"], z_obs=P["z"], xs=P["rho"],
-              ys=[0.0], terms=P.get("terms", "all")) for P, c in zip(problems, caches)])
+    items = [dict(cache=c, obs_layer=P["source_layer"], zsrc_local=P["zsrc_local"], z_obs=P["z"], xs=P["rho"],
+                  ys=[0.0], terms=P.get("terms", "all"), precision=P.get("precision", "fp64"))
+             for P, c in zip(problems, caches)]
+    if not device:
+        return api.closed_form_G_batch(items)
+    import torch
+    shapes = [(len(P["rho"]), 1, len(P["z"])) for P in problems]
+    outs = [torch.empty(nx * ny * nz * 9, dtype=torch.complex128, device="cuda") for nx, ny, nz in shapes]
+    api.closed_form_G_batch([dict(it, out=o) for it, o in zip(items, outs)])
+    return [o.view(3, 3, nz, ny, nx).permute(4, 3, 2, 1, 0) for o, (nx, ny, nz) in zip(outs, shapes)]
+
+
+def _agree(pairs, rtol):
+    """Per (G, G_halved) pair: ‖G - G_h‖ ≤ rtol ‖G_h‖ (numpy arrays, or device tensors with
+    one host read for all pairs)."""
+    if not pairs:
+        return []
+    if isinstance(pairs[0][1], np.ndarray):
+        return [np.linalg.norm(a - b) <= rtol * np.linalg.norm(b) for a, b in pairs]
+    import torch
+    nrm = torch.stack([torch.stack([torch.linalg.vector_norm(a - b), torch.linalg.vector_norm(b)]) for a, b in pairs])
+    nrm = nrm.cpu().numpy()
+    return [bool(d <= rtol * n) for d, n in nrm]
 
 
 def _sing(P):
@@ -265,22 +337,24 @@ def _sing(P):
     return sorted(set(api.layer_light_lines(st[0], P["k0"])) | set(api.layer_light_lines(st[-1], P["k0"])))
 
 
-def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, ctx, out):
+def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, ctx, out, device=False):
     """Halve the open problems' rules until G agrees with G on the halved rule (the plain
     method's own check), all open problems per batched level; fills out[i] = (G, k, w,
     halvings, converged)."""
     open_ = list(idx)
+    sing = {i: _sing(problems[i]) for i in open_}
     for h in range(max_halvings + 1):
         if not open_:
             break
         halv = {}
         for i in open_:
-            p2 = api.halve_panels([tuple(p) for p in panels[i]])
-            halv[i] = (p2, api.gl_rule(p2, order, singular=_sing(problems[i]), ctx=ctx))
-        Gh = batch_G([problems[i] for i in open_], [halv[i][1] for i in open_], ctx=ctx)
+            p2 = api.halve_panels(np.asarray(panels[i], np.float64).reshape(-1, 2))
+            halv[i] = (p2, api.gl_rule(p2, order, singular=sing[i], ctx=ctx))
+        Gh = batch_G([problems[i] for i in open_], [halv[i][1] for i in open_], ctx=ctx, device=device)
+        ok = _agree([(G[i], g) for i, g in zip(open_, Gh)], rtol)
         still = []
-        for i, g in zip(open_, Gh):
-            if np.linalg.norm(G[i] - g) <= rtol * np.linalg.norm(g):
+        for i, g, good in zip(open_, Gh, ok):
+            if good:
                 out[i] = (G[i], rules[i][0], rules[i][1], h, True)
             else:
                 panels[i], rules[i], G[i] = halv[i][0], halv[i][1], g
@@ -290,42 +364,45 @@ def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, c
         out[i] = (G[i], rules[i][0], rules[i][1], max_halvings + 1, False)
 
 
-def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None):
+def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, device=False):
     """The plain fixed rule (no pole knowledge: light-line breaks, u² substitution) of every
-    problem, halved until two levels agree. Returns [(G, k, w, halvings, converged)]."""
+    problem, halved until two levels agree. Returns [(G, k, w, halvings, converged)]; with
+    ``device`` every G (and the acceptance check) stays in device memory."""
     rules, panels = [], []
     for P in problems:
         k, w, info = api.point_kx_grid(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
                                        rho_max=P["rho_max"], scan=False, order=order, ctx=ctx)
         rules.append((k, w))
         panels.append(info["panels"])
-    G = batch_G(problems, rules, ctx=ctx)
+    G = batch_G(problems, rules, ctx=ctx, device=device)
     out = [None] * len(problems)
-    _refine_levels(problems, range(len(problems)), rules, panels, G, rtol, max_halvings, order, ctx, out)
+    _refine_levels(problems, range(len(problems)), rules, panels, G, rtol, max_halvings, order, ctx, out, device)
     return out
 
 
-def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=None):
-    """learned_rule for every problem: one network forward over all problems' scan grids,
-    the exact window sampling and fixed_kρ_rule per problem, then the acceptance check and any
+def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=None, device=False):
+    """learned_rule for every problem: the network over all problems' scan grids (features
+    formed on the device), the exact window sampling of all problems in one device call,
+    fixed_kρ_rule per problem, then the acceptance check and any
     plain refinement in batched levels; a problem that never converges falls back to the
-    scanned rule. Returns [(G, k, w, accepted, halvings)]."""
+    scanned rule. Returns [(G, k, w, accepted, halvings)]; ``device`` as plain_rules_batch."""
     n_k = 4096
-    feats = [features(P["layers"], P["k0"], scan_grid(P["k0"], n_k)) for P in problems]
-    pred = net.forward(np.concatenate(feats)).astype(np.float64) if problems else np.zeros((0, 2))
-    rules, panels = [], []
+    pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
+    cands = []
     for j, P in enumerate(problems):
         ks = scan_grid(P["k0"], n_k)
         o = pred[j * n_k:(j + 1) * n_k]
-        cand = _score_candidates(ks, o[:, 1], peaks(ks, o[:, 0] * LOG_SCALE))
-        poles = refine_poles(P["stack"], P["k0"], P["source_layer"], sorted(cand), ctx=ctx)
+        cands.append(sorted(_score_candidates(ks, o[:, 1], peaks(ks, o[:, 0] * LOG_SCALE))))
+    polesets = refine_poles_batch([(P["stack"], P["k0"], P["source_layer"], c) for P, c in zip(problems, cands)], ctx=ctx)
+    rules, panels = [], []
+    for P, poles in zip(problems, polesets):
         k, w, info = api.grid_from_poles(P["stack"], P["k0"], P["source_layer"], poles, h_min=P["h_min"],
                                          rho_max=P["rho_max"], order=order, rtol=rtol, ctx=ctx)
         rules.append((k, w))
         panels.append(info["panels"])
-    G = batch_G(problems, rules, ctx=ctx)
+    G = batch_G(problems, rules, ctx=ctx, device=device)
     out = [None] * len(problems)
-    _refine_levels(problems, range(len(problems)), rules, panels, G, rtol, max_halvings, order, ctx, out)
+    _refine_levels(problems, range(len(problems)), rules, panels, G, rtol, max_halvings, order, ctx, out, device)
     fall = [i for i, r in enumerate(out) if not r[4]]
     if fall:
         fr = []
@@ -334,7 +411,7 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
             k, w, _ = api.point_kx_grid(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
                                         rho_max=P["rho_max"], order=order, rtol=rtol, ctx=ctx)
             fr.append((k, w))
-        Gf = batch_G([problems[i] for i in fall], fr, ctx=ctx)
+        Gf = batch_G([problems[i] for i in fall], fr, ctx=ctx, device=device)
         for i, (k, w), g in zip(fall, fr, Gf):
             out[i] = (g, k, w, out[i][3], False)
     return [(g, k, w, conv and h == 0, h) for (g, k, w, h, conv) in out]
