@@ -1,0 +1,74 @@
+"""Host logic of the learned node placement (no GPU): the peak finder on sampled
+log-responses (the scan's rule of real_axis_poles, mod_KSpaceFeatures.jl:151-204, on
+samples) against a sample-by-sample restatement of the same walk."""
+import numpy as np
+
+
+def _peaks_loop(ks, logR, prominence=np.log(1.05), floor_rel=1e-6):
+    y = np.asarray(logR, np.float64)
+    n = len(y)
+    if n < 3:
+        return []
+    ymin = max(y.max() + np.log(floor_rel), np.log(1e-10))
+    lk = np.log(ks)
+    step = lk[1] - lk[0]
+    W = int(np.ceil(np.log(4.0) / step))
+    out = []
+    for i in range(1, n - 1):
+        if not (y[i] > y[i - 1] and y[i] >= y[i + 1] and y[i] >= ymin):
+            continue
+        lo, hi = max(0, i - W), min(n - 1, i + W)
+        jl = i
+        while jl > lo and y[jl - 1] <= y[i]:
+            jl -= 1
+        jr = i
+        while jr < hi and y[jr + 1] <= y[i]:
+            jr += 1
+        base = max(y[jl:i + 1].min(), y[i:jr + 1].min())
+        if y[i] - base < prominence:
+            continue
+        den = y[i - 1] - 2 * y[i] + y[i + 1]
+        off = 0.5 * (y[i - 1] - y[i + 1]) / den if den < 0 else 0.0
+        q = float(np.exp(lk[i] + np.clip(off, -0.5, 0.5) * step))
+        P = np.exp(y[i])
+        lvl = np.log(np.exp(base) + (P - np.exp(base)) / np.sqrt(2.0))
+        G = np.inf
+        for rng_ in (range(i, jl - 1, -1), range(i, jr + 1)):
+            prev = None
+            for j in rng_:
+                if y[j] <= lvl and prev is not None:
+                    t = (y[prev] - lvl) / (y[prev] - y[j])
+                    kc = np.exp(lk[prev] + t * (lk[j] - lk[prev]))
+                    G = min(G, abs(kc - q))
+                    break
+                prev = j
+        if np.isfinite(G) and G > 0:
+            out.append((q, float(G)))
+    return out
+
+
+def test_peaks_equal_the_sample_walk():
+    """learned.peaks (vectorised walks) returns exactly the (q, Γ) list of the sample-by-sample
+    walk: Lorentzian peaks of several widths on a sloped background, with noise, plateaus, a
+    peak next to the last sample, fine and coarse grids."""
+    from yellowthinfilms_b200 import learned as L
+    rng = np.random.default_rng(12)
+    cases = found = 0
+    for n in (129, 700, 2048, 4096):
+        for trial in range(12):
+            ks = np.exp(np.linspace(np.log(0.25), np.log(20.0), n))
+            y = -0.3 * np.log(ks)
+            for _ in range(int(rng.integers(0, 5))):
+                q, g, a = rng.uniform(0.3, 19.0), 10 ** rng.uniform(-3, -0.5), rng.uniform(0.5, 40.0)
+                y = y + np.log1p(a / (1 + ((ks - q) / g) ** 2))
+            if trial % 3 == 1:
+                y = y + rng.normal(0.0, 0.02, n)
+            if trial % 3 == 2:
+                y = np.round(y, 1)  # plateaus: equal neighbours
+            if trial == 5:
+                y[-2] = y.max() + 1.0
+            got = L.peaks(ks, y)
+            assert got == _peaks_loop(ks, y), (n, trial)
+            cases += 1
+            found += len(got)
+    assert cases == 48 and found > 40

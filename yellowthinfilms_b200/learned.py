@@ -95,12 +95,11 @@ def peaks(ks, logR, prominence=np.log(1.05), floor_rel=1e-6):
     for i in cand:
         i = int(i)
         lo, hi = max(0, i - W), min(n - 1, i + W)
-        jl = i
-        while jl > lo and y[jl - 1] <= y[i]:
-            jl -= 1
-        jr = i
-        while jr < hi and y[jr + 1] <= y[i]:
-            jr += 1
+        # the run of samples ≤ y[i] on each side (bounded by the ±W window)
+        above = np.nonzero(y[lo:i] > y[i])[0]
+        jl = lo + int(above[-1]) + 1 if len(above) else lo
+        above = np.nonzero(y[i + 1:hi + 1] > y[i])[0]
+        jr = i + int(above[0]) if len(above) else hi
         base = max(y[jl:i + 1].min(), y[i:jr + 1].min())
         if y[i] - base < prominence:
             continue
@@ -110,15 +109,16 @@ def peaks(ks, logR, prominence=np.log(1.05), floor_rel=1e-6):
         P = np.exp(y[i])
         lvl = np.log(np.exp(base) + (P - np.exp(base)) / np.sqrt(2.0))
         G = np.inf
-        for rng_ in (range(i, jl - 1, -1), range(i, jr + 1)):
-            prev = None
-            for j in rng_:
-                if y[j] <= lvl and prev is not None:
-                    t = (y[prev] - lvl) / (y[prev] - y[j])
-                    kc = np.exp(lk[prev] + t * (lk[j] - lk[prev]))
-                    G = min(G, abs(kc - q))
-                    break
-                prev = j
+        # the first sample at or below the half-power level on each side, interpolated
+        # linearly in log k against its neighbour towards the peak
+        for js, dj in ((np.arange(i - 1, jl - 1, -1), 1), (np.arange(i + 1, jr + 1), -1)):
+            hit = np.nonzero(y[js] <= lvl)[0]
+            if len(hit):
+                j = int(js[hit[0]])
+                prev = j + dj
+                t = (y[prev] - lvl) / (y[prev] - y[j])
+                kc = np.exp(lk[prev] + t * (lk[j] - lk[prev]))
+                G = min(G, abs(kc - q))
         if np.isfinite(G) and G > 0:
             out.append((q, float(G)))
     return out
