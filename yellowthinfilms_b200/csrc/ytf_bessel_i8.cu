@@ -167,15 +167,17 @@ __global__ void k_aimg_bessel(BesselI8 p) {
 }
 
 // k_aimg_bessel for all three orders at once: J_0 and J_1 once per (ρ, k), J_2 from them
-// (series below |x| = 1, recurrence above, as bessel_j012), three images in the same layout
+// (series below |x| = 1, recurrence above, as bessel_j012), three images in the same layout.
+// One thread per 4 consecutive nodes of a radius (one 32-bit word of each digit plane): the
+// FP64 Bessel chains are latency-bound, so short chains and many threads.
 __global__ void __launch_bounds__(256) k_aimg_bessel3(BesselI8 p, uint8_t* __restrict__ A0, uint8_t* __restrict__ A1,
                                                        uint8_t* __restrict__ A2) {
-  const long groups = p.kchunk / 16;
+  const long words = p.kchunk / 4;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long total = (long)p.ntile_m * BI_M * p.nchunk * groups;
+  const long total = (long)p.ntile_m * BI_M * p.nchunk * words;
   if (t >= total) return;
-  const long g = t % groups;
-  long rest = t / groups;
+  const long wq = t % words;
+  long rest = t / words;
   const int z = (int)(rest % p.nchunk);
   rest /= p.nchunk;
   const int row = (int)(rest % BI_M);
@@ -183,41 +185,34 @@ __global__ void __launch_bounds__(256) k_aimg_bessel3(BesselI8 p, uint8_t* __res
   const int r = mt * BI_M + row;
   const bool rv = r < p.M;
   const double rho = rv ? p.rho[r] : 0.0;
-  uint32_t w[3][3][4];  // [order][plane][word]
+  const long g = wq / 4;
+  const int q = (int)(wq % 4);
+  uint32_t b[3][3][4];  // [order][plane][node]
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    uint32_t b[3][3][4];
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
-      double v[3] = {0.0, 0.0, 0.0};
-      if (rv && k < p.K) {
-        const double x = p.kr[k] * rho;
-        v[0] = j0(x);
-        v[1] = j1(x);
-        if (fabs(x) < 1.0) {
-          double h2 = 0.25 * x * x, tt = 0.5 * h2, ss = tt;
-          for (int m = 0; m < 12; ++m) {
-            tt *= -h2 / ((m + 1.0) * (m + 3.0));
-            ss += tt;
-          }
-          v[2] = ss;
-        } else {
-          v[2] = (2.0 / x) * v[1] - v[0];
+  for (int h = 0; h < 4; ++h) {
+    const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
+    double v[3] = {0.0, 0.0, 0.0};
+    if (rv && k < p.K) {
+      const double x = p.kr[k] * rho;
+      v[0] = j0(x);
+      v[1] = j1(x);
+      if (fabs(x) < 1.0) {
+        double h2 = 0.25 * x * x, tt = 0.5 * h2, ss = tt;
+        for (int m = 0; m < 12; ++m) {
+          tt *= -h2 / ((m + 1.0) * (m + 3.0));
+          ss += tt;
         }
-      }
-#pragma unroll
-      for (int o = 0; o < 3; ++o) {
-        uint32_t d0, d1, d2;
-        digits3b(__double2int_rn(v[o] * BI_SCALE), d0, d1, d2);
-        b[o][0][h] = d0; b[o][1][h] = d1; b[o][2][h] = d2;
+        v[2] = ss;
+      } else {
+        v[2] = (2.0 / x) * v[1] - v[0];
       }
     }
 #pragma unroll
-    for (int o = 0; o < 3; ++o)
-#pragma unroll
-      for (int pl = 0; pl < 3; ++pl)
-        w[o][pl][q] = b[o][pl][0] | (b[o][pl][1] << 8) | (b[o][pl][2] << 16) | (b[o][pl][3] << 24);
+    for (int o = 0; o < 3; ++o) {
+      uint32_t d0, d1, d2;
+      digits3b(__double2int_rn(v[o] * BI_SCALE), d0, d1, d2);
+      b[o][0][h] = d0; b[o][1][h] = d1; b[o][2][h] = d2;
+    }
   }
   const long nstage = p.kchunk / BI_NODES;
   const int s = (int)(g / 4), kb = (int)(g % 4) * 16;
@@ -228,13 +223,13 @@ __global__ void __launch_bounds__(256) k_aimg_bessel3(BesselI8 p, uint8_t* __res
   for (int o = 0; o < 3; ++o)
 #pragma unroll
     for (int pl = 0; pl < 3; ++pl)
-      *reinterpret_cast<uint4*>(out[o] + (size_t)pl * BI_M * 64 + plane_off(row, kb)) =
-          make_uint4(w[o][pl][0], w[o][pl][1], w[o][pl][2], w[o][pl][3]);
+      *reinterpret_cast<uint32_t*>(out[o] + (size_t)pl * BI_M * 64 + plane_off(row, kb) + 4 * q) =
+          b[o][pl][0] | (b[o][pl][1] << 8) | (b[o][pl][2] << 16) | (b[o][pl][3] << 24);
 }
 
 cudaError_t launch_bessel_i8_aimg3(const BesselI8& p, uint8_t* A0, uint8_t* A1, uint8_t* A2, cudaStream_t s) {
   if (p.M <= 0 || p.K <= 0) return cudaSuccess;
-  const long total = (long)p.ntile_m * BI_M * p.nchunk * (p.kchunk / 16);
+  const long total = (long)p.ntile_m * BI_M * p.nchunk * (p.kchunk / 4);
   k_aimg_bessel3<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p, A0, A1, A2);
   return cudaGetLastError();
 }

@@ -162,7 +162,7 @@ def train(net, X, T, steps, batch=4096, lr=1e-3, seed=1):
     return losses
 
 
-def predict_batch(net, stacks, n_k=4096, chunk=256):
+def predict_batch(net, stacks, n_k=2048, chunk=256):
     """The network's outputs (float64 [len(stacks) n_k, 2]) on every (layers, k0) item's scan
     grid: the feature rows are repeated over the grid on the device (the same float32 inputs
     as features()), chunk items per forward."""
@@ -190,7 +190,7 @@ def _score_candidates(ks, logit, cand):
     return cand
 
 
-def propose_poles(net, stack, k0, n_k=4096):
+def propose_poles(net, stack, k0, n_k=2048):
     """Candidate real-axis poles (q, Γ) from the network: peaks of its predicted response and
     maxima of its pole score (> 0.3) on a fine log grid."""
     ks = scan_grid(k0, n_k)
@@ -380,13 +380,17 @@ def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, de
     return out
 
 
-def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=None, device=False):
+def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=None, device=False, build_rtol=None,
+                        n_scan=2048):
     """learned_rule for every problem: the network over all problems' scan grids (features
     formed on the device), the exact window sampling of all problems in one device call,
     fixed_kρ_rule per problem, then the acceptance check and any
     plain refinement in batched levels; a problem that never converges falls back to the
-    scanned rule. Returns [(G, k, w, accepted, halvings)]; ``device`` as plain_rules_batch."""
-    n_k = 4096
+    scanned rule. Returns [(G, k, w, accepted, halvings)]; ``device`` as plain_rules_batch.
+    ``build_rtol`` (default rtol): the tolerance the proposed rules are built for; the
+    acceptance check always uses rtol. ``n_scan``: points of the log grid the network is
+    evaluated on per problem."""
+    n_k = n_scan
     pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
     cands = []
     for j, P in enumerate(problems):
@@ -397,7 +401,8 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     rules, panels = [], []
     for P, poles in zip(problems, polesets):
         k, w, info = api.grid_from_poles(P["stack"], P["k0"], P["source_layer"], poles, h_min=P["h_min"],
-                                         rho_max=P["rho_max"], order=order, rtol=rtol, ctx=ctx)
+                                         rho_max=P["rho_max"], order=order,
+                                         rtol=rtol if build_rtol is None else build_rtol, ctx=ctx)
         rules.append((k, w))
         panels.append(info["panels"])
     G = batch_G(problems, rules, ctx=ctx, device=device)
