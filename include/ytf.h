@@ -259,6 +259,13 @@ int ytf_gauss_legendre(int n, double* x, double* w);
 int ytf_gl_rule(ytf_ctx* ctx, int npanels, const double* pa, const double* pb, int order, int nsing,
                 const double* singular, double* nodes, double* weights);
 
+/* ytf_gl_rule for many panel sets with one synchronisation (gl_rule, mod_KxGrid.jl:361-384,
+ * per set): set j has npanels[j] panels (pa, pb concatenated over the sets) and nsing[j]
+ * singular points (concatenated likewise); its npanels[j] x order nodes and weights go to the
+ * same places of nodes and weights. Every set's rule equals its own ytf_gl_rule call. */
+int ytf_gl_rule_batch(ytf_ctx* ctx, int nsets, const int* npanels, const double* pa, const double* pb, int order,
+                      const int* nsing, const double* singular, double* nodes, double* weights);
+
 /* Allocation-free variant of ytf_green for 2D caches (no counterpart in the reference).
  * For callers that must not have the library allocate device memory: a host that owns all
  * device memory through its own pool (e.g. a Julia CUDA.jl session or a caching

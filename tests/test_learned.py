@@ -232,3 +232,24 @@ def test_device_resident_rules_equal_host_rules(L):
         for a, b in zip(host, dev):
             assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]) and a[3:] == b[3:]
             assert np.array_equal(a[0], b[0].cpu().numpy())
+
+
+def test_gl_rule_batch_equals_single_calls(L):
+    """ytf_gl_rule_batch: every panel set's nodes and weights bit for bit as its own
+    ytf_gl_rule call (each set with its own singular points; empty sets included)."""
+    from yellowthinfilms_b200 import api
+    rng = np.random.default_rng(5)
+    sets = []
+    for j in range(6):
+        n = 0 if j == 3 else int(rng.integers(1, 60))
+        e = np.sort(rng.uniform(0.0, 3.0, n + 1))
+        P = np.stack([e[:-1], e[1:]], 1)
+        sing = [float(e[0]), float(e[-1])] if j % 2 == 0 and n else []
+        sets.append((P, sing))
+    got = api.gl_rule_batch(sets, 8)
+    for (P, sing), (k, w) in zip(sets, got):
+        if len(P) == 0:
+            assert len(k) == 0 and len(w) == 0
+            continue
+        k1, w1 = api.gl_rule(P, 8, singular=sing)
+        assert np.array_equal(k, k1) and np.array_equal(w, w1)

@@ -78,6 +78,7 @@ SIGNATURES = {
                                            _d]),
     "ytf_cavity_response_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), _d, _i,
                                                  ctypes.POINTER(ctypes.c_long), _d, ctypes.c_double, _d]),
+    "ytf_gl_rule_batch": (ctypes.c_int, [_vp, ctypes.c_int, _i, _d, _d, ctypes.c_int, _i, _d, _d, _d]),
     "ytf_layer_light_lines": (ctypes.c_int, [_d, _d, ctypes.c_double, ctypes.c_double, _d, _i]),
     "ytf_nodes_1d": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams), ctypes.c_long, _d,
                                     _d, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(GridInfo)]),

@@ -762,6 +762,28 @@ def gl_rule(panels: Sequence, order: int = 8, singular=(), ctx: Optional[Context
     return nodes, wts
 
 
+def gl_rule_batch(sets, order: int = 8, ctx: Optional[Context] = None):
+    """gl_rule for many (panels, singular) sets with one device call (ytf_gl_rule_batch);
+    panels as [n, 2] arrays or pair sequences. Returns [(nodes, weights)] in order, each equal
+    to its own gl_rule call."""
+    ctx = ctx or default_context()
+    if not sets:
+        return []
+    P = [np.asarray(p, np.float64).reshape(-1, 2) for p, _ in sets]
+    S = [_f64(list(sg)) for _, sg in sets]
+    npan = np.array([len(p) for p in P], np.int32)
+    nsing = np.array([len(sg) for sg in S], np.int32)
+    pa = _f64(np.concatenate([p[:, 0] for p in P])) if npan.sum() else np.zeros(1)
+    pb = _f64(np.concatenate([p[:, 1] for p in P])) if npan.sum() else np.zeros(1)
+    sg = _f64(np.concatenate(S)) if nsing.sum() else np.zeros(1)
+    tot = int(npan.sum()) * order
+    nodes, wts = np.zeros(max(tot, 1)), np.zeros(max(tot, 1))
+    ctx.check(lib().ytf_gl_rule_batch(ctx.h, len(sets), ptr(npan, _i), ptr(pa), ptr(pb), int(order), ptr(nsing, _i),
+                                      ptr(sg), ptr(nodes), ptr(wts)))
+    cuts = np.cumsum(npan.astype(np.int64) * order)[:-1]
+    return list(zip(np.split(nodes[:tot], cuts), np.split(wts[:tot], cuts)))
+
+
 def halve_panels(panels):
     """`panels` with every panel split in two (mod_KxGrid.jl:387-388). A [n, 2] array gives a
     [2n, 2] array (the same midpoints (a + b) / 2), a sequence of pairs a list of pairs."""

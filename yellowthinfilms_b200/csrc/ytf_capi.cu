@@ -1664,6 +1664,47 @@ int ytf_gl_rule(ytf_ctx* ctx, int npanels, const double* pa, const double* pb, i
   return YTF_OK;
 }
 
+int ytf_gl_rule_batch(ytf_ctx* ctx, int nsets, const int* npanels, const double* pa, const double* pb, int order,
+                      const int* nsing, const double* singular, double* nodes, double* weights) {
+  if (!ctx || nsets < 0 || order < 1 || (nsets > 0 && (!npanels || !nsing))) return YTF_ERR_ARG;
+  size_t np = 0, ns = 0;
+  for (int j = 0; j < nsets; ++j) {
+    if (npanels[j] < 0 || nsing[j] < 0) return fail(ctx, YTF_ERR_ARG, "gl_rule: negative count (set " + std::to_string(j) + ")");
+    np += npanels[j];
+    ns += nsing[j];
+  }
+  if (np == 0) return YTF_OK;
+  if (!pa || !pb || !nodes || !weights || (ns > 0 && !singular)) return YTF_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<double> xi(order), wx(order);
+  ytf_gauss_legendre(order, xi.data(), wx.data());
+  // each panel's substitution side from its own set's singular points, as ytf_gl_rule
+  std::vector<int> side(np);
+  size_t p0 = 0, s0 = 0;
+  for (int j = 0; j < nsets; ++j) {
+    std::set<double> S(singular + s0, singular + s0 + nsing[j]);
+    for (int i = 0; i < npanels[j]; ++i) {
+      const size_t q = p0 + i;
+      side[q] = S.count(pa[q]) ? 1 : (S.count(pb[q]) ? -1 : 0);
+    }
+    p0 += npanels[j];
+    s0 += nsing[j];
+  }
+  const size_t tot = np * order;
+  WS(buf, double, "glb_buf", 2 * np + 2 * (size_t)order + 2 * tot);
+  WS(dside, int, "glb_side", np);
+  double *da = buf, *db = buf + np, *dxi = buf + 2 * np, *dwx = dxi + order, *dn = dwx + order, *dw = dn + tot;
+  int rc;
+  if ((rc = upload(ctx, da, pa, 8 * np)) || (rc = upload(ctx, db, pb, 8 * np)) || (rc = upload(ctx, dxi, xi.data(), 8 * (size_t)order)) ||
+      (rc = upload(ctx, dwx, wx.data(), 8 * (size_t)order)) || (rc = upload(ctx, dside, side.data(), 4 * np)))
+    return rc;
+  CK(LAUNCH("k_gl_nodes", launch_gl_nodes((int)np, da, db, dside, dxi, dwx, order, dn, dw, ctx->stream)));
+  CK(cudaMemcpyAsync(nodes, dn, 8 * tot, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(weights, dw, 8 * tot, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return YTF_OK;
+}
+
 }  // extern "C"
 
 // =====================================================================================

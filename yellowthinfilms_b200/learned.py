@@ -339,18 +339,26 @@ def _sing(P):
 
 def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, ctx, out, device=False):
     """Halve the open problems' rules until G agrees with G on the halved rule (the plain
-    method's own check), all open problems per batched level; fills out[i] = (G, k, w,
-    halvings, converged)."""
+    method's own check), all open problems per batched level (the halved rules' nodes of a
+    level in one ytf_gl_rule_batch call); fills out[i] = (G, k, w, halvings, converged).
+    With G None the rules' own G and the first halved level are evaluated in one batch."""
     open_ = list(idx)
     sing = {i: _sing(problems[i]) for i in open_}
     for h in range(max_halvings + 1):
         if not open_:
             break
-        halv = {}
-        for i in open_:
-            p2 = api.halve_panels(np.asarray(panels[i], np.float64).reshape(-1, 2))
-            halv[i] = (p2, api.gl_rule(p2, order, singular=sing[i], ctx=ctx))
-        Gh = batch_G([problems[i] for i in open_], [halv[i][1] for i in open_], ctx=ctx, device=device)
+        p2s = [api.halve_panels(np.asarray(panels[i], np.float64).reshape(-1, 2)) for i in open_]
+        r2s = api.gl_rule_batch([(p2, sing[i]) for p2, i in zip(p2s, open_)], order, ctx=ctx)
+        halv = {i: (p2, r2) for i, p2, r2 in zip(open_, p2s, r2s)}
+        if G is None:
+            both = batch_G([problems[i] for i in open_] * 2, [rules[i] for i in open_] + [halv[i][1] for i in open_],
+                           ctx=ctx, device=device)
+            G = [None] * len(problems)
+            for i, g in zip(open_, both[:len(open_)]):
+                G[i] = g
+            Gh = both[len(open_):]
+        else:
+            Gh = batch_G([problems[i] for i in open_], [halv[i][1] for i in open_], ctx=ctx, device=device)
         ok = _agree([(G[i], g) for i, g in zip(open_, Gh)], rtol)
         still = []
         for i, g, good in zip(open_, Gh, ok):
@@ -374,9 +382,8 @@ def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, de
                                        rho_max=P["rho_max"], scan=False, order=order, ctx=ctx)
         rules.append((k, w))
         panels.append(info["panels"])
-    G = batch_G(problems, rules, ctx=ctx, device=device)
     out = [None] * len(problems)
-    _refine_levels(problems, range(len(problems)), rules, panels, G, rtol, max_halvings, order, ctx, out, device)
+    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device)
     return out
 
 
@@ -405,9 +412,8 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
                                          rtol=rtol if build_rtol is None else build_rtol, ctx=ctx)
         rules.append((k, w))
         panels.append(info["panels"])
-    G = batch_G(problems, rules, ctx=ctx, device=device)
     out = [None] * len(problems)
-    _refine_levels(problems, range(len(problems)), rules, panels, G, rtol, max_halvings, order, ctx, out, device)
+    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device)
     fall = [i for i, r in enumerate(out) if not r[4]]
     if fall:
         fr = []
