@@ -87,13 +87,15 @@ __global__ void k_bcolmax(BesselI8 p) {
 }
 
 // one thread per (column tile, row slot, slice, 16-node group): 16 bytes of each digit plane
+// one thread per 4 consecutive nodes of a column slot (one 32-bit word of each digit plane):
+// adjacent threads read adjacent 32-byte runs of C
 __global__ void k_bimg_real(BesselI8 p) {
-  const long groups = p.kchunk / 16;
+  const long words = p.kchunk / 4;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long total = (long)p.ntile_n * p.Np * p.nchunk * groups;
+  const long total = (long)p.ntile_n * p.Np * p.nchunk * words;
   if (t >= total) return;
-  const long g = t % groups;
-  long rest = t / groups;
+  const long wq = t % words;
+  long rest = t / words;
   const int z = (int)(rest % p.nchunk);
   rest /= p.nchunk;
   const int slot = (int)(rest % p.Np);
@@ -101,20 +103,16 @@ __global__ void k_bimg_real(BesselI8 p) {
   const int col = ct * p.ctile + slot;
   const bool cv = slot < p.ctile && col < p.N;
   const double sB = cv ? col_scale(p.colmax[(long)z * p.N + col]) : 0.0;
-  uint32_t w[3][4];
+  const long g = wq / 4;
+  const int q = (int)(wq % 4);
+  uint32_t b[3][4];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    uint32_t b[3][4];
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
-      const double v = (cv && k < p.K) ? p.C[(long)col * p.K + k] : 0.0;
-      uint32_t d0, d1, d2;
-      digits3b(__double2int_rn(v * sB), d0, d1, d2);
-      b[0][h] = d0; b[1][h] = d1; b[2][h] = d2;
-    }
-#pragma unroll
-    for (int pl = 0; pl < 3; ++pl) w[pl][q] = b[pl][0] | (b[pl][1] << 8) | (b[pl][2] << 16) | (b[pl][3] << 24);
+  for (int h = 0; h < 4; ++h) {
+    const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
+    const double v = (cv && k < p.K) ? p.C[(long)col * p.K + k] : 0.0;
+    uint32_t d0, d1, d2;
+    digits3b(__double2int_rn(v * sB), d0, d1, d2);
+    b[0][h] = d0; b[1][h] = d1; b[2][h] = d2;
   }
   const long nstage = p.kchunk / BI_NODES;
   const int s = (int)(g / 4), kb = (int)(g % 4) * 16;
@@ -122,8 +120,8 @@ __global__ void k_bimg_real(BesselI8 p) {
   uint8_t* blk = p.Bimg + (((size_t)ct * p.nchunk + z) * nstage + s) * sbytes;
 #pragma unroll
   for (int pl = 0; pl < 3; ++pl)
-    *reinterpret_cast<uint4*>(blk + (size_t)pl * p.Np * 64 + plane_off(slot, kb)) =
-        make_uint4(w[pl][0], w[pl][1], w[pl][2], w[pl][3]);
+    *reinterpret_cast<uint32_t*>(blk + (size_t)pl * p.Np * 64 + plane_off(slot, kb) + 4 * q) =
+        b[pl][0] | (b[pl][1] << 8) | (b[pl][2] << 16) | (b[pl][3] << 24);
 }
 
 // one thread per (radius tile, row, slice, 16-node group): J_n(k ρ) straight into digits
@@ -403,7 +401,7 @@ cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s) {
   k_bcolmax<<<dim3((unsigned)p.N, (unsigned)p.nchunk), 256, 0, s>>>(p);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   {
-    const long total = (long)p.ntile_n * p.Np * p.nchunk * (p.kchunk / 16);
+    const long total = (long)p.ntile_n * p.Np * p.nchunk * (p.kchunk / 4);
     k_bimg_real<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
