@@ -763,10 +763,28 @@ int ytf_cavity_response_batch(ytf_ctx* ctx, int nitems, const ytf_stack* const* 
   int rc;
   if ((rc = upload(ctx, dk, kr, 8 * (size_t)total))) return rc;
   if ((rc = upload(ctx, dphi, &phi, 8))) return rc;
-  // each item is its own (kρ, φ) grid of counts[i] x 1 nodes, solved in stream order on the
-  // shared node scratch; one download and one synchronisation for all
+  // each item is its own (kρ, φ) grid of counts[i] x 1 nodes; the items run round-robin on
+  // the context's side streams (each with its own node scratch: an item is a chain of a few
+  // small dependent launches), forked from and joined to its stream; one download and one
+  // synchronisation for all
+  constexpr int kSlots = 4;
+  const int nslot = nitems >= 2 ? std::min(kSlots, nitems) : 0;
+  if (nslot) {
+    while ((int)ctx->slot_streams.size() < kSlots) {
+      cudaStream_t s;
+      cudaEvent_t e;
+      CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ctx->slot_streams.push_back(s);
+      ctx->slot_events.push_back(e);
+    }
+    CK(cudaEventRecord(ctx->slot_events[0], ctx->stream));
+    for (int s = 0; s < nslot; ++s) CK(cudaStreamWaitEvent(ctx->slot_streams[s], ctx->slot_events[0], 0));
+  }
+  cudaStream_t main = ctx->stream;
   long off = 0;
-  for (int i = 0; i < nitems; ++i) {
+  rc = YTF_OK;
+  for (int i = 0; i < nitems && !rc; ++i) {
     const long n = counts[i];
     if (n == 0) continue;
     TransferParams p;
@@ -785,8 +803,22 @@ int ytf_cavity_response_batch(ytf_ctx* ctx, int nitems, const ytf_stack* const* 
     p.nout = n;
     p.status = dstat + off;
     p.resp = dresp + off;
-    if ((rc = run_transfer(ctx, p, n))) return rc;
+    if (nslot) {
+      ctx->stream = ctx->slot_streams[i % nslot];
+      ctx->ws_slot = 1 + i % nslot;
+    }
+    rc = run_transfer(ctx, p, n);
     off += n;
+  }
+  ctx->stream = main;
+  ctx->ws_slot = 0;
+  for (int s = 0; s < nslot; ++s) {
+    cudaEventRecord(ctx->slot_events[s], ctx->slot_streams[s]);
+    cudaStreamWaitEvent(main, ctx->slot_events[s], 0);
+  }
+  if (rc) {
+    cudaStreamSynchronize(main);
+    return rc;
   }
   CK(cudaMemcpyAsync(out, dresp, 8 * (size_t)total, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
