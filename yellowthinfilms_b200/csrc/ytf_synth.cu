@@ -560,10 +560,13 @@ __global__ void __launch_bounds__(128, 4) k_reflect2d(SynthParams p, double2* __
 
 // 1D coefficient columns from the reflected amplitudes k_reflect2d wrote once per node (the
 // amplitudes do not depend on the z row); the arithmetic per (node, row) is k_coef1d's
+// heights per thread of k_coef1d_amp: a node's amplitudes are loaded once for COEF1D_ZB
+// z rows (the per-row arithmetic and outputs are those of one row per thread)
+constexpr int COEF1D_ZB = 4;
+
 __global__ void __launch_bounds__(128) k_coef1d_amp(SynthParams p, const double2* __restrict__ amp, double* C0,
                                                      double* C1, double* C2) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int zi = blockIdx.y;
   const long n = p.c.n;
   if (k >= n) return;
   cd Af[2][3], Ab[2][3];
@@ -574,26 +577,31 @@ __global__ void __launch_bounds__(128) k_coef1d_amp(SynthParams p, const double2
       Af[m][q] = ldc(amp, 3 * m + q, n, k);
       Ab[m][q] = ldc(amp, 6 + 3 * m + q, n, k);
     }
-  cd c0[5], c1[4], c2[4];
-  coef1d_row(p, k, p.zo[zi], Af, Ab, c0, c1, c2);
-  for (int i = 0; i < 5; ++i) {
-    long r = 2L * (zi * 5 + i);
-    C0[r * n + k] = c0[i].x;
-    C0[(r + 1) * n + k] = c0[i].y;
-  }
-  for (int i = 0; i < 4; ++i) {
-    long r = 2L * (zi * 4 + i);
-    C1[r * n + k] = c1[i].x;
-    C1[(r + 1) * n + k] = c1[i].y;
-    C2[r * n + k] = c2[i].x;
-    C2[(r + 1) * n + k] = c2[i].y;
+  const int z0 = blockIdx.y * COEF1D_ZB;
+  const int z1 = min(p.nz, z0 + COEF1D_ZB);
+  for (int zi = z0; zi < z1; ++zi) {
+    cd c0[5], c1[4], c2[4];
+    coef1d_row(p, k, p.zo[zi], Af, Ab, c0, c1, c2);
+    for (int i = 0; i < 5; ++i) {
+      long r = 2L * (zi * 5 + i);
+      C0[r * n + k] = c0[i].x;
+      C0[(r + 1) * n + k] = c0[i].y;
+    }
+    for (int i = 0; i < 4; ++i) {
+      long r = 2L * (zi * 4 + i);
+      C1[r * n + k] = c1[i].x;
+      C1[(r + 1) * n + k] = c1[i].y;
+      C2[r * n + k] = c2[i].x;
+      C2[(r + 1) * n + k] = c2[i].y;
+    }
   }
 }
 
 cudaError_t launch_coef1d_amp(const SynthParams& p, double2* amp, double* C0, double* C1, double* C2, cudaStream_t s) {
   if (p.c.n <= 0 || p.nz <= 0) return cudaSuccess;
   k_reflect2d<<<(unsigned)((p.c.n + 127) / 128), 128, 0, s>>>(p, amp);
-  k_coef1d_amp<<<dim3((unsigned)((p.c.n + 127) / 128), (unsigned)p.nz), 128, 0, s>>>(p, amp, C0, C1, C2);
+  k_coef1d_amp<<<dim3((unsigned)((p.c.n + 127) / 128), (unsigned)((p.nz + COEF1D_ZB - 1) / COEF1D_ZB)), 128, 0, s>>>(
+      p, amp, C0, C1, C2);
   return cudaGetLastError();
 }
 
