@@ -274,9 +274,13 @@ int ytf_gl_rule_batch(ytf_ctx* ctx, int nsets, const int* npanels, const double*
  * (held on every GPU that loads it until exit) instead of cudaMalloc'd workspace. Limit:
  * 9*nz*(n_nodes + nx*ny) <= 4,194,304 complex values; larger requests return YTF_ERR_ARG.
  * z_obs_dev, xs_dev, ys_dev and out_dev are DEVICE pointers (out: nx*ny*nz*9 complex,
- * Julia layout). The first call on a device looks up the array's device address; make it
- * before any stream capture. All calls share the array: calls that overlap on the GPU
- * (other streams, other host threads) race and must be serialised by the caller. */
+ * Julia layout). As ytf_green: an empty grid returns YTF_OK, an empty rule writes zeros.
+ * The first call on a device looks up the array's device address and keeps it for the life
+ * of the process; make that first call before any stream capture, and do not call this entry
+ * point on a device after cudaDeviceReset (the kept address is then stale). The call
+ * synchronises the context's stream before it returns. All calls share the array: calls that
+ * overlap on the GPU (other streams, other host threads) race and must be serialised by the
+ * caller. */
 int ytf_green_noalloc(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, double zsrc_local, int nz,
                       const double* z_obs_dev, int nx, const double* xs_dev, int ny, const double* ys_dev, int terms,
                       double* out_dev);

@@ -78,3 +78,21 @@ def test_halve_panels_array_form_equals_pair_form():
     assert arr.shape == (80, 2)
     assert np.array_equal(arr, np.array(lst))
     assert np.array_equal(api.halve_panels(arr), np.array(api.halve_panels(lst)))
+
+
+def test_noalloc_wrapper_refuses_host_tensors_and_wrong_dtypes():
+    """closed_form_G_noalloc hands raw addresses to the library, so it must refuse a host
+    tensor (the kernels would read a host address) and a complex64 output (the reduction
+    would write twice its size) before any call."""
+    import pytest
+    import torch
+    from yellowthinfilms_b200 import api
+    z = torch.zeros(2, dtype=torch.float64)
+    out = torch.zeros(2 * 2 * 2 * 9, dtype=torch.complex128)
+    with pytest.raises(api.YTFError, match="must be on cuda:0"):
+        api._noalloc_tensors(0, z, z, z, out)
+    meta = lambda dt: torch.empty(2 * 2 * 2 * 9, dtype=dt, device="meta")
+    with pytest.raises(api.YTFError, match="must be"):
+        api._noalloc_tensors(0, z, z, z, meta(torch.complex64))
+    with pytest.raises(api.YTFError, match="must be a torch tensor"):
+        api._noalloc_tensors(0, np.zeros(2), z, z, out)

@@ -806,6 +806,23 @@ def build_kphi_grid(N_phi: int):
     return np.array([2 * np.pi * p / N_phi for p in range(N_phi)]), np.full(N_phi, 2 * np.pi / N_phi)
 
 
+def _noalloc_tensors(device: int, z_obs, xs, ys, out) -> None:
+    """Refuse what ytf_green_noalloc would misread: it takes raw device addresses, so every
+    tensor must be a contiguous CUDA tensor on the cache's device, the coordinates float64
+    and ``out`` complex128."""
+    import torch
+    for name, t, dt in (("z_obs", z_obs, torch.float64), ("xs", xs, torch.float64), ("ys", ys, torch.float64),
+                        ("out", out, torch.complex128)):
+        if not isinstance(t, torch.Tensor):
+            raise YTFError(f"closed_form_G_noalloc: {name} must be a torch tensor on cuda:{device}")
+        if not t.is_cuda or t.device.index != device:
+            raise YTFError(f"closed_form_G_noalloc: {name} must be on cuda:{device} (got {t.device})")
+        if t.dtype != dt:
+            raise YTFError(f"closed_form_G_noalloc: {name} must be {dt} (got {t.dtype})")
+        if not t.is_contiguous():
+            raise YTFError(f"closed_form_G_noalloc: {name} must be contiguous")
+
+
 def closed_form_G_noalloc(cache: CavityTransferCache2D, obs_layer: int, zsrc_local: float, z_obs, xs, ys, out,
                           terms: str = "all"):
     """closed_form_G for a 2D cache that allocates no device memory inside the library.
@@ -813,12 +830,14 @@ def closed_form_G_noalloc(cache: CavityTransferCache2D, obs_layer: int, zsrc_loc
     For hosts that keep all device memory in their own pool, or that must not trigger the
     device-wide synchronisation of cudaMalloc: the library's scratch is a fixed 64 MiB
     array (limit 9·nz·(n_nodes + Nx·Ny) ≤ 4,194,304 complex values). ``z_obs``, ``xs``,
-    ``ys`` (float64) and ``out`` (complex128, Nx·Ny·Nz·9, Julia order) are CUDA tensors
-    the caller allocated. Concurrent calls on the GPU share the scratch and must be
-    serialised by the caller; the first call on a device should precede any stream capture.
+    ``ys`` (float64) and ``out`` (complex128, Nx·Ny·Nz·9, Julia order) are contiguous CUDA
+    tensors on the cache's device that the caller allocated; anything else raises
+    YTFError. Concurrent calls on the GPU share the scratch and must be serialised by the
+    caller; the first call on a device should precede any stream capture.
     """
     if terms not in TERMS:
         raise YTFError(f"closed_form_G: terms must be :all, :direct, :scattered, :toeplitz or :hankel (got :{terms})")
+    _noalloc_tensors(cache.ctx.device, z_obs, xs, ys, out)
     nz, nx, ny = z_obs.numel(), xs.numel(), ys.numel()
     if out.numel() != nx * ny * nz * 9:
         raise YTFError("closed_form_G: out has the wrong size")

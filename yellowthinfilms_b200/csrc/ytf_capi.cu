@@ -2443,7 +2443,9 @@ extern "C" int ytf_plan_destroy(ytf_plan* P) {
 // the split-k partial sums) in this fixed array instead of the context's workspace. The
 // array is part of the loaded library: every GPU that loads libytf holds its 64 MiB
 // until the process exits. Its device address is looked up once per device, on that
-// device's first call (so make that first call before any stream capture).
+// device's first call (so make that first call before any stream capture) and cached for
+// the life of the process: after a cudaDeviceReset the cached address is stale, so a host
+// that resets a device must not call this entry point on it again.
 // =====================================================================================
 #include <mutex>
 
@@ -2473,26 +2475,25 @@ cudaError_t noalloc_scratch(int device, double2** out) {
 extern "C" int ytf_green_noalloc(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local, int nz,
                                  const double* z_obs_dev, int nx, const double* xs_dev, int ny, const double* ys_dev,
                                  int terms, double* out_dev) {
-  if (!ctx || !c || !out_dev || !z_obs_dev || !xs_dev || !ys_dev) return YTF_ERR_ARG;
+  if (!ctx) return YTF_ERR_ARG;
+  if (!c || !out_dev || !z_obs_dev || !xs_dev || !ys_dev)
+    return fail(ctx, YTF_ERR_ARG, "ytf_green_noalloc: null cache, coordinate or output pointer");
   if (c->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "ytf_green_noalloc: cache belongs to another context");
   if (!c->is2d) return fail(ctx, YTF_ERR_ARG, "ytf_green_noalloc: needs a 2D (kρ, φ) cache");
-  int oi = c->oidx(obs_layer);
-  if (oi < 0)
-    return fail(ctx, YTF_ERR_ARG, "amplitude_at: obs_layer=" + std::to_string(obs_layer) +
-                                      " not in this cache's obs_layers " + obs_str(c->obs, c->nobs));
-  if (terms < 0 || terms > 4)
-    return fail(ctx, YTF_ERR_ARG, "closed_form_G: terms must be :all, :direct, :scattered, :toeplitz or :hankel");
-  bool same = obs_layer == c->src;
-  if ((terms == YTF_TERMS_TOEPLITZ || terms == YTF_TERMS_HANKEL || terms == YTF_TERMS_DIRECT) && !same)
-    return fail(ctx, YTF_ERR_ARG, "closed_form_G: terms needs obs_layer == source_layer (" + std::to_string(c->src) +
-                                      "), got " + std::to_string(obs_layer));
-  double zpos = c->src == 1 ? c->d_src - zsrc_local : zsrc_local;
-  const double se = 1.4901161193847656e-08;
-  if (!(-se <= zpos && zpos <= c->d_src + se))
-    return fail(ctx, YTF_ERR_ARG, "amplitude_at: zsrc_local=" + std::to_string(zsrc_local) + " outside [0," +
-                                      std::to_string(c->d_src) + "]");
-  if (nz <= 0 || nx <= 0 || ny <= 0 || c->n <= 0)
-    return fail(ctx, YTF_ERR_ARG, "ytf_green_noalloc: empty grid or empty rule");
+  SynthParams sp;
+  {
+    int rc0 = synth_setup(ctx, c, obs_layer, zsrc_local, terms, nz, sp);
+    if (rc0) return rc0;
+  }
+  if (nz < 0 || nx < 0 || ny < 0) return fail(ctx, YTF_ERR_ARG, "closed_form_G: negative grid size");
+  // as ytf_green: an empty grid writes nothing, an empty rule integrates to zero
+  if ((long)nx * ny * nz == 0) return YTF_OK;
+  CK(cudaSetDevice(ctx->device));
+  if (c->n == 0) {
+    CK(cudaMemsetAsync(out_dev, 0, sizeof(double2) * 9 * (size_t)nx * ny * nz, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return YTF_OK;
+  }
   const long npix = (long)nx * ny, ncol = 9L * nz, n = c->n;
   // scratch: strengths [ncol][n] then splits x [npix][ncol] partial sums
   const long need1 = ncol * n + npix * ncol;
@@ -2500,7 +2501,6 @@ extern "C" int ytf_green_noalloc(ytf_ctx* ctx, const ytf_cache* c, int obs_layer
     return fail(ctx, YTF_ERR_ARG, "ytf_green_noalloc: 9*nz*(n_nodes + Nx*Ny) = " + std::to_string(need1) +
                                       " complex values exceed the fixed scratch of " +
                                       std::to_string((long)YTF_NOALLOC_SCRATCH_COMPLEX) + " (64 MiB)");
-  CK(cudaSetDevice(ctx->device));
   double2* scratch = nullptr;
   CK(noalloc_scratch(ctx->device, &scratch));
   int nsm = 148;
@@ -2512,28 +2512,7 @@ extern "C" int ytf_green_noalloc(ytf_ctx* ctx, const ytf_cache* c, int obs_layer
   splits = lateral_splits(n, splits);
   double2* S = scratch;
   double2* Gp = scratch + ncol * n;
-  SynthParams sp;
-  std::memset(&sp, 0, sizeof(sp));
-  CacheView& v = sp.c;
-  v.n = n; v.Nk = c->Nk; v.Np = c->Np; v.src = c->src; v.d_src = c->d_src;
-  v.kr = c->d_kr; v.wr = c->d_wr; v.phi = c->d_phi; v.wphi = c->d_wphi;
-  v.kri = c->d_kri; v.wri = c->d_wri;
-  v.valid = c->d_valid;
-  v.tvalid = c->d_tvalid + (size_t)oi * n;
-  v.T = c->d_T + (size_t)oi * 16 * n;
-  v.Qf = c->d_Qf; v.Qb = c->d_Qb; v.sf = c->d_sf; v.sb = c->d_sb;
-  v.basis = c->d_basis + (size_t)oi * 16 * n;
-  sp.same = same;
-  switch (terms) {
-    case YTF_TERMS_ALL: sp.uf_F = sp.ub_F = sp.uf_B = sp.ub_B = 1.0; sp.with_direct = same; break;
-    case YTF_TERMS_SCATTERED: sp.uf_F = sp.ub_F = sp.uf_B = sp.ub_B = 1.0; sp.with_direct = 0; break;
-    case YTF_TERMS_DIRECT: sp.with_direct = 1; break;
-    case YTF_TERMS_TOEPLITZ: sp.uf_F = 1.0; sp.ub_B = 1.0; sp.with_direct = 1; break;
-    case YTF_TERMS_HANKEL: sp.ub_F = 1.0; sp.uf_B = 1.0; sp.with_direct = 0; break;
-  }
-  sp.zpos = zpos;
-  sp.d_obs = c->d_layer[obs_layer - 1];
-  sp.nz = nz;
+  const CacheView& v = sp.c;
   sp.zo = z_obs_dev;
   // every element of S and of the used partial sums is written before it is read in this
   // call, so nothing left by an earlier call needs clearing
