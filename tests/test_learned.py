@@ -58,86 +58,75 @@ def test_mlp_training_reduces_loss(L):
     assert l1 < 0.6 * l0, (l0, l1)
 
 
+Z_ROWS = np.linspace(0.0, 200.0, 8)  # observer heights over 0-200 nm above the film
+H_MIN = 20.0 + Z_ROWS.min()          # source height + lowest observer: the shortest reflected path
+
+
 def _check_fn(api, st, k0, rho_max_wl=5.0):
     lam = 2 * np.pi / k0
     rho = np.exp(np.linspace(np.log(0.01 * lam), np.log(rho_max_wl * lam), 16))
-    z = np.linspace(60.0, 200.0, 6)
 
     def G(k, w):
         c = api.build_cavity_transfer_1d(st, k0, 1, k, w, obs_layers=[1])
-        return api.closed_form_G(c, 1, 20.0, z, rho, [0.0], terms="scattered")
+        return api.closed_form_G(c, 1, 20.0, Z_ROWS, rho, [0.0], terms="scattered")
     return G
 
 
-def plain_nodes_to(L, api, st, k0, rho_max, G, Gref, tol, max_halvings=7):
-    """Nodes of the plain fixed rule (point_kx_grid without the pole scan), halved until G is
-    within tol of the reference; None if it never is."""
-    k, w, info = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rho_max, scan=False)
+def plain_solved_to_agreement(L, api, st, k0, rho_max, G, max_halvings=8):
+    """The plain fixed rule (point_kx_grid without the pole scan) halved until G on two
+    successive levels agrees to 1e-6: (nodes solved over all levels, G of the finer level)."""
+    k, w, info = api.point_kx_grid(st, k0, 1, h_min=H_MIN, rho_max=rho_max, scan=False)
     panels = info["panels"]
     sing = sorted(set(api.layer_light_lines(st[0], k0)) | set(api.layer_light_lines(st[-1], k0)))
+    Gk, solved = G(k, w), len(k)
     for _ in range(max_halvings + 1):
-        if np.linalg.norm(G(k, w) - Gref) <= tol * np.linalg.norm(Gref):
-            return len(k)
         panels = api.halve_panels([tuple(p) for p in panels])
         k, w = api.gl_rule(panels, 8, singular=sing)
-    return None
+        Gh = G(k, w)
+        solved += len(k)
+        if np.linalg.norm(Gk - Gh) <= 1e-6 * np.linalg.norm(Gh):
+            return solved, Gh
+        Gk = Gh
+    return solved, None
 
 
 def test_learned_rule_gains_over_the_method_without_it(L):
-    """What the trained network gains. On held-out stacks (losses from sharp to broad guided
-    modes): the network proposes candidate poles, one batched device call samples the exact
-    response around them, fixed_kρ_rule is built on the result, and the halving check accepts
-    the rule or falls back to the scanned rule. Against a converged reference (scanned rule at
-    rtol 1e-10, halving-checked):
-      * every rule the check accepts is within 2e-6 (the check is a reliable judge), and most
-        are accepted;
-      * accepted rules are built at least twice as fast as the scanned rule (the reference's
-        method: thousands of device solves and ~110 sequential refinement rounds; ~2.7x on a
-        B200, where each refinement round is a short chain of small launches) with as few
-        nodes;
-      * against the plain fixed rule without pole knowledge (light-line breaks, u² substitution,
-        halved until 1e-6): for lateral offsets out to 5 λ the Bessel oscillation sets the panel
-        width and both need about the same nodes; for a near-field set (ρ ≤ 0.2 λ) the sharp
-        poles set the plain rule's count and the learned rule needs fewer nodes."""
-    import time
+    """What the trained network gains, at the dipole problem's observation heights (0-200 nm
+    above the film, h_min = 20 nm, so the rule runs to Kcut = 25 / h_min and meets the
+    films' high-k guided modes). On held-out stacks the network proposes candidate poles,
+    one batched device call samples the exact response around them, fixed_kρ_rule is built on
+    the result, and the halving check accepts the rule (returning the finer level) or the plain
+    method halves it until two levels agree. Against a converged reference (scanned rule at
+    rtol 1e-10, halved):
+      * every returned G is within 1e-6 (the metric's bound);
+      * most proposals are accepted by the check;
+      * the plain fixed rule without pole knowledge (light-line breaks, u² substitution),
+        halved until two levels agree, solves more nodes in total than the learned method."""
     from yellowthinfilms_b200 import api
     X, T = L.training_set(600, n_k=1024, seed=11)
     net = L.new_network(seed=2)
     L.train(net, X, T, steps=4000, batch=4096, lr=1e-3)
-    st0, lam0 = L.film_stack(np.random.default_rng(0))
-    L.propose_poles(net, st0, 2 * np.pi / lam0)  # warm the path
     rng = np.random.default_rng(123)
     rows = []
-    for _ in range(6):
+    for _ in range(8):
         st, lam = L.film_stack(rng)
         k0 = 2 * np.pi / lam
-        for rw in (5.0, 0.2):
-            G = _check_fn(api, st, k0, rw)
-            kr, wr, ir = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rw * lam, rtol=1e-10)
-            Gref = G(*L.halved(st, k0, ir["panels"], 8))
-            assert np.linalg.norm(G(kr, wr) - Gref) <= 1e-9 * np.linalg.norm(Gref)
-            t = time.perf_counter()
-            ks, ws, _ = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=rw * lam)
-            t_scan = time.perf_counter() - t
-            t = time.perf_counter()
-            k, w, info = L.learned_rule(net, st, k0, 1, h_min=80.0, rho_max=rw * lam)
-            t_learned = time.perf_counter() - t
-            Gk = G(k, w)
-            acc = bool(np.linalg.norm(Gk - G(*L.halved(st, k0, info["panels"], 8))) <= 1e-6 * np.linalg.norm(Gk))
-            err = np.linalg.norm(Gk - Gref) / np.linalg.norm(Gref)
-            n_plain = plain_nodes_to(L, api, st, k0, rw * lam, G, Gref, 1e-6)
-            rows.append(dict(rw=rw, acc=acc, err=err, n=len(k), n_scan=len(ks), n_plain=n_plain,
-                             speedup=t_scan / t_learned))
+        G = _check_fn(api, st, k0, 5.0)
+        kr, wr, ir = api.point_kx_grid(st, k0, 1, h_min=H_MIN, rho_max=5 * lam, rtol=1e-10)
+        Gref = G(*L.halved(st, k0, ir["panels"], 8))
+        assert np.linalg.norm(G(kr, wr) - Gref) <= 1e-9 * np.linalg.norm(Gref)
+        k, w, info = L.learned_rule(net, st, k0, 1, h_min=H_MIN, rho_max=5 * lam, check=G)
+        err = np.linalg.norm(info["G"] - Gref) / np.linalg.norm(Gref)
+        solved_learned = len(k) * 3 // 2 if info["learned"] else len(k) * 2
+        n_plain, Gp = plain_solved_to_agreement(L, api, st, k0, 5 * lam, G)
+        err_plain = np.linalg.norm(Gp - Gref) / np.linalg.norm(Gref) if Gp is not None else np.inf
+        rows.append(dict(acc=bool(info["learned"]), err=err, err_plain=err_plain, n=len(k),
+                         solved=solved_learned, solved_plain=n_plain))
     msg = "\n".join(str(r) for r in rows)
-    acc = [r for r in rows if r["acc"]]
-    assert all(r["err"] <= 2e-6 for r in acc), msg
-    assert len(acc) >= 8, msg
-    assert np.mean([r["n"] / r["n_scan"] for r in acc]) <= 1.25, msg
-    assert np.median([r["speedup"] for r in acc]) >= 2.0, msg
-    far = [r for r in acc if r["rw"] == 5.0 and r["n_plain"]]
-    near = [r for r in acc if r["rw"] == 0.2 and r["n_plain"]]
-    assert np.mean([r["n_plain"] / r["n"] for r in far]) >= 0.9, msg
-    assert max(r["n_plain"] / r["n"] for r in near) >= 1.5, msg
+    assert all(r["err"] <= 1e-6 for r in rows), msg
+    assert all(r["err_plain"] <= 1e-6 for r in rows), msg
+    assert sum(r["acc"] for r in rows) >= 5, msg
+    assert np.mean([r["solved_plain"] / r["solved"] for r in rows]) >= 1.2, msg
 
 
 def test_untrained_network_falls_back_to_the_plain_method(L):
@@ -150,11 +139,11 @@ def test_untrained_network_falls_back_to_the_plain_method(L):
     st, lam = L.film_stack(rng)
     k0 = 2 * np.pi / lam
     G = _check_fn(api, st, k0, 0.2)
-    kr, wr, ir = api.point_kx_grid(st, k0, 1, h_min=80.0, rho_max=0.2 * lam, rtol=1e-10)
+    kr, wr, ir = api.point_kx_grid(st, k0, 1, h_min=H_MIN, rho_max=0.2 * lam, rtol=1e-10)
     Gref = G(*L.halved(st, k0, ir["panels"], 8))
-    k, w, info = L.learned_rule(net, st, k0, 1, h_min=80.0, rho_max=0.2 * lam, check=G)
+    k, w, info = L.learned_rule(net, st, k0, 1, h_min=H_MIN, rho_max=0.2 * lam, check=G)
     assert np.array_equal(info["G"], G(k, w))
-    assert np.linalg.norm(info["G"] - Gref) <= 2e-6 * np.linalg.norm(Gref)
+    assert np.linalg.norm(info["G"] - Gref) <= 1e-6 * np.linalg.norm(Gref)
     if not info["learned"]:
         assert info["halvings"] >= 1
 
@@ -184,7 +173,7 @@ def test_batched_rules_equal_per_stack_rules(L):
         assert np.array_equal(k, kl) and np.array_equal(info["G"], gl) and bool(info["learned"]) == bool(acc)
         k2, w2, inf2 = api.point_kx_grid(P["stack"], P["k0"], 1, h_min=80.0, rho_max=P["rho_max"], scan=False)
         panels, Gk = inf2["panels"], G(k2, w2)
-        for _ in range(hp):
+        for _ in range(hp + 1 if conv else hp):  # a converged problem returns the finer level of its pair
             panels = api.halve_panels([tuple(p) for p in panels])
             k2, w2 = api.gl_rule(panels, 8, singular=L._sing(P))
             Gk = G(k2, w2)

@@ -27,7 +27,7 @@ from .materials import FlatOpticalLayer, IsotropicMaterial, UniaxialMaterial, st
 MAX_LAYERS = 8
 N_FEATURES = MAX_LAYERS * 19 + 2  # 154
 LAMBDA_REF = 600.0                 # nm: frequency feature = λ_ref / λ
-K_LO, K_HI = 0.25, 20.0            # scan range in units of k0
+K_LO, K_HI = 0.25, 160.0           # scan range in units of k0 (covers Kcut = 25 / 20 nm at 450-750 nm)
 LOG_SCALE = 4.0                    # target 0 = log R / LOG_SCALE
 
 
@@ -249,12 +249,12 @@ def _poles_from_windows(wins, R, n_local):
     return merged
 
 
-def halved(stack, omega, panels, order):
+def halved(stack, omega, panels, order, ctx=None):
     """The rule on the same panels split in two (the acceptance check), with the u²
     substitution at the half-space light lines as the original rule."""
     sing = sorted(set(api.layer_light_lines(stack[0], omega)) | set(api.layer_light_lines(stack[-1], omega)))
     p2 = api.halve_panels([tuple(p) for p in panels])
-    return api.gl_rule(p2, order, singular=sing)
+    return api.gl_rule(p2, order, singular=sing, ctx=ctx)
 
 
 def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol=1e-6, check=None, max_halvings=6,
@@ -265,9 +265,11 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
     fixed_kρ_rule on them. With ``check`` (a callable rule -> G) the rule is accepted when G
     agrees with G on the halved rule to rtol; otherwise the plain method takes over: the rule
     is halved again until two successive levels agree (at most max_halvings times), and if
-    they never do, the scanned rule is returned. Returns (k, w, info): info["learned"] is True
-    when the proposed rule itself was accepted, info["halvings"] counts the plain refinements,
-    info["G"] is G on the returned rule when ``check`` was given."""
+    they never do, the scanned rule is returned. On agreement the finer level of the agreeing
+    pair is returned (its G is already computed and the more accurate of the two). Returns
+    (k, w, info): info["learned"] is True when the proposed rule itself was accepted,
+    info["halvings"] counts the plain refinements, info["G"] is G on the returned rule when
+    ``check`` was given."""
     poles = refine_poles(stack, k0, source_layer, propose_poles(net, stack, k0), ctx=ctx)
     k, w, info = api.grid_from_poles(stack, k0, source_layer, poles, h_min=h_min, rho_max=rho_max, order=order,
                                      rtol=rtol, ctx=ctx)
@@ -282,8 +284,10 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
         kh, wh = api.gl_rule(panels2, order, singular=sing)
         Gh = check(kh, wh)
         if np.linalg.norm(G - Gh) <= rtol * np.linalg.norm(Gh):
-            info.update(learned=h == 0, halvings=h, G=G, panels=np.asarray(panels))
-            return k, w, info
+            # the check passed: return the finer of the two levels (already solved, and the
+            # more accurate; its difference to the coarser one bounds the coarser one's error)
+            info.update(learned=h == 0, halvings=h, G=Gh, panels=np.asarray(panels2))
+            return kh, wh, info
         panels, k, w, G = panels2, kh, wh, Gh
     k, w, info2 = api.point_kx_grid(stack, k0, source_layer, h_min=h_min, rho_max=rho_max, order=order, rtol=rtol,
                                     ctx=ctx)
@@ -337,11 +341,14 @@ def _sing(P):
     return sorted(set(api.layer_light_lines(st[0], P["k0"])) | set(api.layer_light_lines(st[-1], P["k0"])))
 
 
-def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, ctx, out, device=False):
+def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, ctx, out, device=False, solved=None):
     """Halve the open problems' rules until G agrees with G on the halved rule (the plain
     method's own check), all open problems per batched level (the halved rules' nodes of a
-    level in one ytf_gl_rule_batch call); fills out[i] = (G, k, w, halvings, converged).
-    With G None the rules' own G and the first halved level are evaluated in one batch."""
+    level in one ytf_gl_rule_batch call); fills out[i] = (G, k, w, halvings, converged) with
+    the finer level of the agreeing pair (already solved, and the more accurate one). With G
+    None the rules' own G and the first halved level are evaluated in one batch. ``solved``
+    (optional list): solved[i] grows by the nodes of every rule problem i is solved and
+    synthesised on."""
     open_ = list(idx)
     sing = {i: _sing(problems[i]) for i in open_}
     for h in range(max_halvings + 1):
@@ -350,6 +357,9 @@ def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, c
         p2s = [api.halve_panels(np.asarray(panels[i], np.float64).reshape(-1, 2)) for i in open_]
         r2s = api.gl_rule_batch([(p2, sing[i]) for p2, i in zip(p2s, open_)], order, ctx=ctx)
         halv = {i: (p2, r2) for i, p2, r2 in zip(open_, p2s, r2s)}
+        if solved is not None:
+            for i in open_:
+                solved[i] += len(halv[i][1][0]) + (len(rules[i][0]) if G is None else 0)
         if G is None:
             both = batch_G([problems[i] for i in open_] * 2, [rules[i] for i in open_] + [halv[i][1] for i in open_],
                            ctx=ctx, device=device)
@@ -363,7 +373,8 @@ def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, c
         still = []
         for i, g, good in zip(open_, Gh, ok):
             if good:
-                out[i] = (G[i], rules[i][0], rules[i][1], h, True)
+                out[i] = (g, halv[i][1][0], halv[i][1][1], h, True)
+                G[i] = None
             else:
                 panels[i], rules[i], G[i] = halv[i][0], halv[i][1], g
                 still.append(i)
@@ -372,10 +383,11 @@ def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, c
         out[i] = (G[i], rules[i][0], rules[i][1], max_halvings + 1, False)
 
 
-def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, device=False):
+def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, device=False, solved=None):
     """The plain fixed rule (no pole knowledge: light-line breaks, u² substitution) of every
     problem, halved until two levels agree. Returns [(G, k, w, halvings, converged)]; with
-    ``device`` every G (and the acceptance check) stays in device memory."""
+    ``device`` every G (and the acceptance check) stays in device memory; ``solved`` as
+    _refine_levels."""
     rules, panels = [], []
     for P in problems:
         k, w, info = api.point_kx_grid(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
@@ -383,12 +395,13 @@ def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, de
         rules.append((k, w))
         panels.append(info["panels"])
     out = [None] * len(problems)
-    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device)
+    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device,
+                   solved)
     return out
 
 
 def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=None, device=False, build_rtol=None,
-                        n_scan=2048):
+                        n_scan=2048, solved=None):
     """learned_rule for every problem: the network over all problems' scan grids (features
     formed on the device), the exact window sampling of all problems in one device call,
     fixed_kρ_rule per problem, then the acceptance check and any
@@ -396,7 +409,7 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     scanned rule. Returns [(G, k, w, accepted, halvings)]; ``device`` as plain_rules_batch.
     ``build_rtol`` (default rtol): the tolerance the proposed rules are built for; the
     acceptance check always uses rtol. ``n_scan``: points of the log grid the network is
-    evaluated on per problem."""
+    evaluated on per problem. ``solved`` as _refine_levels."""
     n_k = n_scan
     pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
     cands = []
@@ -413,7 +426,8 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
         rules.append((k, w))
         panels.append(info["panels"])
     out = [None] * len(problems)
-    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device)
+    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device,
+                   solved)
     fall = [i for i, r in enumerate(out) if not r[4]]
     if fall:
         fr = []
@@ -422,6 +436,9 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
             k, w, _ = api.point_kx_grid(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
                                         rho_max=P["rho_max"], order=order, rtol=rtol, ctx=ctx)
             fr.append((k, w))
+        if solved is not None:
+            for i, (k, _) in zip(fall, fr):
+                solved[i] += len(k)
         Gf = batch_G([problems[i] for i in fall], fr, ctx=ctx, device=device)
         for i, (k, w), g in zip(fall, fr, Gf):
             out[i] = (g, k, w, out[i][3], False)
