@@ -52,6 +52,15 @@ int ytf_version(void);
 int ytf_ctx_create(ytf_ctx** out, int device);
 int ytf_ctx_destroy(ytf_ctx* ctx);
 int ytf_ctx_set_stream(ytf_ctx* ctx, void* cuda_stream);
+
+/* Polls of each bounded mbarrier wait inside the int8 tensor-core pipelines (the Bessel and
+ * lateral contractions) before the wait gives up; 0 restores the default 2^22 (about a
+ * second). No counterpart in the reference (its loops have no waits). A wait that runs out
+ * ends its kernel early without touching its output: the kernel lets its issued copies and
+ * MMAs finish, releases its tensor memory and sets an error word, and the call returns
+ * YTF_ERR_CUDA with "a tensor-core pipeline wait timed out"; the context stays usable.
+ * Tests set a tiny limit to drive that path. */
+int ytf_ctx_set_wait_limit(ytf_ctx* ctx, long polls);
 int ytf_ctx_sync(ytf_ctx* ctx);
 const char* ytf_last_error(const ytf_ctx* ctx);
 
@@ -180,6 +189,18 @@ int ytf_nodes_1d(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_
 int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer,
                          const ytf_grid_params* params, int npoles, const double* q, const double* G, long cap,
                          double* k, double* w, long* n, ytf_grid_info* info);
+
+/* point_kρ_grid_2d (mod_ClosedFormGrid.jl:536-585) with the :fixed engine and an explicit
+ * h_min: kspace_features with dims = 2 (mod_KSpaceFeatures.jl:295-360) -- the scanned
+ * directions (φ = 0 for an azimuthally symmetric stack; N_φ_scan/4 + 1 over [0, π/2] when
+ * every tensor is diagonal; N_φ_scan over [0, 2π) otherwise), light lines at every scanned
+ * direction, the pole scan along each of them on the device, clusters merged at the φ step,
+ * N_φ from the lateral factor (2.5 Kcut ρ_max) and the pole tracks (_pole_track_η, :243-259),
+ * at least 64, even -- then fixed_kρ_rule: one kρ rule shared by every φ. Returns the kρ
+ * nodes/weights as ytf_nodes_1d and in *n_phi the size of the uniform φ trapezoid
+ * (build_kphi_grid: φ_p = 2π p / N_φ, weights 2π / N_φ). k = w = NULL: size query. */
+int ytf_nodes_2d(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer, const ytf_grid_params* params,
+                 int n_phi_scan, long cap, double* k, double* w, long* n, long* n_phi, ytf_grid_info* info);
 
 /* One problem of a batched transfer build: the arguments of build_cavity_transfer_1d
  * (is2d = 0: k_nodes/k_weights are kx nodes and weights, check_symmetry applies) or of

@@ -125,6 +125,12 @@ static bool allfinite(const Mt<R, C>& a) {
 }
 
 struct Singular : std::runtime_error { Singular() : std::runtime_error("singular") {} };
+// Julia's eigen(::Matrix) refuses non-finite input (LAPACK's chkfinite raises ArgumentError)
+// and raises LAPACKException when zgeevx fails; the per-node try/catch of
+// build_cavity_transfer_1d/2d (mod_CavityTransfer.jl:249-251) catches neither, so either ends
+// the whole build with that error. EigenError carries the message; the node loops record it
+// and the build raises it once the loop is done (an exception must not leave an OpenMP region).
+struct EigenError : std::runtime_error { using std::runtime_error::runtime_error; };
 
 // 2x2 solve by Cramer's rule, column by column (StaticArrays `\` for a 2x2 system).
 template <int C>
@@ -306,6 +312,8 @@ static M4 berreman_core(const Layer& L, double w, double kx, double ky) {
 // sortperm by (real, imag) (LinearAlgebra.eigsortby).
 static void eigen4(const M4& B, cd Q[4], M4& V) {
   if (!g_zgeevx) throw std::runtime_error("oracle: LAPACK zgeevx not installed");
+  for (int i = 0; i < 16; ++i)
+    if (!isfinc(B.v[i])) throw EigenError("ArgumentError: matrix contains Infs or NaNs");
   cd a[16];
   for (int i = 0; i < 16; ++i) a[i] = B.v[i];
   char balanc = 'B', jobvl = 'N', jobvr = 'V', sense = 'N';
@@ -319,7 +327,7 @@ static void eigen4(const M4& B, cd Q[4], M4& V) {
   for (int i = 0; i < 16; ++i) a[i] = B.v[i];
   g_zgeevx(&balanc, &jobvl, &jobvr, &sense, &n, a, &lda, w, vl, &ldvl, vr, &ldvr, &ilo, &ihi, scale,
            &abnrm, rconde, rcondv, work.data(), &lwork, rwork, &info);
-  if (info != 0) throw std::runtime_error("zgeevx failed");
+  if (info != 0) throw EigenError("LAPACKException(" + std::to_string(info) + ")");
   int p[4] = {0, 1, 2, 3};
   std::stable_sort(p, p + 4, [&](int x, int y) {
     if (w[x].real() != w[y].real()) return w[x].real() < w[y].real();
@@ -810,6 +818,7 @@ struct Cache {
   std::vector<std::vector<Basis>> basis;  // [obs index][node]
   std::vector<double> d_obs;
   double d_src = 0;
+  mutable std::string node_error;  // set by a node that raised past the per-node catch
   int n() const { return Nk * Np; }
   int oidx(int o) const {
     for (size_t i = 0; i < obs.size(); ++i) if (obs[i] == o) return (int)i;
@@ -859,7 +868,16 @@ static bool solve_node(const Cache& c, double kx, double ky, std::vector<Modes>&
     return true;
   } catch (Singular&) {
     return false;
+  } catch (EigenError& e) {
+#pragma omp critical(ytfo_node_error)
+    if (c.node_error.empty()) c.node_error = e.what();
+    return false;
   }
+}
+
+// the error a node of the build raised past the reference's per-node catch, if any
+static void raise_node_error(const Cache& c) {
+  if (!c.node_error.empty()) throw std::runtime_error(c.node_error);
 }
 
 // build_cavity_transfer_1d (:196-258)
@@ -874,6 +892,7 @@ static void build_1d(Cache& c) {
     if (!solve_node(c, c.kr[k], 0.0, modes, Tk)) continue;
     fill_node(c, k, c.kr[k], 0.0, modes, Tk);
   }
+  raise_node_error(c);
 }
 
 // build_cavity_transfer_2d (:307-398)
@@ -912,6 +931,7 @@ static void build_2d(Cache& c) {
       fill_node(c, k + Nk * p, kx, ky, modes, Tk);
     }
   }
+  raise_node_error(c);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1516,6 +1536,94 @@ static Features kspace_features_1d(const Stack& st, double w, int src, double h_
   return F;
 }
 
+// _pole_track_η (mod_KSpaceFeatures.jl:243-259): the smallest φ-width Γ dφ / |dq| of a pole
+// track between neighbouring scanned directions (a wrap pair closes a full circle); ∞ with
+// fewer than two directions or no track
+static double pole_track_eta(const std::vector<Pole>& poles, std::vector<double> phis) {
+  std::sort(phis.begin(), phis.end());
+  phis.erase(std::unique(phis.begin(), phis.end()), phis.end());
+  if (phis.size() < 2) return INFINITY;
+  struct Pair { double p1, p2, dp; };
+  std::vector<Pair> pairs;
+  for (size_t i = 0; i + 1 < phis.size(); ++i) pairs.push_back({phis[i], phis[i + 1], phis[i + 1] - phis[i]});
+  const double step = phis[1] - phis[0];
+  if (std::fabs(phis.back() - phis.front() + step - 2 * M_PI) < 1e-9) pairs.push_back({phis.back(), phis.front(), step});
+  double eta = INFINITY;
+  for (auto& pr : pairs)
+    for (auto& p : poles)
+      for (auto& r : poles) {
+        if (!(p.phi == pr.p1 && r.phi == pr.p2)) continue;
+        const double dq = std::fabs(p.q - r.q);
+        if (!(0 < dq && dq <= pr.dp * std::max(p.q, r.q))) continue;
+        eta = std::min(eta, std::min(p.G, r.G) * pr.dp / dq);
+      }
+  return eta;
+}
+
+// kspace_features, dims = 2 (mod_KSpaceFeatures.jl:295-360): the scanned directions (φ = 0
+// for an azimuthally symmetric stack; N_φ_scan/4 + 1 over [0, π/2] when every tensor is
+// diagonal; N_φ_scan over [0, 2π) otherwise), light lines at every scanned φ mod π, the
+// union of the poles of every direction, clusters merged at the φ step, and N_φ, the largest
+// of N_φ_min, c_φ Kcut ρ_max and c_η log(10/rtol)/η_min, rounded up to even. The scan
+// directions are p (π/2)/(n - 1) and 2πp/N_φ_scan.
+static Features kspace_features_2d(const Stack& st, double w, int src, double h_min, double rho_max, double target_decay,
+                                   double kr_cap, double kr_cap_rel, bool scan, double scan_step, double prominence,
+                                   int n_phi_scan, double c_phi, int n_phi_min, double rtol, double c_eta) {
+  Features F;
+  const int N = (int)st.size();
+  const bool sym = azimuthally_symmetric(st);
+  bool diag = true;
+  for (auto& L : st)
+    for (int i = 1; i <= 3; ++i)
+      for (int j = 1; j <= 3; ++j)
+        if (i != j && (L.E(i, j) != cd(0.0, 0.0) || L.U(i, j) != cd(0.0, 0.0))) diag = false;
+  std::vector<double> phis;
+  double merge_rel = 0.0;
+  if (sym) {
+    phis = {0.0};
+  } else if (diag) {
+    const int m = std::max(2, n_phi_scan / 4 + 1);
+    for (int p = 0; p < m; ++p) phis.push_back((M_PI / 2) * p / (m - 1));
+    merge_rel = (M_PI / 2) / std::max(1, n_phi_scan / 4);
+  } else {
+    for (int p = 0; p < n_phi_scan; ++p) phis.push_back(2 * M_PI * p / n_phi_scan);
+    merge_rel = 2 * M_PI / n_phi_scan;
+  }
+  std::vector<double> phi_ll;  // light lines are even in the direction: φ mod π, first occurrences
+  if (sym) phi_ll = {0.0};
+  else
+    for (double ph : phis) {
+      const double m = std::fmod(ph, M_PI);
+      if (std::find(phi_ll.begin(), phi_ll.end(), m) == phi_ll.end()) phi_ll.push_back(m);
+    }
+  std::vector<double> ll, sing;
+  for (int j = 0; j < N; ++j)
+    for (double ph : phi_ll) {
+      auto L = layer_light_lines(st[j], w, ph);
+      ll.insert(ll.end(), L.begin(), L.end());
+      if (j == 0 || j == N - 1) sing.insert(sing.end(), L.begin(), L.end());
+    }
+  std::sort(ll.begin(), ll.end()); std::sort(sing.begin(), sing.end());
+  F.light_lines = dedup(ll); F.singular_lines = dedup(sing);
+  F.kmax = F.light_lines.empty() ? w : F.light_lines.back();
+  F.K_geom = target_decay / h_min;
+  F.K_cap = kr_cap > 0 ? kr_cap : kr_cap_rel * F.kmax;
+  F.Kcut = std::min(std::max(F.K_geom, 2.0 * F.kmax), F.K_cap);
+  F.capped = F.Kcut < F.K_geom;
+  F.h_min = h_min; F.rho_max = rho_max;
+  if (scan) {
+    double k_lo = 0.5 * (F.light_lines.empty() ? w : F.light_lines[0]);
+    F.poles = real_axis_poles(st, w, src, phis, k_lo, F.Kcut, scan_step, prominence, F.light_lines);
+  }
+  F.cl = clusters(F.poles, merge_rel);
+  const long n_lat = (long)std::ceil(c_phi * F.Kcut * rho_max);
+  const double eta = pole_track_eta(F.poles, phis);
+  const long n_pole = std::isfinite(eta) ? (long)std::ceil(c_eta * std::log(10 / rtol) / eta) : 0;
+  const long m = std::max(std::max((long)n_phi_min, n_lat), n_pole);
+  F.N_phi = (int)(2 * ((m + 1) / 2));
+  return F;
+}
+
 // graded_panels (mod_KxGrid.jl:331-347)
 template <class Wf>
 static std::vector<std::pair<double, double>> graded_panels(std::vector<double> bs, Wf width, double alpha, long max_panels = 10000000) {
@@ -1920,6 +2028,29 @@ int ytfo_fixed_grid_1d(int nL, const int* ekind, const int* mkind, const double*
     fixed_kr_rule(F, order, rtol, 0.5, 12, 0.05, 4.0, 4.0, 0.5, nd, wt, panels);
     *n = (int)nd.size();
     if (info) { info[0] = F.Kcut; info[1] = F.kmax; info[2] = (double)F.poles.size(); info[3] = (double)panels.size(); }
+    if (nodes) { std::memcpy(nodes, nd.data(), nd.size() * sizeof(double)); std::memcpy(wts, wt.data(), wt.size() * sizeof(double)); }
+    return 0;
+  } catch (std::exception& e) { g_err = e.what(); return 1; }
+}
+
+// point_kρ_grid_2d (mod_ClosedFormGrid.jl:536-585) with an explicit h_min: kspace_features
+// (dims = 2) + fixed_kρ_rule; the kρ rule, and N_φ of the uniform φ trapezoid.
+// info: Kcut, kmax, poles, panels, N_φ.
+int ytfo_fixed_grid_2d(int nL, const int* ekind, const int* mkind, const double* eps, const double* mu, const double* d,
+                       double w, int src, double h_min, double rho_max, double target_decay, double kr_cap, int scan,
+                       int order, double rtol, int n_phi_scan, double* nodes, double* wts, int* n, double* info) {
+  try {
+    Stack st = make_stack(nL, ekind, mkind, eps, mu, d);
+    Features F = kspace_features_2d(st, w, src, h_min, rho_max, target_decay, kr_cap, 1e5, scan != 0, 1e-3, 1.05,
+                                    n_phi_scan, 2.5, 64, rtol, 1.5);
+    std::vector<double> nd, wt;
+    std::vector<std::pair<double, double>> panels;
+    fixed_kr_rule(F, order, rtol, 0.5, 12, 0.05, 4.0, 4.0, 0.5, nd, wt, panels);
+    *n = (int)nd.size();
+    if (info) {
+      info[0] = F.Kcut; info[1] = F.kmax; info[2] = (double)F.poles.size(); info[3] = (double)panels.size();
+      info[4] = (double)F.N_phi;
+    }
     if (nodes) { std::memcpy(nodes, nd.data(), nd.size() * sizeof(double)); std::memcpy(wts, wt.data(), wt.size() * sizeof(double)); }
     return 0;
   } catch (std::exception& e) { g_err = e.what(); return 1; }

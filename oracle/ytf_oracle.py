@@ -292,6 +292,23 @@ def fixed_grid_1d(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=2
     return nodes, wts, dict(Kcut=info[0], kmax=info[1], n_poles=int(info[2]), n_panels=int(info[3]))
 
 
+def fixed_grid_2d(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=25.0, kr_cap=0.0, scan=True, order=8,
+                  rtol=1e-6, n_phi_scan=32):
+    """point_kρ_grid_2d: kspace_features(dims=2) + fixed_kρ_rule: (kρ nodes, weights, info)
+    with info["N_phi"] the φ trapezoid's size."""
+    a = _StackArrays(stack)
+    n = ctypes.c_int(0); info = np.zeros(5)
+    args = (*a.args(), ctypes.c_double(omega), ctypes.c_int(source_layer), ctypes.c_double(h_min), ctypes.c_double(rho_max),
+            ctypes.c_double(target_decay), ctypes.c_double(kr_cap), ctypes.c_int(int(scan)), ctypes.c_int(order),
+            ctypes.c_double(rtol), ctypes.c_int(n_phi_scan))
+    rc = lib().ytfo_fixed_grid_2d(*args, None, None, ctypes.byref(n), _p(info))
+    if rc != 0:
+        raise RuntimeError(_err())
+    nodes = np.zeros(n.value); wts = np.zeros(n.value)
+    lib().ytfo_fixed_grid_2d(*args, _p(nodes), _p(wts), ctypes.byref(n), _p(info))
+    return nodes, wts, dict(Kcut=info[0], kmax=info[1], n_poles=int(info[2]), n_panels=int(info[3]), N_phi=int(info[4]))
+
+
 def own_reflectance(stack, k0, theta_deg, pol):
     a = _StackArrays(stack)
     return float(lib().ytfo_own_reflectance(*a.args(), ctypes.c_double(k0), ctypes.c_double(theta_deg),

@@ -638,3 +638,38 @@ def test_config1_contour_matches_real_axis_oracle(ytf, oracle):
     Go = oracle.closed_form_G(oc, 1, 20.0, zo, rho, [0.0])
     assert relerr(Gc, Go) < 1e-6, relerr(Gc, Go)
     assert relerr(Gc[..., 2, 2], Go[..., 2, 2]) < 1e-6
+
+
+def test_point_krho_grid_2d_without_scan_bit_exact(ytf, oracle):
+    """point_kρ_grid_2d with the pole scan off: the scanned directions' light lines, the
+    panels and N_φ (host) and the Gauss–Legendre nodes (device) equal the oracle's bit for bit,
+    for an azimuthally symmetric, a diagonal (biaxial) and a non-diagonal (gyrotropic) stack."""
+    for idx in (2, 3, 4):
+        _, st = FOUNDATION_STACKS[idx]
+        for h, rho in ((0.05, 1.0), (0.2, 0.0)):
+            k, w, ph, wp, info = ytf.point_krho_grid_2d(st, W, 2, h_min=h, rho_max=rho, scan=False)
+            ko, wo, io = oracle.fixed_grid_2d(st, W, 2, h_min=h, rho_max=rho, scan=False)
+            assert np.array_equal(k, ko) and np.array_equal(w, wo), idx
+            assert info["Kcut"] == io["Kcut"] and info["n_panels"] == io["n_panels"]
+            assert info["N_phi"] == io["N_phi"] and len(ph) == io["N_phi"] and np.allclose(wp.sum(), 2 * np.pi)
+
+
+def test_point_krho_grid_2d_with_pole_scan_matches_oracle(ytf, oracle):
+    """With the pole scan along every scanned direction (device cavity responses, host peak
+    search): the same poles, panels and N_φ (the pole-track term included) as the oracle's
+    scan to refinement precision, and G on a (kρ, φ) grid built from either rule agrees."""
+    for idx, n_scan in ((3, 8), (4, 8)):
+        _, st = FOUNDATION_STACKS[idx]
+        k, w, ph, wp, info = ytf.point_krho_grid_2d(st, W, 2, h_min=0.1, rho_max=0.5, N_phi_scan=n_scan)
+        ko, wo, io = oracle.fixed_grid_2d(st, W, 2, h_min=0.1, rho_max=0.5, n_phi_scan=n_scan)
+        assert info["n_poles"] == io["n_poles"] and info["n_panels"] == io["n_panels"], idx
+        assert len(k) == len(ko) and np.max(np.abs(k - ko)) <= 1e-9 * info["Kcut"]
+        assert abs(info["N_phi"] - io["N_phi"]) <= max(2, 1e-6 * io["N_phi"])
+        phs, wps = uniform_phi(16)
+        c = ytf.build_cavity_transfer_2d(st, W, 2, k, w, phs, wps, obs_layers=[2])
+        co = ytf.build_cavity_transfer_2d(st, W, 2, ko, wo, phs, wps, obs_layers=[2])
+        xs = np.array([0.1, 0.4])
+        d = st[1].d
+        G = ytf.closed_form_G(c, 2, 0.3 * d, [0.6 * d], xs, xs)
+        Go = ytf.closed_form_G(co, 2, 0.3 * d, [0.6 * d], xs, xs)
+        assert relerr(G, Go) < 1e-9

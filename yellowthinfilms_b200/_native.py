@@ -56,6 +56,7 @@ SIGNATURES = {
     "ytf_ctx_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int]),
     "ytf_ctx_destroy": (ctypes.c_int, [_vp]),
     "ytf_ctx_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "ytf_ctx_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_long]),
     "ytf_ctx_sync": (ctypes.c_int, [_vp]),
     "ytf_last_error": (ctypes.c_char_p, [_vp]),
     "ytf_ctx_profile": (ctypes.c_int, [_vp, ctypes.c_int]),
@@ -93,6 +94,9 @@ SIGNATURES = {
                                          ctypes.c_int]),
     "ytf_mlp_train": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                      ctypes.c_ulonglong, _vp]),
+    "ytf_nodes_2d": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams), ctypes.c_int,
+                                    ctypes.c_long, _d, _d, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long),
+                                    ctypes.POINTER(GridInfo)]),
     "ytf_nodes_from_poles": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams),
                                             ctypes.c_int, _d, _d, ctypes.c_long, _d, _d, ctypes.POINTER(ctypes.c_long),
                                             ctypes.POINTER(GridInfo)]),

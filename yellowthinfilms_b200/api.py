@@ -44,6 +44,11 @@ class Context:
     def set_stream(self, cuda_stream: int) -> None:
         lib().ytf_ctx_set_stream(self.h, ctypes.c_void_p(int(cuda_stream)))
 
+    def set_wait_limit(self, polls: int = 0) -> None:
+        """Polls of each bounded wait in the int8 tensor-core pipelines before it gives up
+        (0: the default); a wait that runs out makes the call raise RuntimeError."""
+        self.check(lib().ytf_ctx_set_wait_limit(self.h, int(polls)))
+
     def sync(self) -> None:
         self.check(lib().ytf_ctx_sync(self.h))
 
@@ -354,6 +359,38 @@ def _grid(stack, omega, source_layer, h_min, rho_max, target_decay, kr_cap, scan
                 poles=[(info.poles[i][0], info.poles[i][1]) for i in range(min(info.n_poles, 256))],
                 light_lines=[info.light_lines[i] for i in range(min(info.n_light_lines, 64))])
     return k, w, meta
+
+
+def point_krho_grid_2d(stack, omega, source_layer, h_min, rho_max, target_decay=25.0, kr_cap=0.0, scan=True, order=8,
+                       rtol=1e-6, N_phi=None, N_phi_scan=32, ctx: Optional[Context] = None):
+    """point_kρ_grid_2d (mod_ClosedFormGrid.jl:536-585) with the :fixed engine:
+    (kρ, wρ, φ, wφ, info). kspace_features with dims = 2 scans the poles along every
+    scanned direction on the device and sizes the uniform φ trapezoid (info["N_phi"]: the
+    largest of 64, 2.5 Kcut ρ_max and the pole-track term, even); ``N_phi`` overrides it.
+    One kρ rule serves every φ."""
+    from ._native import GridInfo, GridParams
+    st = _as_stack(stack, ctx)
+    prm = GridParams(float(h_min), float(rho_max), float(target_decay), float(kr_cap), int(bool(scan)), int(order),
+                     float(rtol))
+    info = GridInfo()
+    n, nphi = ctypes.c_long(0), ctypes.c_long(0)
+    call = lambda cap, kp, wp: lib().ytf_nodes_2d(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm),
+                                                  int(N_phi_scan), cap, kp, wp, ctypes.byref(n), ctypes.byref(nphi),
+                                                  ctypes.byref(info))
+    st.ctx.check(call(0, None, None))
+    k = np.zeros(n.value)
+    w = np.zeros(n.value)
+    pan = np.zeros(2 * max(1, info.n_panels))
+    info.panels = ptr(pan)
+    info.panels_cap = info.n_panels
+    st.ctx.check(call(n.value, ptr(k), ptr(w)))
+    Np = int(nphi.value) if N_phi is None else int(N_phi)
+    phi, wphi = build_kphi_grid(Np)
+    meta = dict(Kcut=info.Kcut, kmax=info.kmax, n_poles=info.n_poles, n_panels=info.n_panels, N_phi=Np,
+                N_phi_features=int(nphi.value), panels=pan[:2 * info.n_panels].reshape(-1, 2).copy(),
+                poles=[(info.poles[i][0], info.poles[i][1]) for i in range(min(info.n_poles, 256))],
+                light_lines=[info.light_lines[i] for i in range(min(info.n_light_lines, 64))])
+    return k, w, phi, wphi, meta
 
 
 class MLP:

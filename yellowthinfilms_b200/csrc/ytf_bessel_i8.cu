@@ -26,7 +26,7 @@ constexpr int BI_STAGES = 4;
 constexpr int BI_THREADS = 192;
 constexpr int BI_ACC_STRIDE = 160;
 constexpr int BI_TMEM_COLS = 512;
-constexpr long BI_WAIT_LIMIT = 1L << 22;
+constexpr long BI_WAIT_LIMIT = 1L << 22;  // polls of the drain waits (the pipeline waits: p.wait_limit)
 constexpr double BI_SCALE = 8355000.0;
 
 size_t bessel_i8_stage_bytes_a() { return 3ul * BI_M * 64; }
@@ -238,8 +238,9 @@ struct BiShared {
   int abort_flag;
 };
 
-__device__ __forceinline__ bool bi_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, unsigned* err) {
-  for (long it = 0; it < BI_WAIT_LIMIT; ++it) {
+__device__ __forceinline__ bool bi_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, unsigned* err,
+                                        long limit) {
+  for (long it = 0; it < limit; ++it) {
     if (mbar_try(bar, parity)) return true;
     if ((it & 255) == 255 && *abort_flag) return false;
   }
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img(BesselI8 p) {
       int issued = 0;
       for (int s = 0; s < nst; ++s) {
         const int slot = s % BI_STAGES;
-        if (s >= BI_STAGES && !bi_wait(smem_u32(&sh->empty[slot]), ((s / BI_STAGES) - 1) & 1, abort_flag, p.err))
+        if (s >= BI_STAGES && !bi_wait(smem_u32(&sh->empty[slot]), ((s / BI_STAGES) - 1) & 1, abort_flag, p.err, p.wait_limit))
           break;
         const uint32_t bar = smem_u32(&sh->full[slot]);
         mbar_arrive_tx(bar, stageA + stageB);
@@ -312,7 +313,7 @@ __global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img(BesselI8 p) {
       const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
       for (int s = 0; s < nst; ++s) {
         const int slot = s % BI_STAGES;
-        if (!bi_wait(smem_u32(&sh->full[slot]), (s / BI_STAGES) & 1, abort_flag, p.err)) break;
+        if (!bi_wait(smem_u32(&sh->full[slot]), (s / BI_STAGES) & 1, abort_flag, p.err, p.wait_limit)) break;
         tc_fence_after();
         const uint32_t a0 = smem_u32(smA + slot * stageA), b0 = smem_u32(smB + slot * stageB);
 #pragma unroll
@@ -337,7 +338,7 @@ __global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img(BesselI8 p) {
     }
   } else {
     // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31 (rows of the radius tile)
-    bool ok = bi_wait(smem_u32(&sh->done), 0, abort_flag, p.err);
+    bool ok = bi_wait(smem_u32(&sh->done), 0, abort_flag, p.err, p.wait_limit);
     ok = __all_sync(0xffffffffu, ok) && !*abort_flag;
     if (ok && nst > 0) {
       tc_fence_after();
@@ -370,8 +371,15 @@ __global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img(BesselI8 p) {
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0)
+  if (warp == 0) {
+    // after a timeout the epilogue may have stopped waiting for `done` while MMAs still run:
+    // the MMA thread has committed `done` (it is past its loop), so wait for it before the
+    // tensor memory is released
+    if (*abort_flag && lane == 0) bi_drain_wait(smem_u32(&sh->done), 0);
+    __syncwarp();
+    tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BI_TMEM_COLS) : "memory");
+  }
 }
 
 // P[r][c] = Σ_z partial[z][c][r] through a 32 x 32 shared-memory transpose

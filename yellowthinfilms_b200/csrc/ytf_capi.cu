@@ -48,6 +48,9 @@ struct ytf_ctx {
   std::vector<cudaStream_t> slot_streams;
   std::vector<cudaEvent_t> slot_events;
   int ws_slot = 0;
+  // polls of each bounded mbarrier wait in the int8 tensor-core pipelines before it gives up
+  // (ytf_ctx_set_wait_limit)
+  long wait_limit = 1L << 22;
   ~ytf_ctx() {
     for (auto s : slot_streams) cudaStreamDestroy(s);
     for (auto e : slot_events) cudaEventDestroy(e);
@@ -194,6 +197,14 @@ std::string obs_str(const int* obs, int n) {
 }
 
 bool closed_form(const LayerDev& L) { return (L.ekind == 0 || L.ekind == 1) && L.mkind == 0; }
+
+// a layer's Berreman matrix is finite at every node: finite ε and μ with ε33 ≠ 0 and μ33 ≠ 0
+// (_berreman_core divides by both, mod_ModeSolver.jl:134-135)
+bool berreman_finite(const LayerDev& L) {
+  for (int i = 0; i < 18; ++i)
+    if (!std::isfinite(L.eps[i]) || !std::isfinite(L.mu[i])) return false;
+  return !(L.eps[16] == 0.0 && L.eps[17] == 0.0) && !(L.mu[16] == 0.0 && L.mu[17] == 0.0);
+}
 
 int upload(ytf_ctx* ctx, void* dst, const void* src, size_t bytes) {
   CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
@@ -475,6 +486,13 @@ int ytf_ctx_profile_read(ytf_ctx* ctx, int max_entries, char* names, double* tot
   return YTF_OK;
 }
 
+int ytf_ctx_set_wait_limit(ytf_ctx* ctx, long polls) {
+  if (!ctx) return YTF_ERR_ARG;
+  if (polls < 0) return fail(ctx, YTF_ERR_ARG, "ytf_ctx_set_wait_limit: polls must be >= 0");
+  ctx->wait_limit = polls == 0 ? (1L << 22) : polls;
+  return YTF_OK;
+}
+
 int ytf_ctx_set_stream(ytf_ctx* ctx, void* stream) {
   if (!ctx) return YTF_ERR_ARG;
   ctx->stream = (cudaStream_t)stream;
@@ -573,6 +591,14 @@ int prepare_cache(ytf_ctx* ctx, const ytf_stack* st, bool is2d, double omega, in
     if (*use_rot && !sym)
       return fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: rotation=true requires an azimuthally symmetric stack");
   }
+  // A layer on the general path goes through Julia's eigen, which refuses a non-finite
+  // matrix with an ArgumentError that the reference's per-node try/catch does not catch
+  // (mod_CavityTransfer.jl:249-251): the whole build fails at its first node. Closed-form
+  // layers (isotropic/uniaxial ε, isotropic μ) never call eigen; their non-finite nodes
+  // become invalid data, as in the reference.
+  if ((is2d ? (long)nk * nphi : (long)nk) > 0)
+    for (auto& L : st->host)
+      if (!closed_form(L) && !berreman_finite(L)) return fail(ctx, YTF_ERR_ARG, "matrix contains Infs or NaNs");
   CK(cudaSetDevice(ctx->device));
   ytf_cache* c = new ytf_cache();
   c->ctx = ctx;
@@ -836,6 +862,9 @@ int ytf_layer_light_lines(const double* eps, const double* mu, double omega, dou
   return YTF_OK;
 }
 
+static int rule_from_features(ytf_ctx* ctx, const grid::Features& F, const ytf_grid_params* prm, long cap, double* k,
+                              double* w, long* n, ytf_grid_info* info, const char* fn);
+
 static int nodes_1d_impl(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm,
                          int npoles, const double* pq, const double* pG, long cap, double* k, double* w, long* n,
                          ytf_grid_info* info) {
@@ -867,6 +896,12 @@ static int nodes_1d_impl(ytf_ctx* ctx, const ytf_stack* st, double omega, int so
       if (pq[i] > 0 && pG[i] > 0 && pq[i] < F.Kcut) F.poles.push_back({pq[i], pG[i], 0.0, 0.0});
     F.cl = grid::clusters(F.poles, 0.0);
   }
+  return rule_from_features(ctx, F, prm, cap, k, w, n, info, "point_kx_grid");
+}
+
+// fixed_kρ_rule on the features: panels, the info block, the Gauss-Legendre nodes
+static int rule_from_features(ytf_ctx* ctx, const grid::Features& F, const ytf_grid_params* prm, long cap, double* k,
+                              double* w, long* n, ytf_grid_info* info, const char* fn) {
   std::vector<std::pair<double, double>> panels;
   try {
     panels = grid::fixed_kr_panels(F, prm->order, prm->rtol, 0.5, 12, 0.05, 4.0, 4.0, 0.5);
@@ -896,8 +931,8 @@ static int nodes_1d_impl(ytf_ctx* ctx, const ytf_stack* st, double omega, int so
   }
   if (!k || !w) return YTF_OK;  // size query
   if (cap < tot)
-    return fail(ctx, YTF_ERR_ARG, "point_kx_grid: output capacity " + std::to_string(cap) + " < " + std::to_string(tot) +
-                                      " nodes");
+    return fail(ctx, YTF_ERR_ARG, std::string(fn) + ": output capacity " + std::to_string(cap) + " < " +
+                                      std::to_string(tot) + " nodes");
   std::vector<double> pa(panels.size()), pb(panels.size());
   for (size_t i = 0; i < panels.size(); ++i) { pa[i] = panels[i].first; pb[i] = panels[i].second; }
   return ytf_gl_rule(ctx, (int)panels.size(), pa.data(), pb.data(), prm->order, (int)F.singular_lines.size(),
@@ -914,6 +949,49 @@ int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* st, double omega, int so
                          ytf_grid_info* info) {
   if (npoles < 0 || (npoles > 0 && (!q || !G))) return YTF_ERR_ARG;
   return nodes_1d_impl(ctx, st, omega, source_layer, prm, npoles, q, G, cap, k, w, n, info);
+}
+
+int ytf_nodes_2d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm,
+                 int n_phi_scan, long cap, double* k, double* w, long* n, long* n_phi, ytf_grid_info* info) {
+  if (!ctx || !prm || !n || !n_phi) return YTF_ERR_ARG;
+  if (!st) return fail(ctx, YTF_ERR_ARG, "point_kρ_grid_2d: stack is NULL");
+  if (st->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "point_kρ_grid_2d: stack belongs to another context");
+  const int N = st->nL;
+  if (!(1 <= source_layer && source_layer < N))
+    return fail(ctx, YTF_ERR_ARG, "point_kρ_grid_2d: source_layer=" + std::to_string(source_layer) +
+                                      " must be in 1:" + std::to_string(N - 1));
+  if (!(prm->h_min > 0)) return fail(ctx, YTF_ERR_ARG, "point_kρ_grid_2d: h_min must be positive");
+  if (prm->order < 1) return fail(ctx, YTF_ERR_ARG, "point_kρ_grid_2d: order must be ≥ 1");
+  if (!(prm->rtol > 0 && prm->rtol < 1)) return fail(ctx, YTF_ERR_ARG, "point_kρ_grid_2d: rtol must be in (0, 1)");
+  if (n_phi_scan < 1) return fail(ctx, YTF_ERR_ARG, "point_kρ_grid_2d: N_φ_scan must be ≥ 1");
+  std::vector<const double*> eps(N), mu(N);
+  bool sym = true, diag = true;
+  for (int j = 0; j < N; ++j) {
+    const LayerDev& L = st->host[j];
+    eps[j] = L.eps;
+    mu[j] = L.mu;
+    sym = sym && closed_form(L);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        if (a != b) {
+          const int e = 2 * (a + 3 * b);
+          if (L.eps[e] != 0.0 || L.eps[e + 1] != 0.0 || L.mu[e] != 0.0 || L.mu[e + 1] != 0.0) diag = false;
+        }
+  }
+  // the pole scan's evaluator along each direction: the source layer's cavity response on the device
+  grid::EvalAt f = [&](double phi) -> grid::Eval {
+    return [&, phi](const std::vector<double>& ks, std::vector<double>& out) -> int {
+      out.assign(ks.size(), 0.0);
+      if (ks.empty()) return 0;
+      return ytf_cavity_response(ctx, st, omega, source_layer, (long)ks.size(), ks.data(), phi, out.data());
+    };
+  };
+  grid::Features F;
+  int rc = grid::features_2d(eps, mu, sym, diag, omega, prm->h_min, prm->rho_max, prm->target_decay, prm->kr_cap, 1e5,
+                             prm->scan != 0, 1e-3, 1.05, n_phi_scan, 2.5, 64, prm->rtol, 1.5, f, F);
+  if (rc) return rc;
+  *n_phi = F.N_phi;
+  return rule_from_features(ctx, F, prm, cap, k, w, n, info, "point_kρ_grid_2d");
 }
 
 int ytf_transfer_1d_contour(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, int nk,
@@ -1387,6 +1465,7 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
         WS(pt, double, "g_bi_part", (size_t)bp.nchunk * bp.N * nr);
         bp.kr = c->d_kr; bp.rho = drho; bp.C = Cn8[o];
         bp.Aimg = Aord[o]; bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
+        bp.wait_limit = ctx->wait_limit;
         if (o == 0) CK(LAUNCH("k_bessel_i8", launch_bessel_i8_aimg3(bp, A0i, A1i, A2i, ctx->stream)));
         bp.aimg_ready = 1;
         CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pn8[o], ctx->stream)));
@@ -1474,6 +1553,7 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
         CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
       }
       lp.Bq = Bq; lp.colmax = cmax; lp.partial = Gp; lp.err = err;
+      lp.wait_limit = ctx->wait_limit;
       CK(LAUNCH("k_lateral_i8", launch_lateral_i8(lp, ctx->stream)));
       CK(LAUNCH("k_reduce_splits2", launch_reduce_splits2(npix * ncol, lp.nchunk, Gp, G, ctx->stream)));
       if (!gb) {

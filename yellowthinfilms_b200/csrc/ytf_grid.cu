@@ -2,6 +2,7 @@
 #include "ytf_grid.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <complex>
 #include <limits>
@@ -283,6 +284,90 @@ int features_1d(const std::vector<const double*>& eps, const std::vector<const d
     if (rc) return rc;
   }
   F.cl = clusters(F.poles, 0.0);
+  return 0;
+}
+
+double pole_track_eta(const std::vector<Pole>& poles, std::vector<double> phis) {
+  std::sort(phis.begin(), phis.end());
+  phis.erase(std::unique(phis.begin(), phis.end()), phis.end());
+  if (phis.size() < 2) return INFINITY;
+  std::vector<std::array<double, 3>> pairs;  // (φ1, φ2, dφ)
+  for (size_t i = 0; i + 1 < phis.size(); ++i) pairs.push_back({phis[i], phis[i + 1], phis[i + 1] - phis[i]});
+  const double step = phis[1] - phis[0];
+  if (std::fabs(phis.back() - phis.front() + step - 2 * M_PI) < 1e-9) pairs.push_back({phis.back(), phis.front(), step});
+  double eta = INFINITY;
+  for (const auto& pr : pairs)
+    for (const auto& p : poles) {
+      if (p.phi != pr[0]) continue;
+      for (const auto& r : poles) {
+        if (r.phi != pr[1]) continue;
+        const double dq = std::fabs(p.q - r.q);
+        if (!(0 < dq && dq <= pr[2] * std::max(p.q, r.q))) continue;
+        eta = std::min(eta, std::min(p.G, r.G) * pr[2] / dq);
+      }
+    }
+  return eta;
+}
+
+int features_2d(const std::vector<const double*>& eps, const std::vector<const double*>& mu, bool sym, bool diag,
+                double w, double h_min, double rho_max, double target_decay, double kr_cap, double kr_cap_rel,
+                bool scan, double scan_step, double prominence, int n_phi_scan, double c_phi, int n_phi_min,
+                double rtol, double c_eta, const EvalAt& f, Features& F) {
+  const int N = (int)eps.size();
+  std::vector<double> phis;
+  double merge_rel = 0.0;
+  if (sym) {
+    phis = {0.0};
+  } else if (diag) {
+    const int m = std::max(2, n_phi_scan / 4 + 1);
+    for (int p = 0; p < m; ++p) phis.push_back((M_PI / 2) * p / (m - 1));
+    merge_rel = (M_PI / 2) / std::max(1, n_phi_scan / 4);
+  } else {
+    for (int p = 0; p < n_phi_scan; ++p) phis.push_back(2 * M_PI * p / n_phi_scan);
+    merge_rel = 2 * M_PI / n_phi_scan;
+  }
+  std::vector<double> phi_ll;  // light lines are even in the direction: φ mod π, first occurrences
+  if (sym) {
+    phi_ll = {0.0};
+  } else {
+    for (double ph : phis) {
+      const double m = std::fmod(ph, M_PI);
+      if (std::find(phi_ll.begin(), phi_ll.end(), m) == phi_ll.end()) phi_ll.push_back(m);
+    }
+  }
+  std::vector<double> ll, sing;
+  for (int j = 0; j < N; ++j)
+    for (double ph : phi_ll) {
+      auto L = layer_light_lines(eps[j], mu[j], w, ph);
+      ll.insert(ll.end(), L.begin(), L.end());
+      if (j == 0 || j == N - 1) sing.insert(sing.end(), L.begin(), L.end());
+    }
+  std::sort(ll.begin(), ll.end());
+  std::sort(sing.begin(), sing.end());
+  F.light_lines = merge_close(ll);
+  F.singular_lines = merge_close(sing);
+  F.kmax = F.light_lines.empty() ? w : F.light_lines.back();
+  F.K_geom = target_decay / h_min;
+  F.K_cap = kr_cap > 0 ? kr_cap : kr_cap_rel * F.kmax;
+  F.Kcut = std::min(std::max(F.K_geom, 2.0 * F.kmax), F.K_cap);
+  F.capped = F.Kcut < F.K_geom;
+  F.h_min = h_min;
+  F.rho_max = rho_max;
+  F.phi_scan = phis;
+  F.poles.clear();
+  if (scan) {
+    const double k_lo = 0.5 * (F.light_lines.empty() ? w : F.light_lines[0]);
+    for (double ph : phis) {
+      int rc = real_axis_poles(f(ph), ph, k_lo, F.Kcut, scan_step, prominence, F.light_lines, F.poles);
+      if (rc) return rc;
+    }
+  }
+  F.cl = clusters(F.poles, merge_rel);
+  F.N_phi_lateral = (long)std::ceil(c_phi * F.Kcut * rho_max);
+  F.eta_min = pole_track_eta(F.poles, phis);
+  F.N_phi_poles = std::isfinite(F.eta_min) ? (long)std::ceil(c_eta * std::log(10 / rtol) / F.eta_min) : 0;
+  const long m = std::max(std::max((long)n_phi_min, F.N_phi_lateral), F.N_phi_poles);
+  F.N_phi = 2 * ((m + 1) / 2);
   return 0;
 }
 

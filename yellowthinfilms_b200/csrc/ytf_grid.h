@@ -42,6 +42,10 @@ struct Features {
   bool capped = false;
   std::vector<Pole> poles;
   std::vector<Cluster> cl;
+  std::vector<double> phi_scan;  // 2D: the scanned directions
+  long N_phi = 0;                // 2D: size of the uniform φ trapezoid
+  long N_phi_lateral = 0, N_phi_poles = 0;
+  double eta_min = 0;
 };
 
 // kspace_features for a point rule at φ = 0 (mod_KSpaceFeatures.jl:295-360): light lines of
@@ -49,6 +53,23 @@ struct Features {
 int features_1d(const std::vector<const double*>& eps, const std::vector<const double*>& mu, double w, double h_min,
                 double rho_max, double target_decay, double kr_cap, double kr_cap_rel, bool scan, double scan_step,
                 double prominence, const Eval& f, Features& F);
+
+// the cavity response along one direction φ
+using EvalAt = std::function<Eval(double phi)>;
+
+// _pole_track_η (mod_KSpaceFeatures.jl:243-259): the smallest φ-width Γ dφ / |dq| of a pole
+// moving between neighbouring scanned directions; ∞ with fewer than two or no track
+double pole_track_eta(const std::vector<Pole>& poles, std::vector<double> phis);
+
+// kspace_features with dims = 2 (mod_KSpaceFeatures.jl:295-360): scanned directions (φ = 0
+// for an azimuthally symmetric stack, (π/2) p / (n - 1) for p < n = N_φ_scan/4 + 1 when every
+// tensor is diagonal, 2π p / N_φ_scan otherwise), light lines at every direction mod π, the
+// poles of every direction, clusters merged at the φ step, and N_φ = the largest of N_φ_min,
+// c_φ Kcut ρ_max and c_η log(10/rtol)/η_min, rounded up to even. sym/diag describe the stack.
+int features_2d(const std::vector<const double*>& eps, const std::vector<const double*>& mu, bool sym, bool diag,
+                double w, double h_min, double rho_max, double target_decay, double kr_cap, double kr_cap_rel,
+                bool scan, double scan_step, double prominence, int n_phi_scan, double c_phi, int n_phi_min,
+                double rtol, double c_eta, const EvalAt& f, Features& F);
 
 // fixed_kρ_rule (mod_KSpaceFeatures.jl:396-419) up to the panels: graded_panels
 // (mod_KxGrid.jl:331-347) between 0, the light lines below Kcut and Kcut. Throws

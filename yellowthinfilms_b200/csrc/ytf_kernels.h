@@ -12,7 +12,7 @@ enum : uint8_t {
   ST_VALID = 1,        // node contributes (valid[k] of the reference)
   ST_EIGEN = 2,        // 4x4 QR did not converge
   ST_SORT = 4,         // more than two modes in one direction (reference: BoundsError)
-  ST_SINGULAR = 8,     // exact zero pivot in an interface or projection solve
+  ST_SINGULAR = 8,     // exact zero pivot in the source projection solve (interfaces fall back to QR)
   ST_SEEDS = 16,       // non-finite point seeds (reference: `continue`)
   ST_TNONFINITE = 32,  // some T^o non-finite (Tvalid[o][k] = false)
 };
@@ -215,6 +215,7 @@ struct LateralI8 {
   const unsigned long long* colmax;  // [nchunk][ncol] bits of max(|Re S|, |Im S|) (k_strengths2d)
   double2* partial;  // [nchunk][npix * ncol]
   unsigned* err;     // nonzero if a pipeline wait timed out
+  long wait_limit;   // polls of each bounded pipeline wait before it gives up
 };
 size_t lateral_i8_stage_bytes(int Np);
 size_t lateral_i8_smem(int Np);
@@ -242,6 +243,7 @@ struct BesselI8 {
   unsigned long long* colmax;  // [nchunk][N]
   double* partial;   // [nchunk][N][M]
   unsigned* err;
+  long wait_limit;   // polls of each bounded pipeline wait before it gives up
   int aimg_ready;    // Aimg already holds this order's J_n digits (launch_bessel_i8_aimg3)
 };
 // the J_0, J_1, J_2 digit images of all three orders in one pass (one Bessel evaluation per

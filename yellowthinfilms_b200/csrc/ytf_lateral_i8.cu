@@ -46,7 +46,7 @@ constexpr int I8_PRODUCERS = 256;    // warps 0-7
 constexpr int I8_THREADS = 320;      // + warp 8 (bulk copies) + warp 9 (MMA issue)
 constexpr int I8_ACC_STRIDE = 160;   // tensor-memory columns per accumulator (max N)
 constexpr int I8_TMEM_COLS = 512;
-constexpr long I8_WAIT_LIMIT = 1L << 22;
+constexpr long I8_WAIT_LIMIT = 1L << 22;  // polls of the drain waits (the pipeline waits: p.wait_limit)
 constexpr float I8_SA = 4194000.0f;      // fixed-point scale of the phase operand
 constexpr float I8_MAGIC = 12582912.0f;  // 1.5 * 2^23: fl(t + MAGIC) has rint(t) in its low 23 bits
 
@@ -260,9 +260,10 @@ struct I8Shared {
   int abort_flag;
 };
 
-// bounded wait; gives up early when another thread of the CTA has already given up
-__device__ __forceinline__ bool i8_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, unsigned* err) {
-  for (long it = 0; it < I8_WAIT_LIMIT; ++it) {
+// bounded wait (limit polls); gives up early when another thread of the CTA has already given up
+__device__ __forceinline__ bool i8_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, unsigned* err,
+                                        long limit) {
+  for (long it = 0; it < limit; ++it) {
     if (mbar_try(bar, parity)) return true;
     if ((it & 255) == 255 && *abort_flag) return false;
   }
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
       const int slot = s % I8_STAGES;
       if (s + 1 < nst) i8_load(pxb + (s + 1) * I8_NODES * sx, pyb + (s + 1) * I8_NODES * sy, sx, sy, pre);
       bool ok = true;
-      if (s >= I8_STAGES) ok = i8_wait(smem_u32(&sh->empty[slot]), ((s / I8_STAGES) - 1) & 1, abort_flag, p.err);
+      if (s >= I8_STAGES) ok = i8_wait(smem_u32(&sh->empty[slot]), ((s / I8_STAGES) - 1) & 1, abort_flag, p.err, p.wait_limit);
       if (!__all_sync(0xffffffffu, ok)) return false;
       uint8_t* A = smA + slot * stageA;
 #pragma unroll
@@ -407,7 +408,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
       int issued = 0;
       for (int s = 0; s < nst; ++s) {
         const int slot = s % I8_STAGES;
-        if (s >= I8_STAGES && !i8_wait(smem_u32(&sh->empty[slot]), ((s / I8_STAGES) - 1) & 1, abort_flag, p.err))
+        if (s >= I8_STAGES && !i8_wait(smem_u32(&sh->empty[slot]), ((s / I8_STAGES) - 1) & 1, abort_flag, p.err, p.wait_limit))
           break;
         const uint32_t bar = smem_u32(&sh->full_b[slot]);
         mbar_arrive_tx(bar, stageB);
@@ -429,8 +430,8 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
       for (int s = 0; s < nst; ++s) {
         const int slot = s % I8_STAGES;
         const uint32_t par = (s / I8_STAGES) & 1;
-        if (!i8_wait(smem_u32(&sh->full_b[slot]), par, abort_flag, p.err)) break;
-        if (!i8_wait(smem_u32(&sh->full_a[slot]), par, abort_flag, p.err)) break;
+        if (!i8_wait(smem_u32(&sh->full_b[slot]), par, abort_flag, p.err, p.wait_limit)) break;
+        if (!i8_wait(smem_u32(&sh->full_a[slot]), par, abort_flag, p.err, p.wait_limit)) break;
         tc_fence_after();
         const uint32_t a0 = smem_u32(smA + slot * stageA), b0 = smem_u32(smB + slot * stageB);
 #pragma unroll
@@ -453,7 +454,7 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
 
   // ---------------- epilogue: INT32 accumulators -> FP64 partial sums ----------------
   if (warp < I8_PRODUCERS / 32) {
-    bool ok = i8_wait(smem_u32(&sh->done), 0, abort_flag, p.err);
+    bool ok = i8_wait(smem_u32(&sh->done), 0, abort_flag, p.err, p.wait_limit);
     ok = __all_sync(0xffffffffu, ok) && !*abort_flag;
     if (ok && nst > 0) {
       tc_fence_after();
@@ -486,8 +487,15 @@ __global__ void __launch_bounds__(I8_THREADS, 1) k_lateral_i8(LateralI8 p) {
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0)
+  if (warp == 0) {
+    // after a timeout the epilogue may have stopped waiting for `done` while MMAs still run:
+    // the MMA thread has committed `done` (it is past its loop), so wait for it before the
+    // tensor memory is released
+    if (*abort_flag && lane == 0) i8_drain_wait(smem_u32(&sh->done), 0);
+    __syncwarp();
+    tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(I8_TMEM_COLS) : "memory");
+  }
 }
 
 cudaError_t launch_lateral_i8(const LateralI8& p, cudaStream_t s) {

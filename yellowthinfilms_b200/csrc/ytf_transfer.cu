@@ -615,19 +615,98 @@ __device__ __forceinline__ bool lu_solve4(cd A[4][4], cd B[4][NR]) {
   return true;
 }
 
-// _S_Interface_Matrix (mod_ScatteringMatrix.jl:27-47): [-Vf_B Vb_A] \ [-Vf_A Vb_B]
-__device__ __forceinline__ bool interface_matrix(const Mode4& A, const Mode4& B, S4& S) {
-  cd L[4][4], R[4][4];
+__device__ __forceinline__ void interface_lhs_rhs(const Mode4& A, const Mode4& B, cd L[4][4], cd R[4][4]) {
   for (int i = 0; i < 4; ++i) {
     L[i][0] = -B.vf[i][0]; L[i][1] = -B.vf[i][1]; L[i][2] = A.vb[i][0]; L[i][3] = A.vb[i][1];
     R[i][0] = -A.vf[i][0]; R[i][1] = -A.vf[i][1]; R[i][2] = B.vb[i][0]; R[i][3] = B.vb[i][1];
   }
-  bool ok = lu_solve4<4>(L, R);
+}
+
+// The singular-interface branch of _S_Interface_Matrix (mod_ScatteringMatrix.jl:35-44,
+// qr(LHS, ColumnNorm()) \ RHS), taken when the LU meets an exactly zero pivot (e.g. two
+// identical layers at tangential incidence, where both forward modes coincide). Householder
+// QR with column pivoting: step k moves the remaining column of largest 2-norm to the front
+// and reflects it onto e_k (reflector v = x + e^{i arg x_k} |x| e_k, applied to the
+// right-hand sides as well); the numerical rank counts the diagonal entries of R above
+// 4 eps |R_11|; the basic least-squares solution sets the unknowns past the rank to zero and
+// undoes the column permutation. Exact degeneracies are rare, so this stays out of line and
+// costs the LU path no registers.
+__device__ __noinline__ void interface_qr(const Mode4& A, const Mode4& B, S4& S) {
+  cd a[4][4], r[4][4], x[4][4];
+  int perm[4] = {0, 1, 2, 3};
+  interface_lhs_rhs(A, B, a, r);
+  for (int k = 0; k < 4; ++k) {
+    int pc = k;
+    double best = -1.0;
+    for (int j = k; j < 4; ++j) {
+      double c = 0.0;
+      for (int i = k; i < 4; ++i) c += norm2(a[i][j]);
+      if (c > best) { best = c; pc = j; }
+    }
+    if (pc != k) {
+      for (int i = 0; i < 4; ++i) { const cd t = a[i][pc]; a[i][pc] = a[i][k]; a[i][k] = t; }
+      const int t = perm[pc]; perm[pc] = perm[k]; perm[k] = t;
+    }
+    double nx = 0.0;
+    for (int i = k; i < 4; ++i) nx += norm2(a[i][k]);
+    nx = sqrt(nx);
+    if (nx == 0.0) continue;
+    const cd xk = a[k][k];
+    const double axk = cabs(xk);
+    const cd ph = axk > 0.0 ? xk / axk : cd{1.0, 0.0};
+    cd v[4] = {};
+    v[k] = xk + ph * nx;
+    for (int i = k + 1; i < 4; ++i) v[i] = a[i][k];
+    double vv = 0.0;
+    for (int i = k; i < 4; ++i) vv += norm2(v[i]);
+    if (vv == 0.0) continue;
+    for (int j = k; j < 4; ++j) {
+      cd t{0.0, 0.0};
+      for (int i = k; i < 4; ++i) t += conj(v[i]) * a[i][j];
+      t = t * (2.0 / vv);
+      for (int i = k; i < 4; ++i) a[i][j] -= t * v[i];
+    }
+    for (int j = 0; j < 4; ++j) {
+      cd t{0.0, 0.0};
+      for (int i = k; i < 4; ++i) t += conj(v[i]) * r[i][j];
+      t = t * (2.0 / vv);
+      for (int i = k; i < 4; ++i) r[i][j] -= t * v[i];
+    }
+  }
+  const double tol = 2.220446049250313e-16 * 4.0 * cabs(a[0][0]);
+  int rank = 0;
+  for (int k = 0; k < 4; ++k)
+    if (cabs(a[k][k]) > tol) rank = k + 1;
+  for (int j = 0; j < 4; ++j) {
+    cd y[4] = {};
+    for (int i = rank - 1; i >= 0; --i) {
+      cd t = r[i][j];
+      for (int k = i + 1; k < rank; ++k) t -= a[i][k] * y[k];
+      y[i] = t / a[i][i];
+    }
+    for (int i = 0; i < 4; ++i) x[perm[i]][j] = y[i];
+  }
+  S.b11 = M2{x[0][0], x[0][1], x[1][0], x[1][1]};
+  S.b12 = M2{x[0][2], x[0][3], x[1][2], x[1][3]};
+  S.b21 = M2{x[2][0], x[2][1], x[3][0], x[3][1]};
+  S.b22 = M2{x[2][2], x[2][3], x[3][2], x[3][3]};
+}
+
+// _S_Interface_Matrix (mod_ScatteringMatrix.jl:27-47): [-Vf_B Vb_A] \ [-Vf_A Vb_B] by LU with
+// partial pivoting, and by the pivoted-QR least-squares solve when a pivot is exactly zero;
+// always succeeds (a non-finite result is caught downstream as in the reference)
+__device__ __forceinline__ bool interface_matrix(const Mode4& A, const Mode4& B, S4& S) {
+  cd L[4][4], R[4][4];
+  interface_lhs_rhs(A, B, L, R);
+  if (!lu_solve4<4>(L, R)) {
+    interface_qr(A, B, S);
+    return true;
+  }
   S.b11 = M2{R[0][0], R[0][1], R[1][0], R[1][1]};
   S.b12 = M2{R[0][2], R[0][3], R[1][2], R[1][3]};
   S.b21 = M2{R[2][0], R[2][1], R[3][0], R[3][1]};
   S.b22 = M2{R[2][2], R[2][3], R[3][2], R[3][3]};
-  return ok;
+  return true;
 }
 
 __device__ __forceinline__ void st_s4(double2* base, long slot, long n, long node, const S4& S) {
