@@ -190,6 +190,15 @@ int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* stack, double omega, int
                          const ytf_grid_params* params, int npoles, const double* q, const double* G, long cap,
                          double* k, double* w, long* n, ytf_grid_info* info);
 
+/* adaptive_seeds(kspace_features(...; dims=1); rtol) (mod_KSpaceFeatures.jl:421-445): the
+ * starting breakpoints of the reference's adaptive engine for a point rule -- light lines,
+ * geometric grading L (1 ± 2^-j), j = 1..min(50, ceil(2 log2(10/rtol))), onto the half-space
+ * light lines, each pole cluster's [a - 4Γ, a, b, b + 4Γ], and 2 kmax, 4 kmax, ... below Kcut --
+ * sorted and unique within (0, Kcut). The features (and the pole scan, if params->scan) as
+ * ytf_nodes_1d. seeds = NULL: size query. */
+int ytf_adaptive_seeds(ytf_ctx* ctx, const ytf_stack* stack, double omega, int source_layer,
+                       const ytf_grid_params* params, long cap, double* seeds, long* n);
+
 /* point_kρ_grid_2d (mod_ClosedFormGrid.jl:536-585) with the :fixed engine and an explicit
  * h_min: kspace_features with dims = 2 (mod_KSpaceFeatures.jl:295-360) -- the scanned
  * directions (φ = 0 for an azimuthally symmetric stack; N_φ_scan/4 + 1 over [0, π/2] when

@@ -2033,6 +2033,31 @@ int ytfo_fixed_grid_1d(int nL, const int* ekind, const int* mkind, const double*
   } catch (std::exception& e) { g_err = e.what(); return 1; }
 }
 
+// adaptive_seeds (mod_KSpaceFeatures.jl:421-445) of kspace_features(dims = 1): light lines,
+// L (1 ± 2^-j) for j = 1..grade at the singular lines (grade = _grade_for(rtol) =
+// min(50, ceil(2 log2(10/rtol)))), [a - 4Γ, a, b, b + 4Γ] per cluster, 2 kmax, 4 kmax, ...
+// below Kcut; kept in (0, Kcut), unique, sorted.
+int ytfo_adaptive_seeds(int nL, const int* ekind, const int* mkind, const double* eps, const double* mu, const double* d,
+                        double w, int src, double h_min, double rho_max, double target_decay, double kr_cap, int scan,
+                        double rtol, double* seeds, int* n) {
+  try {
+    Stack st = make_stack(nL, ekind, mkind, eps, mu, d);
+    Features F = kspace_features_1d(st, w, src, h_min, rho_max, target_decay, kr_cap, 1e5, scan != 0, 1e-3, 1.05);
+    const int grade = std::min(50, (int)std::ceil(2 * std::log2(10 / rtol)));
+    std::vector<double> s = F.light_lines;
+    for (double L : F.singular_lines)
+      for (int j = 1; j <= grade; ++j) { s.push_back(L * (1 - std::ldexp(1.0, -j))); s.push_back(L * (1 + std::ldexp(1.0, -j))); }
+    for (auto& c : F.cl) { s.push_back(c.a - 4.0 * c.G); s.push_back(c.a); s.push_back(c.b); s.push_back(c.b + 4.0 * c.G); }
+    for (double k = 2 * F.kmax; k < F.Kcut; k *= 2) s.push_back(k);
+    std::vector<double> o;
+    for (double x : s) if (0 < x && x < F.Kcut && std::find(o.begin(), o.end(), x) == o.end()) o.push_back(x);
+    std::sort(o.begin(), o.end());
+    *n = (int)o.size();
+    if (seeds) std::memcpy(seeds, o.data(), o.size() * sizeof(double));
+    return 0;
+  } catch (std::exception& e) { g_err = e.what(); return 1; }
+}
+
 // point_kρ_grid_2d (mod_ClosedFormGrid.jl:536-585) with an explicit h_min: kspace_features
 // (dims = 2) + fixed_kρ_rule; the kρ rule, and N_φ of the uniform φ trapezoid.
 // info: Kcut, kmax, poles, panels, N_φ.

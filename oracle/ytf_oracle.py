@@ -292,6 +292,19 @@ def fixed_grid_1d(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=2
     return nodes, wts, dict(Kcut=info[0], kmax=info[1], n_poles=int(info[2]), n_panels=int(info[3]))
 
 
+def adaptive_seeds(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=25.0, kr_cap=0.0, scan=True, rtol=1e-6):
+    """adaptive_seeds(kspace_features(dims=1); rtol)."""
+    a = _StackArrays(stack)
+    n = ctypes.c_int(0)
+    args = (*a.args(), ctypes.c_double(omega), ctypes.c_int(source_layer), ctypes.c_double(h_min), ctypes.c_double(rho_max),
+            ctypes.c_double(target_decay), ctypes.c_double(kr_cap), ctypes.c_int(int(scan)), ctypes.c_double(rtol))
+    if lib().ytfo_adaptive_seeds(*args, None, ctypes.byref(n)) != 0:
+        raise RuntimeError(_err())
+    out = np.zeros(n.value)
+    lib().ytfo_adaptive_seeds(*args, _p(out), ctypes.byref(n))
+    return out
+
+
 def fixed_grid_2d(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=25.0, kr_cap=0.0, scan=True, order=8,
                   rtol=1e-6, n_phi_scan=32):
     """point_kρ_grid_2d: kspace_features(dims=2) + fixed_kρ_rule: (kρ nodes, weights, info)

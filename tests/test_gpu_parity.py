@@ -673,3 +673,38 @@ def test_point_krho_grid_2d_with_pole_scan_matches_oracle(ytf, oracle):
         G = ytf.closed_form_G(c, 2, 0.3 * d, [0.6 * d], xs, xs)
         Go = ytf.closed_form_G(co, 2, 0.3 * d, [0.6 * d], xs, xs)
         assert relerr(G, Go) < 1e-9
+
+
+def test_adaptive_seeds_match_oracle(ytf, oracle):
+    """adaptive_seeds on the features of a point rule: bit for bit without the pole scan; with
+    it, the same seeds to the scan's refinement precision."""
+    for idx in (0, 1, 2):
+        _, st = FOUNDATION_STACKS[idx]
+        s = ytf.adaptive_seeds(st, W, 2 if len(st) > 2 else 1, h_min=0.05, rho_max=1.0, scan=False)
+        so = oracle.adaptive_seeds(st, W, 2 if len(st) > 2 else 1, h_min=0.05, rho_max=1.0, scan=False)
+        assert np.array_equal(s, so), idx
+    _, st = FOUNDATION_STACKS[1]
+    s = ytf.adaptive_seeds(st, W, 2, h_min=0.05, rho_max=1.0)
+    so = oracle.adaptive_seeds(st, W, 2, h_min=0.05, rho_max=1.0)
+    assert len(s) == len(so) and np.max(np.abs(s - so)) <= 1e-9 * so[-1]
+
+
+def test_1d_synthesis_in_node_passes_equals_the_sum_of_its_parts(ytf):
+    """A 1D rule larger than one synthesis pass (262144 nodes) is synthesised in passes whose
+    P_n are summed: G on the whole rule equals the sum of G on two halves of it (each one
+    pass) to rounding in FP64, and the int8x3 form agrees with FP64 to its tolerance."""
+    from helpers import config1_like_stack
+    st = config1_like_stack()
+    n = 300_000
+    e = np.linspace(0.0, 30.0 * W, n // 8 + 1)
+    x, wg = np.polynomial.legendre.leggauss(8)
+    k = (0.5 * (e[1:] + e[:-1])[:, None] + 0.5 * np.diff(e)[:, None] * x[None, :]).ravel()
+    w = (0.5 * np.diff(e)[:, None] * wg[None, :]).ravel()
+    zo, rho = [0.05, 0.2], np.geomspace(0.02, 3.0, 16)
+    G = lambda kk, ww, p="fp64": ytf.closed_form_G(ytf.build_cavity_transfer_1d(st, W, 1, kk, ww, obs_layers=[1]), 1,
+                                                   0.03, zo, rho, [0.0], terms="scattered", precision=p)
+    whole = G(k, w)
+    h = n // 2
+    parts = G(k[:h], w[:h]) + G(k[h:], w[h:])
+    assert relerr(whole, parts) < 1e-12
+    assert relerr(G(k, w, "int8x3"), whole) < 1e-6

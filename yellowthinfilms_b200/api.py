@@ -361,6 +361,22 @@ def _grid(stack, omega, source_layer, h_min, rho_max, target_decay, kr_cap, scan
     return k, w, meta
 
 
+def adaptive_seeds(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=25.0, kr_cap=0.0, scan=True,
+                   rtol=1e-6, ctx: Optional[Context] = None):
+    """adaptive_seeds(kspace_features(stack, ω, s; h_min, ρ_max, dims=1); rtol)
+    (mod_KSpaceFeatures.jl:421-445): the adaptive engine's starting breakpoints."""
+    from ._native import GridParams
+    st = _as_stack(stack, ctx)
+    prm = GridParams(float(h_min), float(rho_max), float(target_decay), float(kr_cap), int(bool(scan)), 8, float(rtol))
+    n = ctypes.c_long(0)
+    st.ctx.check(lib().ytf_adaptive_seeds(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm), 0, None,
+                                          ctypes.byref(n)))
+    out = np.zeros(n.value)
+    st.ctx.check(lib().ytf_adaptive_seeds(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm), n.value,
+                                          ptr(out), ctypes.byref(n)))
+    return out
+
+
 def point_krho_grid_2d(stack, omega, source_layer, h_min, rho_max, target_decay=25.0, kr_cap=0.0, scan=True, order=8,
                        rtol=1e-6, N_phi=None, N_phi_scan=32, ctx: Optional[Context] = None):
     """point_kρ_grid_2d (mod_ClosedFormGrid.jl:536-585) with the :fixed engine:

@@ -951,6 +951,36 @@ int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* st, double omega, int so
   return nodes_1d_impl(ctx, st, omega, source_layer, prm, npoles, q, G, cap, k, w, n, info);
 }
 
+int ytf_adaptive_seeds(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm,
+                       long cap, double* seeds, long* n) {
+  if (!ctx || !prm || !n) return YTF_ERR_ARG;
+  if (!st) return fail(ctx, YTF_ERR_ARG, "adaptive_seeds: stack is NULL");
+  if (st->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "adaptive_seeds: stack belongs to another context");
+  const int N = st->nL;
+  if (!(1 <= source_layer && source_layer < N))
+    return fail(ctx, YTF_ERR_ARG, "point_kx_grid: source_layer=" + std::to_string(source_layer) + " must be in 1:" +
+                                      std::to_string(N - 1));
+  if (!(prm->h_min > 0)) return fail(ctx, YTF_ERR_ARG, "adaptive_seeds: h_min must be positive");
+  if (!(prm->rtol > 0 && prm->rtol < 1)) return fail(ctx, YTF_ERR_ARG, "adaptive_seeds: rtol must be in (0, 1)");
+  std::vector<const double*> eps(N), mu(N);
+  for (int j = 0; j < N; ++j) { eps[j] = st->host[j].eps; mu[j] = st->host[j].mu; }
+  grid::Eval f = [&](const std::vector<double>& ks, std::vector<double>& out) -> int {
+    out.assign(ks.size(), 0.0);
+    if (ks.empty()) return 0;
+    return ytf_cavity_response(ctx, st, omega, source_layer, (long)ks.size(), ks.data(), 0.0, out.data());
+  };
+  grid::Features F;
+  int rc = grid::features_1d(eps, mu, omega, prm->h_min, prm->rho_max, prm->target_decay, prm->kr_cap, 1e5,
+                             prm->scan != 0, 1e-3, 1.05, f, F);
+  if (rc) return rc;
+  auto S = grid::adaptive_seeds(F, prm->rtol);
+  *n = (long)S.size();
+  if (!seeds) return YTF_OK;
+  if (cap < *n) return fail(ctx, YTF_ERR_ARG, "adaptive_seeds: output capacity too small");
+  std::copy(S.begin(), S.end(), seeds);
+  return YTF_OK;
+}
+
 int ytf_nodes_2d(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm,
                  int n_phi_scan, long cap, double* k, double* w, long* n, long* n_phi, ytf_grid_info* info) {
   if (!ctx || !prm || !n || !n_phi) return YTF_ERR_ARG;
@@ -1324,6 +1354,151 @@ static int synth_setup(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double z
   return YTF_OK;
 }
 
+// P_n (n = 0, 1, 2; 26 nz real columns x nr radii) of the 1D synthesis over the nodes of sp.c:
+// the per-node coefficient columns (k_coef1d) and the three order contractions -- complex J_n
+// with FP64 GEMMs on a deformed contour, the int8x3 tensor-core pipeline, or FP64 GEMMs
+static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const double* drho, int precision, int nsm,
+                     const GreenBatch* gb, double* P0, double* P1, double* P2) {
+  const long nk = sp.c.n;
+    WS(C, double, "g_C", 26 * (size_t)nz * nk);
+    double *C0 = C, *C1 = C + 10 * (size_t)nz * nk, *C2 = C + 18 * (size_t)nz * nk;
+    WS(amp1, double2, "g_amp", (size_t)12 * nk);
+    CK(LAUNCH("k_coef1d", launch_coef1d_amp(sp, amp1, C0, C1, C2, ctx->stream)));
+    if (sp.c.kri) {
+      // nodes on a deformed contour: complex J_n(kρ ρ) tables, two FP64 GEMMs per order
+      // (Re J and Im J against the real/imaginary coefficient columns), then the complex combine
+      WS(Jc, double, "g_Jc", 6 * (size_t)nr * nk);
+      CK(LAUNCH("k_bessel_c", launch_bessel_c(sp.c.kr, sp.c.kri, nk, drho, nr, Jc, ctx->stream)));
+      const double* Cn[3] = {C0, C1, C2};
+      double* Pn[3] = {P0, P1, P2};
+      const int Nn[3] = {10 * nz, 8 * nz, 8 * nz};
+      WS(Pab, double, "g_Pab", 2 * (size_t)nr * 10 * nz);
+      for (int o = 0; o < 3; ++o) {
+        long tiles = (long)((nr + 127) / 128) * ((Nn[o] + 127) / 128);
+        long want = (2L * nsm + tiles - 1) / tiles;
+        int sp0 = dgemm_splits((int)nk, (int)std::max(1L, std::min(want, std::max(1L, nk / 256))));
+        WS(Pp, double, "g_partial", (size_t)sp0 * nr * Nn[o]);
+        for (int part = 0; part < 2; ++part) {
+          const double* Jp = Jc + (size_t)(2 * o + part) * nr * nk;
+          CK(LAUNCH("k_dgemm_nt", launch_dgemm_nt(nr, Nn[o], (int)nk, Jp, Cn[o], Pp, sp0, ctx->stream)));
+          CK(LAUNCH("k_reduce_splits", launch_reduce_splits((long)nr * Nn[o], sp0, Pp,
+                                                            Pab + (size_t)part * nr * 10 * nz, ctx->stream)));
+        }
+        CK(LAUNCH("k_combine_complex", launch_combine_complex(nr, Nn[o], Pab, Pab + (size_t)nr * 10 * nz, Pn[o],
+                                                              ctx->stream)));
+      }
+      return YTF_OK;
+    }
+    if (precision == YTF_PREC_INT8X3) {
+      // int8 tensor cores: J_n(kρ) and the coefficient columns as fixed-point digit images,
+      // exact INT32 accumulation, FP64 sum of the node slices into P_n
+      const double* Cn8[3] = {C0, C1, C2};
+      double* Pn8[3] = {P0, P1, P2};
+      const int Nn8[3] = {10 * nz, 8 * nz, 8 * nz};
+      unsigned* err = gb ? gb->err : nullptr;
+      if (!err) {
+        WS(e1, unsigned, "g_tc_err", 1);
+        err = e1;
+        CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+      }
+      // one node slicing for the three orders (that of order 0, the widest), so the J_n
+      // digit images of all three come from one Bessel evaluation per (ρ, k)
+      long kchunk;
+      {
+        const int ct0 = bessel_i8_ctile(Nn8[0]);
+        const long tiles = (long)((nr + 127) / 128) * ((Nn8[0] + ct0 - 1) / ct0);
+        const long want = std::max(1L, (long)nsm / tiles);
+        kchunk = (nk + want - 1) / want;
+        kchunk = std::min(16384L, std::max(64L, ((kchunk + 63) / 64) * 64));
+      }
+      const int nchunk = (int)((nk + kchunk - 1) / kchunk);
+      const size_t nst = (size_t)(kchunk / 64);
+      const size_t abytes = (size_t)((nr + 127) / 128) * nchunk * nst * bessel_i8_stage_bytes_a();
+      WS(A0i, uint8_t, "g_bi_a0", abytes);
+      WS(A1i, uint8_t, "g_bi_a1", abytes);
+      WS(A2i, uint8_t, "g_bi_a2", abytes);
+      uint8_t* Aord[3] = {A0i, A1i, A2i};
+      for (int o = 0; o < 3; ++o) {
+        BesselI8 bp;
+        std::memset(&bp, 0, sizeof(bp));
+        bp.M = nr; bp.N = Nn8[o]; bp.K = nk; bp.order = o;
+        bp.ctile = bessel_i8_ctile(bp.N);
+        bp.Np = ((bp.ctile + 15) / 16) * 16;
+        bp.ntile_n = (bp.N + bp.ctile - 1) / bp.ctile;
+        bp.ntile_m = (nr + 127) / 128;
+        bp.kchunk = kchunk;
+        bp.nchunk = nchunk;
+        WS(Bi, uint8_t, "g_bi_b", (size_t)bp.ntile_n * bp.nchunk * nst * bessel_i8_stage_bytes_b(bp.Np));
+        WS(cm, unsigned long long, "g_bi_cmax", (size_t)bp.nchunk * bp.N);
+        WS(pt, double, "g_bi_part", (size_t)bp.nchunk * bp.N * nr);
+        bp.kr = sp.c.kr; bp.rho = drho; bp.C = Cn8[o];
+        bp.Aimg = Aord[o]; bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
+        bp.wait_limit = ctx->wait_limit;
+        if (o == 0) CK(LAUNCH("k_bessel_i8", launch_bessel_i8_aimg3(bp, A0i, A1i, A2i, ctx->stream)));
+        bp.aimg_ready = 1;
+        CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pn8[o], ctx->stream)));
+      }
+      if (!gb) {
+        unsigned herr = 0;
+        CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
+      }
+      return YTF_OK;
+    }
+    WS(J, double, "g_J", 3 * (size_t)nr * nk);
+    double *J0 = J, *J1 = J + (size_t)nr * nk, *J2 = J + 2 * (size_t)nr * nk;
+    CK(LAUNCH("k_bessel", launch_bessel(sp.c.kr, nk, drho, nr, J0, J1, J2, ctx->stream)));
+    auto splits_for = [&](int M, int N) {
+      long tiles = (long)((M + 127) / 128) * ((N + 127) / 128);
+      long want = (2L * nsm + tiles - 1) / tiles;
+      long maxs = std::max(1L, nk / 256);
+      return (int)std::max(1L, std::min(want, maxs));
+    };
+    int s0 = splits_for(nr, 10 * nz), s1 = splits_for(nr, 8 * nz);
+    size_t part = std::max((size_t)s0 * nr * 10 * nz, (size_t)s1 * nr * 8 * nz);
+    WS(Pp, double, "g_partial", part);
+    const double* Jn[3] = {J0, J1, J2};
+    const double* Cn[3] = {C0, C1, C2};
+    double* Pn[3] = {P0, P1, P2};
+    const int Nn[3] = {10 * nz, 8 * nz, 8 * nz};
+    for (int o = 0; o < 3; ++o) {
+      int sp_ = dgemm_splits((int)nk, o == 0 ? s0 : s1);
+      CK(LAUNCH("k_dgemm_nt", launch_dgemm_nt(nr, Nn[o], (int)nk, Jn[o], Cn[o], Pp, sp_, ctx->stream)));
+      CK(LAUNCH("k_reduce_splits", launch_reduce_splits((long)nr * Nn[o], sp_, Pp, Pn[o], ctx->stream)));
+    }
+  return YTF_OK;
+}
+
+// the node range [b0, b0 + nb) of a 1D cache as a cache view of its own: per-node scalars by
+// pointer offset, the multi-row arrays (T, Qf, Qb, sf, sb, basis: rows of n entries) copied
+// into a compact [row][nb] block with one strided copy each
+static int node_chunk_view(ytf_ctx* ctx, const CacheView& v, long b0, long nb, double2* buf, CacheView& out) {
+  out = v;
+  out.n = nb;
+  out.Nk = nb;
+  out.kr = v.kr + b0;
+  out.wr = v.wr + b0;
+  if (v.kri) { out.kri = v.kri + b0; out.wri = v.wri + b0; }
+  out.valid = v.valid + b0;
+  out.tvalid = v.tvalid + b0;
+  struct Rows { const double2* src; int rows; const double2** dst; } rows[6] = {
+      {v.T, 16, &out.T}, {v.Qf, 2, &out.Qf}, {v.Qb, 2, &out.Qb}, {v.sf, 6, &out.sf}, {v.sb, 6, &out.sb},
+      {v.basis, 16, &out.basis}};
+  double2* d = buf;
+  for (auto& r : rows) {
+    CK(cudaMemcpy2DAsync(d, sizeof(double2) * nb, r.src + b0, sizeof(double2) * v.n, sizeof(double2) * nb, r.rows,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+    *r.dst = d;
+    d += (size_t)r.rows * nb;
+  }
+  return YTF_OK;
+}
+
+// nodes per pass of the 1D synthesis: the coefficient columns and digit images of a pass take
+// about 18 KB per node at 64 heights, so a pass stays within a few GB whatever the rule's size
+constexpr long SYNTH1D_NODE_CHUNK = 1L << 18;
+
 static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local, int nz, const double* z_obs,
                       int nx, const double* xs, int ny, const double* ys, int terms, int precision, double* out,
                       int out_is_device, const GreenBatch* gb) {
@@ -1389,116 +1564,29 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
       drho = urho;
       drmap = urmap;
     }
-    WS(C, double, "g_C", 26 * (size_t)nz * nk);
     WS(P, double, "g_P", 26 * (size_t)nz * nr);
-    double *C0 = C, *C1 = C + 10 * (size_t)nz * nk, *C2 = C + 18 * (size_t)nz * nk;
     double *P0 = P, *P1 = P + 10 * (size_t)nz * nr, *P2 = P + 18 * (size_t)nz * nr;
-    WS(amp1, double2, "g_amp", (size_t)12 * nk);
-    CK(LAUNCH("k_coef1d", launch_coef1d_amp(sp, amp1, C0, C1, C2, ctx->stream)));
-    if (c->d_kri) {
-      // nodes on a deformed contour: complex J_n(kρ ρ) tables, two FP64 GEMMs per order
-      // (Re J and Im J against the real/imaginary coefficient columns), then the complex combine
-      WS(Jc, double, "g_Jc", 6 * (size_t)nr * nk);
-      CK(LAUNCH("k_bessel_c", launch_bessel_c(c->d_kr, c->d_kri, nk, drho, nr, Jc, ctx->stream)));
-      const double* Cn[3] = {C0, C1, C2};
-      double* Pn[3] = {P0, P1, P2};
-      const int Nn[3] = {10 * nz, 8 * nz, 8 * nz};
-      WS(Pab, double, "g_Pab", 2 * (size_t)nr * 10 * nz);
-      for (int o = 0; o < 3; ++o) {
-        long tiles = (long)((nr + 127) / 128) * ((Nn[o] + 127) / 128);
-        long want = (2L * nsm + tiles - 1) / tiles;
-        int sp0 = dgemm_splits((int)nk, (int)std::max(1L, std::min(want, std::max(1L, nk / 256))));
-        WS(Pp, double, "g_partial", (size_t)sp0 * nr * Nn[o]);
-        for (int part = 0; part < 2; ++part) {
-          const double* Jp = Jc + (size_t)(2 * o + part) * nr * nk;
-          CK(LAUNCH("k_dgemm_nt", launch_dgemm_nt(nr, Nn[o], (int)nk, Jp, Cn[o], Pp, sp0, ctx->stream)));
-          CK(LAUNCH("k_reduce_splits", launch_reduce_splits((long)nr * Nn[o], sp0, Pp,
-                                                            Pab + (size_t)part * nr * 10 * nz, ctx->stream)));
-        }
-        CK(LAUNCH("k_combine_complex", launch_combine_complex(nr, Nn[o], Pab, Pab + (size_t)nr * 10 * nz, Pn[o],
-                                                              ctx->stream)));
+    if (nk <= SYNTH1D_NODE_CHUNK) {
+      if ((rc = synth1d_P(ctx, sp, nz, nr, drho, precision, nsm, gb, P0, P1, P2))) return rc;
+    } else {
+      // G is linear in the node sum: the rule in passes of at most SYNTH1D_NODE_CHUNK nodes,
+      // their P_n summed (the reference sums closed_form_G over node chunks the same way,
+      // chunked_2d, mod_ClosedFormGrid.jl:449-467)
+      const size_t np = 26 * (size_t)nz * nr;
+      WS(Pacc, double, "g_Pacc", np);
+      WS(Pc, double, "g_Pchunk", np);
+      WS(cbuf, double2, "g_chunk_cache", (size_t)48 * SYNTH1D_NODE_CHUNK);
+      CK(cudaMemsetAsync(Pacc, 0, sizeof(double) * np, ctx->stream));
+      for (long b0 = 0; b0 < nk; b0 += SYNTH1D_NODE_CHUNK) {
+        const long nb = std::min(SYNTH1D_NODE_CHUNK, nk - b0);
+        SynthParams spc = sp;
+        if ((rc = node_chunk_view(ctx, sp.c, b0, nb, cbuf, spc.c))) return rc;
+        if ((rc = synth1d_P(ctx, spc, nz, nr, drho, precision, nsm, gb, Pc, Pc + 10 * (size_t)nz * nr,
+                            Pc + 18 * (size_t)nz * nr)))
+          return rc;
+        CK(LAUNCH("k_add", launch_add(np, Pc, Pacc, ctx->stream)));
       }
-      CK(LAUNCH("k_assemble1d", launch_assemble1d(nx, ny, nz, dxs, dys, drmap, nr, P0, P1, P2, G, ctx->stream)));
-      goto synthesis_done;
-    }
-    if (precision == YTF_PREC_INT8X3) {
-      // int8 tensor cores: J_n(kρ) and the coefficient columns as fixed-point digit images,
-      // exact INT32 accumulation, FP64 sum of the node slices into P_n
-      const double* Cn8[3] = {C0, C1, C2};
-      double* Pn8[3] = {P0, P1, P2};
-      const int Nn8[3] = {10 * nz, 8 * nz, 8 * nz};
-      unsigned* err = gb ? gb->err : nullptr;
-      if (!err) {
-        WS(e1, unsigned, "g_tc_err", 1);
-        err = e1;
-        CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
-      }
-      // one node slicing for the three orders (that of order 0, the widest), so the J_n
-      // digit images of all three come from one Bessel evaluation per (ρ, k)
-      long kchunk;
-      {
-        const int ct0 = bessel_i8_ctile(Nn8[0]);
-        const long tiles = (long)((nr + 127) / 128) * ((Nn8[0] + ct0 - 1) / ct0);
-        const long want = std::max(1L, (long)nsm / tiles);
-        kchunk = (nk + want - 1) / want;
-        kchunk = std::min(16384L, std::max(64L, ((kchunk + 63) / 64) * 64));
-      }
-      const int nchunk = (int)((nk + kchunk - 1) / kchunk);
-      const size_t nst = (size_t)(kchunk / 64);
-      const size_t abytes = (size_t)((nr + 127) / 128) * nchunk * nst * bessel_i8_stage_bytes_a();
-      WS(A0i, uint8_t, "g_bi_a0", abytes);
-      WS(A1i, uint8_t, "g_bi_a1", abytes);
-      WS(A2i, uint8_t, "g_bi_a2", abytes);
-      uint8_t* Aord[3] = {A0i, A1i, A2i};
-      for (int o = 0; o < 3; ++o) {
-        BesselI8 bp;
-        std::memset(&bp, 0, sizeof(bp));
-        bp.M = nr; bp.N = Nn8[o]; bp.K = nk; bp.order = o;
-        bp.ctile = bessel_i8_ctile(bp.N);
-        bp.Np = ((bp.ctile + 15) / 16) * 16;
-        bp.ntile_n = (bp.N + bp.ctile - 1) / bp.ctile;
-        bp.ntile_m = (nr + 127) / 128;
-        bp.kchunk = kchunk;
-        bp.nchunk = nchunk;
-        WS(Bi, uint8_t, "g_bi_b", (size_t)bp.ntile_n * bp.nchunk * nst * bessel_i8_stage_bytes_b(bp.Np));
-        WS(cm, unsigned long long, "g_bi_cmax", (size_t)bp.nchunk * bp.N);
-        WS(pt, double, "g_bi_part", (size_t)bp.nchunk * bp.N * nr);
-        bp.kr = c->d_kr; bp.rho = drho; bp.C = Cn8[o];
-        bp.Aimg = Aord[o]; bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
-        bp.wait_limit = ctx->wait_limit;
-        if (o == 0) CK(LAUNCH("k_bessel_i8", launch_bessel_i8_aimg3(bp, A0i, A1i, A2i, ctx->stream)));
-        bp.aimg_ready = 1;
-        CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pn8[o], ctx->stream)));
-      }
-      if (!gb) {
-        unsigned herr = 0;
-        CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
-      }
-      CK(LAUNCH("k_assemble1d", launch_assemble1d(nx, ny, nz, dxs, dys, drmap, nr, P0, P1, P2, G, ctx->stream)));
-      goto synthesis_done;
-    }
-    WS(J, double, "g_J", 3 * (size_t)nr * nk);
-    double *J0 = J, *J1 = J + (size_t)nr * nk, *J2 = J + 2 * (size_t)nr * nk;
-    CK(LAUNCH("k_bessel", launch_bessel(c->d_kr, nk, drho, nr, J0, J1, J2, ctx->stream)));
-    auto splits_for = [&](int M, int N) {
-      long tiles = (long)((M + 127) / 128) * ((N + 127) / 128);
-      long want = (2L * nsm + tiles - 1) / tiles;
-      long maxs = std::max(1L, nk / 256);
-      return (int)std::max(1L, std::min(want, maxs));
-    };
-    int s0 = splits_for(nr, 10 * nz), s1 = splits_for(nr, 8 * nz);
-    size_t part = std::max((size_t)s0 * nr * 10 * nz, (size_t)s1 * nr * 8 * nz);
-    WS(Pp, double, "g_partial", part);
-    const double* Jn[3] = {J0, J1, J2};
-    const double* Cn[3] = {C0, C1, C2};
-    double* Pn[3] = {P0, P1, P2};
-    const int Nn[3] = {10 * nz, 8 * nz, 8 * nz};
-    for (int o = 0; o < 3; ++o) {
-      int sp_ = dgemm_splits((int)nk, o == 0 ? s0 : s1);
-      CK(LAUNCH("k_dgemm_nt", launch_dgemm_nt(nr, Nn[o], (int)nk, Jn[o], Cn[o], Pp, sp_, ctx->stream)));
-      CK(LAUNCH("k_reduce_splits", launch_reduce_splits((long)nr * Nn[o], sp_, Pp, Pn[o], ctx->stream)));
+      CK(cudaMemcpyAsync(P, Pacc, sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
     }
     CK(LAUNCH("k_assemble1d", launch_assemble1d(nx, ny, nz, dxs, dys, drmap, nr, P0, P1, P2, G, ctx->stream)));
   } else {

@@ -371,6 +371,27 @@ int features_2d(const std::vector<const double*>& eps, const std::vector<const d
   return 0;
 }
 
+std::vector<double> adaptive_seeds(const Features& F, double rtol, double n_gamma, int grade) {
+  if (grade <= 0) grade = std::min(50, (int)std::ceil(2 * std::log2(10 / rtol)));
+  std::vector<double> s(F.light_lines);
+  for (double L : F.singular_lines)
+    for (int j = 1; j <= grade; ++j)
+      for (int sg : {-1, 1}) s.push_back(L * (1 + sg * std::ldexp(1.0, -j)));
+  for (const auto& c : F.cl) {
+    s.push_back(c.a - n_gamma * c.G);
+    s.push_back(c.a);
+    s.push_back(c.b);
+    s.push_back(c.b + n_gamma * c.G);
+  }
+  for (double k = 2 * F.kmax; k < F.Kcut; k *= 2) s.push_back(k);
+  std::vector<double> out;
+  for (double x : s)
+    if (0 < x && x < F.Kcut) out.push_back(x);
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+  return out;
+}
+
 std::vector<std::pair<double, double>> fixed_kr_panels(const Features& F, int order, double rtol, double alpha,
                                                        int grade, double r_rel, double c_h, double c_rho,
                                                        double pole_safety) {

@@ -71,6 +71,12 @@ int features_2d(const std::vector<const double*>& eps, const std::vector<const d
                 bool scan, double scan_step, double prominence, int n_phi_scan, double c_phi, int n_phi_min,
                 double rtol, double c_eta, const EvalAt& f, Features& F);
 
+// adaptive_seeds (mod_KSpaceFeatures.jl:421-445): starting breakpoints of the adaptive engine
+// -- the light lines, L (1 ± 2^-j), j = 1..grade, at every singular line, each cluster's
+// [a - nΓ Γ, a, b, b + nΓ Γ], and 2 kmax, 4 kmax, ... below Kcut; those in (0, Kcut), sorted,
+// duplicates removed. grade <= 0: min(50, ceil(2 log2(10 / rtol))).
+std::vector<double> adaptive_seeds(const Features& F, double rtol, double n_gamma = 4.0, int grade = 0);
+
 // fixed_kρ_rule (mod_KSpaceFeatures.jl:396-419) up to the panels: graded_panels
 // (mod_KxGrid.jl:331-347) between 0, the light lines below Kcut and Kcut. Throws
 // std::runtime_error with the reference's messages.

@@ -137,6 +137,8 @@ int dgemm_splits(int K, int splits);  // effective split count of launch_dgemm_n
 cudaError_t launch_dgemm_nt(int M, int N, int K, const double* A, const double* B, double* partial, int splits,
                             cudaStream_t s);
 cudaError_t launch_reduce_splits(long len, int splits, const double* partial, double* C, cudaStream_t s);
+// acc[i] += x[i], i < len
+cudaError_t launch_add(long len, const double* x, double* acc, cudaStream_t s);
 cudaError_t launch_assemble1d(int nx, int ny, int nz, const double* xs, const double* ys, const int* rmap, int nr,
                               const double* P0, const double* P1, const double* P2, double2* G, cudaStream_t s);
 // 2D direct lateral synthesis

@@ -372,6 +372,16 @@ cudaError_t launch_dgemm_nt(int M, int N, int K, const double* A, const double* 
   return cudaGetLastError();
 }
 
+__global__ void k_add(long len, const double* __restrict__ x, double* __restrict__ acc) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long)gridDim.x * blockDim.x) acc[i] += x[i];
+}
+
+cudaError_t launch_add(long len, const double* x, double* acc, cudaStream_t s) {
+  if (len <= 0) return cudaSuccess;
+  k_add<<<(unsigned)std::min<long>((len + 255) / 256, 148L * 8), 256, 0, s>>>(len, x, acc);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_reduce_splits(long len, int splits, const double* partial, double* C, cudaStream_t s) {
   if (len <= 0) return cudaSuccess;
   k_reduce_splits<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(len, splits, partial, C);
