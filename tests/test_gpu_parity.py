@@ -657,13 +657,16 @@ def test_point_krho_grid_2d_without_scan_bit_exact(ytf, oracle):
 def test_point_krho_grid_2d_with_pole_scan_matches_oracle(ytf, oracle):
     """With the pole scan along every scanned direction (device cavity responses, host peak
     search): the same poles, panels and N_φ (the pole-track term included) as the oracle's
-    scan to refinement precision, and G on a (kρ, φ) grid built from either rule agrees."""
+    scan to refinement precision -- a golden-section maximum is fixed only to about √eps of
+    its position (the response is flat to rounding within that), so the device's and the
+    host's rounding move node positions by up to ~1e-8 Kcut -- and G on a (kρ, φ) grid built
+    from either rule agrees to 1e-9."""
     for idx, n_scan in ((3, 8), (4, 8)):
         _, st = FOUNDATION_STACKS[idx]
         k, w, ph, wp, info = ytf.point_krho_grid_2d(st, W, 2, h_min=0.1, rho_max=0.5, N_phi_scan=n_scan)
         ko, wo, io = oracle.fixed_grid_2d(st, W, 2, h_min=0.1, rho_max=0.5, n_phi_scan=n_scan)
         assert info["n_poles"] == io["n_poles"] and info["n_panels"] == io["n_panels"], idx
-        assert len(k) == len(ko) and np.max(np.abs(k - ko)) <= 1e-9 * info["Kcut"]
+        assert len(k) == len(ko) and np.max(np.abs(k - ko)) <= 1e-7 * info["Kcut"]
         assert abs(info["N_phi"] - io["N_phi"]) <= max(2, 1e-6 * io["N_phi"])
         phs, wps = uniform_phi(16)
         c = ytf.build_cavity_transfer_2d(st, W, 2, k, w, phs, wps, obs_layers=[2])

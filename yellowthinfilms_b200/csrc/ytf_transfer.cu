@@ -415,6 +415,12 @@ __device__ __forceinline__ uint8_t classify_store(const TransferParams& p, int l
                                                   const cd V[4][4]) {
   const long n = p.n;
   const double tol = 1.4901161193847656e-08;
+  // complex nodes (a deformed contour, or circles around complex poles): the two half-spaces
+  // take the proper sheet, the wave that decays away from the stack (Im Q > 0) as forward,
+  // so the integrand is the analytic continuation of its real-axis values on both sides of
+  // the real axis (the principal square root alone gives the growing wave above it, past the
+  // half-space's light line). On the real axis and below it the two rules agree.
+  const bool proper = p.kr_im && (layer == 0 || layer == p.nL - 1);
   int cls[4];  // 0 forward, 1 backward, 2 degenerate
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -424,7 +430,8 @@ __device__ __forceinline__ uint8_t classify_store(const TransferParams& p, int l
     s += conj(V[2][j]) * (-V[1][j]);
     s += conj(V[3][j]) * V[0][j];
     double Pz = 0.25 * s.x;
-    if (fabs(Pz) > tol) cls[j] = Pz > 0 ? 0 : 1;
+    if (proper && fabs(Q[j].y) > tol * cabs(Q[j])) cls[j] = Q[j].y > 0 ? 0 : 1;
+    else if (fabs(Pz) > tol) cls[j] = Pz > 0 ? 0 : 1;
     else if (fabs(Q[j].y) > tol) cls[j] = Q[j].y > tol ? 0 : 1;
     else cls[j] = 2;
   }

@@ -11,8 +11,8 @@ which fixes each pole's (q, Γ) for fixed_kρ_rule (ytf_nodes_from_poles) in pla
 scan's thousands of samples and sequential refinement rounds. Every node of the resulting
 rule is then solved exactly by the transfer path. The plain method stays the judge and the fallback: a
 proposed rule is accepted only if it agrees with its own refinement (every panel halved) to
-the requested tolerance; otherwise the plain method refines it by halving until two levels
-agree (and the scanned rule is the last resort).
+the requested tolerance; otherwise the rule of one exact scan of the response is refined by
+halving until two levels agree (and the reference's scanned rule is the last resort).
 
 Training data come from the solver itself: random stacks of the air / uniaxial film /
 substrate form, each scanned on a log kρ grid by ytf_cavity_response on the device.
@@ -178,11 +178,13 @@ def predict_batch(net, stacks, n_k=2048, chunk=256):
     return np.concatenate(out) if out else np.zeros((0, 2))
 
 
-def _score_candidates(ks, logit, cand):
-    """cand plus the local maxima of the pole score σ(logit) above 0.3 that lie more than 2Γ
-    from every candidate so far (in increasing k), each with Γ = 2e-3 k."""
+def _score_candidates(ks, logit, cand, threshold=0.1):
+    """cand plus the local maxima of the pole score σ(logit) above ``threshold`` that lie more
+    than 2Γ from every candidate so far (in increasing k), each with Γ = 2e-3 k. A false
+    candidate costs one exact window sampling; a missed pole costs a refinement level, so the
+    threshold is low."""
     sc = 1.0 / (1.0 + np.exp(-np.asarray(logit, np.float64)))
-    idx = np.nonzero((sc[1:-1] > 0.3) & (sc[1:-1] >= sc[:-2]) & (sc[1:-1] > sc[2:]))[0] + 1
+    idx = np.nonzero((sc[1:-1] > threshold) & (sc[1:-1] >= sc[:-2]) & (sc[1:-1] > sc[2:]))[0] + 1
     cand = list(cand)
     for i in idx:
         if all(abs(ks[i] - q) > 2 * G for q, G in cand):
@@ -200,10 +202,11 @@ def propose_poles(net, stack, k0, n_k=2048):
 
 
 def _windows(cand, n_local):
-    """The log windows (±6 max(Γ/q, 2e-3), n_local points) around the candidates."""
+    """The log windows (±6 max(Γ/q, 3e-3), n_local points) around the candidates: wide enough
+    for the network's position error, fine enough to resolve the pole's width."""
     wins = []
     for q, G in cand:
-        w = max(G / q, 2e-3)
+        w = max(G / q, 3e-3)
         wins.append(q * np.exp(np.linspace(-6 * w, 6 * w, n_local)))
     return wins
 
@@ -233,13 +236,11 @@ def refine_poles_batch(items, n_local=129, ctx=None):
 
 
 def _poles_from_windows(wins, R, n_local):
-    """Per window the strongest peak of the sampled response, merged across windows."""
+    """Every peak of the sampled response in each window, merged across windows."""
     out = []
     for i, ks in enumerate(wins):
         y = np.log(np.maximum(R[i * n_local:(i + 1) * n_local], 1e-12))
-        pk = peaks(ks, y)
-        if pk:
-            out.append(max(pk, key=lambda qg: y[np.searchsorted(ks, qg[0]) - 1]))
+        out += peaks(ks, y)
     out.sort()
     merged = []
     for q, G in out:  # windows of neighbouring candidates may find the same pole
@@ -263,13 +264,14 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
 
     Proposes poles with the network, fixes them with one exact batched sampling, and builds
     fixed_kρ_rule on them. With ``check`` (a callable rule -> G) the rule is accepted when G
-    agrees with G on the halved rule to rtol; otherwise the plain method takes over: the rule
-    is halved again until two successive levels agree (at most max_halvings times), and if
-    they never do, the scanned rule is returned. On agreement the finer level of the agreeing
-    pair is returned (its G is already computed and the more accurate of the two). Returns
-    (k, w, info): info["learned"] is True when the proposed rule itself was accepted,
-    info["halvings"] counts the plain refinements, info["G"] is G on the returned rule when
-    ``check`` was given."""
+    agrees with G on the halved rule to rtol; otherwise the proposal missed a pole and the
+    plain method takes over: the rule of one exact scan of the response
+    (exact_scan_poles_batch), halved until two successive levels agree (at most max_halvings
+    times), and if they never do, the reference's scanned rule. On agreement the finer level
+    of the agreeing pair is returned (its G is already computed and the more accurate of the
+    two). Returns (k, w, info): info["learned"] is True when the proposed rule itself was
+    accepted, info["halvings"] counts the levels past it, info["G"] is G on the returned rule
+    when ``check`` was given."""
     poles = refine_poles(stack, k0, source_layer, propose_poles(net, stack, k0), ctx=ctx)
     k, w, info = api.grid_from_poles(stack, k0, source_layer, poles, h_min=h_min, rho_max=rho_max, order=order,
                                      rtol=rtol, ctx=ctx)
@@ -279,6 +281,19 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
     sing = sorted(set(api.layer_light_lines(stack[0], k0)) | set(api.layer_light_lines(stack[-1], k0)))
     panels = info["panels"]
     G = check(k, w)
+    panels2 = api.halve_panels([tuple(p) for p in panels])
+    kh, wh = api.gl_rule(panels2, order, singular=sing)
+    Gh = check(kh, wh)
+    if np.linalg.norm(G - Gh) <= rtol * np.linalg.norm(Gh):
+        info.update(learned=True, halvings=0, G=Gh, panels=np.asarray(panels2))
+        return kh, wh, info
+    # the proposal missed a pole: the rule of one exact scan, halved until two levels agree
+    P = dict(stack=stack, layers=list(stack), k0=k0, source_layer=source_layer, h_min=h_min)
+    poles = exact_scan_poles_batch([P], ctx=ctx)[0]
+    k, w, info2 = api.grid_from_poles(stack, k0, source_layer, poles, h_min=h_min, rho_max=rho_max, order=order,
+                                      rtol=rtol, ctx=ctx)
+    panels = info2["panels"]
+    G = check(k, w)
     for h in range(max_halvings + 1):
         panels2 = api.halve_panels([tuple(p) for p in panels])
         kh, wh = api.gl_rule(panels2, order, singular=sing)
@@ -286,12 +301,12 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
         if np.linalg.norm(G - Gh) <= rtol * np.linalg.norm(Gh):
             # the check passed: return the finer of the two levels (already solved, and the
             # more accurate; its difference to the coarser one bounds the coarser one's error)
-            info.update(learned=h == 0, halvings=h, G=Gh, panels=np.asarray(panels2))
+            info.update(learned=False, halvings=h + 1, G=Gh, panels=np.asarray(panels2))
             return kh, wh, info
         panels, k, w, G = panels2, kh, wh, Gh
     k, w, info2 = api.point_kx_grid(stack, k0, source_layer, h_min=h_min, rho_max=rho_max, order=order, rtol=rtol,
                                     ctx=ctx)
-    info.update(info2, learned=False, halvings=max_halvings + 1, G=check(k, w))
+    info.update(info2, learned=False, halvings=max_halvings + 2, G=check(k, w))
     return k, w, info
 
 
@@ -404,9 +419,9 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
                         n_scan=2048, solved=None):
     """learned_rule for every problem: the network over all problems' scan grids (features
     formed on the device), the exact window sampling of all problems in one device call,
-    fixed_kρ_rule per problem, then the acceptance check and any
-    plain refinement in batched levels; a problem that never converges falls back to the
-    scanned rule. Returns [(G, k, w, accepted, halvings)]; ``device`` as plain_rules_batch.
+    fixed_kρ_rule per problem, then the acceptance check; the rejected problems take the rule
+    of one exact scan (exact_scan_poles_batch) refined in batched halving levels; a problem that
+    never converges falls back to the reference's scanned rule. Returns [(G, k, w, accepted, halvings)]; ``device`` as plain_rules_batch.
     ``build_rtol`` (default rtol): the tolerance the proposed rules are built for; the
     acceptance check always uses rtol. ``n_scan``: points of the log grid the network is
     evaluated on per problem. ``solved`` as _refine_levels."""
@@ -416,7 +431,7 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     for j, P in enumerate(problems):
         ks = scan_grid(P["k0"], n_k)
         o = pred[j * n_k:(j + 1) * n_k]
-        cands.append(sorted(_score_candidates(ks, o[:, 1], peaks(ks, o[:, 0] * LOG_SCALE))))
+        cands.append(sorted(_score_candidates(ks, o[:, 1], peaks(ks, o[:, 0] * LOG_SCALE, prominence=np.log(1.01)))))
     polesets = refine_poles_batch([(P["stack"], P["k0"], P["source_layer"], c) for P, c in zip(problems, cands)], ctx=ctx)
     rules, panels = [], []
     for P, poles in zip(problems, polesets):
@@ -426,8 +441,23 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
         rules.append((k, w))
         panels.append(info["panels"])
     out = [None] * len(problems)
-    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device,
-                   solved)
+    # the proposals' own check (one level); a rejected proposal missed a pole: its rule comes
+    # from one exact log scan of the response instead (batched over the rejected problems),
+    # refined by halving until two levels agree
+    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, 0, order, ctx, out, device, solved)
+    rej = [i for i, r in enumerate(out) if not r[4]]
+    if rej:
+        scanned = exact_scan_poles_batch([problems[i] for i in rej], ctx=ctx)
+        for i, poles in zip(rej, scanned):
+            P = problems[i]
+            k, w, info = api.grid_from_poles(P["stack"], P["k0"], P["source_layer"], poles, h_min=P["h_min"],
+                                             rho_max=P["rho_max"], order=order, rtol=rtol, ctx=ctx)
+            rules[i], panels[i] = (k, w), info["panels"]
+        sub = [None] * len(problems)
+        _refine_levels(problems, rej, rules, panels, None, rtol, max_halvings, order, ctx, sub, device, solved)
+        for i in rej:
+            g, k, w, h, conv = sub[i]
+            out[i] = (g, k, w, h + 1, conv)
     fall = [i for i, r in enumerate(out) if not r[4]]
     if fall:
         fr = []
@@ -443,6 +473,33 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
         for i, (k, w), g in zip(fall, fr, Gf):
             out[i] = (g, k, w, out[i][3], False)
     return [(g, k, w, conv and h == 0, h) for (g, k, w, h, conv) in out]
+
+
+def exact_scan_poles_batch(problems, step=1e-3, n_local=129, ctx=None):
+    """Real-axis poles (q, Γ) of every problem from its exact cavity response: one log scan from
+    half the lowest light line to Kcut = min(max(target 25 / h_min, 2 kmax), 1e5 kmax) at
+    relative step ``step`` (the reference's scan grid, mod_KSpaceFeatures.jl:151-204), the
+    peaks of the sampled curve (prominence 1.05, light lines excluded), then exact windows
+    around them for the widths the scan step cannot resolve: two batched device calls in all,
+    in place of the reference's sequential refinement rounds."""
+    items, grids = [], []
+    for P in problems:
+        st = P["layers"]
+        ll = sorted({float(x) for L in st for x in api.layer_light_lines(L, P["k0"])})
+        kmax = ll[-1] if ll else P["k0"]
+        kcut = min(max(25.0 / P["h_min"], 2.0 * kmax), 1e5 * kmax)
+        k_lo = 0.5 * (ll[0] if ll else P["k0"])
+        n = int(np.floor(np.log(kcut / k_lo) / step + 1e-10)) + 1
+        ks = k_lo * np.exp(step * np.arange(n))
+        grids.append((ks, ll))
+        items.append((P["stack"], P["k0"], P["source_layer"], ks))
+    Rs = api.cavity_response_batch(items, ctx=ctx)
+    cands = []
+    for (ks, ll), R in zip(grids, Rs):
+        pk = peaks(ks, np.log(np.maximum(R, 1e-300)))
+        cands.append([(q, G) for q, G in pk if all(abs(q - L) > 1e-6 * q for L in ll)])
+    return refine_poles_batch([(P["stack"], P["k0"], P["source_layer"], c) for P, c in zip(problems, cands)],
+                              n_local=n_local, ctx=ctx)
 
 
 def uniform_rule(k0, kmax, npanels, order=8):
