@@ -613,17 +613,20 @@ def test_contour_with_zero_indentation_equals_real_axis_path(ytf):
 
 
 def test_config1_contour_matches_real_axis_oracle(ytf, oracle):
-    """Config 1: vertical dipole 20 nm above the uniaxial film; 4096 nodes (512 GL-8 panels)
-    on the contour kρ = t - 0.05 i k0 sin(π t / 20 k0), t in [0, 20 k0]. With the film's loss
-    every pole and branch point lies above the real axis, so by Cauchy's theorem the contour
-    integral equals the oracle's real-axis integral over [0, 20 k0] (dense rule: breaks at the
-    light lines, u² substitution at the half-space ones): G within 1e-6."""
+    """The 3-layer dipole problem at its full size: vertical dipole 20 nm above the uniaxial
+    film, 4096 nodes (512 GL-8 panels) on the contour kρ = t - 0.05 i k0 sin(π t / 20 k0),
+    t in [0, 20 k0], G on 256 radii log-spaced over 6-3000 nm x 64 heights over 0-200 nm. With
+    the film's loss every pole lies above the real axis and the branch points on it, so by
+    Cauchy's theorem the contour integral equals the oracle's real-axis integral over
+    [0, 20 k0] (dense rule: breaks at the light lines, u² substitution at the half-space
+    ones, ~48k nodes): G and Gzz within 1e-6."""
     st = config1_stack()
     k0 = 2 * np.pi / 600.0
+    oracle.set_threads(__import__("os").cpu_count() or 1)
     k, w = ytf.contour_rule(k0, npanels=512, order=8)
     gc = ytf.build_cavity_transfer_1d_contour(st, k0, 1, k, w, obs_layers=[1])
-    rho = np.geomspace(6.0, 3000.0, 24)
-    zo = np.linspace(0.0, 200.0, 9)
+    rho = np.geomspace(6.0, 3000.0, 256)
+    zo = np.linspace(0.0, 200.0, 64)
     Gc = ytf.closed_form_G(gc, 1, 20.0, zo, rho, [0.0])
     lines = sorted({float(x) for L in st for x in oracle.light_lines(L, k0, 0.0) if 0 < x < 20 * k0})
     sing = sorted({float(x) for L in (st[0], st[-1]) for x in oracle.light_lines(L, k0, 0.0)})

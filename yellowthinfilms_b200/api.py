@@ -491,14 +491,23 @@ def grid_from_poles(stack, omega, source_layer, poles, h_min, rho_max=0.0, targe
     return _grid(stack, omega, source_layer, h_min, rho_max, target_decay, kr_cap, False, order, rtol, ctx, list(poles))
 
 
-def contour_rule(k0, npanels=512, order=8, L=None, h=None):
+def contour_rule(k0, npanels=512, order=8, L=None, h=None, breaks=()):
     """Gauss–Legendre rule on the deformed path kρ(t) = t - i h sin(π t / L), t in [0, L]
     (defaults L = 20 k0, h = 0.05 k0: below the real axis, back on it at both ends). Returns
-    complex nodes and weights (w = kρ'(t) w_t)."""
+    complex nodes and weights (w = kρ'(t) w_t). ``breaks``: values of t in (0, L) where panels
+    must end (the half-space light lines: the path passes closest to those branch points there,
+    and a panel edge at them keeps the rule's convergence geometric); the npanels are shared
+    among the segments in proportion to their lengths, uniform within each."""
     L = 20.0 * k0 if L is None else float(L)
     h = 0.05 * k0 if h is None else float(h)
     x, wx = gausslegendre(order)
-    edges = np.linspace(0.0, L, npanels + 1)
+    bs = sorted({0.0, L} | {float(b) for b in breaks if 0.0 < float(b) < L})
+    if len(bs) == 2:
+        edges = np.linspace(0.0, L, npanels + 1)
+    else:
+        seg = np.diff(bs)
+        cnt = np.maximum(1, np.round(npanels * seg / L).astype(int))
+        edges = np.unique(np.concatenate([np.linspace(a, b, n + 1) for a, b, n in zip(bs[:-1], bs[1:], cnt)]))
     c = 0.5 * (edges[1:] + edges[:-1])
     hw = 0.5 * np.diff(edges)
     t = (c[:, None] + hw[:, None] * x[None, :]).ravel()
