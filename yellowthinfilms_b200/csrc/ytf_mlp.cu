@@ -13,69 +13,176 @@
 //   forward  Z[b][o]  = Σ_i H[b][i] W[o][i] + bias[o]   (then GELU)
 //   input    dH[b][i] = Σ_o dZ[b][o] W[o][i]
 //   weights  dW[o][i] = Σ_b dZ[b][o] H[b][i]
-// C[m][n] = Σ_k A(m, k) B(k, n), A(m, k) = A[m sam + k sak], B(k, n) = B[k sbk + n sbn],
-// 64 x 64 tiles, 16-deep K steps through shared memory, 256 threads with 4 x 4 outputs each.
+// C[m][n] = Σ_k A(m, k) B(k, n), A(m, k) = A[m sam + k sak], B(k, n) = B[k sbk + n sbn], on the
+// tensor cores (tcgen05.mma kind::f16, BF16 operands, FP32 accumulation in tensor memory). The
+// BF16 weights enter as they are; an FP32 operand (activations, gradients) is split into two
+// BF16 terms hi = bf16(v), lo = bf16(v - hi), and the products hi·hi, hi·lo, lo·hi are summed,
+// so an FP32 operand keeps about 16 significant bits (the dropped lo·lo is below 2^-16 of it).
+// A CTA computes a 128 x Np tile (Np = N rounded up to 16, at most 256) over K in blocks of
+// 128: its 128 threads convert the block's operands into shared memory (planes of 64-byte rows,
+// 32 BF16 each, the canonical no-swizzle K-major layout), one thread issues the block's MMAs,
+// their commit frees the buffers for the next block; the 4 warps then drain the accumulator
+// (warp w: tensor-memory lanes 32w..32w+31 = the tile's rows) with bias, accumulation and GELU.
 #include <cuda_bf16.h>
 
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/ytf.h"
+#include "ytf_tcgen05.cuh"
 
 namespace ytf {
 namespace mlp {
 
-constexpr int TM = 64, TN = 64, TK = 16;
+constexpr int GM = 128;          // tile rows (MMA M)
+constexpr int GNMAX = 256;       // largest tile width (MMA N)
+constexpr int GKB = 128;         // K per block: 4 planes of 32
+constexpr long GWAIT = 1L << 24; // polls of the bounded commit wait
+
+__device__ __forceinline__ uint32_t plane_bf(int r, int k) { return plane_off(r, 2 * k); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred PD;\n\t"
+      "setp.ne.b32 PD, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, PD;\n\t}" ::"r"(tmem),
+      "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+// the two BF16 terms of a source value (the second is 0 for a BF16 source)
+__device__ __forceinline__ void split_bf(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(v);
+  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
 
 template <class TA, class TB>
-__global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const TA* __restrict__ A, long sam, long sak,
-                                              const TB* __restrict__ B, long sbk, long sbn, float* __restrict__ C,
-                                              long ldc, const float* __restrict__ bias, float* __restrict__ H, int act,
-                                              int accumulate) {
-  __shared__ float As[TK][TM + 1];
-  __shared__ float Bs[TK][TN + 1];
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
-  float acc[4][4] = {};
-  for (int k0 = 0; k0 < K; k0 += TK) {
-    for (int e = threadIdx.x; e < TK * TM; e += 256) {
-      const int kk = e / TM, mm = e % TM;
-      const int m = m0 + mm, k = k0 + kk;
-      As[kk][mm] = (m < M && k < K) ? (float)A[m * sam + k * sak] : 0.f;
-    }
-    for (int e = threadIdx.x; e < TK * TN; e += 256) {
-      const int kk = e / TN, nn = e % TN;
-      const int n = n0 + nn, k = k0 + kk;
-      Bs[kk][nn] = (n < N && k < K) ? (float)B[k * sbk + n * sbn] : 0.f;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < TK; ++kk) {
-      float a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
+__global__ void __launch_bounds__(128, 1) k_gemm_tc(int M, int N, int K, const TA* __restrict__ A, long sam, long sak,
+                                                     const TB* __restrict__ B, long sbk, long sbn,
+                                                     float* __restrict__ C, long ldc, const float* __restrict__ bias,
+                                                     float* __restrict__ H, int act, int accumulate,
+                                                     unsigned* __restrict__ err) {
+  constexpr bool SA = std::is_same<TA, float>::value;  // split A into two terms
+  constexpr bool SB = std::is_same<TB, float>::value;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t done;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * GM, n0 = blockIdx.x * GNMAX;
+  const int nt = min(GNMAX, N - n0);
+  const int Np = ((nt + 15) / 16) * 16;
+  const uint32_t planeA = GM * 64u, planeB = (uint32_t)Np * 64u;
+  constexpr int NPL = GKB / 32;
+  uint8_t* Ahi = smem;
+  uint8_t* Alo = Ahi + NPL * planeA;
+  uint8_t* Bhi = Alo + (SA ? NPL * planeA : 0);
+  uint8_t* Blo = Bhi + NPL * planeB;
+  if (tid == 0) {
+    mbar_init(smem_u32(&done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
-      if (m >= M || n >= N) continue;
-      float z = acc[i][j] + (bias ? bias[n] : 0.f);
-      if (accumulate) z += C[m * ldc + n];
-      C[m * ldc + n] = z;
-      if (H) H[m * ldc + n] = act ? 0.5f * z * (1.f + erff(z * 0.70710678118654752f)) : z;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(GNMAX)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+  // kind::f16: D F32 (bit 4), A BF16 (bits 7-9 = 1), B BF16 (bits 10-12 = 1), both K-major
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(Np >> 3) << 17) | ((uint32_t)(GM >> 4) << 24);
+  bool ok = true;
+  int round = 0;
+  for (int k0 = 0; k0 < K; k0 += GKB, ++round) {
+    if (round > 0) {
+      // the previous block's MMAs have read the buffers before they are overwritten
+      bool got = false;
+      for (long it = 0; it < GWAIT && !got; ++it) got = mbar_try(smem_u32(&done), (round - 1) & 1);
+      if (!got) { ok = false; if (tid == 0) atomicOr(err, 1u); break; }
     }
+    for (int e = tid; e < GM * GKB; e += 128) {
+      int r, k;
+      if (sak == 1) { r = e / GKB; k = e % GKB; } else { k = e / GM; r = e % GM; }
+      const int m = m0 + r, kk = k0 + k;
+      const float v = (m < M && kk < K) ? (float)A[(long)m * sam + (long)kk * sak] : 0.f;
+      __nv_bfloat16 hi, lo;
+      split_bf(v, hi, lo);
+      const uint32_t off = (k >> 5) * planeA + plane_bf(r, k & 31);
+      *reinterpret_cast<__nv_bfloat16*>(Ahi + off) = hi;
+      if (SA) *reinterpret_cast<__nv_bfloat16*>(Alo + off) = lo;
+    }
+    for (int e = tid; e < Np * GKB; e += 128) {
+      int r, k;
+      if (sbk == 1) { r = e / GKB; k = e % GKB; } else { k = e / Np; r = e % Np; }
+      const int n = n0 + r, kk = k0 + k;
+      const float v = (r < nt && kk < K) ? (float)B[(long)kk * sbk + (long)n * sbn] : 0.f;
+      __nv_bfloat16 hi, lo;
+      split_bf(v, hi, lo);
+      const uint32_t off = (k >> 5) * planeB + plane_bf(r, k & 31);
+      *reinterpret_cast<__nv_bfloat16*>(Bhi + off) = hi;
+      if (SB) *reinterpret_cast<__nv_bfloat16*>(Blo + off) = lo;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int pl = 0; pl < NPL; ++pl)
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const uint32_t oa = pl * planeA + t * 256u, ob = pl * planeB + t * 256u;
+          // the first MMA of the tile overwrites the accumulator, every other one adds to it
+          mma_bf16(tmem, umma_desc(smem_u32(Ahi + oa)), umma_desc(smem_u32(Bhi + ob)), idesc,
+                   (k0 > 0 || pl > 0 || t > 0) ? 1u : 0u);
+          if (SB) mma_bf16(tmem, umma_desc(smem_u32(Ahi + oa)), umma_desc(smem_u32(Blo + ob)), idesc, 1u);
+          if (SA) mma_bf16(tmem, umma_desc(smem_u32(Alo + oa)), umma_desc(smem_u32(Bhi + ob)), idesc, 1u);
+        }
+      tc_commit(smem_u32(&done));
+    }
+  }
+  // the last block's MMAs (and with them every earlier one) complete before the drain
+  if (round > 0) {
+    bool got = false;
+    for (long it = 0; it < GWAIT && !got; ++it) got = mbar_try(smem_u32(&done), (round - 1) & 1);
+    if (!got) { ok = false; if (tid == 0) atomicOr(err, 1u); }
+  }
+  ok = __all_sync(0xffffffffu, ok);
+  tc_fence_after();
+  if (ok && round > 0) {
+    const int m = m0 + 32 * warp + lane;
+    const uint32_t lanebase = (uint32_t)(32 * warp) << 16;
+    for (int c0 = 0; c0 < Np; c0 += 8) {
+      uint32_t v[8];
+      tmem_ld8(tmem + lanebase + c0, v);
+      tmem_wait_ld();
+      if (m < M) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int n = n0 + c0 + j;
+          if (c0 + j >= nt) break;
+          float z = __uint_as_float(v[j]) + (bias ? bias[n] : 0.f);
+          if (accumulate) z += C[(long)m * ldc + n];
+          C[(long)m * ldc + n] = z;
+          if (H) H[(long)m * ldc + n] = act ? 0.5f * z * (1.f + erff(z * 0.70710678118654752f)) : z;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(GNMAX) : "memory");
+}
+
+template <class TA, class TB>
+size_t gemm_tc_smem(int Np) {
+  constexpr bool SA = std::is_same<TA, float>::value, SB = std::is_same<TB, float>::value;
+  return (size_t)(GKB / 32) * ((SA ? 2 : 1) * GM * 64 + (SB ? 2 : 1) * (size_t)Np * 64);
 }
 
 // dZ = dH * GELU'(Z), GELU'(z) = Φ(z) + z φ(z)
@@ -162,6 +269,7 @@ struct ytf_mlp {
   long cap = 0;
   std::vector<float*> Z, H, dZ, dH;
   float *T = nullptr, *lb = nullptr, *X = nullptr;
+  unsigned* tc_err = nullptr;      // set by a tensor-core GEMM whose commit wait ran out
   std::string err;
   ~ytf_mlp() {
     cudaFree(p); cudaFree(g); cudaFree(m); cudaFree(v); cudaFree(wb);
@@ -169,7 +277,7 @@ struct ytf_mlp {
     for (auto* q : H) cudaFree(q);
     for (auto* q : dZ) cudaFree(q);
     for (auto* q : dH) cudaFree(q);
-    cudaFree(T); cudaFree(lb); cudaFree(X);
+    cudaFree(T); cudaFree(lb); cudaFree(X); cudaFree(tc_err);
   }
 };
 
@@ -186,10 +294,16 @@ int mfail(ytf_mlp* n, int code, const std::string& msg) {
   } while (0)
 
 template <class TA, class TB>
-cudaError_t gemm(cudaStream_t s, int M, int N, int K, const TA* A, long sam, long sak, const TB* B, long sbk, long sbn,
+cudaError_t gemm(ytf_mlp* net, int M, int N, int K, const TA* A, long sam, long sak, const TB* B, long sbk, long sbn,
                  float* C, long ldc, const float* bias, float* H, int act, int accumulate) {
-  dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM);
-  k_gemm<TA, TB><<<grid, 256, 0, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, bias, H, act, accumulate);
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  const int Np = ((std::min(N, GNMAX) + 15) / 16) * 16;
+  const size_t sm = gemm_tc_smem<TA, TB>(Np);
+  cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  dim3 grid((N + GNMAX - 1) / GNMAX, (M + GM - 1) / GM);
+  k_gemm_tc<TA, TB><<<grid, 128, sm, net->stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, bias, H, act, accumulate,
+                                                   net->tc_err);
   return cudaGetLastError();
 }
 
@@ -227,7 +341,7 @@ int forward(ytf_mlp* net, int B) {
   MCK(cudaGetLastError());
   for (int l = 1; l <= L; ++l) {
     const int in = net->sizes[l - 1], out = net->sizes[l];
-    MCK((gemm<float, __nv_bfloat16>(net->stream, B, out, in, net->H[l - 1], in, 1, net->wb + net->woff[l - 1], 1, in,
+    MCK((gemm<float, __nv_bfloat16>(net, B, out, in, net->H[l - 1], in, 1, net->wb + net->woff[l - 1], 1, in,
                                    net->Z[l], out, net->p + net->boff[l - 1], net->H[l], l < L ? 1 : 0, 0)));
   }
   return YTF_OK;
@@ -246,12 +360,12 @@ int backward(ytf_mlp* net, int B) {
       MCK(cudaGetLastError());
     }
     // dW = dZ^T H, db = Σ dZ
-    MCK((gemm<float, float>(net->stream, out, in, B, net->dZ[l], 1, out, net->H[l - 1], in, 1, net->g + net->woff[l - 1],
+    MCK((gemm<float, float>(net, out, in, B, net->dZ[l], 1, out, net->H[l - 1], in, 1, net->g + net->woff[l - 1],
                            in, nullptr, nullptr, 0, 0)));
     k_colsum<<<(out + 255) / 256, 256, 0, net->stream>>>(B, out, net->dZ[l], net->g + net->boff[l - 1]);
     MCK(cudaGetLastError());
     if (l > 1)
-      MCK((gemm<float, __nv_bfloat16>(net->stream, B, in, out, net->dZ[l], out, 1, net->wb + net->woff[l - 1], in, 1,
+      MCK((gemm<float, __nv_bfloat16>(net, B, in, out, net->dZ[l], out, 1, net->wb + net->woff[l - 1], in, 1,
                                      net->dH[l - 1], in, nullptr, nullptr, 0, 0)));
   }
   return YTF_OK;
@@ -293,11 +407,11 @@ int ytf_mlp_create(int device, int nlayers, const int* sizes, unsigned long long
   int rc = YTF_OK;
   if (cudaMalloc(&net->p, 4 * o) != cudaSuccess || cudaMalloc(&net->g, 4 * o) != cudaSuccess ||
       cudaMalloc(&net->m, 4 * o) != cudaSuccess || cudaMalloc(&net->v, 4 * o) != cudaSuccess ||
-      cudaMalloc(&net->wb, 2 * o) != cudaSuccess)
+      cudaMalloc(&net->wb, 2 * o) != cudaSuccess || cudaMalloc(&net->tc_err, sizeof(unsigned)) != cudaSuccess)
     rc = YTF_ERR_NOMEM;
   if (!rc && (cudaMemcpy(net->p, h.data(), 4 * o, cudaMemcpyHostToDevice) != cudaSuccess ||
               cudaMemset(net->m, 0, 4 * o) != cudaSuccess || cudaMemset(net->v, 0, 4 * o) != cudaSuccess ||
-              cudaMemset(net->g, 0, 4 * o) != cudaSuccess))
+              cudaMemset(net->g, 0, 4 * o) != cudaSuccess || cudaMemset(net->tc_err, 0, sizeof(unsigned)) != cudaSuccess))
     rc = YTF_ERR_CUDA;
   if (rc) { delete net; return rc; }
   *out = net;
