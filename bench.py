@@ -684,7 +684,7 @@ def run_learned(args):
     prec = args.precision if args.precision != "split_bf16" else "int8x3"
 
     # training (outside the timed region, reported beside it)
-    n_train = N_TRAIN_SAMPLES // N_SCAN
+    n_train = args.train_samples // N_SCAN
     t = time.perf_counter()
     X, T = L.training_set(n_train, n_k=N_SCAN, seed=SEED, ctx=ctx)
     t_data = time.perf_counter() - t
@@ -701,8 +701,9 @@ def run_learned(args):
     t_train = a.elapsed_time(b) * 1e-3
     del Xd, Td
 
-    stacks = learned_stacks()
-    chunks = [list(range(c, min(c + CHUNK, N_TEST))) for c in range(0, N_TEST, CHUNK)]
+    n_test = args.stacks
+    stacks = learned_stacks(n_test)
+    chunks = [list(range(c, min(c + CHUNK, n_test))) for c in range(0, n_test, CHUNK)]
     mine = chunks[rank::world] or chunks[:1]
     dev_stacks = {}
 
@@ -833,7 +834,8 @@ def run_learned(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": f"f64 node solve, {prec} tensor-core synthesis; MLP bf16 weights, fp32 accum",
             "data": "synthetic (seeded)", "impl": "learned-adaptive",
-            "config": dict(LEARNED_CONFIG, precision=prec, steps_cover_stacks=rec["stacks"] * world),
+            "config": dict(LEARNED_CONFIG, precision=prec, steps_cover_stacks=rec["stacks"] * world,
+                           held_out_stacks=n_test, train_samples=n_train * N_SCAN),
             "plain_entries_per_s": plain, "learned_vs_plain": t_p / t_l,
             "gzz_entries_per_s": value / 9,
             "max_rel_err_vs_reference": max(err_l, err_p), "max_rel_err_learned": err_l, "max_rel_err_plain": err_p,
@@ -1000,6 +1002,10 @@ def main():
                          "(default, the headline metric); gyro32: the 8-layer stack at 32 wavelengths; uneven: 1024 "
                          "uneven stacks; bessel: the 1D Bessel synthesis at 4096 radii x 65536 nodes x 256 heights; "
                          "contour: the config-1 path on the deformed contour")
+    ap.add_argument("--stacks", type=int, default=N_TEST,
+                    help="learned workload: held-out stacks (default 4096; fewer only for profiling runs)")
+    ap.add_argument("--train-samples", type=int, default=N_TRAIN_SAMPLES,
+                    help="learned workload: training samples (default 1e7; fewer only for profiling runs)")
     ap.add_argument("--retune", action="store_true",
                     help="uneven workload: tune the plan again even if the tuning database has its class")
     ap.add_argument("--calls", default="plan", choices=["plan", "batched", "per-call"],

@@ -17,17 +17,17 @@
 #include "ytf_complex.cuh"
 #include "ytf_kernels.h"
 #include "ytf_tcgen05.cuh"
-#include "ytf_digits.cuh"
 
 namespace ytf {
 
 constexpr int BI_M = 128;
-
+constexpr int BI_NODES = 64;  // nodes per stage: one byte each, 64-byte rows (2 MMAs of K = 32)
 constexpr int BI_STAGES = 4;
 constexpr int BI_THREADS = 192;
 constexpr int BI_ACC_STRIDE = 160;
 constexpr int BI_TMEM_COLS = 512;
 constexpr long BI_WAIT_LIMIT = 1L << 22;  // polls of the drain waits (the pipeline waits: p.wait_limit)
+constexpr double BI_SCALE = 8355000.0;
 
 size_t bessel_i8_stage_bytes_a() { return 3ul * BI_M * 64; }
 size_t bessel_i8_stage_bytes_b(int Np) { return 3ul * (size_t)Np * 64; }
@@ -55,6 +55,114 @@ __device__ __forceinline__ double bessel_j012(int order, double x) {
   return (2.0 / x) * j1(x) - j0(x);
 }
 
+__device__ __forceinline__ void digits3b(int Y, uint32_t& d0, uint32_t& d1, uint32_t& d2) {
+  d2 = (uint32_t)Y & 255u;
+  d1 = (uint32_t)((Y + 128) >> 8) & 255u;
+  d0 = (uint32_t)((Y + 32896) >> 16) & 255u;
+}
+
+__device__ __forceinline__ double col_scale(unsigned long long bits) {
+  const double m = __longlong_as_double((long long)bits);
+  return (m > 0.0 && isfinite(m)) ? BI_SCALE / m : 0.0;
+}
+
+// per (slice, column) max |C| as IEEE bits (Inf for a non-finite entry)
+__global__ void k_bcolmax(BesselI8 p) {
+  const int col = blockIdx.x, z = blockIdx.y;
+  const long k0 = (long)z * p.kchunk, k1 = min(p.K, k0 + p.kchunk);
+  const double* c = p.C + (long)col * p.K;
+  double m = 0.0;
+  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    const double v = c[k];
+    m = isfinite(v) ? fmax(m, fabs(v)) : __longlong_as_double(0x7ff0000000000000LL);
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) p.colmax[(long)z * p.N + col] = (unsigned long long)__double_as_longlong(red[0]);
+}
+
+// one thread per (column tile, row slot, slice, 16-node group): 16 bytes of each digit plane
+// one thread per 4 consecutive nodes of a column slot (one 32-bit word of each digit plane):
+// adjacent threads read adjacent 32-byte runs of C
+__global__ void k_bimg_real(BesselI8 p) {
+  const long words = p.kchunk / 4;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = (long)p.ntile_n * p.Np * p.nchunk * words;
+  if (t >= total) return;
+  const long wq = t % words;
+  long rest = t / words;
+  const int z = (int)(rest % p.nchunk);
+  rest /= p.nchunk;
+  const int slot = (int)(rest % p.Np);
+  const int ct = (int)(rest / p.Np);
+  const int col = ct * p.ctile + slot;
+  const bool cv = slot < p.ctile && col < p.N;
+  const double sB = cv ? col_scale(p.colmax[(long)z * p.N + col]) : 0.0;
+  const long g = wq / 4;
+  const int q = (int)(wq % 4);
+  uint32_t b[3][4];
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
+    const double v = (cv && k < p.K) ? p.C[(long)col * p.K + k] : 0.0;
+    uint32_t d0, d1, d2;
+    digits3b(__double2int_rn(v * sB), d0, d1, d2);
+    b[0][h] = d0; b[1][h] = d1; b[2][h] = d2;
+  }
+  const long nstage = p.kchunk / BI_NODES;
+  const int s = (int)(g / 4), kb = (int)(g % 4) * 16;
+  const size_t sbytes = 3ul * (size_t)p.Np * 64;
+  uint8_t* blk = p.Bimg + (((size_t)ct * p.nchunk + z) * nstage + s) * sbytes;
+#pragma unroll
+  for (int pl = 0; pl < 3; ++pl)
+    *reinterpret_cast<uint32_t*>(blk + (size_t)pl * p.Np * 64 + plane_off(slot, kb) + 4 * q) =
+        b[pl][0] | (b[pl][1] << 8) | (b[pl][2] << 16) | (b[pl][3] << 24);
+}
+
+// one thread per (radius tile, row, slice, 16-node group): J_n(k ρ) straight into digits
+__global__ void k_aimg_bessel(BesselI8 p) {
+  const long groups = p.kchunk / 16;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = (long)p.ntile_m * BI_M * p.nchunk * groups;
+  if (t >= total) return;
+  const long g = t % groups;
+  long rest = t / groups;
+  const int z = (int)(rest % p.nchunk);
+  rest /= p.nchunk;
+  const int row = (int)(rest % BI_M);
+  const int mt = (int)(rest / BI_M);
+  const int r = mt * BI_M + row;
+  const bool rv = r < p.M;
+  const double rho = rv ? p.rho[r] : 0.0;
+  uint32_t w[3][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint32_t b[3][4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
+      const double v = (rv && k < p.K) ? bessel_j012(p.order, p.kr[k] * rho) : 0.0;
+      uint32_t d0, d1, d2;
+      digits3b(__double2int_rn(v * BI_SCALE), d0, d1, d2);
+      b[0][h] = d0; b[1][h] = d1; b[2][h] = d2;
+    }
+#pragma unroll
+    for (int pl = 0; pl < 3; ++pl) w[pl][q] = b[pl][0] | (b[pl][1] << 8) | (b[pl][2] << 16) | (b[pl][3] << 24);
+  }
+  const long nstage = p.kchunk / BI_NODES;
+  const int s = (int)(g / 4), kb = (int)(g % 4) * 16;
+  const size_t sbytes = 3ul * BI_M * 64;
+  uint8_t* blk = p.Aimg + (((size_t)mt * p.nchunk + z) * nstage + s) * sbytes;
+#pragma unroll
+  for (int pl = 0; pl < 3; ++pl)
+    *reinterpret_cast<uint4*>(blk + (size_t)pl * BI_M * 64 + plane_off(row, kb)) =
+        make_uint4(w[pl][0], w[pl][1], w[pl][2], w[pl][3]);
+}
 
 // k_aimg_bessel for all three orders at once: J_0 and J_1 once per (ρ, k), J_2 from them
 // (series below |x| = 1, recurrence above, as bessel_j012), three images in the same layout.
@@ -298,6 +406,18 @@ cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s) {
       (long)p.nchunk * p.kchunk < p.K)
     return cudaErrorInvalidValue;
   cudaError_t e;
+  k_bcolmax<<<dim3((unsigned)p.N, (unsigned)p.nchunk), 256, 0, s>>>(p);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  {
+    const long total = (long)p.ntile_n * p.Np * p.nchunk * (p.kchunk / 4);
+    k_bimg_real<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (!p.aimg_ready) {
+    const long total = (long)p.ntile_m * BI_M * p.nchunk * (p.kchunk / 16);
+    k_aimg_bessel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   const size_t sm = bessel_i8_smem(p.Np);
   if ((e = cudaFuncSetAttribute(k_gemm_i8_img, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
     return e;

@@ -1360,86 +1360,6 @@ static int synth_setup(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double z
 static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const double* drho, int precision, int nsm,
                      const GreenBatch* gb, double* P0, double* P1, double* P2) {
   const long nk = sp.c.n;
-  if (precision == YTF_PREC_INT8X3 && !sp.c.kri) {
-    // int8 tensor cores: J_n(kρ) and the coefficient columns as fixed-point digit images,
-    // exact INT32 accumulation, FP64 sum of the node slices into P_n. The coefficient digit
-    // images of the three orders come straight from the reflected amplitudes (two passes:
-    // column maxima, digits), so no FP64 coefficient column is stored
-    double* Pn8[3] = {P0, P1, P2};
-    const int Nn8[3] = {10 * nz, 8 * nz, 8 * nz};
-    unsigned* err = gb ? gb->err : nullptr;
-    if (!err) {
-      WS(e1, unsigned, "g_tc_err", 1);
-      err = e1;
-      CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
-    }
-    // one node slicing for the three orders (that of order 0, the widest), so the J_n digit
-    // images of all three come from one Bessel evaluation per (ρ, k)
-    long kchunk;
-    {
-      const int ct0 = bessel_i8_ctile(Nn8[0]);
-      const long tiles = (long)((nr + 127) / 128) * ((Nn8[0] + ct0 - 1) / ct0);
-      const long want = std::max(1L, (long)nsm / tiles);
-      kchunk = (nk + want - 1) / want;
-      kchunk = std::min(16384L, std::max(64L, ((kchunk + 63) / 64) * 64));
-    }
-    const int nchunk = (int)((nk + kchunk - 1) / kchunk);
-    const size_t nst = (size_t)(kchunk / 64);
-    const size_t abytes = (size_t)((nr + 127) / 128) * nchunk * nst * bessel_i8_stage_bytes_a();
-    WS(A0i, uint8_t, "g_bi_a0", abytes);
-    WS(A1i, uint8_t, "g_bi_a1", abytes);
-    WS(A2i, uint8_t, "g_bi_a2", abytes);
-    uint8_t* Aord[3] = {A0i, A1i, A2i};
-    BesselI8 bp[3];
-    CoefImg ci;
-    std::memset(&ci, 0, sizeof(ci));
-    ci.kchunk = kchunk;
-    ci.nchunk = nchunk;
-    size_t ptot = 0;
-    for (int o = 0; o < 3; ++o) {
-      BesselI8& b = bp[o];
-      std::memset(&b, 0, sizeof(b));
-      b.M = nr; b.N = Nn8[o]; b.K = nk; b.order = o;
-      b.ctile = bessel_i8_ctile(b.N);
-      b.Np = ((b.ctile + 15) / 16) * 16;
-      b.ntile_n = (b.N + b.ctile - 1) / b.ctile;
-      b.ntile_m = (nr + 127) / 128;
-      b.kchunk = kchunk;
-      b.nchunk = nchunk;
-      b.kr = sp.c.kr; b.rho = drho; b.Aimg = Aord[o]; b.err = err;
-      b.wait_limit = ctx->wait_limit;
-      ptot = std::max(ptot, (size_t)b.nchunk * b.N * nr);
-      ci.N[o] = b.N; ci.ctile[o] = b.ctile; ci.Np[o] = b.Np;
-    }
-    static const char* bnames[3] = {"g_bi_b0", "g_bi_b1", "g_bi_b2"};
-    for (int o = 0; o < 3; ++o) {
-      WS(Bi, uint8_t, bnames[o], (size_t)bp[o].ntile_n * nchunk * nst * bessel_i8_stage_bytes_b(bp[o].Np));
-      bp[o].Bimg = ci.Bimg[o] = Bi;
-    }
-    size_t cmtot = (size_t)nchunk * (Nn8[0] + Nn8[1] + Nn8[2]);
-    WS(cm, unsigned long long, "g_bi_cmax", cmtot);
-    CK(cudaMemsetAsync(cm, 0, sizeof(unsigned long long) * cmtot, ctx->stream));
-    bp[0].colmax = ci.colmax[0] = cm;
-    bp[1].colmax = ci.colmax[1] = cm + (size_t)nchunk * Nn8[0];
-    bp[2].colmax = ci.colmax[2] = cm + (size_t)nchunk * (Nn8[0] + Nn8[1]);
-    WS(pt, double, "g_bi_part", ptot);
-    WS(amp1, double2, "g_amp", (size_t)12 * nk);
-    CK(LAUNCH("k_reflect2d", launch_reflect_amp(sp, amp1, ctx->stream)));
-    CK(LAUNCH("k_coef_img", launch_coef_colmax(sp, amp1, ci, ctx->stream)));
-    CK(LAUNCH("k_coef_img", launch_coef_bimg(sp, amp1, ci, ctx->stream)));
-    CK(LAUNCH("k_bessel_img", launch_bessel_i8_aimg3(bp[0], A0i, A1i, A2i, ctx->stream)));
-    for (int o = 0; o < 3; ++o) {
-      bp[o].partial = pt;
-      CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp[o], Pn8[o], ctx->stream)));
-    }
-    if (!gb) {
-      unsigned herr = 0;
-      CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
-    }
-    return YTF_OK;
-  }
     WS(C, double, "g_C", 26 * (size_t)nz * nk);
     double *C0 = C, *C1 = C + 10 * (size_t)nz * nk, *C2 = C + 18 * (size_t)nz * nk;
     WS(amp1, double2, "g_amp", (size_t)12 * nk);
@@ -1466,6 +1386,63 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
         }
         CK(LAUNCH("k_combine_complex", launch_combine_complex(nr, Nn[o], Pab, Pab + (size_t)nr * 10 * nz, Pn[o],
                                                               ctx->stream)));
+      }
+      return YTF_OK;
+    }
+    if (precision == YTF_PREC_INT8X3) {
+      // int8 tensor cores: J_n(kρ) and the coefficient columns as fixed-point digit images,
+      // exact INT32 accumulation, FP64 sum of the node slices into P_n
+      const double* Cn8[3] = {C0, C1, C2};
+      double* Pn8[3] = {P0, P1, P2};
+      const int Nn8[3] = {10 * nz, 8 * nz, 8 * nz};
+      unsigned* err = gb ? gb->err : nullptr;
+      if (!err) {
+        WS(e1, unsigned, "g_tc_err", 1);
+        err = e1;
+        CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+      }
+      // one node slicing for the three orders (that of order 0, the widest), so the J_n
+      // digit images of all three come from one Bessel evaluation per (ρ, k)
+      long kchunk;
+      {
+        const int ct0 = bessel_i8_ctile(Nn8[0]);
+        const long tiles = (long)((nr + 127) / 128) * ((Nn8[0] + ct0 - 1) / ct0);
+        const long want = std::max(1L, (long)nsm / tiles);
+        kchunk = (nk + want - 1) / want;
+        kchunk = std::min(16384L, std::max(64L, ((kchunk + 63) / 64) * 64));
+      }
+      const int nchunk = (int)((nk + kchunk - 1) / kchunk);
+      const size_t nst = (size_t)(kchunk / 64);
+      const size_t abytes = (size_t)((nr + 127) / 128) * nchunk * nst * bessel_i8_stage_bytes_a();
+      WS(A0i, uint8_t, "g_bi_a0", abytes);
+      WS(A1i, uint8_t, "g_bi_a1", abytes);
+      WS(A2i, uint8_t, "g_bi_a2", abytes);
+      uint8_t* Aord[3] = {A0i, A1i, A2i};
+      for (int o = 0; o < 3; ++o) {
+        BesselI8 bp;
+        std::memset(&bp, 0, sizeof(bp));
+        bp.M = nr; bp.N = Nn8[o]; bp.K = nk; bp.order = o;
+        bp.ctile = bessel_i8_ctile(bp.N);
+        bp.Np = ((bp.ctile + 15) / 16) * 16;
+        bp.ntile_n = (bp.N + bp.ctile - 1) / bp.ctile;
+        bp.ntile_m = (nr + 127) / 128;
+        bp.kchunk = kchunk;
+        bp.nchunk = nchunk;
+        WS(Bi, uint8_t, "g_bi_b", (size_t)bp.ntile_n * bp.nchunk * nst * bessel_i8_stage_bytes_b(bp.Np));
+        WS(cm, unsigned long long, "g_bi_cmax", (size_t)bp.nchunk * bp.N);
+        WS(pt, double, "g_bi_part", (size_t)bp.nchunk * bp.N * nr);
+        bp.kr = sp.c.kr; bp.rho = drho; bp.C = Cn8[o];
+        bp.Aimg = Aord[o]; bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
+        bp.wait_limit = ctx->wait_limit;
+        if (o == 0) CK(LAUNCH("k_bessel_i8", launch_bessel_i8_aimg3(bp, A0i, A1i, A2i, ctx->stream)));
+        bp.aimg_ready = 1;
+        CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pn8[o], ctx->stream)));
+      }
+      if (!gb) {
+        unsigned herr = 0;
+        CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
       }
       return YTF_OK;
     }

@@ -239,32 +239,15 @@ struct BesselI8 {
   int nchunk;
   const double* kr;  // [K]
   const double* rho; // [M]
+  const double* C;   // [N][K]
   uint8_t* Aimg;     // [ntile_m][nchunk][kchunk/64][3][128 x 64 B]
   uint8_t* Bimg;     // [ntile_n][nchunk][kchunk/64][3][Np x 64 B]
   unsigned long long* colmax;  // [nchunk][N]
   double* partial;   // [nchunk][N][M]
   unsigned* err;
   long wait_limit;   // polls of each bounded pipeline wait before it gives up
+  int aimg_ready;    // Aimg already holds this order's J_n digits (launch_bessel_i8_aimg3)
 };
-// The int8x3 coefficient images of a 1D synthesis straight from the reflected amplitudes, for
-// the three Bessel orders at once (no FP64 coefficient columns in memory): order o has N[o]
-// real columns (10 nz, 8 nz, 8 nz), its per-(slice, column) maxima colmax[o] ([nchunk][N[o]],
-// IEEE bits of |C|, zeroed before the first pass) and its digit image Bimg[o] in
-// k_gemm_i8_img's layout ([ntile_n][nchunk][kchunk/64][3][Np x 64 B]). One node slicing
-// (kchunk, nchunk) for the three orders.
-struct CoefImg {
-  uint8_t* Bimg[3];
-  unsigned long long* colmax[3];
-  int N[3], ctile[3], Np[3];
-  long kchunk;
-  int nchunk;
-};
-// pass 1: the column maxima (warp max, one atomicMax per warp and column); pass 2: the digits
-cudaError_t launch_coef_colmax(const SynthParams& p, const double2* amp, const CoefImg& ci, cudaStream_t s);
-cudaError_t launch_coef_bimg(const SynthParams& p, const double2* amp, const CoefImg& ci, cudaStream_t s);
-// k_reflect2d alone: the 12 reflected amplitudes of every node into amp ([12][n])
-cudaError_t launch_reflect_amp(const SynthParams& p, double2* amp, cudaStream_t s);
-
 // the J_0, J_1, J_2 digit images of all three orders in one pass (one Bessel evaluation per
 // (ρ, k)); p gives the shared layout (M, K, ntile_m, kchunk, nchunk, kr, rho)
 cudaError_t launch_bessel_i8_aimg3(const BesselI8& p, uint8_t* A0, uint8_t* A1, uint8_t* A2, cudaStream_t s);
@@ -272,9 +255,6 @@ size_t bessel_i8_stage_bytes_a();
 size_t bessel_i8_stage_bytes_b(int Np);
 size_t bessel_i8_smem(int Np);
 int bessel_i8_ctile(int N);
-// the contraction of one order from prebuilt digit images (launch_bessel_i8_aimg3 for A,
-// launch_coef_colmax + launch_coef_bimg for B and colmax): k_gemm_i8_img over the node slices,
-// then the transposing sum of the slices into P ([N][M])
 cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s);
 
 // Gauss-Legendre panels -> nodes/weights, bit-exact with the CPU restatement

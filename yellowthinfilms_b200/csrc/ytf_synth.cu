@@ -17,8 +17,6 @@
 #include "ytf_complex.cuh"
 #include "ytf_kernels.h"
 #include "ytf_bessel.cuh"
-#include "ytf_digits.cuh"
-#include "ytf_tcgen05.cuh"
 
 #include <algorithm>
 
@@ -614,127 +612,6 @@ cudaError_t launch_coef1d_amp(const SynthParams& p, double2* amp, double* C0, do
   k_reflect2d<<<(unsigned)((p.c.n + 127) / 128), 128, 0, s>>>(p, amp);
   k_coef1d_amp<<<dim3((unsigned)((p.c.n + 127) / 128), (unsigned)((p.nz + COEF1D_ZB - 1) / COEF1D_ZB)), 128, 0, s>>>(
       p, amp, C0, C1, C2);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_reflect_amp(const SynthParams& p, double2* amp, cudaStream_t s) {
-  if (p.c.n <= 0) return cudaSuccess;
-  k_reflect2d<<<(unsigned)((p.c.n + 127) / 128), 128, 0, s>>>(p, amp);
-  return cudaGetLastError();
-}
-
-// ------------------------------------------------------------------------------------
-// int8x3 coefficient images straight from the reflected amplitudes (see CoefImg): the 13
-// complex coefficient columns of a (node, z row) are formed by coef1d_row, as k_coef1d_amp
-// does, and never stored in FP64. One thread per (node, z row); the real column of order o
-// for coefficient i, part re/im is 2 (zi n_o + i) + part with n_o = 5, 4, 4.
-// ------------------------------------------------------------------------------------
-__device__ __forceinline__ void coef_of_node(const SynthParams& p, const double2* __restrict__ amp, long k, int zi,
-                                             cd c0[5], cd c1[4], cd c2[4]) {
-  const long n = p.c.n;
-  cd Af[2][3], Ab[2][3];
-#pragma unroll
-  for (int m = 0; m < 2; ++m)
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      Af[m][q] = ldc(amp, 3 * m + q, n, k);
-      Ab[m][q] = ldc(amp, 6 + 3 * m + q, n, k);
-    }
-  coef1d_row(p, k, p.zo[zi], Af, Ab, c0, c1, c2);
-}
-
-__device__ __forceinline__ unsigned long long abs_bits(double v) {
-  return isfinite(v) ? (unsigned long long)__double_as_longlong(fabs(v)) : 0x7ff0000000000000ULL;
-}
-
-// pass 1: per (slice, column) max |C|; a warp's 32 nodes lie in one slice (kchunk % 64 == 0)
-__global__ void __launch_bounds__(128) k_coef_colmax(SynthParams p, const double2* __restrict__ amp, CoefImg ci) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int zi = blockIdx.y;
-  const bool kv = k < p.c.n;
-  cd c[13] = {};
-  if (kv) coef_of_node(p, amp, k, zi, c, c + 5, c + 9);
-  const long slice = (kv ? k : p.c.n - 1) / ci.kchunk;
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int e = 0; e < 26; ++e) {
-    const int i = e >> 1;
-    const cd v = c[i];
-    unsigned long long b = kv ? abs_bits((e & 1) ? v.y : v.x) : 0ULL;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const unsigned long long o = __shfl_xor_sync(0xffffffffu, b, off);
-      b = o > b ? o : b;
-    }
-    if (lane == 0 && b > 0) {
-      const int o = i < 5 ? 0 : (i < 9 ? 1 : 2);
-      const int ii = i < 5 ? i : (i < 9 ? i - 5 : i - 9);
-      const int col = 2 * (zi * (o == 0 ? 5 : 4) + ii) + (e & 1);
-      atomicMax(ci.colmax[o] + slice * ci.N[o] + col, b);
-    }
-  }
-}
-
-// pass 2: the digits; the four lanes of a quad hold four consecutive nodes, and the quad's
-// first lane writes their bytes as one 32-bit word per digit plane (k_bimg_real's layout)
-__global__ void __launch_bounds__(128) k_coef_bimg(SynthParams p, const double2* __restrict__ amp, CoefImg ci) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int zi = blockIdx.y;
-  const long n = p.c.n;
-  const bool kv = k < n;
-  cd c[13] = {};
-  if (kv) coef_of_node(p, amp, k, zi, c, c + 5, c + 9);
-  const int lane = threadIdx.x & 31;
-  const long kq = k & ~3L;  // the quad's first node
-  const long slice = kq / ci.kchunk;
-  const long local = kq - slice * ci.kchunk;
-  const long g = local / 16;
-  const int q = (int)((local % 16) / 4);
-  const long nstage = ci.kchunk / BI_NODES;
-  const int st = (int)(g / 4), kb = (int)(g % 4) * 16;
-  const bool leader = (lane & 3) == 0 && kq < n;
-#pragma unroll
-  for (int e = 0; e < 26; ++e) {
-    const int i = e >> 1;
-    const int o = i < 5 ? 0 : (i < 9 ? 1 : 2);
-    const int ii = i < 5 ? i : (i < 9 ? i - 5 : i - 9);
-    const int col = 2 * (zi * (o == 0 ? 5 : 4) + ii) + (e & 1);
-    const long cm = kq < n ? slice * ci.N[o] + col : 0;
-    const double sB = col_scale(ci.colmax[o][cm]);
-    const double v = kv ? ((e & 1) ? c[i].y : c[i].x) : 0.0;
-    uint32_t d0, d1, d2;
-    digits3b(__double2int_rn(v * sB), d0, d1, d2);
-    const uint32_t mine = d0 | (d1 << 8) | (d2 << 16);
-    const uint32_t w1 = __shfl_down_sync(0xffffffffu, mine, 1);
-    const uint32_t w2 = __shfl_down_sync(0xffffffffu, mine, 2);
-    const uint32_t w3 = __shfl_down_sync(0xffffffffu, mine, 3);
-    if (leader) {
-      const int ct = col / ci.ctile[o], slot = col % ci.ctile[o];
-      const size_t sbytes = 3ul * (size_t)ci.Np[o] * 64;
-      uint8_t* blk = ci.Bimg[o] + (((size_t)ct * ci.nchunk + slice) * nstage + st) * sbytes;
-      const uint32_t base = plane_off(slot, kb) + 4 * q;
-#pragma unroll
-      for (int pl = 0; pl < 3; ++pl) {
-        const int sh = 8 * pl;
-        const uint32_t word = ((mine >> sh) & 255u) | (((w1 >> sh) & 255u) << 8) | (((w2 >> sh) & 255u) << 16) |
-                              (((w3 >> sh) & 255u) << 24);
-        *reinterpret_cast<uint32_t*>(blk + (size_t)pl * ci.Np[o] * 64 + base) = word;
-      }
-    }
-  }
-}
-
-cudaError_t launch_coef_colmax(const SynthParams& p, const double2* amp, const CoefImg& ci, cudaStream_t s) {
-  if (p.c.n <= 0 || p.nz <= 0) return cudaSuccess;
-  if (ci.kchunk % BI_NODES != 0) return cudaErrorInvalidValue;
-  k_coef_colmax<<<dim3((unsigned)((p.c.n + 127) / 128), (unsigned)p.nz), 128, 0, s>>>(p, amp, ci);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_coef_bimg(const SynthParams& p, const double2* amp, const CoefImg& ci, cudaStream_t s) {
-  if (p.c.n <= 0 || p.nz <= 0) return cudaSuccess;
-  if (ci.kchunk % BI_NODES != 0) return cudaErrorInvalidValue;
-  k_coef_bimg<<<dim3((unsigned)((p.c.n + 127) / 128), (unsigned)p.nz), 128, 0, s>>>(p, amp, ci);
   return cudaGetLastError();
 }
 
