@@ -190,6 +190,17 @@ int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* stack, double omega, int
                          const ytf_grid_params* params, int npoles, const double* q, const double* G, long cap,
                          double* k, double* w, long* n, ytf_grid_info* info);
 
+/* The peak rule of real_axis_poles (mod_KSpaceFeatures.jl:151-204) on sampled responses,
+ * without its refinement rounds: for each of nwin log-uniform grids of npts points (ks,
+ * logR: nwin x npts, row-major) the local maxima at or above max + log(floor_rel) that stand
+ * `prominence` (log) above the higher valley within a factor 4 in k, positioned by a
+ * parabola in log k, with Γ from the nearer half-power crossing. counts[w] peaks per window;
+ * their (q, Γ) concatenated into q, G (capacity cap; q = G = NULL: counting only), *total
+ * peaks in all. Host arithmetic; needs no context. The learned node placement reads the
+ * exact windows it samples around the network's candidates through it. */
+int ytf_peaks_batch(int nwin, int npts, const double* ks, const double* logR, double prominence, double floor_rel,
+                    long cap, int* counts, double* q, double* G, long* total);
+
 /* adaptive_seeds(kspace_features(...; dims=1); rtol) (mod_KSpaceFeatures.jl:421-445): the
  * starting breakpoints of the reference's adaptive engine for a point rule -- light lines,
  * geometric grading L (1 ± 2^-j), j = 1..min(50, ceil(2 log2(10/rtol))), onto the half-space

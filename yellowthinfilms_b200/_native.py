@@ -94,6 +94,8 @@ SIGNATURES = {
                                          ctypes.c_int]),
     "ytf_mlp_train": (ctypes.c_int, [_vp, ctypes.c_long, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                      ctypes.c_ulonglong, _vp]),
+    "ytf_peaks_batch": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _d, _d, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_long, _i, _d, _d, ctypes.POINTER(ctypes.c_long)]),
     "ytf_adaptive_seeds": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams),
                                           ctypes.c_long, _d, ctypes.POINTER(ctypes.c_long)]),
     "ytf_nodes_2d": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams), ctypes.c_int,

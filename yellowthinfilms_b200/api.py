@@ -409,6 +409,53 @@ def point_krho_grid_2d(stack, omega, source_layer, h_min, rho_max, target_decay=
     return k, w, phi, wphi, meta
 
 
+def peaks_batch(ks, logR, prominence=np.log(1.05), floor_rel=1e-6):
+    """Peaks (q, Γ) of many sampled log-responses at once (ytf_peaks_batch): ks and logR are
+    [windows, points] arrays on log-uniform grids; returns one list of (q, Γ) per window."""
+    K = np.ascontiguousarray(np.asarray(ks, np.float64))
+    Y = np.ascontiguousarray(np.asarray(logR, np.float64))
+    nw, npts = K.shape
+    counts = np.zeros(max(nw, 1), np.int32)
+    cap = nw * max(1, npts // 2)
+    q, G = np.zeros(max(cap, 1)), np.zeros(max(cap, 1))
+    tot = ctypes.c_long(0)
+    rc = lib().ytf_peaks_batch(nw, npts, ptr(K), ptr(Y), float(prominence), float(floor_rel), cap, ptr(counts, _i),
+                               ptr(q), ptr(G), ctypes.byref(tot))
+    if rc != 0:
+        raise YTFError("peaks_batch: bad arguments")
+    cuts = np.cumsum(counts[:nw])[:-1]
+    return [list(zip(a.tolist(), b.tolist())) for a, b in zip(np.split(q[:tot.value], cuts), np.split(G[:tot.value], cuts))]
+
+
+def rule_panels(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=25.0, kr_cap=0.0, scan=False, order=8,
+                rtol=1e-6, poles=None, ctx: Optional[Context] = None):
+    """The panels (an [n, 2] array) of point_kx_grid's rule (``poles`` given: of
+    grid_from_poles's), host work only: the nodes of many rules then come from one
+    gl_rule_batch call over (panels, singular) with the half-space light lines as singular
+    points, bit for bit the nodes point_kx_grid / grid_from_poles return."""
+    from ._native import GridInfo, GridParams
+    st = _as_stack(stack, ctx)
+    prm = GridParams(float(h_min), float(rho_max), float(target_decay), float(kr_cap), int(bool(scan)), int(order),
+                     float(rtol))
+    info = GridInfo()
+    n = ctypes.c_long(0)
+    if poles is None:
+        call = lambda: lib().ytf_nodes_1d(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm), 0, None,
+                                          None, ctypes.byref(n), ctypes.byref(info))
+    else:
+        pq = _f64([p[0] for p in poles]) if len(poles) else np.zeros(1)
+        pg = _f64([p[1] for p in poles]) if len(poles) else np.zeros(1)
+        call = lambda: lib().ytf_nodes_from_poles(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm),
+                                                  len(poles), ptr(pq), ptr(pg), 0, None, None, ctypes.byref(n),
+                                                  ctypes.byref(info))
+    st.ctx.check(call())
+    pan = np.zeros(2 * max(1, info.n_panels))
+    info.panels = ptr(pan)
+    info.panels_cap = info.n_panels
+    st.ctx.check(call())
+    return pan[:2 * info.n_panels].reshape(-1, 2).copy()
+
+
 class MLP:
     """The node-placement MLP on the device (ytf_mlp_*): widths sizes[0] -> ... -> 2, GELU
     between layers, BF16 weights with FP32 accumulation, trained by libytf's own forward,

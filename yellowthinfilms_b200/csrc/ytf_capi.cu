@@ -951,6 +951,24 @@ int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* st, double omega, int so
   return nodes_1d_impl(ctx, st, omega, source_layer, prm, npoles, q, G, cap, k, w, n, info);
 }
 
+int ytf_peaks_batch(int nwin, int npts, const double* ks, const double* logR, double prominence, double floor_rel,
+                    long cap, int* counts, double* q, double* G, long* total) {
+  if (nwin < 0 || npts < 0 || (nwin > 0 && npts > 0 && (!ks || !logR)) || !counts || !total) return YTF_ERR_ARG;
+  long t = 0;
+  std::vector<std::pair<double, double>> pk;
+  for (int w = 0; w < nwin; ++w) {
+    pk.clear();
+    grid::sampled_peaks(ks + (size_t)w * npts, logR + (size_t)w * npts, npts, prominence, floor_rel, pk);
+    counts[w] = (int)pk.size();
+    for (auto& e : pk) {
+      if (q && G && t < cap) { q[t] = e.first; G[t] = e.second; }
+      ++t;
+    }
+  }
+  *total = t;
+  return (q && G && t > cap) ? YTF_ERR_ARG : YTF_OK;
+}
+
 int ytf_adaptive_seeds(ytf_ctx* ctx, const ytf_stack* st, double omega, int source_layer, const ytf_grid_params* prm,
                        long cap, double* seeds, long* n) {
   if (!ctx || !prm || !n) return YTF_ERR_ARG;

@@ -371,6 +371,50 @@ int features_2d(const std::vector<const double*>& eps, const std::vector<const d
   return 0;
 }
 
+void sampled_peaks(const double* ks, const double* y, int n, double prominence, double floor_rel,
+                   std::vector<std::pair<double, double>>& out) {
+  if (n < 3) return;
+  double ymax = -INFINITY;
+  for (int i = 0; i < n; ++i) ymax = std::max(ymax, y[i]);
+  const double ymin = std::max(ymax + std::log(floor_rel), std::log(1e-10));
+  const double l0 = std::log(ks[0]), step = std::log(ks[1]) - l0;
+  const int W = (int)std::ceil(std::log(4.0) / step);
+  for (int i = 1; i < n - 1; ++i) {
+    if (!(y[i] > y[i - 1] && y[i] >= y[i + 1] && y[i] >= ymin)) continue;
+    const int lo = std::max(0, i - W), hi = std::min(n - 1, i + W);
+    int jl = lo, jr = hi;
+    for (int j = i - 1; j >= lo; --j)
+      if (y[j] > y[i]) { jl = j + 1; break; }
+    for (int j = i + 1; j <= hi; ++j)
+      if (y[j] > y[i]) { jr = j - 1; break; }
+    double lmin = y[i], rmin = y[i];
+    for (int j = jl; j <= i; ++j) lmin = std::min(lmin, y[j]);
+    for (int j = i; j <= jr; ++j) rmin = std::min(rmin, y[j]);
+    const double base = std::max(lmin, rmin);
+    if (y[i] - base < prominence) continue;
+    const double den = y[i - 1] - 2 * y[i] + y[i + 1];
+    const double off = den < 0 ? 0.5 * (y[i - 1] - y[i + 1]) / den : 0.0;
+    const double lki = std::log(ks[i]);
+    const double q = std::exp(lki + std::min(0.5, std::max(-0.5, off)) * step);
+    const double P = std::exp(y[i]), eb = std::exp(base);
+    const double lvl = std::log(eb + (P - eb) / std::sqrt(2.0));
+    double G = INFINITY;
+    for (int side = 0; side < 2; ++side) {
+      const int dj = side == 0 ? 1 : -1;  // towards the peak
+      for (int j = side == 0 ? i - 1 : i + 1; side == 0 ? j >= jl : j <= jr; j += side == 0 ? -1 : 1) {
+        if (y[j] <= lvl) {
+          const int prev = j + dj;
+          const double t = (y[prev] - lvl) / (y[prev] - y[j]);
+          const double lp = std::log(ks[prev]), lj = std::log(ks[j]);
+          G = std::min(G, std::fabs(std::exp(lp + t * (lj - lp)) - q));
+          break;
+        }
+      }
+    }
+    if (std::isfinite(G) && G > 0) out.push_back({q, G});
+  }
+}
+
 std::vector<double> adaptive_seeds(const Features& F, double rtol, double n_gamma, int grade) {
   if (grade <= 0) grade = std::min(50, (int)std::ceil(2 * std::log2(10 / rtol)));
   std::vector<double> s(F.light_lines);

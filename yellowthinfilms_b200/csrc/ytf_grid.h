@@ -71,6 +71,15 @@ int features_2d(const std::vector<const double*>& eps, const std::vector<const d
                 bool scan, double scan_step, double prominence, int n_phi_scan, double c_phi, int n_phi_min,
                 double rtol, double c_eta, const EvalAt& f, Features& F);
 
+// peaks of a sampled log-response on a log-uniform k grid (the scan's peak rule of
+// real_axis_poles applied to samples, mod_KSpaceFeatures.jl:151-204, without the refinement
+// rounds): local maxima at or above max(y) + log(floor_rel) (and log 1e-10) that stand at
+// least `prominence` (log) above the higher of their two valleys (searched over a factor 4 in
+// k), position by a parabola through the three samples in log k (offset clipped to half a
+// step), Γ from the nearer crossing of the half-power level, linear in log k. Appends (q, Γ).
+void sampled_peaks(const double* ks, const double* y, int n, double prominence, double floor_rel,
+                   std::vector<std::pair<double, double>>& out);
+
 // adaptive_seeds (mod_KSpaceFeatures.jl:421-445): starting breakpoints of the adaptive engine
 // -- the light lines, L (1 ± 2^-j), j = 1..grade, at every singular line, each cluster's
 // [a - nΓ Γ, a, b, b + nΓ Γ], and 2 kmax, 4 kmax, ... below Kcut; those in (0, Kcut), sorted,

@@ -197,7 +197,7 @@ def propose_poles(net, stack, k0, n_k=2048):
     maxima of its pole score (> 0.3) on a fine log grid."""
     ks = scan_grid(k0, n_k)
     out = net.forward(features(stack, k0, ks)).astype(np.float64)
-    cand = peaks(ks, out[:, 0] * LOG_SCALE)
+    cand = api.peaks_batch(ks[None, :], out[None, :, 0] * LOG_SCALE, prominence=np.log(1.01))[0]
     return sorted(_score_candidates(ks, out[:, 1], cand))
 
 
@@ -236,11 +236,13 @@ def refine_poles_batch(items, n_local=129, ctx=None):
 
 
 def _poles_from_windows(wins, R, n_local):
-    """Every peak of the sampled response in each window, merged across windows."""
-    out = []
-    for i, ks in enumerate(wins):
-        y = np.log(np.maximum(R[i * n_local:(i + 1) * n_local], 1e-12))
-        out += peaks(ks, y)
+    """Every peak of the sampled response in each window (the peak rule of peaks(), run for
+    all windows in one host call, api.peaks_batch), merged across windows."""
+    if not wins:
+        return []
+    K = np.stack(wins)
+    Y = np.log(np.maximum(np.asarray(R, np.float64)[:len(wins) * n_local].reshape(len(wins), n_local), 1e-12))
+    out = [p for pk in api.peaks_batch(K, Y) for p in pk]
     out.sort()
     merged = []
     for q, G in out:  # windows of neighbouring candidates may find the same pole
@@ -403,12 +405,9 @@ def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, de
     problem, halved until two levels agree. Returns [(G, k, w, halvings, converged)]; with
     ``device`` every G (and the acceptance check) stays in device memory; ``solved`` as
     _refine_levels."""
-    rules, panels = [], []
-    for P in problems:
-        k, w, info = api.point_kx_grid(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
-                                       rho_max=P["rho_max"], scan=False, order=order, ctx=ctx)
-        rules.append((k, w))
-        panels.append(info["panels"])
+    panels = [api.rule_panels(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"], rho_max=P["rho_max"],
+                              scan=False, order=order, ctx=ctx) for P in problems]
+    rules = api.gl_rule_batch([(p, _sing(P)) for p, P in zip(panels, problems)], order, ctx=ctx)
     out = [None] * len(problems)
     _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device,
                    solved)
@@ -427,19 +426,14 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     evaluated on per problem. ``solved`` as _refine_levels."""
     n_k = n_scan
     pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
-    cands = []
-    for j, P in enumerate(problems):
-        ks = scan_grid(P["k0"], n_k)
-        o = pred[j * n_k:(j + 1) * n_k]
-        cands.append(sorted(_score_candidates(ks, o[:, 1], peaks(ks, o[:, 0] * LOG_SCALE, prominence=np.log(1.01)))))
+    KS = np.stack([scan_grid(P["k0"], n_k) for P in problems])
+    pk = api.peaks_batch(KS, pred[:, 0].reshape(len(problems), n_k) * LOG_SCALE, prominence=np.log(1.01))
+    cands = [sorted(_score_candidates(KS[j], pred[j * n_k:(j + 1) * n_k, 1], pk[j])) for j in range(len(problems))]
     polesets = refine_poles_batch([(P["stack"], P["k0"], P["source_layer"], c) for P, c in zip(problems, cands)], ctx=ctx)
-    rules, panels = [], []
-    for P, poles in zip(problems, polesets):
-        k, w, info = api.grid_from_poles(P["stack"], P["k0"], P["source_layer"], poles, h_min=P["h_min"],
-                                         rho_max=P["rho_max"], order=order,
-                                         rtol=rtol if build_rtol is None else build_rtol, ctx=ctx)
-        rules.append((k, w))
-        panels.append(info["panels"])
+    panels = [api.rule_panels(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"], rho_max=P["rho_max"],
+                              order=order, rtol=rtol if build_rtol is None else build_rtol, poles=poles, ctx=ctx)
+              for P, poles in zip(problems, polesets)]
+    rules = api.gl_rule_batch([(p, _sing(P)) for p, P in zip(panels, problems)], order, ctx=ctx)
     out = [None] * len(problems)
     # the proposals' own check (one level); a rejected proposal missed a pole: its rule comes
     # from one exact log scan of the response instead (batched over the rejected problems),
@@ -450,9 +444,10 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
         scanned = exact_scan_poles_batch([problems[i] for i in rej], ctx=ctx)
         for i, poles in zip(rej, scanned):
             P = problems[i]
-            k, w, info = api.grid_from_poles(P["stack"], P["k0"], P["source_layer"], poles, h_min=P["h_min"],
-                                             rho_max=P["rho_max"], order=order, rtol=rtol, ctx=ctx)
-            rules[i], panels[i] = (k, w), info["panels"]
+            panels[i] = api.rule_panels(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
+                                        rho_max=P["rho_max"], order=order, rtol=rtol, poles=poles, ctx=ctx)
+        for i, r in zip(rej, api.gl_rule_batch([(panels[i], _sing(problems[i])) for i in rej], order, ctx=ctx)):
+            rules[i] = r
         sub = [None] * len(problems)
         _refine_levels(problems, rej, rules, panels, None, rtol, max_halvings, order, ctx, sub, device, solved)
         for i in rej:
@@ -496,7 +491,7 @@ def exact_scan_poles_batch(problems, step=1e-3, n_local=129, ctx=None):
     Rs = api.cavity_response_batch(items, ctx=ctx)
     cands = []
     for (ks, ll), R in zip(grids, Rs):
-        pk = peaks(ks, np.log(np.maximum(R, 1e-300)))
+        pk = api.peaks_batch(ks[None, :], np.log(np.maximum(R, 1e-300))[None, :])[0]
         cands.append([(q, G) for q, G in pk if all(abs(q - L) > 1e-6 * q for L in ll)])
     return refine_poles_batch([(P["stack"], P["k0"], P["source_layer"], c) for P, c in zip(problems, cands)],
                               n_local=n_local, ctx=ctx)
