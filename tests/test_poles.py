@@ -63,7 +63,7 @@ def test_extracting_a_sharp_guided_mode_needs_fewer_nodes(oracle):
     st = _stack(-3.0 + 0.01j)
     Go = _real_axis_oracle(oracle, st)
     sto, bps, poles = _setup(st)
-    assert any(abs(kp / K0 - 2.408) < 0.01 and 0 < kp.imag / K0 < 0.03 for kp, _ in poles), poles
+    assert any(abs(kp.real / K0 - 2.408) < 0.01 and 0 < kp.imag / K0 < 0.03 for kp, _ in poles), poles
     G128, n128 = _contour_G(sto, bps, 128, ())
     G64p, n64 = _contour_G(sto, bps, 64, poles)
     assert relerr(G128, Go) > 1e-6

@@ -789,28 +789,15 @@ int ytf_cavity_response_batch(ytf_ctx* ctx, int nitems, const ytf_stack* const* 
   int rc;
   if ((rc = upload(ctx, dk, kr, 8 * (size_t)total))) return rc;
   if ((rc = upload(ctx, dphi, &phi, 8))) return rc;
-  // each item is its own (kρ, φ) grid of counts[i] x 1 nodes; the items run round-robin on
-  // the context's side streams (each with its own node scratch: an item is a chain of a few
-  // small dependent launches), forked from and joined to its stream; one download and one
-  // synchronisation for all
-  constexpr int kSlots = 4;
-  const int nslot = nitems >= 2 ? std::min(kSlots, nitems) : 0;
-  if (nslot) {
-    while ((int)ctx->slot_streams.size() < kSlots) {
-      cudaStream_t s;
-      cudaEvent_t e;
-      CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      ctx->slot_streams.push_back(s);
-      ctx->slot_events.push_back(e);
-    }
-    CK(cudaEventRecord(ctx->slot_events[0], ctx->stream));
-    for (int s = 0; s < nslot; ++s) CK(cudaStreamWaitEvent(ctx->slot_streams[s], ctx->slot_events[0], 0));
-  }
-  cudaStream_t main = ctx->stream;
+  // each item is its own (kρ, φ) grid of counts[i] x 1 nodes, solved by the forward-only
+  // chain in response mode; all items of a pass share the same five batched launches (the
+  // batched kernels map a flat index to (item, node) and run the single-item per-node code),
+  // passes bounded by the 6 GiB scratch budget
+  const size_t budget = (size_t)6 << 30;
+  std::vector<TransferParams> ps;
+  std::vector<size_t> scr;
   long off = 0;
-  rc = YTF_OK;
-  for (int i = 0; i < nitems && !rc; ++i) {
+  for (int i = 0; i < nitems; ++i) {
     const long n = counts[i];
     if (n == 0) continue;
     TransferParams p;
@@ -826,25 +813,66 @@ int ytf_cavity_response_batch(ytf_ctx* ctx, int nitems, const ytf_stack* const* 
     p.Np = 1;
     p.kr = dk + off;
     p.phi = dphi;
+    p.n = n;
+    p.off = 0;
     p.nout = n;
     p.status = dstat + off;
     p.resp = dresp + off;
-    if (nslot) {
-      ctx->stream = ctx->slot_streams[i % nslot];
-      ctx->ws_slot = 1 + i % nslot;
-    }
-    rc = run_transfer(ctx, p, n);
+    ps.push_back(p);
+    scr.push_back(scratch_per_node(p.nL, 0, 0) * (size_t)n + 4 * 256);
     off += n;
   }
-  ctx->stream = main;
-  ctx->ws_slot = 0;
-  for (int s = 0; s < nslot; ++s) {
-    cudaEventRecord(ctx->slot_events[s], ctx->slot_streams[s]);
-    cudaStreamWaitEvent(main, ctx->slot_events[s], 0);
-  }
-  if (rc) {
-    cudaStreamSynchronize(main);
-    return rc;
+  size_t first = 0;
+  while (first < ps.size()) {
+    size_t last = first, used = 0;
+    while (last < ps.size() && (last == first || used + scr[last] <= budget)) used += scr[last++];
+    const int m = (int)(last - first);
+    if (used > budget) {  // one item larger than a pass: its own chunked solve
+      if ((rc = run_transfer(ctx, ps[first], ps[first].n))) return rc;
+      first = last;
+      continue;
+    }
+    WS(arena, char, "crb_scratch", used);
+    size_t o = 0;
+    auto carve = [&](size_t bytes) {
+      char* q = arena + o;
+      o += (bytes + 255) & ~size_t(255);
+      return q;
+    };
+    std::vector<long> offm(m + 1, 0), offs(m + 1, 0), offi(m + 1, 0);
+    std::vector<TransferParams> part(ps.begin() + first, ps.begin() + last);
+    for (int j = 0; j < m; ++j) {
+      TransferParams& q = part[j];
+      const int N = q.nL;
+      const long n = q.n;
+      q.modes = (double2*)carve((size_t)N * 20 * 16 * n);
+      q.lstat = (uint8_t*)carve((size_t)N * n);
+      q.sint = (double2*)carve((size_t)std::max(N - 1, 1) * 16 * 16 * n);
+      q.dec = (uint8_t*)carve((size_t)std::max(N - 1, 1) * n);
+      offm[j + 1] = offm[j] + (long)N * n;
+      offs[j + 1] = offs[j] + n;
+      offi[j + 1] = offi[j] + (long)(N - 1) * n;
+    }
+    const size_t pbytes = sizeof(TransferParams) * m, lbytes = sizeof(long) * (m + 1);
+    WS(dpar, char, "crb_params", pbytes + 3 * lbytes);
+    std::vector<char> hbuf(pbytes + 3 * lbytes);
+    std::memcpy(hbuf.data(), part.data(), pbytes);
+    std::memcpy(hbuf.data() + pbytes, offm.data(), lbytes);
+    std::memcpy(hbuf.data() + pbytes + lbytes, offs.data(), lbytes);
+    std::memcpy(hbuf.data() + pbytes + 2 * lbytes, offi.data(), lbytes);
+    CK(cudaMemcpyAsync(dpar, hbuf.data(), hbuf.size(), cudaMemcpyHostToDevice, ctx->stream));
+    const TransferParams* dp = (const TransferParams*)dpar;
+    const long* doffm = (const long*)(dpar + pbytes);
+    const long* doffs = doffm + (m + 1);
+    const long* doffi = doffs + (m + 1);
+    CK(LAUNCH("k_layer_modes", launch_transfer_batch(0, dp, doffm, m, offm[m], ctx->stream)));
+    CK(LAUNCH("k_layer_modes_qr", launch_transfer_batch(1, dp, doffm, m, offm[m], ctx->stream)));
+    if (offi[m]) CK(LAUNCH("k_iface", launch_transfer_batch(6, dp, doffi, m, offi[m], ctx->stream)));
+    CK(LAUNCH("k_seeds", launch_transfer_batch(5, dp, doffs, m, offs[m], ctx->stream)));
+    CK(LAUNCH("k_scan", launch_transfer_batch(7, dp, doffs, m, offs[m], ctx->stream)));
+    // the host block is read by the copy above before the next pass reuses it
+    CK(cudaStreamSynchronize(ctx->stream));
+    first = last;
   }
   CK(cudaMemcpyAsync(out, dresp, 8 * (size_t)total, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));

@@ -59,20 +59,25 @@ __device__ __forceinline__ void split_bf(float v, __nv_bfloat16& hi, __nv_bfloat
   lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
 
+// tn: the tile width (128 or 256). With ksl > 0 the K range is split: CTA (x, y, z) sums
+// K in [z ksl, (z + 1) ksl) and writes its raw sums to part[z][M][N] (k_splitk_finish adds
+// the slices, the bias, the accumulation and GELU); otherwise it finishes the tile itself.
 template <class TA, class TB>
 __global__ void __launch_bounds__(128, 1) k_gemm_tc(int M, int N, int K, const TA* __restrict__ A, long sam, long sak,
                                                      const TB* __restrict__ B, long sbk, long sbn,
                                                      float* __restrict__ C, long ldc, const float* __restrict__ bias,
-                                                     float* __restrict__ H, int act, int accumulate,
-                                                     unsigned* __restrict__ err) {
+                                                     float* __restrict__ H, int act, int accumulate, int tn, int ksl,
+                                                     float* __restrict__ part, unsigned* __restrict__ err) {
   constexpr bool SA = std::is_same<TA, float>::value;  // split A into two terms
   constexpr bool SB = std::is_same<TB, float>::value;
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t done;
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int m0 = blockIdx.y * GM, n0 = blockIdx.x * GNMAX;
-  const int nt = min(GNMAX, N - n0);
+  const int m0 = blockIdx.y * GM, n0 = blockIdx.x * tn;
+  const int nt = min(tn, N - n0);
+  const int kbeg = ksl > 0 ? (int)blockIdx.z * ksl : 0;
+  const int kend = ksl > 0 ? min(K, kbeg + ksl) : K;
   const int Np = ((nt + 15) / 16) * 16;
   const uint32_t planeA = GM * 64u, planeB = (uint32_t)Np * 64u;
   constexpr int NPL = GKB / 32;
@@ -98,7 +103,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(int M, int N, int K, const T
   const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(Np >> 3) << 17) | ((uint32_t)(GM >> 4) << 24);
   bool ok = true;
   int round = 0;
-  for (int k0 = 0; k0 < K; k0 += GKB, ++round) {
+  for (int k0 = kbeg; k0 < kend; k0 += GKB, ++round) {
     if (round > 0) {
       // the previous block's MMAs have read the buffers before they are overwritten
       bool got = false;
@@ -109,7 +114,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(int M, int N, int K, const T
       int r, k;
       if (sak == 1) { r = e / GKB; k = e % GKB; } else { k = e / GM; r = e % GM; }
       const int m = m0 + r, kk = k0 + k;
-      const float v = (m < M && kk < K) ? (float)A[(long)m * sam + (long)kk * sak] : 0.f;
+      const float v = (m < M && kk < kend) ? (float)A[(long)m * sam + (long)kk * sak] : 0.f;
       __nv_bfloat16 hi, lo;
       split_bf(v, hi, lo);
       const uint32_t off = (k >> 5) * planeA + plane_bf(r, k & 31);
@@ -120,7 +125,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(int M, int N, int K, const T
       int r, k;
       if (sbk == 1) { r = e / GKB; k = e % GKB; } else { k = e / Np; r = e % Np; }
       const int n = n0 + r, kk = k0 + k;
-      const float v = (r < nt && kk < K) ? (float)B[(long)kk * sbk + (long)n * sbn] : 0.f;
+      const float v = (r < nt && kk < kend) ? (float)B[(long)kk * sbk + (long)n * sbn] : 0.f;
       __nv_bfloat16 hi, lo;
       split_bf(v, hi, lo);
       const uint32_t off = (k >> 5) * planeB + plane_bf(r, k & 31);
@@ -138,7 +143,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(int M, int N, int K, const T
           const uint32_t oa = pl * planeA + t * 256u, ob = pl * planeB + t * 256u;
           // the first MMA of the tile overwrites the accumulator, every other one adds to it
           mma_bf16(tmem, umma_desc(smem_u32(Ahi + oa)), umma_desc(smem_u32(Bhi + ob)), idesc,
-                   (k0 > 0 || pl > 0 || t > 0) ? 1u : 0u);
+                   (k0 > kbeg || pl > 0 || t > 0) ? 1u : 0u);
           if (SB) mma_bf16(tmem, umma_desc(smem_u32(Ahi + oa)), umma_desc(smem_u32(Blo + ob)), idesc, 1u);
           if (SA) mma_bf16(tmem, umma_desc(smem_u32(Alo + oa)), umma_desc(smem_u32(Bhi + ob)), idesc, 1u);
         }
@@ -165,6 +170,10 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(int M, int N, int K, const T
         for (int j = 0; j < 8; ++j) {
           const int n = n0 + c0 + j;
           if (c0 + j >= nt) break;
+          if (part) {
+            part[((long)blockIdx.z * M + m) * N + n] = __uint_as_float(v[j]);
+            continue;
+          }
           float z = __uint_as_float(v[j]) + (bias ? bias[n] : 0.f);
           if (accumulate) z += C[(long)m * ldc + n];
           C[(long)m * ldc + n] = z;
@@ -177,6 +186,20 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(int M, int N, int K, const T
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(GNMAX) : "memory");
+}
+
+// the K slices of a split GEMM summed in slice order, then bias, accumulation and GELU
+__global__ void k_splitk_finish(int M, int N, int S, const float* __restrict__ part, float* __restrict__ C, long ldc,
+                                const float* __restrict__ bias, float* __restrict__ H, int act, int accumulate) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)M * N) return;
+  const int m = (int)(t / N), n = (int)(t % N);
+  float z = 0.f;
+  for (int sl = 0; sl < S; ++sl) z += part[(long)sl * M * N + t];
+  z += bias ? bias[n] : 0.f;
+  if (accumulate) z += C[(long)m * ldc + n];
+  C[(long)m * ldc + n] = z;
+  if (H) H[(long)m * ldc + n] = act ? 0.5f * z * (1.f + erff(z * 0.70710678118654752f)) : z;
 }
 
 template <class TA, class TB>
@@ -270,6 +293,8 @@ struct ytf_mlp {
   std::vector<float*> Z, H, dZ, dH;
   float *T = nullptr, *lb = nullptr, *X = nullptr;
   unsigned* tc_err = nullptr;      // set by a tensor-core GEMM whose commit wait ran out
+  float* part = nullptr;           // K-slice sums of split GEMMs
+  size_t part_cap = 0;
   std::string err;
   ~ytf_mlp() {
     cudaFree(p); cudaFree(g); cudaFree(m); cudaFree(v); cudaFree(wb);
@@ -277,7 +302,7 @@ struct ytf_mlp {
     for (auto* q : H) cudaFree(q);
     for (auto* q : dZ) cudaFree(q);
     for (auto* q : dH) cudaFree(q);
-    cudaFree(T); cudaFree(lb); cudaFree(X); cudaFree(tc_err);
+    cudaFree(T); cudaFree(lb); cudaFree(X); cudaFree(tc_err); cudaFree(part);
   }
 };
 
@@ -297,13 +322,41 @@ template <class TA, class TB>
 cudaError_t gemm(ytf_mlp* net, int M, int N, int K, const TA* A, long sam, long sak, const TB* B, long sbk, long sbn,
                  float* C, long ldc, const float* bias, float* H, int act, int accumulate) {
   if (M <= 0 || N <= 0) return cudaSuccess;
-  const int Np = ((std::min(N, GNMAX) + 15) / 16) * 16;
+  // fill the 148 SMs: 128-wide tiles when 256-wide ones are too few, then K slices
+  const int mt = (M + GM - 1) / GM;
+  const int tn = (long)mt * ((N + GNMAX - 1) / GNMAX) < 148 && N > 128 ? 128 : GNMAX;
+  const int tiles = mt * ((N + tn - 1) / tn);
+  int S = 1, ksl = 0;
+  if (tiles < 74 && K >= 2 * GKB) {
+    S = std::min((148 + tiles - 1) / tiles, (K + GKB - 1) / GKB);
+    ksl = (((K + S - 1) / S + GKB - 1) / GKB) * GKB;
+    S = (K + ksl - 1) / ksl;
+  }
+  float* part = nullptr;
+  if (S > 1) {
+    const size_t need = (size_t)S * M * N;
+    if (need > net->part_cap) {
+      cudaFree(net->part);
+      net->part = nullptr;
+      net->part_cap = 0;
+      cudaError_t e = cudaMalloc(&net->part, sizeof(float) * need);
+      if (e != cudaSuccess) return e;
+      net->part_cap = need;
+    }
+    part = net->part;
+  } else {
+    ksl = 0;
+  }
+  const int Np = ((std::min(N, tn) + 15) / 16) * 16;
   const size_t sm = gemm_tc_smem<TA, TB>(Np);
   cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  dim3 grid((N + GNMAX - 1) / GNMAX, (M + GM - 1) / GM);
+  dim3 grid((N + tn - 1) / tn, mt, S);
   k_gemm_tc<TA, TB><<<grid, 128, sm, net->stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, bias, H, act, accumulate,
-                                                   net->tc_err);
+                                                   tn, ksl, part, net->tc_err);
+  if ((e = cudaGetLastError()) != cudaSuccess || S == 1) return e;
+  k_splitk_finish<<<(unsigned)(((long)M * N + 255) / 256), 256, 0, net->stream>>>(M, N, S, part, C, ldc, bias, H, act,
+                                                                              accumulate);
   return cudaGetLastError();
 }
 
