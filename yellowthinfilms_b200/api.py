@@ -448,11 +448,15 @@ def rule_panels(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=25.
         call = lambda: lib().ytf_nodes_from_poles(st.ctx.h, st.h, float(omega), int(source_layer), ctypes.byref(prm),
                                                   len(poles), ptr(pq), ptr(pg), 0, None, None, ctypes.byref(n),
                                                   ctypes.byref(info))
-    st.ctx.check(call())
-    pan = np.zeros(2 * max(1, info.n_panels))
+    pan = np.zeros(2 * 16384)  # one call when the rule has at most 16384 panels (the panels are host work)
     info.panels = ptr(pan)
-    info.panels_cap = info.n_panels
+    info.panels_cap = 16384
     st.ctx.check(call())
+    if info.n_panels > 16384:
+        pan = np.zeros(2 * info.n_panels)
+        info.panels = ptr(pan)
+        info.panels_cap = info.n_panels
+        st.ctx.check(call())
     return pan[:2 * info.n_panels].reshape(-1, 2).copy()
 
 

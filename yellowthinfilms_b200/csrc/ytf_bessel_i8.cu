@@ -70,7 +70,7 @@ __device__ __forceinline__ double col_scale(unsigned long long bits) {
 __global__ void k_bcolmax(BesselI8 p) {
   const int col = blockIdx.x, z = blockIdx.y;
   const long k0 = (long)z * p.kchunk, k1 = min(p.K, k0 + p.kchunk);
-  const double* c = p.C + (long)col * p.K;
+  const float* c = p.C + (long)col * p.K;
   double m = 0.0;
   for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
     const double v = c[k];
@@ -109,7 +109,7 @@ __global__ void k_bimg_real(BesselI8 p) {
 #pragma unroll
   for (int h = 0; h < 4; ++h) {
     const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
-    const double v = (cv && k < p.K) ? p.C[(long)col * p.K + k] : 0.0;
+    const double v = (cv && k < p.K) ? (double)p.C[(long)col * p.K + k] : 0.0;
     uint32_t d0, d1, d2;
     digits3b(__double2int_rn(v * sB), d0, d1, d2);
     b[0][h] = d0; b[1][h] = d1; b[2][h] = d2;

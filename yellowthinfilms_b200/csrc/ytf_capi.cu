@@ -1406,10 +1406,20 @@ static int synth_setup(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double z
 static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const double* drho, int precision, int nsm,
                      const GreenBatch* gb, double* P0, double* P1, double* P2) {
   const long nk = sp.c.n;
+  WS(amp1, double2, "g_amp", (size_t)12 * nk);
+  const bool i8 = precision == YTF_PREC_INT8X3 && !sp.c.kri;
+  // FP64 coefficient columns for the FP64 contractions, FP32 ones for the int8x3 digits
+  double *C0 = nullptr, *C1 = nullptr, *C2 = nullptr;
+  float *F0 = nullptr, *F1 = nullptr, *F2 = nullptr;
+  if (i8) {
+    WS(Cf, float, "g_Cf", 26 * (size_t)nz * nk);
+    F0 = Cf; F1 = Cf + 10 * (size_t)nz * nk; F2 = Cf + 18 * (size_t)nz * nk;
+    CK(LAUNCH("k_coef1d", launch_coef1d_amp(sp, amp1, F0, F1, F2, ctx->stream)));
+  } else {
     WS(C, double, "g_C", 26 * (size_t)nz * nk);
-    double *C0 = C, *C1 = C + 10 * (size_t)nz * nk, *C2 = C + 18 * (size_t)nz * nk;
-    WS(amp1, double2, "g_amp", (size_t)12 * nk);
+    C0 = C; C1 = C + 10 * (size_t)nz * nk; C2 = C + 18 * (size_t)nz * nk;
     CK(LAUNCH("k_coef1d", launch_coef1d_amp(sp, amp1, C0, C1, C2, ctx->stream)));
+  }
     if (sp.c.kri) {
       // nodes on a deformed contour: complex J_n(kρ ρ) tables, two FP64 GEMMs per order
       // (Re J and Im J against the real/imaginary coefficient columns), then the complex combine
@@ -1435,10 +1445,10 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
       }
       return YTF_OK;
     }
-    if (precision == YTF_PREC_INT8X3) {
+    if (i8) {
       // int8 tensor cores: J_n(kρ) and the coefficient columns as fixed-point digit images,
       // exact INT32 accumulation, FP64 sum of the node slices into P_n
-      const double* Cn8[3] = {C0, C1, C2};
+      const float* Cn8[3] = {F0, F1, F2};
       double* Pn8[3] = {P0, P1, P2};
       const int Nn8[3] = {10 * nz, 8 * nz, 8 * nz};
       unsigned* err = gb ? gb->err : nullptr;

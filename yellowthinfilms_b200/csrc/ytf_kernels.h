@@ -126,6 +126,8 @@ struct SynthParams {
 cudaError_t launch_coef1d(const SynthParams& p, double* C0, double* C1, double* C2, cudaStream_t s);
 // the same through per-node reflected amplitudes in amp ([12][n] complex scratch)
 cudaError_t launch_coef1d_amp(const SynthParams& p, double2* amp, double* C0, double* C1, double* C2, cudaStream_t s);
+// the same columns rounded to FP32 (the int8x3 contraction's input)
+cudaError_t launch_coef1d_amp(const SynthParams& p, double2* amp, float* C0, float* C1, float* C2, cudaStream_t s);
 cudaError_t launch_bessel_c(const double* kr, const double* kri, long nk, const double* rho, int nr, double* J,
                             cudaStream_t s);
 cudaError_t launch_combine_complex(long M, int N2, const double* A, const double* B, double* P, cudaStream_t s);
@@ -239,7 +241,7 @@ struct BesselI8 {
   int nchunk;
   const double* kr;  // [K]
   const double* rho; // [M]
-  const double* C;   // [N][K]
+  const float* C;    // [N][K] coefficient columns (FP32)
   uint8_t* Aimg;     // [ntile_m][nchunk][kchunk/64][3][128 x 64 B]
   uint8_t* Bimg;     // [ntile_n][nchunk][kchunk/64][3][Np x 64 B]
   unsigned long long* colmax;  // [nchunk][N]

@@ -574,8 +574,12 @@ __global__ void __launch_bounds__(128, 4) k_reflect2d(SynthParams p, double2* __
 // z rows (the per-row arithmetic and outputs are those of one row per thread)
 constexpr int COEF1D_ZB = 4;
 
-__global__ void __launch_bounds__(128) k_coef1d_amp(SynthParams p, const double2* __restrict__ amp, double* C0,
-                                                     double* C1, double* C2) {
+// T = double for the FP64 contraction; float for the int8x3 one, whose digit images need 24
+// significant bits (an FP32 rounding of a column's value adds at most half a step of its
+// fixed-point scale) and whose coefficient columns are then half the memory traffic
+template <class T>
+__global__ void __launch_bounds__(128) k_coef1d_amp(SynthParams p, const double2* __restrict__ amp, T* C0, T* C1,
+                                                     T* C2) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long n = p.c.n;
   if (k >= n) return;
@@ -594,25 +598,34 @@ __global__ void __launch_bounds__(128) k_coef1d_amp(SynthParams p, const double2
     coef1d_row(p, k, p.zo[zi], Af, Ab, c0, c1, c2);
     for (int i = 0; i < 5; ++i) {
       long r = 2L * (zi * 5 + i);
-      C0[r * n + k] = c0[i].x;
-      C0[(r + 1) * n + k] = c0[i].y;
+      C0[r * n + k] = (T)c0[i].x;
+      C0[(r + 1) * n + k] = (T)c0[i].y;
     }
     for (int i = 0; i < 4; ++i) {
       long r = 2L * (zi * 4 + i);
-      C1[r * n + k] = c1[i].x;
-      C1[(r + 1) * n + k] = c1[i].y;
-      C2[r * n + k] = c2[i].x;
-      C2[(r + 1) * n + k] = c2[i].y;
+      C1[r * n + k] = (T)c1[i].x;
+      C1[(r + 1) * n + k] = (T)c1[i].y;
+      C2[r * n + k] = (T)c2[i].x;
+      C2[(r + 1) * n + k] = (T)c2[i].y;
     }
   }
 }
 
-cudaError_t launch_coef1d_amp(const SynthParams& p, double2* amp, double* C0, double* C1, double* C2, cudaStream_t s) {
+template <class T>
+static cudaError_t coef1d_amp_impl(const SynthParams& p, double2* amp, T* C0, T* C1, T* C2, cudaStream_t s) {
   if (p.c.n <= 0 || p.nz <= 0) return cudaSuccess;
   k_reflect2d<<<(unsigned)((p.c.n + 127) / 128), 128, 0, s>>>(p, amp);
-  k_coef1d_amp<<<dim3((unsigned)((p.c.n + 127) / 128), (unsigned)((p.nz + COEF1D_ZB - 1) / COEF1D_ZB)), 128, 0, s>>>(
+  k_coef1d_amp<T><<<dim3((unsigned)((p.c.n + 127) / 128), (unsigned)((p.nz + COEF1D_ZB - 1) / COEF1D_ZB)), 128, 0, s>>>(
       p, amp, C0, C1, C2);
   return cudaGetLastError();
+}
+
+cudaError_t launch_coef1d_amp(const SynthParams& p, double2* amp, double* C0, double* C1, double* C2, cudaStream_t s) {
+  return coef1d_amp_impl<double>(p, amp, C0, C1, C2, s);
+}
+
+cudaError_t launch_coef1d_amp(const SynthParams& p, double2* amp, float* C0, float* C1, float* C2, cudaStream_t s) {
+  return coef1d_amp_impl<float>(p, amp, C0, C1, C2, s);
 }
 
 // per node of a k_strengths_rows block: 12 amplitudes, the obs-layer basis (16), sf, sb (6 each),
