@@ -61,6 +61,10 @@ int ytf_ctx_set_stream(ytf_ctx* ctx, void* cuda_stream);
  * YTF_ERR_CUDA with "a tensor-core pipeline wait timed out"; the context stays usable.
  * Tests set a tiny limit to drive that path. */
 int ytf_ctx_set_wait_limit(ytf_ctx* ctx, long polls);
+/* Workspace bound, in bytes, of one group of ytf_green_batch's grouped 1D int8x3 synthesis
+ * (about 14 KB per node at 64 heights); 0 restores the default 4 GiB. No counterpart in the
+ * reference. A smaller bound gives more groups (more launches), never a different item set. */
+int ytf_ctx_set_group_bytes(ytf_ctx* ctx, long bytes);
 int ytf_ctx_sync(ytf_ctx* ctx);
 const char* ytf_last_error(const ytf_ctx* ctx);
 
@@ -284,7 +288,11 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, double zsrc_l
 
 /* closed_form_G over many (cache, observation set) items with one synchronisation: the
  * same results as ytf_green per item, in order, on the context's stream; the coordinates of
- * all items go up in one copy and the items' kernels queue back to back. The reference
+ * all items go up in one copy and the items' kernels queue back to back. 1D items of real
+ * nodes (at most 262144) at YTF_PREC_INT8X3 are synthesised together, six launches per
+ * group of items (ytf_ctx_set_group_bytes): each such item's G equals ytf_green's to the
+ * int8x3 tolerance (the contraction's node slices, and so the slices' fixed-point scales,
+ * differ); every other item's G is ytf_green's bit for bit. The reference
  * calls closed_form_G once per cache (mod_ClosedFormField.jl:435, :711); its callers loop
  * (e.g. build_closed_form_green, mod_ClosedFormAssembly.jl:114). */
 int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* desc);

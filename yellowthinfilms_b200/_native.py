@@ -57,6 +57,7 @@ SIGNATURES = {
     "ytf_ctx_destroy": (ctypes.c_int, [_vp]),
     "ytf_ctx_set_stream": (ctypes.c_int, [_vp, _vp]),
     "ytf_ctx_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_long]),
+    "ytf_ctx_set_group_bytes": (ctypes.c_int, [_vp, ctypes.c_long]),
     "ytf_ctx_sync": (ctypes.c_int, [_vp]),
     "ytf_last_error": (ctypes.c_char_p, [_vp]),
     "ytf_ctx_profile": (ctypes.c_int, [_vp, ctypes.c_int]),

@@ -49,6 +49,11 @@ class Context:
         (0: the default); a wait that runs out makes the call raise RuntimeError."""
         self.check(lib().ytf_ctx_set_wait_limit(self.h, int(polls)))
 
+    def set_group_bytes(self, nbytes: int = 0) -> None:
+        """Workspace bound of one group of closed_form_G_batch's grouped 1D int8x3 synthesis
+        (0: the default 4 GiB)."""
+        self.check(lib().ytf_ctx_set_group_bytes(self.h, int(nbytes)))
+
     def sync(self) -> None:
         self.check(lib().ytf_ctx_sync(self.h))
 

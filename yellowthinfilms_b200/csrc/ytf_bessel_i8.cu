@@ -66,9 +66,9 @@ __device__ __forceinline__ double col_scale(unsigned long long bits) {
   return (m > 0.0 && isfinite(m)) ? BI_SCALE / m : 0.0;
 }
 
-// per (slice, column) max |C| as IEEE bits (Inf for a non-finite entry)
-__global__ void k_bcolmax(BesselI8 p) {
-  const int col = blockIdx.x, z = blockIdx.y;
+// per (slice, column) max |C| as IEEE bits (Inf for a non-finite entry); 256 threads, every
+// thread of the block calls it
+__device__ __forceinline__ void bcolmax_body(const BesselI8& p, int col, int z) {
   const long k0 = (long)z * p.kchunk, k1 = min(p.K, k0 + p.kchunk);
   const float* c = p.C + (long)col * p.K;
   double m = 0.0;
@@ -85,13 +85,13 @@ __global__ void k_bcolmax(BesselI8 p) {
   }
   if (threadIdx.x == 0) p.colmax[(long)z * p.N + col] = (unsigned long long)__double_as_longlong(red[0]);
 }
+__global__ void __launch_bounds__(256) k_bcolmax(BesselI8 p) { bcolmax_body(p, blockIdx.x, blockIdx.y); }
 
 // one thread per (column tile, row slot, slice, 16-node group): 16 bytes of each digit plane
 // one thread per 4 consecutive nodes of a column slot (one 32-bit word of each digit plane):
 // adjacent threads read adjacent 32-byte runs of C
-__global__ void k_bimg_real(BesselI8 p) {
+__device__ __forceinline__ void bimg_real_body(const BesselI8& p, long t) {
   const long words = p.kchunk / 4;
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long total = (long)p.ntile_n * p.Np * p.nchunk * words;
   if (t >= total) return;
   const long wq = t % words;
@@ -122,6 +122,90 @@ __global__ void k_bimg_real(BesselI8 p) {
   for (int pl = 0; pl < 3; ++pl)
     *reinterpret_cast<uint32_t*>(blk + (size_t)pl * p.Np * 64 + plane_off(slot, kb) + 4 * q) =
         b[pl][0] | (b[pl][1] << 8) | (b[pl][2] << 16) | (b[pl][3] << 24);
+}
+__global__ void k_bimg_real(BesselI8 p) { bimg_real_body(p, (long)blockIdx.x * blockDim.x + threadIdx.x); }
+
+// the same digit images with the (slice, column) maxima taken in the same kernel: one block of
+// 256 threads per (column tile, 8-slot row group, node slice). Thread (j, r8) = (tid >> 3,
+// tid & 7) takes column slot 8 rg + r8 and the slice's 16-node groups j, j + 32, ...: a first
+// pass reduces max |C| (IEEE bits into colmax, as k_bcolmax: a non-finite entry counts as Inf),
+// a second pass reads the same bytes again (from L2) and writes the digits. Each thread reads
+// 64 consecutive bytes of its column per group; a warp (four groups x eight slots) writes each
+// digit plane's 512-byte block of a stage whole. Blocks: ntile_n x (Np / 8) x nchunk.
+// 16 entries c[k0 .. k0 + 15] (k0 a multiple of 16, c's rows on 16 bytes), zero at k >= K: four
+// 16-byte loads when the group lies wholly below K
+__device__ __forceinline__ void load16(const float* c, long k0, long K, float v[16]) {
+  if (k0 + 16 <= K) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 f = __ldg(reinterpret_cast<const float4*>(c + k0) + q);
+      v[4 * q] = f.x; v[4 * q + 1] = f.y; v[4 * q + 2] = f.z; v[4 * q + 3] = f.w;
+    }
+  } else {
+#pragma unroll
+    for (int h = 0; h < 16; ++h) v[h] = k0 + h < K ? c[k0 + h] : 0.0f;
+  }
+}
+
+__device__ __forceinline__ void bimg_slice_body(const BesselI8& p, long b) {
+  __shared__ float wmax[8][8];
+  const int tid = threadIdx.x, r8 = tid & 7, j = tid >> 3;
+  const int rgroups = p.Np / 8;
+  const int rg = (int)(b % rgroups);
+  const long rest = b / rgroups;
+  const int z = (int)(rest % p.nchunk);
+  const int ct = (int)(rest / p.nchunk);
+  const int slot = rg * 8 + r8;
+  const int col = ct * p.ctile + slot;
+  const bool cv = slot < p.ctile && col < p.N;
+  const float* c = p.C + (long)(cv ? col : 0) * p.ldc;
+  const long kbase = (long)z * p.kchunk;
+  const int groups = (int)(p.kchunk / 16);
+  float m = 0.0f;
+  for (int g = j; g < groups; g += 32) {
+    float v[16];
+    load16(c, kbase + 16L * g, cv ? p.K : 0, v);
+#pragma unroll
+    for (int h = 0; h < 16; ++h) m = isfinite(v[h]) ? fmaxf(m, fabsf(v[h])) : __int_as_float(0x7f800000);
+  }
+  // lanes 8 apart share a slot: reduce over them, then over the block's eight warps
+  m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 8));
+  m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 16));
+  if ((tid & 31) < 8) wmax[tid >> 5][r8] = m;
+  __syncthreads();
+  float mm = wmax[0][r8];
+#pragma unroll
+  for (int w = 1; w < 8; ++w) mm = fmaxf(mm, wmax[w][r8]);
+  const unsigned long long bits = (unsigned long long)__double_as_longlong((double)mm);
+  if (j == 0 && cv) p.colmax[(long)z * p.N + col] = bits;
+  const double sB = cv ? col_scale(bits) : 0.0;
+  const long nstage = p.kchunk / BI_NODES;
+  const size_t sbytes = 3ul * (size_t)p.Np * 64;
+  uint8_t* base = p.Bimg + ((size_t)ct * p.nchunk + z) * nstage * sbytes;
+  for (int g = j; g < groups; g += 32) {
+    float v16[16];
+    load16(c, kbase + 16L * g, cv ? p.K : 0, v16);
+    uint32_t w[3][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      uint32_t b0 = 0, b1 = 0, b2 = 0;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const double v = (double)v16[4 * q + h];
+        uint32_t d0, d1, d2;
+        digits3b(__double2int_rn(v * sB), d0, d1, d2);
+        b0 |= d0 << (8 * h);
+        b1 |= d1 << (8 * h);
+        b2 |= d2 << (8 * h);
+      }
+      w[0][q] = b0; w[1][q] = b1; w[2][q] = b2;
+    }
+    uint8_t* blk = base + (size_t)(g / 4) * sbytes;
+#pragma unroll
+    for (int pl = 0; pl < 3; ++pl)
+      *reinterpret_cast<uint4*>(blk + (size_t)pl * p.Np * 64 + plane_off(slot, (g % 4) * 16)) =
+          make_uint4(w[pl][0], w[pl][1], w[pl][2], w[pl][3]);
+  }
 }
 
 // one thread per (radius tile, row, slice, 16-node group): J_n(k ρ) straight into digits
@@ -168,10 +252,9 @@ __global__ void k_aimg_bessel(BesselI8 p) {
 // (series below |x| = 1, recurrence above, as bessel_j012), three images in the same layout.
 // One thread per 4 consecutive nodes of a radius (one 32-bit word of each digit plane): the
 // FP64 Bessel chains are latency-bound, so short chains and many threads.
-__global__ void __launch_bounds__(256) k_aimg_bessel3(BesselI8 p, uint8_t* __restrict__ A0, uint8_t* __restrict__ A1,
-                                                       uint8_t* __restrict__ A2) {
+__device__ __forceinline__ void aimg_bessel3_body(const BesselI8& p, long t, uint8_t* __restrict__ A0,
+                                                  uint8_t* __restrict__ A1, uint8_t* __restrict__ A2) {
   const long words = p.kchunk / 4;
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long total = (long)p.ntile_m * BI_M * p.nchunk * words;
   if (t >= total) return;
   const long wq = t % words;
@@ -224,6 +307,10 @@ __global__ void __launch_bounds__(256) k_aimg_bessel3(BesselI8 p, uint8_t* __res
       *reinterpret_cast<uint32_t*>(out[o] + (size_t)pl * BI_M * 64 + plane_off(row, kb) + 4 * q) =
           b[o][pl][0] | (b[o][pl][1] << 8) | (b[o][pl][2] << 16) | (b[o][pl][3] << 24);
 }
+__global__ void __launch_bounds__(256) k_aimg_bessel3(BesselI8 p, uint8_t* __restrict__ A0, uint8_t* __restrict__ A1,
+                                                       uint8_t* __restrict__ A2) {
+  aimg_bessel3_body(p, (long)blockIdx.x * blockDim.x + threadIdx.x, A0, A1, A2);
+}
 
 cudaError_t launch_bessel_i8_aimg3(const BesselI8& p, uint8_t* A0, uint8_t* A1, uint8_t* A2, cudaStream_t s) {
   if (p.M <= 0 || p.K <= 0) return cudaSuccess;
@@ -253,10 +340,9 @@ __device__ __forceinline__ void bi_drain_wait(uint32_t bar, uint32_t parity) {
     if (mbar_try(bar, parity)) return;
 }
 
-__global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img(BesselI8 p) {
-  extern __shared__ __align__(1024) uint8_t smem[];
+// one CTA's (radius tile mt, column tile ct, node slice z) contraction; every thread calls it
+__device__ __forceinline__ void gemm_i8_img_body(const BesselI8& p, int mt, int ct, int z, uint8_t* smem) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int mt = blockIdx.x, ct = blockIdx.y, z = blockIdx.z;
   const int c0 = ct * p.ctile;
   const int nct = min(p.ctile, p.N - c0);
   const long k0 = (long)z * p.kchunk, k1 = min(p.K, k0 + p.kchunk);
@@ -381,6 +467,10 @@ __global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img(BesselI8 p) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BI_TMEM_COLS) : "memory");
   }
 }
+__global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img(BesselI8 p) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  gemm_i8_img_body(p, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+}
 
 // P[r][c] = Σ_z partial[z][c][r] through a 32 x 32 shared-memory transpose
 __global__ void k_reduce_transpose(int M, int N, int nz, const double* __restrict__ part, double* __restrict__ P) {
@@ -426,6 +516,62 @@ cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s) {
   k_reduce_transpose<<<dim3((unsigned)((p.M + 31) / 32), (unsigned)((p.N + 31) / 32)), dim3(32, 8), 0, s>>>(
       p.M, p.N, p.nchunk, p.partial, P);
   return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// Grouped launches: every (item, order) entry of a group in one grid per stage. Entry
+// e = 3 i + o holds item i's order-o parameters; its J_n images share item i's node slicing
+// (bp[3 i] gives the layout), so one Bessel evaluation per (ρ, k) serves the three orders.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_aimg_bessel3_group(const BesselI8* __restrict__ bp, const long* __restrict__ first,
+                                                          int ni) {
+  const int i = group_entry(first, ni, blockIdx.x);
+  const BesselI8& p = bp[3 * i];
+  aimg_bessel3_body(p, (long)(blockIdx.x - first[i]) * blockDim.x + threadIdx.x, bp[3 * i].Aimg, bp[3 * i + 1].Aimg,
+                    bp[3 * i + 2].Aimg);
+}
+
+// ntile_n x (Np / 8) x nchunk blocks per entry (bimg_slice_body)
+__global__ void __launch_bounds__(256) k_bimg_real_group(const BesselI8* __restrict__ bp, const long* __restrict__ first,
+                                                       int ne) {
+  const int e = group_entry(first, ne, blockIdx.x);
+  bimg_slice_body(bp[e], blockIdx.x - first[e]);
+}
+
+// ntile_m x ntile_n x nchunk CTAs per entry, radius tile fastest (the CTAs that share a
+// column tile's B images run side by side)
+__global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img_group(const BesselI8* __restrict__ bp,
+                                                                     const long* __restrict__ first, int ne) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int e = group_entry(first, ne, blockIdx.x);
+  const BesselI8& p = bp[e];
+  const long b = blockIdx.x - first[e];
+  const int mt = (int)(b % p.ntile_m);
+  const long rest = b / p.ntile_m;
+  gemm_i8_img_body(p, mt, (int)(rest % p.ntile_n), (int)(rest / p.ntile_n), smem);
+}
+
+cudaError_t launch_bessel_i8_group(const Synth1DGroup& g, cudaStream_t s) {
+  if (g.ni <= 0) return cudaSuccess;
+  const int ne = 3 * g.ni;
+  cudaError_t e;
+  if (g.grid[2] > 0) {
+    k_aimg_bessel3_group<<<(unsigned)g.grid[2], 256, 0, s>>>(g.bp, g.first_aimg, g.ni);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (g.grid[3] > 0) {
+    k_bimg_real_group<<<(unsigned)g.grid[3], 256, 0, s>>>(g.bp, g.first_bimg, ne);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (g.grid[4] > 0) {
+    const size_t sm = bessel_i8_smem(BI_ACC_STRIDE);
+    if ((e = cudaFuncSetAttribute(k_gemm_i8_img_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) !=
+        cudaSuccess)
+      return e;
+    k_gemm_i8_img_group<<<(unsigned)g.grid[4], BI_THREADS, sm, s>>>(g.bp, g.first_gemm, ne);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace ytf

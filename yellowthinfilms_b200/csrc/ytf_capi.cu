@@ -51,6 +51,8 @@ struct ytf_ctx {
   // polls of each bounded mbarrier wait in the int8 tensor-core pipelines before it gives up
   // (ytf_ctx_set_wait_limit)
   long wait_limit = 1L << 22;
+  // workspace bound of one group of the grouped 1D int8x3 synthesis (ytf_ctx_set_group_bytes)
+  size_t group_bytes = (size_t)4 << 30;
   ~ytf_ctx() {
     for (auto s : slot_streams) cudaStreamDestroy(s);
     for (auto e : slot_events) cudaEventDestroy(e);
@@ -490,6 +492,12 @@ int ytf_ctx_set_wait_limit(ytf_ctx* ctx, long polls) {
   if (!ctx) return YTF_ERR_ARG;
   if (polls < 0) return fail(ctx, YTF_ERR_ARG, "ytf_ctx_set_wait_limit: polls must be >= 0");
   ctx->wait_limit = polls == 0 ? (1L << 22) : polls;
+  return YTF_OK;
+}
+
+int ytf_ctx_set_group_bytes(ytf_ctx* ctx, long bytes) {
+  if (!ctx || bytes < 0) return YTF_ERR_ARG;
+  ctx->group_bytes = bytes == 0 ? ((size_t)4 << 30) : (size_t)bytes;
   return YTF_OK;
 }
 
@@ -1487,7 +1495,7 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
         WS(Bi, uint8_t, "g_bi_b", (size_t)bp.ntile_n * bp.nchunk * nst * bessel_i8_stage_bytes_b(bp.Np));
         WS(cm, unsigned long long, "g_bi_cmax", (size_t)bp.nchunk * bp.N);
         WS(pt, double, "g_bi_part", (size_t)bp.nchunk * bp.N * nr);
-        bp.kr = sp.c.kr; bp.rho = drho; bp.C = Cn8[o];
+        bp.kr = sp.c.kr; bp.rho = drho; bp.C = Cn8[o]; bp.ldc = nk;
         bp.Aimg = Aord[o]; bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
         bp.wait_limit = ctx->wait_limit;
         if (o == 0) CK(LAUNCH("k_bessel_i8", launch_bessel_i8_aimg3(bp, A0i, A1i, A2i, ctx->stream)));
@@ -1769,6 +1777,83 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
                     nullptr);
 }
 
+// ------------------------------------------------------------------------------------
+// Grouped 1D int8x3 synthesis inside ytf_green_batch: the batch's 1D items of real nodes
+// (at most SYNTH1D_NODE_CHUNK nodes) in groups whose workspace stays within the context's
+// group bound (ytf_ctx_set_group_bytes, default 4 GiB); each group is six launches whatever
+// its item count (amplitudes, coefficient columns, J_n images, coefficient images with their
+// slice maxima, contraction, slice sum + assembly), with every item's blocks side by side in each
+// grid; items with host outputs get a device G in the group's workspace, copied out after it. Per item the
+// arithmetic is the per-item path's; only the node slicing of the contraction differs
+// (slices of about SYNTH1D_GROUP_SLICE nodes, whose fixed-point scales are per slice).
+// ------------------------------------------------------------------------------------
+constexpr long SYNTH1D_GROUP_SLICE = 4096;
+
+struct Group1DLayout {
+  int item;
+  long nk;
+  int nz, nr, ntm;
+  long kchunk, ldc;
+  int nchunk;
+  int N[3], ctile[3], Np[3], ntn[3];
+  size_t off_amp, off_C, off_A[3], off_B[3], off_pt[3];
+  size_t cm_off[3], cm_bytes;  // slice maxima, in the group's separate maxima block
+  size_t off_G;  // device G of an item whose output is host memory (copied out after its group)
+  size_t bytes;
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+static Group1DLayout group1d_layout(int item, long nk, int nz, int nr, long npix, bool host_out, long slice) {
+  Group1DLayout L;
+  std::memset(&L, 0, sizeof(L));
+  L.item = item; L.nk = nk; L.nz = nz; L.nr = nr;
+  L.ntm = (nr + 127) / 128;
+  int nchunk = (int)std::max(1L, (nk + slice - 1) / slice);
+  long kchunk = (nk + nchunk - 1) / nchunk;
+  kchunk = std::min(16384L, std::max(64L, ((kchunk + 63) / 64) * 64));
+  L.kchunk = kchunk;
+  L.nchunk = (int)((nk + kchunk - 1) / kchunk);
+  const size_t nst = (size_t)(kchunk / 64);
+  size_t off = 0;
+  auto take = [&](size_t b) { size_t o = off; off += align256(b); return o; };
+  L.off_amp = take(sizeof(double2) * 12 * (size_t)nk);
+  L.ldc = (nk + 3) / 4 * 4;
+  L.off_C = take(sizeof(float) * 26 * (size_t)nz * L.ldc);
+  for (int o = 0; o < 3; ++o) {
+    L.N[o] = (o == 0 ? 10 : 8) * nz;
+    L.ctile[o] = bessel_i8_ctile(L.N[o]);
+    L.Np[o] = ((L.ctile[o] + 15) / 16) * 16;
+    L.ntn[o] = (L.N[o] + L.ctile[o] - 1) / L.ctile[o];
+    L.off_A[o] = take((size_t)L.ntm * L.nchunk * nst * bessel_i8_stage_bytes_a());
+    L.off_B[o] = take((size_t)L.ntn[o] * L.nchunk * nst * bessel_i8_stage_bytes_b(L.Np[o]));
+    L.off_pt[o] = take(sizeof(double) * (size_t)L.nchunk * L.N[o] * nr);
+  }
+  L.off_G = host_out ? take(sizeof(double2) * 9 * (size_t)npix * nz) : 0;
+  L.bytes = off;
+  size_t cm = 0;
+  for (int o = 0; o < 3; ++o) {
+    L.cm_off[o] = cm;
+    cm += sizeof(unsigned long long) * (size_t)L.nchunk * L.N[o];
+  }
+  L.cm_bytes = cm;
+  return L;
+}
+
+// device descriptor block of one group: items, entries and the seven block tables
+struct Group1DDesc {
+  size_t off_it, off_bp, off_first, bytes;
+  int ni;
+  long grid[6];
+
+};
+
+static bool group1d_eligible(const ytf_ctx* ctx, const ytf_green_desc& g) {
+  const ytf_cache* c = g.cache;
+  return c && c->ctx == ctx && !c->is2d && !c->d_kri && c->n > 0 && c->n <= SYNTH1D_NODE_CHUNK &&
+         g.precision == YTF_PREC_INT8X3 && g.out && g.nz > 0 && g.nx > 0 && g.ny > 0 && g.xs && g.ys && g.z_obs;
+}
+
 int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
   if (!ctx || nb < 0 || (nb > 0 && !d)) return YTF_ERR_ARG;
   if (nb == 0) return YTF_OK;
@@ -1797,7 +1882,74 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
   }
   const size_t nd = std::max<size_t>(tot + tot_r, 1);  // doubles, then the int maps
   const size_t bytes = 8 * nd + 4 * tot_m;
-  double* h = (double*)pinned_staging(ctx, bytes);
+  // the grouped 1D int8x3 items: layouts, groups within the workspace budget (largest items
+  // first, so each grid starts with its longest blocks), descriptor sizes
+  std::vector<SynthParams> gsp(nb);
+  std::vector<char> grouped(nb, 0);
+  std::vector<Group1DLayout> lay;
+  {
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+    double ctas = 0.0;  // contraction CTAs of all candidates at one-node slices
+    std::vector<int> cand;
+    for (int i = 0; i < nb; ++i) {
+      if (!group1d_eligible(ctx, d[i]) || ur[i].empty()) continue;
+      SynthParams sp;
+      if (synth_setup(ctx, d[i].cache, d[i].obs_layer, d[i].zsrc_local, d[i].terms, d[i].nz, sp) != YTF_OK) {
+        ctx->err.clear();  // the item takes the per-item path, which reports its error
+        continue;
+      }
+      gsp[i] = sp;
+      cand.push_back(i);
+      const double ntm = (double)((ur[i].size() + 127) / 128);
+      for (int od = 0; od < 3; ++od) {
+        const int N = (od == 0 ? 10 : 8) * d[i].nz, ct = bessel_i8_ctile(N);
+        ctas += ntm * (double)((N + ct - 1) / ct) * (double)d[i].cache->n;
+      }
+    }
+    // slices of SYNTH1D_GROUP_SLICE nodes, finer when that leaves under two CTAs per SM
+    long slice = SYNTH1D_GROUP_SLICE;
+    if (!cand.empty() && ctas / (double)slice < 2.0 * nsm)
+      slice = std::max(64L, std::min(slice, (long)(ctas / (2.0 * nsm)) / 64 * 64));
+    for (int i : cand)
+      lay.push_back(group1d_layout(i, d[i].cache->n, d[i].nz, (int)ur[i].size(), (long)d[i].nx * d[i].ny,
+                                   !d[i].out_is_device, slice));
+    std::stable_sort(lay.begin(), lay.end(), [](const Group1DLayout& a, const Group1DLayout& b) { return a.nk > b.nk; });
+  }
+  std::vector<std::pair<size_t, size_t>> groups;  // [begin, end) into lay
+  std::vector<size_t> item_base(lay.size(), 0), item_cm(lay.size(), 0);
+  size_t group_ws = 0, group_cm_max = 0;
+  for (size_t j = 0, cur = 0, cur_cm = 0; j < lay.size(); ++j) {
+    if (groups.empty() || (cur > 0 && cur + lay[j].bytes > ctx->group_bytes)) {
+      groups.push_back({j, j});
+      cur = cur_cm = 0;
+    }
+    item_base[j] = cur;
+    item_cm[j] = cur_cm;
+    cur += lay[j].bytes;
+    cur_cm += lay[j].cm_bytes;
+    groups.back().second = j + 1;
+    group_ws = std::max(group_ws, cur);
+    group_cm_max = std::max(group_cm_max, cur_cm);
+    grouped[lay[j].item] = 1;
+  }
+  std::vector<Group1DDesc> gdesc(groups.size());
+  const size_t desc_off = align256(bytes);
+  size_t desc_bytes = 0;
+  for (size_t g = 0; g < groups.size(); ++g) {
+    const int ni = (int)(groups[g].second - groups[g].first);
+    Group1DDesc& D = gdesc[g];
+    D.ni = ni;
+    D.off_it = desc_off + desc_bytes;
+    D.off_bp = D.off_it + align256(sizeof(Synth1DItem) * ni);
+    D.off_first = D.off_bp + align256(sizeof(BesselI8) * 3 * ni);
+    D.bytes = align256(sizeof(Synth1DItem) * ni) + align256(sizeof(BesselI8) * 3 * ni) +
+              align256(sizeof(long) * (4 * (size_t)(ni + 1) + 2 * (size_t)(3 * ni + 1)));
+
+    desc_bytes += D.bytes;
+  }
+  const size_t total_bytes = desc_off + desc_bytes;
+  double* h = (double*)pinned_staging(ctx, total_bytes);
   if (!h) return fail(ctx, YTF_ERR_NOMEM, "closed_form_G: page-locked staging allocation failed");
   std::vector<size_t> o(nb);
   size_t k = 0;
@@ -1815,11 +1967,124 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
     if (!ur[i].empty()) std::memcpy(h + tot + orho[i], ur[i].data(), 8 * ur[i].size());
     if (!rmap[i].empty()) std::memcpy(hm + omap[i], rmap[i].data(), 4 * rmap[i].size());
   }
-  WS(dc, double, "gb_coords", (bytes + 7) / 8);
+  WS(dc, double, "gb_coords", (total_bytes + 7) / 8);
   WS(err, unsigned, "gb_tc_err", 1);
-  CK(cudaMemcpyAsync(dc, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
   const int* dm = (const int*)(dc + nd);
+  uint8_t* gws = nullptr;
+  uint8_t* gcm = nullptr;
+  if (group_ws) {
+    WS(w, uint8_t, "gb1_ws", group_ws);
+    WS(wc, uint8_t, "gb1_cmax", group_cm_max);
+    gws = w;
+    gcm = wc;
+  }
+  // the groups' descriptors, behind the coordinates in the same staging block and copy
+  for (size_t g = 0; g < groups.size(); ++g) {
+    Group1DDesc& D = gdesc[g];
+    const int ni = D.ni;
+    Synth1DItem* hit = (Synth1DItem*)((char*)h + D.off_it);
+    BesselI8* hbp = (BesselI8*)((char*)h + D.off_bp);
+    long* hf = (long*)((char*)h + D.off_first);
+    long* f_ref = hf;
+    long* f_coef = f_ref + (ni + 1);
+    long* f_aimg = f_coef + (ni + 1);
+    long* f_asm = f_aimg + (ni + 1);
+    long* f_bimg = f_asm + (ni + 1);
+    long* f_gemm = f_bimg + (3 * ni + 1);
+    long nref = 0, ncoef = 0, naimg = 0, nasm = 0, nbimg = 0, ngemm = 0;
+    for (int q = 0; q < ni; ++q) {
+      const size_t j = groups[g].first + q;
+      const Group1DLayout& L = lay[j];
+      const int i = L.item;
+      uint8_t* base = gws + item_base[j];
+      Synth1DItem& it = hit[q];
+      std::memset(&it, 0, sizeof(it));
+      it.sp = gsp[i];
+      it.sp.zo = dc + o[i];
+      it.amp = (double2*)(base + L.off_amp);
+      it.C = (float*)(base + L.off_C);
+      it.ldc = L.ldc;
+      it.nx = d[i].nx; it.ny = d[i].ny; it.nr = L.nr;
+      it.xs = dc + o[i] + d[i].nz;
+      it.ys = dc + o[i] + d[i].nz + d[i].nx;
+      it.rmap = dm + omap[i];
+      it.G = d[i].out_is_device ? (double2*)d[i].out : (double2*)(base + L.off_G);
+      it.nchunk = L.nchunk;
+      it.kchunk = L.kchunk;
+      {  // evenly spaced heights (to 4 ulp of the progression): rows by recurrence
+        const double* zv = d[i].z_obs;
+        const int m = d[i].nz;
+        const double dz = m > 1 ? (zv[m - 1] - zv[0]) / (m - 1) : 0.0;
+        const double tol = 4 * 2.220446049250313e-16 * std::max(std::fabs(zv[0]), std::fabs(zv[m - 1]));
+        bool even = m > 1 && std::isfinite(dz) && dz != 0.0;
+        for (int r = 0; r < m && even; ++r) even = std::fabs(zv[r] - (zv[0] + r * dz)) <= tol;
+        it.dz = even ? dz : 0.0;
+      }
+      for (int od = 0; od < 3; ++od) it.part[od] = (const double*)(base + L.off_pt[od]);
+      const long nkb = (L.nk + 127) / 128;
+      f_ref[q] = nref; nref += nkb;
+      f_coef[q] = ncoef; ncoef += nkb * ((L.nz + COEF1D_ZB_GROUP - 1) / COEF1D_ZB_GROUP);
+      f_aimg[q] = naimg; naimg += ((long)L.ntm * 128 * L.nchunk * (L.kchunk / 4) + 255) / 256;
+      f_asm[q] = nasm; nasm += ((long)d[i].nx * d[i].ny * L.nz + 127) / 128;
+      const size_t coff[3] = {0, 10 * (size_t)L.nz * L.ldc, 18 * (size_t)L.nz * L.ldc};
+      for (int od = 0; od < 3; ++od) {
+        BesselI8& bp = hbp[3 * q + od];
+        std::memset(&bp, 0, sizeof(bp));
+        bp.M = L.nr; bp.N = L.N[od]; bp.K = L.nk; bp.order = od;
+        bp.ctile = L.ctile[od]; bp.Np = L.Np[od];
+        bp.ntile_m = L.ntm; bp.ntile_n = L.ntn[od];
+        bp.kchunk = L.kchunk; bp.nchunk = L.nchunk;
+        bp.kr = gsp[i].c.kr;
+        bp.rho = dc + tot + orho[i];
+        bp.C = it.C + coff[od];
+        bp.ldc = L.ldc;
+        bp.Aimg = base + L.off_A[od];
+        bp.Bimg = base + L.off_B[od];
+        bp.colmax = (unsigned long long*)(gcm + item_cm[j] + L.cm_off[od]);
+        bp.partial = (double*)(base + L.off_pt[od]);
+        bp.err = err;
+        bp.wait_limit = ctx->wait_limit;
+        bp.aimg_ready = 1;
+        const int e = 3 * q + od;
+        f_bimg[e] = nbimg;
+        nbimg += (long)bp.ntile_n * (bp.Np / 8) * bp.nchunk;
+        f_gemm[e] = ngemm; ngemm += (long)bp.ntile_m * bp.ntile_n * bp.nchunk;
+      }
+    }
+    f_ref[ni] = nref; f_coef[ni] = ncoef; f_aimg[ni] = naimg; f_asm[ni] = nasm;
+    f_bimg[3 * ni] = nbimg; f_gemm[3 * ni] = ngemm;
+    const long grid[6] = {nref, ncoef, naimg, nbimg, ngemm, nasm};
+    for (int k = 0; k < 6; ++k) D.grid[k] = grid[k];
+  }
+  CK(cudaMemcpyAsync(dc, h, total_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+  for (size_t g = 0; g < groups.size(); ++g) {
+    const Group1DDesc& D = gdesc[g];
+    const int ni = D.ni;
+    const char* dbase = (const char*)dc;
+    Synth1DGroup G;
+    G.ni = ni;
+    G.it = (const Synth1DItem*)(dbase + D.off_it);
+    G.bp = (const BesselI8*)(dbase + D.off_bp);
+    const long* df = (const long*)(dbase + D.off_first);
+    G.first_reflect = df;
+    G.first_coef = df + (ni + 1);
+    G.first_aimg = df + 2 * (ni + 1);
+    G.first_asm = df + 3 * (ni + 1);
+    G.first_bimg = df + 4 * (ni + 1);
+    G.first_gemm = G.first_bimg + (3 * ni + 1);
+    for (int k = 0; k < 6; ++k) G.grid[k] = D.grid[k];
+    CK(LAUNCH("k_coef1d", launch_reflect_coef_group(G, ctx->stream)));
+    CK(LAUNCH("k_bessel_i8", launch_bessel_i8_group(G, ctx->stream)));
+    CK(LAUNCH("k_assemble1d", launch_assemble1d_group(G, ctx->stream)));
+    for (size_t j = groups[g].first; j < groups[g].second; ++j) {
+      const int i = lay[j].item;
+      if (d[i].out_is_device) continue;
+      CK(cudaMemcpyAsync(d[i].out, gws + item_base[j] + lay[j].off_G,
+                         sizeof(double2) * 9 * (size_t)d[i].nx * d[i].ny * d[i].nz, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    }
+  }
   // an all-1D batch runs its items round-robin on kSlots side streams (each item is a chain
   // of small dependent launches; independent items overlap), forked from and joined to the
   // context's stream
@@ -1840,6 +2105,7 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
   cudaStream_t main = ctx->stream;
   int rc = YTF_OK;
   for (int i = 0; i < nb && !rc; ++i) {
+    if (grouped[i]) continue;
     GreenBatch gb{dc + o[i], dc + o[i] + d[i].nz, dc + o[i] + d[i].nz + d[i].nx, err};
     if (!ur[i].empty()) {
       gb.drho = dc + tot + orho[i];

@@ -241,7 +241,8 @@ struct BesselI8 {
   int nchunk;
   const double* kr;  // [K]
   const double* rho; // [M]
-  const float* C;    // [N][K] coefficient columns (FP32)
+  const float* C;    // [N][ldc] coefficient columns (FP32)
+  long ldc;          // row stride of C: K on the per-item path; K rounded up to 4 (16-byte rows) in groups
   uint8_t* Aimg;     // [ntile_m][nchunk][kchunk/64][3][128 x 64 B]
   uint8_t* Bimg;     // [ntile_n][nchunk][kchunk/64][3][Np x 64 B]
   unsigned long long* colmax;  // [nchunk][N]
@@ -258,6 +259,59 @@ size_t bessel_i8_stage_bytes_b(int Np);
 size_t bessel_i8_smem(int Np);
 int bessel_i8_ctile(int N);
 cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------
+// Grouped 1D int8x3 synthesis: the items of a batch (each a 1D cache of real nodes with its
+// own radii, heights and output) through one launch per stage for the whole group. A
+// stage's blocks are the concatenation of every item's (or every (item, order) entry's)
+// blocks; `first[e]` is the first block of entry e (first[ne] = the grid), and a block finds
+// its entry by binary search.
+// ------------------------------------------------------------------------------------
+struct Synth1DItem {
+  SynthParams sp;          // the item's node data (real nodes), term masks, heights (device)
+  double2* amp;            // [12][nk] reflected amplitudes
+  float* C;                // [26 nz][ldc] coefficient columns: orders 0, 1, 2 at rows 0, 10 nz, 18 nz
+  long ldc;                // row stride of C: nk rounded up to 4, so every row starts on 16 bytes
+  int nx, ny, nr;          // pixel grid, distinct radii
+  const double* xs;        // [nx] device
+  const double* ys;        // [ny] device
+  const int* rmap;         // [nx ny] pixel -> radius index
+  double2* G;              // [nx][ny][nz][3][3] output (Julia's column-major layout)
+  int nchunk;              // node slices of the contraction
+  long kchunk;             // nodes per slice (a multiple of 64)
+  double dz;               // spacing of evenly spaced heights (to 4 ulp), else 0
+  const double* part[3];   // [nchunk][N_o][nr] slice partials of order o (N_0 = 10 nz, N_1 = N_2 = 8 nz)
+};
+// every stage of the group, in order, on stream s; `it`/`bp` and the `first_*` tables are
+// device arrays (bp: 3 entries per item, orders 0, 1, 2; bp[3i] also carries the layout of
+// item i's J_n images). Host copies (ni, grid sizes) come in `grid`: {reflect, coef, aimg,
+// bimg, gemm, assemble}.
+struct Synth1DGroup {
+  int ni;
+  const Synth1DItem* it;
+  const BesselI8* bp;
+  const long* first_reflect;   // [ni + 1]
+  const long* first_coef;      // [ni + 1]
+  const long* first_aimg;      // [ni + 1]
+  const long* first_bimg;      // [3 ni + 1]
+  const long* first_gemm;      // [3 ni + 1]
+  const long* first_asm;       // [ni + 1]
+  long grid[6];
+};
+// the entry whose block range holds block b: the last e with first[e] <= b (first ascending)
+__device__ __forceinline__ int group_entry(const long* first, int ne, long b) {
+  int lo = 0, hi = ne;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (first[mid] <= b) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+cudaError_t launch_reflect_coef_group(const Synth1DGroup& g, cudaStream_t s);  // amplitudes, FP32 columns
+cudaError_t launch_bessel_i8_group(const Synth1DGroup& g, cudaStream_t s);     // images (with slice maxima), contraction
+cudaError_t launch_assemble1d_group(const Synth1DGroup& g, cudaStream_t s);    // slice sum + pixel assembly
+constexpr int COEF1D_ZB_GROUP = 8;   // heights per thread of the grouped coefficient kernel
 
 // Gauss-Legendre panels -> nodes/weights, bit-exact with the CPU restatement
 cudaError_t launch_gl_nodes(int npanels, const double* pa, const double* pb, const int* sing_side, const double* xi,

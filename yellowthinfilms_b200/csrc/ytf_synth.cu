@@ -1105,4 +1105,267 @@ cudaError_t launch_synth_finish(const SynthItem* items, int nitems, const long* 
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------------
+// Grouped 1D synthesis (int8x3 path): the reflected amplitudes, the FP32 coefficient columns
+// and the final slice sum + pixel assembly of every item of a group, one launch each. The
+// per-node and per-pixel arithmetic is that of k_reflect2d, k_coef1d_amp and k_assemble1d.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 4) k_reflect2d_group(const Synth1DItem* __restrict__ items,
+                                                            const long* __restrict__ first, int ni) {
+  const int i = group_entry(first, ni, blockIdx.x);
+  const Synth1DItem& it = items[i];
+  const long n = it.sp.c.n;
+  const long node = (long)(blockIdx.x - first[i]) * blockDim.x + threadIdx.x;
+  if (node >= n) return;
+  cd Af[2][3], Ab[2][3];
+  reflected_amp(it.sp, node, Af, Ab);
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      it.amp[(long)(3 * m + q) * n + node] = make_double2(Af[m][q].x, Af[m][q].y);
+      it.amp[(long)(6 + 3 * m + q) * n + node] = make_double2(Ab[m][q].x, Ab[m][q].y);
+    }
+}
+
+// one FP32 coefficient value (the int8x3 digits come from it; their scales from the
+// (slice, column) maxima the digit-image kernel takes)
+__device__ __forceinline__ void coef_store(float* C, long row, long stride, long k, double v) {
+  C[row * stride + k] = (float)v;
+}
+
+// a read-only load the compiler keeps in place (volatile asm: not hoisted out of the row loop),
+// so the node's mode fields are re-read from L1 per row instead of held in registers
+__device__ __forceinline__ cd ldc_row(const double2* b, long e, long n, long i) {
+  double x, y;
+  asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "l"(b + e * n + i));
+  return cd{x, y};
+}
+
+// the 13 coefficient columns of one (node, z row) of the scattered terms (no direct term), as
+// coef1d_row, from the W-weighted amplitudes (fin0 applied; shared memory, aw[(m 2 + br) 3 + q]
+// [thread]) and the four branch phases g[m][br] (phase_cl(kz, z or z - d_obs) kx)
+__device__ __forceinline__ void coef_row_scat(const CacheView& c, long k, const double2 (*aw)[128], const cd g[2][2],
+                                              cd c0[5], cd c1[4], cd c2[4]) {
+  const long n = c.n;
+  const cd half_i{0.0, 0.5};
+#pragma unroll
+  for (int i = 0; i < 5; ++i) c0[i] = cd{0, 0};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) { c1[i] = cd{0, 0}; c2[i] = cd{0, 0}; }
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int br = 0; br < 2; ++br) {
+      const cd ex = ldc_row(c.basis, (br == 0 ? 0 : 6) + m, n, k);
+      const cd ey = ldc_row(c.basis, (br == 0 ? 2 : 8) + m, n, k);
+      const cd ez = ldc_row(c.basis, (br == 0 ? 4 : 10) + m, n, k);
+      const int e0 = (m * 2 + br) * 3;
+      const double2 a0 = aw[e0][threadIdx.x], a1 = aw[e0 + 1][threadIdx.x], a2 = aw[e0 + 2][threadIdx.x];
+      const cd ax = cd{a0.x, a0.y} * g[m][br], ay = cd{a1.x, a1.y} * g[m][br], az = cd{a2.x, a2.y} * g[m][br];
+      c0[0] += half_i * (-(ax * ex) - ay * ey);
+      c2[0] += half_i * (ax * ex - ay * ey);
+      c0[1] += half_i * (-(ax * ey) + ay * ex);
+      c2[1] += half_i * (ax * ey + ay * ex);
+      c1[0] += ax * ez;
+      c0[2] += half_i * (-(ay * ex) + ax * ey);
+      c2[2] += half_i * (ay * ex + ax * ey);
+      c0[3] += half_i * (-(ay * ey) - ax * ex);
+      c2[3] += half_i * (ay * ey - ax * ex);
+      c1[1] += ay * ez;
+      c1[2] += az * ex;
+      c1[3] += az * ey;
+      c0[4] += cd{0.0, -1.0} * (az * ez);
+    }
+}
+
+// rows z0..z1-1 of a node with the same-layer direct term (coef1d_row), out of line so that its
+// registers and local arrays stay out of the scattered path
+__device__ __noinline__ void coef_rows_direct(const Synth1DItem& it, long k, int z0, int z1) {
+  const SynthParams& p = it.sp;
+  const long n = p.c.n;
+  const int nz = p.nz;
+  const long cst = it.ldc;  // row stride of the coefficient columns
+  float* C0 = it.C;
+  float* C1 = it.C + 10L * nz * cst;
+  float* C2 = it.C + 18L * nz * cst;
+  cd Af[2][3], Ab[2][3];
+  for (int m = 0; m < 2; ++m)
+    for (int q = 0; q < 3; ++q) {
+      Af[m][q] = ldc(it.amp, 3 * m + q, n, k);
+      Ab[m][q] = ldc(it.amp, 6 + 3 * m + q, n, k);
+    }
+  for (int zi = z0; zi < z1; ++zi) {
+    cd c0[5], c1[4], c2[4];
+    coef1d_row(p, k, p.zo[zi], Af, Ab, c0, c1, c2);
+    for (int j = 0; j < 5; ++j) {
+      coef_store(C0, 2L * (zi * 5 + j), cst, k, c0[j].x);
+      coef_store(C0, 2L * (zi * 5 + j) + 1, cst, k, c0[j].y);
+    }
+    for (int j = 0; j < 4; ++j) {
+      const long r = 2L * (zi * 4 + j);
+      coef_store(C1, r, cst, k, c1[j].x);
+      coef_store(C1, r + 1, cst, k, c1[j].y);
+      coef_store(C2, r, cst, k, c2[j].x);
+      coef_store(C2, r + 1, cst, k, c2[j].y);
+    }
+  }
+}
+
+// e^{a + i b}, out of line: the exact phases are the rare case of the recurrence below
+__device__ __noinline__ cd cexp_call(double a, double b) { return cexp(cd{a, b}); }
+
+// blocks of an item: ceil(n / 128) node blocks x ceil(nz / COEF1D_ZB_GROUP) height blocks,
+// node block fastest. For
+// the scattered terms at evenly spaced heights (it.dz != 0) the branch phases of a thread's
+// consecutive rows follow by one complex product each, e^{i kz (z + dz)} = e^{i kz z} e^{i kz dz};
+// a row whose exponent leaves phase_cl's range (or a step that overflows) takes phase_cl itself.
+__global__ void __launch_bounds__(128, 3) k_coef1d_group(const Synth1DItem* __restrict__ items,
+                                                      const long* __restrict__ first, int ni) {
+  const int i = group_entry(first, ni, blockIdx.x);
+  const Synth1DItem& it = items[i];
+  const SynthParams& p = it.sp;
+  const CacheView& c = p.c;
+  const long n = c.n;
+  const long nkb = (n + 127) / 128;
+  const long b = blockIdx.x - first[i];
+  const long k = (b % nkb) * 128 + threadIdx.x;
+  if (k >= n) return;
+  const int nz = p.nz;
+  const long cst = it.ldc;  // row stride of the coefficient columns
+  float* C0 = it.C;
+  float* C1 = it.C + 10L * nz * cst;
+  float* C2 = it.C + 18L * nz * cst;
+  const int z0 = (int)(b / nkb) * COEF1D_ZB_GROUP;
+  const int z1 = min(nz, z0 + COEF1D_ZB_GROUP);
+  if (p.with_direct) {
+    coef_rows_direct(it, k, z0, z1);
+    return;
+  }
+  // the node's W-weighted amplitudes and its four kz in shared memory (read once per row and
+  // branch; registers hold the row's accumulators and phases)
+  __shared__ double2 aw[12][128];
+  __shared__ double2 skz[4][128];
+  const cd W = cd{0.0, 1.0 / (2.0 * 3.14159265358979323846)} * cd{c.wr[k], 0.0};
+  const cd kx{c.kr[k], 0.0};
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const cd f = fin0(W * ldc(it.amp, 3 * m + q, n, k)), bk = fin0(W * ldc(it.amp, 6 + 3 * m + q, n, k));
+      aw[(m * 2) * 3 + q][threadIdx.x] = make_double2(f.x, f.y);
+      aw[(m * 2 + 1) * 3 + q][threadIdx.x] = make_double2(bk.x, bk.y);
+    }
+    skz[m * 2][threadIdx.x] = c.basis[(12L + m) * n + k];
+    skz[m * 2 + 1][threadIdx.x] = c.basis[(14L + m) * n + k];
+  }
+  const double dz = it.dz;
+  cd ph[2][2], step[2][2];
+  bool have[2][2];
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int br = 0; br < 2; ++br) {
+      have[m][br] = false;
+      ph[m][br] = cd{0, 0};
+      const double2 q = skz[m * 2 + br][threadIdx.x];
+      step[m][br] = dz != 0.0 ? cexp_call(-q.y * dz, q.x * dz) : cd{0, 0};
+      if (!(dz != 0.0 && isfin(step[m][br]))) step[m][br] = cd{0, 0};
+    }
+  for (int zi = z0; zi < z1; ++zi) {
+    const double zf = p.zo[zi], zb = zf - p.d_obs;
+    cd g[2][2];
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int br = 0; br < 2; ++br) {
+        const double2 q = skz[m * 2 + br][threadIdx.x];
+        const double zz = br == 0 ? zf : zb;
+        const double a = -q.y * zz, bb = q.x * zz;
+        if (!isfinite(a) || !isfinite(bb) || a > 700.0 || a < -700.0) {
+          ph[m][br] = cd{0, 0};
+          have[m][br] = false;
+        } else if (have[m][br] && (step[m][br].x != 0.0 || step[m][br].y != 0.0)) {
+          ph[m][br] = ph[m][br] * step[m][br];
+        } else {
+          ph[m][br] = cexp_call(a, bb);
+          have[m][br] = true;
+        }
+        g[m][br] = ph[m][br] * kx;
+      }
+    cd c0[5], c1[4], c2[4];
+    coef_row_scat(c, k, aw, g, c0, c1, c2);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      coef_store(C0, 2L * (zi * 5 + j), cst, k, c0[j].x);
+      coef_store(C0, 2L * (zi * 5 + j) + 1, cst, k, c0[j].y);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const long r = 2L * (zi * 4 + j);
+      coef_store(C1, r, cst, k, c1[j].x);
+      coef_store(C1, r + 1, cst, k, c1[j].y);
+      coef_store(C2, r, cst, k, c2[j].x);
+      coef_store(C2, r + 1, cst, k, c2[j].y);
+    }
+  }
+}
+
+cudaError_t launch_reflect_coef_group(const Synth1DGroup& g, cudaStream_t s) {
+  if (g.ni <= 0) return cudaSuccess;
+  if (g.grid[0] > 0) k_reflect2d_group<<<(unsigned)g.grid[0], 128, 0, s>>>(g.it, g.first_reflect, g.ni);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (g.grid[1] > 0) k_coef1d_group<<<(unsigned)g.grid[1], 128, 0, s>>>(g.it, g.first_coef, g.ni);
+  return cudaGetLastError();
+}
+
+// one thread per (pixel, height) of an item: P_n(r, c) = Σ_z part_n[z][c][r] (slices in
+// order, as k_reduce_transpose), then assemble1d_pixel
+__global__ void __launch_bounds__(128) k_assemble1d_group(const Synth1DItem* __restrict__ items,
+                                                          const long* __restrict__ first, int ni) {
+  const int i = group_entry(first, ni, blockIdx.x);
+  const Synth1DItem& it = items[i];
+  const long npix = (long)it.nx * it.ny;
+  const int nz = it.sp.nz;
+  const long t = (long)(blockIdx.x - first[i]) * blockDim.x + threadIdx.x;
+  if (t >= npix * nz) return;
+  const long pix = t % npix;
+  const int zi = (int)(t / npix);
+  const int ix = (int)(pix % it.nx), iy = (int)(pix / it.nx);
+  const int r = it.rmap[pix];
+  const long M = it.nr;
+  const int nch = it.nchunk;
+  const long N0 = 10L * nz, N1 = 8L * nz;
+  cd g0[5], g1[4], g2[4];
+  for (int col = 0; col < 5; ++col) {
+    const long c = 2L * (zi * 5 + col);
+    double re = 0.0, im = 0.0;
+    for (int z = 0; z < nch; ++z) {
+      re += it.part[0][((long)z * N0 + c) * M + r];
+      im += it.part[0][((long)z * N0 + c + 1) * M + r];
+    }
+    g0[col] = cd{re, im};
+  }
+  for (int col = 0; col < 4; ++col) {
+    const long c = 2L * (zi * 4 + col);
+    double r1 = 0.0, i1 = 0.0, r2 = 0.0, i2 = 0.0;
+    for (int z = 0; z < nch; ++z) {
+      r1 += it.part[1][((long)z * N1 + c) * M + r];
+      i1 += it.part[1][((long)z * N1 + c + 1) * M + r];
+      r2 += it.part[2][((long)z * N1 + c) * M + r];
+      i2 += it.part[2][((long)z * N1 + c + 1) * M + r];
+    }
+    g1[col] = cd{r1, i1};
+    g2[col] = cd{r2, i2};
+  }
+  assemble1d_pixel(it.xs[ix], it.ys[iy], g0, g1, g2, pix, npix, zi, nz, it.G);
+}
+
+cudaError_t launch_assemble1d_group(const Synth1DGroup& g, cudaStream_t s) {
+  if (g.ni <= 0 || g.grid[5] <= 0) return cudaSuccess;
+  k_assemble1d_group<<<(unsigned)g.grid[5], 128, 0, s>>>(g.it, g.first_asm, g.ni);
+  return cudaGetLastError();
+}
+
 }  // namespace ytf
