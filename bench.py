@@ -848,7 +848,11 @@ def run_learned(args):
                       "learned_proposals_accepted": rec["acc"], "stacks": rec["stacks"],
                       "mean_halvings_learned": float(np.mean(rec["h_l"])),
                       "mean_halvings_plain": float(np.mean(rec["h_p"]))},
-            "e2e": {"value": e2e, "unit": "entries/s", "h2d_bytes_per_step": int(16 * np.sum(rec["solved_l"]) / max(args.steps, 1)),
+            # host -> device per step: the rules' panel edges (16 B per 8-node panel; the nodes are
+            # expanded on the device) and every stack's observation coordinates
+            "e2e": {"value": e2e, "unit": "entries/s",
+                    "h2d_bytes_per_step": int((2 * np.sum(rec["solved_l"]) + 8 * (N_RHO + N_ZOBS + 1) * rec["stacks"])
+                                              / max(args.steps, 1)),
                     "d2h_bytes_per_step": CHUNK * ENTRIES_PER_STACK * 16,
                     "ms_per_step": 1e3 * t_e2e / max(args.steps, 1)},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),

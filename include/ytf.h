@@ -245,6 +245,9 @@ typedef struct {
   int check_symmetry;
   int rotation;          /* YTF_ROT_* */
   int is2d;
+  int nodes_on_device;   /* 1D items: k_nodes/k_weights are device pointers (this context's GPU),
+                            read on the context's stream during the call (e.g. from
+                            ytf_gl_rule_batch_device); not accepted by ytf_plan_create */
 } ytf_transfer_desc;
 
 /* Many independent builds (stacks, frequencies, source layers, grids of any sizes) in one
@@ -314,6 +317,14 @@ int ytf_gl_rule(ytf_ctx* ctx, int npanels, const double* pa, const double* pb, i
  * same places of nodes and weights. Every set's rule equals its own ytf_gl_rule call. */
 int ytf_gl_rule_batch(ytf_ctx* ctx, int nsets, const int* npanels, const double* pa, const double* pb, int order,
                       const int* nsing, const double* singular, double* nodes, double* weights);
+
+/* ytf_gl_rule_batch with the nodes and weights left in device memory: d_nodes/d_weights are
+ * device pointers (this context's GPU, npanels-sum x order doubles each), written on the
+ * context's stream; the call returns without synchronising, so work queued after it on that
+ * stream (ytf_transfer_batch with nodes_on_device) sees the rule. No counterpart in the
+ * reference. */
+int ytf_gl_rule_batch_device(ytf_ctx* ctx, int nsets, const int* npanels, const double* pa, const double* pb, int order,
+                             const int* nsing, const double* singular, double* d_nodes, double* d_weights);
 
 /* Allocation-free variant of ytf_green for 2D caches (no counterpart in the reference).
  * For callers that must not have the library allocate device memory: a host that owns all

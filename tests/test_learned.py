@@ -205,7 +205,9 @@ def test_cavity_response_batch_equals_single_calls(L):
 
 def test_device_resident_rules_equal_host_rules(L):
     """learned_rules_batch / plain_rules_batch with G and the acceptance checks in device
-    memory return the same rules and, bit for bit, the same G as the host-array form."""
+    memory (the rules as CUDA tensors, straight from the device Gauss-Legendre expansion into
+    the transfer build) return the same rules and, bit for bit, the same G as the host-array
+    form."""
     from yellowthinfilms_b200 import api
     net = _random_net(L, 7)
     rng = np.random.default_rng(41)
@@ -219,7 +221,8 @@ def test_device_resident_rules_equal_host_rules(L):
     for fn in (lambda d: L.plain_rules_batch(probs, device=d), lambda d: L.learned_rules_batch(net, probs, device=d)):
         host, dev = fn(False), fn(True)
         for a, b in zip(host, dev):
-            assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]) and a[3:] == b[3:]
+            npy = lambda x: x.cpu().numpy() if hasattr(x, "cpu") else np.asarray(x)
+            assert np.array_equal(a[1], npy(b[1])) and np.array_equal(a[2], npy(b[2])) and a[3:] == b[3:]
             assert np.array_equal(a[0], b[0].cpu().numpy())
 
 
@@ -227,6 +230,7 @@ def test_gl_rule_batch_equals_single_calls(L):
     """ytf_gl_rule_batch: every panel set's nodes and weights bit for bit as its own
     ytf_gl_rule call (each set with its own singular points; empty sets included)."""
     from yellowthinfilms_b200 import api
+    from yellowthinfilms_b200.materials import FlatOpticalLayer, IsotropicMaterial
     rng = np.random.default_rng(5)
     sets = []
     for j in range(6):
@@ -242,3 +246,15 @@ def test_gl_rule_batch_equals_single_calls(L):
             continue
         k1, w1 = api.gl_rule(P, 8, singular=sing)
         assert np.array_equal(k, k1) and np.array_equal(w, w1)
+    # the device form (ytf_gl_rule_batch_device): the same rules as CUDA tensors, and a 1D
+    # transfer build from them equal to one from the host arrays
+    dev = api.gl_rule_batch(sets, 8, device=True)
+    for (k, w), (kd, wd) in zip(got, dev):
+        assert kd.is_cuda and np.array_equal(k, kd.cpu().numpy()) and np.array_equal(w, wd.cpu().numpy())
+    st = [FlatOpticalLayer(IsotropicMaterial(1.0), 0.5), FlatOpticalLayer(IsotropicMaterial(2.25), 0.3),
+          FlatOpticalLayer(IsotropicMaterial(1.0), 0.5)]
+    items = [dict(stack=st, omega=2.0, source_layer=1, kx_nodes=k, wt_nodes=w, obs_layers=[1]) for k, w in got if len(k)]
+    items_d = [dict(stack=st, omega=2.0, source_layer=1, kx_nodes=k, wt_nodes=w, obs_layers=[1]) for k, w in dev if len(k)]
+    for a, b in zip(api.build_cavity_transfer_batch(items), api.build_cavity_transfer_batch(items_d)):
+        ea, eb = a.export(), b.export()
+        assert all(np.array_equal(ea[x], eb[x]) for x in ea)

@@ -18,16 +18,18 @@ _vp = ctypes.c_void_p
 
 class TransferDesc(ctypes.Structure):
     """ytf_transfer_desc (include/ytf.h)."""
+    # array fields as raw addresses (ints): the same C ABI as typed pointers, filled without a
+    # ctypes cast per field
     _fields_ = [("stack", _vp), ("omega", ctypes.c_double), ("source_layer", ctypes.c_int), ("nk", ctypes.c_int),
-                ("k_nodes", _d), ("k_weights", _d), ("nphi", ctypes.c_int), ("phi_nodes", _d), ("phi_weights", _d),
-                ("nobs", ctypes.c_int), ("obs_layers", _i), ("check_symmetry", ctypes.c_int),
-                ("rotation", ctypes.c_int), ("is2d", ctypes.c_int)]
+                ("k_nodes", _vp), ("k_weights", _vp), ("nphi", ctypes.c_int), ("phi_nodes", _vp), ("phi_weights", _vp),
+                ("nobs", ctypes.c_int), ("obs_layers", _vp), ("check_symmetry", ctypes.c_int),
+                ("rotation", ctypes.c_int), ("is2d", ctypes.c_int), ("nodes_on_device", ctypes.c_int)]
 
 
 class GreenDesc(ctypes.Structure):
     """ytf_green_desc (include/ytf.h)."""
     _fields_ = [("cache", _vp), ("obs_layer", ctypes.c_int), ("zsrc_local", ctypes.c_double), ("nz", ctypes.c_int),
-                ("z_obs", _d), ("nx", ctypes.c_int), ("xs", _d), ("ny", ctypes.c_int), ("ys", _d),
+                ("z_obs", _vp), ("nx", ctypes.c_int), ("xs", _vp), ("ny", ctypes.c_int), ("ys", _vp),
                 ("terms", ctypes.c_int), ("precision", ctypes.c_int), ("out", _vp), ("out_is_device", ctypes.c_int)]
 
 
@@ -81,6 +83,7 @@ SIGNATURES = {
     "ytf_cavity_response_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), _d, _i,
                                                  ctypes.POINTER(ctypes.c_long), _d, ctypes.c_double, _d]),
     "ytf_gl_rule_batch": (ctypes.c_int, [_vp, ctypes.c_int, _i, _d, _d, ctypes.c_int, _i, _d, _d, _d]),
+    "ytf_gl_rule_batch_device": (ctypes.c_int, [_vp, ctypes.c_int, _i, _d, _d, ctypes.c_int, _i, _d, _vp, _vp]),
     "ytf_layer_light_lines": (ctypes.c_int, [_d, _d, ctypes.c_double, ctypes.c_double, _d, _i]),
     "ytf_nodes_1d": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams), ctypes.c_long, _d,
                                     _d, ctypes.POINTER(ctypes.c_long), ctypes.POINTER(GridInfo)]),
@@ -144,3 +147,8 @@ def lib():
 
 def ptr(a, t=_d):
     return None if a is None else a.ctypes.data_as(t)
+
+
+def addr(a):
+    """The address of a numpy array's data (for c_void_p descriptor fields); None for None."""
+    return None if a is None else a.ctypes.data

@@ -19,7 +19,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _native
-from ._native import _i, _u8, lib, ptr
+from ._native import _i, _u8, addr, lib, ptr
 from .materials import stack_arrays
 
 TERMS = {"all": 0, "direct": 1, "scattered": 2, "toeplitz": 3, "hankel": 4}
@@ -618,6 +618,13 @@ def build_cavity_transfer_batch(items, ctx: Optional[Context] = None):
             ph, wp = _f64(it["phi_nodes"]), _f64(it["phi_weights"])
             if len(ph) != len(wp):
                 raise YTFError("build_cavity_transfer_2d: φ nodes/weights length mismatch")
+        elif getattr(it["kx_nodes"], "is_cuda", False):
+            # a device-resident rule (gl_rule_batch(device=True)): float64 CUDA tensors on
+            # this context's GPU, read on its stream
+            k, w = it["kx_nodes"], it["wt_nodes"]
+            if k.dtype != w.dtype or str(k.dtype) != "torch.float64" or not (k.is_contiguous() and w.is_contiguous()):
+                raise YTFError("build_cavity_transfer_1d: device nodes must be contiguous float64 CUDA tensors")
+            ph = wp = np.zeros(0)
         else:
             k, w = _f64(it["kx_nodes"]), _f64(it["wt_nodes"])
             ph = wp = np.zeros(0)
@@ -630,10 +637,12 @@ def build_cavity_transfer_batch(items, ctx: Optional[Context] = None):
         d.omega = float(it["omega"])
         d.source_layer = int(it["source_layer"])
         d.nk = len(k)
-        d.k_nodes, d.k_weights = ptr(k), ptr(w)
+        dev = hasattr(k, "data_ptr")
+        d.k_nodes, d.k_weights = (k.data_ptr(), w.data_ptr()) if dev else (addr(k), addr(w))
+        d.nodes_on_device = int(dev)
         d.nphi = len(ph)
-        d.phi_nodes, d.phi_weights = ptr(ph), ptr(wp)
-        d.nobs, d.obs_layers = no, ptr(ob, _i)
+        d.phi_nodes, d.phi_weights = addr(ph), addr(wp)
+        d.nobs, d.obs_layers = no, addr(ob)
         d.check_symmetry = int(bool(it.get("check_symmetry", True)))
         d.rotation = -1 if rot == "auto" else int(bool(rot))
         d.is2d = int(is2d)
@@ -683,7 +692,7 @@ def closed_form_G_batch(items, precision: str = "fp64"):
             outs.append((G, nx, ny, nz))
         d = descs[i]
         d.cache, d.obs_layer, d.zsrc_local = cache.h, int(it["obs_layer"]), float(it["zsrc_local"])
-        d.nz, d.z_obs, d.nx, d.xs, d.ny, d.ys = nz, ptr(zo), nx, ptr(x), ny, ptr(y)
+        d.nz, d.z_obs, d.nx, d.xs, d.ny, d.ys = nz, addr(zo), nx, addr(x), ny, addr(y)
         d.terms, d.precision = TERMS[terms], PRECISION[it.get("precision", precision)]
         d.out, d.out_is_device = optr, on_dev
         keep += [zo, x, y]
@@ -734,9 +743,9 @@ class BatchPlan:
             no, ob = _obs_arg(it.get("obs_layers"))
             d = self._td[i]
             d.stack, d.omega, d.source_layer = st.h, float(it["omega"]), int(it["source_layer"])
-            d.nk, d.k_nodes, d.k_weights = len(k), ptr(k), ptr(w)
-            d.nphi, d.phi_nodes, d.phi_weights = len(ph), ptr(ph), ptr(wp)
-            d.nobs, d.obs_layers = no, ptr(ob, _i)
+            d.nk, d.k_nodes, d.k_weights = len(k), addr(k), addr(w)
+            d.nphi, d.phi_nodes, d.phi_weights = len(ph), addr(ph), addr(wp)
+            d.nobs, d.obs_layers = no, addr(ob)
             d.check_symmetry = int(bool(it.get("check_symmetry", True)))
             d.rotation = 0
             d.is2d = int(is2d)
@@ -762,7 +771,7 @@ class BatchPlan:
                 e.out, e.out_is_device = G.ctypes.data, 0
                 self._outs.append((G, nx, ny, nz))
             e.cache, e.obs_layer, e.zsrc_local = None, int(g["obs_layer"]), float(g["zsrc_local"])
-            e.nz, e.z_obs, e.nx, e.xs, e.ny, e.ys = nz, ptr(zo), nx, ptr(x), ny, ptr(y)
+            e.nz, e.z_obs, e.nx, e.xs, e.ny, e.ys = nz, addr(zo), nx, addr(x), ny, addr(y)
             e.terms, e.precision = TERMS[terms], PRECISION[prec]
             self._keep += [k, w, ph, wp, ob, zo, x, y]
             self._inputs.append(dict(k=k, w=w, phi=ph, wphi=wp, z=zo, x=x, y=y))
@@ -880,10 +889,12 @@ def gl_rule(panels: Sequence, order: int = 8, singular=(), ctx: Optional[Context
     return nodes, wts
 
 
-def gl_rule_batch(sets, order: int = 8, ctx: Optional[Context] = None):
+def gl_rule_batch(sets, order: int = 8, ctx: Optional[Context] = None, device: bool = False):
     """gl_rule for many (panels, singular) sets with one device call (ytf_gl_rule_batch);
     panels as [n, 2] arrays or pair sequences. Returns [(nodes, weights)] in order, each equal
-    to its own gl_rule call."""
+    to its own gl_rule call. With ``device`` the rules stay in device memory
+    (ytf_gl_rule_batch_device): float64 CUDA tensors, views of one allocation, ready for
+    build_cavity_transfer_batch on the context's stream."""
     ctx = ctx or default_context()
     if not sets:
         return []
@@ -895,6 +906,13 @@ def gl_rule_batch(sets, order: int = 8, ctx: Optional[Context] = None):
     pb = _f64(np.concatenate([p[:, 1] for p in P])) if npan.sum() else np.zeros(1)
     sg = _f64(np.concatenate(S)) if nsing.sum() else np.zeros(1)
     tot = int(npan.sum()) * order
+    if device:
+        import torch
+        buf = torch.empty(2 * max(tot, 1), dtype=torch.float64, device=f"cuda:{ctx.device}")
+        ctx.check(lib().ytf_gl_rule_batch_device(ctx.h, len(sets), ptr(npan, _i), ptr(pa), ptr(pb), int(order),
+                                                 ptr(nsing, _i), ptr(sg), buf.data_ptr(), buf.data_ptr() + 8 * max(tot, 1)))
+        sizes = (npan.astype(np.int64) * order).tolist()
+        return list(zip(torch.split(buf[:tot], sizes), torch.split(buf[max(tot, 1):max(tot, 1) + tot], sizes)))
     nodes, wts = np.zeros(max(tot, 1)), np.zeros(max(tot, 1))
     ctx.check(lib().ytf_gl_rule_batch(ctx.h, len(sets), ptr(npan, _i), ptr(pa), ptr(pb), int(order), ptr(nsing, _i),
                                       ptr(sg), ptr(nodes), ptr(wts)))

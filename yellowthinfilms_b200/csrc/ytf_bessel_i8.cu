@@ -523,7 +523,7 @@ cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s) {
 // e = 3 i + o holds item i's order-o parameters; its J_n images share item i's node slicing
 // (bp[3 i] gives the layout), so one Bessel evaluation per (ρ, k) serves the three orders.
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_aimg_bessel3_group(const BesselI8* __restrict__ bp, const long* __restrict__ first,
+__global__ void __launch_bounds__(256, 5) k_aimg_bessel3_group(const BesselI8* __restrict__ bp, const long* __restrict__ first,
                                                           int ni) {
   const int i = group_entry(first, ni, blockIdx.x);
   const BesselI8& p = bp[3 * i];

@@ -83,6 +83,10 @@ struct ytf_cache {
   double omega = 0, d_src = 0;
   std::vector<double> kr, wr, phi, wphi, d_layer;
   std::vector<double> kri, wri;  // imaginary parts of 1D nodes/weights on a deformed contour (else empty)
+  // 1D nodes handed over in device memory (ytf_transfer_desc.nodes_on_device): kr/wr stay
+  // empty and the build copies them device to device from these (valid during the build call)
+  const double* src_kr = nullptr;
+  const double* src_wr = nullptr;
   void* block = nullptr;  // one device allocation for every array below
   size_t block_bytes = 0;
   double *d_kr = nullptr, *d_wr = nullptr, *d_phi = nullptr, *d_wphi = nullptr;
@@ -173,6 +177,9 @@ void* ws_get(ytf_ctx* ctx, const char* name_, size_t bytes, cudaError_t* e) {
   auto it = ctx->ws.find(name);
   if (it != ctx->ws.end() && it->second.second >= bytes) return it->second.first;
   if (it != ctx->ws.end()) {
+    // a buffer that has to grow grows by half again at least, so that calls of slowly
+    // rising size do not each pay a device synchronisation and a cudaMalloc
+    bytes = std::max(bytes, it->second.second + it->second.second / 2);
     cudaStreamSynchronize(ctx->stream);
     cudaFree(it->second.first);
     ctx->ws.erase(it);
@@ -267,7 +274,7 @@ int alloc_cache(ytf_ctx* ctx, ytf_cache* c, bool upload_nodes = true) {
     off += (bytes + 255) & ~size_t(255);
     return o;
   };
-  size_t o_kr = take(8 * c->kr.size()), o_wr = take(8 * c->wr.size()), o_phi = take(8 * std::max<size_t>(1, c->phi.size())),
+  size_t o_kr = take(8 * (size_t)c->Nk), o_wr = take(8 * (size_t)c->Nk), o_phi = take(8 * std::max<size_t>(1, c->phi.size())),
          o_wphi = take(8 * std::max<size_t>(1, c->wphi.size()));
   size_t o_kri = take(8 * std::max<size_t>(1, c->kri.size())), o_wri = take(8 * std::max<size_t>(1, c->wri.size()));
   size_t o_status = take(n), o_valid = take(n), o_tvalid = take((size_t)n * c->nobs);
@@ -294,8 +301,13 @@ int alloc_cache(ytf_ctx* ctx, ytf_cache* c, bool upload_nodes = true) {
   (void)o_status;
   int rc;
   if (!upload_nodes) return YTF_OK;
-  if ((rc = upload(ctx, c->d_kr, c->kr.data(), 8 * c->kr.size()))) return rc;
-  if ((rc = upload(ctx, c->d_wr, c->wr.data(), 8 * c->wr.size()))) return rc;
+  if (c->src_kr) {
+    CK(cudaMemcpyAsync(c->d_kr, c->src_kr, 8 * (size_t)c->Nk, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(c->d_wr, c->src_wr, 8 * (size_t)c->Nk, cudaMemcpyDeviceToDevice, ctx->stream));
+  } else {
+    if ((rc = upload(ctx, c->d_kr, c->kr.data(), 8 * c->kr.size()))) return rc;
+    if ((rc = upload(ctx, c->d_wr, c->wr.data(), 8 * c->wr.size()))) return rc;
+  }
   if (!c->kri.empty()) {
     if ((rc = upload(ctx, c->d_kri, c->kri.data(), 8 * c->kri.size()))) return rc;
     if ((rc = upload(ctx, c->d_wri, c->wri.data(), 8 * c->wri.size()))) return rc;
@@ -572,7 +584,7 @@ namespace {
 int prepare_cache(ytf_ctx* ctx, const ytf_stack* st, bool is2d, double omega, int source_layer, int nk,
                   const double* k_nodes, const double* k_weights, int nphi, const double* phi_nodes,
                   const double* phi_weights, int nobs, const int* obs_layers, int check_symmetry, int rotation,
-                  bool upload_nodes, ytf_cache** out, bool* use_rot) {
+                  bool upload_nodes, ytf_cache** out, bool* use_rot, bool nodes_dev = false) {
   *out = nullptr;
   *use_rot = false;
   const char* fn = is2d ? "build_cavity_transfer_2d" : "build_cavity_transfer_1d";
@@ -622,8 +634,13 @@ int prepare_cache(ytf_ctx* ctx, const ytf_stack* st, bool is2d, double omega, in
   c->Nk = nk;
   c->Np = is2d ? nphi : 1;
   c->n = is2d ? (long)nk * nphi : nk;
-  c->kr.assign(k_nodes, k_nodes + nk);
-  c->wr.assign(k_weights, k_weights + nk);
+  if (nodes_dev) {
+    c->src_kr = k_nodes;
+    c->src_wr = k_weights;
+  } else {
+    c->kr.assign(k_nodes, k_nodes + nk);
+    c->wr.assign(k_weights, k_weights + nk);
+  }
   if (is2d) {
     c->phi.assign(phi_nodes, phi_nodes + nphi);
     c->wphi.assign(phi_weights, phi_weights + nphi);
@@ -1141,9 +1158,13 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
   for (int i = 0; i < nb; ++i) {
     bool r = false;
     const bool is2d = d[i].nphi > 0 || d[i].is2d;
-    int rc = prepare_cache(ctx, d[i].stack, is2d, d[i].omega, d[i].source_layer, d[i].nk, d[i].k_nodes, d[i].k_weights,
-                           d[i].nphi, d[i].phi_nodes, d[i].phi_weights, d[i].nobs, d[i].obs_layers,
-                           d[i].check_symmetry, d[i].rotation, false, &cs[i], &r);
+    int rc = YTF_OK;
+    if (is2d && d[i].nodes_on_device)
+      rc = fail(ctx, YTF_ERR_ARG, "build_cavity_transfer_2d: nodes_on_device applies to 1D items only");
+    if (!rc)
+      rc = prepare_cache(ctx, d[i].stack, is2d, d[i].omega, d[i].source_layer, d[i].nk, d[i].k_nodes, d[i].k_weights,
+                         d[i].nphi, d[i].phi_nodes, d[i].phi_weights, d[i].nobs, d[i].obs_layers,
+                         d[i].check_symmetry, d[i].rotation, false, &cs[i], &r, d[i].nodes_on_device != 0);
     if (rc) {
       std::string m = ctx->err;
       abort_all(rc);
@@ -1189,6 +1210,12 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
       if ((rc = put(c->d_kr, c->kr)) || (rc = put(c->d_wr, c->wr)) || (rc = put(c->d_phi, c->phi)) ||
           (rc = put(c->d_wphi, c->wphi)))
         return abort_all(rc);
+      if (c->src_kr && c->Nk > 0) {  // device-resident nodes: device to device, on the same stream
+        cudaError_t e = cudaMemcpyAsync(c->d_kr, c->src_kr, 8 * (size_t)c->Nk, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(c->d_wr, c->src_wr, 8 * (size_t)c->Nk, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e != cudaSuccess) return abort_all(fail(ctx, YTF_ERR_CUDA, cudaGetErrorString(e)));
+      }
     }
     h += ((8 * k + 63) / 64) * 64;
   }
@@ -2186,8 +2213,25 @@ int ytf_gl_rule(ytf_ctx* ctx, int npanels, const double* pa, const double* pb, i
   return YTF_OK;
 }
 
+static int gl_rule_batch_impl(ytf_ctx* ctx, int nsets, const int* npanels, const double* pa, const double* pb,
+                              int order, const int* nsing, const double* singular, double* nodes, double* weights,
+                              bool out_dev);
+
 int ytf_gl_rule_batch(ytf_ctx* ctx, int nsets, const int* npanels, const double* pa, const double* pb, int order,
                       const int* nsing, const double* singular, double* nodes, double* weights) {
+  return gl_rule_batch_impl(ctx, nsets, npanels, pa, pb, order, nsing, singular, nodes, weights, false);
+}
+
+int ytf_gl_rule_batch_device(ytf_ctx* ctx, int nsets, const int* npanels, const double* pa, const double* pb, int order,
+                             const int* nsing, const double* singular, double* d_nodes, double* d_weights) {
+  return gl_rule_batch_impl(ctx, nsets, npanels, pa, pb, order, nsing, singular, d_nodes, d_weights, true);
+}
+
+}  // extern "C"
+
+static int gl_rule_batch_impl(ytf_ctx* ctx, int nsets, const int* npanels, const double* pa, const double* pb,
+                              int order, const int* nsing, const double* singular, double* nodes, double* weights,
+                              bool out_dev) {
   if (!ctx || nsets < 0 || order < 1 || (nsets > 0 && (!npanels || !nsing))) return YTF_ERR_ARG;
   size_t np = 0, ns = 0;
   for (int j = 0; j < nsets; ++j) {
@@ -2213,21 +2257,21 @@ int ytf_gl_rule_batch(ytf_ctx* ctx, int nsets, const int* npanels, const double*
     s0 += nsing[j];
   }
   const size_t tot = np * order;
-  WS(buf, double, "glb_buf", 2 * np + 2 * (size_t)order + 2 * tot);
+  WS(buf, double, "glb_buf", 2 * np + 2 * (size_t)order + (out_dev ? 0 : 2 * tot));
   WS(dside, int, "glb_side", np);
-  double *da = buf, *db = buf + np, *dxi = buf + 2 * np, *dwx = dxi + order, *dn = dwx + order, *dw = dn + tot;
+  double *da = buf, *db = buf + np, *dxi = buf + 2 * np, *dwx = dxi + order;
+  double *dn = out_dev ? nodes : dwx + order, *dw = out_dev ? weights : dn + tot;
   int rc;
   if ((rc = upload(ctx, da, pa, 8 * np)) || (rc = upload(ctx, db, pb, 8 * np)) || (rc = upload(ctx, dxi, xi.data(), 8 * (size_t)order)) ||
       (rc = upload(ctx, dwx, wx.data(), 8 * (size_t)order)) || (rc = upload(ctx, dside, side.data(), 4 * np)))
     return rc;
   CK(LAUNCH("k_gl_nodes", launch_gl_nodes((int)np, da, db, dside, dxi, dwx, order, dn, dw, ctx->stream)));
+  if (out_dev) return YTF_OK;  // stream-ordered: later work on the context's stream sees the rule
   CK(cudaMemcpyAsync(nodes, dn, 8 * tot, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(weights, dw, 8 * tot, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return YTF_OK;
 }
-
-}  // extern "C"
 
 // =====================================================================================
 // Uneven-batch plans (no counterpart in the reference; the contract is in ytf.h). Creation
@@ -2429,6 +2473,8 @@ int plan_build(ytf_plan* P) {
     const ytf_green_desc& g = P->gr[i];
     const bool is2d = d.nphi > 0 || d.is2d;
     bool rot = false;
+    if (d.nodes_on_device)
+      return plan_fail(ctx, fail(ctx, YTF_ERR_ARG, "ytf_plan_create: plans take host node arrays (nodes_on_device = 0)"), i);
     int rc = prepare_cache(ctx, d.stack, is2d, d.omega, d.source_layer, d.nk, d.k_nodes, d.k_weights, d.nphi,
                            d.phi_nodes, d.phi_weights, d.nobs, d.obs_layers, d.check_symmetry, YTF_ROT_OFF, false,
                            &P->cs[i], &rot);

@@ -203,12 +203,14 @@ def propose_poles(net, stack, k0, n_k=2048):
 
 def _windows(cand, n_local):
     """The log windows (±6 max(Γ/q, 3e-3), n_local points) around the candidates: wide enough
-    for the network's position error, fine enough to resolve the pole's width."""
-    wins = []
-    for q, G in cand:
-        w = max(G / q, 3e-3)
-        wins.append(q * np.exp(np.linspace(-6 * w, 6 * w, n_local)))
-    return wins
+    for the network's position error, fine enough to resolve the pole's width. An array
+    [len(cand), n_local]."""
+    if not len(cand):
+        return np.zeros((0, n_local))
+    c = np.asarray(cand, np.float64).reshape(-1, 2)
+    w = np.maximum(c[:, 1] / c[:, 0], 3e-3)
+    t = np.linspace(-6.0, 6.0, n_local)
+    return c[:, :1] * np.exp(w[:, None] * t[None, :])
 
 
 def refine_poles(stack, k0, source_layer, cand, n_local=129, ctx=None):
@@ -218,38 +220,51 @@ def refine_poles(stack, k0, source_layer, cand, n_local=129, ctx=None):
     if not cand:
         return []
     wins = _windows(cand, n_local)
-    R = api.cavity_response(stack, k0, source_layer, np.concatenate(wins), ctx=ctx)
+    R = api.cavity_response(stack, k0, source_layer, wins.reshape(-1), ctx=ctx)
     return _poles_from_windows(wins, R, n_local)
 
 
 def refine_poles_batch(items, n_local=129, ctx=None):
     """refine_poles for many (stack, k0, source_layer, cand) items: every window of every
-    item in ONE device call (ytf_cavity_response_batch). Returns the poles per item."""
+    item in ONE device call (ytf_cavity_response_batch) and the peaks of all windows in one
+    host call. Returns the poles per item."""
     wins = [_windows(c, n_local) for (_, _, _, c) in items]
-    idx = [i for i, w in enumerate(wins) if w]
-    Rs = api.cavity_response_batch([(items[i][0], items[i][1], items[i][2], np.concatenate(wins[i])) for i in idx],
-                                   ctx=ctx)
+    idx = [i for i, w in enumerate(wins) if len(w)]
     out = [[] for _ in items]
-    for i, R in zip(idx, Rs):
-        out[i] = _poles_from_windows(wins[i], R, n_local)
+    if not idx:
+        return out
+    Rs = api.cavity_response_batch([(items[i][0], items[i][1], items[i][2], wins[i].reshape(-1)) for i in idx], ctx=ctx)
+    K = np.concatenate([wins[i] for i in idx])
+    Y = np.log(np.maximum(np.concatenate([np.asarray(R, np.float64).reshape(-1, n_local) for R in Rs]), 1e-12))
+    pk = api.peaks_batch(K, Y)
+    w0 = 0
+    for i in idx:
+        nw = len(wins[i])
+        out[i] = _merge_peaks(pk[w0:w0 + nw])
+        w0 += nw
     return out
+
+
+def _merge_peaks(per_window):
+    """The peaks of an item's windows, sorted and merged (windows of neighbouring candidates
+    may find the same pole)."""
+    found = sorted(p for pk in per_window for p in pk)
+    merged = []
+    for q, G in found:
+        if merged and abs(q - merged[-1][0]) <= 1e-6 * q:
+            continue
+        merged.append((q, G))
+    return merged
 
 
 def _poles_from_windows(wins, R, n_local):
     """Every peak of the sampled response in each window (the peak rule of peaks(), run for
     all windows in one host call, api.peaks_batch), merged across windows."""
-    if not wins:
+    if not len(wins):
         return []
-    K = np.stack(wins)
-    Y = np.log(np.maximum(np.asarray(R, np.float64)[:len(wins) * n_local].reshape(len(wins), n_local), 1e-12))
-    out = [p for pk in api.peaks_batch(K, Y) for p in pk]
-    out.sort()
-    merged = []
-    for q, G in out:  # windows of neighbouring candidates may find the same pole
-        if merged and abs(q - merged[-1][0]) <= 1e-6 * q:
-            continue
-        merged.append((q, G))
-    return merged
+    K = np.asarray(wins).reshape(-1, n_local)
+    Y = np.log(np.maximum(np.asarray(R, np.float64)[:len(K) * n_local].reshape(len(K), n_local), 1e-12))
+    return _merge_peaks(api.peaks_batch(K, Y))
 
 
 def halved(stack, omega, panels, order, ctx=None):
@@ -354,8 +369,14 @@ def _agree(pairs, rtol):
 
 
 def _sing(P):
-    st = P["layers"]
-    return sorted(set(api.layer_light_lines(st[0], P["k0"])) | set(api.layer_light_lines(st[-1], P["k0"])))
+    """The half-space light lines of problem P (the rule's u² points), kept in P["singular"]
+    after the first call."""
+    s = P.get("singular")
+    if s is None:
+        st = P["layers"]
+        s = sorted(set(api.layer_light_lines(st[0], P["k0"])) | set(api.layer_light_lines(st[-1], P["k0"])))
+        P["singular"] = s
+    return s
 
 
 def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, ctx, out, device=False, solved=None):
@@ -372,7 +393,7 @@ def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, c
         if not open_:
             break
         p2s = [api.halve_panels(np.asarray(panels[i], np.float64).reshape(-1, 2)) for i in open_]
-        r2s = api.gl_rule_batch([(p2, sing[i]) for p2, i in zip(p2s, open_)], order, ctx=ctx)
+        r2s = api.gl_rule_batch([(p2, sing[i]) for p2, i in zip(p2s, open_)], order, ctx=ctx, device=device)
         halv = {i: (p2, r2) for i, p2, r2 in zip(open_, p2s, r2s)}
         if solved is not None:
             for i in open_:
@@ -403,11 +424,12 @@ def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, c
 def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, device=False, solved=None):
     """The plain fixed rule (no pole knowledge: light-line breaks, u² substitution) of every
     problem, halved until two levels agree. Returns [(G, k, w, halvings, converged)]; with
-    ``device`` every G (and the acceptance check) stays in device memory; ``solved`` as
-    _refine_levels."""
+    ``device`` every G (and the acceptance check) stays in device memory, and so do the
+    rules (k, w as float64 CUDA tensors; a fallback rule of the scanned grid stays numpy);
+    ``solved`` as _refine_levels."""
     panels = [api.rule_panels(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"], rho_max=P["rho_max"],
                               scan=False, order=order, ctx=ctx) for P in problems]
-    rules = api.gl_rule_batch([(p, _sing(P)) for p, P in zip(panels, problems)], order, ctx=ctx)
+    rules = api.gl_rule_batch([(p, _sing(P)) for p, P in zip(panels, problems)], order, ctx=ctx, device=device)
     out = [None] * len(problems)
     _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device,
                    solved)
@@ -433,7 +455,7 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     panels = [api.rule_panels(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"], rho_max=P["rho_max"],
                               order=order, rtol=rtol if build_rtol is None else build_rtol, poles=poles, ctx=ctx)
               for P, poles in zip(problems, polesets)]
-    rules = api.gl_rule_batch([(p, _sing(P)) for p, P in zip(panels, problems)], order, ctx=ctx)
+    rules = api.gl_rule_batch([(p, _sing(P)) for p, P in zip(panels, problems)], order, ctx=ctx, device=device)
     out = [None] * len(problems)
     # the proposals' own check (one level); a rejected proposal missed a pole: its rule comes
     # from one exact log scan of the response instead (batched over the rejected problems),
@@ -446,7 +468,8 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
             P = problems[i]
             panels[i] = api.rule_panels(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
                                         rho_max=P["rho_max"], order=order, rtol=rtol, poles=poles, ctx=ctx)
-        for i, r in zip(rej, api.gl_rule_batch([(panels[i], _sing(problems[i])) for i in rej], order, ctx=ctx)):
+        for i, r in zip(rej, api.gl_rule_batch([(panels[i], _sing(problems[i])) for i in rej], order, ctx=ctx,
+                                               device=device)):
             rules[i] = r
         sub = [None] * len(problems)
         _refine_levels(problems, rej, rules, panels, None, rtol, max_halvings, order, ctx, sub, device, solved)
