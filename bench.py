@@ -655,6 +655,39 @@ def run_reference_learned(args):
     return 0
 
 
+# FP64 operations per (ρ, k) pair of k_aimg_bessel3 (J_0 and J_1 by the CUDA math library, J_2
+# by series or recurrence, digits): ncu's DFMA x 2 + DMUL + DADD of one grouped launch divided
+# by its (ρ, k) slots, 3.285e9 / 18.19e6
+AIMG_FP64_PER_PAIR = 180.0
+
+
+def learned_roofline(name, prof, nodes_synth):
+    """Roofline entry of one kernel of the learned step's synthesis from its CUDA-event time in
+    the profiled step: the int8x3 contraction against the sustained bf16 tensor peak (its
+    algorithmic flops: 2 x radii x 1664 real coefficient columns per node synthesised), the
+    J_n image kernel against the nominal FP64 peak (its counted FP64 operations)."""
+    roof = {"kernel": name, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None,
+            "traffic": TRAFFIC.get(name)}
+    if name not in prof or not prof[name][1]:
+        return roof
+    t_k, nl = prof[name][0] * 1e-3, prof[name][1]
+    peaks = measured_peaks()
+    if name in ("k_gemm_i8_img", "k_bessel_i8"):
+        flops = 2.0 * N_RHO * (26 * N_ZOBS) * nodes_synth  # 13 complex coefficient columns per height, 3 orders
+        peak, src = peaks["bf16_sustained"]
+        roof.update(bound="tensor", achieved=flops / t_k / 1e12, peak=peak, unit="TFLOP/s",
+                    frac=flops / t_k / 1e12 / peak, peak_source=src, launches=nl,
+                    work=f"2 x {N_RHO} radii x 1664 real coefficient columns x nodes synthesised "
+                         f"({int(nodes_synth)} over the chunk's syntheses) = {flops:.3e} flop in {nl} launches")
+    elif name == "k_aimg_bessel3":
+        ops = AIMG_FP64_PER_PAIR * N_RHO * nodes_synth
+        roof.update(bound="fp64", achieved=ops / t_k / 1e12, peak=FP64_NOMINAL, unit="TFLOP/s",
+                    frac=ops / t_k / 1e12 / FP64_NOMINAL, peak_source="nominal FP64; no measured FP64 peak",
+                    launches=nl, work=f"{AIMG_FP64_PER_PAIR:.0f} FP64 ops (ncu count) x {N_RHO} radii x "
+                                      f"{int(nodes_synth)} nodes synthesised = {ops:.3e} in {nl} launches")
+    return roof
+
+
 def run_learned(args):
     """Learned adaptive quadrature vs the plain fixed rule. The node-placement MLP is trained
     on 1e7 solver samples (timed separately); then every step takes one chunk of 256 held-out
@@ -707,12 +740,26 @@ def run_learned(args):
     mine = chunks[rank::world] or chunks[:1]
     dev_stacks = {}
 
-    def problems(idx):
-        out = []
-        for i in idx:
-            if i not in dev_stacks:
-                dev_stacks[i] = api.Stack(stacks[i][0], ctx)
-            out.append(learned_problem(stacks[i][0], stacks[i][1], dev_stacks[i], prec))
+    # every step runs each method as two concurrent shares of the chunk (alternate stacks), one
+    # host thread, libytf context and CUDA stream each (learned.concurrent_shares), so that one
+    # share's host steps overlap the other's device work; the network's forward for the whole
+    # chunk runs first, on the main stream
+    ctx2 = api.Context(local)
+    stream2 = torch.cuda.Stream()
+    ctx2.set_stream(stream2.cuda_stream)
+    ctxs, streams = [ctx, ctx2], [stream, stream2]
+
+    def stack_of(i, c):
+        if (i, c) not in dev_stacks:
+            dev_stacks[(i, c)] = api.Stack(stacks[i][0], ctxs[c])
+        return dev_stacks[(i, c)]
+
+    def problems(idx, c=0):
+        return [learned_problem(stacks[i][0], stacks[i][1], stack_of(i, c), prec) for i in idx]
+
+    def interleave(a, b):
+        out = [None] * (len(a) + len(b))
+        out[0::2], out[1::2] = a, b
         return out
 
     G_host = torch.empty((CHUNK, ENTRIES_PER_STACK), dtype=torch.complex128, pin_memory=True)
@@ -724,20 +771,34 @@ def run_learned(args):
 
     def step(s, timed):
         idx = mine[s % len(mine)]
-        P = problems(idx)
-        sl, sp = [0] * len(P), [0] * len(P)
+        Pa, Pb = problems(idx[0::2], 0), problems(idx[1::2], 1)
+        P = interleave(Pa, Pb)
+        sla, slb, spa, spb = [0] * len(Pa), [0] * len(Pb), [0] * len(Pa), [0] * len(Pb)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         torch.cuda.synchronize()
         with torch.cuda.stream(stream):
             ev[0].record(stream)
-            outl = L.learned_rules_batch(net, P, ctx=ctx, device=True, n_scan=N_SCAN, solved=sl)
+            stream2.wait_stream(stream)
+            pred = L.predict_batch(net, [(q["layers"], q["k0"]) for q in Pa + Pb], N_SCAN)
+            na = len(Pa) * N_SCAN
+            outa, outb = L.concurrent_shares(
+                lambda sh, c: L.learned_rules_batch(net, sh[0], ctx=c, device=True, n_scan=N_SCAN, solved=sh[1],
+                                                    pred=sh[2]),
+                [(Pa, sla, pred[:na]), (Pb, slb, pred[na:])], ctxs, streams)
+            stream.wait_stream(stream2)
             ev[1].record(stream)
+            outl = interleave(outa, outb)
             for j, o in enumerate(outl):
                 G_host[j].copy_(o[0].permute(4, 3, 2, 1, 0).reshape(-1), non_blocking=True)
             ev[2].record(stream)
-            outp = L.plain_rules_batch(P, ctx=ctx, device=True, solved=sp)
+            stream2.wait_stream(stream)
+            outa, outb = L.concurrent_shares(lambda sh, c: L.plain_rules_batch(sh[0], ctx=c, device=True, solved=sh[1]),
+                                             [(Pa, spa), (Pb, spb)], ctxs, streams)
+            stream.wait_stream(stream2)
             ev[3].record(stream)
+            outp = interleave(outa, outb)
         torch.cuda.synchronize()
+        sl, sp = interleave(sla, slb), interleave(spa, spb)
         if not timed:
             return
         rec["t_l"].append(ev[0].elapsed_time(ev[1]) * 1e-3)
@@ -789,7 +850,7 @@ def run_learned(args):
     if not args.no_check:
         for c0 in range(0, len(checked), 32):
             part = checked[c0:c0 + 32]
-            P = [learned_problem(stacks[i][0], stacks[i][1], dev_stacks[i], "fp64") for i in part]
+            P = [learned_problem(stacks[i][0], stacks[i][1], stack_of(i, 0), "fp64") for i in part]
             rules, panels = [], []
             for Pi in P:
                 kr, wr, ir = api.point_kx_grid(Pi["stack"], Pi["k0"], 1, h_min=Pi["h_min"], rho_max=Pi["rho_max"],
@@ -814,20 +875,12 @@ def run_learned(args):
                "sample": "2 held-out stacks, each whole: the reference's scanned fixed rule, the 1D cache and "
                          "closed_form_G (oracle, all host threads)"}
 
-    # roofline of the dominant kernel of the profiled pass
+    # roofline of the dominant kernel of the profiled pass, and of the tensor-core contraction
     top = max(prof.items(), key=lambda kv: kv[1][0])[0] if prof else None
-    peaks = measured_peaks()
-    roof = {"kernel": top, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None,
-            "traffic": TRAFFIC.get(top)}
-    flops = 2.0 * N_RHO * (26 * N_ZOBS) * float(np.sum(sl))  # 13 complex coefficient columns per height, 3 orders
-    if top == "k_bessel_i8":
-        t_k = prof[top][0] * 1e-3
-        peak, src = peaks["bf16_sustained"]
-        roof.update(bound="tensor", achieved=flops / t_k / 1e12, peak=peak, unit="TFLOP/s",
-                    frac=flops / t_k / 1e12 / peak, peak_source=src, launches=prof[top][1],
-                    work=f"2 x {N_RHO} radii x 1664 real coefficient columns x nodes synthesised "
-                         f"({int(np.sum(sl))} over the chunk's syntheses) = {flops:.3e} flop in "
-                         f"{prof[top][1]} launches")
+    nodes_synth = float(np.sum(sl))
+    roof = learned_roofline(top, prof, nodes_synth)
+    if top != "k_gemm_i8_img" and "k_gemm_i8_img" in prof:
+        roof["contraction"] = learned_roofline("k_gemm_i8_img", prof, nodes_synth)
     nl, npl = np.asarray(rec["n_l"]), np.asarray(rec["n_p"])
     line = {"metric": LEARNED_METRIC, "value": value, "unit": "entries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_l / max(args.steps, 1), "higher_is_better": True,

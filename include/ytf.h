@@ -194,6 +194,18 @@ int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* stack, double omega, int
                          const ytf_grid_params* params, int npoles, const double* q, const double* G, long cap,
                          double* k, double* w, long* n, ytf_grid_info* info);
 
+/* The panels of ytf_nodes_1d (scan = 0: no pole knowledge, npoles[j] < 0) or of
+ * ytf_nodes_from_poles (npoles[j] >= 0 poles) for many 1D problems at once, on the host
+ * threads: problem j has stacks[j], omega[j], source_layer[j], prm[j] and its poles at
+ * q/G[sum of the earlier npoles (negative counted as 0) ...]. counts[j] receives its panel
+ * count and panels (pairs a, b) receive every problem's panels in problem order. *total is
+ * the sum; when it exceeds cap (panel pairs) nothing is written and YTF_ERR_ARG returned, so
+ * the caller can retry with a larger buffer. Each problem's panels equal its own call's
+ * (ytf_grid_info.panels). No counterpart in the reference (one grid per call). */
+int ytf_rule_panels_batch(ytf_ctx* ctx, int nprob, const ytf_stack* const* stacks, const double* omega,
+                          const int* source_layer, const ytf_grid_params* prm, const int* npoles, const double* q,
+                          const double* G, long cap, double* panels, long* counts, long* total);
+
 /* The peak rule of real_axis_poles (mod_KSpaceFeatures.jl:151-204) on sampled responses,
  * without its refinement rounds: for each of nwin log-uniform grids of npts points (ks,
  * logR: nwin x npts, row-major) the local maxima at or above max + log(floor_rel) that stand

@@ -258,3 +258,59 @@ def test_gl_rule_batch_equals_single_calls(L):
     for a, b in zip(api.build_cavity_transfer_batch(items), api.build_cavity_transfer_batch(items_d)):
         ea, eb = a.export(), b.export()
         assert all(np.array_equal(ea[x], eb[x]) for x in ea)
+
+
+def test_rule_panels_batch_equals_single_calls(L):
+    """ytf_rule_panels_batch (host threads): every problem's panels bit for bit as its own
+    rule_panels call, with and without given poles (none, some, empty lists), and a bad
+    problem named in the error."""
+    from yellowthinfilms_b200 import api
+    rng = np.random.default_rng(19)
+    probs = []
+    for j in range(40):
+        st, lam = L.film_stack(rng)
+        k0 = 2 * np.pi / lam
+        poles = None if j % 3 == 0 else ([] if j % 3 == 1 else [(k0 * rng.uniform(1.2, 30.0), k0 * 1e-3)])
+        probs.append(dict(stack=api.Stack(st), omega=k0, source_layer=1, h_min=20.0 + 5 * (j % 4),
+                          rho_max=5 * lam, poles=poles))
+    got = api.rule_panels_batch(probs)
+    for P, g in zip(probs, got):
+        ref = api.rule_panels(P["stack"], P["omega"], 1, h_min=P["h_min"], rho_max=P["rho_max"], poles=P["poles"])
+        assert np.array_equal(g, ref)
+    bad = list(probs)
+    bad[7] = dict(probs[7], h_min=-1.0)
+    with pytest.raises(api.YTFError, match="problem 7"):
+        api.rule_panels_batch(bad)
+
+
+def test_concurrent_shares_equal_serial_calls(L):
+    """learned.concurrent_shares: two shares of problems run at once on two host threads,
+    each with its own libytf context and CUDA stream, return bit for bit what the same shares
+    return one after the other (device rules, int8x3 grouped synthesis, device G)."""
+    import torch
+    from yellowthinfilms_b200 import api
+    net = _random_net(L, 11)
+    rng = np.random.default_rng(53)
+    ctxs = [api.Context(0), api.Context(0)]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    for c, s in zip(ctxs, streams):
+        c.set_stream(s.cuda_stream)
+    shares = [[], []]
+    for j in range(6):
+        st, lam = L.film_stack(rng)
+        k0 = 2 * np.pi / lam
+        shares[j % 2].append(dict(stack=api.Stack(st, ctxs[j % 2]), layers=st, k0=k0, source_layer=1, zsrc_local=20.0,
+                                  z=np.linspace(0.0, 200.0, 8), h_min=20.0, terms="scattered", precision="int8x3",
+                                  rho=np.exp(np.linspace(np.log(0.01 * lam), np.log(5 * lam), 24)), rho_max=5 * lam))
+    # the network's forward runs before the shares (one MLP object is not shared by threads)
+    preds = [L.predict_batch(net, [(P["layers"], P["k0"]) for P in sh], 512) for sh in shares]
+    for fn in (lambda j, c: L.plain_rules_batch(shares[j], ctx=c, device=True),
+               lambda j, c: L.learned_rules_batch(net, shares[j], ctx=c, device=True, n_scan=512, pred=preds[j])):
+        both = L.concurrent_shares(fn, [0, 1], ctxs, streams)
+        torch.cuda.synchronize()
+        for j in range(2):
+            with torch.cuda.stream(streams[j]):
+                one = fn(j, ctxs[j])
+            torch.cuda.synchronize()
+            for a, b in zip(both[j], one):
+                assert torch.equal(a[0], b[0]) and len(a[1]) == len(b[1]) and a[3:] == b[3:]

@@ -83,6 +83,9 @@ SIGNATURES = {
     "ytf_cavity_response_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), _d, _i,
                                                  ctypes.POINTER(ctypes.c_long), _d, ctypes.c_double, _d]),
     "ytf_gl_rule_batch": (ctypes.c_int, [_vp, ctypes.c_int, _i, _d, _d, ctypes.c_int, _i, _d, _d, _d]),
+    "ytf_rule_panels_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), _d, _i, ctypes.POINTER(GridParams),
+                                             _i, _d, _d, ctypes.c_long, _d, ctypes.POINTER(ctypes.c_long),
+                                             ctypes.POINTER(ctypes.c_long)]),
     "ytf_gl_rule_batch_device": (ctypes.c_int, [_vp, ctypes.c_int, _i, _d, _d, ctypes.c_int, _i, _d, _vp, _vp]),
     "ytf_layer_light_lines": (ctypes.c_int, [_d, _d, ctypes.c_double, ctypes.c_double, _d, _i]),
     "ytf_nodes_1d": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(GridParams), ctypes.c_long, _d,

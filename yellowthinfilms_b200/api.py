@@ -465,6 +465,46 @@ def rule_panels(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=25.
     return pan[:2 * info.n_panels].reshape(-1, 2).copy()
 
 
+def rule_panels_batch(problems, order=8, rtol=1e-6, target_decay=25.0, kr_cap=0.0, ctx: Optional[Context] = None):
+    """rule_panels for many problems in one call (ytf_rule_panels_batch, host threads): each
+    problem a dict with stack, omega, source_layer, h_min, rho_max and optionally poles
+    ([(q, Γ)]: grid_from_poles's panels; absent or None: point_kx_grid's without the scan).
+    Returns the [n, 2] panel arrays in order, each equal to its own rule_panels call."""
+    from ._native import GridParams
+    ctx = ctx or default_context()
+    n = len(problems)
+    if n == 0:
+        return []
+    sts = [_as_stack(P["stack"], ctx) for P in problems]
+    hs = (ctypes.c_void_p * n)(*[st.h for st in sts])
+    om = _f64([P["omega"] for P in problems])
+    src = np.ascontiguousarray([int(P["source_layer"]) for P in problems], np.int32)
+    prm = (GridParams * n)(*[GridParams(float(P["h_min"]), float(P.get("rho_max", 0.0)), float(target_decay),
+                                        float(kr_cap), 0, int(order), float(rtol)) for P in problems])
+    npl = np.ascontiguousarray([-1 if P.get("poles") is None else len(P["poles"]) for P in problems], np.int32)
+    allp = [p for P in problems if P.get("poles") is not None for p in P["poles"]]
+    q = _f64([p[0] for p in allp]) if allp else np.zeros(1)
+    g = _f64([p[1] for p in allp]) if allp else np.zeros(1)
+    counts = np.zeros(n, np.int64)
+    total = ctypes.c_long(0)
+    cap = max(16384, 4096 * n)
+    for _ in range(2):
+        buf = np.zeros(2 * cap)
+        rc = lib().ytf_rule_panels_batch(ctx.h, n, hs, ptr(om), ptr(src, _i), prm, ptr(npl, _i), ptr(q), ptr(g), cap,
+                                         ptr(buf), counts.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
+                                         ctypes.byref(total))
+        if rc == 0:
+            break
+        if total.value > cap:
+            cap = int(total.value)
+            continue
+        ctx.check(rc)
+    else:
+        ctx.check(rc)
+    cuts = np.cumsum(counts)[:-1]
+    return [a.reshape(-1, 2) for a in np.split(buf[:2 * int(total.value)], 2 * cuts)]
+
+
 class MLP:
     """The node-placement MLP on the device (ytf_mlp_*): widths sizes[0] -> ... -> 2, GELU
     between layers, BF16 weights with FP32 accumulation, trained by libytf's own forward,

@@ -551,19 +551,19 @@ __global__ void __launch_bounds__(BI_THREADS, 1) k_gemm_i8_img_group(const Besse
   gemm_i8_img_body(p, mt, (int)(rest % p.ntile_n), (int)(rest / p.ntile_n), smem);
 }
 
-cudaError_t launch_bessel_i8_group(const Synth1DGroup& g, cudaStream_t s) {
+cudaError_t launch_bessel_i8_group(const Synth1DGroup& g, int stage, cudaStream_t s) {
   if (g.ni <= 0) return cudaSuccess;
   const int ne = 3 * g.ni;
   cudaError_t e;
-  if (g.grid[2] > 0) {
+  if (stage == 0 && g.grid[2] > 0) {
     k_aimg_bessel3_group<<<(unsigned)g.grid[2], 256, 0, s>>>(g.bp, g.first_aimg, g.ni);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  if (g.grid[3] > 0) {
+  if (stage == 1 && g.grid[3] > 0) {
     k_bimg_real_group<<<(unsigned)g.grid[3], 256, 0, s>>>(g.bp, g.first_bimg, ne);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  if (g.grid[4] > 0) {
+  if (stage == 2 && g.grid[4] > 0) {
     const size_t sm = bessel_i8_smem(BI_ACC_STRIDE);
     if ((e = cudaFuncSetAttribute(k_gemm_i8_img_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) !=
         cudaSuccess)

@@ -8,6 +8,7 @@
 #include <map>
 #include <set>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -1002,6 +1003,89 @@ int ytf_nodes_from_poles(ytf_ctx* ctx, const ytf_stack* st, double omega, int so
                          ytf_grid_info* info) {
   if (npoles < 0 || (npoles > 0 && (!q || !G))) return YTF_ERR_ARG;
   return nodes_1d_impl(ctx, st, omega, source_layer, prm, npoles, q, G, cap, k, w, n, info);
+}
+
+int ytf_rule_panels_batch(ytf_ctx* ctx, int nprob, const ytf_stack* const* stacks, const double* omega,
+                          const int* source_layer, const ytf_grid_params* prm, const int* npoles, const double* q,
+                          const double* G, long cap, double* panels, long* counts, long* total) {
+  if (!ctx || nprob < 0 || (nprob > 0 && (!stacks || !omega || !source_layer || !prm || !npoles || !counts)) || !total)
+    return YTF_ERR_ARG;
+  // the checks of nodes_1d_impl, in problem order (the first failing problem is reported)
+  std::vector<long> qoff(nprob + 1, 0);
+  for (int j = 0; j < nprob; ++j) {
+    const std::string tag = " (problem " + std::to_string(j) + ")";
+    const ytf_stack* st = stacks[j];
+    if (!st) return fail(ctx, YTF_ERR_ARG, "point_kx_grid: stack is NULL" + tag);
+    if (st->ctx != ctx) return fail(ctx, YTF_ERR_STATE, "point_kx_grid: stack belongs to another context" + tag);
+    if (!(1 <= source_layer[j] && source_layer[j] < st->nL))
+      return fail(ctx, YTF_ERR_ARG, "point_kx_grid: source_layer=" + std::to_string(source_layer[j]) + " must be in 1:" +
+                                        std::to_string(st->nL - 1) + tag);
+    const ytf_grid_params& P = prm[j];
+    if (!(P.h_min > 0)) return fail(ctx, YTF_ERR_ARG, "point_kx_grid: h_min must be positive" + tag);
+    if (P.order < 1) return fail(ctx, YTF_ERR_ARG, "point_kx_grid: order must be ≥ 1" + tag);
+    if (!(P.rtol > 0 && P.rtol < 1)) return fail(ctx, YTF_ERR_ARG, "point_kx_grid: rtol must be in (0, 1)" + tag);
+    if (npoles[j] < 0 && P.scan) return fail(ctx, YTF_ERR_ARG, "ytf_rule_panels_batch: the pole scan runs per problem" + tag);
+    qoff[j + 1] = qoff[j] + std::max(npoles[j], 0);
+  }
+  if (qoff[nprob] > 0 && (!q || !G)) return YTF_ERR_ARG;
+  // features and panels per problem on the host threads (host arithmetic only: no scan)
+  std::vector<std::vector<std::pair<double, double>>> out(nprob);
+  std::vector<std::string> errs(nprob);
+  auto one = [&](int j) {
+    const ytf_stack* st = stacks[j];
+    const int N = st->nL;
+    std::vector<const double*> eps(N), mu(N);
+    for (int l = 0; l < N; ++l) { eps[l] = st->host[l].eps; mu[l] = st->host[l].mu; }
+    const ytf_grid_params& P = prm[j];
+    grid::Eval none = [](const std::vector<double>&, std::vector<double>& o) -> int { o.clear(); return 0; };
+    grid::Features F;
+    try {
+      if (grid::features_1d(eps, mu, omega[j], P.h_min, P.rho_max, P.target_decay, P.kr_cap, 1e5, false, 1e-3, 1.05,
+                            none, F)) {
+        errs[j] = "point_kx_grid: feature extraction failed";
+        return;
+      }
+      if (npoles[j] >= 0) {
+        F.poles.clear();
+        for (long i = qoff[j]; i < qoff[j + 1]; ++i)
+          if (q[i] > 0 && G[i] > 0 && q[i] < F.Kcut) F.poles.push_back({q[i], G[i], 0.0, 0.0});
+        F.cl = grid::clusters(F.poles, 0.0);
+      }
+      out[j] = grid::fixed_kr_panels(F, P.order, P.rtol, 0.5, 12, 0.05, 4.0, 4.0, 0.5);
+    } catch (std::exception& e) {
+      errs[j] = e.what();
+    }
+  };
+  const int nthr = (int)std::max(1u, std::min<unsigned>(std::min(std::thread::hardware_concurrency(), 32u),
+                                                        (unsigned)std::max(nprob, 1)));
+  if (nthr <= 1 || nprob < 8) {
+    for (int j = 0; j < nprob; ++j) one(j);
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthr; ++t)
+      pool.emplace_back([&, t]() {
+        for (int j = t; j < nprob; j += nthr) one(j);
+      });
+    for (auto& th : pool) th.join();
+  }
+  long tot = 0;
+  for (int j = 0; j < nprob; ++j) {
+    if (!errs[j].empty()) return fail(ctx, YTF_ERR_ARG, errs[j] + " (problem " + std::to_string(j) + ")");
+    counts[j] = (long)out[j].size();
+    tot += counts[j];
+  }
+  *total = tot;
+  if (tot > cap || (tot > 0 && !panels))
+    return fail(ctx, YTF_ERR_ARG, "ytf_rule_panels_batch: " + std::to_string(tot) + " panels exceed the capacity " +
+                                      std::to_string(cap));
+  long o = 0;
+  for (int j = 0; j < nprob; ++j)
+    for (auto& pr : out[j]) {
+      panels[2 * o] = pr.first;
+      panels[2 * o + 1] = pr.second;
+      ++o;
+    }
+  return YTF_OK;
 }
 
 int ytf_peaks_batch(int nwin, int npts, const double* ks, const double* logR, double prominence, double floor_rel,
@@ -2101,8 +2185,11 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
     G.first_bimg = df + 4 * (ni + 1);
     G.first_gemm = G.first_bimg + (3 * ni + 1);
     for (int k = 0; k < 6; ++k) G.grid[k] = D.grid[k];
-    CK(LAUNCH("k_coef1d", launch_reflect_coef_group(G, ctx->stream)));
-    CK(LAUNCH("k_bessel_i8", launch_bessel_i8_group(G, ctx->stream)));
+    CK(LAUNCH("k_reflect2d", launch_reflect_coef_group(G, 0, ctx->stream)));
+    CK(LAUNCH("k_coef1d", launch_reflect_coef_group(G, 1, ctx->stream)));
+    CK(LAUNCH("k_aimg_bessel3", launch_bessel_i8_group(G, 0, ctx->stream)));
+    CK(LAUNCH("k_bimg_real", launch_bessel_i8_group(G, 1, ctx->stream)));
+    CK(LAUNCH("k_gemm_i8_img", launch_bessel_i8_group(G, 2, ctx->stream)));
     CK(LAUNCH("k_assemble1d", launch_assemble1d_group(G, ctx->stream)));
     for (size_t j = groups[g].first; j < groups[g].second; ++j) {
       const int i = lay[j].item;

@@ -308,8 +308,10 @@ __device__ __forceinline__ int group_entry(const long* first, int ne, long b) {
   }
   return lo;
 }
-cudaError_t launch_reflect_coef_group(const Synth1DGroup& g, cudaStream_t s);  // amplitudes, FP32 columns
-cudaError_t launch_bessel_i8_group(const Synth1DGroup& g, cudaStream_t s);     // images (with slice maxima), contraction
+// stage 0: reflected amplitudes, 1: FP32 coefficient columns
+cudaError_t launch_reflect_coef_group(const Synth1DGroup& g, int stage, cudaStream_t s);
+// stage 0: J_n digit images, 1: coefficient digit images with their slice maxima, 2: contraction
+cudaError_t launch_bessel_i8_group(const Synth1DGroup& g, int stage, cudaStream_t s);
 cudaError_t launch_assemble1d_group(const Synth1DGroup& g, cudaStream_t s);    // slice sum + pixel assembly
 constexpr int COEF1D_ZB_GROUP = 8;   // heights per thread of the grouped coefficient kernel
 

@@ -1311,12 +1311,10 @@ __global__ void __launch_bounds__(128, 3) k_coef1d_group(const Synth1DItem* __re
   }
 }
 
-cudaError_t launch_reflect_coef_group(const Synth1DGroup& g, cudaStream_t s) {
+cudaError_t launch_reflect_coef_group(const Synth1DGroup& g, int stage, cudaStream_t s) {
   if (g.ni <= 0) return cudaSuccess;
-  if (g.grid[0] > 0) k_reflect2d_group<<<(unsigned)g.grid[0], 128, 0, s>>>(g.it, g.first_reflect, g.ni);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  if (g.grid[1] > 0) k_coef1d_group<<<(unsigned)g.grid[1], 128, 0, s>>>(g.it, g.first_coef, g.ni);
+  if (stage == 0 && g.grid[0] > 0) k_reflect2d_group<<<(unsigned)g.grid[0], 128, 0, s>>>(g.it, g.first_reflect, g.ni);
+  if (stage == 1 && g.grid[1] > 0) k_coef1d_group<<<(unsigned)g.grid[1], 128, 0, s>>>(g.it, g.first_coef, g.ni);
   return cudaGetLastError();
 }
 

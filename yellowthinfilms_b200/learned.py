@@ -427,8 +427,8 @@ def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, de
     ``device`` every G (and the acceptance check) stays in device memory, and so do the
     rules (k, w as float64 CUDA tensors; a fallback rule of the scanned grid stays numpy);
     ``solved`` as _refine_levels."""
-    panels = [api.rule_panels(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"], rho_max=P["rho_max"],
-                              scan=False, order=order, ctx=ctx) for P in problems]
+    panels = api.rule_panels_batch([dict(stack=P["stack"], omega=P["k0"], source_layer=P["source_layer"],
+                                         h_min=P["h_min"], rho_max=P["rho_max"]) for P in problems], order=order, ctx=ctx)
     rules = api.gl_rule_batch([(p, _sing(P)) for p, P in zip(panels, problems)], order, ctx=ctx, device=device)
     out = [None] * len(problems)
     _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, max_halvings, order, ctx, out, device,
@@ -437,7 +437,7 @@ def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, de
 
 
 def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=None, device=False, build_rtol=None,
-                        n_scan=2048, solved=None):
+                        n_scan=2048, solved=None, pred=None):
     """learned_rule for every problem: the network over all problems' scan grids (features
     formed on the device), the exact window sampling of all problems in one device call,
     fixed_kρ_rule per problem, then the acceptance check; the rejected problems take the rule
@@ -445,16 +445,19 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     never converges falls back to the reference's scanned rule. Returns [(G, k, w, accepted, halvings)]; ``device`` as plain_rules_batch.
     ``build_rtol`` (default rtol): the tolerance the proposed rules are built for; the
     acceptance check always uses rtol. ``n_scan``: points of the log grid the network is
-    evaluated on per problem. ``solved`` as _refine_levels."""
+    evaluated on per problem. ``solved`` as _refine_levels. ``pred``: the network's outputs on
+    the problems' scan grids when already evaluated (predict_batch), else evaluated here."""
     n_k = n_scan
-    pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
+    if pred is None:
+        pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
     KS = np.stack([scan_grid(P["k0"], n_k) for P in problems])
     pk = api.peaks_batch(KS, pred[:, 0].reshape(len(problems), n_k) * LOG_SCALE, prominence=np.log(1.01))
     cands = [sorted(_score_candidates(KS[j], pred[j * n_k:(j + 1) * n_k, 1], pk[j])) for j in range(len(problems))]
     polesets = refine_poles_batch([(P["stack"], P["k0"], P["source_layer"], c) for P, c in zip(problems, cands)], ctx=ctx)
-    panels = [api.rule_panels(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"], rho_max=P["rho_max"],
-                              order=order, rtol=rtol if build_rtol is None else build_rtol, poles=poles, ctx=ctx)
-              for P, poles in zip(problems, polesets)]
+    panels = api.rule_panels_batch([dict(stack=P["stack"], omega=P["k0"], source_layer=P["source_layer"],
+                                         h_min=P["h_min"], rho_max=P["rho_max"], poles=poles)
+                                    for P, poles in zip(problems, polesets)],
+                                   order=order, rtol=rtol if build_rtol is None else build_rtol, ctx=ctx)
     rules = api.gl_rule_batch([(p, _sing(P)) for p, P in zip(panels, problems)], order, ctx=ctx, device=device)
     out = [None] * len(problems)
     # the proposals' own check (one level); a rejected proposal missed a pole: its rule comes
@@ -464,10 +467,11 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     rej = [i for i, r in enumerate(out) if not r[4]]
     if rej:
         scanned = exact_scan_poles_batch([problems[i] for i in rej], ctx=ctx)
-        for i, poles in zip(rej, scanned):
-            P = problems[i]
-            panels[i] = api.rule_panels(P["stack"], P["k0"], P["source_layer"], h_min=P["h_min"],
-                                        rho_max=P["rho_max"], order=order, rtol=rtol, poles=poles, ctx=ctx)
+        for i, pn in zip(rej, api.rule_panels_batch(
+                [dict(stack=problems[i]["stack"], omega=problems[i]["k0"], source_layer=problems[i]["source_layer"],
+                      h_min=problems[i]["h_min"], rho_max=problems[i]["rho_max"], poles=poles)
+                 for i, poles in zip(rej, scanned)], order=order, rtol=rtol, ctx=ctx)):
+            panels[i] = pn
         for i, r in zip(rej, api.gl_rule_batch([(panels[i], _sing(problems[i])) for i in rej], order, ctx=ctx,
                                                device=device)):
             rules[i] = r
@@ -491,6 +495,36 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
         for i, (k, w), g in zip(fall, fr, Gf):
             out[i] = (g, k, w, out[i][3], False)
     return [(g, k, w, conv and h == 0, h) for (g, k, w, h, conv) in out]
+
+
+def concurrent_shares(fn, shares, ctxs, streams):
+    """fn(share, ctx) for every share at once, one host thread per share, each with its own
+    libytf context and CUDA stream (the thread's current torch stream too): while one share
+    waits on the GPU (the library calls release the interpreter lock), another does its host
+    work, so the host steps of a method (peaks, panels, levels) overlap the device work of the
+    other shares. The problems of a share must use its context's Stack objects, and fn must not
+    share other stateful objects between threads (an MLP's forward: evaluate the network before,
+    learned_rules_batch(pred=...)). Returns the
+    results in share order; the first exception of any share is raised after all finish."""
+    import threading
+    import torch
+    out, err = [None] * len(shares), [None] * len(shares)
+
+    def work(j):
+        try:
+            with torch.cuda.stream(streams[j]):
+                out[j] = fn(shares[j], ctxs[j])
+        except BaseException as e:  # re-raised in the calling thread
+            err[j] = e
+    ths = [threading.Thread(target=work, args=(j,)) for j in range(len(shares))]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    for e in err:
+        if e is not None:
+            raise e
+    return out
 
 
 def exact_scan_poles_batch(problems, step=1e-3, n_local=129, ctx=None):
