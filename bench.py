@@ -890,6 +890,8 @@ def run_learned(args):
             "config": dict(LEARNED_CONFIG, precision=prec, steps_cover_stacks=rec["stacks"] * world,
                            held_out_stacks=n_test, train_samples=n_train * N_SCAN),
             "plain_entries_per_s": plain, "learned_vs_plain": t_p / t_l,
+            "step_ms": {"learned": [round(1e3 * x, 2) for x in rec["t_l"]],
+                        "plain": [round(1e3 * x, 2) for x in rec["t_p"]]},
             "gzz_entries_per_s": value / 9,
             "max_rel_err_vs_reference": max(err_l, err_p), "max_rel_err_learned": err_l, "max_rel_err_plain": err_p,
             "reference_checked_stacks": len(checked) * world, "max_rel_diff_learned_vs_plain": rec["mutual"],

@@ -1890,7 +1890,7 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
 
 // ------------------------------------------------------------------------------------
 // Grouped 1D int8x3 synthesis inside ytf_green_batch: the batch's 1D items of real nodes
-// (at most SYNTH1D_NODE_CHUNK nodes) in groups whose workspace stays within the context's
+// (at most SYNTH1D_GROUP_MAX_NODES nodes) in groups whose workspace stays within the context's
 // group bound (ytf_ctx_set_group_bytes, default 4 GiB); each group is six launches whatever
 // its item count (amplitudes, coefficient columns, J_n images, coefficient images with their
 // slice maxima, contraction, slice sum + assembly), with every item's blocks side by side in each
@@ -1899,6 +1899,9 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
 // (slices of about SYNTH1D_GROUP_SLICE nodes, whose fixed-point scales are per slice).
 // ------------------------------------------------------------------------------------
 constexpr long SYNTH1D_GROUP_SLICE = 4096;
+// largest item of the grouped path (about 14 KB of workspace per node at 64 heights, so an item
+// of this size is a group of its own of ~15 GB); larger rules take the per-item node passes
+constexpr long SYNTH1D_GROUP_MAX_NODES = 1L << 20;
 
 struct Group1DLayout {
   int item;
@@ -1961,7 +1964,7 @@ struct Group1DDesc {
 
 static bool group1d_eligible(const ytf_ctx* ctx, const ytf_green_desc& g) {
   const ytf_cache* c = g.cache;
-  return c && c->ctx == ctx && !c->is2d && !c->d_kri && c->n > 0 && c->n <= SYNTH1D_NODE_CHUNK &&
+  return c && c->ctx == ctx && !c->is2d && !c->d_kri && c->n > 0 && c->n <= SYNTH1D_GROUP_MAX_NODES &&
          g.precision == YTF_PREC_INT8X3 && g.out && g.nz > 0 && g.nx > 0 && g.ny > 0 && g.xs && g.ys && g.z_obs;
 }
 
