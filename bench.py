@@ -997,6 +997,69 @@ def run_bessel(args):
     return 0
 
 
+def run_synth(args):
+    """The grouped 1D int8x3 synthesis alone (ytf_green_batch): --stacks held-out stacks of the
+    learned workload (default 64) with their plain fixed rules (point_kx_grid without the
+    scan), G on the dipole problem's 256 radii x 64 heights (scattered term, device outputs),
+    all items in one batched call per step; --group-bytes bounds a group's workspace. Reports
+    entries/s, ns per node and the per-kernel CUDA-event split of a profiled step, and the
+    largest relative difference to the FP64 synthesis of the same items."""
+    import torch
+    from yellowthinfilms_b200 import api
+    from yellowthinfilms_b200 import learned as L
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    api._default_ctx = ctx
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    if args.group_bytes:
+        ctx.set_group_bytes(args.group_bytes)
+    n = args.stacks if args.stacks != N_TEST else 64
+    P = [learned_problem(st, lam, api.Stack(st, ctx), "int8x3") for st, lam in learned_stacks(n)]
+    panels = api.rule_panels_batch([dict(stack=q["stack"], omega=q["k0"], source_layer=1, h_min=q["h_min"],
+                                         rho_max=q["rho_max"]) for q in P], ctx=ctx)
+    rules = api.gl_rule_batch([(pn, L._sing(q)) for pn, q in zip(panels, P)], ORDER, ctx=ctx, device=True)
+    caches = api.build_cavity_transfer_batch([dict(stack=q["stack"], omega=q["k0"], source_layer=1, kx_nodes=k,
+                                                   wt_nodes=w, obs_layers=[1]) for q, (k, w) in zip(P, rules)], ctx=ctx)
+    nodes = int(sum(len(k) for k, _ in rules))
+    outs = [torch.empty(N_RHO * N_ZOBS * 9, dtype=torch.complex128, device="cuda") for _ in P]
+    items = [dict(cache=c, obs_layer=1, zsrc_local=q["zsrc_local"], z_obs=q["z"], xs=q["rho"], ys=[0.0],
+                  terms="scattered", precision="int8x3", out=o) for c, q, o in zip(caches, P, outs)]
+    for _ in range(args.warmup):
+        api.closed_form_G_batch(items)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            api.closed_form_G_batch(items)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    ctx.profile(True)
+    api.closed_form_G_batch(items)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    G8 = [o.clone() for o in outs]
+    api.closed_form_G_batch([dict(it, precision="fp64") for it in items])
+    err = max(float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) for a, b in zip(G8, outs))
+    entries = len(P) * ENTRIES_PER_STACK
+    roof = learned_roofline("k_gemm_i8_img", prof, nodes)
+    line = {"metric": METRIC, "value": entries / (ms * 1e-3), "unit": "entries/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": DTYPE["int8x3"], "data": "synthetic (seeded)",
+            "config": {"workload": f"grouped 1D int8x3 synthesis: {len(P)} held-out film stacks of the learned workload "
+                                   f"on their plain fixed rules ({nodes} nodes), {N_RHO} radii x {N_ZOBS} heights x 9 "
+                                   "components each, one batched call per step",
+                       "items": len(P), "nodes": nodes, "group_bytes": args.group_bytes or "default (4 GiB)"},
+            "ns_per_node": ms * 1e6 / nodes, "max_rel_err_vs_fp64": err, "roofline": roof, "clocks": clk.summary(),
+            "kernels_ms_per_step": {k: round(v[0], 4) for k, v in sorted(prof.items())},
+            "kernels_note": "per-kernel CUDA-event times of one separately profiled step"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_contour(args):
     """The config-1 path: vertical dipole 20 nm above the uniaxial film, 4096 nodes on the
     deformed contour (512 GL-8 panels, indentation 0.05 k0) to 20 k0, G at 256 radii
@@ -1056,7 +1119,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-check", action="store_true")
-    ap.add_argument("--workload", default="learned", choices=["learned", "gyro32", "uneven", "bessel", "contour"],
+    ap.add_argument("--group-bytes", type=int, default=0,
+                    help="synth workload: workspace bound of one synthesis group (0: the library default)")
+    ap.add_argument("--workload", default="learned", choices=["learned", "gyro32", "uneven", "bessel", "contour",
+                                                              "synth"],
                     help="learned: learned adaptive quadrature vs the plain fixed rule on 4096 held-out stacks "
                          "(default, the headline metric); gyro32: the 8-layer stack at 32 wavelengths; uneven: 1024 "
                          "uneven stacks; bessel: the 1D Bessel synthesis at 4096 radii x 65536 nodes x 256 heights; "
@@ -1090,6 +1156,8 @@ def main():
         return run_uneven(args)
     if args.workload == "learned":
         return run_learned(args)
+    if args.workload == "synth":
+        return run_synth(args)
     if args.workload == "bessel":
         return run_bessel(args)
     if args.workload == "contour":

@@ -4,7 +4,7 @@
 //   P_n[r][c] = Σ_k J_n(k_k ρ_r) C_n[c][k]
 // (C_n: the real and imaginary parts of the order's coefficient columns, k_coef1d). Both
 // operands are fixed point in three signed base-256 digits, as in the 2D lateral kernel:
-//   J: X = rint(8355000 J)            (|J_n| ≤ 1: one scale for every entry)
+//   J: X = rint(8355000 J / j_env(k_min ρ))   per (radius, node slice): |J_n| ≤ j_env
 //   C: Y = rint(8355000 C / max|C|)   per (node slice, column)
 // and the six digit products of weight ≥ 256² are summed exactly in INT32 in tensor memory.
 // Unlike the lateral kernel, both operands are prepared once per launch as the exact shared-
@@ -53,6 +53,35 @@ __device__ __forceinline__ double bessel_j012(int order, double x) {
     return s;
   }
   return (2.0 / x) * j1(x) - j0(x);
+}
+
+// |J_n(x)| <= j_env(x) = min(1, 0.9 / sqrt(x)) for n = 0, 1, 2 and x >= 0 (the suprema of
+// sqrt(x) |J_n(x)| are 0.798, 0.825, 0.868 for n = 0, 1, 2); non-increasing, so j_env(k_min ρ)
+// bounds J_n(k ρ) over a node slice whose smallest node is k_min. The J digits of a (radius,
+// slice) are fixed point relative to it, so far radii keep their 24 bits.
+__device__ __forceinline__ double j_env(double x) { return x > 0.81 ? 0.9 / sqrt(x) : 1.0; }
+
+// the smallest node of every slice: one block of 256 threads per slice (kmin[z])
+__device__ __forceinline__ void slice_kmin_body(const double* kr, long K, long kchunk, int z, double* kmin) {
+  __shared__ double red[256];
+  const long k0 = (long)z * kchunk, k1 = min(K, k0 + kchunk);
+  double m = INFINITY;
+  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) m = fmin(m, kr[k]);
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] = fmin(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) kmin[z] = isfinite(red[0]) ? red[0] : 0.0;
+}
+__global__ void __launch_bounds__(256) k_slice_kmin(const double* kr, long K, long kchunk, double* kmin) {
+  slice_kmin_body(kr, K, kchunk, blockIdx.x, kmin);
+}
+cudaError_t launch_slice_kmin(const double* kr, long K, long kchunk, int nchunk, double* kmin, cudaStream_t s) {
+  if (nchunk <= 0) return cudaSuccess;
+  k_slice_kmin<<<(unsigned)nchunk, 256, 0, s>>>(kr, K, kchunk, kmin);
+  return cudaGetLastError();
 }
 
 __device__ __forceinline__ void digits3b(int Y, uint32_t& d0, uint32_t& d1, uint32_t& d2) {
@@ -223,6 +252,7 @@ __global__ void k_aimg_bessel(BesselI8 p) {
   const int r = mt * BI_M + row;
   const bool rv = r < p.M;
   const double rho = rv ? p.rho[r] : 0.0;
+  const double sA = BI_SCALE / j_env(p.kmin[z] * rho);
   uint32_t w[3][4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -232,7 +262,7 @@ __global__ void k_aimg_bessel(BesselI8 p) {
       const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
       const double v = (rv && k < p.K) ? bessel_j012(p.order, p.kr[k] * rho) : 0.0;
       uint32_t d0, d1, d2;
-      digits3b(__double2int_rn(v * BI_SCALE), d0, d1, d2);
+      digits3b(__double2int_rn(v * sA), d0, d1, d2);
       b[0][h] = d0; b[1][h] = d1; b[2][h] = d2;
     }
 #pragma unroll
@@ -266,6 +296,7 @@ __device__ __forceinline__ void aimg_bessel3_body(const BesselI8& p, long t, uin
   const int r = mt * BI_M + row;
   const bool rv = r < p.M;
   const double rho = rv ? p.rho[r] : 0.0;
+  const double sA = BI_SCALE / j_env(p.kmin[z] * rho);
   const long g = wq / 4;
   const int q = (int)(wq % 4);
   uint32_t b[3][3][4];  // [order][plane][node]
@@ -291,7 +322,7 @@ __device__ __forceinline__ void aimg_bessel3_body(const BesselI8& p, long t, uin
 #pragma unroll
     for (int o = 0; o < 3; ++o) {
       uint32_t d0, d1, d2;
-      digits3b(__double2int_rn(v[o] * BI_SCALE), d0, d1, d2);
+      digits3b(__double2int_rn(v[o] * sA), d0, d1, d2);
       b[o][0][h] = d0; b[o][1][h] = d1; b[o][2][h] = d2;
     }
   }
@@ -431,6 +462,7 @@ __device__ __forceinline__ void gemm_i8_img_body(const BesselI8& p, int mt, int 
       const int q = warp & 3;
       const uint32_t lanebase = (uint32_t)(32 * q) << 16;
       const int r = mt * BI_M + 32 * q + lane;
+      const double eA = r < p.M ? j_env(p.kmin[z] * p.rho[r]) : 1.0;  // the row's J digit scale
       double* out = p.partial + (long)z * p.N * p.M;
       const unsigned long long* cmax = p.colmax + (long)z * p.N;
       for (int e0 = 0; e0 < p.Np; e0 += 8) {
@@ -449,7 +481,7 @@ __device__ __forceinline__ void gemm_i8_img_body(const BesselI8& p, int mt, int 
             double f;
             if (!isfinite(m)) f = __longlong_as_double(0x7ff8000000000000LL);
             else f = m > 0.0 ? 65536.0 / (BI_SCALE * col_scale(bits)) : 0.0;
-            out[(long)(c0 + cl) * p.M + r] = (double)v * f;
+            out[(long)(c0 + cl) * p.M + r] = (double)v * f * eA;
           }
         }
       }
@@ -492,7 +524,7 @@ __global__ void k_reduce_transpose(int M, int N, int nz, const double* __restric
 
 cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s) {
   if (p.M <= 0 || p.N <= 0 || p.K <= 0) return cudaSuccess;
-  if (p.kchunk % BI_NODES != 0 || p.kchunk > 16384 || p.Np % 16 != 0 || p.Np > BI_ACC_STRIDE || p.Np < p.ctile ||
+  if (!p.kmin || p.kchunk % BI_NODES != 0 || p.kchunk > 16384 || p.Np % 16 != 0 || p.Np > BI_ACC_STRIDE || p.Np < p.ctile ||
       (long)p.nchunk * p.kchunk < p.K)
     return cudaErrorInvalidValue;
   cudaError_t e;
@@ -531,6 +563,14 @@ __global__ void __launch_bounds__(256, 5) k_aimg_bessel3_group(const BesselI8* _
                     bp[3 * i + 2].Aimg);
 }
 
+// nchunk blocks per item: the slices' smallest nodes (bp[3 i].kmin, shared by the orders)
+__global__ void __launch_bounds__(256) k_slice_kmin_group(const BesselI8* __restrict__ bp,
+                                                        const long* __restrict__ first, int ni) {
+  const int i = group_entry(first, ni, blockIdx.x);
+  const BesselI8& p = bp[3 * i];
+  slice_kmin_body(p.kr, p.K, p.kchunk, (int)(blockIdx.x - first[i]), p.kmin);
+}
+
 // ntile_n x (Np / 8) x nchunk blocks per entry (bimg_slice_body)
 __global__ void __launch_bounds__(256) k_bimg_real_group(const BesselI8* __restrict__ bp, const long* __restrict__ first,
                                                        int ne) {
@@ -555,6 +595,10 @@ cudaError_t launch_bessel_i8_group(const Synth1DGroup& g, int stage, cudaStream_
   if (g.ni <= 0) return cudaSuccess;
   const int ne = 3 * g.ni;
   cudaError_t e;
+  if (stage == 0 && g.grid[6] > 0) {
+    k_slice_kmin_group<<<(unsigned)g.grid[6], 256, 0, s>>>(g.bp, g.first_kmin, g.ni);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if (stage == 0 && g.grid[2] > 0) {
     k_aimg_bessel3_group<<<(unsigned)g.grid[2], 256, 0, s>>>(g.bp, g.first_aimg, g.ni);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

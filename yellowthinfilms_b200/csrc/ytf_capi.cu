@@ -1593,6 +1593,8 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
       WS(A1i, uint8_t, "g_bi_a1", abytes);
       WS(A2i, uint8_t, "g_bi_a2", abytes);
       uint8_t* Aord[3] = {A0i, A1i, A2i};
+      WS(kminb, double, "g_bi_kmin", nchunk);
+      CK(LAUNCH("k_bessel_i8", launch_slice_kmin(sp.c.kr, nk, kchunk, nchunk, kminb, ctx->stream)));
       for (int o = 0; o < 3; ++o) {
         BesselI8 bp;
         std::memset(&bp, 0, sizeof(bp));
@@ -1609,6 +1611,7 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
         bp.kr = sp.c.kr; bp.rho = drho; bp.C = Cn8[o]; bp.ldc = nk;
         bp.Aimg = Aord[o]; bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
         bp.wait_limit = ctx->wait_limit;
+        bp.kmin = kminb;
         if (o == 0) CK(LAUNCH("k_bessel_i8", launch_bessel_i8_aimg3(bp, A0i, A1i, A2i, ctx->stream)));
         bp.aimg_ready = 1;
         CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pn8[o], ctx->stream)));
@@ -1913,6 +1916,7 @@ struct Group1DLayout {
   size_t off_amp, off_C, off_A[3], off_B[3], off_pt[3];
   size_t cm_off[3], cm_bytes;  // slice maxima, in the group's separate maxima block
   size_t off_G;  // device G of an item whose output is host memory (copied out after its group)
+  size_t off_kmin;  // [nchunk] smallest node of each slice
   size_t bytes;
 };
 
@@ -1944,6 +1948,7 @@ static Group1DLayout group1d_layout(int item, long nk, int nz, int nr, long npix
     L.off_pt[o] = take(sizeof(double) * (size_t)L.nchunk * L.N[o] * nr);
   }
   L.off_G = host_out ? take(sizeof(double2) * 9 * (size_t)npix * nz) : 0;
+  L.off_kmin = take(sizeof(double) * (size_t)L.nchunk);
   L.bytes = off;
   size_t cm = 0;
   for (int o = 0; o < 3; ++o) {
@@ -1958,7 +1963,7 @@ static Group1DLayout group1d_layout(int item, long nk, int nz, int nr, long npix
 struct Group1DDesc {
   size_t off_it, off_bp, off_first, bytes;
   int ni;
-  long grid[6];
+  long grid[7];
 
 };
 
@@ -2058,7 +2063,7 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
     D.off_bp = D.off_it + align256(sizeof(Synth1DItem) * ni);
     D.off_first = D.off_bp + align256(sizeof(BesselI8) * 3 * ni);
     D.bytes = align256(sizeof(Synth1DItem) * ni) + align256(sizeof(BesselI8) * 3 * ni) +
-              align256(sizeof(long) * (4 * (size_t)(ni + 1) + 2 * (size_t)(3 * ni + 1)));
+              align256(sizeof(long) * (5 * (size_t)(ni + 1) + 2 * (size_t)(3 * ni + 1)));
 
     desc_bytes += D.bytes;
   }
@@ -2103,9 +2108,10 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
     long* f_coef = f_ref + (ni + 1);
     long* f_aimg = f_coef + (ni + 1);
     long* f_asm = f_aimg + (ni + 1);
-    long* f_bimg = f_asm + (ni + 1);
+    long* f_kmin = f_asm + (ni + 1);
+    long* f_bimg = f_kmin + (ni + 1);
     long* f_gemm = f_bimg + (3 * ni + 1);
-    long nref = 0, ncoef = 0, naimg = 0, nasm = 0, nbimg = 0, ngemm = 0;
+    long nref = 0, ncoef = 0, naimg = 0, nasm = 0, nbimg = 0, ngemm = 0, nkmin = 0;
     for (int q = 0; q < ni; ++q) {
       const size_t j = groups[g].first + q;
       const Group1DLayout& L = lay[j];
@@ -2140,6 +2146,7 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
       f_coef[q] = ncoef; ncoef += nkb * ((L.nz + COEF1D_ZB_GROUP - 1) / COEF1D_ZB_GROUP);
       f_aimg[q] = naimg; naimg += ((long)L.ntm * 128 * L.nchunk * (L.kchunk / 4) + 255) / 256;
       f_asm[q] = nasm; nasm += ((long)d[i].nx * d[i].ny * L.nz + 127) / 128;
+      f_kmin[q] = nkmin; nkmin += L.nchunk;
       const size_t coff[3] = {0, 10 * (size_t)L.nz * L.ldc, 18 * (size_t)L.nz * L.ldc};
       for (int od = 0; od < 3; ++od) {
         BesselI8& bp = hbp[3 * q + od];
@@ -2159,16 +2166,17 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
         bp.err = err;
         bp.wait_limit = ctx->wait_limit;
         bp.aimg_ready = 1;
+        bp.kmin = (double*)(base + L.off_kmin);
         const int e = 3 * q + od;
         f_bimg[e] = nbimg;
         nbimg += (long)bp.ntile_n * (bp.Np / 8) * bp.nchunk;
         f_gemm[e] = ngemm; ngemm += (long)bp.ntile_m * bp.ntile_n * bp.nchunk;
       }
     }
-    f_ref[ni] = nref; f_coef[ni] = ncoef; f_aimg[ni] = naimg; f_asm[ni] = nasm;
+    f_ref[ni] = nref; f_coef[ni] = ncoef; f_aimg[ni] = naimg; f_asm[ni] = nasm; f_kmin[ni] = nkmin;
     f_bimg[3 * ni] = nbimg; f_gemm[3 * ni] = ngemm;
-    const long grid[6] = {nref, ncoef, naimg, nbimg, ngemm, nasm};
-    for (int k = 0; k < 6; ++k) D.grid[k] = grid[k];
+    const long grid[7] = {nref, ncoef, naimg, nbimg, ngemm, nasm, nkmin};
+    for (int k = 0; k < 7; ++k) D.grid[k] = grid[k];
   }
   CK(cudaMemcpyAsync(dc, h, total_bytes, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
@@ -2185,9 +2193,10 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
     G.first_coef = df + (ni + 1);
     G.first_aimg = df + 2 * (ni + 1);
     G.first_asm = df + 3 * (ni + 1);
-    G.first_bimg = df + 4 * (ni + 1);
+    G.first_kmin = df + 4 * (ni + 1);
+    G.first_bimg = df + 5 * (ni + 1);
     G.first_gemm = G.first_bimg + (3 * ni + 1);
-    for (int k = 0; k < 6; ++k) G.grid[k] = D.grid[k];
+    for (int k = 0; k < 7; ++k) G.grid[k] = D.grid[k];
     CK(LAUNCH("k_reflect2d", launch_reflect_coef_group(G, 0, ctx->stream)));
     CK(LAUNCH("k_coef1d", launch_reflect_coef_group(G, 1, ctx->stream)));
     CK(LAUNCH("k_aimg_bessel3", launch_bessel_i8_group(G, 0, ctx->stream)));

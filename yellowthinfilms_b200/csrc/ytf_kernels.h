@@ -250,7 +250,10 @@ struct BesselI8 {
   unsigned* err;
   long wait_limit;   // polls of each bounded pipeline wait before it gives up
   int aimg_ready;    // Aimg already holds this order's J_n digits (launch_bessel_i8_aimg3)
+  double* kmin;      // [nchunk] smallest node of each slice (the J digits' scale, launch_slice_kmin)
 };
+// kmin[z] = min over slice z of kr (a slice of kchunk nodes, the last one up to K)
+cudaError_t launch_slice_kmin(const double* kr, long K, long kchunk, int nchunk, double* kmin, cudaStream_t s);
 // the J_0, J_1, J_2 digit images of all three orders in one pass (one Bessel evaluation per
 // (ρ, k)); p gives the shared layout (M, K, ntile_m, kchunk, nchunk, kr, rho)
 cudaError_t launch_bessel_i8_aimg3(const BesselI8& p, uint8_t* A0, uint8_t* A1, uint8_t* A2, cudaStream_t s);
@@ -285,7 +288,7 @@ struct Synth1DItem {
 // every stage of the group, in order, on stream s; `it`/`bp` and the `first_*` tables are
 // device arrays (bp: 3 entries per item, orders 0, 1, 2; bp[3i] also carries the layout of
 // item i's J_n images). Host copies (ni, grid sizes) come in `grid`: {reflect, coef, aimg,
-// bimg, gemm, assemble}.
+// bimg, gemm, assemble, slice minima}.
 struct Synth1DGroup {
   int ni;
   const Synth1DItem* it;
@@ -296,7 +299,8 @@ struct Synth1DGroup {
   const long* first_bimg;      // [3 ni + 1]
   const long* first_gemm;      // [3 ni + 1]
   const long* first_asm;       // [ni + 1]
-  long grid[6];
+  const long* first_kmin;      // [ni + 1]
+  long grid[7];
 };
 // the entry whose block range holds block b: the last e with first[e] <= b (first ascending)
 __device__ __forceinline__ int group_entry(const long* first, int ne, long b) {
@@ -310,7 +314,8 @@ __device__ __forceinline__ int group_entry(const long* first, int ne, long b) {
 }
 // stage 0: reflected amplitudes, 1: FP32 coefficient columns
 cudaError_t launch_reflect_coef_group(const Synth1DGroup& g, int stage, cudaStream_t s);
-// stage 0: J_n digit images, 1: coefficient digit images with their slice maxima, 2: contraction
+// stage 0: slice minima and J_n digit images, 1: coefficient digit images with their slice
+// maxima, 2: contraction
 cudaError_t launch_bessel_i8_group(const Synth1DGroup& g, int stage, cudaStream_t s);
 cudaError_t launch_assemble1d_group(const Synth1DGroup& g, cudaStream_t s);    // slice sum + pixel assembly
 constexpr int COEF1D_ZB_GROUP = 8;   // heights per thread of the grouped coefficient kernel
