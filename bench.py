@@ -659,6 +659,10 @@ def run_reference_learned(args):
 # by series or recurrence, digits): ncu's DFMA x 2 + DMUL + DADD of one grouped launch divided
 # by its (ρ, k) slots, 3.285e9 / 18.19e6
 AIMG_FP64_PER_PAIR = 180.0
+# DRAM bytes per node synthesised of the grouped kernels (dram__bytes_read + write of one ncu
+# capture of group 1 of `--workload synth --stacks 8 --group-bytes 1073741824`, 71,040 nodes;
+# traffic grows with the nodes of a launch), scaled to a launch's nodes
+TRAFFIC_PER_NODE = {"k_gemm_i8_img": 7999.0, "k_aimg_bessel3": 1792.0, "k_coef1d": 6406.0, "k_bimg_real": 15192.0}
 
 
 def learned_roofline(name, prof, nodes_synth):
@@ -671,6 +675,9 @@ def learned_roofline(name, prof, nodes_synth):
     if name not in prof or not prof[name][1]:
         return roof
     t_k, nl = prof[name][0] * 1e-3, prof[name][1]
+    if name in TRAFFIC_PER_NODE:
+        roof["traffic"] = TRAFFIC_PER_NODE[name] * nodes_synth / nl
+        roof["traffic_note"] = "bytes per launch: ncu bytes per node (71,040-node capture) x nodes per launch"
     peaks = measured_peaks()
     if name in ("k_gemm_i8_img", "k_bessel_i8"):
         flops = 2.0 * N_RHO * (26 * N_ZOBS) * nodes_synth  # 13 complex coefficient columns per height, 3 orders
