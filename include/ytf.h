@@ -143,6 +143,12 @@ int ytf_transfer_1d_contour(ytf_ctx* ctx, const ytf_stack* stack, double omega, 
                             const double* k_re, const double* k_im, const double* w_re, const double* w_im, int nobs,
                             const int* obs_layers, ytf_cache** out);
 
+/* J_0(x) and J_1(x) of real x exactly as the int8x3 1D synthesis evaluates them for its J
+ * digit images: the CUDA math library's j0/j1 below |x| = 25, Hankel's asymptotic expansions
+ * with one shared phase above (absolute error below 1e-12). For tests and callers that want
+ * the same values; no counterpart in the reference (SpecialFunctions.besselj). */
+int ytf_bessel_j01(ytf_ctx* ctx, long n, const double* x, double* j0, double* j1);
+
 /* J_order(z) (order 0, 1, 2) at n complex points z = z_re + i z_im, evaluated by the device
  * functions of the contour synthesis (power series, Miller recurrence, Hankel expansion). */
 int ytf_bessel_j(ytf_ctx* ctx, int order, long n, const double* z_re, const double* z_im, double* out_re,

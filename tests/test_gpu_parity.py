@@ -801,3 +801,16 @@ def test_1d_synthesis_in_node_passes_equals_the_sum_of_its_parts(ytf):
     parts = G(k[:h], w[:h]) + G(k[h:], w[h:])
     assert relerr(whole, parts) < 1e-12
     assert relerr(G(k, w, "int8x3"), whole) < 1e-6
+
+
+def test_real_bessel_pair_of_the_int8_synthesis(ytf):
+    """ytf_bessel_j01: J_0, J_1 of real arguments as the int8x3 J images take them (the CUDA
+    library below 25, Hankel's asymptotic pair with a shared phase above) against scipy, to
+    2e-12 absolute over 0-8000 (dense around the switch at 25), odd/even symmetry for x < 0."""
+    from scipy.special import j0, j1
+    x = np.concatenate([np.linspace(0.0, 40.0, 40001), np.linspace(24.9, 25.1, 2001), np.geomspace(40.0, 8000.0, 200001)])
+    a, b = ytf.bessel_j01(x)
+    assert np.max(np.abs(a - j0(x))) < 2e-12
+    assert np.max(np.abs(b - j1(x))) < 2e-12
+    an, bn = ytf.bessel_j01(-x)
+    assert np.max(np.abs(an - a)) < 1e-15 and np.max(np.abs(bn + b)) < 1e-15

@@ -113,6 +113,7 @@ SIGNATURES = {
                                             ctypes.POINTER(GridInfo)]),
     "ytf_transfer_1d_contour": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _d, _d, _d, _d,
                                                ctypes.c_int, _i, ctypes.POINTER(_vp)]),
+    "ytf_bessel_j01": (ctypes.c_int, [_vp, ctypes.c_long, _d, _d, _d]),
     "ytf_bessel_j": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_long, _d, _d, _d, _d]),
     "ytf_transfer_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(TransferDesc), ctypes.POINTER(_vp)]),
     "ytf_green_batch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(GreenDesc)]),

@@ -465,6 +465,16 @@ def rule_panels(stack, omega, source_layer, h_min, rho_max=0.0, target_decay=25.
     return pan[:2 * info.n_panels].reshape(-1, 2).copy()
 
 
+def bessel_j01(x, ctx: Optional[Context] = None):
+    """(J_0(x), J_1(x)) of real x as the int8x3 1D synthesis evaluates them
+    (ytf_bessel_j01: the CUDA library below |x| = 25, Hankel's asymptotic pair above)."""
+    ctx = ctx or default_context()
+    x = _f64(x)
+    a, b = np.zeros(len(x)), np.zeros(len(x))
+    ctx.check(lib().ytf_bessel_j01(ctx.h, len(x), ptr(x), ptr(a), ptr(b)))
+    return a, b
+
+
 def rule_panels_batch(problems, order=8, rtol=1e-6, target_decay=25.0, kr_cap=0.0, ctx: Optional[Context] = None):
     """rule_panels for many problems in one call (ytf_rule_panels_batch, host threads): each
     problem a dict with stack, omega, source_layer, h_min, rho_max and optionally poles

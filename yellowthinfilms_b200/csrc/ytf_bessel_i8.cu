@@ -39,20 +39,102 @@ int bessel_i8_ctile(int N) {
   return (N + nt - 1) / nt;
 }
 
-// J_0, J_1 (the CUDA math library), J_2 by its power series below |x| = 1 (A&S 9.1.10; exact
-// 0 at x = 0) and the three-term recurrence above (A&S 9.1.27), as k_bessel
-__device__ __forceinline__ double bessel_j012(int order, double x) {
-  if (order == 0) return j0(x);
-  if (order == 1) return j1(x);
+// J_2 from J_0, J_1: its power series below |x| = 1 (A&S 9.1.10; exact 0 at x = 0; the term
+// ratio -h²/((m + 1)(m + 3)) with the reciprocals as constants) and the three-term recurrence
+// above (A&S 9.1.27)
+__device__ __forceinline__ double j2_from(double x, double J0, double J1) {
   if (fabs(x) < 1.0) {
-    double h2 = 0.25 * x * x, t = 0.5 * h2, s = t;
+    constexpr double inv[12] = {1.0 / 3, 1.0 / 8, 1.0 / 15, 1.0 / 24, 1.0 / 35, 1.0 / 48,
+                                1.0 / 63, 1.0 / 80, 1.0 / 99, 1.0 / 120, 1.0 / 143, 1.0 / 168};
+    const double h2 = 0.25 * x * x;
+    double t = 0.5 * h2, s = t;
+#pragma unroll
     for (int m = 0; m < 12; ++m) {
-      t *= -h2 / ((m + 1.0) * (m + 3.0));
+      t *= -h2 * inv[m];
       s += t;
     }
     return s;
   }
-  return (2.0 / x) * j1(x) - j0(x);
+  return (2.0 / x) * J1 - J0;
+}
+
+// J_0, J_1 (j01_real below: the CUDA math library under x = 25, the asymptotic pair above),
+// J_2 from them
+__device__ __forceinline__ void j01_real(double x, double& J0, double& J1);
+__device__ __forceinline__ double bessel_j012(int order, double x) {
+  double J0, J1;
+  j01_real(x, J0, J1);
+  if (order == 0) return J0;
+  if (order == 1) return J1;
+  return j2_from(x, J0, J1);
+}
+
+// J_0(x) and J_1(x) for x >= 25 (absolute error below 1e-12): Hankel's asymptotic expansions
+// (A&S 9.2.5, 9.2.9, 9.2.10), J_n(x) = sqrt(2 / (π x)) (P_n cos χ_n - Q_n sin χ_n) with
+// χ_n = x - (2n + 1) π / 4, five terms each of P_n and Q_n in y = 1/x (the coefficient of y^m
+// is ±a_m / 8^m, a_m = Π_{j<=m} (4n² - (2j - 1)²) / m!). Both orders share one phase
+// (χ_1 = χ_0 - π/2): cos x and sin x from a Cody-Waite reduction by π/2 (a three-part
+// constant whose first two parts carry 33 bits, so n π/2 is exact for n < 2^20) and Taylor
+// polynomials on |r| <= π/4 (to r^17 and r^18), then cos χ_0 = (cos x + sin x)/√2 and
+// sin χ_0 = (sin x - cos x)/√2. The library's j0 and j1 evaluate each order with its own phase.
+constexpr double J_ASYM_MIN = 25.0;
+__device__ __forceinline__ void j01_large(double x, double& J0, double& J1) {
+  const double y = 1.0 / x, y2 = y * y;
+  const double p0 = fma(fma(fma(fma(6.074042001273483, y2, -0.5725014209747314), y2, 0.112152099609375), y2,
+                            -0.0703125), y2, 1.0);
+  const double q0 = y * fma(fma(fma(fma(-24.380529699556064, y2, 1.7277275025844574), y2, -0.22710800170898438), y2,
+                                0.0732421875), y2, -0.125);
+  const double p1 = fma(fma(fma(fma(-6.883914268109947, y2, 0.6765925884246826), y2, -0.144195556640625), y2,
+                            0.1171875), y2, 1.0);
+  const double q1 = y * fma(fma(fma(fma(27.248827311268542, y2, -1.993531733751297), y2, 0.2775764465332031), y2,
+                                -0.1025390625), y2, 0.375);
+  // x = n π/2 + r, |r| <= π/4
+  const double n = rint(x * 0.6366197723675814);
+  double r = fma(-n, 1.5707963267341256, x);
+  r = fma(-n, 6.077100506303966e-11, r);
+  r = fma(-n, 2.0222662487959506e-21, r);
+  const double r2 = r * r;
+  double sr = fma(fma(fma(fma(fma(fma(fma(2.8114572543455206e-15, r2, -7.647163731819816e-13), r2,
+                                          1.6059043836821613e-10), r2, -2.505210838544172e-08), r2,
+                                  2.7557319223985893e-06), r2, -0.0001984126984126984), r2, 0.008333333333333333), r2,
+                  -0.16666666666666666);
+  sr = fma(r * r2, sr, r);
+  double cr = fma(fma(fma(fma(fma(fma(fma(fma(-1.5619206968586225e-16, r2, 4.779477332387385e-14), r2,
+                                          -1.1470745597729725e-11), r2, 2.08767569878681e-09), r2,
+                                  -2.755731922398589e-07), r2, 2.48015873015873e-05), r2, -0.001388888888888889), r2,
+                  0.041666666666666664), r2, -0.5);
+  cr = fma(r2, cr, 1.0);
+  const int q = (int)((long long)n & 3);
+  const double sx = q == 0 ? sr : q == 1 ? cr : q == 2 ? -sr : -cr;
+  const double cx = q == 0 ? cr : q == 1 ? -sr : q == 2 ? -cr : sr;
+  const double c0 = (cx + sx) * 0.7071067811865476, s0 = (sx - cx) * 0.7071067811865476;
+  const double a = 0.7978845608028654 * sqrt(y);
+  J0 = a * (p0 * c0 - q0 * s0);
+  J1 = a * (p1 * s0 + q1 * c0);
+}
+// J_0, J_1 as the int8x3 J images take them: the asymptotic pair from x = 25, the library below
+__device__ __forceinline__ void j01_real(double x, double& J0, double& J1) {
+  if (fabs(x) >= J_ASYM_MIN) {
+    j01_large(fabs(x), J0, J1);
+    if (x < 0) J1 = -J1;  // J_1 is odd
+  } else {
+    J0 = j0(x);
+    J1 = j1(x);
+  }
+}
+
+__global__ void k_bessel_j01(const double* __restrict__ x, long n, double* __restrict__ J0, double* __restrict__ J1) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a, b;
+  j01_real(x[i], a, b);
+  J0[i] = a;
+  J1[i] = b;
+}
+cudaError_t launch_bessel_j01(const double* x, long n, double* J0, double* J1, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_bessel_j01<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, n, J0, J1);
+  return cudaGetLastError();
 }
 
 // |J_n(x)| <= j_env(x) = min(1, 0.9 / sqrt(x)) for n = 0, 1, 2 and x >= 0 (the suprema of
@@ -306,18 +388,8 @@ __device__ __forceinline__ void aimg_bessel3_body(const BesselI8& p, long t, uin
     double v[3] = {0.0, 0.0, 0.0};
     if (rv && k < p.K) {
       const double x = p.kr[k] * rho;
-      v[0] = j0(x);
-      v[1] = j1(x);
-      if (fabs(x) < 1.0) {
-        double h2 = 0.25 * x * x, tt = 0.5 * h2, ss = tt;
-        for (int m = 0; m < 12; ++m) {
-          tt *= -h2 / ((m + 1.0) * (m + 3.0));
-          ss += tt;
-        }
-        v[2] = ss;
-      } else {
-        v[2] = (2.0 / x) * v[1] - v[0];
-      }
+      j01_real(x, v[0], v[1]);
+      v[2] = j2_from(x, v[0], v[1]);
     }
 #pragma unroll
     for (int o = 0; o < 3; ++o) {
@@ -555,7 +627,7 @@ cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s) {
 // e = 3 i + o holds item i's order-o parameters; its J_n images share item i's node slicing
 // (bp[3 i] gives the layout), so one Bessel evaluation per (ρ, k) serves the three orders.
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 5) k_aimg_bessel3_group(const BesselI8* __restrict__ bp, const long* __restrict__ first,
+__global__ void __launch_bounds__(256) k_aimg_bessel3_group(const BesselI8* __restrict__ bp, const long* __restrict__ first,
                                                           int ni) {
   const int i = group_entry(first, ni, blockIdx.x);
   const BesselI8& p = bp[3 * i];

@@ -1224,6 +1224,20 @@ int ytf_bessel_j(ytf_ctx* ctx, int order, long n, const double* z_re, const doub
   return YTF_OK;
 }
 
+int ytf_bessel_j01(ytf_ctx* ctx, long n, const double* x, double* j0, double* j1) {
+  if (!ctx || n < 0 || (n > 0 && (!x || !j0 || !j1))) return YTF_ERR_ARG;
+  if (n == 0) return YTF_OK;
+  CK(cudaSetDevice(ctx->device));
+  WS(buf, double, "bj01", 3 * (size_t)n);
+  int rc;
+  if ((rc = upload(ctx, buf, x, 8 * (size_t)n))) return rc;
+  CK(launch_bessel_j01(buf, n, buf + n, buf + 2 * n, ctx->stream));
+  CK(cudaMemcpyAsync(j0, buf + n, 8 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(j1, buf + 2 * n, 8 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return YTF_OK;
+}
+
 int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cache** out) {
   if (!ctx || nb < 0 || (nb > 0 && (!d || !out))) return YTF_ERR_ARG;
   for (int i = 0; i < nb; ++i) out[i] = nullptr;

@@ -252,6 +252,8 @@ struct BesselI8 {
   int aimg_ready;    // Aimg already holds this order's J_n digits (launch_bessel_i8_aimg3)
   double* kmin;      // [nchunk] smallest node of each slice (the J digits' scale, launch_slice_kmin)
 };
+// J_0(x), J_1(x) as the int8x3 1D synthesis evaluates them (library below 25, asymptotic above)
+cudaError_t launch_bessel_j01(const double* x, long n, double* J0, double* J1, cudaStream_t s);
 // kmin[z] = min over slice z of kr (a slice of kchunk nodes, the last one up to K)
 cudaError_t launch_slice_kmin(const double* kr, long K, long kchunk, int nchunk, double* kmin, cudaStream_t s);
 // the J_0, J_1, J_2 digit images of all three orders in one pass (one Bessel evaluation per
