@@ -1089,31 +1089,43 @@ def run_contour(args):
     zo = np.linspace(0.0, 200.0, 64)
     out = torch.empty(256 * 64 * 9, dtype=torch.complex128, device="cuda")
 
-    def step():
-        c = api.build_cavity_transfer_1d_contour(st, k0, 1, k, w, obs_layers=[1])
-        api.closed_form_G(c, 1, 20.0, zo, rho, [0.0], out=out)
+    prec = "int8x3" if args.precision != "fp64" else "fp64"
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    ctx.profile(True)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(0) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            step()
-        e1.record(stream)
+    def step(p):
+        c = api.build_cavity_transfer_1d_contour(st, k0, 1, k, w, obs_layers=[1])
+        api.closed_form_G(c, 1, 20.0, zo, rho, [0.0], out=out, precision=p)
+
+    def run(p):
+        for _ in range(args.warmup):
+            step(p)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    prof = ctx.profile_read()
+        ctx.profile(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(0) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                step(p)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        return e0.elapsed_time(e1) / args.steps, prof, clk.summary(), out.clone()
+
+    ms64, prof64, clocks64, G64 = run("fp64")
+    ms, prof, clocks, G = run(prec) if prec != "fp64" else (ms64, prof64, clocks64, G64)
     line = {"metric": METRIC, "value": 256 * 64 * 9 / (ms * 1e-3), "unit": "entries/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128 (complex nodes, complex J_n)",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128 node solve; complex J_n; " + ("int8x3 tensor-core contraction (Re J, Im J digit images)"
+                                                         if prec != "fp64" else "FP64 contraction"),
+            "fp64_entries_per_s": 256 * 64 * 9 / (ms64 * 1e-3),
+            "max_rel_diff_vs_fp64": float(torch.linalg.vector_norm(G - G64) / torch.linalg.vector_norm(G64)),
+            "fp64_kernels_ms_per_step": {kk: round(v[0] / args.steps, 4) for kk, v in sorted(prof64.items())},
             "data": "synthetic (the config-1 stack)",
             "config": {"workload": "vertical dipole 20 nm above a uniaxial film (εo = -3+0.4i, εe = 4+0.2i, 50 nm) on "
                                    "glass, λ = 600 nm; 4096 nodes on kρ = t - 0.05 i k0 sin(π t / 20 k0); 256 ρ x 64 z",
                        "entries_per_step": 256 * 64 * 9, "gzz_entries_per_step": 256 * 64},
-            "gzz_entries_per_s": 256 * 64 / (ms * 1e-3), "clocks": clk.summary(),
+            "gzz_entries_per_s": 256 * 64 / (ms * 1e-3), "clocks": clocks,
             "kernels_ms_per_step": {kk: round(v[0] / args.steps, 4) for kk, v in sorted(prof.items())}}
     print(json.dumps(line), flush=True)
     return 0

@@ -301,7 +301,8 @@ typedef struct {
  * YTF_PREC_SPLIT_BF16 (tensor-core contraction, split-BF16 operands, FP32 accumulation) or
  * YTF_PREC_INT8X3 (int8 tensor-core contraction: operands in three fixed-point base-256
  * digits, exact INT32 accumulation). INT8X3 applies to the 2D lateral sum and to the 1D Bessel
- * contraction (J_n(kρ) and the coefficient columns in digits); SPLIT_BF16 to the 2D lateral
+ * contraction (J_n(kρ) and the coefficient columns in digits; on a deformed contour the complex
+ * J_n's real and imaginary parts, two contractions per order); SPLIT_BF16 to the 2D lateral
  * sum only (1D: FP64). */
 int ytf_green(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, double zsrc_local, int nz, const double* z_obs,
               int nx, const double* xs, int ny, const double* ys, int terms, int precision, double* out,

@@ -706,7 +706,8 @@ def test_config1_contour_matches_real_axis_oracle(ytf, oracle):
     the film's loss every pole lies above the real axis and the branch points on it, so by
     Cauchy's theorem the contour integral equals the oracle's real-axis integral over
     [0, 20 k0] (dense rule: breaks at the light lines, u² substitution at the half-space
-    ones, ~48k nodes): G and Gzz within 1e-6."""
+    ones, ~48k nodes): G and Gzz within 1e-6 (FP64 contraction; the int8x3 one within 1e-6
+    of it)."""
     st = config1_stack()
     k0 = 2 * np.pi / 600.0
     oracle.set_threads(__import__("os").cpu_count() or 1)
@@ -728,6 +729,13 @@ def test_config1_contour_matches_real_axis_oracle(ytf, oracle):
     Go = oracle.closed_form_G(oc, 1, 20.0, zo, rho, [0.0])
     assert relerr(Gc, Go) < 1e-6, relerr(Gc, Go)
     assert relerr(Gc[..., 2, 2], Go[..., 2, 2]) < 1e-6
+    # the int8 tensor-core contraction on the contour (complex J_n as real and imaginary digit
+    # images, two int8x3 contractions per order): within 1e-6 of the FP64 contour G, and so of
+    # the oracle's real-axis integral
+    G8 = ytf.closed_form_G(gc, 1, 20.0, zo, rho, [0.0], precision="int8x3")
+    assert relerr(G8, Gc) < 1e-6, relerr(G8, Gc)
+    assert relerr(G8, Go) < 1.5e-6, relerr(G8, Go)
+    assert relerr(G8[..., 2, 2], Go[..., 2, 2]) < 1.5e-6
 
 
 def test_point_krho_grid_2d_without_scan_bit_exact(ytf, oracle):

@@ -257,7 +257,8 @@ def closed_form_G(cache: _Cache, obs_layer: int, zsrc_local: float, z_obs, xs, y
     ``precision`` selects the arithmetic of the 2D lateral sum: "fp64" (CUDA-core FP64),
     "split_bf16" (tensor cores, split-BF16 operands, FP32 accumulation) or "int8x3" (int8
     tensor cores, operands in three fixed-point base-256 digits, exact INT32 accumulation).
-    For 1D caches "int8x3" also runs the Bessel contraction on the int8 tensor cores;
+    For 1D caches "int8x3" also runs the Bessel contraction on the int8 tensor cores (on a
+    deformed contour: the complex J_n's real and imaginary parts as two digit images);
     "split_bf16" keeps it FP64.
 
     ``out``: optional torch tensor (complex128, Nx*Ny*Nz*9 elements, Julia order) to write

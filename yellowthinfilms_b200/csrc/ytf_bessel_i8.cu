@@ -534,7 +534,8 @@ __device__ __forceinline__ void gemm_i8_img_body(const BesselI8& p, int mt, int 
       const int q = warp & 3;
       const uint32_t lanebase = (uint32_t)(32 * q) << 16;
       const int r = mt * BI_M + 32 * q + lane;
-      const double eA = r < p.M ? j_env(p.kmin[z] * p.rho[r]) : 1.0;  // the row's J digit scale
+      const double eA = r >= p.M ? 1.0 : p.rowscale ? p.rowscale[(long)z * p.M + r]
+                                                     : j_env(p.kmin[z] * p.rho[r]);  // the row's J digit scale
       double* out = p.partial + (long)z * p.N * p.M;
       const unsigned long long* cmax = p.colmax + (long)z * p.N;
       for (int e0 = 0; e0 < p.Np; e0 += 8) {
@@ -594,9 +595,87 @@ __global__ void k_reduce_transpose(int M, int N, int nz, const double* __restric
   }
 }
 
+// per (order, slice, radius): max(|Re J|, |Im J|) over the slice's nodes (1 where it is 0)
+__global__ void __launch_bounds__(256) k_jtab_max(BesselI8 p, const double* __restrict__ J, double* __restrict__ rs) {
+  const int z = blockIdx.x, r = blockIdx.y, o = blockIdx.z;
+  const long plane = (long)p.M * p.K;
+  const double* re = J + (2L * o) * plane + (long)r * p.K;
+  const double* im = re + plane;
+  const long k0 = (long)z * p.kchunk, k1 = min(p.K, k0 + p.kchunk);
+  double m = 0.0;
+  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) m = fmax(m, fmax(fabs(re[k]), fabs(im[k])));
+  __shared__ double red[256];
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) rs[((long)o * p.nchunk + z) * p.M + r] = red[0] > 0.0 && isfinite(red[0]) ? red[0] : 1.0;
+}
+
+// one thread per (image, radius tile, row, slice, 4-node word): the digits of Re or Im J_o
+// relative to the row's slice maximum, written as one 32-bit word of each digit plane
+struct Img6 {
+  uint8_t* p[6];
+};
+__global__ void __launch_bounds__(256) k_jtab_img(BesselI8 p, const double* __restrict__ J,
+                                                  const double* __restrict__ rs, Img6 img) {
+  const long words = p.kchunk / 4;
+  const long per = (long)p.ntile_m * BI_M * p.nchunk * words;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 6 * per) return;
+  const int im = (int)(t / per);  // 2 o + part
+  long u = t % per;
+  const long wq = u % words;
+  u /= words;
+  const int z = (int)(u % p.nchunk);
+  u /= p.nchunk;
+  const int row = (int)(u % BI_M);
+  const int mt = (int)(u / BI_M);
+  const int r = mt * BI_M + row;
+  const bool rv = r < p.M;
+  const int o = im / 2;
+  const double sA = rv ? BI_SCALE / rs[((long)o * p.nchunk + z) * p.M + r] : 0.0;
+  const double* tab = J + (long)im * p.M * p.K + (long)(rv ? r : 0) * p.K;
+  const long g = wq / 4;
+  const int q = (int)(wq % 4);
+  uint32_t w[3] = {0u, 0u, 0u};
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const long k = (long)z * p.kchunk + 16 * g + 4 * q + h;
+    const double v = (rv && k < p.K) ? tab[k] : 0.0;
+    uint32_t d0, d1, d2;
+    digits3b(__double2int_rn(v * sA), d0, d1, d2);
+    w[0] |= d0 << (8 * h);
+    w[1] |= d1 << (8 * h);
+    w[2] |= d2 << (8 * h);
+  }
+  const long nstage = p.kchunk / BI_NODES;
+  const int s = (int)(g / 4), kb = (int)(g % 4) * 16;
+  const size_t sbytes = 3ul * BI_M * 64;
+  uint8_t* blk = img.p[im] + (((size_t)mt * p.nchunk + z) * nstage + s) * sbytes;
+#pragma unroll
+  for (int pl = 0; pl < 3; ++pl)
+    *reinterpret_cast<uint32_t*>(blk + (size_t)pl * BI_M * 64 + plane_off(row, kb) + 4 * q) = w[pl];
+}
+
+cudaError_t launch_jtable_images(const BesselI8& bp, const double* Jtab, double* rowscale, uint8_t* const img[6],
+                                 cudaStream_t s) {
+  if (bp.M <= 0 || bp.K <= 0) return cudaSuccess;
+  k_jtab_max<<<dim3((unsigned)bp.nchunk, (unsigned)bp.M, 3), 256, 0, s>>>(bp, Jtab, rowscale);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long tot = 6L * bp.ntile_m * BI_M * bp.nchunk * (bp.kchunk / 4);
+  Img6 im6;
+  for (int i = 0; i < 6; ++i) im6.p[i] = img[i];
+  k_jtab_img<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(bp, Jtab, rowscale, im6);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_bessel_i8(const BesselI8& p, double* P, cudaStream_t s) {
   if (p.M <= 0 || p.N <= 0 || p.K <= 0) return cudaSuccess;
-  if (!p.kmin || p.kchunk % BI_NODES != 0 || p.kchunk > 16384 || p.Np % 16 != 0 || p.Np > BI_ACC_STRIDE || p.Np < p.ctile ||
+  if ((!p.kmin && !p.rowscale) || p.kchunk % BI_NODES != 0 || p.kchunk > 16384 || p.Np % 16 != 0 || p.Np > BI_ACC_STRIDE || p.Np < p.ctile ||
       (long)p.nchunk * p.kchunk < p.K)
     return cudaErrorInvalidValue;
   cudaError_t e;

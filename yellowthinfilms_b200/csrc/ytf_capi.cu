@@ -1540,7 +1540,7 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
                      const GreenBatch* gb, double* P0, double* P1, double* P2) {
   const long nk = sp.c.n;
   WS(amp1, double2, "g_amp", (size_t)12 * nk);
-  const bool i8 = precision == YTF_PREC_INT8X3 && !sp.c.kri;
+  const bool i8 = precision == YTF_PREC_INT8X3;
   // FP64 coefficient columns for the FP64 contractions, FP32 ones for the int8x3 digits
   double *C0 = nullptr, *C1 = nullptr, *C2 = nullptr;
   float *F0 = nullptr, *F1 = nullptr, *F2 = nullptr;
@@ -1553,6 +1553,75 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
     C0 = C; C1 = C + 10 * (size_t)nz * nk; C2 = C + 18 * (size_t)nz * nk;
     CK(LAUNCH("k_coef1d", launch_coef1d_amp(sp, amp1, C0, C1, C2, ctx->stream)));
   }
+    if (sp.c.kri && i8) {
+      // nodes on a deformed contour, int8 tensor cores: the complex J_n(kρ ρ) tables (FP64),
+      // their real and imaginary parts as digit images fixed point per (order, slice, radius)
+      // relative to the slice's largest part, two int8x3 contractions per order against the
+      // FP32 coefficient columns (Re J and Im J), then the complex combine as the FP64 path
+      const float* Cn8[3] = {F0, F1, F2};
+      double* Pn8[3] = {P0, P1, P2};
+      const int Nn8[3] = {10 * nz, 8 * nz, 8 * nz};
+      unsigned* err = gb ? gb->err : nullptr;
+      if (!err) {
+        WS(e1, unsigned, "g_tc_err", 1);
+        err = e1;
+        CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+      }
+      WS(Jc, double, "g_Jc", 6 * (size_t)nr * nk);
+      CK(LAUNCH("k_bessel_c", launch_bessel_c(sp.c.kr, sp.c.kri, nk, drho, nr, Jc, ctx->stream)));
+      long kchunk;
+      {
+        const int ct0 = bessel_i8_ctile(Nn8[0]);
+        const long tiles = (long)((nr + 127) / 128) * ((Nn8[0] + ct0 - 1) / ct0);
+        const long want = std::max(1L, (long)nsm / tiles);
+        kchunk = (nk + want - 1) / want;
+        kchunk = std::min(16384L, std::max(64L, ((kchunk + 63) / 64) * 64));
+      }
+      const int nchunk = (int)((nk + kchunk - 1) / kchunk);
+      const size_t nst = (size_t)(kchunk / 64);
+      const size_t abytes = (size_t)((nr + 127) / 128) * nchunk * nst * bessel_i8_stage_bytes_a();
+      WS(Ai, uint8_t, "g_bic_a", 6 * abytes);
+      WS(rs, double, "g_bic_rs", 3 * (size_t)nchunk * nr);
+      uint8_t* imgs[6];
+      for (int i = 0; i < 6; ++i) imgs[i] = Ai + i * abytes;
+      BesselI8 lay;
+      std::memset(&lay, 0, sizeof(lay));
+      lay.M = nr; lay.K = nk; lay.ntile_m = (nr + 127) / 128; lay.kchunk = kchunk; lay.nchunk = nchunk;
+      CK(LAUNCH("k_bessel_i8", launch_jtable_images(lay, Jc, rs, imgs, ctx->stream)));
+      WS(Pab, double, "g_Pab", 2 * (size_t)nr * 10 * nz);
+      for (int o = 0; o < 3; ++o) {
+        BesselI8 bp;
+        std::memset(&bp, 0, sizeof(bp));
+        bp.M = nr; bp.N = Nn8[o]; bp.K = nk; bp.order = o;
+        bp.ctile = bessel_i8_ctile(bp.N);
+        bp.Np = ((bp.ctile + 15) / 16) * 16;
+        bp.ntile_n = (bp.N + bp.ctile - 1) / bp.ctile;
+        bp.ntile_m = (nr + 127) / 128;
+        bp.kchunk = kchunk;
+        bp.nchunk = nchunk;
+        WS(Bi, uint8_t, "g_bi_b", (size_t)bp.ntile_n * bp.nchunk * nst * bessel_i8_stage_bytes_b(bp.Np));
+        WS(cm, unsigned long long, "g_bi_cmax", (size_t)bp.nchunk * bp.N);
+        WS(pt, double, "g_bi_part", (size_t)bp.nchunk * bp.N * nr);
+        bp.kr = sp.c.kr; bp.rho = drho; bp.C = Cn8[o]; bp.ldc = nk;
+        bp.Bimg = Bi; bp.colmax = cm; bp.partial = pt; bp.err = err;
+        bp.wait_limit = ctx->wait_limit;
+        bp.aimg_ready = 1;
+        bp.rowscale = rs + (size_t)o * nchunk * nr;
+        for (int part = 0; part < 2; ++part) {
+          bp.Aimg = imgs[2 * o + part];
+          CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pab + (size_t)part * nr * 10 * nz, ctx->stream)));
+        }
+        CK(LAUNCH("k_combine_complex", launch_combine_complex(nr, Nn8[o], Pab, Pab + (size_t)nr * 10 * nz, Pn8[o],
+                                                              ctx->stream)));
+      }
+      if (!gb) {
+        unsigned herr = 0;
+        CK(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (herr) return fail(ctx, YTF_ERR_CUDA, "closed_form_G: a tensor-core pipeline wait timed out");
+      }
+      return YTF_OK;
+    }
     if (sp.c.kri) {
       // nodes on a deformed contour: complex J_n(kρ ρ) tables, two FP64 GEMMs per order
       // (Re J and Im J against the real/imaginary coefficient columns), then the complex combine

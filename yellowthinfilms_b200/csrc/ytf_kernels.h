@@ -251,7 +251,16 @@ struct BesselI8 {
   long wait_limit;   // polls of each bounded pipeline wait before it gives up
   int aimg_ready;    // Aimg already holds this order's J_n digits (launch_bessel_i8_aimg3)
   double* kmin;      // [nchunk] smallest node of each slice (the J digits' scale, launch_slice_kmin)
+  const double* rowscale;  // [nchunk][M] the J digits' scale per (slice, radius) when set (digits
+                           // rint(J 8355000 / rowscale)); else j_env(kmin[z] ρ_r)
 };
+// complex J_n tables ([6][nr][nk]: Re J_0, Im J_0, Re J_1, ... from launch_bessel_c) into the
+// int8x3 layout: rowscale[o][z][r] = max over slice z of max(|Re J_o|, |Im J_o|) at radius r
+// (1 where it is 0), then for each order o and part (0 Re, 1 Im) the digit image
+// img[2 o + part] in bp's A layout (ntile_m x nchunk x stages); bp gives M, K, ntile_m, kchunk,
+// nchunk
+cudaError_t launch_jtable_images(const BesselI8& bp, const double* Jtab, double* rowscale, uint8_t* const img[6],
+                                 cudaStream_t s);
 // J_0(x), J_1(x) as the int8x3 1D synthesis evaluates them (library below 25, asymptotic above)
 cudaError_t launch_bessel_j01(const double* x, long n, double* J0, double* J1, cudaStream_t s);
 // kmin[z] = min over slice z of kr (a slice of kchunk nodes, the last one up to K)
