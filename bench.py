@@ -668,7 +668,7 @@ TRAFFIC_PER_NODE = {"k_gemm_i8_img": 7999.0, "k_aimg_bessel3": 1792.0, "k_coef1d
 def learned_roofline(name, prof, nodes_synth):
     """Roofline entry of one kernel of the learned step's synthesis from its CUDA-event time in
     the profiled step: the int8x3 contraction against the sustained bf16 tensor peak (its
-    algorithmic flops: 2 x radii x 1664 real coefficient columns per node synthesised), the
+    algorithmic flops: 2 x radii x 1152 real coefficient columns per node synthesised), the
     J_n image kernel against the nominal FP64 peak (its counted FP64 operations)."""
     roof = {"kernel": name, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None,
             "traffic": TRAFFIC.get(name)}
@@ -680,11 +680,11 @@ def learned_roofline(name, prof, nodes_synth):
         roof["traffic_note"] = "bytes per launch: ncu bytes per node (71,040-node capture) x nodes per launch"
     peaks = measured_peaks()
     if name in ("k_gemm_i8_img", "k_bessel_i8"):
-        flops = 2.0 * N_RHO * (26 * N_ZOBS) * nodes_synth  # 13 complex coefficient columns per height, 3 orders
+        flops = 2.0 * N_RHO * (18 * N_ZOBS) * nodes_synth  # the 9 stored complex coefficient columns per height
         peak, src = peaks["bf16_sustained"]
         roof.update(bound="tensor", achieved=flops / t_k / 1e12, peak=peak, unit="TFLOP/s",
                     frac=flops / t_k / 1e12 / peak, peak_source=src, launches=nl,
-                    work=f"2 x {N_RHO} radii x 1664 real coefficient columns x nodes synthesised "
+                    work=f"2 x {N_RHO} radii x 1152 real coefficient columns x nodes synthesised "
                          f"({int(nodes_synth)} over the chunk's syntheses) = {flops:.3e} flop in {nl} launches")
     elif name == "k_aimg_bessel3":
         ops = AIMG_FP64_PER_PAIR * N_RHO * nodes_synth
@@ -975,14 +975,14 @@ def run_bessel(args):
     ms, prof, clocks, G = run(prec)
     ms64, prof64, _, G64 = run("fp64")
     entries = G.size
-    flops = 2.0 * 4096 * 65536 * 26 * 256  # 13 complex coefficient columns (26 real) per height
+    flops = 2.0 * 4096 * 65536 * 18 * 256  # the 9 stored complex coefficient columns (18 real) per height
     name = "k_bessel_i8" if prec == "int8x3" else "k_dgemm_nt"
     t_k = prof[name][0] / prof[name][1] * 1e-3 if name in prof else None
     peak, src = measured_peaks()["bf16_sustained"]
     roof = {"kernel": name, "bound": "tensor" if prec == "int8x3" else "fp64",
             "achieved": flops / 3 / t_k / 1e12 if t_k else None, "unit": "TFLOP/s",
             "peak": peak if prec == "int8x3" else FP64_NOMINAL, "traffic": None,
-            "work": "2 x 4096 radii x 65536 nodes x 26 real columns x 256 heights = 3.57e12 flop over the 3 orders "
+            "work": "2 x 4096 radii x 65536 nodes x 18 real columns x 256 heights = 2.47e12 flop over the 3 orders "
                     "(one launch per order: a third each)",
             "peak_source": src if prec == "int8x3" else "nominal FP64"}
     if roof["achieved"]:

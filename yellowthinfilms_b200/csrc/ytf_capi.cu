@@ -1545,12 +1545,12 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
   double *C0 = nullptr, *C1 = nullptr, *C2 = nullptr;
   float *F0 = nullptr, *F1 = nullptr, *F2 = nullptr;
   if (i8) {
-    WS(Cf, float, "g_Cf", 26 * (size_t)nz * nk);
-    F0 = Cf; F1 = Cf + 10 * (size_t)nz * nk; F2 = Cf + 18 * (size_t)nz * nk;
+    WS(Cf, float, "g_Cf", (size_t)C1D_RT * nz * nk);
+    F0 = Cf; F1 = Cf + (size_t)C1D_OFF1 * nz * nk; F2 = Cf + (size_t)C1D_OFF2 * nz * nk;
     CK(LAUNCH("k_coef1d", launch_coef1d_amp(sp, amp1, F0, F1, F2, ctx->stream)));
   } else {
-    WS(C, double, "g_C", 26 * (size_t)nz * nk);
-    C0 = C; C1 = C + 10 * (size_t)nz * nk; C2 = C + 18 * (size_t)nz * nk;
+    WS(C, double, "g_C", (size_t)C1D_RT * nz * nk);
+    C0 = C; C1 = C + (size_t)C1D_OFF1 * nz * nk; C2 = C + (size_t)C1D_OFF2 * nz * nk;
     CK(LAUNCH("k_coef1d", launch_coef1d_amp(sp, amp1, C0, C1, C2, ctx->stream)));
   }
     if (sp.c.kri && i8) {
@@ -1560,7 +1560,7 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
       // FP32 coefficient columns (Re J and Im J), then the complex combine as the FP64 path
       const float* Cn8[3] = {F0, F1, F2};
       double* Pn8[3] = {P0, P1, P2};
-      const int Nn8[3] = {10 * nz, 8 * nz, 8 * nz};
+      const int Nn8[3] = {C1D_R0 * nz, C1D_R1 * nz, C1D_R2 * nz};
       unsigned* err = gb ? gb->err : nullptr;
       if (!err) {
         WS(e1, unsigned, "g_tc_err", 1);
@@ -1588,7 +1588,8 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
       std::memset(&lay, 0, sizeof(lay));
       lay.M = nr; lay.K = nk; lay.ntile_m = (nr + 127) / 128; lay.kchunk = kchunk; lay.nchunk = nchunk;
       CK(LAUNCH("k_bessel_i8", launch_jtable_images(lay, Jc, rs, imgs, ctx->stream)));
-      WS(Pab, double, "g_Pab", 2 * (size_t)nr * 10 * nz);
+      const size_t pab = (size_t)nr * C1D_RMAX * nz;
+      WS(Pab, double, "g_Pab", 2 * pab);
       for (int o = 0; o < 3; ++o) {
         BesselI8 bp;
         std::memset(&bp, 0, sizeof(bp));
@@ -1609,10 +1610,9 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
         bp.rowscale = rs + (size_t)o * nchunk * nr;
         for (int part = 0; part < 2; ++part) {
           bp.Aimg = imgs[2 * o + part];
-          CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pab + (size_t)part * nr * 10 * nz, ctx->stream)));
+          CK(LAUNCH("k_bessel_i8", launch_bessel_i8(bp, Pab + (size_t)part * pab, ctx->stream)));
         }
-        CK(LAUNCH("k_combine_complex", launch_combine_complex(nr, Nn8[o], Pab, Pab + (size_t)nr * 10 * nz, Pn8[o],
-                                                              ctx->stream)));
+        CK(LAUNCH("k_combine_complex", launch_combine_complex(nr, Nn8[o], Pab, Pab + pab, Pn8[o], ctx->stream)));
       }
       if (!gb) {
         unsigned herr = 0;
@@ -1629,8 +1629,9 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
       CK(LAUNCH("k_bessel_c", launch_bessel_c(sp.c.kr, sp.c.kri, nk, drho, nr, Jc, ctx->stream)));
       const double* Cn[3] = {C0, C1, C2};
       double* Pn[3] = {P0, P1, P2};
-      const int Nn[3] = {10 * nz, 8 * nz, 8 * nz};
-      WS(Pab, double, "g_Pab", 2 * (size_t)nr * 10 * nz);
+      const int Nn[3] = {C1D_R0 * nz, C1D_R1 * nz, C1D_R2 * nz};
+      const size_t pab = (size_t)nr * C1D_RMAX * nz;
+      WS(Pab, double, "g_Pab", 2 * pab);
       for (int o = 0; o < 3; ++o) {
         long tiles = (long)((nr + 127) / 128) * ((Nn[o] + 127) / 128);
         long want = (2L * nsm + tiles - 1) / tiles;
@@ -1640,10 +1641,9 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
           const double* Jp = Jc + (size_t)(2 * o + part) * nr * nk;
           CK(LAUNCH("k_dgemm_nt", launch_dgemm_nt(nr, Nn[o], (int)nk, Jp, Cn[o], Pp, sp0, ctx->stream)));
           CK(LAUNCH("k_reduce_splits", launch_reduce_splits((long)nr * Nn[o], sp0, Pp,
-                                                            Pab + (size_t)part * nr * 10 * nz, ctx->stream)));
+                                                            Pab + (size_t)part * pab, ctx->stream)));
         }
-        CK(LAUNCH("k_combine_complex", launch_combine_complex(nr, Nn[o], Pab, Pab + (size_t)nr * 10 * nz, Pn[o],
-                                                              ctx->stream)));
+        CK(LAUNCH("k_combine_complex", launch_combine_complex(nr, Nn[o], Pab, Pab + pab, Pn[o], ctx->stream)));
       }
       return YTF_OK;
     }
@@ -1652,7 +1652,7 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
       // exact INT32 accumulation, FP64 sum of the node slices into P_n
       const float* Cn8[3] = {F0, F1, F2};
       double* Pn8[3] = {P0, P1, P2};
-      const int Nn8[3] = {10 * nz, 8 * nz, 8 * nz};
+      const int Nn8[3] = {C1D_R0 * nz, C1D_R1 * nz, C1D_R2 * nz};
       unsigned* err = gb ? gb->err : nullptr;
       if (!err) {
         WS(e1, unsigned, "g_tc_err", 1);
@@ -1716,15 +1716,16 @@ static int synth1d_P(ytf_ctx* ctx, const SynthParams& sp, int nz, int nr, const 
       long maxs = std::max(1L, nk / 256);
       return (int)std::max(1L, std::min(want, maxs));
     };
-    int s0 = splits_for(nr, 10 * nz), s1 = splits_for(nr, 8 * nz);
-    size_t part = std::max((size_t)s0 * nr * 10 * nz, (size_t)s1 * nr * 8 * nz);
+    const int Nn[3] = {C1D_R0 * nz, C1D_R1 * nz, C1D_R2 * nz};
+    const int sps[3] = {splits_for(nr, Nn[0]), splits_for(nr, Nn[1]), splits_for(nr, Nn[2])};
+    size_t part = 0;
+    for (int o = 0; o < 3; ++o) part = std::max(part, (size_t)sps[o] * nr * Nn[o]);
     WS(Pp, double, "g_partial", part);
     const double* Jn[3] = {J0, J1, J2};
     const double* Cn[3] = {C0, C1, C2};
     double* Pn[3] = {P0, P1, P2};
-    const int Nn[3] = {10 * nz, 8 * nz, 8 * nz};
     for (int o = 0; o < 3; ++o) {
-      int sp_ = dgemm_splits((int)nk, o == 0 ? s0 : s1);
+      int sp_ = dgemm_splits((int)nk, sps[o]);
       CK(LAUNCH("k_dgemm_nt", launch_dgemm_nt(nr, Nn[o], (int)nk, Jn[o], Cn[o], Pp, sp_, ctx->stream)));
       CK(LAUNCH("k_reduce_splits", launch_reduce_splits((long)nr * Nn[o], sp_, Pp, Pn[o], ctx->stream)));
     }
@@ -1825,15 +1826,15 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
       drho = urho;
       drmap = urmap;
     }
-    WS(P, double, "g_P", 26 * (size_t)nz * nr);
-    double *P0 = P, *P1 = P + 10 * (size_t)nz * nr, *P2 = P + 18 * (size_t)nz * nr;
+    WS(P, double, "g_P", (size_t)C1D_RT * nz * nr);
+    double *P0 = P, *P1 = P + (size_t)C1D_OFF1 * nz * nr, *P2 = P + (size_t)C1D_OFF2 * nz * nr;
     if (nk <= SYNTH1D_NODE_CHUNK) {
       if ((rc = synth1d_P(ctx, sp, nz, nr, drho, precision, nsm, gb, P0, P1, P2))) return rc;
     } else {
       // G is linear in the node sum: the rule in passes of at most SYNTH1D_NODE_CHUNK nodes,
       // their P_n summed (the reference sums closed_form_G over node chunks the same way,
       // chunked_2d, mod_ClosedFormGrid.jl:449-467)
-      const size_t np = 26 * (size_t)nz * nr;
+      const size_t np = (size_t)C1D_RT * nz * nr;
       WS(Pacc, double, "g_Pacc", np);
       WS(Pc, double, "g_Pchunk", np);
       WS(cbuf, double2, "g_chunk_cache", (size_t)48 * SYNTH1D_NODE_CHUNK);
@@ -1842,8 +1843,8 @@ static int green_impl(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zs
         const long nb = std::min(SYNTH1D_NODE_CHUNK, nk - b0);
         SynthParams spc = sp;
         if ((rc = node_chunk_view(ctx, sp.c, b0, nb, cbuf, spc.c))) return rc;
-        if ((rc = synth1d_P(ctx, spc, nz, nr, drho, precision, nsm, gb, Pc, Pc + 10 * (size_t)nz * nr,
-                            Pc + 18 * (size_t)nz * nr)))
+        if ((rc = synth1d_P(ctx, spc, nz, nr, drho, precision, nsm, gb, Pc, Pc + (size_t)C1D_OFF1 * nz * nr,
+                            Pc + (size_t)C1D_OFF2 * nz * nr)))
           return rc;
         CK(LAUNCH("k_add", launch_add(np, Pc, Pacc, ctx->stream)));
       }
@@ -2020,9 +2021,9 @@ static Group1DLayout group1d_layout(int item, long nk, int nz, int nr, long npix
   auto take = [&](size_t b) { size_t o = off; off += align256(b); return o; };
   L.off_amp = take(sizeof(double2) * 12 * (size_t)nk);
   L.ldc = (nk + 3) / 4 * 4;
-  L.off_C = take(sizeof(float) * 26 * (size_t)nz * L.ldc);
+  L.off_C = take(sizeof(float) * C1D_RT * (size_t)nz * L.ldc);
   for (int o = 0; o < 3; ++o) {
-    L.N[o] = (o == 0 ? 10 : 8) * nz;
+    L.N[o] = (o == 0 ? C1D_R0 : o == 1 ? C1D_R1 : C1D_R2) * nz;
     L.ctile[o] = bessel_i8_ctile(L.N[o]);
     L.Np[o] = ((L.ctile[o] + 15) / 16) * 16;
     L.ntn[o] = (L.N[o] + L.ctile[o] - 1) / L.ctile[o];
@@ -2105,7 +2106,7 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
       cand.push_back(i);
       const double ntm = (double)((ur[i].size() + 127) / 128);
       for (int od = 0; od < 3; ++od) {
-        const int N = (od == 0 ? 10 : 8) * d[i].nz, ct = bessel_i8_ctile(N);
+        const int N = (od == 0 ? C1D_R0 : od == 1 ? C1D_R1 : C1D_R2) * d[i].nz, ct = bessel_i8_ctile(N);
         ctas += ntm * (double)((N + ct - 1) / ct) * (double)d[i].cache->n;
       }
     }
@@ -2230,7 +2231,7 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
       f_aimg[q] = naimg; naimg += ((long)L.ntm * 128 * L.nchunk * (L.kchunk / 4) + 255) / 256;
       f_asm[q] = nasm; nasm += ((long)d[i].nx * d[i].ny * L.nz + 127) / 128;
       f_kmin[q] = nkmin; nkmin += L.nchunk;
-      const size_t coff[3] = {0, 10 * (size_t)L.nz * L.ldc, 18 * (size_t)L.nz * L.ldc};
+      const size_t coff[3] = {0, (size_t)C1D_OFF1 * L.nz * L.ldc, (size_t)C1D_OFF2 * L.nz * L.ldc};
       for (int od = 0; od < 3; ++od) {
         BesselI8& bp = hbp[3 * q + od];
         std::memset(&bp, 0, sizeof(bp));

@@ -122,6 +122,16 @@ struct SynthParams {
   const double* zo;  // [nz] device
 };
 
+// 1D coefficient columns per height: of the 13 complex coefficients (order 0: xx yx xy yy zz;
+// order 1: zx zy xz yz; order 2: xx yx xy yy) the synthesis stores the 9 independent ones,
+// order 0: xx yx zz, order 1: zx zy xz yz, order 2: xx yx, because in the azimuthally
+// symmetric 1D integrand yy = xx and xy = -yx of order 0, xy = yx and yy = -xx of order 2
+// exactly (the same products summed in swapped order, or negated: bit for bit); the pixel
+// assembly restores them. Real columns per height of orders 0, 1, 2 and the orders' offsets.
+constexpr int C1D_R0 = 6, C1D_R1 = 8, C1D_R2 = 4;
+constexpr int C1D_OFF1 = C1D_R0, C1D_OFF2 = C1D_R0 + C1D_R1, C1D_RT = C1D_R0 + C1D_R1 + C1D_R2;
+constexpr int C1D_RMAX = C1D_R1;  // the widest order
+
 // 1D Jacobi-Anger synthesis
 cudaError_t launch_coef1d(const SynthParams& p, double* C0, double* C1, double* C2, cudaStream_t s);
 // the same through per-node reflected amplitudes in amp ([12][n] complex scratch)

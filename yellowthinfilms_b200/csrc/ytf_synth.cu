@@ -93,7 +93,8 @@ __device__ __forceinline__ void direct_amp(const SynthParams& p, long k, double 
 
 // ------------------------------------------------------------------------------------
 // 1D coefficients. Columns per z-row: order 0: xx yx xy yy zz; order 1: zx zy xz yz;
-// order 2: xx yx xy yy (c q). Output rows are real: row 2*(zi*ncol + col) + part, node fastest.
+// order 2: xx yx xy yy (c q); stored: the 9 independent ones (store_coef_row, C1D_R* real rows
+// per height). Output rows are real: row 2*(zi*ncol + col) + part, node fastest.
 // ------------------------------------------------------------------------------------
 // the 13 coefficient columns of one (node, z row) (_integrate_pixel_1d's integrand,
 // mod_ClosedFormField.jl:435-487): order 0: xx yx xy yy zz; order 1: zx zy xz yz; order 2:
@@ -153,6 +154,49 @@ __device__ __forceinline__ void coef1d_row(const SynthParams& p, long k, double 
   }
 }
 
+// the 9 stored complex columns of one (node, height) as real rows (C1D_R* per height) of
+// C0, C1, C2 (row stride `stride`)
+template <class T>
+__device__ __forceinline__ void store_coef_row(T* C0, T* C1, T* C2, long stride, long k, int zi, const cd c0[5],
+                                               const cd c1[4], const cd c2[4]) {
+  const cd s0[3] = {c0[0], c0[1], c0[4]};
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const long r = 2L * (zi * 3 + j);
+    C0[r * stride + k] = (T)s0[j].x;
+    C0[(r + 1) * stride + k] = (T)s0[j].y;
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const long r = 2L * (zi * 4 + j);
+    C1[r * stride + k] = (T)c1[j].x;
+    C1[(r + 1) * stride + k] = (T)c1[j].y;
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const long r = 2L * (zi * 2 + j);
+    C2[r * stride + k] = (T)c2[j].x;
+    C2[(r + 1) * stride + k] = (T)c2[j].y;
+  }
+}
+
+// the 13 order sums of one (radius, height) from the stored ones (Pn(col) = the complex value
+// of stored column col of order n): yy = xx, xy = -yx of order 0; xy = yx, yy = -xx of order 2
+template <class F0, class F1, class F2>
+__device__ __forceinline__ void unpack_order_sums(F0 P0, F1 P1, F2 P2, cd g0[5], cd g1[4], cd g2[4]) {
+  g0[0] = P0(0);
+  g0[1] = P0(1);
+  g0[2] = -g0[1];
+  g0[3] = g0[0];
+  g0[4] = P0(2);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) g1[j] = P1(j);
+  g2[0] = P2(0);
+  g2[1] = P2(1);
+  g2[2] = g2[1];
+  g2[3] = -g2[0];
+}
+
 __global__ void __launch_bounds__(128) k_coef1d(SynthParams p, double* C0, double* C1, double* C2) {
   long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   int zi = blockIdx.y;
@@ -163,18 +207,7 @@ __global__ void __launch_bounds__(128) k_coef1d(SynthParams p, double* C0, doubl
   reflected_amp(p, k, Af, Ab);
   cd c0[5], c1[4], c2[4];
   coef1d_row(p, k, p.zo[zi], Af, Ab, c0, c1, c2);
-  for (int i = 0; i < 5; ++i) {
-    long r = 2L * (zi * 5 + i);
-    C0[r * n + k] = c0[i].x;
-    C0[(r + 1) * n + k] = c0[i].y;
-  }
-  for (int i = 0; i < 4; ++i) {
-    long r = 2L * (zi * 4 + i);
-    C1[r * n + k] = c1[i].x;
-    C1[(r + 1) * n + k] = c1[i].y;
-    C2[r * n + k] = c2[i].x;
-    C2[(r + 1) * n + k] = c2[i].y;
-  }
+  store_coef_row(C0, C1, C2, n, k, zi, c0, c1, c2);
 }
 
 cudaError_t launch_coef1d(const SynthParams& p, double* C0, double* C1, double* C2, cudaStream_t s) {
@@ -481,14 +514,12 @@ __global__ void k_assemble1d(int nx, int ny, int nz, const double* xs, const dou
   int zi = (int)(t / npix);
   int i = (int)(pix % nx), j = (int)(pix / nx);
   int r = rmap[pix];
-  const long n0 = 10L * nz, n1 = 8L * nz;
+  const long n0 = (long)C1D_R0 * nz, n1 = (long)C1D_R1 * nz, n2 = (long)C1D_R2 * nz;
   cd g0[5], g1[4], g2[4];
-  for (int col = 0; col < 5; ++col) { long o = (long)r * n0 + 2L * (zi * 5 + col); g0[col] = cd{P0[o], P0[o + 1]}; }
-  for (int col = 0; col < 4; ++col) {
-    long o = (long)r * n1 + 2L * (zi * 4 + col);
-    g1[col] = cd{P1[o], P1[o + 1]};
-    g2[col] = cd{P2[o], P2[o + 1]};
-  }
+  unpack_order_sums([&](int c) { const long o = (long)r * n0 + 2L * (zi * 3 + c); return cd{P0[o], P0[o + 1]}; },
+                    [&](int c) { const long o = (long)r * n1 + 2L * (zi * 4 + c); return cd{P1[o], P1[o + 1]}; },
+                    [&](int c) { const long o = (long)r * n2 + 2L * (zi * 2 + c); return cd{P2[o], P2[o + 1]}; },
+                    g0, g1, g2);
   assemble1d_pixel(xs[i], ys[j], g0, g1, g2, pix, npix, zi, nz, G);
 }
 
@@ -596,18 +627,7 @@ __global__ void __launch_bounds__(128) k_coef1d_amp(SynthParams p, const double2
   for (int zi = z0; zi < z1; ++zi) {
     cd c0[5], c1[4], c2[4];
     coef1d_row(p, k, p.zo[zi], Af, Ab, c0, c1, c2);
-    for (int i = 0; i < 5; ++i) {
-      long r = 2L * (zi * 5 + i);
-      C0[r * n + k] = (T)c0[i].x;
-      C0[(r + 1) * n + k] = (T)c0[i].y;
-    }
-    for (int i = 0; i < 4; ++i) {
-      long r = 2L * (zi * 4 + i);
-      C1[r * n + k] = (T)c1[i].x;
-      C1[(r + 1) * n + k] = (T)c1[i].y;
-      C2[r * n + k] = (T)c2[i].x;
-      C2[(r + 1) * n + k] = (T)c2[i].y;
-    }
+    store_coef_row(C0, C1, C2, n, k, zi, c0, c1, c2);
   }
 }
 
@@ -1128,12 +1148,6 @@ __global__ void __launch_bounds__(128, 4) k_reflect2d_group(const Synth1DItem* _
     }
 }
 
-// one FP32 coefficient value (the int8x3 digits come from it; their scales from the
-// (slice, column) maxima the digit-image kernel takes)
-__device__ __forceinline__ void coef_store(float* C, long row, long stride, long k, double v) {
-  C[row * stride + k] = (float)v;
-}
-
 // a read-only load the compiler keeps in place (volatile asm: not hoisted out of the row loop),
 // so the node's mode fields are re-read from L1 per row instead of held in registers
 __device__ __forceinline__ cd ldc_row(const double2* b, long e, long n, long i) {
@@ -1187,8 +1201,8 @@ __device__ __noinline__ void coef_rows_direct(const Synth1DItem& it, long k, int
   const int nz = p.nz;
   const long cst = it.ldc;  // row stride of the coefficient columns
   float* C0 = it.C;
-  float* C1 = it.C + 10L * nz * cst;
-  float* C2 = it.C + 18L * nz * cst;
+  float* C1 = it.C + (long)C1D_OFF1 * nz * cst;
+  float* C2 = it.C + (long)C1D_OFF2 * nz * cst;
   cd Af[2][3], Ab[2][3];
   for (int m = 0; m < 2; ++m)
     for (int q = 0; q < 3; ++q) {
@@ -1198,17 +1212,7 @@ __device__ __noinline__ void coef_rows_direct(const Synth1DItem& it, long k, int
   for (int zi = z0; zi < z1; ++zi) {
     cd c0[5], c1[4], c2[4];
     coef1d_row(p, k, p.zo[zi], Af, Ab, c0, c1, c2);
-    for (int j = 0; j < 5; ++j) {
-      coef_store(C0, 2L * (zi * 5 + j), cst, k, c0[j].x);
-      coef_store(C0, 2L * (zi * 5 + j) + 1, cst, k, c0[j].y);
-    }
-    for (int j = 0; j < 4; ++j) {
-      const long r = 2L * (zi * 4 + j);
-      coef_store(C1, r, cst, k, c1[j].x);
-      coef_store(C1, r + 1, cst, k, c1[j].y);
-      coef_store(C2, r, cst, k, c2[j].x);
-      coef_store(C2, r + 1, cst, k, c2[j].y);
-    }
+    store_coef_row(C0, C1, C2, cst, k, zi, c0, c1, c2);
   }
 }
 
@@ -1234,8 +1238,8 @@ __global__ void __launch_bounds__(128, 3) k_coef1d_group(const Synth1DItem* __re
   const int nz = p.nz;
   const long cst = it.ldc;  // row stride of the coefficient columns
   float* C0 = it.C;
-  float* C1 = it.C + 10L * nz * cst;
-  float* C2 = it.C + 18L * nz * cst;
+  float* C1 = it.C + (long)C1D_OFF1 * nz * cst;
+  float* C2 = it.C + (long)C1D_OFF2 * nz * cst;
   const int z0 = (int)(b / nkb) * COEF1D_ZB_GROUP;
   const int z1 = min(nz, z0 + COEF1D_ZB_GROUP);
   if (p.with_direct) {
@@ -1295,19 +1299,7 @@ __global__ void __launch_bounds__(128, 3) k_coef1d_group(const Synth1DItem* __re
       }
     cd c0[5], c1[4], c2[4];
     coef_row_scat(c, k, aw, g, c0, c1, c2);
-#pragma unroll
-    for (int j = 0; j < 5; ++j) {
-      coef_store(C0, 2L * (zi * 5 + j), cst, k, c0[j].x);
-      coef_store(C0, 2L * (zi * 5 + j) + 1, cst, k, c0[j].y);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const long r = 2L * (zi * 4 + j);
-      coef_store(C1, r, cst, k, c1[j].x);
-      coef_store(C1, r + 1, cst, k, c1[j].y);
-      coef_store(C2, r, cst, k, c2[j].x);
-      coef_store(C2, r + 1, cst, k, c2[j].y);
-    }
+    store_coef_row(C0, C1, C2, cst, k, zi, c0, c1, c2);
   }
 }
 
@@ -1334,29 +1326,20 @@ __global__ void __launch_bounds__(128) k_assemble1d_group(const Synth1DItem* __r
   const int r = it.rmap[pix];
   const long M = it.nr;
   const int nch = it.nchunk;
-  const long N0 = 10L * nz, N1 = 8L * nz;
-  cd g0[5], g1[4], g2[4];
-  for (int col = 0; col < 5; ++col) {
-    const long c = 2L * (zi * 5 + col);
+  const long N0 = (long)C1D_R0 * nz, N1 = (long)C1D_R1 * nz, N2 = (long)C1D_R2 * nz;
+  // the slices' partials summed in order, as k_reduce_transpose
+  auto sum = [&](const double* part, long N, long c) {
     double re = 0.0, im = 0.0;
     for (int z = 0; z < nch; ++z) {
-      re += it.part[0][((long)z * N0 + c) * M + r];
-      im += it.part[0][((long)z * N0 + c + 1) * M + r];
+      re += part[((long)z * N + c) * M + r];
+      im += part[((long)z * N + c + 1) * M + r];
     }
-    g0[col] = cd{re, im};
-  }
-  for (int col = 0; col < 4; ++col) {
-    const long c = 2L * (zi * 4 + col);
-    double r1 = 0.0, i1 = 0.0, r2 = 0.0, i2 = 0.0;
-    for (int z = 0; z < nch; ++z) {
-      r1 += it.part[1][((long)z * N1 + c) * M + r];
-      i1 += it.part[1][((long)z * N1 + c + 1) * M + r];
-      r2 += it.part[2][((long)z * N1 + c) * M + r];
-      i2 += it.part[2][((long)z * N1 + c + 1) * M + r];
-    }
-    g1[col] = cd{r1, i1};
-    g2[col] = cd{r2, i2};
-  }
+    return cd{re, im};
+  };
+  cd g0[5], g1[4], g2[4];
+  unpack_order_sums([&](int c) { return sum(it.part[0], N0, 2L * (zi * 3 + c)); },
+                    [&](int c) { return sum(it.part[1], N1, 2L * (zi * 4 + c)); },
+                    [&](int c) { return sum(it.part[2], N2, 2L * (zi * 2 + c)); }, g0, g1, g2);
   assemble1d_pixel(it.xs[ix], it.ys[iy], g0, g1, g2, pix, npix, zi, nz, it.G);
 }
 
