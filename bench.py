@@ -655,14 +655,14 @@ def run_reference_learned(args):
     return 0
 
 
-# FP64 operations per (ρ, k) pair of k_aimg_bessel3 (J_0 and J_1 by the CUDA math library, J_2
-# by series or recurrence, digits): ncu's DFMA x 2 + DMUL + DADD of one grouped launch divided
-# by its (ρ, k) slots, 3.285e9 / 18.19e6
-AIMG_FP64_PER_PAIR = 180.0
+# FP64 operations per (ρ, k) pair of k_aimg_bessel3 (J_0, J_1 by Hankel's asymptotic pair from
+# x = 25 and the CUDA math library below, J_2 by series or recurrence, digits): ncu's DFMA x 2 +
+# DMUL + DADD of one grouped launch divided by its (ρ, k) slots, 3.32e9 / 23.05e6
+AIMG_FP64_PER_PAIR = 144.0
 # DRAM bytes per node synthesised of the grouped kernels (dram__bytes_read + write of one ncu
-# capture of group 1 of `--workload synth --stacks 8 --group-bytes 1073741824`, 71,040 nodes;
+# capture of `--workload synth --stacks 8 --group-bytes 1073741824`, one group of 89,144 nodes;
 # traffic grows with the nodes of a launch), scaled to a launch's nodes
-TRAFFIC_PER_NODE = {"k_gemm_i8_img": 7999.0, "k_aimg_bessel3": 1792.0, "k_coef1d": 6406.0, "k_bimg_real": 15192.0}
+TRAFFIC_PER_NODE = {"k_gemm_i8_img": 6316.0, "k_aimg_bessel3": 1748.0, "k_coef1d": 4581.0, "k_bimg_real": 10357.0}
 
 
 def learned_roofline(name, prof, nodes_synth):
@@ -677,7 +677,7 @@ def learned_roofline(name, prof, nodes_synth):
     t_k, nl = prof[name][0] * 1e-3, prof[name][1]
     if name in TRAFFIC_PER_NODE:
         roof["traffic"] = TRAFFIC_PER_NODE[name] * nodes_synth / nl
-        roof["traffic_note"] = "bytes per launch: ncu bytes per node (71,040-node capture) x nodes per launch"
+        roof["traffic_note"] = "bytes per launch: ncu bytes per node (89,144-node capture) x nodes per launch"
     peaks = measured_peaks()
     if name in ("k_gemm_i8_img", "k_bessel_i8"):
         flops = 2.0 * N_RHO * (18 * N_ZOBS) * nodes_synth  # the 9 stored complex coefficient columns per height
