@@ -311,7 +311,7 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* cache, int obs_layer, double zsrc_l
 /* closed_form_G over many (cache, observation set) items with one synchronisation: the
  * same results as ytf_green per item, in order, on the context's stream; the coordinates of
  * all items go up in one copy and the items' kernels queue back to back. 1D items of real
- * nodes (at most 1048576) at YTF_PREC_INT8X3 are synthesised together, six launches per
+ * nodes (at most 1048576) at YTF_PREC_INT8X3 are synthesised together, seven launches per
  * group of items (ytf_ctx_set_group_bytes): each such item's G equals ytf_green's to the
  * int8x3 tolerance (the contraction's node slices, and so the slices' fixed-point scales,
  * differ); every other item's G is ytf_green's bit for bit. The reference

@@ -1978,9 +1978,9 @@ int ytf_green(ytf_ctx* ctx, const ytf_cache* c, int obs_layer, double zsrc_local
 // ------------------------------------------------------------------------------------
 // Grouped 1D int8x3 synthesis inside ytf_green_batch: the batch's 1D items of real nodes
 // (at most SYNTH1D_GROUP_MAX_NODES nodes) in groups whose workspace stays within the context's
-// group bound (ytf_ctx_set_group_bytes, default 4 GiB); each group is six launches whatever
-// its item count (amplitudes, coefficient columns, J_n images, coefficient images with their
-// slice maxima, contraction, slice sum + assembly), with every item's blocks side by side in each
+// group bound (ytf_ctx_set_group_bytes, default 4 GiB); each group is seven launches whatever
+// its item count (amplitudes, coefficient columns, slice minima, J_n images, coefficient
+// images with their slice maxima, contraction, slice sum + assembly), with every item's blocks side by side in each
 // grid; items with host outputs get a device G in the group's workspace, copied out after it. Per item the
 // arithmetic is the per-item path's; only the node slicing of the contraction differs
 // (slices of about SYNTH1D_GROUP_SLICE nodes, whose fixed-point scales are per slice).
@@ -2431,10 +2431,13 @@ static int gl_rule_batch_impl(ytf_ctx* ctx, int nsets, const int* npanels, const
   std::vector<int> side(np);
   size_t p0 = 0, s0 = 0;
   for (int j = 0; j < nsets; ++j) {
-    std::set<double> S(singular + s0, singular + s0 + nsing[j]);
+    // a set's few singular points (exact matches, as the set lookup of ytf_gl_rule)
+    const double* S0 = singular + s0;
+    const double* S1 = S0 + nsing[j];
+    auto has = [&](double v) { return std::find(S0, S1, v) != S1; };
     for (int i = 0; i < npanels[j]; ++i) {
       const size_t q = p0 + i;
-      side[q] = S.count(pa[q]) ? 1 : (S.count(pb[q]) ? -1 : 0);
+      side[q] = has(pa[q]) ? 1 : (has(pb[q]) ? -1 : 0);
     }
     p0 += npanels[j];
     s0 += nsing[j];
