@@ -747,14 +747,17 @@ def run_learned(args):
     mine = chunks[rank::world] or chunks[:1]
     dev_stacks = {}
 
-    # every step runs each method as two concurrent shares of the chunk (alternate stacks), one
+    # every step runs each method as --shares concurrent shares of the chunk (stacks dealt in turn), one
     # host thread, libytf context and CUDA stream each (learned.concurrent_shares), so that one
     # share's host steps overlap the other's device work; the network's forward for the whole
     # chunk runs first, on the main stream
-    ctx2 = api.Context(local)
-    stream2 = torch.cuda.Stream()
-    ctx2.set_stream(stream2.cuda_stream)
-    ctxs, streams = [ctx, ctx2], [stream, stream2]
+    ns = max(1, args.shares)
+    ctxs, streams = [ctx], [stream]
+    for _ in range(ns - 1):
+        c2, s2 = api.Context(local), torch.cuda.Stream()
+        c2.set_stream(s2.cuda_stream)
+        ctxs.append(c2)
+        streams.append(s2)
 
     def stack_of(i, c):
         if (i, c) not in dev_stacks:
@@ -764,9 +767,10 @@ def run_learned(args):
     def problems(idx, c=0):
         return [learned_problem(stacks[i][0], stacks[i][1], stack_of(i, c), prec) for i in idx]
 
-    def interleave(a, b):
-        out = [None] * (len(a) + len(b))
-        out[0::2], out[1::2] = a, b
+    def interleave(parts):
+        out = [None] * sum(len(q) for q in parts)
+        for j, q in enumerate(parts):
+            out[j::len(parts)] = q
         return out
 
     G_host = torch.empty((CHUNK, ENTRIES_PER_STACK), dtype=torch.complex128, pin_memory=True)
@@ -778,34 +782,38 @@ def run_learned(args):
 
     def step(s, timed):
         idx = mine[s % len(mine)]
-        Pa, Pb = problems(idx[0::2], 0), problems(idx[1::2], 1)
-        P = interleave(Pa, Pb)
-        sla, slb, spa, spb = [0] * len(Pa), [0] * len(Pb), [0] * len(Pa), [0] * len(Pb)
+        Ps = [problems(idx[j::ns], j) for j in range(ns)]
+        P = interleave(Ps)
+        sls, sps = [[0] * len(q) for q in Ps], [[0] * len(q) for q in Ps]
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         torch.cuda.synchronize()
         with torch.cuda.stream(stream):
             ev[0].record(stream)
-            stream2.wait_stream(stream)
-            pred = L.predict_batch(net, [(q["layers"], q["k0"]) for q in Pa + Pb], N_SCAN)
-            na = len(Pa) * N_SCAN
-            outa, outb = L.concurrent_shares(
+            for s2 in streams[1:]:
+                s2.wait_stream(stream)
+            pred = L.predict_batch(net, [(q["layers"], q["k0"]) for Pj in Ps for q in Pj], N_SCAN)
+            offs = np.cumsum([0] + [len(q) * N_SCAN for q in Ps])
+            outs = L.concurrent_shares(
                 lambda sh, c: L.learned_rules_batch(net, sh[0], ctx=c, device=True, n_scan=N_SCAN, solved=sh[1],
                                                     pred=sh[2]),
-                [(Pa, sla, pred[:na]), (Pb, slb, pred[na:])], ctxs, streams)
-            stream.wait_stream(stream2)
+                [(Ps[j], sls[j], pred[offs[j]:offs[j + 1]]) for j in range(ns)], ctxs, streams)
+            for s2 in streams[1:]:
+                stream.wait_stream(s2)
             ev[1].record(stream)
-            outl = interleave(outa, outb)
+            outl = interleave(outs)
             for j, o in enumerate(outl):
                 G_host[j].copy_(o[0].permute(4, 3, 2, 1, 0).reshape(-1), non_blocking=True)
             ev[2].record(stream)
-            stream2.wait_stream(stream)
-            outa, outb = L.concurrent_shares(lambda sh, c: L.plain_rules_batch(sh[0], ctx=c, device=True, solved=sh[1]),
-                                             [(Pa, spa), (Pb, spb)], ctxs, streams)
-            stream.wait_stream(stream2)
+            for s2 in streams[1:]:
+                s2.wait_stream(stream)
+            outs = L.concurrent_shares(lambda sh, c: L.plain_rules_batch(sh[0], ctx=c, device=True, solved=sh[1]),
+                                       [(Ps[j], sps[j]) for j in range(ns)], ctxs, streams)
+            for s2 in streams[1:]:
+                stream.wait_stream(s2)
             ev[3].record(stream)
-            outp = interleave(outa, outb)
+            outp = interleave(outs)
         torch.cuda.synchronize()
-        sl, sp = interleave(sla, slb), interleave(spa, spb)
+        sl, sp = interleave(sls), interleave(sps)
         if not timed:
             return
         rec["t_l"].append(ev[0].elapsed_time(ev[1]) * 1e-3)
@@ -894,7 +902,7 @@ def run_learned(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": f"f64 node solve, {prec} tensor-core synthesis; MLP bf16 weights, fp32 accum",
             "data": "synthetic (seeded)", "impl": "learned-adaptive",
-            "config": dict(LEARNED_CONFIG, precision=prec, steps_cover_stacks=rec["stacks"] * world,
+            "config": dict(LEARNED_CONFIG, precision=prec, shares_per_method=ns, steps_cover_stacks=rec["stacks"] * world,
                            held_out_stacks=n_test, train_samples=n_train * N_SCAN),
             "plain_entries_per_s": plain, "learned_vs_plain": t_p / t_l,
             "step_ms": {"learned": [round(1e3 * x, 2) for x in rec["t_l"]],
@@ -1138,6 +1146,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--shares", type=int, default=2,
+                    help="learned workload: concurrent shares of a chunk per method (host thread, context, stream each)")
     ap.add_argument("--group-bytes", type=int, default=0,
                     help="synth workload: workspace bound of one synthesis group (0: the library default)")
     ap.add_argument("--workload", default="learned", choices=["learned", "gyro32", "uneven", "bessel", "contour",

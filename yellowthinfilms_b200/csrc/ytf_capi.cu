@@ -159,7 +159,10 @@ void ctx_release(ytf_ctx* ctx) {
   if (--ctx->refs <= 0 && ctx->closing) delete ctx;
 }
 
-void* ws_get(ytf_ctx* ctx, const char* name_, size_t bytes, cudaError_t* e) {
+// `reserve`: the size a first allocation takes at least (a buffer whose size varies from call to
+// call up to a known bound is allocated at the bound once, so that later calls do not pay a
+// cudaFree's device-wide synchronisation to grow it)
+void* ws_get(ytf_ctx* ctx, const char* name_, size_t bytes, cudaError_t* e, size_t reserve = 0) {
   *e = cudaSuccess;
   if (bytes == 0) bytes = 16;
   const std::string name = ctx->ws_slot > 0 ? std::string(name_) + "#" + std::to_string(ctx->ws_slot) : std::string(name_);
@@ -186,11 +189,28 @@ void* ws_get(ytf_ctx* ctx, const char* name_, size_t bytes, cudaError_t* e) {
     ctx->ws.erase(it);
   }
   void* p = nullptr;
+  if (it == ctx->ws.end() && reserve > bytes) {  // first allocation: at the bound if it fits
+    if (cudaMalloc(&p, reserve) == cudaSuccess) {
+      ctx->ws[name] = {p, reserve};
+      return p;
+    }
+    cudaGetLastError();
+    p = nullptr;
+  }
   *e = cudaMalloc(&p, bytes);
   if (*e != cudaSuccess) return nullptr;
   ctx->ws[name] = {p, bytes};
   return p;
 }
+
+// WS with a first-allocation bound (ws_get's reserve, in bytes)
+#define WSR(ptr, type, name, count, reserve)                                                                 \
+  type* ptr = nullptr;                                                                                       \
+  {                                                                                                          \
+    cudaError_t e_;                                                                                          \
+    ptr = (type*)ws_get(ctx, name, sizeof(type) * (size_t)(count), &e_, (reserve));                          \
+    if (!ptr) return fail(ctx, YTF_ERR_NOMEM, std::string("workspace ") + name + ": " + cudaGetErrorString(e_)); \
+  }
 
 #define WS(ptr, type, name, count)                                                                           \
   type* ptr = nullptr;                                                                                       \
@@ -1337,7 +1357,7 @@ int ytf_transfer_batch(ytf_ctx* ctx, int nb, const ytf_transfer_desc* d, ytf_cac
     }
     first = i;
     if (items.empty()) continue;
-    WS(arena, char, "tb_scratch", used);
+    WSR(arena, char, "tb_scratch", used, budget);
     size_t o = 0;
     auto carve = [&](size_t bytes) {
       char* q = arena + o;
@@ -2176,7 +2196,7 @@ int ytf_green_batch(ytf_ctx* ctx, int nb, const ytf_green_desc* d) {
   uint8_t* gws = nullptr;
   uint8_t* gcm = nullptr;
   if (group_ws) {
-    WS(w, uint8_t, "gb1_ws", group_ws);
+    WSR(w, uint8_t, "gb1_ws", group_ws, ctx->group_bytes);
     WS(wc, uint8_t, "gb1_cmax", group_cm_max);
     gws = w;
     gcm = wc;
