@@ -276,12 +276,13 @@ def halved(stack, omega, panels, order, ctx=None):
 
 
 def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol=1e-6, check=None, max_halvings=6,
-                 ctx=None):
+                 ctx=None, check_order=12):
     """The learned point rule with the plain method as judge and fallback.
 
     Proposes poles with the network, fixes them with one exact batched sampling, and builds
     fixed_kρ_rule on them. With ``check`` (a callable rule -> G) the rule is accepted when G
-    agrees with G on the halved rule to rtol; otherwise the proposal missed a pole and the
+    agrees to rtol with G on the same panels at Gauss–Legendre order ``check_order`` (None:
+    on the halved panels at ``order``); otherwise the proposal missed a pole and the
     plain method takes over: the rule of one exact scan of the response
     (exact_scan_poles_batch), halved until two successive levels agree (at most max_halvings
     times), and if they never do, the reference's scanned rule. On agreement the finer level
@@ -298,8 +299,12 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
     sing = sorted(set(api.layer_light_lines(stack[0], k0)) | set(api.layer_light_lines(stack[-1], k0)))
     panels = info["panels"]
     G = check(k, w)
-    panels2 = api.halve_panels([tuple(p) for p in panels])
-    kh, wh = api.gl_rule(panels2, order, singular=sing)
+    if check_order:
+        panels2 = [tuple(p) for p in panels]
+        kh, wh = api.gl_rule(panels2, check_order, singular=sing)
+    else:
+        panels2 = api.halve_panels([tuple(p) for p in panels])
+        kh, wh = api.gl_rule(panels2, order, singular=sing)
     Gh = check(kh, wh)
     if np.linalg.norm(G - Gh) <= rtol * np.linalg.norm(Gh):
         info.update(learned=True, halvings=0, G=Gh, panels=np.asarray(panels2))
@@ -384,21 +389,28 @@ def _sing(P):
     return s
 
 
-def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, ctx, out, device=False, solved=None):
+def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, ctx, out, device=False, solved=None,
+                   check_order=None):
     """Halve the open problems' rules until G agrees with G on the halved rule (the plain
     method's own check), all open problems per batched level (the halved rules' nodes of a
     level in one ytf_gl_rule_batch call); fills out[i] = (G, k, w, halvings, converged) with
     the finer level of the agreeing pair (already solved, and the more accurate one). With G
     None the rules' own G and the first halved level are evaluated in one batch. ``solved``
     (optional list): solved[i] grows by the nodes of every rule problem i is solved and
-    synthesised on."""
+    synthesised on. ``check_order`` (optional): the first level's finer rule is the same panels
+    at that Gauss–Legendre order instead of the halved panels at ``order`` (fewer nodes for a
+    higher degree of exactness; later levels halve)."""
     open_ = list(idx)
     sing = {i: _sing(problems[i]) for i in open_}
     for h in range(max_halvings + 1):
         if not open_:
             break
-        p2s = [api.halve_panels(np.asarray(panels[i], np.float64).reshape(-1, 2)) for i in open_]
-        r2s = api.gl_rule_batch([(p2, sing[i]) for p2, i in zip(p2s, open_)], order, ctx=ctx, device=device)
+        if h == 0 and check_order:
+            p2s = [np.asarray(panels[i], np.float64).reshape(-1, 2) for i in open_]
+            r2s = api.gl_rule_batch([(p2, sing[i]) for p2, i in zip(p2s, open_)], check_order, ctx=ctx, device=device)
+        else:
+            p2s = [api.halve_panels(np.asarray(panels[i], np.float64).reshape(-1, 2)) for i in open_]
+            r2s = api.gl_rule_batch([(p2, sing[i]) for p2, i in zip(p2s, open_)], order, ctx=ctx, device=device)
         halv = {i: (p2, r2) for i, p2, r2 in zip(open_, p2s, r2s)}
         if solved is not None:
             for i in open_:
@@ -442,7 +454,7 @@ def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, de
 
 
 def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=None, device=False, build_rtol=None,
-                        n_scan=2048, solved=None, pred=None):
+                        n_scan=2048, solved=None, pred=None, check_order=12):
     """learned_rule for every problem: the network over all problems' scan grids (features
     formed on the device), the exact window sampling of all problems in one device call,
     fixed_kρ_rule per problem, then the acceptance check; the rejected problems take the rule
@@ -451,7 +463,10 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     ``build_rtol`` (default rtol): the tolerance the proposed rules are built for; the
     acceptance check always uses rtol. ``n_scan``: points of the log grid the network is
     evaluated on per problem. ``solved`` as _refine_levels. ``pred``: the network's outputs on
-    the problems' scan grids when already evaluated (predict_batch), else evaluated here."""
+    the problems' scan grids when already evaluated (predict_batch), else evaluated here.
+    ``check_order``: the proposal's check compares its G with G on the same panels at this
+    Gauss–Legendre order (12: 20 nodes solved per panel where the halving check takes 24,
+    the order-12 rule returned on agreement); None checks by halving."""
     n_k = n_scan
     if pred is None:
         pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
@@ -468,7 +483,8 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     # the proposals' own check (one level); a rejected proposal missed a pole: its rule comes
     # from one exact log scan of the response instead (batched over the rejected problems),
     # refined by halving until two levels agree
-    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, 0, order, ctx, out, device, solved)
+    _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, 0, order, ctx, out, device, solved,
+                   check_order=check_order)
     rej = [i for i, r in enumerate(out) if not r[4]]
     if rej:
         scanned = exact_scan_poles_batch([problems[i] for i in rej], ctx=ctx)
