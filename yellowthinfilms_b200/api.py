@@ -86,7 +86,7 @@ class Context:
         raise RuntimeError(f"libytf error {rc}: {msg}")
 
     def __del__(self):
-        if getattr(self, "h", None) is not None and _native._lib is not None:
+        if getattr(self, "h", None) is not None and getattr(_native, "_lib", None) is not None:
             _native._lib.ytf_ctx_destroy(self.h)
             self.h = None
 
@@ -122,7 +122,7 @@ class Stack:
         return self.layers[i]
 
     def __del__(self):
-        if getattr(self, "h", None) is not None and _native._lib is not None:
+        if getattr(self, "h", None) is not None and getattr(_native, "_lib", None) is not None:
             _native._lib.ytf_stack_destroy(self.h)
             self.h = None
 
@@ -153,7 +153,8 @@ class _Cache:
 
     def __del__(self):
         # a cache lent by a BatchPlan (_plan set) belongs to the plan
-        if getattr(self, "h", None) is not None and _native._lib is not None and getattr(self, "_plan", None) is None:
+        if (getattr(self, "h", None) is not None and getattr(_native, "_lib", None) is not None
+                and getattr(self, "_plan", None) is None):
             _native._lib.ytf_cache_destroy(self.h)
         self.h = None
 
@@ -533,7 +534,7 @@ class MLP:
         self.nparam = int(lib().ytf_mlp_num_params(h))
 
     def __del__(self):
-        if getattr(self, "h", None) is not None and _native._lib is not None:
+        if getattr(self, "h", None) is not None and getattr(_native, "_lib", None) is not None:
             _native._lib.ytf_mlp_destroy(self.h)
             self.h = None
 
@@ -907,7 +908,7 @@ class BatchPlan:
                     d2h_bytes=int(ho.value))
 
     def close(self):
-        if getattr(self, "h", None) is not None and _native._lib is not None:
+        if getattr(self, "h", None) is not None and getattr(_native, "_lib", None) is not None:
             _native._lib.ytf_plan_destroy(self.h)
         self.h = None
 
