@@ -284,8 +284,8 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
     agrees to rtol with G on the same panels at Gauss–Legendre order ``check_order`` (None:
     on the halved panels at ``order``); otherwise the proposal missed a pole and the
     plain method takes over: the rule of one exact scan of the response
-    (exact_scan_poles_batch), halved until two successive levels agree (at most max_halvings
-    times), and if they never do, the reference's scanned rule. On agreement the finer level
+    (exact_scan_poles_batch), checked the same way, then halved until two successive levels
+    agree (max_halvings + 1 levels in all), and if they never do, the reference's scanned rule. On agreement the finer level
     of the agreeing pair is returned (its G is already computed and the more accurate of the
     two). Returns (k, w, info): info["learned"] is True when the proposed rule itself was
     accepted, info["halvings"] counts the levels past it, info["G"] is G on the returned rule
@@ -317,15 +317,21 @@ def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol
     panels = info2["panels"]
     G = check(k, w)
     for h in range(max_halvings + 1):
-        panels2 = api.halve_panels([tuple(p) for p in panels])
-        kh, wh = api.gl_rule(panels2, order, singular=sing)
+        if h == 0 and check_order:
+            # the scanned rule's first check as the proposal's: the same panels at check_order
+            panels2 = [tuple(p) for p in panels]
+            kh, wh = api.gl_rule(panels2, check_order, singular=sing)
+        else:
+            panels2 = api.halve_panels([tuple(p) for p in panels])
+            kh, wh = api.gl_rule(panels2, order, singular=sing)
         Gh = check(kh, wh)
         if np.linalg.norm(G - Gh) <= rtol * np.linalg.norm(Gh):
             # the check passed: return the finer of the two levels (already solved, and the
             # more accurate; its difference to the coarser one bounds the coarser one's error)
             info.update(learned=False, halvings=h + 1, G=Gh, panels=np.asarray(panels2))
             return kh, wh, info
-        panels, k, w, G = panels2, kh, wh, Gh
+        if not (h == 0 and check_order):
+            panels, k, w, G = panels2, kh, wh, Gh
     k, w, info2 = api.point_kx_grid(stack, k0, source_layer, h_min=h_min, rho_max=rho_max, order=order, rtol=rtol,
                                     ctx=ctx)
     info.update(info2, learned=False, halvings=max_halvings + 2, G=check(k, w))
@@ -399,7 +405,8 @@ def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, c
     (optional list): solved[i] grows by the nodes of every rule problem i is solved and
     synthesised on. ``check_order`` (optional): the first level's finer rule is the same panels
     at that Gauss–Legendre order instead of the halved panels at ``order`` (fewer nodes for a
-    higher degree of exactness; later levels halve)."""
+    higher degree of exactness); a problem that fails it keeps its order-``order`` rule and G,
+    which the later levels halve. max_halvings + 1 levels in all."""
     open_ = list(idx)
     sing = {i: _sing(problems[i]) for i in open_}
     for h in range(max_halvings + 1):
@@ -431,7 +438,8 @@ def _refine_levels(problems, idx, rules, panels, G, rtol, max_halvings, order, c
                 out[i] = (g, halv[i][1][0], halv[i][1][1], h, True)
                 G[i] = None
             else:
-                panels[i], rules[i], G[i] = halv[i][0], halv[i][1], g
+                if not (h == 0 and check_order):
+                    panels[i], rules[i], G[i] = halv[i][0], halv[i][1], g
                 still.append(i)
         open_ = still
     for i in open_:
@@ -466,7 +474,8 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     the problems' scan grids when already evaluated (predict_batch), else evaluated here.
     ``check_order``: the proposal's check compares its G with G on the same panels at this
     Gauss–Legendre order (12: 20 nodes solved per panel where the halving check takes 24,
-    the order-12 rule returned on agreement); None checks by halving."""
+    the order-12 rule returned on agreement), and so does the first level of a rejected
+    problem's scanned rule; None checks by halving."""
     n_k = n_scan
     if pred is None:
         pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
@@ -482,7 +491,7 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     out = [None] * len(problems)
     # the proposals' own check (one level); a rejected proposal missed a pole: its rule comes
     # from one exact log scan of the response instead (batched over the rejected problems),
-    # refined by halving until two levels agree
+    # checked the same way, then refined by halving until two levels agree
     _refine_levels(problems, range(len(problems)), rules, panels, None, rtol, 0, order, ctx, out, device, solved,
                    check_order=check_order)
     rej = [i for i, r in enumerate(out) if not r[4]]
@@ -497,7 +506,8 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
                                                device=device)):
             rules[i] = r
         sub = [None] * len(problems)
-        _refine_levels(problems, rej, rules, panels, None, rtol, max_halvings, order, ctx, sub, device, solved)
+        _refine_levels(problems, rej, rules, panels, None, rtol, max_halvings, order, ctx, sub, device, solved,
+                       check_order=check_order)
         for i in rej:
             g, k, w, h, conv = sub[i]
             out[i] = (g, k, w, h + 1, conv)
