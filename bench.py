@@ -700,8 +700,8 @@ def run_learned(args):
     on 1e7 solver samples (timed separately); then every step takes one chunk of 256 held-out
     stacks through both methods, each to a G accurate to 1e-6: the learned rule (network
     proposals, exact window sampling, fixed_kρ_rule, the check against G on the same panels
-    at Gauss–Legendre order 12, plain halving on rejection) and the plain rule without pole knowledge halved until two levels agree. Every
-    node of both is solved exactly; both synthesise with the int8x3 tensor-core contraction.
+    at Gauss–Legendre order 10, plain halving on rejection) and the plain rule without pole
+    knowledge halved until two levels agree. Every node of both is solved exactly; both synthesise with the int8x3 tensor-core contraction.
     `value` is the learned method's entries/s with G left in HBM, `e2e` the same with every G
     copied to page-locked host memory inside the timed region; `plain_entries_per_s` is the
     plain method on the same stacks. A seeded sample of >= 512 returned G of both methods is

@@ -276,7 +276,7 @@ def halved(stack, omega, panels, order, ctx=None):
 
 
 def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol=1e-6, check=None, max_halvings=6,
-                 ctx=None, check_order=12):
+                 ctx=None, check_order=10):
     """The learned point rule with the plain method as judge and fallback.
 
     Proposes poles with the network, fixes them with one exact batched sampling, and builds
@@ -462,7 +462,7 @@ def plain_rules_batch(problems, order=8, rtol=1e-6, max_halvings=8, ctx=None, de
 
 
 def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=None, device=False, build_rtol=None,
-                        n_scan=2048, solved=None, pred=None, check_order=12):
+                        n_scan=2048, solved=None, pred=None, check_order=10):
     """learned_rule for every problem: the network over all problems' scan grids (features
     formed on the device), the exact window sampling of all problems in one device call,
     fixed_kρ_rule per problem, then the acceptance check; the rejected problems take the rule
@@ -473,9 +473,10 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     evaluated on per problem. ``solved`` as _refine_levels. ``pred``: the network's outputs on
     the problems' scan grids when already evaluated (predict_batch), else evaluated here.
     ``check_order``: the proposal's check compares its G with G on the same panels at this
-    Gauss–Legendre order (12: 20 nodes solved per panel where the halving check takes 24,
-    the order-12 rule returned on agreement), and so does the first level of a rejected
-    problem's scanned rule; None checks by halving."""
+    Gauss–Legendre order (10: 18 nodes solved per panel where the halving check takes 24, the
+    order-10 rule returned on agreement; on panels sized for order 8 its error is a few
+    percent of the order-8 rule's, which the agreement bounds), and so does the first level of
+    a rejected problem's scanned rule; None checks by halving."""
     n_k = n_scan
     if pred is None:
         pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
