@@ -23,6 +23,7 @@ units of the same workload (a held-out stack, or a whole wavelength), with no sc
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -160,12 +161,25 @@ class Clocks:
         self.proc = None
 
     def __enter__(self):
+        import threading
+        self.lines, self.first = [], threading.Event()
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (FileNotFoundError, OSError):
             self.proc = None
+            return self
+
+        def read():
+            for line in self.proc.stdout:
+                self.lines.append(line)
+                self.first.set()
+            self.first.set()
+        self.reader = threading.Thread(target=read, daemon=True)
+        self.reader.start()
+        # the sampler's start-up (NVML initialisation) ends before the timed region begins
+        self.first.wait(10.0)
         return self
 
     def __exit__(self, *a):
@@ -173,10 +187,12 @@ class Clocks:
         if self.proc is not None:
             self.proc.terminate()
             try:
-                self.out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                self.out, _ = self.proc.communicate()
+                self.proc.wait()
+            self.reader.join(5.0)
+            self.out = "".join(self.lines)
 
     def summary(self):
         rows = [r.split(",") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
@@ -837,11 +853,16 @@ def run_learned(args):
                 kept[i] = (outl[int(j)][0].clone(), outp[int(j)][0].clone())
         del outl, outp
 
+    # the objects of the setup (held-out stacks, network, imported modules) leave the cyclic
+    # collector's generations, so that a full collection during a step does not re-scan them
+    gc.collect()
+    gc.freeze()
     for s in range(args.warmup):
         step(s, False)
     with Clocks(local) as clk:
         for s in range(args.steps):
             step(args.warmup + s, True)
+    gc.unfreeze()
     t_l, t_e2e, t_p = (max_over_ranks(float(np.sum(rec[k])), dist, f"cuda:{local}") for k in ("t_l", "t_e2e", "t_p"))
     entries = rec["entries"]
     value = job_rate(entries, world, t_l * 1e3)
