@@ -765,15 +765,18 @@ def run_learned(args):
 
     # every step runs each method as --shares concurrent shares of the chunk (stacks dealt in turn), one
     # host thread, libytf context and CUDA stream each (learned.concurrent_shares), so that one
-    # share's host steps overlap the other's device work; the network's forward for the whole
-    # chunk runs first, on the main stream
+    # share's host steps overlap the other's device work; each share evaluates the network on its
+    # own stacks with its own copy of the trained network (learned.copy_network)
     ns = max(1, args.shares)
-    ctxs, streams = [ctx], [stream]
+    ctxs, streams, nets = [ctx], [stream], [net]
     for _ in range(ns - 1):
         c2, s2 = api.Context(local), torch.cuda.Stream()
         c2.set_stream(s2.cuda_stream)
+        n2 = L.copy_network(net, device=local)
+        n2.set_stream(s2.cuda_stream)
         ctxs.append(c2)
         streams.append(s2)
+        nets.append(n2)
 
     def stack_of(i, c):
         if (i, c) not in dev_stacks:
@@ -807,12 +810,10 @@ def run_learned(args):
             ev[0].record(stream)
             for s2 in streams[1:]:
                 s2.wait_stream(stream)
-            pred = L.predict_batch(net, [(q["layers"], q["k0"]) for Pj in Ps for q in Pj], N_SCAN)
-            offs = np.cumsum([0] + [len(q) * N_SCAN for q in Ps])
+            # each share evaluates the network on its own stacks with its own copy of it
             outs = L.concurrent_shares(
-                lambda sh, c: L.learned_rules_batch(net, sh[0], ctx=c, device=True, n_scan=N_SCAN, solved=sh[1],
-                                                    pred=sh[2]),
-                [(Ps[j], sls[j], pred[offs[j]:offs[j + 1]]) for j in range(ns)], ctxs, streams)
+                lambda sh, c: L.learned_rules_batch(sh[2], sh[0], ctx=c, device=True, n_scan=N_SCAN, solved=sh[1]),
+                [(Ps[j], sls[j], nets[j]) for j in range(ns)], ctxs, streams)
             for s2 in streams[1:]:
                 stream.wait_stream(s2)
             ev[1].record(stream)

@@ -72,3 +72,28 @@ def test_peaks_equal_the_sample_walk():
             cases += 1
             found += len(got)
     assert cases == 48 and found > 40
+
+
+def test_vectorised_scan_grids_and_feature_rows_are_bit_identical():
+    """scan_grids and the batched k feature of predict_batch equal scan_grid / k_feature per
+    item bit for bit, and feature_row equals its definition on stack_arrays (ε column-major
+    / 10, thickness in wavelengths, λ_ref / λ)."""
+    from yellowthinfilms_b200 import learned as L
+    from yellowthinfilms_b200.materials import stack_arrays
+    rng = np.random.default_rng(8)
+    items = [L.film_stack(rng) for _ in range(16)]
+    k0s = np.array([2 * np.pi / lam for _, lam in items])
+    G = L.scan_grids(k0s, 512)
+    assert np.array_equal(G, np.stack([L.scan_grid(k0, 512) for k0 in k0s]))
+    kf = (G / (L.K_HI * k0s)[:, None]).astype(np.float32)
+    assert np.array_equal(kf, np.stack([L.k_feature(k0, L.scan_grid(k0, 512)) for k0 in k0s]))
+    for st, lam in items:
+        k0 = 2 * np.pi / lam
+        _, _, eps, _, d = stack_arrays(st)
+        ref = np.zeros(L.N_FEATURES)
+        for l in range(min(len(st), L.MAX_LAYERS)):
+            ref[19 * l:19 * l + 9] = eps[l].real / 10.0
+            ref[19 * l + 9:19 * l + 18] = eps[l].imag / 10.0
+            ref[19 * l + 18] = d[l] * k0 / (2 * np.pi)
+        ref[-2] = k0 * L.LAMBDA_REF / (2 * np.pi)
+        assert np.array_equal(L.feature_row(st, k0), ref.astype(np.float32))

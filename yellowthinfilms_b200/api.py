@@ -319,8 +319,9 @@ def cavity_response_batch(items, phi=0.0, ctx: Optional[Context] = None):
 
 def layer_light_lines(layer, omega, phi=0.0):
     """layer_light_lines(layer, ω, φ) (mod_KxGrid.jl:41-59): host arithmetic of libytf."""
-    from .materials import stack_arrays
-    _, _, eps, mu, _ = stack_arrays([layer])
+    # ε and μ column-major, as stack_arrays lays out one layer
+    eps = np.ascontiguousarray(np.asarray(layer.eps, np.complex128).T.reshape(9))
+    mu = np.ascontiguousarray(np.asarray(layer.mu, np.complex128).T.reshape(9))
     out = np.zeros(3)
     n = ctypes.c_int(0)
     rc = lib().ytf_layer_light_lines(ptr(eps), ptr(mu), float(omega), float(phi), ptr(out), ctypes.byref(n))

@@ -22,7 +22,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import api
-from .materials import FlatOpticalLayer, IsotropicMaterial, UniaxialMaterial, stack_arrays
+from .materials import FlatOpticalLayer, IsotropicMaterial, UniaxialMaterial
 
 MAX_LAYERS = 8
 N_FEATURES = MAX_LAYERS * 19 + 2  # 154
@@ -51,15 +51,20 @@ def scan_grid(k0, n):
     return k0 * np.exp(np.linspace(np.log(K_LO), np.log(K_HI), n))
 
 
+def scan_grids(k0s, n):
+    """scan_grid of every k0 (rows of an [len(k0s), n] array, the same products)."""
+    return np.asarray(k0s, np.float64)[:, None] * np.exp(np.linspace(np.log(K_LO), np.log(K_HI), n))[None, :]
+
+
 def feature_row(stack, k0):
     """The k-independent part of a feature row (float32 [154], last entry 0): per layer (up
     to 8) Re and Im of the 9 ε entries / 10 and the thickness in wavelengths; then λ_ref / λ."""
-    _, _, eps, _, d = stack_arrays(stack)
     row = np.zeros(N_FEATURES)
-    for l in range(min(len(stack), MAX_LAYERS)):
-        row[19 * l:19 * l + 9] = eps[l].real / 10.0
-        row[19 * l + 9:19 * l + 18] = eps[l].imag / 10.0
-        row[19 * l + 18] = d[l] * k0 / (2 * np.pi)
+    for l, layer in enumerate(stack[:MAX_LAYERS]):
+        e = np.asarray(layer.eps, np.complex128).T.reshape(9)  # column-major, as stack_arrays
+        row[19 * l:19 * l + 9] = e.real / 10.0
+        row[19 * l + 9:19 * l + 18] = e.imag / 10.0
+        row[19 * l + 18] = float(layer.d) * k0 / (2 * np.pi)
     row[-2] = k0 * LAMBDA_REF / (2 * np.pi)
     return row.astype(np.float32)
 
@@ -152,6 +157,13 @@ def new_network(seed=0, device=0):
     return api.MLP((N_FEATURES, 256, 256, 256, 256, 2), seed=seed, device=device)
 
 
+def copy_network(net, device=0):
+    """A network with net's parameters (its own buffers: one per concurrent share)."""
+    c = new_network(device=device)
+    c.params = net.params
+    return c
+
+
 def train(net, X, T, steps, batch=4096, lr=1e-3, seed=1):
     """Adam on the device-resident set; returns the mini-batch losses."""
     import torch
@@ -171,7 +183,9 @@ def predict_batch(net, stacks, n_k=2048, chunk=256):
     for c0 in range(0, len(stacks), chunk):
         part = stacks[c0:c0 + chunk]
         rows = torch.from_numpy(np.stack([feature_row(st, k0) for st, k0 in part])).cuda()
-        kf = torch.from_numpy(np.stack([k_feature(k0, scan_grid(k0, n_k)) for _, k0 in part])).cuda()
+        k0s = np.array([k0 for _, k0 in part], np.float64)
+        # k_feature(k0, scan_grid(k0, n_k)) of every item, row by row the same operations
+        kf = torch.from_numpy((scan_grids(k0s, n_k) / (K_HI * k0s)[:, None]).astype(np.float32)).cuda()
         X = rows[:, None, :].repeat(1, n_k, 1)
         X[:, :, -1] = kf
         out.append(net.forward(X.view(-1, N_FEATURES)).cpu().numpy().astype(np.float64))
@@ -480,7 +494,7 @@ def learned_rules_batch(net, problems, order=8, rtol=1e-6, max_halvings=6, ctx=N
     n_k = n_scan
     if pred is None:
         pred = predict_batch(net, [(P["layers"], P["k0"]) for P in problems], n_k)
-    KS = np.stack([scan_grid(P["k0"], n_k) for P in problems])
+    KS = scan_grids([P["k0"] for P in problems], n_k)
     pk = api.peaks_batch(KS, pred[:, 0].reshape(len(problems), n_k) * LOG_SCALE, prominence=np.log(1.01))
     cands = [sorted(_score_candidates(KS[j], pred[j * n_k:(j + 1) * n_k, 1], pk[j])) for j in range(len(problems))]
     polesets = refine_poles_batch([(P["stack"], P["k0"], P["source_layer"], c) for P, c in zip(problems, cands)], ctx=ctx)
@@ -536,7 +550,7 @@ def concurrent_shares(fn, shares, ctxs, streams):
     work, so the host steps of a method (peaks, panels, levels) overlap the device work of the
     other shares. The problems of a share must use its context's Stack objects, and fn must not
     share other stateful objects between threads (an MLP's forward: evaluate the network before,
-    learned_rules_batch(pred=...)). Returns the
+    learned_rules_batch(pred=...), or give each share its own copy_network). Returns the
     results in share order; the first exception of any share is raised after all finish."""
     import threading
     import torch
