@@ -159,6 +159,17 @@ void ctx_release(ytf_ctx* ctx) {
   if (--ctx->refs <= 0 && ctx->closing) delete ctx;
 }
 
+// cudaMalloc that, when the device is out of memory, releases the context's pool of idle cache
+// blocks (every block enters the pool after its stream has finished with it) and tries once more
+cudaError_t dev_malloc(ytf_ctx* ctx, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaErrorMemoryAllocation || ctx->pool.empty()) return e;
+  cudaGetLastError();
+  for (auto& kv : ctx->pool) cudaFree(kv.second);
+  ctx->pool.clear();
+  return cudaMalloc(p, bytes);
+}
+
 // `reserve`: the size a first allocation takes at least (a buffer whose size varies from call to
 // call up to a known bound is allocated at the bound once, so that later calls do not pay a
 // cudaFree's device-wide synchronisation to grow it)
@@ -197,7 +208,7 @@ void* ws_get(ytf_ctx* ctx, const char* name_, size_t bytes, cudaError_t* e, size
     cudaGetLastError();
     p = nullptr;
   }
-  *e = cudaMalloc(&p, bytes);
+  *e = dev_malloc(ctx, &p, bytes);
   if (*e != cudaSuccess) return nullptr;
   ctx->ws[name] = {p, bytes};
   return p;
@@ -308,7 +319,7 @@ int alloc_cache(ytf_ctx* ctx, ytf_cache* c, bool upload_nodes = true) {
     c->block_bytes = it->first;
     ctx->pool.erase(it);
   } else {
-    CK(cudaMalloc(&c->block, off));
+    CK(dev_malloc(ctx, &c->block, off));
   }
   char* b = (char*)c->block;
   c->d_kr = (double*)(b + o_kr); c->d_wr = (double*)(b + o_wr);
