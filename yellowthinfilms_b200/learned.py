@@ -9,10 +9,11 @@ score — from a stack descriptor, the frequency and k. Its peaks are candidate 
 batched device call samples the EXACT response on a small window around every candidate,
 which fixes each pole's (q, Γ) for fixed_kρ_rule (ytf_nodes_from_poles) in place of the
 scan's thousands of samples and sequential refinement rounds. Every node of the resulting
-rule is then solved exactly by the transfer path. The plain method stays the judge and the fallback: a
-proposed rule is accepted only if it agrees with its own refinement (every panel halved) to
-the requested tolerance; otherwise the rule of one exact scan of the response is refined by
-halving until two levels agree (and the reference's scanned rule is the last resort).
+rule is then solved exactly by the transfer path. A proposed rule (Gauss–Legendre order 8) is
+accepted only if its G agrees to the requested tolerance with G on the same panels at order 10,
+and the order-10 rule is returned; otherwise the rule of one exact scan of the response is
+checked the same way, then refined by halving until two levels agree, the plain method's own
+check (and the reference's scanned rule is the last resort).
 
 Training data come from the solver itself: random stacks of the air / uniaxial film /
 substrate form, each scanned on a log kρ grid by ytf_cavity_response on the device.
@@ -291,7 +292,7 @@ def halved(stack, omega, panels, order, ctx=None):
 
 def learned_rule(net, stack, k0, source_layer, h_min, rho_max=0.0, order=8, rtol=1e-6, check=None, max_halvings=6,
                  ctx=None, check_order=10):
-    """The learned point rule with the plain method as judge and fallback.
+    """The learned point rule, with the plain method's refinement as the fallback.
 
     Proposes poles with the network, fixes them with one exact batched sampling, and builds
     fixed_kρ_rule on them. With ``check`` (a callable rule -> G) the rule is accepted when G
