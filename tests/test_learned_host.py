@@ -97,3 +97,46 @@ def test_vectorised_scan_grids_and_feature_rows_are_bit_identical():
             ref[19 * l + 18] = d[l] * k0 / (2 * np.pi)
         ref[-2] = k0 * L.LAMBDA_REF / (2 * np.pi)
         assert np.array_equal(L.feature_row(st, k0), ref.astype(np.float32))
+
+
+def test_refine_levels_with_a_check_order(monkeypatch):
+    """_refine_levels with check_order: the first level compares the order-8 rule with the
+    same panels at the check order and returns the latter on agreement; a problem that fails
+    keeps its order-8 rule and G, which the next levels halve until two levels agree. Rules and
+    G are stand-ins with a known error model: G = 1 + (panel width / scale)^order."""
+    from yellowthinfilms_b200 import learned as L
+
+    def fake_gl(sets, order, ctx=None, device=False):
+        # k: every panel's width repeated order times; w: the order
+        out = []
+        for p, _ in sets:
+            p = np.asarray(p, np.float64).reshape(-1, 2)
+            out.append((np.repeat(p[:, 1] - p[:, 0], order), np.full(len(p) * order, float(order))))
+        return out
+
+    def fake_G(problems, rules, ctx=None, device=False):
+        return [np.array([1.0 + (k.max() / P["scale"]) ** w[0]]) for P, (k, w) in zip(problems, rules)]
+
+    monkeypatch.setattr(L.api, "gl_rule_batch", fake_gl)
+    monkeypatch.setattr(L, "batch_G", fake_G)
+    panels = [np.array([[0.0, 1.0], [1.0, 2.0], [2.0, 3.0]]) for _ in range(2)]
+    # easy: (1/4)^8 - (1/4)^10 < 1e-3, accepted at the check; hard: (1/1.2)^8 vs (1/1.2)^10 is not,
+    # nor is halving once ((0.5/1.2)^8 against (1/1.2)^8); halving twice agrees
+    probs = [dict(scale=4.0, singular=[]), dict(scale=1.2, singular=[])]
+    rules = fake_gl([(p, []) for p in panels], 8)
+    out, solved = [None, None], [0, 0]
+    L._refine_levels(probs, range(2), rules, [p.copy() for p in panels], None, 1e-3, 4, 8, None, out, False, solved,
+                     check_order=10)
+    G, k, w, h, conv = out[0]
+    assert conv and h == 0 and w[0] == 10 and k.max() == 1.0 and len(k) == 30
+    assert solved[0] == 3 * 8 + 3 * 10
+    G, k, w, h, conv = out[1]
+    assert conv and h == 2 and w[0] == 8 and k.max() == 0.25 and len(k) == 12 * 8
+    assert G[0] == 1.0 + (0.25 / 1.2) ** 8
+    # the check level (8 + 10 nodes per panel), then the halved levels of the order-8 rule
+    assert solved[1] == 3 * 8 + 3 * 10 + 6 * 8 + 12 * 8
+    # without a check order the first level halves: the easy problem returns its halved rule
+    rules = fake_gl([(p, []) for p in panels], 8)
+    out, solved = [None, None], [0, 0]
+    L._refine_levels(probs[:1], range(1), rules[:1], [panels[0].copy()], None, 1e-3, 4, 8, None, out, False, solved)
+    assert out[0][4] and out[0][3] == 0 and out[0][2][0] == 8 and out[0][1].max() == 0.5 and solved[0] == 3 * 8 + 6 * 8
